@@ -1,0 +1,294 @@
+"""Benchmark of the GFMC branching step on B200 (walker-steps/s).
+
+Workload (the headline configuration): periodic 16x16 square-lattice
+Heisenberg model in the Marshall-rotated frame (J_x = J_y = -1, J_z = +1,
+512 bonds, M_total = 513), long-range Jastrow guide on all 32640 pairs with
+beta_ij = v(r_ij) = 0.3 / r (periodic minimum-image distance), 32768 walkers
+initialised as random Sz = 0 bitstrings, cont_time with tau = 0.05.  Inputs
+are synthetic (the configuration itself; no dataset is involved).
+
+A step is one production branching step (evolve + systematic resampling)
+over the whole population.  ``value`` times steps with the population
+resident in HBM; L2 is flushed (a 256 MB write) before every timed step, and
+each step is timed with CUDA events on the launching stream.  ``e2e`` times
+the same step through the C ABI with the walkers in pinned host memory
+(packed configurations copied in, and configurations, parent map and the
+step's log G / E copied out, every step).
+
+Multi-GPU (torchrun): every rank runs its own population (replicas, weak
+scaling, no data-path collective); time is the max over ranks.
+
+``--impl reference``: the reference's algorithm on the host cores -- PyGFMC
+itself is JAX-based and cannot run here, so its CPU restatement (``oracle/``,
+C + OpenMP on every host thread) runs a bounded sample of the same workload.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_WALKERS = 32768
+L = 16
+TAU = 0.05
+
+
+def build_system(P, precision):
+    lat = P.square(L)
+    H = P.SpinHalf.create(lat.edges, J_x=-1.0, J_y=-1.0, J_z=1.0, dtype=np.float64)
+    pos = lat.extras["positions"]
+    n = lat.N
+    iu = np.triu_indices(n, 1)
+    pairs = np.stack(iu, axis=1)
+    d = np.abs(pos[pairs[:, 0]] - pos[pairs[:, 1]])
+    d = np.minimum(d, L - d)
+    r = np.sqrt((d ** 2).sum(1))
+    G = P.JastrowSpinHalf(n, pairs, beta=0.3 / r)
+    return lat, H, G, pairs, 0.3 / r
+
+
+def sample_clocks(stop, out):
+    cmd = ["nvidia-smi", "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,"
+           "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+           "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+           "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits"]
+    while not stop.is_set():
+        try:
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=5)
+            if r.returncode == 0 and r.stdout.strip():
+                out.append(r.stdout.strip().splitlines()[0])
+        except Exception:
+            pass
+        stop.wait(0.2)
+
+
+def summarize_clocks(lines):
+    sm, mx, reasons = [], None, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for ln in lines:
+        f = [x.strip() for x in ln.split(",")]
+        if len(f) < 9:
+            continue
+        try:
+            sm.append(float(f[1]))
+            mx = float(f[2])
+        except ValueError:
+            continue
+        for nm, v in zip(names, f[5:9]):
+            if v.lower() == "active":
+                reasons.add(nm)
+    return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+            "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def cpu_reference(P, cfg_sample, alw, steps, warmup, seed_key):
+    """The oracle (C, OpenMP) on a sample of walkers: walker-steps/s."""
+    from oracle import oracle as O
+    O.build()
+    lat, H, G, pairs, beta = build_system(P, "fp64")
+    m = O.spin_half(lat.edges, J_x=-1.0, J_y=-1.0, J_z=1.0)
+    g = O.jastrow_spin_half(lat.N, pairs, beta, None, m)
+    cfg = np.array(cfg_sample, dtype=np.float64, copy=True)
+    lw = np.zeros(len(cfg)); el = np.zeros(len(cfg))
+    key = np.asarray(seed_key, np.uint32)
+    threads = O.lib().om_threads()
+    times = []
+    for s in range(warmup + steps):
+        key, r = O.split(key, 2)
+        k1, k2 = O.fold_in(r, 0), O.fold_in(r, 1)
+        t0 = time.perf_counter()
+        O.evolve(m, g, "cont_time", TAU, None, alw, k1, cfg, lw, el)
+        O.reconfigure(k2, cfg, lw, el)
+        if s >= warmup:
+            times.append(time.perf_counter() - t0)
+    return len(cfg) * steps / sum(times), threads, sum(times)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--walkers", type=int, default=N_WALKERS)
+    ap.add_argument("--cpu-sample", type=int, default=512)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    import pygfmc_b200 as P
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        w = P.prepare_walkers_sz(args.cpu_sample, L * L, P.PRNGKey(0), sz=0)
+        # alw: minus the mean local energy of the sample (what the warm-up starts from)
+        lat, H, G, pairs, beta = build_system(P, "fp64")
+        from oracle import oracle as O
+        O.build()
+        m = O.spin_half(lat.edges, J_x=-1.0, J_y=-1.0, J_z=1.0)
+        g = O.jastrow_spin_half(lat.N, pairs, beta, None, m)
+        alw = O.initial_alw(m, g, "cont_time", None, w.config)
+        steps = max(1, args.steps)
+        val, threads, secs = cpu_reference(P, w.config, alw, steps, min(args.warmup, 1), P.PRNGKey(7))
+        line = {"metric": "walker-steps/s", "value": val, "unit": "walker-steps/s", "n_gpus": 0,
+                "steps": steps, "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * secs / steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "impl": "reference",
+                "config": {"workload": "heisenberg_16x16_longrange_jastrow_cont_time",
+                           "n_walkers_sample": args.cpu_sample, "tau": TAU},
+                "cpu_baseline": {"value": val, "unit": "walker-steps/s", "cores": threads,
+                                 "kind": "port",
+                                 "sample": f"{args.cpu_sample} walkers x {steps} steps of the "
+                                           "headline workload (PyGFMC is JAX-based and not "
+                                           "runnable here; C restatement of its algorithm)"},
+                "e2e": {"value": val, "unit": "walker-steps/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    if world > 1:
+        import torch.distributed as dist
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device("cuda", torch.cuda.current_device())
+    lat, H, G, pairs, beta = build_system(P, args.precision)
+    n = args.walkers
+    w = P.prepare_walkers_sz(n, L * L, P.PRNGKey(rank), sz=0)
+    eng = P.GFMCEngine(H, G, n, precision=args.precision)
+    eng.load(w.config)
+    e0 = eng.local_energy()
+    alw = float((-e0).mean().item())
+    stream = torch.cuda.current_stream()
+    logG = torch.empty(1, dtype=torch.float64, device=dev)
+    Es = torch.empty(1, dtype=torch.float64, device=dev)
+    key = P.PRNGKey(1000 + rank)
+    # warm-up: equilibrate (also refines alw)
+    wk = max(args.warmup, 3)
+    keys, key = P.engine.key_schedule(key, wk)
+    lgw = torch.empty(wk, dtype=torch.float64, device=dev)
+    Ew = torch.empty(wk, dtype=torch.float64, device=dev)
+    eng.steps("cont_time", TAU, None, alw, keys, lgw, Ew)
+    torch.cuda.synchronize()
+    alw = alw + float(torch.logsumexp(lgw, 0).item() - np.log(wk)) / TAU
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    hops = torch.zeros(1, dtype=torch.int64, device=dev)
+    keys, key = P.engine.key_schedule(key, args.steps)
+
+    stop = threading.Event()
+    clock_lines = []
+    th = threading.Thread(target=sample_clocks, args=(stop, clock_lines), daemon=True)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    th.start()
+    step_ms = []
+    evolve_ms = []
+    total_hops = 0
+    for s in range(args.steps):
+        flush.fill_(float(s))
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        eng.steps("cont_time", TAU, None, alw, keys[s:s + 1], logG, Es, hops)
+        b.record(stream)
+        b.synchronize()
+        step_ms.append(a.elapsed_time(b))
+        total_hops += int(hops.item())
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    stop.set()
+    th.join(timeout=5)
+    t_step = float(np.sum(step_ms)) / 1e3
+    if world > 1:
+        t = torch.tensor([t_step], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        t_step = float(t.item())
+    value = n * args.steps * world / t_step
+    ms_per_step = 1e3 * t_step / args.steps
+
+    # ---- e2e: host-resident walkers through the C ABI, every step
+    import ctypes
+    packed_h = torch.empty(n * eng.cfg_bytes, dtype=torch.uint8, pin_memory=True)
+    packed_h.copy_(eng.cfg)
+    par_h = torch.empty(n, dtype=torch.int32, pin_memory=True)
+    out_h = torch.empty(2, dtype=torch.float64, pin_memory=True)
+    ident = torch.arange(n, dtype=torch.int32, device=dev)
+    e2e_steps = max(1, min(args.steps, 10))
+    keys2, key = P.engine.key_schedule(key, e2e_steps)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for s in range(e2e_steps):
+        eng.cfg.copy_(packed_h, non_blocking=True)
+        eng.parents.copy_(ident)
+        eng.parents_valid = 0
+        eng.steps("cont_time", TAU, None, alw, keys2[s:s + 1], logG, Es)
+        packed_h.copy_(eng.cfg, non_blocking=True)
+        par_h.copy_(eng.parents, non_blocking=True)
+        out_h[0:1].copy_(logG, non_blocking=True)
+        out_h[1:2].copy_(Es, non_blocking=True)
+        stream.synchronize()
+    t_e2e = time.perf_counter() - t0
+    e2e_val = n * e2e_steps / t_e2e * world
+
+    pk, pk_kind = peaks()
+    clocks = summarize_clocks(clock_lines)
+    C = eng.cfg_bytes
+    alg_bytes = 4 + 2 * C + 16 + (2 * C + 36)   # evolve (gather fused) + reconfiguration
+    achieved_gbs = alg_bytes * n / (ms_per_step / 1e3) / 1e9
+    line = {
+        "metric": "walker-steps/s", "value": value, "unit": "walker-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": wk, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+        "data": "synthetic",
+        "config": {"workload": "heisenberg_16x16_longrange_jastrow_cont_time", "n_walkers": n,
+                   "n_sites": 256, "n_bonds": 512, "jastrow_pairs": int(len(pairs)), "tau": TAU,
+                   "precision": args.precision, "l2": "flushed (256 MB write) before every timed step",
+                   "hops_per_walker_step": total_hops / (n * args.steps),
+                   "parallelism": f"replicas x{world}"},
+        "e2e": {"value": e2e_val, "unit": "walker-steps/s", "h2d_bytes_per_step": n * C,
+                "d2h_bytes_per_step": n * C + 4 * n + 16},
+        "gpu_launches": 5 * args.steps,
+        "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": pk["hbm_gbs"],
+                     "unit": "GB/s", "frac": achieved_gbs / pk["hbm_gbs"], "traffic": None,
+                     "peak_source": pk_kind,
+                     "note": f"algorithmic bytes per walker-step {alg_bytes} (packed configs "
+                             "in/out, parent index, weights, resampling); the step is "
+                             "compute-bound (float64 exp + guide-ratio arithmetic), see profiles/"},
+        "clocks": clocks,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        cfg_d, _ = eng.population()
+        sample = cfg_d[: args.cpu_sample].cpu().numpy()
+        val, threads, secs = cpu_reference(P, sample, alw, 2, 0, P.PRNGKey(7))
+        line["cpu_baseline"] = {"value": val, "unit": "walker-steps/s", "cores": threads,
+                                "kind": "port",
+                                "sample": f"{args.cpu_sample} equilibrated walkers x 2 steps "
+                                          f"({secs:.1f} s), C+OpenMP restatement of the reference"}
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

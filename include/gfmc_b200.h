@@ -1,0 +1,176 @@
+/*
+ * gfmc_b200.h -- C ABI of the B200 Green's-function Monte Carlo engine.
+ *
+ * The drop-in boundary behind pygfmc_b200.run(...), which mirrors PyGFMC's
+ * pygfmc.run (engine/multi_gpu.py:822-868 -> engine/driver.py:1148).  Plain C
+ * types only: host descriptors for the model and the guide, raw device
+ * pointers for walker state (e.g. torch.Tensor.data_ptr()), and a CUDA stream
+ * handle (e.g. torch.cuda.current_stream().cuda_stream).  Every function
+ * returns GFMC_OK (0) or a negative error code; gfmc_last_error() gives the
+ * message of the calling thread's last failure.
+ *
+ * Ownership: the caller owns every buffer it passes; the engine owns only
+ * its handle, the device copies of the tables and its scratch.  A handle is
+ * not thread-safe: use one handle per host thread / stream.
+ *
+ * Random numbers are the JAX Threefry-2x32 stream PyGFMC draws from, with
+ * its key semantics (split(key)[i] = fold_in(key, i)); fed the same keys and
+ * walkers, the float64 engine reproduces PyGFMC's trajectories.
+ */
+#ifndef GFMC_B200_H
+#define GFMC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GFMC_OK 0
+#define GFMC_ERR_INVALID (-1)     /* bad argument (ValueError in the Python layer) */
+#define GFMC_ERR_CUDA (-2)        /* a CUDA call failed */
+#define GFMC_ERR_UNSUPPORTED (-3) /* model/guide/method combination not built */
+#define GFMC_ERR_DEVICE (-4)      /* a kernel raised a status bit (see gfmc_read_status) */
+
+#define GFMC_MODEL_SPIN_HALF 0
+#define GFMC_MODEL_BOSE_HUBBARD 1
+
+#define GFMC_GUIDE_NONE 0
+#define GFMC_GUIDE_JASTROW_SPIN_HALF 1
+#define GFMC_GUIDE_JASTROW_BOSE_HUBBARD 2
+
+#define GFMC_METHOD_CONT_TIME 0
+#define GFMC_METHOD_SINGLE_STEP 1
+#define GFMC_METHOD_MULTI_STEP 2
+
+#define GFMC_PRECISION_FP64 0  /* every step quantity in float64 */
+#define GFMC_PRECISION_MIXED 1 /* rates, ratios, local energies in float32; weight
+                                  accumulators, resampling sums, energies in float64 */
+
+/* Device status bits (gfmc_read_status). */
+#define GFMC_STATUS_HOP_CAP 1     /* a walker hit the per-step iteration cap */
+#define GFMC_STATUS_BAD_CONFIG 2  /* a configuration value outside the model's basis */
+#define GFMC_STATUS_NONFINITE 4   /* non-finite mean branch weight (extinct population) */
+
+/* Model description (host arrays, float64, read during gfmc_create only).
+ * SpinHalf: the stored-sign fields of hamiltonian/SpinHalf.py:101-117
+ *   (jpm = (J_x+J_y)/4, jpmpm = (J_x-J_y)/4 per edge; jz one value when
+ *   uniform_jz, else per edge; hz = -h_z per site; hx_half = -h_x/2 per site;
+ *   n_hx in {0, N}, n_jpm in {0, n_edges}).
+ * BoseHubbard: hamiltonian/bose_hubbard.py:67-103 (t, eta per edge; U, mu per
+ *   site; hpm = -h_pm per site; n_hop, n_eta in {0, 2 n_edges}; n_hpm in {0, N}). */
+typedef struct {
+  int kind;
+  int n_sites, n_edges;
+  const int32_t *edge_i, *edge_j;
+  int n_hx, n_jpm, has_jz, uniform_jz, has_hz;
+  const double *jz, *jpm, *jpmpm, *hz, *hx_half;
+  int n_max, n_hop, n_eta, n_hpm, has_U, has_mu;
+  const double *t, *eta, *U, *mu, *hpm;
+} gfmc_model_desc;
+
+/* Guide description.
+ * JastrowSpinHalf (wavefunction/jastrow_spin_half.py:79-157): pair list with
+ *   pair_w = J = -beta per pair, h per site (NULL: zero).
+ * JastrowBoseHubbard (wavefunction/jastrow_bose_hubbard.py:97-125): pair list
+ *   with pair_w = the neighbour-sum weight (-beta per pair, or 1 for a tied
+ *   beta with beta_tied = 1, beta0 = beta); h_mode/d_mode 0 none, 1 tied
+ *   (h0/d0), 2 per site (h/d). */
+typedef struct {
+  int kind;
+  int n_pairs;
+  const int32_t *pair_i, *pair_j;
+  const double *pair_w;
+  const double *h;
+  int beta_tied;
+  double beta0;
+  int h_mode;
+  double h0;
+  int d_mode;
+  double d0;
+  const double *d;
+} gfmc_guide_desc;
+
+typedef struct gfmc_handle gfmc_handle;
+
+/* Builds the device tables of (model, guide) once -- the analogue of
+ * guide.build_cache(hamiltonian) (engine/evolution.py guide_cache:192) -- on
+ * the current CUDA device.  precision: GFMC_PRECISION_*. */
+int gfmc_create(const gfmc_model_desc *model, const gfmc_guide_desc *guide, int precision,
+                gfmc_handle **out);
+int gfmc_destroy(gfmc_handle *h);
+
+/* Bytes of one packed walker configuration: ceil(N/64) uint64 words for a
+ * spin-1/2 model (bit 1 = +1), ceil(N/16)*16 uint8 occupations for bosons. */
+int gfmc_config_bytes(const gfmc_handle *h);
+int gfmc_n_transitions(const gfmc_handle *h); /* M_total */
+
+/* Walker.config (float64, row-major (n, N), +-1 or occupations; device) <->
+ * packed device configurations. */
+int gfmc_pack(gfmc_handle *h, int n_walkers, const double *cfg, void *packed, void *stream);
+int gfmc_unpack(gfmc_handle *h, int n_walkers, const void *packed, double *cfg, void *stream);
+
+/* n_steps branching steps of the production/warm-up scan
+ * (engine/driver.py _make_prod_step_fn:194-342 main chain): per step s,
+ * evolve_walkers with key keys[4s..4s+1] (engine/evolution.py
+ * evolve_walkers:761, per-walker split) then reconfiguration with key
+ * keys[4s+2..4s+3] (walkers/reconfiguration.py:27).  keys is host memory.
+ * State: the packed configurations cfg (device) and the parent map of the
+ * last reconfiguration (device, n_walkers int32); the population is
+ * cfg[parents[i]].  parents_valid = 0 means identity (a fresh population).
+ * cfg_tmp is a second packed buffer of the same size.  log_w/e_loc (device,
+ * float64, n_walkers) receive the pre-resampling weights and local energies
+ * of the last step.  logG_out/E_out (device, float64, n_steps) receive
+ * log G_n = logsumexp(log_w) - log N and E_n = sum w e_L / sum w; hops_out
+ * (device, uint64, n_steps, nullable) the moves made per step.
+ * method: GFMC_METHOD_*; step = beta (cont_time) or the integer n_bra;
+ * lam is used by the discrete methods; alw = avg_log_weight. */
+int gfmc_run_steps(gfmc_handle *h, int method, double step, double lam, double alw, int n_steps,
+                   const uint32_t *keys, int n_walkers, void *cfg, void *cfg_tmp, int32_t *parents,
+                   int parents_valid, double *log_w, double *e_loc, double *logG_out,
+                   double *E_out, uint64_t *hops_out, void *stream);
+
+/* Local energies e_L(x) = sum of the guide-transformed rates
+ * (engine/estimators.py estimate_average_log_branch_weight:722-751 input) of
+ * cfg[parents[i]] (parents nullable). */
+int gfmc_local_energy(gfmc_handle *h, int n_walkers, const void *cfg, const int32_t *parents,
+                      double *e_loc, void *stream);
+
+/* Applies a parent map: cfg_out[i] = cfg_in[parents[i]], e_out[i] = e_in[parents[i]],
+ * log_w[i] = 0 (any output nullable except cfg_out). */
+int gfmc_gather(gfmc_handle *h, int n_walkers, const int32_t *parents, const void *cfg_in,
+                void *cfg_out, const double *e_in, double *e_out, double *log_w, void *stream);
+
+/* Windowed mixed estimator of the energy (engine/estimators.py
+ * _energy_and_diagonal_estimates:268-305) on the device in float64; p (host,
+ * n_p windows, each < n_steps), out (host, n_p).  Synchronises the stream. */
+int gfmc_windowed_energy(int n_steps, const double *logG, const double *E, int n_p, const int *p,
+                         double *out, void *stream);
+
+/* Per-walker, per-step cap on the propagator's iterations (default 2^22).
+ * A walker reaching it stops its step and raises GFMC_STATUS_HOP_CAP; the
+ * loop never runs unbounded.  No counterpart in PyGFMC (its while_loop is
+ * unbounded). */
+int gfmc_set_max_iters(gfmc_handle *h, int max_iters);
+
+/* Reads and clears the device status word (GFMC_STATUS_* bits); synchronises. */
+int gfmc_read_status(gfmc_handle *h, int *status_out, void *stream);
+
+/* Host-side key schedule of the production chain (engine/driver.py:218-221):
+ * key, rng = split(key); k1, k2 = fold_in(rng, 0), fold_in(rng, 1).  Writes
+ * keys_out[4 s .. 4 s + 3] = (k1, k2) for n_steps steps and the final key. */
+int gfmc_key_schedule(const uint32_t key[2], int n_steps, uint32_t *keys_out,
+                      uint32_t key_next[2]);
+/* Threefry-2x32 and fold_in on the host (jax key semantics). */
+int gfmc_threefry2x32(uint32_t k0, uint32_t k1, uint32_t c0, uint32_t c1, uint32_t out[2]);
+
+/* Message of the calling thread's last error (empty when none). */
+int gfmc_last_error(char *buf, size_t len);
+/* Library version string. */
+const char *gfmc_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GFMC_B200_H */

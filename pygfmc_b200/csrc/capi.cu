@@ -1,0 +1,541 @@
+// C ABI of the engine (include/gfmc_b200.h): table construction, the host
+// loop of a chunk of branching steps, and the small helpers around it.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/gfmc_b200.h"
+#include "engine.cuh"
+
+using namespace gfmc;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+#define GFMC_CUDA(expr)                                                                    \
+  do {                                                                                     \
+    cudaError_t _e = (expr);                                                               \
+    if (_e != cudaSuccess)                                                                 \
+      return fail(GFMC_ERR_CUDA, "%s failed: %s", #expr, cudaGetErrorString(_e));          \
+  } while (0)
+
+// One device allocation holding every table; the builder appends arrays.
+struct Arena {
+  std::vector<unsigned char> host;
+  size_t add(const void *p, size_t bytes) {
+    size_t o = (host.size() + 255) & ~size_t(255);
+    host.resize(o + bytes);
+    if (bytes) memcpy(host.data() + o, p, bytes);
+    return o;
+  }
+};
+
+template <typename T> std::vector<T> conv(const double *src, size_t n) {
+  std::vector<T> v(n);
+  for (size_t i = 0; i < n; ++i) v[i] = (T)src[i];
+  return v;
+}
+
+}  // namespace
+
+struct gfmc_handle {
+  int precision = 0;
+  int family = 0;
+  int max_iters = 1 << 22;
+  int N = 0, E = 0, M = 0;
+  int cfg_bytes = 0;
+  int n_max = 0;
+  void *d_tables = nullptr;
+  DevModel<double> m64{};
+  DevGuide<double> g64{};
+  DevModel<float> m32{};
+  DevGuide<float> g32{};
+  LaunchPlan plan{};
+  // scratch
+  int cap_n = 0, cap_steps = 0;
+  double *pmax = nullptr, *psum = nullptr, *pE = nullptr, *cdf = nullptr, *wbuf = nullptr;
+  int *plp = nullptr, *ctr = nullptr, *status = nullptr;
+  unsigned long long *hops = nullptr;
+};
+
+namespace {
+
+template <typename T>
+int build_tables(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_desc *gd,
+                 DevModel<T> &m, DevGuide<T> &g) {
+  const int N = md->n_sites, E = md->n_edges;
+  Arena A;
+  std::vector<uint32_t> edge(E);
+  for (int e = 0; e < E; ++e) {
+    int i = md->edge_i[e], j = md->edge_j[e];
+    if (i < 0 || j < 0 || i >= N || j >= N || i > 0xFFFF || j > 0xFFFF)
+      return fail(GFMC_ERR_INVALID, "edge %d = (%d, %d) out of range for N=%d", e, i, j, N);
+    edge[e] = (uint32_t)i | ((uint32_t)j << 16);
+  }
+  size_t o_edge = A.add(edge.data(), edge.size() * 4);
+  memset(&m, 0, sizeof(m));
+  memset(&g, 0, sizeof(g));
+  m.family = md->kind;
+  m.N = N;
+  m.E = E;
+  std::map<std::string, size_t> off;
+  auto put = [&](const char *name, const double *src, size_t n) {
+    if (src && n) {
+      std::vector<T> v = conv<T>(src, n);
+      off[name] = A.add(v.data(), n * sizeof(T));
+    }
+  };
+  if (md->kind == GFMC_MODEL_SPIN_HALF) {
+    m.n_hx = md->n_hx;
+    m.n_jpm = md->n_jpm;
+    m.has_jz = md->has_jz;
+    m.uniform_jz = md->uniform_jz;
+    m.has_hz = md->has_hz;
+    if ((m.n_hx != 0 && m.n_hx != N) || (m.n_jpm != 0 && m.n_jpm != E))
+      return fail(GFMC_ERR_INVALID, "SpinHalf layout: n_hx must be 0 or N, n_jpm 0 or n_edges");
+    if (m.n_jpm && (!md->jpm || !md->jpmpm)) return fail(GFMC_ERR_INVALID, "jpm/jpmpm missing");
+    if (m.n_hx && !md->hx_half) return fail(GFMC_ERR_INVALID, "hx_half missing");
+    if (m.has_jz && !md->jz) return fail(GFMC_ERR_INVALID, "jz missing");
+    if (m.has_hz && !md->hz) return fail(GFMC_ERR_INVALID, "hz missing");
+    m.M = 1 + m.n_hx + m.n_jpm;
+    put("jpm", md->jpm, m.n_jpm ? E : 0);
+    put("jpmpm", md->jpmpm, m.n_jpm ? E : 0);
+    put("jz", md->jz, m.has_jz ? (m.uniform_jz ? 1 : E) : 0);
+    put("hz", md->hz, m.has_hz ? N : 0);
+    put("hx_half", md->hx_half, m.n_hx ? N : 0);
+    h->cfg_bytes = ((N + 63) / 64) * 8;
+  } else if (md->kind == GFMC_MODEL_BOSE_HUBBARD) {
+    m.n_max = md->n_max;
+    m.n_hop = md->n_hop;
+    m.n_eta = md->n_eta;
+    m.n_hpm = md->n_hpm;
+    m.has_U = md->has_U;
+    m.has_mu = md->has_mu;
+    if (m.n_max < 1 || m.n_max > 255) return fail(GFMC_ERR_INVALID, "n_max must be in [1, 255]");
+    if ((m.n_hop != 0 && m.n_hop != 2 * E) || (m.n_eta != 0 && m.n_eta != 2 * E) ||
+        (m.n_hpm != 0 && m.n_hpm != N))
+      return fail(GFMC_ERR_INVALID, "BoseHubbard layout sizes inconsistent");
+    m.M = 1 + m.n_hop + m.n_eta + 2 * m.n_hpm;
+    put("t", md->t, m.n_hop ? E : 0);
+    put("eta", md->eta, m.n_eta ? E : 0);
+    put("U", md->U, m.has_U ? N : 0);
+    put("mu", md->mu, m.has_mu ? N : 0);
+    put("hpm", md->hpm, m.n_hpm ? N : 0);
+    h->cfg_bytes = ((N + 15) / 16) * 16;
+  } else {
+    return fail(GFMC_ERR_UNSUPPORTED, "unknown model kind %d", md->kind);
+  }
+  m.n_off = m.M - 1;
+
+  // ---- guide
+  int gk = gd ? gd->kind : GFMC_GUIDE_NONE;
+  if (gk == GFMC_GUIDE_JASTROW_SPIN_HALF && md->kind != GFMC_MODEL_SPIN_HALF)
+    return fail(GFMC_ERR_INVALID, "JastrowSpinHalf needs the SpinHalf transition layout");
+  if (gk == GFMC_GUIDE_JASTROW_BOSE_HUBBARD && md->kind != GFMC_MODEL_BOSE_HUBBARD)
+    return fail(GFMC_ERR_INVALID, "JastrowBoseHubbard needs a BoseHubbard operator");
+  if (gk != GFMC_GUIDE_NONE && gk != GFMC_GUIDE_JASTROW_SPIN_HALF &&
+      gk != GFMC_GUIDE_JASTROW_BOSE_HUBBARD)
+    return fail(GFMC_ERR_UNSUPPORTED, "unknown guide kind %d", gk);
+  g.kind = gk;
+  size_t o_nbr = 0, o_nbrw = 0, o_cnt = 0, o_jsum = 0, o_tpw = 0;
+  if (gk != GFMC_GUIDE_NONE) {
+    // per-site partner lists, duplicates merged (each partner once per site)
+    std::vector<std::map<int, double>> lists(N);
+    for (int p = 0; p < gd->n_pairs; ++p) {
+      int a = gd->pair_i[p], b = gd->pair_j[p];
+      if (a < 0 || b < 0 || a >= N || b >= N || a == b)
+        return fail(GFMC_ERR_INVALID, "pair %d = (%d, %d) invalid for N=%d", p, a, b, N);
+      lists[a][b] += gd->pair_w[p];
+      lists[b][a] += gd->pair_w[p];
+    }
+    int deg = 1;
+    for (auto &l : lists) deg = (int)l.size() > deg ? (int)l.size() : deg;
+    std::vector<uint32_t> nbr((size_t)N * deg, 0);
+    std::vector<T> nbrw((size_t)N * deg, T(0));
+    std::vector<int> cnt(N, 0);
+    for (int k = 0; k < N; ++k) {
+      int c = 0;
+      for (auto &kv : lists[k]) {
+        nbr[(size_t)k * deg + c] = (uint32_t)kv.first;
+        nbrw[(size_t)k * deg + c] = (T)kv.second;
+        ++c;
+      }
+      cnt[k] = c;
+    }
+    g.deg = deg;
+    o_nbr = A.add(nbr.data(), nbr.size() * 4);
+    o_nbrw = A.add(nbrw.data(), nbrw.size() * sizeof(T));
+    o_cnt = A.add(cnt.data(), cnt.size() * 4);
+    auto pair_sum = [&](int a, int b) -> double {
+      if (a == b) return 0.0;
+      auto it = lists[a].find(b);
+      return it == lists[a].end() ? 0.0 : it->second;
+    };
+    if (gk == GFMC_GUIDE_JASTROW_SPIN_HALF) {
+      std::vector<double> hh(N, 0.0);
+      if (gd->h) for (int k = 0; k < N; ++k) hh[k] = gd->h[k];
+      put("gh", hh.data(), N);
+      std::vector<T> js(E > 0 ? E : 1, T(0));
+      for (int e = 0; e < E; ++e) js[e] = (T)pair_sum(md->edge_i[e], md->edge_j[e]);
+      o_jsum = A.add(js.data(), js.size() * sizeof(T));
+    } else {
+      // per-transition summed pair weight (JastrowBoseHubbardOpCache.pair_w)
+      std::vector<T> tpw(m.M, T(0));
+      int t = 1;
+      int blocks = (m.n_hop ? 2 : 0) + (m.n_eta ? 2 : 0);
+      for (int b = 0; b < blocks; ++b)
+        for (int e = 0; e < E; ++e) tpw[t++] = (T)pair_sum(md->edge_i[e], md->edge_j[e]);
+      o_tpw = A.add(tpw.data(), tpw.size() * sizeof(T));
+      g.beta_scale = gd->beta_tied ? (T)(-gd->beta0) : T(1);
+      g.h_mode = gd->h_mode;
+      g.h0 = (T)gd->h0;
+      g.d_mode = gd->d_mode;
+      g.d0 = (T)gd->d0;
+      if (g.h_mode == 2) {
+        if (!gd->h) return fail(GFMC_ERR_INVALID, "h array missing");
+        put("gh", gd->h, N);
+      }
+      if (g.d_mode == 2) {
+        if (!gd->d) return fail(GFMC_ERR_INVALID, "d array missing");
+        put("gd", gd->d, N);
+      }
+    }
+  }
+
+  // ---- upload
+  GFMC_CUDA(cudaMalloc(&h->d_tables, A.host.size() ? A.host.size() : 256));
+  GFMC_CUDA(cudaMemcpy(h->d_tables, A.host.data(), A.host.size(), cudaMemcpyHostToDevice));
+  unsigned char *base = (unsigned char *)h->d_tables;
+  auto ptr = [&](const char *name) -> const T * {
+    auto it = off.find(name);
+    return it == off.end() ? nullptr : (const T *)(base + it->second);
+  };
+  m.edge = E ? (const uint32_t *)(base + o_edge) : nullptr;
+  m.jpm = ptr("jpm"); m.jpmpm = ptr("jpmpm"); m.jz = ptr("jz"); m.hz = ptr("hz");
+  m.hx_half = ptr("hx_half");
+  m.t = ptr("t"); m.eta = ptr("eta"); m.U = ptr("U"); m.mu = ptr("mu"); m.hpm = ptr("hpm");
+  if (gk != GFMC_GUIDE_NONE) {
+    g.nbr = (const uint32_t *)(base + o_nbr);
+    g.nbr_w = (const T *)(base + o_nbrw);
+    g.nbr_cnt = (const int *)(base + o_cnt);
+    g.h = ptr("gh");
+    g.d = ptr("gd");
+    if (gk == GFMC_GUIDE_JASTROW_SPIN_HALF) g.edge_jsum = (const T *)(base + o_jsum);
+    else g.trans_pw = (const T *)(base + o_tpw);
+  }
+  cudaError_t e = plan_evolve<T>(m, g, m.M, &h->plan);
+  if (e != cudaSuccess)
+    return fail(GFMC_ERR_CUDA, "planning the evolve kernel failed: %s", cudaGetErrorString(e));
+  return GFMC_OK;
+}
+
+int ensure_scratch(gfmc_handle *h, int n, int n_steps) {
+  int nb = recon_tiles(n);
+  if (n > h->cap_n) {
+    cudaFree(h->psum); cudaFree(h->cdf); cudaFree(h->wbuf); cudaFree(h->plp);
+    h->psum = h->cdf = h->wbuf = nullptr; h->plp = nullptr;
+    GFMC_CUDA(cudaMalloc(&h->psum, sizeof(double) * nb));
+    GFMC_CUDA(cudaMalloc(&h->plp, sizeof(int) * nb));
+    GFMC_CUDA(cudaMalloc(&h->cdf, sizeof(double) * n));
+    GFMC_CUDA(cudaMalloc(&h->wbuf, sizeof(double) * n));
+    cudaFree(h->pE);
+    h->pE = nullptr;
+    h->cap_steps = 0;
+    h->cap_n = n;
+  }
+  int nbc = recon_tiles(h->cap_n);
+  if (n_steps > h->cap_steps) {
+    cudaFree(h->pE); cudaFree(h->ctr); cudaFree(h->hops);
+    h->pE = nullptr; h->ctr = nullptr; h->hops = nullptr;
+    GFMC_CUDA(cudaMalloc(&h->pE, sizeof(double) * (size_t)nbc * n_steps));
+    GFMC_CUDA(cudaMalloc(&h->ctr, sizeof(int) * n_steps));
+    GFMC_CUDA(cudaMalloc(&h->hops, sizeof(unsigned long long) * n_steps));
+    h->cap_steps = n_steps;
+  }
+  if (!h->pmax) GFMC_CUDA(cudaMalloc(&h->pmax, sizeof(double) * (h->plan.grid > 0 ? h->plan.grid : 1)));
+  if (!h->status) {
+    GFMC_CUDA(cudaMalloc(&h->status, sizeof(int)));
+    GFMC_CUDA(cudaMemset(h->status, 0, sizeof(int)));
+  }
+  return GFMC_OK;
+}
+
+template <typename T>
+int run_steps_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, int method,
+                double step, double lam, double alw, int n_steps, const uint32_t *keys, int n,
+                void *cfg, void *cfg_tmp, int32_t *parents, int parents_valid, double *log_w,
+                double *e_loc, double *logG_out, double *E_out, uint64_t *hops_out,
+                cudaStream_t s) {
+  int rc = ensure_scratch(h, n, n_steps);
+  if (rc) return rc;
+  const int nb = recon_tiles(n);
+  const int nbc = recon_tiles(h->cap_n);
+  GFMC_CUDA(cudaMemsetAsync(h->ctr, 0, sizeof(int) * n_steps, s));
+  unsigned long long *hops = hops_out ? (unsigned long long *)hops_out : h->hops;
+  GFMC_CUDA(cudaMemsetAsync(hops, 0, sizeof(unsigned long long) * n_steps, s));
+  int grid = h->plan.grid;
+  int need = (n + h->plan.wpb - 1) / h->plan.wpb;
+  if (grid > need) grid = need;
+  void *cur = cfg, *nxt = cfg_tmp;
+  for (int st = 0; st < n_steps; ++st) {
+    EvolveArgs a{};
+    a.method = method;
+    a.step = step;
+    a.lam = lam;
+    a.alw = alw;
+    a.key = Key{keys[4 * st + 0], keys[4 * st + 1]};
+    a.n_walkers = n;
+    a.parents = (st == 0 && !parents_valid) ? nullptr : parents;
+    a.cfg_in = cur;
+    a.cfg_out = nxt;
+    a.log_w = log_w;
+    a.e_loc = e_loc;
+    a.hops = hops + st;
+    a.work_ctr = h->ctr + st;
+    a.partial_max = h->pmax;
+    a.status = h->status;
+    a.max_iters = h->max_iters;
+    cudaError_t e = launch_evolve<T>(m, g, h->plan, a, s);
+    if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "evolve launch: %s", cudaGetErrorString(e));
+    ReconArgs r{};
+    r.n = n;
+    r.log_w = log_w;
+    r.e_loc = e_loc;
+    r.partial_max = h->pmax;
+    r.n_partial_max = grid;
+    r.key = Key{keys[4 * st + 2], keys[4 * st + 3]};
+    r.psum = h->psum;
+    r.pE = h->pE + (size_t)st * nb;
+    r.plp = h->plp;
+    r.cdf = h->cdf;
+    r.wbuf = h->wbuf;
+    r.parents = parents;
+    r.logG_out = logG_out + st;
+    r.status = h->status;
+    e = launch_reconfigure(r, s);
+    if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "reconfigure launch: %s", cudaGetErrorString(e));
+    void *t = cur; cur = nxt; nxt = t;
+  }
+  (void)nbc;
+  cudaError_t e = launch_series_reduce(h->pE, nb, n_steps, E_out, s);
+  if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "series reduce: %s", cudaGetErrorString(e));
+  if (cur != cfg)
+    GFMC_CUDA(cudaMemcpyAsync(cfg, cur, (size_t)n * h->cfg_bytes, cudaMemcpyDeviceToDevice, s));
+  return GFMC_OK;
+}
+
+template <typename T>
+int local_energy_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, int n,
+                   const void *cfg, const int32_t *parents, double *e_loc, cudaStream_t s) {
+  int rc = ensure_scratch(h, n, 1);
+  if (rc) return rc;
+  GFMC_CUDA(cudaMemsetAsync(h->ctr, 0, sizeof(int), s));
+  EvolveArgs a{};
+  a.method = EVALUATE;
+  a.n_walkers = n;
+  a.parents = parents;
+  a.cfg_in = cfg;
+  a.cfg_out = nullptr;
+  a.log_w = nullptr;
+  a.e_loc = e_loc;
+  a.hops = nullptr;
+  a.work_ctr = h->ctr;
+  a.partial_max = nullptr;
+  a.status = h->status;
+  a.max_iters = 1;
+  cudaError_t e = launch_evolve<T>(m, g, h->plan, a, s);
+  if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "local energy launch: %s", cudaGetErrorString(e));
+  return GFMC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gfmc_create(const gfmc_model_desc *model, const gfmc_guide_desc *guide, int precision,
+                gfmc_handle **out) {
+  if (!model || !out) return fail(GFMC_ERR_INVALID, "null argument");
+  if (model->n_sites <= 0) return fail(GFMC_ERR_INVALID, "n_sites must be positive");
+  if (model->n_sites > 65535) return fail(GFMC_ERR_UNSUPPORTED, "at most 65535 sites");
+  if (precision != GFMC_PRECISION_FP64 && precision != GFMC_PRECISION_MIXED)
+    return fail(GFMC_ERR_INVALID, "unknown precision %d", precision);
+  gfmc_handle *h = new gfmc_handle();
+  h->precision = precision;
+  h->family = model->kind;
+  h->N = model->n_sites;
+  h->E = model->n_edges;
+  h->n_max = model->n_max;
+  int rc = precision == GFMC_PRECISION_FP64 ? build_tables<double>(h, model, guide, h->m64, h->g64)
+                                            : build_tables<float>(h, model, guide, h->m32, h->g32);
+  if (rc) {
+    gfmc_destroy(h);
+    return rc;
+  }
+  h->M = precision == GFMC_PRECISION_FP64 ? h->m64.M : h->m32.M;
+  *out = h;
+  g_last_error.clear();
+  return GFMC_OK;
+}
+
+int gfmc_destroy(gfmc_handle *h) {
+  if (!h) return GFMC_OK;
+  cudaFree(h->d_tables);
+  cudaFree(h->pmax); cudaFree(h->psum); cudaFree(h->pE); cudaFree(h->cdf); cudaFree(h->wbuf);
+  cudaFree(h->plp); cudaFree(h->ctr); cudaFree(h->status); cudaFree(h->hops);
+  delete h;
+  return GFMC_OK;
+}
+
+int gfmc_config_bytes(const gfmc_handle *h) { return h ? h->cfg_bytes : GFMC_ERR_INVALID; }
+int gfmc_n_transitions(const gfmc_handle *h) { return h ? h->M : GFMC_ERR_INVALID; }
+
+int gfmc_pack(gfmc_handle *h, int n, const double *cfg, void *packed, void *stream) {
+  if (!h || n < 0 || (n && (!cfg || !packed))) return fail(GFMC_ERR_INVALID, "gfmc_pack: bad argument");
+  if (!h->status) {
+    GFMC_CUDA(cudaMalloc(&h->status, sizeof(int)));
+    GFMC_CUDA(cudaMemset(h->status, 0, sizeof(int)));
+  }
+  if (n == 0) return GFMC_OK;
+  cudaError_t e = launch_pack(h->family, n, h->N, h->cfg_bytes, cfg, packed, h->n_max, h->status,
+                              (cudaStream_t)stream);
+  if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "pack: %s", cudaGetErrorString(e));
+  return GFMC_OK;
+}
+
+int gfmc_unpack(gfmc_handle *h, int n, const void *packed, double *cfg, void *stream) {
+  if (!h || n < 0 || (n && (!cfg || !packed))) return fail(GFMC_ERR_INVALID, "gfmc_unpack: bad argument");
+  if (n == 0) return GFMC_OK;
+  cudaError_t e = launch_unpack(h->family, n, h->N, h->cfg_bytes, packed, cfg, (cudaStream_t)stream);
+  if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "unpack: %s", cudaGetErrorString(e));
+  return GFMC_OK;
+}
+
+int gfmc_run_steps(gfmc_handle *h, int method, double step, double lam, double alw, int n_steps,
+                   const uint32_t *keys, int n_walkers, void *cfg, void *cfg_tmp, int32_t *parents,
+                   int parents_valid, double *log_w, double *e_loc, double *logG_out,
+                   double *E_out, uint64_t *hops_out, void *stream) {
+  if (!h) return fail(GFMC_ERR_INVALID, "null handle");
+  if (n_steps <= 0 || n_walkers <= 0) return fail(GFMC_ERR_INVALID, "n_steps and n_walkers must be positive");
+  if (!keys || !cfg || !cfg_tmp || !parents || !log_w || !e_loc || !logG_out || !E_out)
+    return fail(GFMC_ERR_INVALID, "gfmc_run_steps: null buffer");
+  if (method < 0 || method > 2) return fail(GFMC_ERR_INVALID, "unknown method %d", method);
+  if (method != GFMC_METHOD_CONT_TIME && (step < 1.0 || step != (double)(long long)step))
+    return fail(GFMC_ERR_INVALID, "discrete methods need a positive integer step");
+  if (!(step > 0.0)) return fail(GFMC_ERR_INVALID, "step must be > 0");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (h->precision == GFMC_PRECISION_FP64)
+    return run_steps_t<double>(h, h->m64, h->g64, method, step, lam, alw, n_steps, keys, n_walkers,
+                               cfg, cfg_tmp, parents, parents_valid, log_w, e_loc, logG_out, E_out,
+                               hops_out, s);
+  return run_steps_t<float>(h, h->m32, h->g32, method, step, lam, alw, n_steps, keys, n_walkers, cfg,
+                            cfg_tmp, parents, parents_valid, log_w, e_loc, logG_out, E_out,
+                            hops_out, s);
+}
+
+int gfmc_local_energy(gfmc_handle *h, int n, const void *cfg, const int32_t *parents,
+                      double *e_loc, void *stream) {
+  if (!h || n <= 0 || !cfg || !e_loc) return fail(GFMC_ERR_INVALID, "gfmc_local_energy: bad argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (h->precision == GFMC_PRECISION_FP64)
+    return local_energy_t<double>(h, h->m64, h->g64, n, cfg, parents, e_loc, s);
+  return local_energy_t<float>(h, h->m32, h->g32, n, cfg, parents, e_loc, s);
+}
+
+int gfmc_gather(gfmc_handle *h, int n, const int32_t *parents, const void *cfg_in, void *cfg_out,
+                const double *e_in, double *e_out, double *log_w, void *stream) {
+  if (!h || n <= 0 || !cfg_in || !cfg_out || cfg_in == cfg_out)
+    return fail(GFMC_ERR_INVALID, "gfmc_gather: bad argument");
+  cudaError_t e = launch_gather(n, h->cfg_bytes, parents, cfg_in, cfg_out, e_in, e_out, log_w,
+                                (cudaStream_t)stream);
+  if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "gather: %s", cudaGetErrorString(e));
+  return GFMC_OK;
+}
+
+int gfmc_windowed_energy(int n_steps, const double *logG, const double *E, int n_p, const int *p,
+                         double *out, void *stream) {
+  if (n_steps <= 0 || n_p <= 0 || !logG || !E || !p || !out)
+    return fail(GFMC_ERR_INVALID, "gfmc_windowed_energy: bad argument");
+  for (int i = 0; i < n_p; ++i)
+    if (p[i] <= 0 || p[i] >= n_steps)
+      return fail(GFMC_ERR_INVALID, "window p=%d must lie in [1, n_steps)", p[i]);
+  cudaStream_t s = (cudaStream_t)stream;
+  int *dp = nullptr;
+  double *work = nullptr;
+  GFMC_CUDA(cudaMalloc(&dp, sizeof(int) * n_p));
+  cudaError_t e = cudaMalloc(&work, sizeof(double) * (n_steps + n_p));
+  if (e != cudaSuccess) { cudaFree(dp); return fail(GFMC_ERR_CUDA, "windowed alloc: %s", cudaGetErrorString(e)); }
+  e = cudaMemcpyAsync(dp, p, sizeof(int) * n_p, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = launch_windowed(logG, E, n_steps, dp, n_p, work, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(out, work + n_steps, sizeof(double) * n_p, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFree(dp);
+  cudaFree(work);
+  if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "windowed energy: %s", cudaGetErrorString(e));
+  return GFMC_OK;
+}
+
+int gfmc_set_max_iters(gfmc_handle *h, int max_iters) {
+  if (!h || max_iters < 1) return fail(GFMC_ERR_INVALID, "max_iters must be >= 1");
+  h->max_iters = max_iters;
+  return GFMC_OK;
+}
+
+int gfmc_read_status(gfmc_handle *h, int *status_out, void *stream) {
+  if (!h || !status_out) return fail(GFMC_ERR_INVALID, "gfmc_read_status: bad argument");
+  *status_out = 0;
+  if (!h->status) return GFMC_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  int v = 0;
+  GFMC_CUDA(cudaMemcpyAsync(&v, h->status, sizeof(int), cudaMemcpyDeviceToHost, s));
+  GFMC_CUDA(cudaStreamSynchronize(s));
+  GFMC_CUDA(cudaMemsetAsync(h->status, 0, sizeof(int), s));
+  *status_out = v;
+  return GFMC_OK;
+}
+
+int gfmc_key_schedule(const uint32_t key[2], int n_steps, uint32_t *keys_out, uint32_t key_next[2]) {
+  if (!key || n_steps < 0 || (n_steps && !keys_out) || !key_next)
+    return fail(GFMC_ERR_INVALID, "gfmc_key_schedule: bad argument");
+  Key k{key[0], key[1]};
+  for (int s = 0; s < n_steps; ++s) {
+    Key nk = fold(k, 0u), rng = fold(k, 1u);
+    Key k1 = fold(rng, 0u), k2 = fold(rng, 1u);
+    keys_out[4 * s + 0] = k1.a; keys_out[4 * s + 1] = k1.b;
+    keys_out[4 * s + 2] = k2.a; keys_out[4 * s + 3] = k2.b;
+    k = nk;
+  }
+  key_next[0] = k.a;
+  key_next[1] = k.b;
+  return GFMC_OK;
+}
+
+int gfmc_threefry2x32(uint32_t k0, uint32_t k1, uint32_t c0, uint32_t c1, uint32_t out[2]) {
+  if (!out) return fail(GFMC_ERR_INVALID, "null output");
+  threefry2x32(k0, k1, c0, c1, out[0], out[1]);
+  return GFMC_OK;
+}
+
+int gfmc_last_error(char *buf, size_t len) {
+  if (!buf || !len) return GFMC_ERR_INVALID;
+  snprintf(buf, len, "%s", g_last_error.c_str());
+  return GFMC_OK;
+}
+
+const char *gfmc_version(void) { return "gfmc_b200 0.1.0 (sm_100a)"; }
+
+}  // extern "C"

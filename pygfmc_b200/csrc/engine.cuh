@@ -1,0 +1,122 @@
+// Internal interfaces of the GFMC engine: device-resident model and guide
+// tables, kernel parameter blocks and the launchers the C ABI calls.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "gfmc_device.cuh"
+
+namespace gfmc {
+
+enum Family { SPIN_HALF = 0, BOSE_HUBBARD = 1 };
+enum Method { CONT_TIME = 0, SINGLE_STEP = 1, MULTI_STEP = 2, EVALUATE = 3 };
+enum GuideKind { GUIDE_NONE = 0, GUIDE_JASTROW_SPIN = 1, GUIDE_JASTROW_BOSE = 2 };
+
+// Status bits the kernels raise (atomicOr into a device word).
+enum StatusBits {
+  ST_HOP_CAP = 1,        // a walker hit the per-step iteration cap
+  ST_BAD_CONFIG = 2,     // an occupation outside [0, n_max] (Bose-Hubbard)
+  ST_NONFINITE = 4,      // non-finite population weight in reconfiguration
+};
+
+// Model tables (device pointers).  Couplings follow the stored-sign
+// conventions of hamiltonian/SpinHalf.py:101-117 and
+// hamiltonian/bose_hubbard.py:67-103.
+template <typename T> struct DevModel {
+  int family;
+  int N, E, M;            // sites, edges, M_total
+  int n_off;              // M - 1
+  const uint32_t *edge;   // (E,) packed ei | ej << 16
+  // SpinHalf
+  int n_hx, n_jpm, has_jz, uniform_jz, has_hz;
+  const T *jz, *jpm, *jpmpm, *hz, *hx_half;
+  // BoseHubbard
+  int n_max, n_hop, n_eta, n_hpm, has_U, has_mu;
+  const T *t, *eta, *U, *mu, *hpm;
+};
+
+// Guide tables.  Per-site partner lists (deduplicated; each partner at most
+// once per site) carry the coupling the incremental field update needs:
+//   spin-1/2 Jastrow: W_k = sum_p J_kp x_p, J = -beta
+//   Bose-Hubbard Jastrow: S_k = sum_p w_kp n_p, w = -beta (1 for tied beta)
+template <typename T> struct DevGuide {
+  int kind;
+  int deg;                // row stride of the partner tables
+  const uint32_t *nbr;    // (N, deg) partner sites
+  const T *nbr_w;         // (N, deg) couplings
+  const int *nbr_cnt;     // (N,) partners per site
+  const T *h;             // (N,) one-body field (spin: JastrowSpinHalf.h)
+  const T *edge_jsum;     // (E,) spin: summed J of the pairs joining each H edge
+  const T *trans_pw;      // (M,) bose: summed pair weight joining each transition's sites
+  T beta_scale;           // bose: -beta for a tied beta, else 1
+  int h_mode;             // bose: 0 none, 1 tied (h0), 2 array (h)
+  T h0;
+  int d_mode;             // bose: 0 none, 1 tied (d0), 2 array (d)
+  T d0;
+  const T *d;
+};
+
+struct EvolveArgs {
+  int method;
+  double step;            // beta (cont_time) or n_bra (discrete)
+  double lam;
+  double alw;
+  Key key;                // the step's evolve key (split over walkers)
+  int n_walkers;
+  const int *parents;     // gather map applied on load (nullptr: identity)
+  const void *cfg_in;
+  void *cfg_out;
+  double *log_w;
+  double *e_loc;
+  unsigned long long *hops;   // per-step hop counter (nullable)
+  int *work_ctr;          // zeroed work counter of this launch
+  double *partial_max;    // (grid,) block max of log_w
+  int *status;
+  int max_iters;          // per-walker hop cap
+};
+
+struct LaunchPlan {
+  int grid, block, wpb;   // blocks, threads per block, warps per block
+  size_t smem;            // dynamic shared memory bytes
+};
+
+// Launchers (evolve.cu).
+template <typename T>
+cudaError_t launch_evolve(const DevModel<T> &m, const DevGuide<T> &g, const LaunchPlan &plan,
+                          const EvolveArgs &a, cudaStream_t s);
+template <typename T>
+cudaError_t plan_evolve(const DevModel<T> &m, const DevGuide<T> &g, int n_slots_max,
+                        LaunchPlan *plan);
+
+// Reconfiguration (reconfig.cu), always float64.
+struct ReconArgs {
+  int n;                  // walkers
+  const double *log_w;
+  const double *e_loc;
+  const double *partial_max;
+  int n_partial_max;
+  Key key;                // the step's reconfiguration key
+  double *psum;           // (nb,)
+  double *pE;             // (nb,) per-step partial weighted energies
+  int *plp;               // (nb,) last positive index per tile
+  double *cdf;            // (n,)
+  double *wbuf;           // (n,)
+  int *parents;           // (n,) output
+  double *logG_out;       // scalar slot of this step
+  int *status;
+};
+int recon_tiles(int n);
+cudaError_t launch_reconfigure(const ReconArgs &a, cudaStream_t s);
+cudaError_t launch_series_reduce(const double *pE, int nb, int n_steps, double *E_out,
+                                 cudaStream_t s);
+cudaError_t launch_gather(int n, int cfg_bytes, const int *parents, const void *cfg_in,
+                          void *cfg_out, const double *e_in, double *e_out, double *log_w,
+                          cudaStream_t s);
+cudaError_t launch_windowed(const double *logG, const double *E, int n_steps, const int *p,
+                            int n_p, double *out, cudaStream_t s);
+cudaError_t launch_pack(int family, int n, int N, int cfg_bytes, const double *cfg,
+                        void *packed, int n_max, int *status, cudaStream_t s);
+cudaError_t launch_unpack(int family, int n, int N, int cfg_bytes, const void *packed,
+                          double *cfg, cudaStream_t s);
+
+}  // namespace gfmc

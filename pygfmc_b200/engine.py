@@ -1,0 +1,637 @@
+"""The GFMC driver: ``run`` / ``run_gfmc`` on one B200.
+
+Mirrors PyGFMC's ``engine/multi_gpu.py run:822-868`` and
+``engine/driver.py run_gfmc:1148-1547``: the same arguments, validation
+order and errors, warm-up ramp (``_warmup_schedule:567``, side-streams
+``_warmup_stage_key:48``), production key recurrence (``key, rng =
+split(key); k1, k2 = fold_in(rng, 0/1)``, ``driver.py:218-221``), population
+checks (``_check_population:913``) and return tuple ``(walkers, energy, obs,
+stats, raw)``.  The per-step work runs in the CUDA engine through its C ABI
+(``include/gfmc_b200.h``); this module only orchestrates chunks of steps,
+pulls the per-step series and assembles the results.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import secrets
+import time
+from types import SimpleNamespace
+
+import numpy as np
+
+from . import _lib
+from . import random as _rnd
+from .hamiltonian import BoseHubbard, SpinHalf
+from .walkers import Walker
+from .wavefunction import JastrowBoseHubbard, JastrowSpinHalf
+from .estimators import autocorrelation_stats, validated_p_array, windowed_energy_host
+
+__all__ = ["run", "run_gfmc", "GFMCEngine", "DEFAULT_WARMUP_STEPS"]
+
+DEFAULT_WARMUP_STEPS = 1000
+_AUX_ROOT = 9_000
+_WARMUP_CHUNK = 50
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise _lib.GFMCError("pygfmc_b200 needs a CUDA device (B200, sm_100a); none is visible -- "
+                             "there is no CPU fallback")
+    return torch
+
+
+def _emit(msg, verbosity, level=1):
+    if verbosity >= level:
+        print(msg, flush=True)
+
+
+def _validated_int(name, value, minimum):
+    """_validation.py _validated_int:7-19."""
+    if isinstance(value, (bool, np.bool_)):
+        raise ValueError(f"{name} must be an integer >= {minimum}, got {value!r}.")
+    try:
+        result = int(value)
+        ok = float(result) == float(value)
+    except (TypeError, ValueError, OverflowError):
+        ok, result = False, minimum - 1
+    if not ok or result < minimum:
+        raise ValueError(f"{name} must be an integer >= {minimum}, got {value!r}.")
+    return result
+
+
+def require_step_size(method, step_size):
+    """engine/evolution.py require_step_size:744-758."""
+    if not math.isfinite(float(step_size)):
+        raise ValueError(f"step_size must be finite; got step_size={step_size!r}")
+    if not (float(step_size) > 0):
+        raise ValueError(f"step_size must be > 0; got step_size={step_size!r}")
+    if method != "cont_time" and float(int(step_size)) != float(step_size):
+        raise ValueError(f"method={method!r} requires an integer step_size; got step_size={step_size!r}")
+
+
+def require_lam(method, lam):
+    """engine/evolution.py require_lam:724-741."""
+    if method == "cont_time":
+        return None
+    if method in ("single_step", "multi_step"):
+        if lam is None:
+            raise ValueError(
+                f"method={method!r} needs the GFMC shift: pass lam=<float> with lam >= max_x H_xx "
+                "over the reachable configurations (cont_time is the only method that does without it).")
+        v = float(lam)
+        if not math.isfinite(v):
+            raise ValueError(f"lam must be finite; got lam={lam!r}")
+        return v
+    raise ValueError(f"Unknown method: {method!r}")
+
+
+# ---- lowering of host objects to the C descriptors ---------------------------
+class _Keep:
+    """Keeps the numpy arrays a descriptor points into alive."""
+
+    def __init__(self):
+        self.arrays = []
+
+    def f64(self, a):
+        a = np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+        self.arrays.append(a)
+        return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+    def i32(self, a):
+        a = np.ascontiguousarray(np.asarray(a, dtype=np.int32))
+        self.arrays.append(a)
+        return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+
+
+def _is_spin_half(op):
+    return all(hasattr(op, a) for a in ("n_hx_static", "n_jpm_static", "edge_i", "edge_j",
+                                        "J_pm", "J_pmpm", "J_z"))
+
+
+def _is_bose(op):
+    return all(hasattr(op, a) for a in ("n_hop_off", "n_eta_off", "n_hpm_off", "n_max", "edge_i"))
+
+
+def require_operator_protocol(op, role="hamiltonian"):
+    """The engine runs the SpinHalf and BoseHubbard layouts; anything else is
+    refused up front (engine/evolution.py require_operator_protocol:62-92)."""
+    missing = [n for n in ("M_total", "get_rates") if not hasattr(op, n)]
+    if missing:
+        raise TypeError(f"{role} {type(op).__name__!r} is missing required attribute(s) "
+                        f"{', '.join(missing)}; the operator protocol (pygfmc.Operator) requires "
+                        "M_total, get_rates.")
+    if not (_is_spin_half(op) or _is_bose(op)):
+        raise TypeError(f"{role} {type(op).__name__!r} is not a SpinHalf or BoseHubbard operator; "
+                        "the B200 engine has device kernels for those two transition layouts only.")
+
+
+def require_guide_protocol(guide):
+    if guide is None:
+        return
+    if not any(hasattr(guide, n) for n in ("log_diff_from_operator", "log_diff_from_configs", "log_psi")):
+        raise TypeError(f"Guide {type(guide).__name__!r} must implement at least one of "
+                        "log_diff_from_operator, log_diff_from_configs, or log_psi "
+                        "(the guide protocol, pygfmc.Guide).")
+    if not isinstance(guide, (JastrowSpinHalf, JastrowBoseHubbard)) and \
+            not hasattr(guide, "_gfmc_guide_desc"):
+        raise TypeError(f"Guide {type(guide).__name__!r} has no device implementation in the B200 "
+                        "engine (supported: JastrowSpinHalf, JastrowBoseHubbard).")
+
+
+def model_desc(op, keep):
+    d = _lib.ModelDesc()
+    E = int(len(op.edge_i))
+    N = int(op.N)
+    d.n_sites, d.n_edges = N, E
+    d.edge_i, d.edge_j = keep.i32(op.edge_i), keep.i32(op.edge_j)
+    if _is_spin_half(op):
+        d.kind = _lib.MODEL_SPIN_HALF
+        d.n_hx, d.n_jpm = int(op.n_hx_static), int(op.n_jpm_static)
+        d.has_jz, d.uniform_jz, d.has_hz = int(op.has_jz), int(op.uniform_jz), int(op.has_hz)
+        jz = np.asarray(op.J_z, np.float64)
+        d.jz = keep.f64(jz[:1] if op.uniform_jz else np.broadcast_to(jz, (E,)))
+        d.jpm = keep.f64(np.broadcast_to(np.asarray(op.J_pm, np.float64), (E,)) if E else np.zeros(1))
+        d.jpmpm = keep.f64(np.broadcast_to(np.asarray(op.J_pmpm, np.float64), (E,)) if E else np.zeros(1))
+        if op.h_z is not None:
+            d.hz = keep.f64(np.broadcast_to(np.asarray(op.h_z, np.float64), (N,)))
+        if op.h_x_half is not None:
+            d.hx_half = keep.f64(np.broadcast_to(np.asarray(op.h_x_half, np.float64), (N,)))
+    else:
+        d.kind = _lib.MODEL_BOSE_HUBBARD
+        d.n_max = int(op.n_max)
+        d.n_hop, d.n_eta, d.n_hpm = int(op.n_hop_off), int(op.n_eta_off), int(op.n_hpm_off)
+        d.has_U, d.has_mu = int(op.has_U), int(op.has_mu)
+        if E:
+            d.t = keep.f64(np.broadcast_to(np.asarray(op.t, np.float64), (E,)))
+            d.eta = keep.f64(np.broadcast_to(np.asarray(op.eta, np.float64), (E,)))
+        d.U = keep.f64(np.broadcast_to(np.asarray(op.U, np.float64), (N,)))
+        d.mu = keep.f64(np.broadcast_to(np.asarray(op.mu, np.float64), (N,)))
+        if op.h_pm is not None:
+            d.hpm = keep.f64(np.broadcast_to(np.asarray(op.h_pm, np.float64), (N,)))
+    return d
+
+
+def guide_desc(guide, op, keep):
+    g = _lib.GuideDesc()
+    if guide is None:
+        g.kind = _lib.GUIDE_NONE
+        return g
+    if hasattr(guide, "_gfmc_guide_desc"):
+        return guide._gfmc_guide_desc(op, keep)
+    if isinstance(guide, JastrowSpinHalf):
+        if not _is_spin_half(op):
+            raise TypeError(f"JastrowSpinHalf needs an operator with the SpinHalf transition layout "
+                            f"(n_hx_static, n_jpm_static, edge_i, edge_j); got {type(op).__name__}")
+        g.kind = _lib.GUIDE_JASTROW_SPIN_HALF
+        g.n_pairs = len(guide.pairs)
+        g.pair_i, g.pair_j = keep.i32(guide.pairs[:, 0]), keep.i32(guide.pairs[:, 1])
+        g.pair_w = keep.f64(guide.J_pairs)
+        g.h = keep.f64(guide.h)
+        return g
+    if isinstance(guide, JastrowBoseHubbard):
+        if not _is_bose(op):
+            raise TypeError(f"JastrowBoseHubbard needs a BoseHubbard operator; got {type(op).__name__}")
+        g.kind = _lib.GUIDE_JASTROW_BOSE_HUBBARD
+        P = len(guide.pair_i)
+        g.n_pairs = P
+        g.pair_i, g.pair_j = keep.i32(guide.pair_i), keep.i32(guide.pair_j)
+        tied = np.ndim(guide._beta) == 0
+        g.beta_tied = int(tied)
+        g.beta0 = float(guide._beta) if tied else 0.0
+        g.pair_w = keep.f64(np.ones(P) if tied else -np.asarray(guide._beta, np.float64))
+        for name in ("h", "d"):
+            v = getattr(guide, "_" + name)
+            mode = 0 if v is None else (1 if np.ndim(v) == 0 else 2)
+            setattr(g, name + "_mode", mode)
+            if mode == 1:
+                setattr(g, name + "0", float(v))
+            elif mode == 2:
+                setattr(g, name, keep.f64(v))
+        return g
+    raise TypeError(f"Guide {type(guide).__name__!r} has no device implementation")
+
+
+class GFMCEngine:
+    """Device state of one walker population on one model/guide pair.
+
+    Holds the packed configurations (``cfg``, ``cfg_tmp``), the parent map
+    of the last reconfiguration, and the per-walker float64 weights and
+    local energies, all as torch CUDA tensors; every step runs in the CUDA
+    engine (``gfmc_run_steps``) on the current torch stream.
+    """
+
+    def __init__(self, hamiltonian, guide, n_walkers, precision="fp64"):
+        torch = _torch()
+        self.torch = torch
+        L = _lib.load()
+        self.L = L
+        self.hamiltonian, self.guide = hamiltonian, guide
+        self.n = int(n_walkers)
+        self.N = int(hamiltonian.N)
+        self.family = _lib.MODEL_SPIN_HALF if _is_spin_half(hamiltonian) else _lib.MODEL_BOSE_HUBBARD
+        self.precision = {"fp64": _lib.PRECISION_FP64, "mixed": _lib.PRECISION_MIXED}[precision]
+        keep = _Keep()
+        md = model_desc(hamiltonian, keep)
+        gd = guide_desc(guide, hamiltonian, keep)
+        h = ctypes.c_void_p()
+        _lib.check(L.gfmc_create(ctypes.byref(md), ctypes.byref(gd), self.precision, ctypes.byref(h)),
+                   "gfmc_create")
+        self.h = h
+        self.cfg_bytes = L.gfmc_config_bytes(h)
+        self.M = L.gfmc_n_transitions(h)
+        dev = torch.device("cuda", torch.cuda.current_device())
+        self.device = dev
+        self.cfg = torch.zeros(self.n * self.cfg_bytes, dtype=torch.uint8, device=dev)
+        self.cfg_tmp = torch.zeros_like(self.cfg)
+        self.parents = torch.arange(self.n, dtype=torch.int32, device=dev)
+        self.parents_valid = 0
+        self.log_w = torch.zeros(self.n, dtype=torch.float64, device=dev)
+        self.e_loc = torch.zeros(self.n, dtype=torch.float64, device=dev)
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None) is not None and self.h.value:
+                self.L.gfmc_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    def _stream(self):
+        return ctypes.c_void_p(self.torch.cuda.current_stream().cuda_stream)
+
+    @staticmethod
+    def _ptr(t):
+        return ctypes.c_void_p(t.data_ptr())
+
+    def load(self, config, e_loc=None):
+        """Packs a host or device (n, N) configuration array into ``cfg``."""
+        torch = self.torch
+        c = torch.as_tensor(np.asarray(config) if not torch.is_tensor(config) else config)
+        c = c.to(device=self.device, dtype=torch.float64).contiguous()
+        if tuple(c.shape) != (self.n, self.N):
+            raise ValueError(f"walker configurations must have shape ({self.n}, {self.N}); got {tuple(c.shape)}")
+        _lib.check(self.L.gfmc_pack(self.h, self.n, self._ptr(c), self._ptr(self.cfg), self._stream()),
+                   "gfmc_pack")
+        st = self.status()
+        if st & _lib.STATUS_BAD_CONFIG:
+            raise ValueError("walker configurations hold values outside the model's local basis "
+                             "(+-1 for spin-1/2, integers in [0, n_max] for bosons)")
+        self.parents_valid = 0
+        if e_loc is not None:
+            self.e_loc.copy_(torch.as_tensor(np.asarray(e_loc), dtype=torch.float64))
+
+    def set_max_iters(self, max_iters):
+        _lib.check(self.L.gfmc_set_max_iters(self.h, int(max_iters)), "gfmc_set_max_iters")
+
+    def status(self):
+        v = ctypes.c_int(0)
+        _lib.check(self.L.gfmc_read_status(self.h, ctypes.byref(v), self._stream()), "gfmc_read_status")
+        return v.value
+
+    def local_energy(self):
+        """e_L of the current population (float64 device tensor)."""
+        out = self.torch.empty(self.n, dtype=self.torch.float64, device=self.device)
+        par = self._ptr(self.parents) if self.parents_valid else ctypes.c_void_p(0)
+        _lib.check(self.L.gfmc_local_energy(self.h, self.n, self._ptr(self.cfg), par, self._ptr(out),
+                                            self._stream()), "gfmc_local_energy")
+        return out
+
+    def steps(self, method, step, lam, alw, keys, logG, E, hops=None):
+        """len(keys) branching steps; keys is a (n_steps, 4) uint32 host array."""
+        keys = np.ascontiguousarray(keys, dtype=np.uint32)
+        ns = keys.shape[0]
+        _lib.check(self.L.gfmc_run_steps(
+            self.h, _lib.METHODS[method], float(step), float(lam if lam is not None else 0.0),
+            float(alw), ns, keys.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), self.n,
+            self._ptr(self.cfg), self._ptr(self.cfg_tmp), self._ptr(self.parents),
+            int(self.parents_valid), self._ptr(self.log_w), self._ptr(self.e_loc),
+            self._ptr(logG), self._ptr(E), self._ptr(hops) if hops is not None else ctypes.c_void_p(0),
+            self._stream()), "gfmc_run_steps")
+        self.parents_valid = 1
+
+    def population(self):
+        """The current walkers (config float64 (n, N), e_loc) as device tensors."""
+        torch = self.torch
+        cfg = self.cfg
+        e = self.e_loc
+        if self.parents_valid:
+            cfg = torch.empty_like(self.cfg)
+            e = torch.empty_like(self.e_loc)
+            _lib.check(self.L.gfmc_gather(self.h, self.n, self._ptr(self.parents), self._ptr(self.cfg),
+                                          self._ptr(cfg), self._ptr(self.e_loc), self._ptr(e),
+                                          ctypes.c_void_p(0), self._stream()), "gfmc_gather")
+        out = torch.empty((self.n, self.N), dtype=torch.float64, device=self.device)
+        _lib.check(self.L.gfmc_unpack(self.h, self.n, self._ptr(cfg), self._ptr(out), self._stream()),
+                   "gfmc_unpack")
+        return out, e
+
+    def windowed_energy(self, logG, E, p_array):
+        p = np.ascontiguousarray(p_array, dtype=np.int32)
+        out = np.zeros(len(p), dtype=np.float64)
+        _lib.check(self.L.gfmc_windowed_energy(
+            int(logG.numel()), self._ptr(logG), self._ptr(E), len(p),
+            p.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+            out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), self._stream()),
+            "gfmc_windowed_energy")
+        return dict(zip([int(v) for v in p], out.tolist()))
+
+
+def key_schedule(key, n_steps):
+    """(n_steps, 4) production keys (k1, k2 per step) and the next key."""
+    L = _lib.load()
+    key = np.ascontiguousarray(_rnd.as_key(key))
+    out = np.zeros((n_steps, 4), dtype=np.uint32)
+    nxt = np.zeros(2, dtype=np.uint32)
+    P = ctypes.POINTER(ctypes.c_uint32)
+    _lib.check(L.gfmc_key_schedule(key.ctypes.data_as(P), int(n_steps), out.ctypes.data_as(P),
+                                   nxt.ctypes.data_as(P)), "gfmc_key_schedule")
+    return out, nxt
+
+
+def _warmup_keys(rngs):
+    """k1, k2 = split(rng) for every step of a warm-up chunk (driver.py:183-185)."""
+    out = np.zeros((len(rngs), 4), dtype=np.uint32)
+    for i, r in enumerate(rngs):
+        ks = _rnd.split(r, 2)
+        out[i, :2], out[i, 2:] = ks[0], ks[1]
+    return out
+
+
+def warmup_schedule(method, step_f, warmup_steps):
+    """engine/driver.py _warmup_schedule:567-584."""
+    if warmup_steps <= 0:
+        return []
+    base, extra = divmod(warmup_steps, 4)
+    counts = [base + (i < extra) for i in range(4)]
+    if method == "cont_time":
+        sizes = [step_f / 8.0, step_f / 4.0, step_f / 2.0, step_f]
+    else:
+        nb = int(step_f)
+        sizes = [float(max(1, nb // 8)), float(max(1, nb // 4)), float(max(1, nb // 2)), float(nb)]
+    return [(s, c) for s, c in zip(sizes, counts) if c > 0]
+
+
+def _logsumexp(a):
+    a = np.asarray(a, dtype=np.float64)
+    m = np.max(a)
+    if not np.isfinite(m):
+        return float(m)
+    return float(np.log(np.sum(np.exp(a - m))) + m)
+
+
+def _check_population(log_G_chunk, step0, E_chunk=None):
+    """engine/driver.py _check_population:913-937."""
+    bad = np.flatnonzero(~np.isfinite(log_G_chunk))
+    if bad.size:
+        raise ValueError(
+            f"[gfmc] population extinct at step {step0 + int(bad[0])}: the mean branch weight of "
+            "the step is not finite, i.e. every walker's weight is zero (or one overflowed).  The "
+            "ensemble cannot be renormalised; check lam against the diagonal elements (discrete "
+            "methods), the step size and the guide.")
+    if E_chunk is not None:
+        bad = np.flatnonzero(~np.isfinite(E_chunk))
+        if bad.size:
+            raise ValueError(
+                f"[gfmc] non-finite energy at step {step0 + int(bad[0])}: the weighted mean of the "
+                "local energies is not finite while the branch weights are, i.e. a walker's local "
+                "energy overflowed (a guide ratio or a rate of its configuration is inf or NaN); "
+                "check the guide and the Hamiltonian on the configurations the walk reaches.")
+
+
+def _device_status_check(eng):
+    st = eng.status()
+    if st & _lib.STATUS_HOP_CAP:
+        raise _lib.GFMCError("a walker exceeded the per-step iteration cap (max_hops_per_step, "
+                             "default 2**22 holds): the escape rate times the step size is far "
+                             "too large for this model")
+
+
+def _weight_dtype(lw):
+    dt = getattr(lw, "dtype", None)
+    if dt is None:
+        return np.dtype(np.float64)
+    name = str(dt).replace("torch.", "")
+    return np.dtype(np.float32) if name in ("float32", "bfloat16", "float16") else np.dtype(np.float64)
+
+
+def run_gfmc(walkers, n_steps, hamiltonian, step_size, guide, p_array, *, method="cont_time",
+             rng_key=None, lam=None, diag_operators=None, off_diag_operators=None,
+             return_raw=True, avg_log_weight=None, warmup_steps=None, verbosity=7,
+             number_of_outputs=100, off_diag_stride=1, off_diag_batch_size=None,
+             precision=None, max_hops_per_step=None, _step_offset=0):
+    """GFMC on one B200 with PyGFMC's run_gfmc signature and return tuple.
+
+    ``precision``: ``"fp64"`` (every step quantity in float64, the build that
+    reproduces PyGFMC's float64 runs) or ``"mixed"`` (rates, ratios, local
+    energies in float32; weights, resampling sums and energies in float64).
+    Default: ``"fp64"`` for float64 walker weights, ``"mixed"`` for float32.
+    """
+    wall_start = time.time()
+    if rng_key is None:
+        seed = secrets.randbits(32)
+        _emit(f"[gfmc] - [run_gfmc] - rng_key not given; using jax.random.PRNGKey({seed})", verbosity, 1)
+        rng_key = _rnd.PRNGKey(seed)
+    rng_key = _rnd.as_key(rng_key)
+    rng_key_in = rng_key.copy()
+    aux_root = _rnd.fold_in(rng_key, _AUX_ROOT)
+    config = walkers.config
+    N_walker = int(np.shape(config)[0])
+    if N_walker == 0:
+        raise ValueError("At least one walker is required.")
+    weight_dtype = _weight_dtype(walkers.log_weight)
+    n_steps = _validated_int("n_steps", n_steps, 1)
+    require_step_size(method, step_size)
+    if warmup_steps is None:
+        warmup_steps = DEFAULT_WARMUP_STEPS if avg_log_weight is None else 0
+    warmup_steps = _validated_int("warmup_steps", warmup_steps, 0)
+    number_of_outputs = _validated_int("number_of_outputs", number_of_outputs, 1)
+    off_diag_stride = _validated_int("off_diag_stride", off_diag_stride, 1)
+    if off_diag_batch_size is not None:
+        off_diag_batch_size = _validated_int("off_diag_batch_size", off_diag_batch_size, 1)
+        if N_walker % off_diag_batch_size:
+            raise ValueError(f"off_diag_batch_size={off_diag_batch_size} must divide "
+                             f"N_walkers={N_walker} (a remainder would compile a second shape "
+                             "for the tail; keep one shape so throughput and memory stay predictable)")
+    lam_given = lam
+    lam = require_lam(method, lam)
+    require_operator_protocol(hamiltonian, role="hamiltonian")
+    for name, op in (off_diag_operators or {}).items():
+        require_operator_protocol(op, role=f"off-diagonal operator {name!r}")
+    require_guide_protocol(guide)
+    p_in = len(p_array) if p_array is not None else 0
+    p_array = validated_p_array(p_array)
+    if len(p_array) != p_in:
+        _emit(f"[gfmc.run_gfmc] dedup'd p_array: {p_in - len(p_array)} duplicate value(s) "
+              f"dropped, using {p_array}", verbosity)
+    if diag_operators or off_diag_operators:
+        raise NotImplementedError(
+            "diagonal/off-diagonal forward-walking operators are not built into the B200 engine yet")
+    m_array = [p // 2 for p in p_array]
+    if p_array[-1] >= n_steps:
+        raise ValueError(f"every p value must be smaller than n_steps: got n_steps={n_steps} and "
+                         f"max(p)={p_array[-1]}")
+    if avg_log_weight is None and warmup_steps == 0:
+        raise ValueError(
+            "warmup_steps=0 needs an avg_log_weight: without a warm-up nothing measures it. Pass "
+            "avg_log_weight=stats['avg_log_weight'] of the run being continued (run_from_HDF5 does "
+            f"this), or leave warmup_steps unset for the default warm-up of {DEFAULT_WARMUP_STEPS} steps.")
+    if precision is None:
+        precision = "fp64" if weight_dtype == np.float64 else "mixed"
+    step_f = float(step_size)
+
+    torch = _torch()
+    eng = GFMCEngine(hamiltonian, guide, N_walker, precision=precision)
+    if max_hops_per_step is not None:
+        eng.set_max_iters(_validated_int("max_hops_per_step", max_hops_per_step, 1))
+    eng.load(np.asarray(config) if not torch.is_tensor(config) else config)
+
+    # ---- warm-up (driver.py _warmup:747-788)
+    alw_pinned = avg_log_weight is not None
+    if not alw_pinned:
+        e = eng.local_energy().cpu().numpy()
+        alw = float(np.mean(-e)) if method == "cont_time" else float(np.mean(np.log(lam - e)))
+    else:
+        alw = float(avg_log_weight)
+    dev = eng.device
+    stages = warmup_schedule(method, step_f, warmup_steps)
+    for i, (step_, n_w) in enumerate(stages):
+        t0 = time.time()
+        sub = _rnd.fold_in(_rnd.fold_in(aux_root, int(n_w)), int(step_ * 1000))
+        remaining = n_w
+        lg_all = []
+        while remaining > 0:
+            mm = min(_WARMUP_CHUNK, remaining)
+            sub, k = _rnd.split(sub, 2)
+            keys = _warmup_keys(_rnd.split(k, mm))
+            lg = torch.empty(mm, dtype=torch.float64, device=dev)
+            Ee = torch.empty(mm, dtype=torch.float64, device=dev)
+            eng.steps(method, step_, lam, alw, keys, lg, Ee)
+            lg_all.append(lg.cpu().numpy())
+            remaining -= mm
+        _device_status_check(eng)
+        measured = alw + (_logsumexp(np.concatenate(lg_all)) - math.log(n_w)) / step_
+        label = f"{i + 1}/{len(stages)}"
+        el = max(time.time() - t0, 1e-9)
+        if method == "cont_time":
+            _emit(f"[gfmc] - [run_warmup {label}] - step={step_}, {n_w} steps @ {n_w / el:.1f} it/s, "
+                  f"avg_log_weight = {measured:.6f}", verbosity, 8)
+        else:
+            _emit(f"[gfmc] - [run_warmup {label}] - step={step_}, {n_w} steps @ {n_w / el:.1f} it/s, "
+                  f"average_b_x = {math.exp(measured):.6f}", verbosity, 8)
+        if alw_pinned:
+            _emit(f"[gfmc] - [run_warmup {label}] - alw pinned at {alw:.6f}; this stage would have "
+                  f"measured {measured:.6f}", verbosity, 8)
+        else:
+            alw = measured
+    if not stages:
+        _emit(f"[gfmc] - [run_gfmc] - no warmup (warmup_steps=0), avg_log_weight={alw:.6f}", verbosity, 8)
+
+    # ---- production (driver.py _production:940-1143), chunked and pipelined
+    print_every = max(1, n_steps // max(1, number_of_outputs))
+    chunk = print_every if verbosity >= 1 else n_steps
+    logG_d = torch.empty(n_steps, dtype=torch.float64, device=dev)
+    E_d = torch.empty(n_steps, dtype=torch.float64, device=dev)
+    hops_d = torch.zeros(n_steps, dtype=torch.int64, device=dev)
+    logG_h = torch.empty(n_steps, dtype=torch.float64, pin_memory=True)
+    E_h = torch.empty(n_steps, dtype=torch.float64, pin_memory=True)
+    key = rng_key.copy()
+    prod_start = time.time()
+    pending = []
+    step0 = 0
+    last_print_t, last_print_step = prod_start, 0
+    while step0 < n_steps:
+        cs = min(chunk, n_steps - step0)
+        keys, key = key_schedule(key, cs)
+        sl = slice(step0, step0 + cs)
+        eng.steps(method, step_f, lam, alw, keys, logG_d[sl], E_d[sl], hops_d[sl])
+        logG_h[sl].copy_(logG_d[sl], non_blocking=True)
+        E_h[sl].copy_(E_d[sl], non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record()
+        pending.append((step0, cs, ev))
+        step0 += cs
+        # process every chunk but the one just dispatched (pipelining)
+        while len(pending) > 1 or (pending and step0 >= n_steps):
+            s0, c0, e0 = pending.pop(0)
+            e0.synchronize()
+            lgc = logG_h[s0:s0 + c0].numpy()
+            Ec = E_h[s0:s0 + c0].numpy()
+            _check_population(lgc, s0, Ec)
+            done = s0 + c0
+            if verbosity >= 1 and done - 1 > p_array[-1]:
+                now = time.time()
+                rate = (done - last_print_step) / max(now - last_print_t, 1e-9)
+                line = f"[gfmc] - [run_gfmc] - step: {done}/{n_steps}, {rate:.1f} it/s"
+                if verbosity >= 3:
+                    est = windowed_energy_host(p_array, logG_h[:done].numpy(), E_h[:done].numpy())
+                    line += f" Energy[p]: {est}"
+                _emit(line, verbosity)
+                last_print_t, last_print_step = now, done
+    torch.cuda.current_stream().synchronize()
+    runtime = time.time() - prod_start
+    _device_status_check(eng)
+    weights_np = logG_h.numpy().copy()
+    E_np = E_h.numpy().copy()
+    energy = eng.windowed_energy(logG_d, E_d, p_array)
+
+    cfg_d, e_d = eng.population()
+    cfg_np = cfg_d.cpu().numpy()
+    in_dtype = np.asarray(config).dtype if not torch.is_tensor(config) else np.float64
+    if in_dtype.kind == "f":
+        cfg_np = cfg_np.astype(in_dtype)
+    out_w = Walker(config=cfg_np, log_weight=np.zeros(N_walker, dtype=weight_dtype),
+                   e_loc=e_d.cpu().numpy().astype(weight_dtype))
+    hops_np = hops_d.cpu().numpy()
+
+    stats = {
+        "avg_log_weight": float(alw),
+        "it_per_sec": n_steps / runtime,
+        "runtime": runtime,
+        "total_wall_time": time.time() - wall_start,
+        "number_of_devices": 1,
+        "hops_per_step_mean": hops_np / float(N_walker),
+        "parameters/n_steps": int(n_steps),
+        "parameters/n_walkers": N_walker,
+        "parameters/n_sites": int(np.shape(config)[1]),
+        "parameters/step_size": step_f,
+        "parameters/lam": float(lam_given) if lam_given is not None else float("nan"),
+        "parameters/p_array": np.asarray(p_array, dtype=np.int64),
+        "parameters/m_array": np.asarray(m_array, dtype=np.int64),
+        "parameters/warmup_steps": int(warmup_steps),
+        "parameters/verbosity": int(verbosity),
+        "parameters/number_of_outputs": int(number_of_outputs),
+        "parameters/off_diag_stride": int(off_diag_stride),
+        "parameters/method": np.asarray(str(method), dtype="S32"),
+        "parameters/guide": np.asarray(type(guide).__name__ if guide is not None else "none", dtype="S32"),
+        "parameters/hamiltonian": np.asarray(type(hamiltonian).__name__, dtype="S32"),
+        "parameters/has_guide": int(guide is not None),
+        "parameters/precision": np.asarray(precision, dtype="S32"),
+        "parameters/rng_key": rng_key_in,
+        "parameters/rng_key_next": key,
+    }
+    stats.update(autocorrelation_stats(E_np, weights_np))
+    obs = {}
+    if return_raw:
+        raw = dict(log_weights=weights_np, energy=E_np, diag=None, off_diag=None, off_diag_norm=None,
+                   off_diag_steps=None, additional_diag=None, p_array=list(p_array),
+                   m_array=list(m_array), diag_operators=None, off_diag_operators=None)
+        return out_w, energy, obs, stats, raw
+    return out_w, energy, obs, stats
+
+
+def run(walkers, n_steps, hamiltonian, step_size, guide, p_array, *, method="cont_time",
+        rng_key=None, lam=None, **kwargs):
+    """Drop-in for ``pygfmc.run`` (engine/multi_gpu.py:822-868) on one B200.
+
+    ``n_devices`` is accepted; this engine runs one GPU per process, so a
+    value above 1 raises (multi-GPU runs use one process per GPU)."""
+    n_devices = kwargs.pop("n_devices", None)
+    if n_devices is not None:
+        n_devices = _validated_int("n_devices", n_devices, 1)
+        if n_devices > 1:
+            raise ValueError("pygfmc_b200.run drives one GPU per process; launch one process per "
+                             "GPU (torchrun) for more")
+    return run_gfmc(walkers, n_steps, hamiltonian, step_size, guide, p_array, method=method,
+                    rng_key=rng_key, lam=lam, **kwargs)

@@ -1,0 +1,109 @@
+"""Host-side estimator helpers (numpy, float64).
+
+The per-step series come from the device; what is cheap and inherently
+serial on the series stays on the host, as in PyGFMC:
+``validated_p_array`` (engine/estimators.py:30-42), the windowed energy for
+progress lines (:268-305; the final estimate runs on the device),
+``autocorrelation`` (:71-117), and the blocked jackknife of
+``evaluate_observables`` (engine/io.py:1084-1104).
+"""
+import numpy as np
+
+__all__ = ["validated_p_array", "windowed_energy_host", "autocorrelation",
+           "autocorrelation_stats", "jackknife_energy", "evaluate_observables"]
+
+
+def validated_p_array(p_array):
+    if p_array is None or len(p_array) == 0:
+        raise ValueError("p_array must contain at least one positive window size.")
+    out = []
+    for p in p_array:
+        pi = int(p)
+        if float(pi) != float(p):
+            raise ValueError(f"p_array values must be integers, got {p!r}.")
+        if pi <= 0:
+            raise ValueError(f"p_array values must be > 0, got {pi}.")
+        out.append(pi)
+    return sorted(set(out))
+
+
+def windowed_energy_host(p_array, log_weights, E):
+    """E_p = sum_i G_p(i) E(i+p) / sum_i G_p(i), G_p from windowed log weights."""
+    L = np.cumsum(np.asarray(log_weights, dtype=np.float64))
+    E = np.asarray(E, dtype=np.float64)
+    out = {}
+    for p in validated_p_array(p_array):
+        if p >= len(L):
+            continue
+        lg = L[p:] - L[:-p]
+        G = np.exp(lg - np.max(lg))
+        out[p] = float(np.sum(G * E[p:])) / float(np.sum(G))
+    return out
+
+
+def autocorrelation(series, c=5.0):
+    """Integrated autocorrelation time with the self-consistent window
+    (FFT autocovariance; window M >= c (0.5 + sum |rho|))."""
+    if not np.isfinite(c) or c <= 0:
+        raise ValueError("c must be finite and positive.")
+    x = np.asarray(series, dtype=float).ravel()
+    n = x.size
+    if n < 16 or not np.all(np.isfinite(x)):
+        return float("nan"), 0
+    d = x - x.mean()
+    acov0 = float(d @ d) / n
+    if acov0 <= 0.0:
+        return float("nan"), 0
+    m = 1 << (2 * n - 1).bit_length()
+    f = np.fft.rfft(d, m)
+    acov = np.fft.irfft(f * np.conj(f), m)[:n].real / np.arange(n, 0, -1)
+    rho = acov / acov[0]
+    run = 0.5 + np.cumsum(rho[1:])
+    M = np.arange(1, run.size + 1)
+    env = 0.5 + np.cumsum(np.abs(rho[1:]))
+    hit = np.flatnonzero(M >= c * env)
+    if hit.size == 0:
+        return float("nan"), 0
+    i = int(hit[0])
+    if run[i] <= 0 or not np.isfinite(run[i]):
+        return float("nan"), int(M[i])
+    return float(run[i]), int(M[i])
+
+
+def autocorrelation_stats(E_np, log_weights_np):
+    return {"autocorrelation/energy_estimator": autocorrelation(E_np)[0],
+            "autocorrelation/log_weights": autocorrelation(log_weights_np)[0]}
+
+
+def jackknife_energy(p_array, log_weights, E, n_blocks):
+    """Blocked jackknife of the windowed energy: leave-one-block-out replicas
+    (the survivors concatenated), err = sqrt((nb-1)/nb sum (x_b - mean)^2)."""
+    n = len(E)
+    blen = n // n_blocks
+    if n_blocks < 2 or blen < 1:
+        raise ValueError(f"n_blocks={n_blocks} over {n} steps leaves {blen} steps per block; "
+                         "a jackknife needs at least 2 usable blocks.")
+    usable = blen * n_blocks
+    lw = np.asarray(log_weights, dtype=np.float64)[:usable]
+    EE = np.asarray(E, dtype=np.float64)[:usable]
+    grid = validated_p_array(p_array)
+    reps = []
+    for b in range(n_blocks):
+        mask = np.ones(usable, dtype=bool)
+        mask[b * blen:(b + 1) * blen] = False
+        est = windowed_energy_host(grid, lw[mask], EE[mask])
+        reps.append([est[p] for p in grid])
+    arr = np.asarray(reps)
+    c = arr - arr.mean(axis=0, keepdims=True)
+    err = np.sqrt((n_blocks - 1) / n_blocks * np.sum(c ** 2, axis=0))
+    return windowed_energy_host(grid, lw, EE), dict(zip(grid, err.tolist()))
+
+
+def evaluate_observables(raw, p_array=None, n_blocks=None):
+    """Energy re-estimation from a ``raw`` dict, with jackknife errors when
+    ``n_blocks`` is given (engine/io.py evaluate_observables, energy part)."""
+    grid = validated_p_array(p_array if p_array is not None else raw["p_array"])
+    if n_blocks is None:
+        return windowed_energy_host(grid, raw["log_weights"], raw["energy"]), {}
+    E, err = jackknife_energy(grid, raw["log_weights"], raw["energy"], n_blocks)
+    return E, {}, err, {}

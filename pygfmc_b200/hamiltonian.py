@@ -1,0 +1,477 @@
+"""Hamiltonians and lattices of the engine, with PyGFMC's constructors.
+
+``SpinHalf.create`` and ``BoseHubbard.create`` take the arguments, apply the
+sign conventions and raise the errors of PyGFMC's
+``hamiltonian/SpinHalf.py:144-288`` and ``hamiltonian/bose_hubbard.py:129-267``,
+and expose the same stored fields (``edge_i``, ``J_pm``, ``h_x_half``,
+``n_hx_static``, ``M_total`` ...).  The objects are plain host data (numpy);
+the engine lowers them to device tables when a run starts.  ``get_rates`` /
+``generate_state`` / ``diagonal_weight`` are host (numpy) versions of the
+protocol methods, for inspection and exact diagonalisation; the propagation
+itself never calls them.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+__all__ = ["SpinHalf", "BoseHubbard", "Lattice", "chain", "square", "kagome", "edges_array"]
+
+
+def edges_array(edges):
+    """hamiltonian/_common.py edges_array:7-31: validated (n_edges, 2) int64."""
+    raw = np.asarray(edges)
+    if raw.shape == (0,):
+        return np.zeros((0, 2), dtype=np.int64), 0, 0
+    if raw.ndim != 2 or raw.shape[1] != 2:
+        raise ValueError("edges must have shape (n_edges, 2).")
+    if (raw.dtype.kind not in "iuf" or not np.all(np.isfinite(raw)) or np.any(raw < 0)
+            or np.any(raw >= 2 ** 63) or np.any(raw != np.floor(raw))):
+        raise ValueError("edge indices must be nonnegative integers fitting in int64.")
+    e = raw.astype(np.int64)
+    if np.any(e[:, 0] == e[:, 1]):
+        raise ValueError("self-edges are not supported; edge endpoints must differ.")
+    return e, len(e), int(e.max()) + 1 if e.size else 0
+
+
+def _jpmpm_message(value):
+    return (f"J_pmpm = (J_x - J_y) / 4 = {value:.6g} > 0 violates the sign-problem-free "
+            "convention (J_pmpm <= 0).\n  Fix: swap S^x <-> S^y, i.e. pass J_x and J_y the "
+            "other way round (a symmetry only when h_x = 0), or pass sign_check=False for a "
+            "measurement operator.")
+
+
+def _jpm_message(value):
+    return (f"J_pm = (J_x + J_y) / 4 = {value:.6g} > 0 violates the sign-problem-free "
+            "convention (J_pm <= 0).\n  On a bipartite lattice apply the sublattice rotation "
+            "(pass -J_x and -J_y; an equivalence only when h_x = 0).  For an off-diagonal "
+            "MEASUREMENT operator J_pm >= 0 is what is required -- build it with "
+            "sign_check=False.")
+
+
+class SpinHalf:
+    """Spin-1/2 XYZ model with longitudinal and transverse fields.
+
+        H = sum_<ij> [J_x S^x_i S^x_j + J_y S^y_i S^y_j + J_z S^z_i S^z_j]
+            - sum_i [h_z S^z_i + h_x S^x_i]
+
+    Configurations are +-1 (sigma_i = 2 S^z_i).  Rate layout::
+
+        rates[0]                 diagonal H_xx
+        rates[1 : 1+n_hx]        single-site flips, -h_x/2 (n_hx = N if h_x != 0)
+        rates[1+n_hx : M_total]  one per edge: J_pm anti-parallel, J_pmpm parallel
+
+    Sign-problem-free: J_pm <= 0, J_pmpm <= 0, h_x >= 0 (enforced by create).
+    """
+
+    def __init__(self, **kw):
+        self.__dict__.update(kw)
+
+    # reference property names
+    @property
+    def edges(self):
+        return np.stack([np.asarray(self.edge_i), np.asarray(self.edge_j)], axis=1)
+
+    @property
+    def n_hx(self):
+        return self.n_hx_static
+
+    @property
+    def n_jpm(self):
+        return self.n_jpm_static
+
+    @property
+    def n_off(self):
+        return self.n_hx_static + self.n_jpm_static
+
+    @property
+    def M_total(self):
+        return self.n_hx_static + self.n_jpm_static + 1
+
+    @property
+    def local_hilbert_space(self):
+        return (1.0, -1.0)
+
+    @classmethod
+    def create(cls, edges, J_x=0, J_y=0, J_z=0, h_z=None, h_x=None, N=None, *,
+               dtype=np.float32, sign_check=True):
+        h_z = None if h_z is None else (-np.asarray(h_z) if isinstance(h_z, (list, tuple)) else -h_z)
+        h_x = None if h_x is None else (-np.asarray(h_x) if isinstance(h_x, (list, tuple)) else -h_x)
+        edges_arr, _, N_min = edges_array(edges)
+        for a in (h_z, h_x):
+            if np.ndim(a) > 0:
+                N_min = max(N_min, np.shape(a)[0])
+        if N is None:
+            N = N_min
+        else:
+            N = int(N)
+            if N < N_min:
+                raise ValueError(f"N={N} is smaller than required by the given edges/site "
+                                 f"arrays (need at least {N_min})")
+        dtype = np.dtype(dtype)
+        n_edges = len(edges_arr)
+        uniform = not (hasattr(J_x, "__len__") or hasattr(J_y, "__len__") or hasattr(J_z, "__len__"))
+        if uniform:
+            J_pmpm = (J_x - J_y) / 4.0
+            if J_pmpm > 0 and sign_check:
+                raise ValueError(_jpmpm_message(float(J_pmpm)))
+            J_z_arr = np.array([J_z], dtype=dtype)
+            J_pm_arr = np.array([(J_x + J_y) / 4.0], dtype=dtype)
+            J_pmpm_arr = np.array([J_pmpm], dtype=dtype)
+        else:
+            def per_edge(v):
+                a = np.asarray(v, dtype=dtype)
+                if a.ndim == 0 or a.shape[0] == 1:
+                    return np.broadcast_to(a.reshape(1), (n_edges,)).copy()
+                return a
+            jx, jy, J_z_arr = per_edge(J_x), per_edge(J_y), per_edge(J_z)
+            if jx.shape[0] != n_edges or jy.shape[0] != n_edges or J_z_arr.shape[0] != n_edges:
+                raise ValueError("Non-uniform couplings must match the number of edges.")
+            J_pm_arr = (jx + jy) / dtype.type(4.0)
+            J_pmpm_arr = (jx - jy) / dtype.type(4.0)
+            if sign_check and np.any(J_pmpm_arr > 0):
+                bad = np.flatnonzero(J_pmpm_arr > 0)
+                raise ValueError(_jpmpm_message(float(J_pmpm_arr[bad[0]]))
+                                 + f"\n  Offending edges: {bad.tolist()[:10]}"
+                                 + (" ..." if bad.size > 10 else "")
+                                 + f" ({bad.size} of {n_edges}).")
+        if h_z is None:
+            h_z_arr = None
+        elif np.ndim(h_z) > 0:
+            h_z_arr = np.asarray(h_z, dtype=dtype)
+            if h_z_arr.shape[0] != N:
+                raise ValueError(f"Non-uniform h_z must have length N={N}, got {h_z_arr.shape[0]}.")
+        else:
+            h_z_arr = np.array([h_z], dtype=dtype)
+        if h_x is None:
+            h_x_half_arr = None
+        elif np.ndim(h_x) > 0:
+            hxa = np.asarray(h_x, dtype=float)
+            if hxa.shape[0] != N:
+                raise ValueError(f"Non-uniform h_x must have length N={N}, got {hxa.shape[0]}.")
+            if sign_check and np.any(hxa > 0):
+                raise ValueError("h_x must be >= 0 for all sites (sign-problem-free convention; "
+                                 "H contains -h_x Σ S^x, so a field written as +a Σ S^x is "
+                                 "passed as h_x = -a).")
+            h_x_half_arr = np.array(hxa / 2, dtype=dtype)
+        else:
+            if sign_check and h_x > 0:
+                raise ValueError("h_x must be >= 0 (sign-problem-free convention; H contains "
+                                 "-h_x Σ S^x, so a field written as +a Σ S^x is passed as h_x = -a).")
+            h_x_half_arr = np.array([h_x / 2], dtype=dtype)
+        if sign_check and np.any(np.asarray(J_pm_arr) > 0):
+            raise ValueError(_jpm_message(float(np.max(J_pm_arr))))
+        idx_dtype = np.int16 if N <= 32767 else np.int32
+        return cls(
+            dtype=dtype,
+            edge_i=np.array(edges_arr[:, 0], dtype=idx_dtype),
+            edge_j=np.array(edges_arr[:, 1], dtype=idx_dtype),
+            N=N, J_z=J_z_arr, J_pm=J_pm_arr, J_pmpm=J_pmpm_arr,
+            h_z=h_z_arr, h_x_half=h_x_half_arr,
+            n_hx_static=N if (h_x_half_arr is not None and np.linalg.norm(h_x_half_arr) > 0) else 0,
+            n_jpm_static=n_edges if (np.linalg.norm(J_pm_arr) > 0 or np.linalg.norm(J_pmpm_arr) > 0) else 0,
+            has_jz=bool(np.linalg.norm(J_z_arr) > 0),
+            uniform_jz=len(J_z_arr) == 1,
+            has_hz=bool(h_z_arr is not None and np.linalg.norm(h_z_arr) > 0),
+        )
+
+    # ---- host versions of the protocol methods -----------------------------
+    def diagonal_weight(self, config):
+        x = np.asarray(config, dtype=np.float64)
+        d = 0.0
+        if self.has_jz:
+            anti = x[..., self.edge_i] != x[..., self.edge_j]
+            if self.uniform_jz:
+                na = anti.sum(-1)
+                d = (float(self.J_z[0]) / 4) * ((len(self.edge_i) - na) - na)
+            else:
+                jz = np.asarray(self.J_z, np.float64)
+                d = np.where(anti, -jz / 4.0, jz / 4.0).sum(-1)
+        if self.has_hz:
+            d = d + (np.asarray(self.h_z, np.float64) * x).sum(-1) / 2
+        return d
+
+    def get_rates(self, config, return_configs=False):
+        x = np.asarray(config, dtype=np.float64)
+        r = np.zeros(self.M_total)
+        r[0] = self.diagonal_weight(x)
+        if self.n_hx_static:
+            r[1:1 + self.N] = np.broadcast_to(np.asarray(self.h_x_half, np.float64), (self.N,))
+        if self.n_jpm_static:
+            anti = x[self.edge_i] != x[self.edge_j]
+            r[1 + self.n_hx_static:] = np.where(anti, np.asarray(self.J_pm, np.float64),
+                                                np.asarray(self.J_pmpm, np.float64))
+        if not return_configs:
+            return r, None
+        return r, np.stack([self.generate_state(x, k) for k in range(self.M_total)])
+
+    def generate_state(self, config, idx):
+        x = np.array(config, dtype=np.float64, copy=True)
+        if idx == 0:
+            return x
+        o = idx - 1
+        if o < self.n_hx_static:
+            x[o] = -x[o]
+        else:
+            e = o - self.n_hx_static
+            i, j = int(self.edge_i[e]), int(self.edge_j[e])
+            xi, xj = x[i], x[j]
+            x[i], x[j] = -xi, -xj
+        return x
+
+
+class BoseHubbard:
+    """Bose-Hubbard model (PyGFMC hamiltonian/bose_hubbard.py).
+
+        H = -t sum_<ij> (b+_i b_j + h.c.) - eta sum_<ij> (b+_i b+_j + b_i b_j)
+            + U/2 sum_i n_i (n_i - 1) - mu sum_i n_i - h_pm sum_i (b+_i + b_i)
+
+    Occupations 0..n_max.  Rate layout: [diag, hop i->j (E), hop j->i (E),
+    pair creation (E), pair annihilation (E), b+ (N), b (N)], blocks dropped
+    when their coupling vanishes.  Sign-problem-free: t, eta, h_pm >= 0.
+    """
+
+    def __init__(self, **kw):
+        self.__dict__.update(kw)
+
+    @property
+    def edges(self):
+        return np.stack([np.asarray(self.edge_i), np.asarray(self.edge_j)], axis=1)
+
+    @property
+    def n_edges(self):
+        return int(len(self.edge_i))
+
+    @property
+    def n_off(self):
+        return self.n_hop_off + self.n_eta_off + 2 * self.n_hpm_off
+
+    @property
+    def M_total(self):
+        return 1 + self.n_off
+
+    @property
+    def local_hilbert_space(self):
+        return tuple(float(n) for n in range(int(self.n_max) + 1))
+
+    @classmethod
+    def create(cls, edges, t=0.0, eta=0.0, U=0.0, mu=0.0, h_pm=None, N=None, n_max=4, *,
+               dtype=np.float32, sign_check=True):
+        h_pm = None if h_pm is None else (-np.asarray(h_pm) if isinstance(h_pm, (list, tuple)) else -h_pm)
+        edges_arr, n_edges, N_min = edges_array(edges)
+        for a in (U, mu, h_pm):
+            if np.ndim(a) > 0:
+                N_min = max(N_min, np.shape(a)[0])
+        if N is None:
+            N = N_min
+        else:
+            N = int(N)
+            if N < N_min:
+                raise ValueError(f"N={N} is smaller than required by the given edges/site "
+                                 f"arrays (need at least {N_min})")
+        if n_max < 1:
+            raise ValueError(f"n_max must be ≥ 1, got {n_max}")
+        dtype = np.dtype(dtype)
+
+        def edge_arr(x, name):
+            if np.ndim(x) > 0:
+                a = np.asarray(x, dtype=dtype)
+                if a.shape[0] != n_edges:
+                    raise ValueError(f"non-uniform {name} must have length n_edges={n_edges}, got {a.shape[0]}")
+                return a, False
+            return np.array([float(x)], dtype=dtype), True
+
+        def site_arr(x, name):
+            if x is None:
+                return None, True
+            if np.ndim(x) > 0:
+                a = np.asarray(x, dtype=dtype)
+                if a.shape[0] != N:
+                    raise ValueError(f"non-uniform {name} must have length N={N}, got {a.shape[0]}")
+                return a, False
+            return np.array([float(x)], dtype=dtype), True
+
+        t_arr, uni_t = edge_arr(t, "t")
+        eta_arr, uni_eta = edge_arr(eta, "eta")
+        U_arr, uni_U = site_arr(U, "U")
+        mu_arr, uni_mu = site_arr(mu, "mu")
+        hpm_arr, uni_hpm = site_arr(h_pm, "h_pm")
+        if sign_check:
+            if np.any(t_arr < 0):
+                raise ValueError("t must be ≥ 0 (sign-problem-free convention).")
+            if np.any(eta_arr < 0):
+                raise ValueError("eta must be ≥ 0 (sign-problem-free convention).")
+            if hpm_arr is not None and np.any(hpm_arr > 0):
+                raise ValueError("h_pm must be ≥ 0 (sign-problem-free convention).")
+
+        def active(a):
+            return a is not None and float(np.linalg.norm(a)) > 0
+        has_t, has_eta, has_U, has_mu, has_hpm = (active(t_arr), active(eta_arr), active(U_arr),
+                                                  active(mu_arr), active(hpm_arr))
+        if not has_hpm:
+            hpm_arr = None
+        if not has_U:
+            U_arr, uni_U = np.zeros((1,), dtype=dtype), True
+        if not has_mu:
+            mu_arr, uni_mu = np.zeros((1,), dtype=dtype), True
+        idx_dtype = np.int16 if N <= 32767 else np.int32
+        return cls(
+            dtype=dtype,
+            edge_i=np.array(edges_arr[:, 0] if n_edges else [], dtype=idx_dtype),
+            edge_j=np.array(edges_arr[:, 1] if n_edges else [], dtype=idx_dtype),
+            N=N, n_max=int(n_max), t=t_arr, eta=eta_arr, U=U_arr, mu=mu_arr, h_pm=hpm_arr,
+            n_hop_off=2 * n_edges if has_t else 0, n_eta_off=2 * n_edges if has_eta else 0,
+            n_hpm_off=N if has_hpm else 0,
+            has_t=has_t, has_eta=has_eta, has_U=has_U, has_mu=has_mu, has_h_pm=has_hpm,
+            uniform_t=uni_t, uniform_eta=uni_eta, uniform_U=uni_U, uniform_mu=uni_mu,
+            uniform_hpm=uni_hpm,
+        )
+
+    def _per_edge(self, a):
+        return np.broadcast_to(np.asarray(a, np.float64), (self.n_edges,))
+
+    def _per_site(self, a):
+        return np.broadcast_to(np.asarray(a, np.float64), (self.N,))
+
+    def moves(self):
+        """(a, b, da, db) of every transition, the layout of _move_blocks."""
+        E, N = self.n_edges, self.N
+        a, b, da, db = [0], [0], [0], [0]
+        ei, ej = np.asarray(self.edge_i, int), np.asarray(self.edge_j, int)
+        blocks = []
+        if self.n_hop_off:
+            blocks += [(-1, +1), (+1, -1)]
+        if self.n_eta_off:
+            blocks += [(+1, +1), (-1, -1)]
+        for sa, sb in blocks:
+            a += list(ei); b += list(ej); da += [sa] * E; db += [sb] * E
+        if self.n_hpm_off:
+            for s in (+1, -1):
+                a += list(range(N)); b += list(range(N)); da += [s] * N; db += [0] * N
+        return np.array(a), np.array(b), np.array(da), np.array(db)
+
+    def diagonal_weight(self, config):
+        n = np.asarray(config, dtype=np.float64)
+        out = 0.0
+        if self.has_U:
+            out = out + 0.5 * np.sum(self._per_site(self.U) * n * (n - 1.0), axis=-1)
+        if self.has_mu:
+            out = out - np.sum(self._per_site(self.mu) * n, axis=-1)
+        return out
+
+    def get_rates(self, config, return_configs=False):
+        n = np.asarray(config, dtype=np.float64)
+        nmax = float(self.n_max)
+        r = [np.array([self.diagonal_weight(n)])]
+        ei, ej = np.asarray(self.edge_i, int), np.asarray(self.edge_j, int)
+        if self.n_hop_off:
+            t = self._per_edge(self.t)
+            ni, nj = n[ei], n[ej]
+            r.append(-t * np.sqrt(ni * (nj + 1.0)) * (nj < nmax))
+            r.append(-t * np.sqrt((ni + 1.0) * nj) * (ni < nmax))
+        if self.n_eta_off:
+            eta = self._per_edge(self.eta)
+            ni, nj = n[ei], n[ej]
+            r.append(-eta * np.sqrt((ni + 1.0) * (nj + 1.0)) * ((ni < nmax) & (nj < nmax)))
+            r.append(-eta * np.sqrt(ni * nj))
+        if self.n_hpm_off:
+            hp = self._per_site(self.h_pm)
+            r.append(hp * np.sqrt(n + 1.0) * (n < nmax))
+            r.append(hp * np.sqrt(n))
+        rates = np.concatenate(r)
+        if not return_configs:
+            return rates, None
+        return rates, np.stack([self.generate_state(n, k) for k in range(self.M_total)])
+
+    def generate_state(self, config, idx):
+        x = np.array(config, dtype=np.float64, copy=True)
+        if idx == 0:
+            return x
+        a, b, da, db = self.moves()
+        x[a[idx]] += da[idx]
+        x[b[idx]] += db[idx]
+        return x
+
+
+# ---- lattices ----------------------------------------------------------------
+@dataclass(frozen=True)
+class Lattice:
+    """A finite lattice: site count, edge list and optional metadata
+    (hamiltonian/lattice.py Lattice:8-33)."""
+    name: str
+    N: int
+    edges: list
+    J_x: object = None
+    J_y: object = None
+    J_z: object = None
+    extras: dict = field(default_factory=dict, compare=False, hash=False)
+
+
+def chain(n_sites: int, periodic: bool = True) -> Lattice:
+    """Nearest-neighbour chain (hamiltonian/lattice.py chain:36-46)."""
+    edges = [(i, i + 1) for i in range(n_sites - 1)]
+    if periodic and n_sites > 2:
+        edges.append((n_sites - 1, 0))
+    return Lattice(name="chain", N=n_sites, edges=edges, J_x=-1.0, J_y=-1.0, J_z=1.0)
+
+
+def square(Lx: int, Ly: int = None, periodic: bool = True) -> Lattice:
+    """Nearest-neighbour square lattice of Lx x Ly sites, site x + Lx*y.
+
+    PyGFMC has no square-lattice factory; this one follows its Lattice
+    conventions.  Periodic boundaries need Lx, Ly >= 3 so that no bond is
+    doubled.  ``extras['positions']`` holds the (N, 2) coordinates and
+    ``extras['torus']`` the periods, for distance-dependent guides.
+    """
+    Ly = Lx if Ly is None else Ly
+    if periodic and (Lx < 3 or Ly < 3):
+        raise ValueError("square requires Lx, Ly >= 3 for periodic boundary conditions")
+    idx = lambda x, y: (x % Lx) + Lx * (y % Ly)
+    edges = set()
+    for y in range(Ly):
+        for x in range(Lx):
+            for dx, dy in ((1, 0), (0, 1)):
+                if not periodic and (x + dx >= Lx or y + dy >= Ly):
+                    continue
+                i, j = idx(x, y), idx(x + dx, y + dy)
+                edges.add((min(i, j), max(i, j)))
+    pos = np.array([(x, y) for y in range(Ly) for x in range(Lx)], dtype=float)
+    return Lattice(name="square", N=Lx * Ly, edges=sorted(edges), J_x=-1.0, J_y=-1.0, J_z=1.0,
+                   extras=dict(positions=pos, torus=np.array([Lx, Ly]), periodic=periodic))
+
+
+def kagome(Lx: int, Ly: int, periodic: bool = True) -> Lattice:
+    """Kagome lattice of Lx x Ly three-site cells (hamiltonian/lattice.py
+    kagome:186-262): site 3*(x + Lx*y) + b, primitive vectors (2, 0) and
+    (1, sqrt 3), sublattice offsets 0, a1/2, a2/2."""
+    if periodic and (Lx < 2 or Ly < 2):
+        raise ValueError(f"kagome requires Lx, Ly >= 2 for periodic boundary conditions "
+                         f"(got {Lx}, {Ly}); smaller tori wrap a bond onto itself.")
+    a1 = np.array([2.0, 0.0])
+    a2 = np.array([1.0, np.sqrt(3.0)])
+    basis = np.array([[0.0, 0.0], a1 / 2, a2 / 2])
+    sub = {(0, 0): 0, (1, 0): 1, (0, 1): 2}
+
+    def index(U, V):
+        x, y = U // 2, V // 2
+        if not periodic and not (0 <= x < Lx and 0 <= y < Ly):
+            return None
+        return 3 * ((x % Lx) + Lx * (y % Ly)) + sub[(U % 2, V % 2)]
+
+    tmpl = [((0, 0), (1, 0)), ((0, 0), (0, 1)), ((1, 0), (0, 1)),
+            ((1, 0), (2, 0)), ((0, 1), (0, 2)), ((1, 0), (2, -1))]
+    edges = set()
+    for x in range(Lx):
+        for y in range(Ly):
+            for (u1, v1), (u2, v2) in tmpl:
+                i, j = index(2 * x + u1, 2 * y + v1), index(2 * x + u2, 2 * y + v2)
+                if i is None or j is None:
+                    continue
+                edges.add((min(i, j), max(i, j)))
+    pos = np.array([x * a1 + y * a2 + basis[b] for y in range(Ly) for x in range(Lx)
+                    for b in range(3)])
+    return Lattice(name="kagome", N=3 * Lx * Ly, edges=sorted(edges),
+                   extras=dict(positions=pos, primitive_vectors=np.array([a1, a2]),
+                               supercell_dims=np.array([Lx, Ly]), sublattice_offsets=basis,
+                               torus=np.array([Lx * a1, Ly * a2])))

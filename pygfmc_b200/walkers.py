@@ -1,0 +1,139 @@
+"""The walker population and its initialisers (PyGFMC walkers/walker.py).
+
+``prepare_walkers_random`` / ``prepare_walkers_sz`` draw exactly what PyGFMC
+draws for the same key (``jax.random.randint`` / ``jax.random.permutation``
+restated over the Threefry stream in :mod:`pygfmc_b200.random`), in PyGFMC's
+float64 mode (``jax_enable_x64``) unless ``x64=False``.
+"""
+from typing import NamedTuple, Sequence
+
+import numpy as np
+
+from . import random as _rnd
+
+__all__ = ["Walker", "prepare_walkers_random", "prepare_walkers_sz",
+           "prepare_walkers_from_configs", "prepare_walkers_occupations"]
+
+
+class Walker(NamedTuple):
+    """Population (or one walker): ``config`` (N_walkers, N_sites), ``log_weight``
+    and ``e_loc`` (N_walkers,) -- walkers/walker.py Walker:50-64."""
+    config: np.ndarray
+    log_weight: np.ndarray
+    e_loc: np.ndarray
+
+
+def _zeros(n, x64):
+    return np.zeros(n, dtype=np.float64 if x64 else np.float32)
+
+
+def prepare_walkers_random(N_walkers, N_sites, rng_key, states=(-1.0, 1.0), x64=True):
+    """Every site an independent uniform draw from ``states`` (walker.py:199-254)."""
+    vals = np.asarray(states)
+    if vals.ndim != 1 or vals.size < 1:
+        raise ValueError(f"states must be a non-empty 1-D sequence of local values; got {states!r}.")
+    if x64 and vals.dtype == np.float32:
+        vals = vals.astype(np.float64)
+    if not x64 and vals.dtype == np.float64:
+        vals = vals.astype(np.float32)
+    idx = _rnd.randint(rng_key, (N_walkers, N_sites), 0, vals.size, x64=x64)
+    return Walker(config=vals[idx], log_weight=_zeros(N_walkers, x64), e_loc=_zeros(N_walkers, x64))
+
+
+def base_config_for_sum(N_sites, target, states):
+    """Greedy multiset of local states summing to ``target`` (walker.py:143-196)."""
+    vals = np.asarray(states, dtype=float).ravel()
+    if vals.size < 1:
+        raise ValueError("states must contain at least one local value.")
+    if np.unique(vals).size != vals.size:
+        raise ValueError(f"states must not repeat a value; got {list(states)}.")
+    den = None
+    for d in (1, 2, 3, 4, 5, 6, 8, 10, 12):
+        if np.allclose(vals * d, np.round(vals * d)) and abs(target * d - round(target * d)) < 1e-9:
+            den = d
+            break
+    if den is None:
+        raise ValueError(f"states={list(states)} and sz={target} are not commensurate with a "
+                         "small common denominator; pass values that are multiples of 1/2, 1/3, 1/4, ...")
+    S = np.sort(np.round(vals * den).astype(np.int64))
+    Z = int(round(target * den))
+    inc = S - S[0]
+    D = Z - N_sites * int(S[0])
+    if D < 0 or D > N_sites * int(inc[-1]):
+        lo, hi = N_sites * vals.min(), N_sites * vals.max()
+        raise ValueError(f"sz={target} is outside the reachable range [{lo}, {hi}] for "
+                         f"N_sites={N_sites} and states={list(states)}.")
+    counts = np.zeros(S.size, dtype=np.int64)
+    remaining, d = N_sites, D
+    for k in range(S.size - 1, 0, -1):
+        take = min(d // int(inc[k]), remaining)
+        counts[k] += take
+        d -= take * int(inc[k])
+        remaining -= take
+    counts[0] += remaining
+    if d != 0:
+        raise ValueError(f"sz={target} is not reachable with N_sites={N_sites} sites drawn from "
+                         f"states={list(states)} (residual {d}/{den}). For a two-state ladder this "
+                         "is the usual parity constraint.")
+    return np.repeat(S, counts).astype(float) / den
+
+
+def prepare_walkers_sz(N_walkers, N_sites, rng_key, sz=0, states=(-1.0, 1.0), x64=True):
+    """Walkers in a fixed-sum sector: one permutation of the greedy base
+    multiset per walker (walker.py:257-306)."""
+    base = base_config_for_sum(N_sites, sz, states)
+    dt = np.asarray(states).dtype
+    if dt.kind == "f":
+        dt = np.float64 if x64 else np.float32
+    keys = _rnd.split(rng_key, N_walkers)
+    configs = _rnd.permutation_rows(keys, base.astype(dt))
+    return Walker(config=configs, log_weight=_zeros(N_walkers, x64), e_loc=_zeros(N_walkers, x64))
+
+
+def prepare_walkers_from_configs(configs, x64=True):
+    """Walkers at given configurations (walker.py:309-342)."""
+    configs = np.asarray(configs)
+    if configs.ndim != 2:
+        raise ValueError(f"configs must have shape (N_walkers, N_sites); got shape {configs.shape}.  "
+                         "For a single configuration copied to every walker use "
+                         "np.tile(config, (N_walkers, 1)).")
+    return Walker(config=configs, log_weight=_zeros(configs.shape[0], x64),
+                  e_loc=_zeros(configs.shape[0], x64))
+
+
+def prepare_walkers_occupations(N_walkers, N_sites, n_total, n_max, rng_key, x64=True):
+    """Occupations drawn uniformly from {n in [0, n_max]^N : sum n = n_total}.
+
+    PyGFMC has no such initialiser (``prepare_walkers_sz`` permutes one greedy
+    base multiset).  Exact uniform sampling over the constrained set: the
+    number of completions ``C(k, s)`` of k remaining sites to the sum s is
+    tabulated, and each site draws its occupation with probability
+    proportional to the completions it leaves.  Draws come from the Threefry
+    stream ``split(rng_key, N_walkers)[w]`` (one 64-bit uniform per site).
+    """
+    if n_total < 0 or n_total > N_sites * n_max:
+        raise ValueError(f"n_total={n_total} unreachable with {N_sites} sites and n_max={n_max}")
+    C = np.zeros((N_sites + 1, n_total + 1), dtype=np.float64)
+    C[0, 0] = 1.0
+    for k in range(1, N_sites + 1):
+        for s in range(n_total + 1):
+            C[k, s] = sum(C[k - 1, s - v] for v in range(0, min(n_max, s) + 1))
+    keys = _rnd.split(rng_key, N_walkers)
+    out = np.zeros((N_walkers, N_sites), dtype=np.float64 if x64 else np.float32)
+    for w in range(N_walkers):
+        y0, y1 = _rnd.threefry2x32(keys[w, 0], keys[w, 1], np.zeros(N_sites, np.uint32),
+                                   np.arange(N_sites, dtype=np.uint32))
+        bits = ((y0.astype(np.uint64) << np.uint64(32)) | y1.astype(np.uint64)) >> np.uint64(11)
+        u = bits.astype(np.float64) * (1.0 / 9007199254740992.0)
+        s = n_total
+        for i in range(N_sites):
+            k = N_sites - i - 1
+            weights = np.array([C[k, s - v] if v <= s else 0.0 for v in range(n_max + 1)])
+            cdf = np.cumsum(weights) / weights.sum()
+            v = int(np.searchsorted(cdf, u[i], side="right"))
+            v = min(v, n_max)
+            while weights[v] == 0:
+                v -= 1
+            out[w, i] = v
+            s -= v
+    return Walker(config=out, log_weight=_zeros(N_walkers, x64), e_loc=_zeros(N_walkers, x64))

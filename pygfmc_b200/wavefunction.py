@@ -1,0 +1,151 @@
+"""Guiding wavefunctions with PyGFMC's constructors.
+
+``JastrowSpinHalf(N, pairs, beta, h=None)`` follows
+``wavefunction/jastrow_spin_half.py:42-157`` and
+``JastrowBoseHubbard(N, pairs, beta, h=None, d=None, incremental=False)``
+follows ``wavefunction/jastrow_bose_hubbard.py:65-125``: the same parameter
+forms (tied scalars or per-pair/per-site arrays), the same conventions
+(``log psi = -sum beta_ij x_i x_j + sum h_i x_i [- sum d_i x_i^2]``) and the
+same validation errors.  ``log_psi`` and ``log_diff_from_operator`` are host
+(numpy) versions for inspection and tests; the engine evaluates the ratios on
+the device from the tables these objects lower to.
+"""
+import numpy as np
+
+from .hamiltonian import BoseHubbard, edges_array
+
+__all__ = ["JastrowSpinHalf", "JastrowBoseHubbard"]
+
+LAYOUT_ATTRS = ("n_hx_static", "n_jpm_static", "edge_i", "edge_j")
+
+
+def require_spin_half_layout(op, guide_name):
+    """wavefunction/_layout.py:14-19."""
+    if not all(hasattr(op, name) for name in LAYOUT_ATTRS):
+        raise TypeError(f"{guide_name} needs an operator with the SpinHalf transition layout "
+                        f"({', '.join(LAYOUT_ATTRS)}); got {type(op).__name__}")
+
+
+class JastrowSpinHalf:
+    """psi_T(x) = exp(sum_{(i,j) in pairs} J_ij x_i x_j + sum_i h_i x_i), J = -beta."""
+
+    def __init__(self, N, pairs, beta, h=None, dtype=np.float32):
+        N = int(N)
+        if pairs is None:
+            raise ValueError("pairs must be provided (n_pairs, 2) int array)")
+        pairs_np, _, n_min = edges_array(pairs)
+        if n_min > N:
+            raise ValueError(f"pair indices must lie in [0, {N}).")
+        pairs_np = np.sort(pairs_np.astype(np.int32), axis=1)
+        n_pairs = pairs_np.shape[0]
+        J = -np.broadcast_to(np.asarray(beta, dtype=np.float64), (n_pairs,))
+        if h is None:
+            h_np = np.zeros(N)
+        else:
+            h_in = np.asarray(h, dtype=np.float64)
+            if h_in.ndim > 1 or (h_in.ndim == 1 and h_in.shape != (N,)):
+                raise ValueError(f"h must be a scalar or have shape ({N},), got {h_in.shape}")
+            h_np = np.broadcast_to(h_in, (N,)).copy()
+        self.dtype = np.dtype(dtype)
+        self.N = N
+        self.pairs = pairs_np
+        self._J = J.copy()
+        self.tied_beta = np.ndim(beta) == 0
+        self._h_given = h
+        self._h = h_np
+
+    @property
+    def beta(self):
+        return -self._J
+
+    @property
+    def h(self):
+        return self._h
+
+    @property
+    def J_pairs(self):
+        return self._J
+
+    def log_psi(self, config):
+        x = np.asarray(config, dtype=np.float64)
+        pair = (self._J * x[..., self.pairs[:, 0]] * x[..., self.pairs[:, 1]]).sum(-1)
+        return pair + (self._h * x).sum(-1)
+
+    def log_diff_from_configs(self, config, new_configs):
+        return self.log_psi(new_configs) - self.log_psi(config)
+
+    def log_diff_from_operator(self, config, op, cache=None):
+        """Host evaluation of the log-ratios in the SpinHalf layout."""
+        require_spin_half_layout(op, type(self).__name__)
+        M = 1 + op.n_hx_static + op.n_jpm_static
+        x = np.asarray(config, dtype=np.float64)
+        base = self.log_psi(x)
+        out = np.zeros(M)
+        for k in range(1, M):
+            out[k] = self.log_psi(op.generate_state(x, k)) - base
+        return out
+
+    def build_cache(self, op):
+        require_spin_half_layout(op, type(self).__name__)
+        return None
+
+
+class JastrowBoseHubbard:
+    """log psi_T(x) = -sum_pairs beta_ij x_i x_j + sum_i h_i x_i - sum_i d_i x_i^2."""
+
+    def __init__(self, N, pairs, beta, h=None, d=None, dtype=np.float32, incremental=False):
+        pairs, _, n_min = edges_array(pairs)
+        if n_min > int(N):
+            raise ValueError(f"pair indices must lie in [0, {N}).")
+        if beta is None:
+            raise ValueError("beta is required (a scalar or an (n_pairs,) array).")
+        self.N = int(N)
+        self.dtype = np.dtype(dtype)
+        self.pair_i = pairs[:, 0].astype(np.int32)
+        self.pair_j = pairs[:, 1].astype(np.int32)
+
+        def param(v, n, name):
+            if v is None:
+                return None
+            a = np.asarray(v, dtype=np.float64)
+            if a.ndim == 0:
+                return float(a)
+            if a.shape != (n,):
+                raise ValueError(f"{name} must be a scalar or have shape ({n},), got {a.shape}")
+            return a
+        self._beta = param(beta, len(pairs), "beta")
+        self._h = param(h, self.N, "h")
+        self._d = param(d, self.N, "d")
+        self.incremental = bool(incremental)
+
+    @property
+    def beta(self):
+        return np.broadcast_to(np.asarray(self._beta, np.float64), self.pair_i.shape)
+
+    @property
+    def h(self):
+        return np.zeros(self.N) if self._h is None else np.broadcast_to(np.asarray(self._h), (self.N,))
+
+    @property
+    def d(self):
+        return np.zeros(self.N) if self._d is None else np.broadcast_to(np.asarray(self._d), (self.N,))
+
+    def log_psi(self, config):
+        n = np.asarray(config, dtype=np.float64)
+        out = -(self.d * n * n).sum(-1)
+        out = out - (self.beta * n[..., self.pair_i] * n[..., self.pair_j]).sum(-1)
+        return out + (self.h * n).sum(-1)
+
+    def log_diff_from_operator(self, config, op, cache=None, state=None):
+        if not isinstance(op, BoseHubbard):
+            raise TypeError(f"{type(self).__name__} evaluates ratios for a BoseHubbard operator; "
+                            f"got {type(op).__name__}")
+        n = np.asarray(config, dtype=np.float64)
+        base = self.log_psi(n)
+        out = np.zeros(op.M_total)
+        for k in range(1, op.M_total):
+            out[k] = self.log_psi(op.generate_state(n, k)) - base
+        return out
+
+    def build_cache(self, op):
+        return None

@@ -1,0 +1,47 @@
+"""The golden-file systems of PyGFMC's tests/core/test_golden_outputs.py
+(_spinhalf:196-216, _bose:233-245), built for the oracle and for the engine."""
+import numpy as np
+
+CASES = [f"{s}_{g}_{m}" for s in ("spinhalf", "bose") for g in ("none", "jastrow")
+         for m in ("cont_time", "single_step", "multi_step")]
+
+
+def oracle_system(O, name):
+    if name.startswith("spinhalf"):
+        e = O.chain_edges(8)
+        m = O.spin_half(e, J_x=-1.0, J_y=-1.0, J_z=1.0, h_x=0.5)
+        cfg = O.prepare_walkers_random(64, 8, O.case_key("spinhalf walkers"))
+        g = O.jastrow_spin_half(8, e, 0.3, 0.05, m) if "_jastrow_" in name else O.no_guide()
+        return m, cfg, g, 0.2, 4.0
+    e = O.chain_edges(6)
+    m = O.bose_hubbard(e, t=1.0, eta=0.3, U=2.0, mu=0.5, h_pm=0.2, n_max=2)
+    cfg = O.prepare_walkers_sz(64, 6, O.case_key("bose walkers"), sz=6, states=(0.0, 1.0, 2.0))
+    g = O.jastrow_bose_hubbard(6, e, 0.05, m, h=0.1, d=0.3) if "_jastrow_" in name else O.no_guide()
+    return m, cfg, g, 0.1, 20.0
+
+
+def engine_system(P, name):
+    if name.startswith("spinhalf"):
+        e = P.chain(8).edges
+        H = P.SpinHalf.create(e, J_x=-1.0, J_y=-1.0, J_z=1.0, h_x=0.5, dtype=np.float64)
+        w = P.prepare_walkers_random(64, 8, P.random.PRNGKey(_crc("spinhalf walkers")))
+        g = P.JastrowSpinHalf(8, e, beta=0.3, h=0.05, dtype=np.float64) if "_jastrow_" in name else None
+        return H, w, g, 0.2, 4.0
+    e = P.chain(6).edges
+    H = P.BoseHubbard.create(e, t=1.0, eta=0.3, U=2.0, mu=0.5, h_pm=0.2, n_max=2, dtype=np.float64)
+    w = P.prepare_walkers_sz(64, 6, P.random.PRNGKey(_crc("bose walkers")), sz=6,
+                             states=(0.0, 1.0, 2.0))
+    g = (P.JastrowBoseHubbard(6, e, beta=0.05, h=0.1, d=0.3, dtype=np.float64)
+         if "_jastrow_" in name else None)
+    return H, w, g, 0.1, 20.0
+
+
+def _crc(s):
+    import zlib
+    return zlib.crc32(s.encode())
+
+
+def method_of(name):
+    for m in ("cont_time", "single_step", "multi_step"):
+        if name.endswith(m):
+            return m

@@ -1,0 +1,54 @@
+"""The C ABI library loads (no GPU needed) and exports every symbol that
+include/gfmc_b200.h declares; host-only entry points work on the CPU."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "gfmc_b200.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(gfmc_[a-z0-9_]+)\s*\(", text)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from pygfmc_b200 import _lib
+    if not os.path.exists(_lib.LIB_PATH):
+        _lib.build()
+    return _lib.load()
+
+
+def test_library_exports_every_declared_symbol(lib):
+    syms = declared_symbols()
+    assert len(syms) >= 15
+    from pygfmc_b200 import _lib
+    for s in syms:
+        assert hasattr(lib, s), s
+        assert s in _lib.SIGNATURES, f"{s} has no ctypes signature"
+
+
+def test_key_schedule_matches_the_reference_recurrence(lib, oracle):
+    from pygfmc_b200.engine import key_schedule
+    key = oracle.case_key("spinhalf_jastrow_cont_time")
+    keys, nxt = key_schedule(key, 300)
+    k = key.copy()
+    for s in range(300):
+        k, r = oracle.split(k, 2)
+        assert np.array_equal(keys[s, :2], oracle.fold_in(r, 0))
+        assert np.array_equal(keys[s, 2:], oracle.fold_in(r, 1))
+    assert np.array_equal(nxt, [4201513499, 1131088919])
+
+
+def test_last_error_and_invalid_arguments(lib):
+    from pygfmc_b200 import _lib
+    rc = lib.gfmc_key_schedule(None, 3, None, None)
+    assert rc == _lib.ERR_INVALID
+    assert "gfmc_key_schedule" in _lib.last_error()
+    with pytest.raises(ValueError):
+        _lib.check(rc, "gfmc_key_schedule")

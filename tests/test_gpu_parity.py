@@ -1,0 +1,154 @@
+"""Parity of the CUDA engine (called through its C ABI) with the oracle and
+with PyGFMC's golden runs.  Float64 build: bit-identical configurations,
+moves and parents; weights, local energies and series within 1e-12 relative
+for one step (1e-10 over whole runs, the golden file's tolerance)."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from golden_cases import CASES, engine_system, method_of, oracle_system
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def P():
+    import pygfmc_b200 as P
+    P._lib.load()
+    return P
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_engine_reproduces_golden_run(P, golden, name):
+    H, w, g, dt, lam = engine_system(P, name)
+    method = method_of(name)
+    step = dt if method == "cont_time" else 2
+    key = golden[name + "/stats/parameters/rng_key"]
+    walkers, energy, obs, stats, raw = P.run(
+        w, 300, H, step, g, [2, 4], method=method, rng_key=key,
+        lam=None if method == "cont_time" else lam, warmup_steps=8, verbosity=0)
+    p = name + "/"
+    assert np.array_equal(walkers.config, golden[p + "config"].astype(np.float64))
+    np.testing.assert_allclose(raw["log_weights"], golden[p + "raw/log_weights"], rtol=1e-10, atol=1e-12)
+    np.testing.assert_allclose(raw["energy"], golden[p + "raw/energy"], rtol=1e-10, atol=1e-12)
+    np.testing.assert_allclose(walkers.e_loc, golden[p + "e_loc"], rtol=1e-10, atol=1e-12)
+    np.testing.assert_allclose(stats["avg_log_weight"], golden[p + "stats/avg_log_weight"], rtol=1e-10)
+    for pp in (2, 4):
+        np.testing.assert_allclose(energy[pp], golden[p + f"energy/{pp}"], rtol=1e-10, atol=1e-12)
+    assert np.array_equal(stats["parameters/rng_key_next"], golden[p + "stats/parameters/rng_key_next"])
+
+
+def _systems(P, O):
+    """(name, engine H, engine guide, oracle model, oracle guide, configs, step, lam)."""
+    out = []
+    e = P.chain(32).edges
+    H = P.SpinHalf.create(e, J_x=-1.0, J_y=-1.0, J_z=1.0, h_x=0.3, dtype=np.float64)
+    m = O.spin_half(e, J_x=-1.0, J_y=-1.0, J_z=1.0, h_x=0.3)
+    cfg = P.prepare_walkers_random(512, 32, P.PRNGKey(11)).config
+    out.append(("chain32_hx_none", H, None, m, O.no_guide(), cfg))
+    G = P.JastrowSpinHalf(32, e, beta=0.3, h=0.05)
+    out.append(("chain32_hx_jastrow", H, G, m, O.jastrow_spin_half(32, e, 0.3, 0.05, m), cfg))
+    sq = P.square(4)
+    Hs = P.SpinHalf.create(sq.edges, J_x=-1.0, J_y=-1.0, J_z=1.0, dtype=np.float64)
+    ms = O.spin_half(sq.edges, J_x=-1.0, J_y=-1.0, J_z=1.0)
+    pairs = np.array([(i, j) for i in range(16) for j in range(i + 1, 16)])
+    pos = sq.extras["positions"]
+    d = pos[pairs[:, 0]] - pos[pairs[:, 1]]
+    d = np.abs(d); d = np.minimum(d, 4 - d); r = np.sqrt((d ** 2).sum(1))
+    beta = 0.3 / r
+    Gs = P.JastrowSpinHalf(16, pairs, beta=beta)
+    cfgs = P.prepare_walkers_sz(512, 16, P.PRNGKey(12), sz=0).config
+    out.append(("square4_longrange", Hs, Gs, ms, O.jastrow_spin_half(16, pairs, beta, None, ms), cfgs))
+    eb = P.chain(12).edges
+    B = P.BoseHubbard.create(eb, t=1.0, eta=0.2, U=3.0, mu=0.4, h_pm=0.1, n_max=3, dtype=np.float64)
+    mb = O.bose_hubbard(eb, t=1.0, eta=0.2, U=3.0, mu=0.4, h_pm=0.1, n_max=3)
+    betas = np.linspace(0.02, 0.2, 12)
+    GB = P.JastrowBoseHubbard(12, eb, beta=betas, h=0.1, d=np.linspace(0.1, 0.3, 12))
+    gb = O.jastrow_bose_hubbard(12, eb, betas, mb, h=0.1, d=np.linspace(0.1, 0.3, 12))
+    occ = P.prepare_walkers_sz(512, 12, P.PRNGKey(13), sz=12, states=(0.0, 1.0, 2.0, 3.0)).config
+    out.append(("bose12_jastrow", B, GB, mb, gb, occ))
+    GBt = P.JastrowBoseHubbard(12, eb, beta=0.1, d=0.2)
+    gbt = O.jastrow_bose_hubbard(12, eb, 0.1, mb, d=0.2)
+    out.append(("bose12_jastrow_tied", B, GBt, mb, gbt, occ))
+    return out
+
+
+def _raw_cfg(eng, torch):
+    out = torch.empty((eng.n, eng.N), dtype=torch.float64, device=eng.device)
+    eng.L.gfmc_unpack(eng.h, eng.n, ctypes.c_void_p(eng.cfg.data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                      eng._stream())
+    return out.cpu().numpy()
+
+
+@pytest.mark.parametrize("method,step,lam", [("cont_time", 0.15, None), ("single_step", 3, 12.0),
+                                             ("multi_step", 4, 12.0)])
+def test_one_step_parity_with_oracle(P, oracle, method, step, lam):
+    import torch
+    O = oracle
+    for name, H, G, m, g, cfg in _systems(P, O):
+        eng = P.GFMCEngine(H, G, cfg.shape[0], precision="fp64")
+        eng.load(cfg)
+        key = P.PRNGKey(77)
+        keys, _ = P.engine.key_schedule(key, 1)
+        lg = torch.empty(1, dtype=torch.float64, device=eng.device)
+        En = torch.empty(1, dtype=torch.float64, device=eng.device)
+        alw = -1.3
+        eng.steps(method, step, lam, alw, keys, lg, En)
+        c_gpu = _raw_cfg(eng, torch)
+        lw_gpu = eng.log_w.cpu().numpy(); el_gpu = eng.e_loc.cpu().numpy()
+        par_gpu = eng.parents.cpu().numpy()
+        c = np.array(cfg, dtype=np.float64, copy=True)
+        lw = np.zeros(len(c)); el = np.zeros(len(c))
+        O.evolve(m, g, method, step, lam, alw, keys[0, :2], c, lw, el)
+        assert np.array_equal(c_gpu, c), f"{name}: configurations differ"
+        np.testing.assert_allclose(lw_gpu, lw, rtol=1e-12, atol=1e-12, err_msg=name)
+        np.testing.assert_allclose(el_gpu, el, rtol=1e-12, atol=1e-12, err_msg=name)
+        par, lG, E = O.reconfigure(keys[0, 2:], c, lw, el)
+        assert np.array_equal(par_gpu, par), f"{name}: parents differ"
+        np.testing.assert_allclose(lg.item(), lG, rtol=1e-12, atol=1e-13, err_msg=name)
+        np.testing.assert_allclose(En.item(), E, rtol=1e-12, atol=1e-12, err_msg=name)
+
+
+def test_trajectory_parity_with_oracle(P, oracle):
+    """60 chained production steps of the long-range Jastrow on the 4x4 torus:
+    the final population is identical and the series agree to 1e-10."""
+    O = oracle
+    name, H, G, m, g, cfg = _systems(P, O)[2]
+    key = P.PRNGKey(5)
+    _, _, _, stats, raw = P.run(P.Walker(cfg, np.zeros(len(cfg)), np.zeros(len(cfg))), 60, H, 0.1, G,
+                                [4], rng_key=key, warmup_steps=8, verbosity=0)
+    r = O.run(cfg, 60, m, 0.1, g, [4], rng_key=key, warmup_steps=8)
+    np.testing.assert_allclose(raw["log_weights"], r.log_weights, rtol=1e-10, atol=1e-12)
+    np.testing.assert_allclose(raw["energy"], r.energy_series, rtol=1e-10, atol=1e-12)
+    np.testing.assert_allclose(stats["avg_log_weight"], r.alw, rtol=1e-10)
+
+
+def test_mixed_precision_agrees_with_fp64(P):
+    """The mixed build (float32 rates/ratios, float64 accumulators) gives the
+    fp64 build's energy within the combined jackknife error."""
+    e = P.chain(16).edges
+    H = P.SpinHalf.create(e, J_x=-1.0, J_y=-1.0, J_z=1.0, dtype=np.float64)
+    G = P.JastrowSpinHalf(16, e, beta=0.3)
+    w = P.prepare_walkers_sz(2048, 16, P.PRNGKey(0), sz=0)
+    res = {}
+    for prec in ("fp64", "mixed"):
+        _, E, _, st, raw = P.run(w, 2000, H, 0.1, G, [8, 32], rng_key=P.PRNGKey(1), warmup_steps=200,
+                                 verbosity=0, precision=prec)
+        Ej, err = P.estimators.jackknife_energy([32], raw["log_weights"], raw["energy"], 20)
+        res[prec] = (Ej[32], err[32])
+    (a, ea), (b, eb) = res["fp64"], res["mixed"]
+    assert abs(a - b) < 4 * np.hypot(ea, eb) + 1e-6, res
+    # exact ground state of the periodic 16-site Heisenberg chain
+    assert abs(a / 16 - (-0.4463935)) < 5e-3
+
+
+def test_hop_cap_is_reported_not_hung(P):
+    """A step so long that every walker exceeds the iteration cap returns
+    with a status error instead of spinning."""
+    e = P.chain(8).edges
+    H = P.SpinHalf.create(e, J_x=-1.0, J_y=-1.0, J_z=1.0, dtype=np.float64)
+    w = P.prepare_walkers_sz(32, 8, P.PRNGKey(0), sz=0)
+    with pytest.raises(P._lib.GFMCError, match="iteration cap"):
+        P.run(w, 4, H, 500.0, None, [2], rng_key=P.PRNGKey(1), warmup_steps=4, verbosity=0,
+              max_hops_per_step=64)

@@ -1,0 +1,123 @@
+"""Host-side API: constructors and validation mirror PyGFMC, the walker
+initialisers draw PyGFMC's walkers, and the lattices are the reference's."""
+import numpy as np
+import pytest
+
+import pygfmc_b200 as P
+
+
+def test_spinhalf_create_conventions_and_errors():
+    H = P.SpinHalf.create(P.chain(6).edges, J_x=-1.0, J_y=-1.0, J_z=1.0, h_x=0.4)
+    assert H.M_total == 1 + 6 + 6 and H.n_hx == 6 and H.n_jpm == 6
+    assert float(H.J_pm[0]) == -0.5 and float(H.J_pmpm[0]) == 0.0
+    assert np.allclose(H.h_x_half, -0.2)
+    with pytest.raises(ValueError, match="J_pmpm"):
+        P.SpinHalf.create([(0, 1)], J_x=1.0, J_y=-1.0)
+    with pytest.raises(ValueError, match="J_pm"):
+        P.SpinHalf.create([(0, 1)], J_x=1.0, J_y=1.0)
+    with pytest.raises(ValueError, match="h_x"):
+        P.SpinHalf.create([(0, 1)], J_x=-1.0, J_y=-1.0, h_x=-0.3)
+    with pytest.raises(ValueError, match="self-edges"):
+        P.SpinHalf.create([(1, 1)], J_x=-1.0, J_y=-1.0)
+    S = P.SpinHalf.create([(0, 1)], J_x=1.0, J_y=1.0, sign_check=False)
+    assert S.M_total == 2
+
+
+def test_bose_hubbard_create_conventions_and_errors():
+    H = P.BoseHubbard.create(P.chain(6).edges, t=1.0, eta=0.3, U=2.0, mu=0.5, h_pm=0.2, n_max=2)
+    assert H.M_total == 1 + 12 + 12 + 12
+    assert np.allclose(H.h_pm, -0.2)
+    with pytest.raises(ValueError, match="t must"):
+        P.BoseHubbard.create([(0, 1)], t=-1.0)
+    with pytest.raises(ValueError, match="n_max"):
+        P.BoseHubbard.create([(0, 1)], t=1.0, n_max=0)
+
+
+def test_host_rates_match_oracle(oracle):
+    e = P.chain(8).edges
+    H = P.SpinHalf.create(e, J_x=-1.0, J_y=-1.0, J_z=1.0, h_x=0.5, h_z=0.1, dtype=np.float64)
+    m = oracle.spin_half(e, J_x=-1.0, J_y=-1.0, J_z=1.0, h_x=0.5, h_z=0.1)
+    cfg = P.prepare_walkers_random(16, 8, P.PRNGKey(3)).config
+    r_or = oracle.rates(m, oracle.no_guide(), cfg)
+    for w in range(16):
+        np.testing.assert_allclose(H.get_rates(cfg[w])[0], r_or[w], rtol=1e-14, atol=1e-15)
+    B = P.BoseHubbard.create(P.chain(6).edges, t=1.0, eta=0.3, U=2.0, mu=0.5, h_pm=0.2, n_max=2,
+                             dtype=np.float64)
+    mb = oracle.bose_hubbard(P.chain(6).edges, t=1.0, eta=0.3, U=2.0, mu=0.5, h_pm=0.2, n_max=2)
+    occ = P.prepare_walkers_sz(16, 6, P.PRNGKey(4), sz=6, states=(0.0, 1.0, 2.0)).config
+    r_or = oracle.rates(mb, oracle.no_guide(), occ)
+    for w in range(16):
+        np.testing.assert_allclose(B.get_rates(occ[w])[0], r_or[w], rtol=1e-14, atol=1e-15)
+
+
+def test_guide_ratios_match_log_psi_differences(oracle):
+    """tests/core/test_guides.py:145 idea: the oracle's ratio tables equal
+    log_psi differences of the guide objects."""
+    e = P.chain(8).edges
+    H = P.SpinHalf.create(e, J_x=-1.0, J_y=-1.0, J_z=1.0, h_x=0.5)
+    G = P.JastrowSpinHalf(8, e, beta=0.3, h=0.05)
+    m = oracle.spin_half(e, J_x=-1.0, J_y=-1.0, J_z=1.0, h_x=0.5)
+    g = oracle.jastrow_spin_half(8, e, 0.3, 0.05, m)
+    cfg = P.prepare_walkers_random(8, 8, P.PRNGKey(5)).config
+    guided = oracle.rates(m, g, cfg)
+    bare = oracle.rates(m, oracle.no_guide(), cfg)
+    for w in range(8):
+        ld = G.log_diff_from_operator(cfg[w], H)
+        expect = bare[w] * np.exp(np.where(bare[w] == 0, 0, ld))
+        np.testing.assert_allclose(guided[w], expect, rtol=1e-12, atol=1e-14)
+    B = P.BoseHubbard.create(P.chain(6).edges, t=1.0, eta=0.3, U=2.0, mu=0.5, h_pm=0.2, n_max=2)
+    GB = P.JastrowBoseHubbard(6, P.chain(6).edges, beta=[0.05, 0.1, 0.02, 0.3, 0.07, 0.01],
+                              h=0.1, d=np.linspace(0.1, 0.4, 6))
+    mb = oracle.bose_hubbard(P.chain(6).edges, t=1.0, eta=0.3, U=2.0, mu=0.5, h_pm=0.2, n_max=2)
+    gb = oracle.jastrow_bose_hubbard(6, P.chain(6).edges, np.array([0.05, 0.1, 0.02, 0.3, 0.07, 0.01]),
+                                     mb, h=0.1, d=np.linspace(0.1, 0.4, 6))
+    occ = P.prepare_walkers_sz(8, 6, P.PRNGKey(6), sz=6, states=(0.0, 1.0, 2.0)).config
+    guided = oracle.rates(mb, gb, occ)
+    bare = oracle.rates(mb, oracle.no_guide(), occ)
+    for w in range(8):
+        ld = GB.log_diff_from_operator(occ[w], B)
+        expect = bare[w] * np.exp(np.where(bare[w] == 0, 0, ld))
+        np.testing.assert_allclose(guided[w], expect, rtol=1e-12, atol=1e-14)
+
+
+def test_walker_initialisers_match_oracle(oracle):
+    k = oracle.case_key("spinhalf walkers")
+    assert np.array_equal(P.prepare_walkers_random(64, 8, k).config, oracle.prepare_walkers_random(64, 8, k))
+    k = oracle.case_key("bose walkers")
+    a = P.prepare_walkers_sz(64, 6, k, sz=6, states=(0.0, 1.0, 2.0)).config
+    assert np.array_equal(a, oracle.prepare_walkers_sz(64, 6, k, sz=6, states=(0.0, 1.0, 2.0)))
+    w = P.prepare_walkers_sz(128, 100, P.PRNGKey(0), sz=0)
+    assert np.all(w.config.sum(1) == 0) and w.config.dtype == np.float64
+    occ = P.prepare_walkers_occupations(64, 16, 16, 4, P.PRNGKey(1)).config
+    assert np.all(occ.sum(1) == 16) and occ.max() <= 4 and occ.min() >= 0
+
+
+def test_lattices():
+    assert P.chain(100).edges[-1] == (99, 0) and len(P.chain(100).edges) == 100
+    sq = P.square(16)
+    assert sq.N == 256 and len(sq.edges) == 512
+    kg = P.kagome(12, 12)
+    assert kg.N == 432 and len(kg.edges) == 864
+    deg = np.bincount(np.asarray(kg.edges).ravel(), minlength=432)
+    assert np.all(deg == 4)
+
+
+def test_run_validation_errors_before_any_work():
+    w = P.prepare_walkers_sz(8, 6, P.PRNGKey(0))
+    H = P.SpinHalf.create(P.chain(6).edges, J_x=-1.0, J_y=-1.0, J_z=1.0)
+    with pytest.raises(ValueError, match="step_size must be > 0"):
+        P.run(w, 10, H, -0.1, None, [2])
+    with pytest.raises(ValueError, match="integer step_size"):
+        P.run(w, 10, H, 0.5, None, [2], method="single_step", lam=4.0)
+    with pytest.raises(ValueError, match="needs the GFMC shift"):
+        P.run(w, 10, H, 2, None, [2], method="single_step")
+    with pytest.raises(ValueError, match="n_steps"):
+        P.run(w, 0, H, 0.1, None, [2])
+    with pytest.raises(ValueError, match="p_array"):
+        P.run(w, 10, H, 0.1, None, [])
+    with pytest.raises(ValueError, match="smaller than n_steps"):
+        P.run(w, 10, H, 0.1, None, [10], rng_key=P.PRNGKey(1))
+    with pytest.raises(ValueError, match="warmup_steps=0 needs"):
+        P.run(w, 10, H, 0.1, None, [2], warmup_steps=0, rng_key=P.PRNGKey(1))
+    with pytest.raises(TypeError):
+        P.run(w, 10, object(), 0.1, None, [2], rng_key=P.PRNGKey(1))
