@@ -1,5 +1,6 @@
 // C ABI of the engine (include/gfmc_b200.h): table construction, the host
 // loop of a chunk of branching steps, and the small helpers around it.
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -70,6 +71,15 @@ struct gfmc_handle {
   double *pmax = nullptr, *psum = nullptr, *pE = nullptr, *cdf = nullptr, *wbuf = nullptr;
   int *plp = nullptr, *ctr = nullptr, *status = nullptr;
   unsigned long long *hops = nullptr;
+  // carried guide fields (W / S per walker), double-buffered through the
+  // parent map; rebuilt from scratch for a fresh population and every
+  // refresh_every steps against rounding drift of the incremental updates
+  int carry = 0;
+  int refresh_every = 100;
+  void *fbuf[2] = {nullptr, nullptr};
+  int fcur = 0, field_valid = 0, since_refresh = 0;
+  const void *field_cfg = nullptr;
+  int cap_field = 0;
 };
 
 namespace {
@@ -117,6 +127,13 @@ int build_tables(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_des
     put("jz", md->jz, m.has_jz ? (m.uniform_jz ? 1 : E) : 0);
     put("hz", md->hz, m.has_hz ? N : 0);
     put("hx_half", md->hx_half, m.n_hx ? N : 0);
+    m.uniform_pm = 1;
+    if (m.n_jpm) {
+      for (int e = 1; e < E; ++e)
+        if (md->jpm[e] != md->jpm[0] || md->jpmpm[e] != md->jpmpm[0]) m.uniform_pm = 0;
+      m.jpm0 = (T)md->jpm[0];
+      m.jpmpm0 = (T)md->jpmpm[0];
+    }
     h->cfg_bytes = ((N + 63) / 64) * 8;
   } else if (md->kind == GFMC_MODEL_BOSE_HUBBARD) {
     m.n_max = md->n_max;
@@ -151,7 +168,7 @@ int build_tables(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_des
       gk != GFMC_GUIDE_JASTROW_BOSE_HUBBARD)
     return fail(GFMC_ERR_UNSUPPORTED, "unknown guide kind %d", gk);
   g.kind = gk;
-  size_t o_nbr = 0, o_nbrw = 0, o_cnt = 0, o_jsum = 0, o_tpw = 0;
+  size_t o_nbr = 0, o_nbrw = 0, o_cnt = 0, o_tpw = 0, o_jd = 0, o_ep = 0, o_em = 0;
   if (gk != GFMC_GUIDE_NONE) {
     // per-site partner lists, duplicates merged (each partner once per site)
     std::vector<std::map<int, double>> lists(N);
@@ -177,9 +194,41 @@ int build_tables(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_des
       cnt[k] = c;
     }
     g.deg = deg;
+    // dense couplings when most pairs are present: coalesced rows, no indices
+    g.dense = (2 * deg > N) ? 1 : 0;
+    if (g.dense) {
+      std::vector<T> Jd((size_t)N * N, T(0));
+      for (int k = 0; k < N; ++k)
+        for (auto &kv : lists[k]) Jd[(size_t)k * N + kv.first] = (T)kv.second;
+      o_jd = A.add(Jd.data(), Jd.size() * sizeof(T));
+      if (gk == GFMC_GUIDE_JASTROW_SPIN_HALF) {
+        // multiplicative factor updates exp(+-4 J_kp) (1 where no pair)
+        std::vector<T> ep((size_t)N * N, T(1)), em((size_t)N * N, T(1));
+        for (int k = 0; k < N; ++k)
+          for (auto &kv : lists[k]) {
+            ep[(size_t)k * N + kv.first] = (T)std::exp(4.0 * kv.second);
+            em[(size_t)k * N + kv.first] = (T)std::exp(-4.0 * kv.second);
+          }
+        o_ep = A.add(ep.data(), ep.size() * sizeof(T));
+        o_em = A.add(em.data(), em.size() * sizeof(T));
+      }
+    } else if (gk == GFMC_GUIDE_JASTROW_SPIN_HALF) {
+      std::vector<T> ep((size_t)N * deg, T(1)), em((size_t)N * deg, T(1));
+      for (int k = 0; k < N; ++k) {
+        int c = 0;
+        for (auto &kv : lists[k]) {
+          ep[(size_t)k * deg + c] = (T)std::exp(4.0 * kv.second);
+          em[(size_t)k * deg + c] = (T)std::exp(-4.0 * kv.second);
+          ++c;
+        }
+      }
+      o_ep = A.add(ep.data(), ep.size() * sizeof(T));
+      o_em = A.add(em.data(), em.size() * sizeof(T));
+    }
     o_nbr = A.add(nbr.data(), nbr.size() * 4);
     o_nbrw = A.add(nbrw.data(), nbrw.size() * sizeof(T));
     o_cnt = A.add(cnt.data(), cnt.size() * 4);
+    h->carry = (g.dense || deg >= 16) ? 1 : 0;
     auto pair_sum = [&](int a, int b) -> double {
       if (a == b) return 0.0;
       auto it = lists[a].find(b);
@@ -188,10 +237,21 @@ int build_tables(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_des
     if (gk == GFMC_GUIDE_JASTROW_SPIN_HALF) {
       std::vector<double> hh(N, 0.0);
       if (gd->h) for (int k = 0; k < N; ++k) hh[k] = gd->h[k];
+      for (int k = 0; k < N; ++k) g.has_h |= (hh[k] != 0.0);
       put("gh", hh.data(), N);
-      std::vector<T> js(E > 0 ? E : 1, T(0));
-      for (int e = 0; e < E; ++e) js[e] = (T)pair_sum(md->edge_i[e], md->edge_j[e]);
-      o_jsum = A.add(js.data(), js.size() * sizeof(T));
+      // per-edge constants of the factored edge-flip ratio: exp(-+4 Jsum_e)
+      std::vector<double> ca(E > 0 ? E : 1, 1.0), cp(E > 0 ? E : 1, 1.0);
+      g.uniform_c = 1;
+      for (int e = 0; e < E; ++e) {
+        const double js = pair_sum(md->edge_i[e], md->edge_j[e]);
+        ca[e] = exp(-4.0 * js);
+        cp[e] = exp(4.0 * js);
+        if (ca[e] != ca[0] || cp[e] != cp[0]) g.uniform_c = 0;
+      }
+      g.c_anti0 = (T)ca[0];
+      g.c_par0 = (T)cp[0];
+      put("c_anti", ca.data(), E);
+      put("c_par", cp.data(), E);
     } else {
       // per-transition summed pair weight (JastrowBoseHubbardOpCache.pair_w)
       std::vector<T> tpw(m.M, T(0));
@@ -234,8 +294,33 @@ int build_tables(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_des
     g.nbr_cnt = (const int *)(base + o_cnt);
     g.h = ptr("gh");
     g.d = ptr("gd");
-    if (gk == GFMC_GUIDE_JASTROW_SPIN_HALF) g.edge_jsum = (const T *)(base + o_jsum);
-    else g.trans_pw = (const T *)(base + o_tpw);
+    if (gk == GFMC_GUIDE_JASTROW_SPIN_HALF) {
+      g.c_anti = ptr("c_anti");
+      g.c_par = ptr("c_par");
+    } else {
+      g.trans_pw = (const T *)(base + o_tpw);
+    }
+    if (g.dense) g.Jd = (const T *)(base + o_jd);
+    if (gk == GFMC_GUIDE_JASTROW_SPIN_HALF) {
+      if (g.dense) {
+        g.Ep = (const T *)(base + o_ep);
+        g.Em = (const T *)(base + o_em);
+      } else {
+        g.nbr_ep = (const T *)(base + o_ep);
+        g.nbr_em = (const T *)(base + o_em);
+      }
+    }
+  }
+  // fast spin layout (see DevModel::fast)
+  if (m.family == SPIN_HALF) {
+    const bool guided_ok = gk == GFMC_GUIDE_NONE || (gk == GFMC_GUIDE_JASTROW_SPIN_HALF && g.uniform_c);
+    m.fast = (m.n_hx == 0 && m.n_jpm == E && E > 0 && m.uniform_pm && (!m.has_jz || m.uniform_jz) &&
+              !m.has_hz && guided_ok) ? 1 : 0;
+    if (m.fast) {
+      const bool gd_on = gk == GFMC_GUIDE_JASTROW_SPIN_HALF;
+      m.k_anti = m.jpm0 * (gd_on ? g.c_anti0 : T(1));
+      m.k_par = m.jpmpm0 * (gd_on ? g.c_par0 : T(1));
+    }
   }
   cudaError_t e = plan_evolve<T>(m, g, m.M, &h->plan);
   if (e != cudaSuccess)
@@ -266,7 +351,18 @@ int ensure_scratch(gfmc_handle *h, int n, int n_steps) {
     GFMC_CUDA(cudaMalloc(&h->hops, sizeof(unsigned long long) * n_steps));
     h->cap_steps = n_steps;
   }
-  if (!h->pmax) GFMC_CUDA(cudaMalloc(&h->pmax, sizeof(double) * (h->plan.grid > 0 ? h->plan.grid : 1)));
+  if (!h->pmax)
+    GFMC_CUDA(cudaMalloc(&h->pmax, sizeof(double) * (size_t)(h->plan.grid > 0 ? h->plan.grid : 1) *
+                                       (h->plan.wpb > 0 ? h->plan.wpb : 1)));
+  if (h->carry && n > h->cap_field) {
+    size_t tsz = h->precision == GFMC_PRECISION_FP64 ? sizeof(double) : sizeof(float);
+    cudaFree(h->fbuf[0]); cudaFree(h->fbuf[1]);
+    h->fbuf[0] = h->fbuf[1] = nullptr;
+    GFMC_CUDA(cudaMalloc(&h->fbuf[0], tsz * (size_t)n * h->N));
+    GFMC_CUDA(cudaMalloc(&h->fbuf[1], tsz * (size_t)n * h->N));
+    h->cap_field = n;
+    h->field_valid = 0;
+  }
   if (!h->status) {
     GFMC_CUDA(cudaMalloc(&h->status, sizeof(int)));
     GFMC_CUDA(cudaMemset(h->status, 0, sizeof(int)));
@@ -287,9 +383,7 @@ int run_steps_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, int 
   GFMC_CUDA(cudaMemsetAsync(h->ctr, 0, sizeof(int) * n_steps, s));
   unsigned long long *hops = hops_out ? (unsigned long long *)hops_out : h->hops;
   GFMC_CUDA(cudaMemsetAsync(hops, 0, sizeof(unsigned long long) * n_steps, s));
-  int grid = h->plan.grid;
-  int need = (n + h->plan.wpb - 1) / h->plan.wpb;
-  if (grid > need) grid = need;
+  const int n_partials = evolve_partials(h->plan, n);
   void *cur = cfg, *nxt = cfg_tmp;
   for (int st = 0; st < n_steps; ++st) {
     EvolveArgs a{};
@@ -309,6 +403,16 @@ int run_steps_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, int 
     a.partial_max = h->pmax;
     a.status = h->status;
     a.max_iters = h->max_iters;
+    if (h->carry) {
+      const bool fresh = (st == 0 && !parents_valid) || !h->field_valid || h->field_cfg != cfg ||
+                         h->since_refresh >= h->refresh_every;
+      a.field_in = fresh ? nullptr : h->fbuf[h->fcur];
+      a.field_out = h->fbuf[1 - h->fcur];
+      h->fcur = 1 - h->fcur;
+      h->field_valid = 1;
+      h->field_cfg = cfg;
+      h->since_refresh = fresh ? 1 : h->since_refresh + 1;
+    }
     cudaError_t e = launch_evolve<T>(m, g, h->plan, a, s);
     if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "evolve launch: %s", cudaGetErrorString(e));
     ReconArgs r{};
@@ -316,7 +420,7 @@ int run_steps_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, int 
     r.log_w = log_w;
     r.e_loc = e_loc;
     r.partial_max = h->pmax;
-    r.n_partial_max = grid;
+    r.n_partial_max = n_partials;
     r.key = Key{keys[4 * st + 2], keys[4 * st + 3]};
     r.psum = h->psum;
     r.pE = h->pE + (size_t)st * nb;
@@ -386,6 +490,8 @@ int gfmc_create(const gfmc_model_desc *model, const gfmc_guide_desc *guide, int 
     return rc;
   }
   h->M = precision == GFMC_PRECISION_FP64 ? h->m64.M : h->m32.M;
+  // float32 factors drift faster under the multiplicative updates
+  h->refresh_every = precision == GFMC_PRECISION_FP64 ? 100 : 50;
   *out = h;
   g_last_error.clear();
   return GFMC_OK;
@@ -396,6 +502,7 @@ int gfmc_destroy(gfmc_handle *h) {
   cudaFree(h->d_tables);
   cudaFree(h->pmax); cudaFree(h->psum); cudaFree(h->pE); cudaFree(h->cdf); cudaFree(h->wbuf);
   cudaFree(h->plp); cudaFree(h->ctr); cudaFree(h->status); cudaFree(h->hops);
+  cudaFree(h->fbuf[0]); cudaFree(h->fbuf[1]);
   delete h;
   return GFMC_OK;
 }
@@ -410,6 +517,7 @@ int gfmc_pack(gfmc_handle *h, int n, const double *cfg, void *packed, void *stre
     GFMC_CUDA(cudaMemset(h->status, 0, sizeof(int)));
   }
   if (n == 0) return GFMC_OK;
+  h->field_valid = 0;
   cudaError_t e = launch_pack(h->family, n, h->N, h->cfg_bytes, cfg, packed, h->n_max, h->status,
                               (cudaStream_t)stream);
   if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "pack: %s", cudaGetErrorString(e));

@@ -30,6 +30,14 @@ template <typename T> struct DevModel {
   // SpinHalf
   int n_hx, n_jpm, has_jz, uniform_jz, has_hz;
   const T *jz, *jpm, *jpmpm, *hz, *hx_half;
+  int uniform_pm;         // every edge has the same (J_pm, J_pmpm)
+  T jpm0, jpmpm0;
+  // Fast spin layout: no site-flip moves, uniform couplings (and uniform
+  // guide edge constants), no h_z.  Edge rate = k_anti |s_i s_j| for
+  // anti-parallel spins, k_par |s_i s_j| for parallel ones, where
+  // s_k = x_k A_k are the signed ratio factors (A = 1 without a guide).
+  int fast;
+  T k_anti, k_par;
   // BoseHubbard
   int n_max, n_hop, n_eta, n_hpm, has_U, has_mu;
   const T *t, *eta, *U, *mu, *hpm;
@@ -46,7 +54,6 @@ template <typename T> struct DevGuide {
   const T *nbr_w;         // (N, deg) couplings
   const int *nbr_cnt;     // (N,) partners per site
   const T *h;             // (N,) one-body field (spin: JastrowSpinHalf.h)
-  const T *edge_jsum;     // (E,) spin: summed J of the pairs joining each H edge
   const T *trans_pw;      // (M,) bose: summed pair weight joining each transition's sites
   T beta_scale;           // bose: -beta for a tied beta, else 1
   int h_mode;             // bose: 0 none, 1 tied (h0), 2 array (h)
@@ -54,6 +61,19 @@ template <typename T> struct DevGuide {
   int d_mode;             // bose: 0 none, 1 tied (d0), 2 array (d)
   T d0;
   const T *d;
+  int has_h;              // spin: any nonzero one-body field
+  // spin-1/2 Jastrow ratio of an edge flip, factored as A_i A_j c_e with the
+  // per-site A_k = exp(-2 x_k (W_k + h_k)) and the per-edge constant
+  // c_e = exp(4 Jsum_e x_i x_j): c_anti = exp(-4 Jsum_e), c_par = exp(4 Jsum_e)
+  const T *c_anti, *c_par;
+  int uniform_c;
+  T c_anti0, c_par0;
+  // multiplicative factor updates after a flip of site s (x_s before the
+  // flip): A_k *= exp(4 x_k x_s J_sk), i.e. Ep = exp(4 J), Em = exp(-4 J)
+  const T *Ep, *Em;       // dense: (N, N)
+  const T *nbr_ep, *nbr_em;   // sparse: (N, deg), aligned with nbr
+  int dense;              // couplings as a dense symmetric (N, N) matrix Jd
+  const T *Jd;            // (N, N) row-major, zero diagonal (dense == 1)
 };
 
 struct EvolveArgs {
@@ -73,6 +93,8 @@ struct EvolveArgs {
   double *partial_max;    // (grid,) block max of log_w
   int *status;
   int max_iters;          // per-walker hop cap
+  const void *field_in;   // carried guide fields (N per walker), read at parents[w]; nullable
+  void *field_out;        // guide fields after the step (N per walker); nullable
 };
 
 struct LaunchPlan {
@@ -87,6 +109,8 @@ cudaError_t launch_evolve(const DevModel<T> &m, const DevGuide<T> &g, const Laun
 template <typename T>
 cudaError_t plan_evolve(const DevModel<T> &m, const DevGuide<T> &g, int n_slots_max,
                         LaunchPlan *plan);
+// Number of per-warp partial maxima an evolve launch over n_walkers writes.
+int evolve_partials(const LaunchPlan &plan, int n_walkers);
 
 // Reconfiguration (reconfig.cu), always float64.
 struct ReconArgs {

@@ -1,21 +1,27 @@
 // The per-walker propagation step of GFMC on B200: one warp per walker.
 //
-// Per warp, in shared memory: the walker configuration (bit-packed spins or
-// uint8 occupations), the guide's local fields (W_k = sum_p J_kp x_p for the
-// spin-1/2 Jastrow, S_k = sum_p w_kp n_p for the Bose-Hubbard Jastrow,
-// updated incrementally after every move), and the scanned transition
-// weights of the current configuration.  Per CTA, in shared memory: the edge
-// list, the couplings and, when they fit, the guide's partner tables.
+// Per warp, in shared memory, the walker's state.  A spin-1/2 walker is held
+// as signed ratio factors s_k = x_k A_k, A_k = exp(-2 x_k (W_k + h_k)) with
+// W_k = sum_p J_kp x_p the Jastrow field (A = 1 without a guide): the sign is
+// the spin, an edge is anti-parallel iff s_i s_j < 0, and the guide ratio of
+// flipping it is |s_i s_j| times a per-edge constant, so a rate costs two
+// shared loads and two multiplies and the hop loop evaluates no exp; a flip
+// updates s multiplicatively (s_k *= exp(+-4 J_ak), s_a -> -1/s_a).  A
+// Bose-Hubbard walker is held as uint8 occupations plus its Jastrow fields
+// S_k = sum_p w_kp n_p, updated additively.  Per CTA, in shared memory: the edge list, the
+// couplings and, when they fit, the guide's partner tables.
 //
-// Each rate evaluation enumerates the off-diagonal moves in rows of 32 slots
-// (one slot per lane), computes the guide-transformed Green's-function
-// elements tau |H_x'x| psi(x')/psi(x) (here: the rates of
-// engine/evolution.py transition_rates:205-261), scans them with warp
-// shuffles and draws the move by inverse CDF (sample_index:30-59).  The
-// propagators follow engine/evolution.py: cont_time (559-721), single_step
-// (322-406), multi_step (409-556); each walker consumes the JAX Threefry
-// stream split(key, N_walkers)[w] with fold_in(., 2 i) / fold_in(., 2 i + 1)
-// per hold (single_step: fold_in(., i) per sub-step).
+// A rate evaluation enumerates the off-diagonal moves (the Green's-function
+// elements tau |H_x'x| psi(x')/psi(x), i.e. the rates of
+// engine/evolution.py transition_rates:205-261) with each lane owning a
+// contiguous chunk of C slots (C odd, so the chunk-strided shared-memory
+// accesses are conflict-free): the lane sums its chunk in order, one warp
+// shuffle scan combines the 32 chunk totals, and the inverse-CDF draw
+// (sample_index:30-59) finds its lane by ballot and its slot by a warp scan
+// of that lane's chunk, re-evaluated by C lanes at once.  The propagators follow engine/evolution.py:
+// cont_time (559-721), single_step (322-406), multi_step (409-556); each
+// walker consumes the JAX Threefry stream split(key, N_walkers)[w] with
+// fold_in(., 2 i) / fold_in(., 2 i + 1) per hold (single_step: fold_in(., i)).
 #include <cfloat>
 
 #include "engine.cuh"
@@ -50,14 +56,15 @@ __host__ __device__ inline size_t stage_tables(DevModel<T> &m, DevGuide<T> &g, i
   size_t off = 0;
   m.edge = stage_arr(m.edge, m.E, base, off, copy);
   if (m.family == SPIN_HALF) {
-    m.jpm = stage_arr(m.jpm, m.n_jpm ? m.E : 0, base, off, copy);
-    m.jpmpm = stage_arr(m.jpmpm, m.n_jpm ? m.E : 0, base, off, copy);
+    m.jpm = stage_arr(m.jpm, (m.n_jpm && !m.uniform_pm) ? m.E : 0, base, off, copy);
+    m.jpmpm = stage_arr(m.jpmpm, (m.n_jpm && !m.uniform_pm) ? m.E : 0, base, off, copy);
     m.jz = stage_arr(m.jz, m.has_jz ? (m.uniform_jz ? 1 : m.E) : 0, base, off, copy);
     m.hz = stage_arr(m.hz, m.has_hz ? m.N : 0, base, off, copy);
     m.hx_half = stage_arr(m.hx_half, m.n_hx ? m.N : 0, base, off, copy);
     if (g.kind == GUIDE_JASTROW_SPIN) {
-      g.h = stage_arr(g.h, m.N, base, off, copy);
-      g.edge_jsum = stage_arr(g.edge_jsum, m.E, base, off, copy);
+      g.h = stage_arr(g.h, g.has_h ? m.N : 0, base, off, copy);
+      g.c_anti = stage_arr(g.c_anti, g.uniform_c ? 0 : m.E, base, off, copy);
+      g.c_par = stage_arr(g.c_par, g.uniform_c ? 0 : m.E, base, off, copy);
     }
   } else {
     m.t = stage_arr(m.t, m.n_hop ? m.E : 0, base, off, copy);
@@ -71,10 +78,14 @@ __host__ __device__ inline size_t stage_tables(DevModel<T> &m, DevGuide<T> &g, i
       g.d = stage_arr(g.d, g.d_mode == 2 ? m.N : 0, base, off, copy);
     }
   }
-  if (g.kind != GUIDE_NONE && stage_nbr) {
+  if (g.kind != GUIDE_NONE && stage_nbr && !g.dense) {
     g.nbr = stage_arr(g.nbr, m.N * g.deg, base, off, copy);
     g.nbr_w = stage_arr(g.nbr_w, m.N * g.deg, base, off, copy);
     g.nbr_cnt = stage_arr(g.nbr_cnt, m.N, base, off, copy);
+    if (g.kind == GUIDE_JASTROW_SPIN) {
+      g.nbr_ep = stage_arr(g.nbr_ep, m.N * g.deg, base, off, copy);
+      g.nbr_em = stage_arr(g.nbr_em, m.N * g.deg, base, off, copy);
+    }
   }
   return (off + 15) & ~size_t(15);
 }
@@ -82,22 +93,30 @@ __host__ __device__ inline size_t stage_tables(DevModel<T> &m, DevGuide<T> &g, i
 __host__ __device__ inline int spin_words(int N) { return (N + 63) / 64; }
 __host__ __device__ inline int bose_bytes(int N) { return ((N + 15) / 16) * 16; }
 
-// Per-warp shared region, sized on the host by the same function.
+// Slots per lane for n_slots moves: ceil(n/32), rounded up to odd.
+__host__ __device__ inline int chunk_of(int n_slots) {
+  int c = (n_slots + 31) / 32;
+  if (c < 1) c = 1;
+  return c | 1;
+}
+
+struct WarpLayout {
+  size_t fa, bytes;
+};
+
+// Per-warp shared region (configuration words or occupations, then the
+// per-site state: the signed ratio factors s_k = x_k A_k of a spin-1/2 walker,
+// or the Jastrow fields of a Bose-Hubbard walker), sized on the host by the
+// same function.
 template <typename T>
-__host__ __device__ inline size_t warp_region(const DevModel<T> &m, const DevGuide<T> &g,
-                                              int n_slots_max, size_t *o_field, size_t *o_q,
-                                              size_t *o_rowend) {
+__host__ __device__ inline WarpLayout warp_layout(const DevModel<T> &m, const DevGuide<T> &g) {
+  WarpLayout L;
   size_t off = (m.family == SPIN_HALF) ? (size_t)spin_words(m.N) * 8 : (size_t)bose_bytes(m.N);
   off = (off + 15) & ~size_t(15);
-  *o_field = off;
-  if (g.kind != GUIDE_NONE) off += (size_t)m.N * sizeof(T);
-  off = (off + 15) & ~size_t(15);
-  *o_q = off;
-  int rows = (n_slots_max + 31) / 32;
-  off += (size_t)rows * 32 * sizeof(T);
-  *o_rowend = off;
-  off += (size_t)rows * sizeof(T);
-  return (off + 15) & ~size_t(15);
+  L.fa = off;
+  if (m.family == SPIN_HALF || g.kind != GUIDE_NONE) off += (size_t)m.N * sizeof(T);
+  L.bytes = (off + 15) & ~size_t(15);
+  return L;
 }
 
 // ---- configuration access ---------------------------------------------------
@@ -109,50 +128,6 @@ template <typename T, int FAM>
 __device__ __forceinline__ T site_val(const uint64_t *bits, const uint8_t *occ, int k) {
   if (FAM == SPIN_HALF) return spin_x<T>(bits, k);
   return T(occ[k]);
-}
-
-// ---- diagonal element -------------------------------------------------------
-// SpinHalf.diagonal_weight:291-314, BoseHubbard.diagonal_weight:271-281.
-template <typename T, int FAM>
-__device__ __forceinline__ T diag_elem(const DevModel<T> &m, const uint64_t *bits,
-                                       const uint8_t *occ, int lane) {
-  if (FAM == SPIN_HALF) {
-    int na = 0;
-    T jzs = T(0), hzs = T(0);
-    if (m.has_jz) {
-      for (int e = lane; e < m.E; e += 32) {
-        uint32_t pe = m.edge[e];
-        int i = pe & 0xFFFF, j = pe >> 16;
-        bool anti = (((bits[i >> 6] >> (i & 63)) ^ (bits[j >> 6] >> (j & 63))) & 1ull) != 0;
-        if (m.uniform_jz) na += anti;
-        else jzs += anti ? -m.jz[e] / T(4) : m.jz[e] / T(4);
-      }
-    }
-    if (m.has_hz)
-      for (int k = lane; k < m.N; k += 32) hzs += m.hz[k] * spin_x<T>(bits, k);
-    T d = T(0);
-    if (m.has_jz) {
-      if (m.uniform_jz) {
-        na = warp_sum(na);
-        d = (m.jz[0] / T(4)) * T(m.E - 2 * na);
-      } else {
-        d = warp_sum(jzs);
-      }
-    }
-    if (m.has_hz) d = d + warp_sum(hzs) / T(2);
-    return d;
-  } else {
-    T su = T(0), sm = T(0);
-    for (int k = lane; k < m.N; k += 32) {
-      T n = T(occ[k]);
-      if (m.has_U) su += m.U[k] * n * (n - T(1));
-      if (m.has_mu) sm += m.mu[k] * n;
-    }
-    T d = T(0);
-    if (m.has_U) d = d + T(0.5) * warp_sum(su);
-    if (m.has_mu) d = d - warp_sum(sm);
-    return d;
-  }
 }
 
 // ---- Bose-Hubbard transition layout (bose_hubbard.py module docstring;
@@ -193,73 +168,60 @@ __device__ __forceinline__ BoseMove bose_decode(const DevModel<T> &m, int o) {
   return mv;
 }
 
-// The off-diagonal matrix element of move o (<= 0 for a sign-free model),
-// with the guide ratio folded in (evolution.transition_rates:255-260).
-template <typename T, int FAM>
-__device__ __forceinline__ T offdiag(const DevModel<T> &m, const DevGuide<T> &g,
-                                     const uint64_t *bits, const uint8_t *occ, const T *F, int o) {
-  if (FAM == SPIN_HALF) {
-    if (o < m.n_hx) {
-      T v = m.hx_half[o];
-      if (g.kind && v != T(0)) {
-        T x = spin_x<T>(bits, o);
-        T ld = T(-2) * x * F[o] - T(2) * g.h[o] * x;           // _site_log_diff:290-297
-        v *= math_exp(ld);
-      }
-      return v;
-    }
-    int e = o - m.n_hx;
-    uint32_t pe = m.edge[e];
-    int i = pe & 0xFFFF, j = pe >> 16;
-    T xi = spin_x<T>(bits, i), xj = spin_x<T>(bits, j);
-    T v = (xi != xj) ? m.jpm[e] : m.jpmpm[e];
-    if (g.kind && v != T(0)) {
-      // _edge_log_diff_from_cache:462-472 with sum_{b!=j} J_ib x_b = W_i - Jsum_ij x_j
-      T pair = xi * F[i] + xj * F[j] - T(2) * g.edge_jsum[e] * xi * xj;
-      T ld = T(-2) * pair - T(2) * (g.h[i] * xi + g.h[j] * xj);
-      v *= math_exp(ld);
-    }
-    return v;
-  } else {
-    BoseMove mv = bose_decode(m, o);
-    T na = T(occ[mv.a]), nb = T(occ[mv.b]);
-    T nmax = T(m.n_max);
-    T v;
-    switch (mv.blk) {
-      case 0: v = -m.t[mv.idx] * math_sqrt(na * (nb + T(1))) * (nb < nmax ? T(1) : T(0)); break;
-      case 1: v = -m.t[mv.idx] * math_sqrt((na + T(1)) * nb) * (na < nmax ? T(1) : T(0)); break;
-      case 2:
-        v = -m.eta[mv.idx] * math_sqrt((na + T(1)) * (nb + T(1))) *
-            ((na < nmax && nb < nmax) ? T(1) : T(0));
-        break;
-      case 3: v = -m.eta[mv.idx] * math_sqrt(na * nb); break;
-      case 4: v = m.hpm[mv.idx] * math_sqrt(na + T(1)) * (na < nmax ? T(1) : T(0)); break;
-      default: v = m.hpm[mv.idx] * math_sqrt(na); break;
-    }
-    if (g.kind && v != T(0)) {
-      // JastrowBoseHubbard.log_diff_from_operator:253-286
-      T da = T(mv.da), db = T(mv.db);
-      T out = T(0);
-      if (g.d_mode) {
-        T dsa = (na + da) * (na + da) - na * na, dsb = (nb + db) * (nb + db) - nb * nb;
-        out = (g.d_mode == 2) ? -(g.d[mv.a] * dsa + g.d[mv.b] * dsb) : -g.d0 * (dsa + dsb);
-      }
-      T pw = g.trans_pw[o + 1];
-      if (g.beta_scale == T(1)) out = out + da * F[mv.a] + db * F[mv.b] + da * db * pw;
-      else out = out + g.beta_scale * (da * F[mv.a] + db * F[mv.b] + da * db * pw);
-      if (g.h_mode == 2) out = out + (g.h[mv.a] * da + g.h[mv.b] * db);
-      else if (g.h_mode == 1) out = out + g.h0 * (da + db);
-      v *= math_exp(out);
-    }
-    return v;
+// Off-diagonal element of Bose-Hubbard move o (<= 0), guide ratio folded in:
+// BoseHubbard.get_rates:285-393, JastrowBoseHubbard.log_diff_from_operator:253-286.
+template <typename T>
+__device__ __forceinline__ T bose_offdiag(const DevModel<T> &m, const DevGuide<T> &g,
+                                          const uint8_t *occ, const T *F, int o) {
+  BoseMove mv = bose_decode(m, o);
+  T na = T(occ[mv.a]), nb = T(occ[mv.b]);
+  T nmax = T(m.n_max);
+  T v;
+  switch (mv.blk) {
+    case 0: v = -m.t[mv.idx] * math_sqrt(na * (nb + T(1))) * (nb < nmax ? T(1) : T(0)); break;
+    case 1: v = -m.t[mv.idx] * math_sqrt((na + T(1)) * nb) * (na < nmax ? T(1) : T(0)); break;
+    case 2:
+      v = -m.eta[mv.idx] * math_sqrt((na + T(1)) * (nb + T(1))) *
+          ((na < nmax && nb < nmax) ? T(1) : T(0));
+      break;
+    case 3: v = -m.eta[mv.idx] * math_sqrt(na * nb); break;
+    case 4: v = m.hpm[mv.idx] * math_sqrt(na + T(1)) * (na < nmax ? T(1) : T(0)); break;
+    default: v = m.hpm[mv.idx] * math_sqrt(na); break;
   }
+  if (g.kind && v != T(0)) {
+    T da = T(mv.da), db = T(mv.db);
+    T out = T(0);
+    if (g.d_mode) {
+      T dsa = (na + da) * (na + da) - na * na, dsb = (nb + db) * (nb + db) - nb * nb;
+      out = (g.d_mode == 2) ? -(g.d[mv.a] * dsa + g.d[mv.b] * dsb) : -g.d0 * (dsa + dsb);
+    }
+    T pw = g.trans_pw[o + 1];
+    if (g.beta_scale == T(1)) out = out + da * F[mv.a] + db * F[mv.b] + da * db * pw;
+    else out = out + g.beta_scale * (da * F[mv.a] + db * F[mv.b] + da * db * pw);
+    if (g.h_mode == 2) out = out + (g.h[mv.a] * da + g.h[mv.b] * db);
+    else if (g.h_mode == 1) out = out + g.h0 * (da + db);
+    v *= math_exp(out);
+  }
+  return v;
 }
 
-// Field of every site from scratch: W_k / S_k.
+// ---- guide state ---------------------------------------------------------------
+// Field of every site from scratch into F.  Dense couplings accumulate the
+// rows of J (coalesced, fixed order p = 0..N-1); sparse ones walk the
+// partner lists.
 template <typename T, int FAM>
 __device__ __forceinline__ void field_init(const DevModel<T> &m, const DevGuide<T> &g,
                                            const uint64_t *bits, const uint8_t *occ, T *F,
                                            int lane) {
+  if (g.dense) {
+    for (int k = lane; k < m.N; k += 32) F[k] = T(0);
+    for (int p = 0; p < m.N; ++p) {
+      const T xp = site_val<T, FAM>(bits, occ, p);
+      const T *row = g.Jd + (size_t)p * m.N;
+      for (int k = lane; k < m.N; k += 32) F[k] += row[k] * xp;
+    }
+    return;
+  }
   for (int k = lane; k < m.N; k += 32) {
     T s = T(0);
     const int c = g.nbr_cnt[k];
@@ -270,7 +232,91 @@ __device__ __forceinline__ void field_init(const DevModel<T> &m, const DevGuide<
   }
 }
 
-// Field update after site k changed by delta (spin: delta = -2 x_old).
+// Signed ratio factors of a spin-1/2 walker from its configuration:
+// s_k = x_k A_k, A_k = exp(-2 x_k (W_k + h_k)) the exp of
+// JastrowSpinHalf._site_log_diff:290-297 (A = 1 without a guide).
+template <typename T>
+__device__ __forceinline__ void signed_init(const DevModel<T> &m, const DevGuide<T> &g,
+                                            const uint64_t *bits, T *S, int lane) {
+  if (g.kind == GUIDE_NONE) {
+    for (int k = lane; k < m.N; k += 32) S[k] = spin_x<T>(bits, k);
+    __syncwarp();
+    return;
+  }
+  field_init<T, SPIN_HALF>(m, g, bits, nullptr, S, lane);
+  __syncwarp();
+  for (int k = lane; k < m.N; k += 32) {
+    const T x = spin_x<T>(bits, k);
+    S[k] = x * math_exp(T(-2) * x * (g.has_h ? S[k] + g.h[k] : S[k]));
+  }
+  __syncwarp();
+}
+
+// Flip of spin a (the sequential update of one flip): its partners k get
+// A_k *= exp(4 x_k x_a J_ak) (x_a before the flip), then s_a -> -1 / s_a.
+template <typename T>
+__device__ __forceinline__ void flip_one(const DevModel<T> &m, const DevGuide<T> &g, T *S, int a,
+                                         int lane) {
+  const T sa = S[a];
+  if (g.kind != GUIDE_NONE) {
+    const bool ua = sa > T(0);
+    if (g.dense) {
+      const T *ep = g.Ep + (size_t)a * m.N, *em = g.Em + (size_t)a * m.N;
+      for (int k = lane; k < m.N; k += 32) {
+        const T sk = S[k];
+        S[k] = sk * (((sk > T(0)) == ua) ? ep[k] : em[k]);
+      }
+    } else {
+      const int c = g.nbr_cnt[a];
+      const uint32_t *nb = g.nbr + (size_t)a * g.deg;
+      const T *ep = g.nbr_ep + (size_t)a * g.deg, *em = g.nbr_em + (size_t)a * g.deg;
+      for (int d = lane; d < c; d += 32) {
+        const int k = (int)nb[d];
+        const T sk = S[k];
+        S[k] = sk * (((sk > T(0)) == ua) ? ep[d] : em[d]);
+      }
+    }
+    __syncwarp();
+    if (lane == 0) S[a] = T(-1) / sa;
+  } else {
+    if (lane == 0) S[a] = -sa;
+  }
+  __syncwarp();
+}
+
+// Flip of the pair (a, b): for dense couplings both rows in one pass (their
+// loads overlap), with the two endpoints fixed up as the sequential flips
+// a-then-b would leave them; sparse couplings flip one after the other.
+template <typename T>
+__device__ __forceinline__ void flip_pair(const DevModel<T> &m, const DevGuide<T> &g, T *S, int a,
+                                          int b, int lane) {
+  if (g.kind == GUIDE_NONE || !g.dense) {
+    flip_one(m, g, S, a, lane);
+    flip_one(m, g, S, b, lane);
+    return;
+  }
+  const T sa = S[a], sb = S[b];
+  const bool ua = sa > T(0), ub = sb > T(0);
+  const T *epa = g.Ep + (size_t)a * m.N, *ema = g.Em + (size_t)a * m.N;
+  const T *epb = g.Ep + (size_t)b * m.N, *emb = g.Em + (size_t)b * m.N;
+  for (int k = lane; k < m.N; k += 32) {
+    const T sk = S[k];
+    const bool uk = sk > T(0);
+    const T fa = (uk == ua) ? epa[k] : ema[k];
+    const T fb = (uk == ub) ? epb[k] : emb[k];
+    S[k] = sk * fa * fb;
+  }
+  __syncwarp();
+  if (lane == 0) {
+    const T fba = ((!ua) == ub) ? epb[a] : emb[a];   // row b at a, x_a after its flip
+    const T fab = (ub == ua) ? epa[b] : ema[b];      // row a at b, x_b before its flip
+    S[a] = (T(-1) / sa) * fba;
+    S[b] = T(-1) / (sb * fab);
+  }
+  __syncwarp();
+}
+
+// Bose-Hubbard Jastrow field update after site k changed by delta.
 template <typename T>
 __device__ __forceinline__ void field_update(const DevGuide<T> &g, T *F, int k, T delta, int lane) {
   const int c = g.nbr_cnt[k];
@@ -280,25 +326,16 @@ __device__ __forceinline__ void field_update(const DevGuide<T> &g, T *F, int k, 
   __syncwarp();
 }
 
-// Apply move o (off-diagonal index) to the warp's configuration and fields.
+// Apply move o (off-diagonal index) to the walker's state.
 template <typename T, int FAM>
 __device__ __forceinline__ void apply_move(const DevModel<T> &m, const DevGuide<T> &g,
-                                           uint64_t *bits, uint8_t *occ, T *F, int o, int lane) {
+                                           uint8_t *occ, T *SF, int o, int lane) {
   if (FAM == SPIN_HALF) {
-    int s0, s1;
-    if (o < m.n_hx) { s0 = o; s1 = -1; }
-    else { uint32_t pe = m.edge[o - m.n_hx]; s0 = pe & 0xFFFF; s1 = pe >> 16; }
-    T x0 = spin_x<T>(bits, s0);
-    T x1 = s1 >= 0 ? spin_x<T>(bits, s1) : T(0);
-    __syncwarp();
-    if (lane == 0) {
-      bits[s0 >> 6] ^= 1ull << (s0 & 63);
-      if (s1 >= 0) bits[s1 >> 6] ^= 1ull << (s1 & 63);
-    }
-    __syncwarp();
-    if (g.kind) {
-      field_update(g, F, s0, T(-2) * x0, lane);
-      if (s1 >= 0) field_update(g, F, s1, T(-2) * x1, lane);
+    if (o < m.n_hx) {
+      flip_one(m, g, SF, o, lane);
+    } else {
+      const uint32_t pe = m.edge[o - m.n_hx];
+      flip_pair(m, g, SF, (int)(pe & 0xFFFF), (int)(pe >> 16), lane);
     }
   } else {
     BoseMove mv = bose_decode(m, o);
@@ -308,91 +345,187 @@ __device__ __forceinline__ void apply_move(const DevModel<T> &m, const DevGuide<
       occ[mv.b] = (uint8_t)(occ[mv.b] + mv.db);
     }
     __syncwarp();
-    if (g.kind) {
-      field_update(g, F, mv.a, T(mv.da), lane);
-      if (mv.db != 0) field_update(g, F, mv.b, T(mv.db), lane);
+    if (g.kind != GUIDE_NONE) {
+      field_update(g, SF, mv.a, T(mv.da), lane);
+      if (mv.db != 0) field_update(g, SF, mv.b, T(mv.db), lane);
     }
   }
 }
 
-// Pass 1: fill q[s] for every slot and scan.  lamform (single_step): slot 0
-// is the diagonal, q = rates, cdf = lam - cumsum(q); otherwise q = -rates
-// of the off-diagonal moves and cdf = cumsum(q).  Returns the scanned total.
-template <typename T, int FAM>
-__device__ __forceinline__ T scan_pass(const DevModel<T> &m, const DevGuide<T> &g,
-                                       const uint64_t *bits, const uint8_t *occ, const T *F,
-                                       T *q, T *rowend, int n_slots, bool lamform, T diag,
-                                       int lane) {
-  const int rows = (n_slots + 31) >> 5;
-  T carry = T(0);
-  for (int r = 0; r < rows; ++r) {
-    const int s = (r << 5) + lane;
-    T v = T(0);
-    if (s < n_slots) {
-      if (lamform) v = (s == 0) ? diag : offdiag<T, FAM>(m, g, bits, occ, F, s - 1);
-      else v = -offdiag<T, FAM>(m, g, bits, occ, F, s);
+// Off-diagonal element of move o (<= 0 for a sign-free model) with the
+// guide ratio folded in (evolution.transition_rates:255-260).  Spin-1/2: a
+// site flip costs -h_x/2 A_k = hx_half |s_k|; an edge flip the coupling of
+// its spin alignment times A_i A_j c_e = |s_i s_j| c_e (c_e = exp(4 Jsum_e
+// x_i x_j), the pair's own term).  *anti: the edge's spins are anti-parallel.
+template <typename T, int FAM, int FAST>
+__device__ __forceinline__ T offdiag(const DevModel<T> &m, const DevGuide<T> &g,
+                                     const uint8_t *occ, const T *SF, int o, int *anti_out) {
+  if (FAM == SPIN_HALF) {
+    if (!FAST && o < m.n_hx) {
+      const T v = m.hx_half[o];
+      return v != T(0) ? v * fabs(SF[o]) : v;
     }
-    q[s] = v;
-    T inc = warp_inclusive_scan(v, lane) + carry;
-    carry = __shfl_sync(FULL, inc, 31);
-    if (lane == 0) rowend[r] = carry;
+    const int e = FAST ? o : o - m.n_hx;
+    const uint32_t pe = m.edge[e];
+    const T p = SF[pe & 0xFFFF] * SF[pe >> 16];
+    const bool anti = p < T(0);
+    *anti_out = anti;
+    if (FAST) return anti ? m.k_anti * (-p) : m.k_par * p;
+    const T b = m.uniform_pm ? (anti ? m.jpm0 : m.jpmpm0) : (anti ? m.jpm[e] : m.jpmpm[e]);
+    if (g.kind != GUIDE_NONE && b != T(0)) {
+      const T c = g.uniform_c ? (anti ? g.c_anti0 : g.c_par0) : (anti ? g.c_anti[e] : g.c_par[e]);
+      return b * fabs(p) * c;
+    }
+    return b;
   }
-  __syncwarp();
-  return carry;
+  return bose_offdiag<T>(m, g, occ, SF, o);
 }
 
-// Pass 2: evolution.sample_index on the scanned slots for the threshold u:
-// the first slot whose cdf exceeds u, stepped back to the nearest slot at or
-// before it with positive weight.
-template <typename T>
-__device__ __forceinline__ int warp_sample(const T *q, const T *rowend, int n_slots,
-                                           bool lamform, T lam, T u, int lane) {
-  const int rows = (n_slots + 31) >> 5;
-  int rstar = rows - 1;
-  for (int base = 0; base < rows; base += 32) {
-    int r = base + lane;
-    bool hit = false;
-    if (r < rows) {
-      T c = lamform ? lam - rowend[r] : rowend[r];
-      hit = c > u;
+// Result of one rate evaluation, per lane.
+template <typename T> struct Eval {
+  T diag;    // H_xx (warp-uniform)
+  T excl;    // scanned total of the lanes before this one
+  T end;     // excl + this lane's chunk total
+  T total;   // scanned total of all slots (warp-uniform)
+  int C;     // slots per lane
+};
+
+// One rate evaluation.  lamform (single_step): slot 0 is the diagonal and
+// the scanned values are the rates, cdf = lam - cumsum(rates); otherwise the
+// slots are the off-diagonal moves and the scanned values their weights
+// -rates, cdf = cumsum(weights).
+template <typename T, int FAM, int FAST>
+__device__ __forceinline__ Eval<T> evaluate(const DevModel<T> &m, const DevGuide<T> &g,
+                                            const uint8_t *occ, const T *SF, int n_slots,
+                                            bool lamform, int lane) {
+  Eval<T> ev;
+  const int C = chunk_of(n_slots);
+  ev.C = C;
+  const bool spin = FAM == SPIN_HALF;
+  const bool fused_diag = spin && m.has_jz && m.n_jpm == m.E && m.E > 0;
+  int na = 0;
+  T jzs = T(0);
+  T acc = T(0);
+  const int s0 = lane * C;
+  int jmax = n_slots - s0;
+  jmax = jmax < 0 ? 0 : (jmax > C ? C : jmax);
+  for (int j = 0; j < jmax; ++j) {
+    const int o = lamform ? s0 + j - 1 : s0 + j;
+    if (o >= 0) {
+      int anti = -1;
+      const T v = offdiag<T, FAM, FAST>(m, g, occ, SF, o, &anti);
+      if (fused_diag && anti >= 0) {
+        if (FAST || m.uniform_jz) na += anti;
+        else jzs += anti ? -m.jz[o - m.n_hx] / T(4) : m.jz[o - m.n_hx] / T(4);
+      }
+      acc += lamform ? v : -v;
     }
-    unsigned bal = __ballot_sync(FULL, hit);
-    if (bal) { rstar = base + __ffs(bal) - 1; break; }
   }
-  T carry = rstar > 0 ? rowend[rstar - 1] : T(0);
-  int s = (rstar << 5) + lane;
-  T inc = warp_inclusive_scan(q[s], lane) + carry;
-  T c = lamform ? lam - inc : inc;
-  unsigned bal = __ballot_sync(FULL, s < n_slots && c > u);
-  int idx = bal ? (rstar << 5) + __ffs(bal) - 1 : (rstar << 5) + 31;
-  if (idx > n_slots - 1) idx = n_slots - 1;
-  for (int r = idx >> 5; r >= 0; --r) {
-    int s2 = (r << 5) + lane;
-    T q2 = q[s2];
-    T w2 = lamform ? (s2 == 0 ? (-q2 + lam) : -q2) : q2;
-    unsigned b2 = __ballot_sync(FULL, s2 <= idx && s2 < n_slots && w2 > T(0));
-    if (b2) return (r << 5) + 31 - __clz(b2);
+  // diagonal element: SpinHalf.diagonal_weight:291-314, BoseHubbard:271-281
+  T d = T(0);
+  if (spin) {
+    if (!FAST && m.has_jz && !fused_diag) {
+      for (int e = lane; e < m.E; e += 32) {
+        const uint32_t pe = m.edge[e];
+        const bool anti = SF[pe & 0xFFFF] * SF[pe >> 16] < T(0);
+        if (m.uniform_jz) na += anti;
+        else jzs += anti ? -m.jz[e] / T(4) : m.jz[e] / T(4);
+      }
+    }
+    if (m.has_jz) {
+      if (FAST || m.uniform_jz) d = (m.jz[0] / T(4)) * T(m.E - 2 * warp_sum(na));
+      else d = warp_sum(jzs);
+    }
+    if (!FAST && m.has_hz) {
+      T hzs = T(0);
+      for (int k = lane; k < m.N; k += 32) hzs += m.hz[k] * (SF[k] > T(0) ? T(1) : T(-1));
+      d = d + warp_sum(hzs) / T(2);
+    }
+  } else {
+    T su = T(0), sm = T(0);
+    for (int k = lane; k < m.N; k += 32) {
+      const T n = T(occ[k]);
+      if (m.has_U) su += m.U[k] * n * (n - T(1));
+      if (m.has_mu) sm += m.mu[k] * n;
+    }
+    if (m.has_U) d = d + T(0.5) * warp_sum(su);
+    if (m.has_mu) d = d - warp_sum(sm);
   }
-  return idx;
+  ev.diag = d;
+  if (lamform && lane == 0) acc = d + acc;   // slot 0 carries the diagonal
+  const T inc = warp_inclusive_scan(acc, lane);
+  T excl = __shfl_up_sync(FULL, inc, 1);
+  if (lane == 0) excl = T(0);
+  ev.excl = excl;
+  ev.end = excl + acc;
+  const int last_lane = n_slots > 0 ? (n_slots - 1) / C : 0;
+  ev.total = __shfl_sync(FULL, ev.end, last_lane);
+  return ev;
 }
 
-template <typename T, int FAM>
-__global__ void __launch_bounds__(256)
-evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int n_slots_max,
-              int cta_bytes, int warp_bytes) {
+// Scanned value and weight of slot s (valid slots only).
+template <typename T, int FAM, int FAST>
+__device__ __forceinline__ T slot_q(const DevModel<T> &m, const DevGuide<T> &g, const uint8_t *occ,
+                                    const T *SF, int s, bool lamform, T diag) {
+  if (lamform && s == 0) return diag;
+  int anti;
+  const T v = offdiag<T, FAM, FAST>(m, g, occ, SF, lamform ? s - 1 : s, &anti);
+  return lamform ? v : -v;
+}
+
+// evolution.sample_index: the first slot whose cdf exceeds u, stepped back to
+// the nearest slot at or before it with positive weight.  The lane whose
+// chunk holds the crossing is found by ballot; its chunk is re-evaluated by
+// C lanes at once and scanned.  The step-back past that chunk (a zero-weight
+// crossing with no positive slot before it in the chunk) re-evaluates the
+// earlier chunks the same way.
+template <typename T, int FAM, int FAST>
+__device__ __forceinline__ int sample_slot(const DevModel<T> &m, const DevGuide<T> &g,
+                                           const uint8_t *occ, const T *SF, const Eval<T> &ev,
+                                           int n_slots, bool lamform, T lam, T u, int lane) {
+  const int C = ev.C;
+  const int last_lane = (n_slots - 1) / C;
+  const T cend = lamform ? lam - ev.end : ev.end;
+  const unsigned bal = __ballot_sync(FULL, lane <= last_lane && cend > u);
+  const int L = bal ? __ffs(bal) - 1 : last_lane;
+  const T exclL = __shfl_sync(FULL, ev.excl, L);
+  int s = L * C + lane;
+  bool valid = lane < C && s < n_slots;
+  T qv = valid ? slot_q<T, FAM, FAST>(m, g, occ, SF, s, lamform, ev.diag) : T(0);
+  const T pre = warp_inclusive_scan(qv, lane);
+  const T c = lamform ? lam - (exclL + pre) : exclL + pre;
+  const unsigned hit = __ballot_sync(FULL, valid && c > u);
+  const int nvalid = (n_slots - L * C) < C ? (n_slots - L * C) : C;
+  const int jh = hit ? __ffs(hit) - 1 : nvalid - 1;
+  T w = lamform ? (s == 0 ? (-qv + lam) : -qv) : qv;
+  unsigned bk = __ballot_sync(FULL, valid && lane <= jh && w > T(0));
+  if (bk) return L * C + 31 - __clz(bk);
+  for (int L2 = L - 1; L2 >= 0; --L2) {
+    s = L2 * C + lane;
+    valid = lane < C && s < n_slots;
+    qv = valid ? slot_q<T, FAM, FAST>(m, g, occ, SF, s, lamform, ev.diag) : T(0);
+    w = lamform ? (s == 0 ? (-qv + lam) : -qv) : qv;
+    bk = __ballot_sync(FULL, valid && w > T(0));
+    if (bk) return L2 * C + 31 - __clz(bk);
+  }
+  return L * C + jh;
+}
+
+// 256 threads and 4 blocks per SM: 64 registers, 32 resident warps per SM
+// (a warp's shared state is ~2 KB, so registers bound the occupancy).
+template <typename T, int FAM, int FAST>
+__global__ void __launch_bounds__(256, FAM == SPIN_HALF ? 4 : 2)
+evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta_bytes) {
   extern __shared__ __align__(16) unsigned char smem[];
   stage_tables(m, g, stage_nbr, smem, true);
   __syncthreads();
 
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  size_t o_field, o_q, o_rowend;
-  warp_region(m, g, n_slots_max, &o_field, &o_q, &o_rowend);
-  unsigned char *wb = smem + cta_bytes + (size_t)wib * warp_bytes;
+  const WarpLayout WL = warp_layout(m, g);
+  unsigned char *wb = smem + cta_bytes + (size_t)wib * WL.bytes;
   uint64_t *bits = reinterpret_cast<uint64_t *>(wb);
   uint8_t *occ = wb;
-  T *F = reinterpret_cast<T *>(wb + o_field);
-  T *q = reinterpret_cast<T *>(wb + o_q);
-  T *rowend = reinterpret_cast<T *>(wb + o_rowend);
+  T *SF = reinterpret_cast<T *>(wb + WL.fa);
 
   const int NW = spin_words(m.N);
   const int CB = bose_bytes(m.N);
@@ -400,7 +533,6 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int n_s
   const bool guided = g.kind != GUIDE_NONE;
   const T lam = T(a.lam);
   double wmax = -DBL_MAX;
-  bool any_walker = false;
   unsigned long long hop_acc = 0;
 
   for (;;) {
@@ -411,40 +543,55 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int n_s
 
     // ---- load (fused gather through the previous step's parent map)
     const int src = a.parents ? a.parents[walker] : walker;
-    if (FAM == SPIN_HALF) {
+    if (guided && a.field_in) {
+      const T *fin = reinterpret_cast<const T *>(a.field_in) + (size_t)src * m.N;
+      for (int k = lane; k < m.N; k += 32) SF[k] = fin[k];
+      if (FAM != SPIN_HALF) {
+        const uint32_t *in = reinterpret_cast<const uint32_t *>(
+            reinterpret_cast<const uint8_t *>(a.cfg_in) + (size_t)src * CB);
+        uint32_t *o32 = reinterpret_cast<uint32_t *>(occ);
+        for (int k = lane; k < CB / 4; k += 32) o32[k] = in[k];
+      }
+      __syncwarp();
+    } else if (FAM == SPIN_HALF) {
       const uint64_t *in = reinterpret_cast<const uint64_t *>(a.cfg_in) + (size_t)src * NW;
       for (int k = lane; k < NW; k += 32) bits[k] = in[k];
+      __syncwarp();
+      signed_init<T>(m, g, bits, SF, lane);
     } else {
-      const uint32_t *in =
-          reinterpret_cast<const uint32_t *>(reinterpret_cast<const uint8_t *>(a.cfg_in) + (size_t)src * CB);
+      const uint32_t *in = reinterpret_cast<const uint32_t *>(
+          reinterpret_cast<const uint8_t *>(a.cfg_in) + (size_t)src * CB);
       uint32_t *o32 = reinterpret_cast<uint32_t *>(occ);
       for (int k = lane; k < CB / 4; k += 32) o32[k] = in[k];
-    }
-    __syncwarp();
-    if (guided) {
-      field_init<T, FAM>(m, g, bits, occ, F, lane);
       __syncwarp();
+      if (guided) {
+        field_init<T, FAM>(m, g, bits, occ, SF, lane);
+        __syncwarp();
+      }
     }
 
     const Key kw = fold(a.key, (uint32_t)walker);
     double lw = 0.0;
     T eloc = T(0);
     int hops = 0;
+    T draws = T(0);   // uniforms of 16 holds (cont/multi) or 32 sub-steps (single)
 
     if (method == CONT_TIME) {
       const T beta = T(a.step);
       T t = T(0);
       uint32_t it = 0;
       while (t < beta) {
-        const T diag = diag_elem<T, FAM>(m, bits, occ, lane);
-        const T R = scan_pass<T, FAM>(m, g, bits, occ, F, q, rowend, m.n_off, false, diag, lane);
-        const T eL = diag - R;
-        const T dr = uniform<T>(fold(kw, 2u * it + (uint32_t)(lane & 1)));
-        const T U1 = __shfl_sync(FULL, dr, 0), psi = __shfl_sync(FULL, dr, 1);
+        const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.n_off, false, lane);
+        const T R = ev.total;
+        const T eL = ev.diag - R;
+        if ((it & 15u) == 0) draws = uniform<T>(fold(kw, 2u * it + (uint32_t)lane));
+        const T U1 = __shfl_sync(FULL, draws, (int)(2u * (it & 15u)));
+        const T psi = __shfl_sync(FULL, draws, (int)(2u * (it & 15u) + 1u));
         int si = 0;
         if (R > T(0)) {
-          T u = U1 * R, cap = next_below(R);
-          si = warp_sample(q, rowend, m.n_off, false, lam, u < cap ? u : cap, lane);
+          const T u = U1 * R, cap = next_below(R);
+          si = sample_slot<T, FAM, FAST>(m, g, occ, SF, ev, m.n_off, false, lam,
+                                         u < cap ? u : cap, lane);
         }
         const T tau_raw = (R > T(0)) ? -math_log1p(-psi) / R : pos_inf<T>();
         const T rem = beta - t;
@@ -452,7 +599,7 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int n_s
         lw = lw - (double)eL * (double)tau;
         t = t + tau;
         if (tau_raw < rem) {
-          apply_move<T, FAM>(m, g, bits, occ, F, si, lane);
+          apply_move<T, FAM>(m, g, occ, SF, si, lane);
           ++hops;
         }
         eloc = eL;
@@ -465,36 +612,38 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int n_s
     } else if (method == SINGLE_STEP) {
       const int n_bra = (int)a.step;
       for (int sidx = 0; sidx < n_bra; ++sidx) {
-        const T diag = diag_elem<T, FAM>(m, bits, occ, lane);
-        const T Q = scan_pass<T, FAM>(m, g, bits, occ, F, q, rowend, m.M, true, diag, lane);
-        const T bx = lam - Q;
-        const T U = uniform<T>(fold(kw, (uint32_t)sidx));
-        T u = U * bx, cap = next_below(bx);
-        const int idx = warp_sample(q, rowend, m.M, true, lam, u < cap ? u : cap, lane);
+        const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.M, true, lane);
+        const T bx = lam - ev.total;
+        if ((sidx & 31) == 0) draws = uniform<T>(fold(kw, (uint32_t)(sidx + lane)));
+        const T U = __shfl_sync(FULL, draws, sidx & 31);
+        const T u = U * bx, cap = next_below(bx);
+        const int idx = sample_slot<T, FAM, FAST>(m, g, occ, SF, ev, m.M, true, lam,
+                                                  u < cap ? u : cap, lane);
         if (idx != 0) {
-          apply_move<T, FAM>(m, g, bits, occ, F, idx - 1, lane);
+          apply_move<T, FAM>(m, g, occ, SF, idx - 1, lane);
           ++hops;
         }
         lw = lw + (double)math_log(bx);
       }
-      const T diag = diag_elem<T, FAM>(m, bits, occ, lane);
-      const T R = scan_pass<T, FAM>(m, g, bits, occ, F, q, rowend, m.n_off, false, diag, lane);
-      eloc = diag - R;
+      const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.n_off, false, lane);
+      eloc = ev.diag - ev.total;
       lw -= a.alw * (double)n_bra;
     } else if (method == MULTI_STEP) {
       const int n_bra = (int)a.step;
       int used = 0;
       uint32_t it = 0;
       while (used < n_bra) {
-        const T diag = diag_elem<T, FAM>(m, bits, occ, lane);
-        const T R = scan_pass<T, FAM>(m, g, bits, occ, F, q, rowend, m.n_off, false, diag, lane);
-        const T bx = lam - diag + R;
-        const T dr = uniform<T>(fold(kw, 2u * it + (uint32_t)(lane & 1)));
-        const T U1 = __shfl_sync(FULL, dr, 0), psi = __shfl_sync(FULL, dr, 1);
+        const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.n_off, false, lane);
+        const T R = ev.total;
+        const T bx = lam - ev.diag + R;
+        if ((it & 15u) == 0) draws = uniform<T>(fold(kw, 2u * it + (uint32_t)lane));
+        const T U1 = __shfl_sync(FULL, draws, (int)(2u * (it & 15u)));
+        const T psi = __shfl_sync(FULL, draws, (int)(2u * (it & 15u) + 1u));
         int si = 0;
         if (R > T(0)) {
-          T u = U1 * R, cap = next_below(R);
-          si = warp_sample(q, rowend, m.n_off, false, lam, u < cap ? u : cap, lane);
+          const T u = U1 * R, cap = next_below(R);
+          si = sample_slot<T, FAM, FAST>(m, g, occ, SF, ev, m.n_off, false, lam,
+                                         u < cap ? u : cap, lane);
         }
         const int remaining = n_bra - used;
         const T hp = R / bx;
@@ -508,7 +657,7 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int n_s
         lw = lw + (double)math_log(bx) * (double)k;
         used += k;
         if (k_raw <= remaining) {
-          apply_move<T, FAM>(m, g, bits, occ, F, si, lane);
+          apply_move<T, FAM>(m, g, occ, SF, si, lane);
           ++hops;
         }
         if (++it >= (uint32_t)a.max_iters) {
@@ -516,23 +665,24 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int n_s
           break;
         }
       }
-      const T diag = diag_elem<T, FAM>(m, bits, occ, lane);
-      const T R = scan_pass<T, FAM>(m, g, bits, occ, F, q, rowend, m.n_off, false, diag, lane);
-      eloc = diag - R;
+      const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.n_off, false, lane);
+      eloc = ev.diag - ev.total;
       lw -= a.alw * (double)n_bra;
     } else {  // EVALUATE: local energy of the loaded configuration
-      const T diag = diag_elem<T, FAM>(m, bits, occ, lane);
-      const T R = m.n_off > 0
-                      ? scan_pass<T, FAM>(m, g, bits, occ, F, q, rowend, m.n_off, false, diag, lane)
-                      : T(0);
-      eloc = diag - R;
+      const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.n_off, false, lane);
+      eloc = ev.diag - ev.total;
     }
 
     // ---- store
     if (a.cfg_out) {
       if (FAM == SPIN_HALF) {
         uint64_t *out = reinterpret_cast<uint64_t *>(a.cfg_out) + (size_t)walker * NW;
-        for (int k = lane; k < NW; k += 32) out[k] = bits[k];
+        for (int w = 0; w < NW; ++w) {
+          const int k0 = 64 * w + lane, k1 = k0 + 32;
+          const unsigned lo = __ballot_sync(FULL, k0 < m.N && SF[k0 < m.N ? k0 : 0] > T(0));
+          const unsigned hi = __ballot_sync(FULL, k1 < m.N && SF[k1 < m.N ? k1 : 0] > T(0));
+          if (lane == 0) out[w] = (uint64_t)lo | ((uint64_t)hi << 32);
+        }
       } else {
         uint32_t *out = reinterpret_cast<uint32_t *>(reinterpret_cast<uint8_t *>(a.cfg_out) +
                                                      (size_t)walker * CB);
@@ -540,34 +690,43 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int n_s
         for (int k = lane; k < CB / 4; k += 32) out[k] = o32[k];
       }
     }
+    if (guided && a.field_out) {
+      T *fout = reinterpret_cast<T *>(a.field_out) + (size_t)walker * m.N;
+      for (int k = lane; k < m.N; k += 32) fout[k] = SF[k];
+    }
     if (lane == 0) {
       if (method != EVALUATE) a.log_w[walker] = lw;
       a.e_loc[walker] = (double)eloc;
     }
     wmax = lw > wmax ? lw : wmax;
-    any_walker = true;
     hop_acc += (unsigned long long)hops;
     __syncwarp();
   }
 
-  // ---- block max of log_w and hop count
-  __shared__ double s_max[32];
-  __shared__ unsigned long long s_hops[32];
+  // ---- per-warp max of log_w and hop count (no block barrier: warps that
+  //      run out of walkers leave at once)
   if (lane == 0) {
-    s_max[wib] = any_walker ? wmax : -DBL_MAX;
-    s_hops[wib] = hop_acc;
+    if (a.partial_max) a.partial_max[(size_t)blockIdx.x * (blockDim.x >> 5) + wib] = wmax;
+    if (a.hops && hop_acc) atomicAdd(a.hops, hop_acc);
   }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double mx = -DBL_MAX;
-    unsigned long long h = 0;
-    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
-      mx = s_max[i] > mx ? s_max[i] : mx;
-      h += s_hops[i];
-    }
-    if (a.partial_max) a.partial_max[blockIdx.x] = mx;
-    if (a.hops && h) atomicAdd(a.hops, h);
-  }
+}
+
+template <typename T>
+void staging_plan(const DevModel<T> &m, const DevGuide<T> &g, int *stage_nbr, size_t *cta) {
+  size_t nbr_bytes =
+      g.kind ? (size_t)m.N * g.deg * (sizeof(uint32_t) + 3 * sizeof(T)) + m.N * 4 : 0;
+  *stage_nbr = (g.kind != GUIDE_NONE) && !g.dense && nbr_bytes <= 48 * 1024;
+  DevModel<T> mm = m;
+  DevGuide<T> gg = g;
+  *cta = stage_tables(mm, gg, *stage_nbr, nullptr, false);
+}
+
+template <typename T>
+using KernelFn = void (*)(DevModel<T>, DevGuide<T>, EvolveArgs, int, int);
+
+template <typename T> KernelFn<T> pick_kernel(const DevModel<T> &m) {
+  if (m.family == SPIN_HALF) return m.fast ? evolve_kernel<T, SPIN_HALF, 1> : evolve_kernel<T, SPIN_HALF, 0>;
+  return evolve_kernel<T, BOSE_HUBBARD, 0>;
 }
 
 }  // namespace
@@ -575,70 +734,56 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int n_s
 template <typename T>
 cudaError_t plan_evolve(const DevModel<T> &m, const DevGuide<T> &g, int n_slots_max,
                         LaunchPlan *plan) {
+  (void)n_slots_max;
   int dev = 0, sms = 0, max_smem = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  DevModel<T> mm = m;
-  DevGuide<T> gg = g;
-  size_t of, oq, orr;
-  size_t warp_bytes = warp_region(m, g, n_slots_max, &of, &oq, &orr);
-  // Partner tables go to shared memory when they fit a 64 KB budget.
-  size_t nbr_bytes = g.kind ? (size_t)m.N * g.deg * (sizeof(uint32_t) + sizeof(T)) + m.N * 4 : 0;
-  int stage_nbr = (g.kind != GUIDE_NONE) && nbr_bytes <= 64 * 1024;
-  size_t cta = stage_tables(mm, gg, stage_nbr, nullptr, false);
-  int wpb = 8;
-  while (wpb > 1 && cta + wpb * warp_bytes > (size_t)max_smem) wpb >>= 1;
-  if (cta + wpb * warp_bytes > (size_t)max_smem) return cudaErrorInvalidConfiguration;
-  plan->wpb = wpb;
-  plan->block = wpb * 32;
-  plan->smem = cta + wpb * warp_bytes;
-  int per_sm = 0;
-  cudaError_t err;
-  if (m.family == SPIN_HALF) {
-    err = cudaFuncSetAttribute(evolve_kernel<T, SPIN_HALF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)plan->smem);
-    if (err != cudaSuccess) return err;
-    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, evolve_kernel<T, SPIN_HALF>,
-                                                        plan->block, plan->smem);
-  } else {
-    err = cudaFuncSetAttribute(evolve_kernel<T, BOSE_HUBBARD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)plan->smem);
-    if (err != cudaSuccess) return err;
-    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, evolve_kernel<T, BOSE_HUBBARD>,
-                                                        plan->block, plan->smem);
-  }
+  int stage_nbr;
+  size_t cta;
+  staging_plan(m, g, &stage_nbr, &cta);
+  const size_t warp_bytes = warp_layout(m, g).bytes;
+  KernelFn<T> kern = pick_kernel(m);
+  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
   if (err != cudaSuccess) return err;
-  if (per_sm < 1) per_sm = 1;
-  plan->grid = sms * per_sm;
-  // stash the table staging decision and region sizes in the plan's upper bits
-  plan->smem = cta + wpb * warp_bytes;
-  (void)stage_nbr;
+  // the warps-per-block choice with the most resident warps per SM
+  int best_w = 0, best = -1;
+  for (int wpb = 8; wpb >= 1; wpb >>= 1) {
+    size_t smem = cta + wpb * warp_bytes;
+    if (smem > (size_t)max_smem) continue;
+    int per_sm = 0;
+    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, wpb * 32, smem);
+    if (err != cudaSuccess) return err;
+    if (per_sm * wpb > best) { best = per_sm * wpb; best_w = wpb; }
+  }
+  if (best <= 0) return cudaErrorInvalidConfiguration;
+  plan->wpb = best_w;
+  plan->block = best_w * 32;
+  plan->smem = cta + best_w * warp_bytes;
+  plan->grid = sms * (best / best_w);
   return cudaSuccess;
 }
 
 template <typename T>
 cudaError_t launch_evolve(const DevModel<T> &m, const DevGuide<T> &g, const LaunchPlan &plan,
                           const EvolveArgs &a, cudaStream_t s) {
-  size_t of, oq, orr;
-  int n_slots_max = m.M;
-  size_t warp_bytes = warp_region(m, g, n_slots_max, &of, &oq, &orr);
-  size_t nbr_bytes = g.kind ? (size_t)m.N * g.deg * (sizeof(uint32_t) + sizeof(T)) + m.N * 4 : 0;
-  int stage_nbr = (g.kind != GUIDE_NONE) && nbr_bytes <= 64 * 1024;
-  DevModel<T> mm = m;
-  DevGuide<T> gg = g;
-  size_t cta = stage_tables(mm, gg, stage_nbr, nullptr, false);
+  int stage_nbr;
+  size_t cta;
+  staging_plan(m, g, &stage_nbr, &cta);
   int grid = plan.grid;
   int need = (a.n_walkers + plan.wpb - 1) / plan.wpb;
   if (grid > need) grid = need;
   if (grid < 1) grid = 1;
-  if (m.family == SPIN_HALF)
-    evolve_kernel<T, SPIN_HALF><<<grid, plan.block, plan.smem, s>>>(
-        m, g, a, stage_nbr, n_slots_max, (int)cta, (int)warp_bytes);
-  else
-    evolve_kernel<T, BOSE_HUBBARD><<<grid, plan.block, plan.smem, s>>>(
-        m, g, a, stage_nbr, n_slots_max, (int)cta, (int)warp_bytes);
+  pick_kernel(m)<<<grid, plan.block, plan.smem, s>>>(m, g, a, stage_nbr, (int)cta);
   return cudaGetLastError();
+}
+
+int evolve_partials(const LaunchPlan &plan, int n_walkers) {
+  int grid = plan.grid;
+  int need = (n_walkers + plan.wpb - 1) / plan.wpb;
+  if (grid > need) grid = need;
+  if (grid < 1) grid = 1;
+  return grid * plan.wpb;
 }
 
 template cudaError_t plan_evolve<double>(const DevModel<double> &, const DevGuide<double> &, int,
