@@ -168,7 +168,8 @@ int build_tables(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_des
       gk != GFMC_GUIDE_JASTROW_BOSE_HUBBARD)
     return fail(GFMC_ERR_UNSUPPORTED, "unknown guide kind %d", gk);
   g.kind = gk;
-  size_t o_nbr = 0, o_nbrw = 0, o_cnt = 0, o_tpw = 0, o_jd = 0, o_ep = 0, o_em = 0;
+  size_t o_nbr = 0, o_nbrw = 0, o_cnt = 0, o_tpw = 0, o_jd = 0, o_ep = 0, o_em = 0, o_tep = 0,
+           o_tem = 0, o_xy = 0;
   if (gk != GFMC_GUIDE_NONE) {
     // per-site partner lists, duplicates merged (each partner once per site)
     std::vector<std::map<int, double>> lists(N);
@@ -202,6 +203,36 @@ int build_tables(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_des
         for (auto &kv : lists[k]) Jd[(size_t)k * N + kv.first] = (T)kv.second;
       o_jd = A.add(Jd.data(), Jd.size() * sizeof(T));
       if (gk == GFMC_GUIDE_JASTROW_SPIN_HALF) {
+        // translation invariance on an Lx x Ly torus: J_ak = J_0[d(a, k)]
+        for (int Lx = 1; Lx <= N && !g.ti; ++Lx) {
+          if (N % Lx) continue;
+          const int Ly = N / Lx;
+          bool ok = true;
+          for (int a = 0; a < N && ok; ++a) {
+            const int xa = a % Lx, ya = a / Lx;
+            for (int k = 0; k < N; ++k) {
+              const int d = (k % Lx - xa + Lx) % Lx + Lx * ((k / Lx - ya + Ly) % Ly);
+              if (Jd[(size_t)a * N + k] != Jd[d]) { ok = false; break; }
+            }
+          }
+          if (ok) {
+            g.ti = 1;
+            g.Lx = Lx;
+            g.Ly = Ly;
+          }
+        }
+        if (g.ti) {
+          std::vector<T> tp(N), tm(N);
+          std::vector<uint32_t> xy(N);
+          for (int d = 0; d < N; ++d) {
+            tp[d] = (T)std::exp(4.0 * (double)Jd[d]);
+            tm[d] = (T)std::exp(-4.0 * (double)Jd[d]);
+            xy[d] = (uint32_t)(d % g.Lx) | ((uint32_t)(d / g.Lx) << 16);
+          }
+          o_tep = A.add(tp.data(), N * sizeof(T));
+          o_tem = A.add(tm.data(), N * sizeof(T));
+          o_xy = A.add(xy.data(), N * 4);
+        }
         // multiplicative factor updates exp(+-4 J_kp) (1 where no pair)
         std::vector<T> ep((size_t)N * N, T(1)), em((size_t)N * N, T(1));
         for (int k = 0; k < N; ++k)
@@ -305,6 +336,11 @@ int build_tables(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_des
       if (g.dense) {
         g.Ep = (const T *)(base + o_ep);
         g.Em = (const T *)(base + o_em);
+        if (g.ti) {
+          g.tEp = (const T *)(base + o_tep);
+          g.tEm = (const T *)(base + o_tem);
+          g.xy = (const uint32_t *)(base + o_xy);
+        }
       } else {
         g.nbr_ep = (const T *)(base + o_ep);
         g.nbr_em = (const T *)(base + o_em);

@@ -72,6 +72,14 @@ template <typename T> struct DevGuide {
   // flip): A_k *= exp(4 x_k x_s J_sk), i.e. Ep = exp(4 J), Em = exp(-4 J)
   const T *Ep, *Em;       // dense: (N, N)
   const T *nbr_ep, *nbr_em;   // sparse: (N, deg), aligned with nbr
+  // Translation-invariant dense couplings on an Lx x Ly torus (site
+  // x + Lx y): J_ak = J_0[d(a, k)] with d the displacement index
+  // ((x_k - x_a) mod Lx) + Lx ((y_k - y_a) mod Ly); the factor rows are then
+  // the N-entry tables tEp = exp(4 J_0), tEm = exp(-4 J_0), staged in shared
+  // memory, and xy[k] = x_k | y_k << 16.
+  int ti, Lx, Ly;
+  const T *tEp, *tEm;
+  const uint32_t *xy;
   int dense;              // couplings as a dense symmetric (N, N) matrix Jd
   const T *Jd;            // (N, N) row-major, zero diagonal (dense == 1)
 };

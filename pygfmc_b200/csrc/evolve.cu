@@ -78,6 +78,11 @@ __host__ __device__ inline size_t stage_tables(DevModel<T> &m, DevGuide<T> &g, i
       g.d = stage_arr(g.d, g.d_mode == 2 ? m.N : 0, base, off, copy);
     }
   }
+  if (g.kind == GUIDE_JASTROW_SPIN && g.ti) {
+    g.tEp = stage_arr(g.tEp, m.N, base, off, copy);
+    g.tEm = stage_arr(g.tEm, m.N, base, off, copy);
+    g.xy = stage_arr(g.xy, m.N, base, off, copy);
+  }
   if (g.kind != GUIDE_NONE && stage_nbr && !g.dense) {
     g.nbr = stage_arr(g.nbr, m.N * g.deg, base, off, copy);
     g.nbr_w = stage_arr(g.nbr_w, m.N * g.deg, base, off, copy);
@@ -252,6 +257,15 @@ __device__ __forceinline__ void signed_init(const DevModel<T> &m, const DevGuide
   __syncwarp();
 }
 
+// Displacement index of site k (packed xy) from (xa, ya) on the torus.
+template <typename T>
+__device__ __forceinline__ int ti_disp(const DevGuide<T> &g, uint32_t pk, int xa, int ya) {
+  int dx = (int)(pk & 0xFFFF) - xa, dy = (int)(pk >> 16) - ya;
+  dx += dx < 0 ? g.Lx : 0;
+  dy += dy < 0 ? g.Ly : 0;
+  return dx + g.Lx * dy;
+}
+
 // Flip of spin a (the sequential update of one flip): its partners k get
 // A_k *= exp(4 x_k x_a J_ak) (x_a before the flip), then s_a -> -1 / s_a.
 template <typename T>
@@ -260,7 +274,15 @@ __device__ __forceinline__ void flip_one(const DevModel<T> &m, const DevGuide<T>
   const T sa = S[a];
   if (g.kind != GUIDE_NONE) {
     const bool ua = sa > T(0);
-    if (g.dense) {
+    if (g.ti) {
+      const uint32_t pa = g.xy[a];
+      const int xa = pa & 0xFFFF, ya = pa >> 16;
+      for (int k = lane; k < m.N; k += 32) {
+        const T sk = S[k];
+        const int d = ti_disp(g, g.xy[k], xa, ya);
+        S[k] = sk * (((sk > T(0)) == ua) ? g.tEp[d] : g.tEm[d]);
+      }
+    } else if (g.dense) {
       const T *ep = g.Ep + (size_t)a * m.N, *em = g.Em + (size_t)a * m.N;
       for (int k = lane; k < m.N; k += 32) {
         const T sk = S[k];
@@ -297,6 +319,29 @@ __device__ __forceinline__ void flip_pair(const DevModel<T> &m, const DevGuide<T
   }
   const T sa = S[a], sb = S[b];
   const bool ua = sa > T(0), ub = sb > T(0);
+  if (g.ti) {
+    const uint32_t pa = g.xy[a], pb = g.xy[b];
+    const int xa = pa & 0xFFFF, ya = pa >> 16, xb = pb & 0xFFFF, yb = pb >> 16;
+    for (int k = lane; k < m.N; k += 32) {
+      const T sk = S[k];
+      const bool uk = sk > T(0);
+      const uint32_t pk = g.xy[k];
+      const int da = ti_disp(g, pk, xa, ya), db = ti_disp(g, pk, xb, yb);
+      const T fa = (uk == ua) ? g.tEp[da] : g.tEm[da];
+      const T fb = (uk == ub) ? g.tEp[db] : g.tEm[db];
+      S[k] = sk * fa * fb;
+    }
+    __syncwarp();
+    if (lane == 0) {
+      const int dba = ti_disp(g, pa, xb, yb), dab = ti_disp(g, pb, xa, ya);
+      const T fba = ((!ua) == ub) ? g.tEp[dba] : g.tEm[dba];
+      const T fab = (ub == ua) ? g.tEp[dab] : g.tEm[dab];
+      S[a] = (T(-1) / sa) * fba;
+      S[b] = T(-1) / (sb * fab);
+    }
+    __syncwarp();
+    return;
+  }
   const T *epa = g.Ep + (size_t)a * m.N, *ema = g.Em + (size_t)a * m.N;
   const T *epb = g.Ep + (size_t)b * m.N, *emb = g.Em + (size_t)b * m.N;
   for (int k = lane; k < m.N; k += 32) {
@@ -715,6 +760,7 @@ template <typename T>
 void staging_plan(const DevModel<T> &m, const DevGuide<T> &g, int *stage_nbr, size_t *cta) {
   size_t nbr_bytes =
       g.kind ? (size_t)m.N * g.deg * (sizeof(uint32_t) + 3 * sizeof(T)) + m.N * 4 : 0;
+  // (translation-invariant dense tables are staged by stage_tables itself)
   *stage_nbr = (g.kind != GUIDE_NONE) && !g.dense && nbr_bytes <= 48 * 1024;
   DevModel<T> mm = m;
   DevGuide<T> gg = g;

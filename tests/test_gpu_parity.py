@@ -60,6 +60,22 @@ def _systems(P, O):
     Gs = P.JastrowSpinHalf(16, pairs, beta=beta)
     cfgs = P.prepare_walkers_sz(512, 16, P.PRNGKey(12), sz=0).config
     out.append(("square4_longrange", Hs, Gs, ms, O.jastrow_spin_half(16, pairs, beta, None, ms), cfgs))
+    # dense couplings without translation invariance, with a field
+    rng = np.random.default_rng(21)
+    bd = rng.uniform(0.05, 0.4, len(pairs))
+    hd = rng.uniform(-0.1, 0.1, 16)
+    Gd = P.JastrowSpinHalf(16, pairs, beta=bd, h=hd)
+    out.append(("square4_dense_random", Hs, Gd, ms, O.jastrow_spin_half(16, pairs, bd, hd, ms), cfgs))
+    # non-uniform couplings and both fields (general spin path)
+    e12 = P.chain(12).edges
+    jx = -rng.uniform(0.5, 1.5, 12)
+    jy = jx + rng.uniform(0.0, 0.2, 12)     # J_pmpm = (J_x - J_y) / 4 <= 0
+    jz = rng.uniform(0.5, 1.5, 12)
+    Hg = P.SpinHalf.create(e12, J_x=jx, J_y=jy, J_z=jz, h_z=0.3, h_x=0.2, dtype=np.float64)
+    mg = O.spin_half(e12, J_x=jx, J_y=jy, J_z=jz, h_z=0.3, h_x=0.2)
+    Gg = P.JastrowSpinHalf(12, e12, beta=0.2, h=0.03)
+    cfgg = P.prepare_walkers_random(512, 12, P.PRNGKey(14)).config
+    out.append(("chain12_xyz_fields", Hg, Gg, mg, O.jastrow_spin_half(12, e12, 0.2, 0.03, mg), cfgg))
     eb = P.chain(12).edges
     B = P.BoseHubbard.create(eb, t=1.0, eta=0.2, U=3.0, mu=0.4, h_pm=0.1, n_max=3, dtype=np.float64)
     mb = O.bose_hubbard(eb, t=1.0, eta=0.2, U=3.0, mu=0.4, h_pm=0.1, n_max=3)
