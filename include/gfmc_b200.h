@@ -154,6 +154,27 @@ int gfmc_windowed_energy(int n_steps, const double *logG, const double *E, int n
  * unbounded). */
 int gfmc_set_max_iters(gfmc_handle *h, int max_iters);
 
+/* Largest population gfmc_reconfigure_noalloc accepts. */
+#define GFMC_NOALLOC_MAX_WALKERS 131072
+
+/* Systematic resampling of a population (the reconfiguration step of
+ * gfmc_run_steps, on its own) that allocates no device memory, for callers
+ * that must not allocate inside a call: a host framework that owns the device
+ * through its own pool allocator, or a latency-critical loop that cannot
+ * take the device synchronisation cudaMalloc/cudaFree imply.  No counterpart
+ * in PyGFMC.  Inputs (device): log_w, e_loc (float64, n_walkers); key (host):
+ * the reconfiguration key.  Outputs (device): parents_out (int32, n_walkers),
+ * logG_out = logsumexp(log_w) - log N, E_out = sum w e_loc / sum w (scalars).
+ * Scratch is a fixed ~2 MB file-scope device array that every GPU loading the
+ * library holds until exit: at most GFMC_NOALLOC_MAX_WALKERS walkers (larger
+ * counts return GFMC_ERR_INVALID); all calls on a device share it, so calls
+ * that overlap on the GPU race.  The first call on a device looks up the
+ * array's address on that (current) device; make it before any stream
+ * capture. */
+int gfmc_reconfigure_noalloc(int n_walkers, const double *log_w, const double *e_loc,
+                             const uint32_t key[2], int32_t *parents_out, double *logG_out,
+                             double *E_out, void *stream);
+
 /* Reads and clears the device status word (GFMC_STATUS_* bits); synchronises. */
 int gfmc_read_status(gfmc_handle *h, int *status_out, void *stream);
 

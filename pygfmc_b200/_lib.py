@@ -70,6 +70,7 @@ SIGNATURES = {
     "gfmc_gather": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gfmc_windowed_energy": (ctypes.c_int, [ctypes.c_int, _vp, _vp, ctypes.c_int, _i32p, _dp, _vp]),
     "gfmc_set_max_iters": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "gfmc_reconfigure_noalloc": (ctypes.c_int, [ctypes.c_int, _vp, _vp, _u32p, _vp, _vp, _vp, _vp]),
     "gfmc_read_status": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int), _vp]),
     "gfmc_key_schedule": (ctypes.c_int, [_u32p, ctypes.c_int, _u32p, _u32p]),
     "gfmc_threefry2x32": (ctypes.c_int, [ctypes.c_uint32] * 4 + [_u32p]),

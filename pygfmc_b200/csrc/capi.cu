@@ -53,6 +53,11 @@ template <typename T> std::vector<T> conv(const double *src, size_t n) {
 
 }  // namespace
 
+namespace gfmc {
+// Records msg as the calling thread's gfmc_last_error message.
+int record_error(int code, const char *msg) { return fail(code, "%s", msg); }
+}  // namespace gfmc
+
 struct gfmc_handle {
   int precision = 0;
   int family = 0;
