@@ -154,6 +154,42 @@ int gfmc_windowed_energy(int n_steps, const double *logG, const double *E, int n
  * unbounded). */
 int gfmc_set_max_iters(gfmc_handle *h, int max_iters);
 
+/* ---- diagonal observables with forward walking ------------------------- */
+#define GFMC_DIAG_SPIN_HALF 0   /* SpinHalf.diagonal_weight (J_z edges, h_z)     */
+#define GFMC_DIAG_BOSE_HUBBARD 1 /* BoseHubbard.diagonal_weight (U, mu)          */
+#define GFMC_DIAG_SZSZ 2        /* SzSzStructureFactor: n_k values per walker    */
+
+/* A diagonal operator (host arrays, float64, read by gfmc_set_diag_operators).
+ * SpinHalf / BoseHubbard fields as in gfmc_model_desc; SZSZ: (n_k, N) cos/sin
+ * tables of k.r and the dropped i == j constant (hamiltonian/observables.py:68). */
+typedef struct {
+  int kind;
+  int n_sites, n_edges;
+  const int32_t *edge_i, *edge_j;
+  int has_jz, uniform_jz, has_hz;
+  const double *jz, *hz;
+  int has_U, has_mu;
+  const double *U, *mu;
+  int n_k;
+  const double *cos_kr, *sin_kr;
+  double offset;
+} gfmc_diag_desc;
+
+/* Diagonal operators measured by the ancestry-traced (forward-walking) pure
+ * estimator of engine/driver.py:228-288 at the windows m_array (sorted, p//2),
+ * at most 16.  Replaces any previous set. */
+int gfmc_set_diag_operators(gfmc_handle *h, int n_ops, const gfmc_diag_desc *ops, int n_p,
+                            const int *m_array);
+/* Values per walker of the operator set (the sum of their widths). */
+int gfmc_diag_width(const gfmc_handle *h);
+/* Resets the ancestry and value ring buffers (identity maps, zeros) for a
+ * population of n_walkers (engine/driver.py _diag_ring_buffers:810-838). */
+int gfmc_reset_diag(gfmc_handle *h, int n_walkers, void *stream);
+/* Device output of the next gfmc_run_steps call: (n_steps, width, n_p)
+ * float64, the mean over walkers of each value traced m steps back; NULL
+ * stops the measurement. */
+int gfmc_set_diag_output(gfmc_handle *h, double *out);
+
 /* Largest population gfmc_reconfigure_noalloc accepts. */
 #define GFMC_NOALLOC_MAX_WALKERS 131072
 

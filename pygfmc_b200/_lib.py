@@ -54,6 +54,19 @@ class GuideDesc(ctypes.Structure):
                 ("d_mode", ctypes.c_int), ("d0", ctypes.c_double), ("d", _dp)]
 
 
+class DiagDesc(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("n_sites", ctypes.c_int), ("n_edges", ctypes.c_int),
+                ("edge_i", _i32p), ("edge_j", _i32p),
+                ("has_jz", ctypes.c_int), ("uniform_jz", ctypes.c_int), ("has_hz", ctypes.c_int),
+                ("jz", _dp), ("hz", _dp), ("has_U", ctypes.c_int), ("has_mu", ctypes.c_int),
+                ("U", _dp), ("mu", _dp), ("n_k", ctypes.c_int), ("cos_kr", _dp), ("sin_kr", _dp),
+                ("offset", ctypes.c_double)]
+
+
+DIAG_SPIN_HALF = 0
+DIAG_BOSE_HUBBARD = 1
+DIAG_SZSZ = 2
+
 # name -> (restype, argtypes); every symbol include/gfmc_b200.h declares
 SIGNATURES = {
     "gfmc_create": (ctypes.c_int, [ctypes.POINTER(ModelDesc), ctypes.POINTER(GuideDesc),
@@ -70,6 +83,11 @@ SIGNATURES = {
     "gfmc_gather": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gfmc_windowed_energy": (ctypes.c_int, [ctypes.c_int, _vp, _vp, ctypes.c_int, _i32p, _dp, _vp]),
     "gfmc_set_max_iters": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "gfmc_set_diag_operators": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(DiagDesc),
+                                               ctypes.c_int, _i32p]),
+    "gfmc_diag_width": (ctypes.c_int, [_vp]),
+    "gfmc_reset_diag": (ctypes.c_int, [_vp, ctypes.c_int, _vp]),
+    "gfmc_set_diag_output": (ctypes.c_int, [_vp, _vp]),
     "gfmc_reconfigure_noalloc": (ctypes.c_int, [ctypes.c_int, _vp, _vp, _u32p, _vp, _vp, _vp, _vp]),
     "gfmc_read_status": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int), _vp]),
     "gfmc_key_schedule": (ctypes.c_int, [_u32p, ctypes.c_int, _u32p, _u32p]),

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "../../include/gfmc_b200.h"
+#include "diag.cuh"
 #include "engine.cuh"
 
 using namespace gfmc;
@@ -85,6 +86,13 @@ struct gfmc_handle {
   int fcur = 0, field_valid = 0, since_refresh = 0;
   const void *field_cfg = nullptr;
   int cap_field = 0;
+  // diagonal observables (forward walking)
+  DiagSet diag{};
+  DiagOp *d_ops = nullptr;
+  void *d_diag_tables = nullptr;
+  int diag_cap_n = 0, diag_slot = 0, diag_ready = 0;
+  double *diag_partial = nullptr;
+  double *diag_out = nullptr;
 };
 
 namespace {
@@ -419,6 +427,8 @@ int run_steps_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, int 
                 cudaStream_t s) {
   int rc = ensure_scratch(h, n, n_steps);
   if (rc) return rc;
+  if (h->diag_out && (!h->diag_ready || h->diag_cap_n != n))
+    return fail(GFMC_ERR_INVALID, "diagonal output set but gfmc_reset_diag not called for %d walkers", n);
   const int nb = recon_tiles(n);
   const int nbc = recon_tiles(h->cap_n);
   GFMC_CUDA(cudaMemsetAsync(h->ctr, 0, sizeof(int) * n_steps, s));
@@ -473,6 +483,14 @@ int run_steps_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, int 
     r.status = h->status;
     e = launch_reconfigure(r, s);
     if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "reconfigure launch: %s", cudaGetErrorString(e));
+    if (h->diag_out && h->diag_ready) {
+      const int NW = (h->N + 63) / 64;
+      e = launch_diag_step(h->diag, h->family, n, NW, h->cfg_bytes, nxt, parents, h->diag_slot,
+                           h->diag_partial,
+                           h->diag_out + (size_t)st * h->diag.width * h->diag.n_p, s);
+      if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "diagonal step: %s", cudaGetErrorString(e));
+      h->diag_slot = (h->diag_slot + 1) % (h->diag.m_max + 1);
+    }
     void *t = cur; cur = nxt; nxt = t;
   }
   (void)nbc;
@@ -544,6 +562,8 @@ int gfmc_destroy(gfmc_handle *h) {
   cudaFree(h->pmax); cudaFree(h->psum); cudaFree(h->pE); cudaFree(h->cdf); cudaFree(h->wbuf);
   cudaFree(h->plp); cudaFree(h->ctr); cudaFree(h->status); cudaFree(h->hops);
   cudaFree(h->fbuf[0]); cudaFree(h->fbuf[1]);
+  cudaFree(h->d_ops); cudaFree(h->d_diag_tables); cudaFree(h->diag.ring_parents);
+  cudaFree(h->diag.ring_vals); cudaFree(h->diag_partial);
   delete h;
   return GFMC_OK;
 }
@@ -635,6 +655,117 @@ int gfmc_windowed_energy(int n_steps, const double *logG, const double *E, int n
   cudaFree(dp);
   cudaFree(work);
   if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "windowed energy: %s", cudaGetErrorString(e));
+  return GFMC_OK;
+}
+
+int gfmc_set_diag_operators(gfmc_handle *h, int n_ops, const gfmc_diag_desc *ops, int n_p,
+                            const int *m_array) {
+  if (!h || n_ops < 0 || (n_ops && !ops) || n_p < 1 || n_p > GFMC_DIAG_MAX_P || !m_array)
+    return fail(GFMC_ERR_INVALID, "gfmc_set_diag_operators: bad argument (1 <= n_p <= %d)",
+                GFMC_DIAG_MAX_P);
+  for (int j = 0; j < n_p; ++j)
+    if (m_array[j] < 0 || (j && m_array[j] < m_array[j - 1]))
+      return fail(GFMC_ERR_INVALID, "m_array must be sorted and non-negative");
+  cudaFree(h->d_ops); cudaFree(h->d_diag_tables);
+  h->d_ops = nullptr; h->d_diag_tables = nullptr;
+  h->diag_ready = 0;
+  Arena A;
+  std::vector<DiagOp> host(n_ops);
+  std::vector<std::map<std::string, size_t>> offs(n_ops);
+  int col = 0;
+  for (int o = 0; o < n_ops; ++o) {
+    const gfmc_diag_desc &d = ops[o];
+    DiagOp &op = host[o];
+    memset(&op, 0, sizeof(op));
+    op.kind = d.kind;
+    op.col = col;
+    op.N = d.n_sites;
+    op.E = d.n_edges;
+    if (d.n_sites != h->N) return fail(GFMC_ERR_INVALID, "diagonal operator %d: n_sites %d != %d", o, d.n_sites, h->N);
+    auto addd = [&](const char *nm, const double *p, size_t cnt) {
+      if (p && cnt) offs[o][nm] = A.add(p, cnt * sizeof(double));
+    };
+    if (d.kind == GFMC_DIAG_SPIN_HALF) {
+      if (h->family != GFMC_MODEL_SPIN_HALF) return fail(GFMC_ERR_INVALID, "SpinHalf operator on bosons");
+      std::vector<int> ei(d.n_edges), ej(d.n_edges);
+      for (int e = 0; e < d.n_edges; ++e) {
+        ei[e] = d.edge_i[e]; ej[e] = d.edge_j[e];
+        if (ei[e] < 0 || ej[e] < 0 || ei[e] >= h->N || ej[e] >= h->N)
+          return fail(GFMC_ERR_INVALID, "diagonal operator %d: edge out of range", o);
+      }
+      if (d.n_edges) {
+        offs[o]["ei"] = A.add(ei.data(), ei.size() * 4);
+        offs[o]["ej"] = A.add(ej.data(), ej.size() * 4);
+      }
+      op.has_jz = d.has_jz; op.uniform_jz = d.uniform_jz; op.has_hz = d.has_hz;
+      addd("jz", d.jz, d.has_jz ? (d.uniform_jz ? 1 : d.n_edges) : 0);
+      addd("hz", d.hz, d.has_hz ? d.n_sites : 0);
+      col += 1;
+    } else if (d.kind == GFMC_DIAG_BOSE_HUBBARD) {
+      if (h->family != GFMC_MODEL_BOSE_HUBBARD) return fail(GFMC_ERR_INVALID, "BoseHubbard operator on spins");
+      op.has_U = d.has_U; op.has_mu = d.has_mu;
+      addd("U", d.U, d.has_U ? d.n_sites : 0);
+      addd("mu", d.mu, d.has_mu ? d.n_sites : 0);
+      col += 1;
+    } else if (d.kind == GFMC_DIAG_SZSZ) {
+      if (d.n_k < 1 || !d.cos_kr || !d.sin_kr) return fail(GFMC_ERR_INVALID, "SzSz operator %d: no wavevectors", o);
+      op.n_k = d.n_k;
+      op.offset = d.offset;
+      addd("cos", d.cos_kr, (size_t)d.n_k * d.n_sites);
+      addd("sin", d.sin_kr, (size_t)d.n_k * d.n_sites);
+      col += d.n_k;
+    } else {
+      return fail(GFMC_ERR_UNSUPPORTED, "unknown diagonal operator kind %d", d.kind);
+    }
+  }
+  GFMC_CUDA(cudaMalloc(&h->d_diag_tables, A.host.size() ? A.host.size() : 256));
+  if (A.host.size())
+    GFMC_CUDA(cudaMemcpy(h->d_diag_tables, A.host.data(), A.host.size(), cudaMemcpyHostToDevice));
+  unsigned char *base = (unsigned char *)h->d_diag_tables;
+  for (int o = 0; o < n_ops; ++o) {
+    auto P = [&](const char *nm) -> const void * {
+      auto it = offs[o].find(nm);
+      return it == offs[o].end() ? nullptr : (const void *)(base + it->second);
+    };
+    host[o].ei = (const int *)P("ei"); host[o].ej = (const int *)P("ej");
+    host[o].jz = (const double *)P("jz"); host[o].hz = (const double *)P("hz");
+    host[o].U = (const double *)P("U"); host[o].mu = (const double *)P("mu");
+    host[o].cos_kr = (const double *)P("cos"); host[o].sin_kr = (const double *)P("sin");
+  }
+  GFMC_CUDA(cudaMalloc(&h->d_ops, sizeof(DiagOp) * (n_ops ? n_ops : 1)));
+  if (n_ops) GFMC_CUDA(cudaMemcpy(h->d_ops, host.data(), sizeof(DiagOp) * n_ops, cudaMemcpyHostToDevice));
+  h->diag.n_ops = n_ops;
+  h->diag.ops = h->d_ops;
+  h->diag.width = col;
+  h->diag.n_p = n_p;
+  for (int j = 0; j < n_p; ++j) h->diag.m[j] = m_array[j];
+  h->diag.m_max = m_array[n_p - 1];
+  h->diag_cap_n = 0;   // rings sized again by gfmc_reset_diag
+  return GFMC_OK;
+}
+
+int gfmc_diag_width(const gfmc_handle *h) { return h ? h->diag.width : GFMC_ERR_INVALID; }
+
+int gfmc_reset_diag(gfmc_handle *h, int n, void *stream) {
+  if (!h || n <= 0 || !h->d_ops) return fail(GFMC_ERR_INVALID, "gfmc_reset_diag: no operators set");
+  cudaFree(h->diag.ring_parents); cudaFree(h->diag.ring_vals); cudaFree(h->diag_partial);
+  h->diag.ring_parents = nullptr; h->diag.ring_vals = nullptr; h->diag_partial = nullptr;
+  const size_t size = (size_t)(h->diag.m_max + 1);
+  GFMC_CUDA(cudaMalloc(&h->diag.ring_parents, sizeof(int) * size * n));
+  GFMC_CUDA(cudaMalloc(&h->diag.ring_vals, sizeof(double) * size * n * (h->diag.width ? h->diag.width : 1)));
+  GFMC_CUDA(cudaMalloc(&h->diag_partial, sizeof(double) * (size_t)diag_walk_blocks(n) *
+                                              (h->diag.width ? h->diag.width : 1) * h->diag.n_p));
+  cudaError_t e = launch_diag_reset(h->diag, n, (cudaStream_t)stream);
+  if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "diag reset: %s", cudaGetErrorString(e));
+  h->diag_cap_n = n;
+  h->diag_slot = 0;
+  h->diag_ready = 1;
+  return GFMC_OK;
+}
+
+int gfmc_set_diag_output(gfmc_handle *h, double *out) {
+  if (!h) return fail(GFMC_ERR_INVALID, "null handle");
+  h->diag_out = out;
   return GFMC_OK;
 }
 

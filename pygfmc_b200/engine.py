@@ -25,7 +25,8 @@ from . import random as _rnd
 from .hamiltonian import BoseHubbard, SpinHalf
 from .walkers import Walker
 from .wavefunction import JastrowBoseHubbard, JastrowSpinHalf
-from .estimators import autocorrelation_stats, validated_p_array, windowed_energy_host
+from .estimators import (autocorrelation_stats, diagonal_estimates, validated_p_array,
+                         windowed_energy_host)
 
 __all__ = ["run", "run_gfmc", "GFMCEngine", "DEFAULT_WARMUP_STEPS"]
 
@@ -171,6 +172,42 @@ def model_desc(op, keep):
         if op.h_pm is not None:
             d.hpm = keep.f64(np.broadcast_to(np.asarray(op.h_pm, np.float64), (N,)))
     return d
+
+
+def diag_desc(op, n_sites, keep):
+    """A diagonal operator (diag_operators) lowered to gfmc_diag_desc:
+    SpinHalf / BoseHubbard diagonal_weight or SzSzStructureFactor."""
+    from .hamiltonian import SzSzStructureFactor
+    d = _lib.DiagDesc()
+    d.n_sites = int(n_sites)
+    if isinstance(op, SzSzStructureFactor) or all(hasattr(op, a) for a in ("cos", "sin", "offset")):
+        cos = np.asarray(op.cos, np.float64)
+        if cos.shape[1] != n_sites:
+            raise ValueError(f"SzSzStructureFactor has {cos.shape[1]} positions for {n_sites} sites")
+        d.kind = _lib.DIAG_SZSZ
+        d.n_k = cos.shape[0]
+        d.cos_kr, d.sin_kr = keep.f64(cos), keep.f64(np.asarray(op.sin, np.float64))
+        d.offset = float(op.offset)
+        return d, int(cos.shape[0])
+    if _is_spin_half(op):
+        d.kind = _lib.DIAG_SPIN_HALF
+        E = int(len(op.edge_i))
+        d.n_edges = E
+        d.edge_i, d.edge_j = keep.i32(op.edge_i), keep.i32(op.edge_j)
+        d.has_jz, d.uniform_jz, d.has_hz = int(op.has_jz), int(op.uniform_jz), int(op.has_hz)
+        jz = np.asarray(op.J_z, np.float64)
+        d.jz = keep.f64(jz[:1] if op.uniform_jz else np.broadcast_to(jz, (E,)))
+        if op.h_z is not None:
+            d.hz = keep.f64(np.broadcast_to(np.asarray(op.h_z, np.float64), (n_sites,)))
+        return d, 1
+    if _is_bose(op):
+        d.kind = _lib.DIAG_BOSE_HUBBARD
+        d.has_U, d.has_mu = int(op.has_U), int(op.has_mu)
+        d.U = keep.f64(np.broadcast_to(np.asarray(op.U, np.float64), (n_sites,)))
+        d.mu = keep.f64(np.broadcast_to(np.asarray(op.mu, np.float64), (n_sites,)))
+        return d, 1
+    raise TypeError(f"diagonal operator {type(op).__name__!r} has no device implementation "
+                    "(supported: SpinHalf, BoseHubbard, SzSzStructureFactor)")
 
 
 def guide_desc(guide, op, keep):
@@ -327,6 +364,34 @@ class GFMCEngine:
                    "gfmc_unpack")
         return out, e
 
+    def set_diag_operators(self, ops, m_array):
+        """Diagonal operators (name -> op) measured by forward walking at the
+        windows m_array; returns the per-operator column widths."""
+        keep = _Keep()
+        descs, widths = [], []
+        for name, op in ops.items():
+            d, w = diag_desc(op, self.N, keep)
+            if (d.kind == _lib.DIAG_BOSE_HUBBARD) != (self.family == _lib.MODEL_BOSE_HUBBARD) and \
+                    d.kind != _lib.DIAG_SZSZ:
+                raise TypeError(f"diagonal operator {name!r} does not act on this model's configurations")
+            descs.append(d)
+            widths.append(w)
+        arr = (_lib.DiagDesc * max(1, len(descs)))(*descs)
+        m = np.ascontiguousarray(m_array, dtype=np.int32)
+        _lib.check(self.L.gfmc_set_diag_operators(self.h, len(descs), arr, len(m),
+                                                  m.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))),
+                   "gfmc_set_diag_operators")
+        self.diag_widths = widths
+        self.diag_width = self.L.gfmc_diag_width(self.h)
+        return widths
+
+    def reset_diag(self):
+        _lib.check(self.L.gfmc_reset_diag(self.h, self.n, self._stream()), "gfmc_reset_diag")
+
+    def set_diag_output(self, out):
+        _lib.check(self.L.gfmc_set_diag_output(self.h, self._ptr(out) if out is not None
+                                               else ctypes.c_void_p(0)), "gfmc_set_diag_output")
+
     def windowed_energy(self, logG, E, p_array):
         p = np.ascontiguousarray(p_array, dtype=np.int32)
         out = np.zeros(len(p), dtype=np.float64)
@@ -336,6 +401,11 @@ class GFMCEngine:
             out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), self._stream()),
             "gfmc_windowed_energy")
         return dict(zip([int(v) for v in p], out.tolist()))
+
+
+def _is_vector_op(op):
+    """Whether diagonal_weight returns a vector (keeps its value axis)."""
+    return all(hasattr(op, a) for a in ("cos", "sin", "offset"))
 
 
 def key_schedule(key, n_steps):
@@ -465,9 +535,10 @@ def run_gfmc(walkers, n_steps, hamiltonian, step_size, guide, p_array, *, method
     if len(p_array) != p_in:
         _emit(f"[gfmc.run_gfmc] dedup'd p_array: {p_in - len(p_array)} duplicate value(s) "
               f"dropped, using {p_array}", verbosity)
-    if diag_operators or off_diag_operators:
+    if off_diag_operators:
         raise NotImplementedError(
-            "diagonal/off-diagonal forward-walking operators are not built into the B200 engine yet")
+            "off-diagonal forward-walking operators are not built into the B200 engine yet")
+    diag_names = list(diag_operators.keys()) if diag_operators else []
     m_array = [p // 2 for p in p_array]
     if p_array[-1] >= n_steps:
         raise ValueError(f"every p value must be smaller than n_steps: got n_steps={n_steps} and "
@@ -528,6 +599,15 @@ def run_gfmc(walkers, n_steps, hamiltonian, step_size, guide, p_array, *, method
     if not stages:
         _emit(f"[gfmc] - [run_gfmc] - no warmup (warmup_steps=0), avg_log_weight={alw:.6f}", verbosity, 8)
 
+    # ---- diagonal forward walking: ring buffers start after the warm-up
+    #      (driver.py _diag_ring_buffers:810-838, called after _warmup)
+    n_p = len(p_array)
+    diag_d = None
+    if diag_names:
+        widths = eng.set_diag_operators(diag_operators, m_array)
+        eng.reset_diag()
+        diag_d = torch.zeros((n_steps, eng.diag_width, n_p), dtype=torch.float64, device=dev)
+
     # ---- production (driver.py _production:940-1143), chunked and pipelined
     print_every = max(1, n_steps // max(1, number_of_outputs))
     chunk = print_every if verbosity >= 1 else n_steps
@@ -545,6 +625,8 @@ def run_gfmc(walkers, n_steps, hamiltonian, step_size, guide, p_array, *, method
         cs = min(chunk, n_steps - step0)
         keys, key = key_schedule(key, cs)
         sl = slice(step0, step0 + cs)
+        if diag_d is not None:
+            eng.set_diag_output(diag_d[sl])
         eng.steps(method, step_f, lam, alw, keys, logG_d[sl], E_d[sl], hops_d[sl])
         logG_h[sl].copy_(logG_d[sl], non_blocking=True)
         E_h[sl].copy_(E_d[sl], non_blocking=True)
@@ -577,6 +659,30 @@ def run_gfmc(walkers, n_steps, hamiltonian, step_size, guide, p_array, *, method
     energy = eng.windowed_energy(logG_d, E_d, p_array)
 
     cfg_d, e_d = eng.population()
+    diag_np = additional_diag_np = None
+    if diag_d is not None:
+        def split_cols(arr):
+            out, c = {}, 0
+            for name, w in zip(diag_names, widths):
+                a = arr[:, c:c + w, :]
+                out[name] = a[:, 0, :].copy() if w == 1 and not _is_vector_op(diag_operators[name]) \
+                    else a.copy()
+                c += w
+            return out
+        diag_np = split_cols(diag_d.cpu().numpy())
+        m_max = max(m_array)
+        if m_max > 0:
+            # the lead-in a continuation substitutes for its first rows: m_max
+            # further steps walked with this run's ancestry (driver.py:1101-1127);
+            # the returned walkers stay the production-final ones
+            keys_x, _ = key_schedule(key, m_max)
+            extra = torch.zeros((m_max, eng.diag_width, n_p), dtype=torch.float64, device=dev)
+            eng.set_diag_output(extra)
+            lgx = torch.empty(m_max, dtype=torch.float64, device=dev)
+            Ex = torch.empty(m_max, dtype=torch.float64, device=dev)
+            eng.steps(method, step_f, lam, alw, keys_x, lgx, Ex)
+            additional_diag_np = split_cols(extra.cpu().numpy())
+        eng.set_diag_output(None)
     cfg_np = cfg_d.cpu().numpy()
     in_dtype = np.asarray(config).dtype if not torch.is_tensor(config) else np.float64
     if in_dtype.kind == "f":
@@ -611,12 +717,15 @@ def run_gfmc(walkers, n_steps, hamiltonian, step_size, guide, p_array, *, method
         "parameters/rng_key": rng_key_in,
         "parameters/rng_key_next": key,
     }
-    stats.update(autocorrelation_stats(E_np, weights_np))
-    obs = {}
+    stats.update(autocorrelation_stats(E_np, weights_np, diag_np=diag_np))
+    stats["parameters/diag_operators"] = np.asarray(diag_names, dtype="S64")
+    stats["parameters/n_diag_operators"] = len(diag_names)
+    obs = diagonal_estimates(p_array, weights_np, diag_np) if diag_np else {}
     if return_raw:
-        raw = dict(log_weights=weights_np, energy=E_np, diag=None, off_diag=None, off_diag_norm=None,
-                   off_diag_steps=None, additional_diag=None, p_array=list(p_array),
-                   m_array=list(m_array), diag_operators=None, off_diag_operators=None)
+        raw = dict(log_weights=weights_np, energy=E_np, diag=diag_np, off_diag=None,
+                   off_diag_norm=None, off_diag_steps=None, additional_diag=additional_diag_np,
+                   p_array=list(p_array), m_array=list(m_array),
+                   diag_operators=list(diag_names) or None, off_diag_operators=None)
         return out_w, energy, obs, stats, raw
     return out_w, energy, obs, stats
 

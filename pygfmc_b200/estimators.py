@@ -9,7 +9,7 @@ progress lines (:268-305; the final estimate runs on the device),
 """
 import numpy as np
 
-__all__ = ["validated_p_array", "windowed_energy_host", "autocorrelation",
+__all__ = ["validated_p_array", "windowed_energy_host", "diagonal_estimates", "autocorrelation",
            "autocorrelation_stats", "jackknife_energy", "evaluate_observables"]
 
 
@@ -38,6 +38,25 @@ def windowed_energy_host(p_array, log_weights, E):
         lg = L[p:] - L[:-p]
         G = np.exp(lg - np.max(lg))
         out[p] = float(np.sum(G * E[p:])) / float(np.sum(G))
+    return out
+
+
+def diagonal_estimates(p_array, log_weights, diag_by_name, m_max_common=0):
+    """Ancestry-traced diagonal estimates (engine/estimators.py:287-303):
+    <D>_p = sum_i G_p(i) D(i+p) / sum_i G_p(i) over the window starts
+    i >= m_max_common; D(t) = raw['diag'][name][t, ..., j]."""
+    L = np.cumsum(np.asarray(log_weights, dtype=np.float64))
+    out = {name: {} for name in diag_by_name}
+    for j, p in enumerate(validated_p_array(p_array)):
+        lg = (L[p:] - L[:-p])[m_max_common:]
+        G = np.exp(lg - np.max(lg))
+        gs = float(np.sum(G))
+        for name, arr in diag_by_name.items():
+            a = np.asarray(arr, dtype=np.float64)
+            if a.ndim == 2:
+                out[name][p] = float(np.sum(G * a[:, j][p:][m_max_common:])) / gs
+            else:
+                out[name][p] = np.sum(G[:, None] * a[:, :, j][p:][m_max_common:], axis=0) / gs
     return out
 
 
@@ -70,9 +89,25 @@ def autocorrelation(series, c=5.0):
     return float(run[i]), int(M[i])
 
 
-def autocorrelation_stats(E_np, log_weights_np):
-    return {"autocorrelation/energy_estimator": autocorrelation(E_np)[0],
-            "autocorrelation/log_weights": autocorrelation(log_weights_np)[0]}
+def _series_tau(arr, scale=1):
+    a = np.asarray(arr)
+    if a.ndim == 1:
+        a = a[:, None]
+    trailing = a.shape[1:]
+    flat = a.reshape(a.shape[0], -1)
+    return np.array([autocorrelation(flat[:, j])[0] * scale for j in range(flat.shape[1])],
+                    dtype=float).reshape(trailing)
+
+
+def autocorrelation_stats(E_np, log_weights_np, diag_np=None, off_diag_np=None, off_diag_stride=1):
+    """engine/estimators.py autocorrelation_stats:172-226."""
+    out = {"autocorrelation/energy_estimator": autocorrelation(E_np)[0],
+           "autocorrelation/log_weights": autocorrelation(log_weights_np)[0]}
+    for name, arr in (diag_np or {}).items():
+        out[f"autocorrelation/diag/{name}"] = _series_tau(arr)
+    for name, arr in (off_diag_np or {}).items():
+        out[f"autocorrelation/off_diag/{name}"] = _series_tau(arr, scale=int(off_diag_stride))
+    return out
 
 
 def jackknife_energy(p_array, log_weights, E, n_blocks):

@@ -16,7 +16,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-__all__ = ["SpinHalf", "BoseHubbard", "Lattice", "chain", "square", "kagome", "edges_array"]
+__all__ = ["SpinHalf", "BoseHubbard", "SzSzStructureFactor", "Lattice", "chain", "square",
+           "kagome", "edges_array"]
 
 
 def edges_array(edges):
@@ -392,6 +393,39 @@ class BoseHubbard:
         x[a[idx]] += da[idx]
         x[b[idx]] += db[idx]
         return x
+
+
+class SzSzStructureFactor:
+    """S^zz(k) for one or many wavevectors (hamiltonian/observables.py:68-176):
+    ``diagonal_weight`` = (|sum_i x_i e^{i k.r_i}|^2 - N) / 4 per k, from
+    float64 cos/sin tables of k.r.  Exact for k in the reciprocal lattice of
+    the simulation cell (the caller's responsibility, as in PyGFMC)."""
+
+    def __init__(self, positions, k_vectors, dtype=np.float32):
+        r = np.atleast_2d(np.asarray(positions, dtype=np.float64))
+        k = np.atleast_2d(np.asarray(k_vectors, dtype=np.float64))
+        if r.ndim != 2 or k.ndim != 2:
+            raise ValueError(f"positions must be (N, d) and k_vectors (n_k, d); got {r.shape} and {k.shape}.")
+        if k.shape[1] != r.shape[1]:
+            raise ValueError(f"k_vectors have dimension {k.shape[1]} but positions have {r.shape[1]}; "
+                             "a wavevector needs one component per spatial dimension of the lattice.")
+        kr = k @ r.T
+        dt = np.dtype(dtype)
+        self.cos = np.cos(kr).astype(dt)
+        self.sin = np.sin(kr).astype(dt)
+        self.offset = dt.type(0.25 * r.shape[0])
+        self.k_vectors = k.astype(dt)
+        self.N = r.shape[0]
+
+    @property
+    def n_k(self):
+        return self.cos.shape[0]
+
+    def diagonal_weight(self, config):
+        x = np.asarray(config, dtype=np.float64)
+        c = x @ np.asarray(self.cos, np.float64).T
+        s_ = x @ np.asarray(self.sin, np.float64).T
+        return 0.25 * (c ** 2 + s_ ** 2) - float(self.offset)
 
 
 # ---- lattices ----------------------------------------------------------------

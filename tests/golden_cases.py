@@ -36,6 +36,18 @@ def engine_system(P, name):
     return H, w, g, 0.1, 20.0
 
 
+def engine_diag_ops(P, name):
+    """The diagonal operators of the golden systems (test_golden_outputs.py
+    _spinhalf:196-216, _bose:233-245)."""
+    if name.startswith("spinhalf"):
+        e = P.chain(8).edges
+        pos = np.arange(8, dtype=float)[:, None]
+        ks = (2 * np.pi * np.arange(3) / 8)[:, None]
+        return {"zz": P.SpinHalf.create(e, J_z=1.0, dtype=np.float64),
+                "sf": P.hamiltonian.SzSzStructureFactor(pos, ks, dtype=np.float64)}
+    return {"nn": P.BoseHubbard.create(P.chain(6).edges, U=2.0, n_max=2, dtype=np.float64)}
+
+
 def _crc(s):
     import zlib
     return zlib.crc32(s.encode())

@@ -7,7 +7,7 @@ import ctypes
 import numpy as np
 import pytest
 
-from golden_cases import CASES, engine_system, method_of, oracle_system
+from golden_cases import CASES, engine_diag_ops, engine_system, method_of, oracle_system
 
 pytestmark = pytest.mark.gpu
 
@@ -27,8 +27,14 @@ def test_engine_reproduces_golden_run(P, golden, name):
     key = golden[name + "/stats/parameters/rng_key"]
     walkers, energy, obs, stats, raw = P.run(
         w, 300, H, step, g, [2, 4], method=method, rng_key=key,
-        lam=None if method == "cont_time" else lam, warmup_steps=8, verbosity=0)
+        lam=None if method == "cont_time" else lam, warmup_steps=8, verbosity=0,
+        diag_operators=engine_diag_ops(P, name))
     p = name + "/"
+    for dn in engine_diag_ops(P, name):
+        np.testing.assert_allclose(raw["diag"][dn], golden[p + f"raw/diag/{dn}"], rtol=1e-10,
+                                   atol=1e-12, err_msg=dn)
+        np.testing.assert_allclose(raw["additional_diag"][dn], golden[p + f"raw/additional_diag/{dn}"],
+                                   rtol=1e-10, atol=1e-12, err_msg=dn)
     assert np.array_equal(walkers.config, golden[p + "config"].astype(np.float64))
     np.testing.assert_allclose(raw["log_weights"], golden[p + "raw/log_weights"], rtol=1e-10, atol=1e-12)
     np.testing.assert_allclose(raw["energy"], golden[p + "raw/energy"], rtol=1e-10, atol=1e-12)
