@@ -190,6 +190,56 @@ int gfmc_reset_diag(gfmc_handle *h, int n_walkers, void *stream);
  * stops the measurement. */
 int gfmc_set_diag_output(gfmc_handle *h, double *out);
 
+/* ---- off-diagonal observables with forward walking ---------------------- */
+/* At most this many windows per forward walk. */
+#define GFMC_FW_MAX_P 16
+
+/* Applies the measurement operator of handle `op` (a model handle built from
+ * the operator and the run's guide) to the population cfg (read through
+ * parents when parents_valid): each walker moves to a successor drawn in
+ * proportion to the operator's guide-transformed rates, slot 0 (the diagonal)
+ * meaning stay, with the uniform of Threefry key fold_in(key, walker); its
+ * value is the sum of the rates, 0 when that is not positive.  A purely
+ * diagonal operator keeps the walker and returns its diagonal element.
+ * Replaces engine/evolution.py apply_operator_one:849-888 (vmapped in
+ * forward_walk_operator:1008-1012).  Outputs (device): cfg_out (packed,
+ * n_walkers), vals (float64, n_walkers). */
+int gfmc_apply_operator(gfmc_handle *op, const uint32_t key[2], int n_walkers, const void *cfg,
+                        const int32_t *parents, int parents_valid, void *cfg_out, double *vals,
+                        void *stream);
+
+/* Forward-walking pure estimator of one operator at one measured step
+ * (engine/evolution.py forward_walk_operator:891-1101): gfmc_apply_operator
+ * with op and apply_key, then a shadow chain of m_max = m_array[n_m - 1]
+ * branching steps of the model of handle `shadow` (the run's model and guide)
+ * started from the operator-applied walkers with zero log weights, keyed by
+ * shadow_keys (host, (m_max, 4): the (k1, k2) pairs of the main chain's next
+ * m_max steps, so the shadow replays the main chain's future draws).  After
+ * every shadow reconfiguration the values follow the parent map.  Outputs
+ * (device, n_m each): val_out[j] = mean of the values after m_array[j] shadow
+ * steps, norm_out[j] = sum of the shadow's log G over those steps (row m = 0:
+ * the plain mean, norm 0).  m_array: host, sorted, non-negative, at most
+ * GFMC_FW_MAX_P entries.  The shadow population lives in s_cfg, s_cfg_tmp,
+ * s_parents, s_log_w, s_e_loc (device, n_walkers each) and vals, vals_tmp
+ * (float64 device scratch, n_walkers); the main population is only read.
+ * `shadow` may be the main chain's handle: its carried guide state is then
+ * rebuilt on the main chain's next step, and its diagonal measurement pauses
+ * during the shadow steps. */
+int gfmc_forward_walk(gfmc_handle *shadow, gfmc_handle *op, int method, double step, double lam,
+                      double alw, const uint32_t apply_key[2], const uint32_t *shadow_keys,
+                      int n_walkers, const void *cfg, const int32_t *parents, int parents_valid,
+                      void *s_cfg, void *s_cfg_tmp, int32_t *s_parents, double *s_log_w,
+                      double *s_e_loc, double *vals, double *vals_tmp, int n_m,
+                      const int *m_array, double *val_out, double *norm_out, void *stream);
+
+/* Smallest guide-transformed rate of the operator of handle `op` over all its
+ * M_total slots, per walker of cfg (read through parents when parents_valid);
+ * NaN where a rate is not finite.  The positivity check of engine/
+ * estimators.py check_off_diag_operator_positivity:631-681 reads it.
+ * Output (device): min_out (float64, n_walkers). */
+int gfmc_operator_min_rate(gfmc_handle *op, int n_walkers, const void *cfg, const int32_t *parents,
+                           int parents_valid, double *min_out, void *stream);
+
 /* Largest population gfmc_reconfigure_noalloc accepts. */
 #define GFMC_NOALLOC_MAX_WALKERS 131072
 
@@ -219,6 +269,11 @@ int gfmc_read_status(gfmc_handle *h, int *status_out, void *stream);
  * keys_out[4 s .. 4 s + 3] = (k1, k2) for n_steps steps and the final key. */
 int gfmc_key_schedule(const uint32_t key[2], int n_steps, uint32_t *keys_out,
                       uint32_t key_next[2]);
+/* The same recurrence with n_sub sub-keys per step: keys_out[2 (s n_sub + j)
+ * .. + 1] = fold_in(rng_s, j), j < n_sub (folds
+ * 0 = evolve, 1 = reconfigure, 2 = off-diagonal measurement; driver.py:218-221). */
+int gfmc_key_schedule_ex(const uint32_t key[2], int n_steps, int n_sub, uint32_t *keys_out,
+                         uint32_t key_next[2]);
 /* Threefry-2x32 and fold_in on the host (jax key semantics). */
 int gfmc_threefry2x32(uint32_t k0, uint32_t k1, uint32_t c0, uint32_t c1, uint32_t out[2]);
 

@@ -494,6 +494,33 @@ int om_reconfigure(const uint32_t key[2], int n, int N, double *cfg, double *lw,
   return 0;
 }
 
+/* evolution.apply_operator_one:849-888, vmapped with per-walker keys
+ * fold_in(key, w) (forward_walk_operator:1008-1012): the successor drawn
+ * from cdf = cumsum(rates) (slot 0 = stay), value = the rate sum, 0 and no
+ * move when it is not positive; M_total == 1 keeps x and returns rates[0]. */
+int om_apply_operator(const om_model *m, const om_guide *g, const uint32_t key[2], int n_walkers,
+                      double *cfg, double *vals) {
+  int M = om_M(m), N = m->N;
+  const om_guide *gg = (g && g->kind) ? g : NULL;
+  double *buf = (double *)malloc(sizeof(double) * (size_t)(3 * M + N + 8));
+  double *r = buf, *cdf = buf + M, *scratch = buf + 2 * M;
+  om_key k = {key[0], key[1]};
+  for (int w = 0; w < n_walkers; ++w) {
+    double *x = cfg + (size_t)w * N;
+    om_rates(m, gg, x, r, scratch);
+    if (M == 1) { vals[w] = r[0]; continue; }
+    double acc = 0.0;
+    for (int s = 0; s < M; ++s) { acc += r[s]; cdf[s] = acc; }
+    double total = cdf[M - 1];
+    if (total <= 0.0) { vals[w] = 0.0; continue; }
+    int idx = om_sample_index(cdf, r, M, om_uniform64(om_fold(k, (uint32_t)w)));
+    om_apply(m, x, idx);
+    vals[w] = total;
+  }
+  free(buf);
+  return 0;
+}
+
 /* sample_index exported for the sampler edge-case tests. */
 int om_sample_index_export(const double *cdf, const double *w, int M, double U) {
   return om_sample_index(cdf, w, M, U);

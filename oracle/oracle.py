@@ -20,7 +20,9 @@ Reference files restated here (paths inside the PyGFMC project):
                                      _base_config_for_sum:143
   engine/driver.py                   run_gfmc:1148, _warmup:747, _warmup_stage:713,
                                      _warmup_schedule:567, _production:940
-  engine/estimators.py               _energy_and_diagonal_estimates:268
+  engine/estimators.py               _energy_and_diagonal_estimates:268,
+                                     _off_diagonal_estimates:308
+  engine/evolution.py                apply_operator_one:849, forward_walk_operator:891
   engine/io.py                       evaluate_observables jackknife:1084-1104
 """
 import ctypes
@@ -86,6 +88,8 @@ def lib():
         L.om_uniform.restype = ctypes.c_double
         L.om_uniform.argtypes = [_up]
         L.om_sample_index_export.argtypes = [_dp, _dp, ctypes.c_int, ctypes.c_double]
+        L.om_apply_operator.argtypes = [ctypes.POINTER(_Model), ctypes.POINTER(_Guide), _up,
+                                        ctypes.c_int, _dp, _dp]
         L.om_threads.restype = ctypes.c_int
         _lib = L
     return _lib
@@ -460,6 +464,61 @@ def initial_alw(model, guide, method, lam, cfg):
                                 cfg.shape[0], _p(cfg))
 
 
+def apply_operator(model, guide, key, cfg):
+    """apply_operator_one over the walkers (per-walker keys fold_in(key, w)),
+    in place on cfg; returns the operator values."""
+    key = np.ascontiguousarray(key, dtype=np.uint32)
+    vals = np.zeros(cfg.shape[0])
+    lib().om_apply_operator(ctypes.byref(model.s), ctypes.byref(guide.s), _p(key, _up),
+                            cfg.shape[0], _p(cfg), _p(vals))
+    return vals
+
+
+def forward_walk(cfg, op_model, op_guide, model, guide, method, step, lam, alw, apply_key,
+                 shadow_key, m_array, n_threads=0):
+    """engine/evolution.py forward_walk_operator:891-1101 restated: apply
+    the operator, then max(m_array) shadow steps of the main model from the
+    applied walkers (zero log weights) under the key recurrence started at
+    shadow_key; the values follow each parent map.  Returns (val, log_norm)
+    at the depths m_array (row m = 0: the plain mean, norm 0)."""
+    x = np.array(cfg, dtype=np.float64, copy=True)
+    n = x.shape[0]
+    v = apply_operator(op_model, op_guide, apply_key, x)
+    lw = np.zeros(n); el = np.zeros(n)
+    m_max = max(m_array)
+    fw = [float(np.mean(v))]
+    nrm = [0.0]
+    acc = 0.0
+    key = np.asarray(shadow_key, np.uint32)
+    for _ in range(m_max):
+        key, r = split(key, 2)
+        evolve(model, guide, method, step, lam, alw, fold_in(r, 0), x, lw, el, n_threads)
+        par, lG, _ = reconfigure(fold_in(r, 1), x, lw, el)
+        v = v[par]
+        acc = acc + lG
+        fw.append(float(np.mean(v)))
+        nrm.append(acc)
+    return np.array([fw[m] for m in m_array]), np.array([nrm[m] for m in m_array])
+
+
+def off_diagonal_estimates(p_array, m_array, log_weights, fw, nrm, steps, m_max_common=0):
+    """engine/estimators.py _off_diagonal_estimates:308-355 restated for one
+    operator: fw, nrm (n_rows, n_p) at main-chain steps `steps`."""
+    L = np.concatenate([[0.0], np.cumsum(np.asarray(log_weights, float))])
+    n = len(log_weights)
+    steps = np.asarray(steps)
+    out = {}
+    for j, (p, m) in enumerate(zip(sorted(p_array), m_array)):
+        sel = (steps >= p + max(0, m_max_common - m)) & (steps < n - m)
+        i = steps[sel] - p
+        num_l = L[p + 1 + i] - L[p - m + 1 + i] + np.asarray(nrm)[sel, j]
+        den_l = L[p + m + 1 + i] - L[p - m + 1 + i]
+        sh = max(np.max(num_l[np.isfinite(num_l)]), np.max(den_l))
+        out[p] = float(np.sum(np.exp(num_l - sh) * np.asarray(fw)[sel, j])) / \
+            float(np.sum(np.exp(den_l - sh)))
+    return out
+
+
 def sample_index(cdf, w, U):
     cdf = np.ascontiguousarray(cdf, np.float64); w = np.ascontiguousarray(w, np.float64)
     return lib().om_sample_index_export(_p(cdf), _p(w), len(cdf), float(U))
@@ -488,10 +547,13 @@ def warmup_schedule(method, step_f, warmup_steps):
 
 
 def run(cfg, n_steps, model, step_size, guide, p_array, method="cont_time", rng_key=None,
-        lam=None, warmup_steps=1000, avg_log_weight=None, n_threads=0):
+        lam=None, warmup_steps=1000, avg_log_weight=None, n_threads=0, off_diag_operators=None):
     """engine/driver.py run_gfmc restated for the main chain (warm-up ramp
     on the aux side-streams, then the production key recurrence
     key, rng = split(key); k1, k2 = fold_in(rng, 0), fold_in(rng, 1)).
+    off_diag_operators: list of (name, op_model, op_guide) measured by
+    forward walking after every production step (stride 1), apply keys
+    fold_in(fold_in(rng, 2), i) and the shadow started from the next key.
     Returns a namespace with the final walkers, alw, raw series, energies."""
     cfg = np.array(cfg, dtype=np.float64, copy=True)
     n = cfg.shape[0]
@@ -520,6 +582,10 @@ def run(cfg, n_steps, model, step_size, guide, p_array, method="cont_time", rng_
     key = rng_key.copy()
     LG = np.zeros(n_steps); E = np.zeros(n_steps); hops = np.zeros(n_steps)
     parents = np.zeros((n_steps, n), np.int32)
+    ops = list(off_diag_operators or [])
+    m_array = [p // 2 for p in sorted(set(int(p) for p in p_array))]
+    off = {nm: np.zeros((n_steps, len(m_array))) for nm, _, _ in ops}
+    off_norm = {nm: np.zeros((n_steps, len(m_array))) for nm, _, _ in ops}
     for s_ in range(n_steps):
         key, r = split(key, 2)
         k1, k2 = fold_in(r, 0), fold_in(r, 1)
@@ -527,10 +593,16 @@ def run(cfg, n_steps, model, step_size, guide, p_array, method="cont_time", rng_
         par, LG[s_], E[s_] = reconfigure(k2, cfg, lw, el)
         parents[s_] = par
         hops[s_] = h.mean()
+        if ops:
+            k3 = fold_in(r, 2)
+            for i, (nm, om, og) in enumerate(ops):
+                off[nm][s_], off_norm[nm][s_] = forward_walk(
+                    cfg, om, og, model, guide, method, step_size, lam, alw, fold_in(k3, i), key,
+                    m_array, n_threads)
     energy = windowed_energy(p_array, LG, E)
     return SimpleNamespace(config=cfg, log_weight=lw, e_loc=el, alw=alw, log_weights=LG,
                            energy_series=E, energy=energy, rng_key_next=key, parents=parents,
-                           hops=hops)
+                           hops=hops, off_diag=off, off_diag_norm=off_norm, m_array=m_array)
 
 
 def windowed_energy(p_array, log_weights, E):

@@ -88,9 +88,17 @@ SIGNATURES = {
     "gfmc_diag_width": (ctypes.c_int, [_vp]),
     "gfmc_reset_diag": (ctypes.c_int, [_vp, ctypes.c_int, _vp]),
     "gfmc_set_diag_output": (ctypes.c_int, [_vp, _vp]),
+    "gfmc_apply_operator": (ctypes.c_int, [_vp, _u32p, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp,
+                                           _vp, _vp]),
+    "gfmc_forward_walk": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                         ctypes.c_double, _u32p, _u32p, ctypes.c_int, _vp, _vp,
+                                         ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                         ctypes.c_int, _i32p, _vp, _vp, _vp]),
+    "gfmc_operator_min_rate": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp, _vp]),
     "gfmc_reconfigure_noalloc": (ctypes.c_int, [ctypes.c_int, _vp, _vp, _u32p, _vp, _vp, _vp, _vp]),
     "gfmc_read_status": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int), _vp]),
     "gfmc_key_schedule": (ctypes.c_int, [_u32p, ctypes.c_int, _u32p, _u32p]),
+    "gfmc_key_schedule_ex": (ctypes.c_int, [_u32p, ctypes.c_int, ctypes.c_int, _u32p, _u32p]),
     "gfmc_threefry2x32": (ctypes.c_int, [ctypes.c_uint32] * 4 + [_u32p]),
     "gfmc_last_error": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_size_t]),
     "gfmc_version": (ctypes.c_char_p, []),

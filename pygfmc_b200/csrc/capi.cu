@@ -10,6 +10,7 @@
 
 #include "../../include/gfmc_b200.h"
 #include "diag.cuh"
+#include "fw.cuh"
 #include "engine.cuh"
 
 using namespace gfmc;
@@ -93,6 +94,11 @@ struct gfmc_handle {
   int diag_cap_n = 0, diag_slot = 0, diag_ready = 0;
   double *diag_partial = nullptr;
   double *diag_out = nullptr;
+  // off-diagonal forward walking through this handle as the shadow chain
+  FwHook *fw = nullptr;              // installed for the length of one walk
+  int *ctr1 = nullptr;               // work counter of single launches (apply, min rate)
+  double *fw_partial = nullptr, *fw_logG = nullptr, *fw_E = nullptr;
+  int fw_cap_rows = 0, fw_cap_nb = 0;
 };
 
 namespace {
@@ -483,6 +489,13 @@ int run_steps_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, int 
     r.status = h->status;
     e = launch_reconfigure(r, s);
     if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "reconfigure launch: %s", cudaGetErrorString(e));
+    if (h->fw) {
+      FwHook &f = *h->fw;
+      double *pp = f.rec[st + 1] ? f.partial + (size_t)(st + 1) * f.nb : nullptr;
+      e = launch_fw_remap(n, parents, f.v[f.cur], f.v[1 - f.cur], pp, s);
+      if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "forward-walk remap: %s", cudaGetErrorString(e));
+      f.cur = 1 - f.cur;
+    }
     if (h->diag_out && h->diag_ready) {
       const int NW = (h->N + 63) / 64;
       e = launch_diag_step(h->diag, h->family, n, NW, h->cfg_bytes, nxt, parents, h->diag_slot,
@@ -498,6 +511,52 @@ int run_steps_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, int 
   if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "series reduce: %s", cudaGetErrorString(e));
   if (cur != cfg)
     GFMC_CUDA(cudaMemcpyAsync(cfg, cur, (size_t)n * h->cfg_bytes, cudaMemcpyDeviceToDevice, s));
+  return GFMC_OK;
+}
+
+// One launch of the per-walker kernel in APPLY or MIN_RATE mode through
+// handle h (an operator's handle): reads cfg[parents[i]], writes the moved
+// configuration (cfg_out, nullable) and one float64 per walker.  Touches only
+// the handle's work counter and status word, so an operator handle holds no
+// population-sized scratch.
+template <typename T>
+int single_launch_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, int method,
+                    Key key, int n, const void *cfg, const int32_t *parents, void *cfg_out,
+                    double *out, cudaStream_t s) {
+  if (!h->ctr1) GFMC_CUDA(cudaMalloc(&h->ctr1, sizeof(int)));
+  if (!h->status) {
+    GFMC_CUDA(cudaMalloc(&h->status, sizeof(int)));
+    GFMC_CUDA(cudaMemset(h->status, 0, sizeof(int)));
+  }
+  GFMC_CUDA(cudaMemsetAsync(h->ctr1, 0, sizeof(int), s));
+  EvolveArgs a{};
+  a.method = method;
+  a.key = key;
+  a.n_walkers = n;
+  a.parents = parents;
+  a.cfg_in = cfg;
+  a.cfg_out = cfg_out;
+  a.e_loc = out;
+  a.work_ctr = h->ctr1;
+  a.status = h->status;
+  a.max_iters = 1;
+  cudaError_t e = launch_evolve<T>(m, g, h->plan, a, s);
+  if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "operator launch: %s", cudaGetErrorString(e));
+  return GFMC_OK;
+}
+
+int single_launch(gfmc_handle *h, int method, Key key, int n, const void *cfg,
+                  const int32_t *parents, void *cfg_out, double *out, cudaStream_t s) {
+  if (h->precision == GFMC_PRECISION_FP64)
+    return single_launch_t<double>(h, h->m64, h->g64, method, key, n, cfg, parents, cfg_out, out, s);
+  return single_launch_t<float>(h, h->m32, h->g32, method, key, n, cfg, parents, cfg_out, out, s);
+}
+
+int check_method(int method, double step) {
+  if (method < 0 || method > 2) return fail(GFMC_ERR_INVALID, "unknown method %d", method);
+  if (method != GFMC_METHOD_CONT_TIME && (step < 1.0 || step != (double)(long long)step))
+    return fail(GFMC_ERR_INVALID, "discrete methods need a positive integer step");
+  if (!(step > 0.0)) return fail(GFMC_ERR_INVALID, "step must be > 0");
   return GFMC_OK;
 }
 
@@ -564,6 +623,7 @@ int gfmc_destroy(gfmc_handle *h) {
   cudaFree(h->fbuf[0]); cudaFree(h->fbuf[1]);
   cudaFree(h->d_ops); cudaFree(h->d_diag_tables); cudaFree(h->diag.ring_parents);
   cudaFree(h->diag.ring_vals); cudaFree(h->diag_partial);
+  cudaFree(h->fw_partial); cudaFree(h->fw_logG); cudaFree(h->fw_E); cudaFree(h->ctr1);
   delete h;
   return GFMC_OK;
 }
@@ -801,6 +861,116 @@ int gfmc_key_schedule(const uint32_t key[2], int n_steps, uint32_t *keys_out, ui
   }
   key_next[0] = k.a;
   key_next[1] = k.b;
+  return GFMC_OK;
+}
+
+int gfmc_key_schedule_ex(const uint32_t key[2], int n_steps, int n_sub, uint32_t *keys_out,
+                         uint32_t key_next[2]) {
+  if (!key || n_steps < 0 || n_sub < 1 || (n_steps && !keys_out) || !key_next)
+    return fail(GFMC_ERR_INVALID, "gfmc_key_schedule_ex: bad argument");
+  Key k{key[0], key[1]};
+  for (int s = 0; s < n_steps; ++s) {
+    const Key nk = fold(k, 0u), rng = fold(k, 1u);
+    for (int j = 0; j < n_sub; ++j) {
+      const Key kj = fold(rng, (uint32_t)j);
+      keys_out[2 * ((size_t)s * n_sub + j) + 0] = kj.a;
+      keys_out[2 * ((size_t)s * n_sub + j) + 1] = kj.b;
+    }
+    k = nk;
+  }
+  key_next[0] = k.a;
+  key_next[1] = k.b;
+  return GFMC_OK;
+}
+
+int gfmc_apply_operator(gfmc_handle *op, const uint32_t key[2], int n, const void *cfg,
+                        const int32_t *parents, int parents_valid, void *cfg_out, double *vals,
+                        void *stream) {
+  if (!op || !key || n <= 0 || !cfg || !cfg_out || !vals || cfg == cfg_out ||
+      (parents_valid && !parents))
+    return fail(GFMC_ERR_INVALID, "gfmc_apply_operator: bad argument");
+  return single_launch(op, APPLY, Key{key[0], key[1]}, n, cfg, parents_valid ? parents : nullptr,
+                       cfg_out, vals, (cudaStream_t)stream);
+}
+
+int gfmc_operator_min_rate(gfmc_handle *op, int n, const void *cfg, const int32_t *parents,
+                           int parents_valid, double *min_out, void *stream) {
+  if (!op || n <= 0 || !cfg || !min_out || (parents_valid && !parents))
+    return fail(GFMC_ERR_INVALID, "gfmc_operator_min_rate: bad argument");
+  return single_launch(op, MIN_RATE, Key{0u, 0u}, n, cfg, parents_valid ? parents : nullptr,
+                       nullptr, min_out, (cudaStream_t)stream);
+}
+
+int gfmc_forward_walk(gfmc_handle *sh, gfmc_handle *op, int method, double step, double lam,
+                      double alw, const uint32_t apply_key[2], const uint32_t *shadow_keys, int n,
+                      const void *cfg, const int32_t *parents, int parents_valid, void *s_cfg,
+                      void *s_cfg_tmp, int32_t *s_parents, double *s_log_w, double *s_e_loc,
+                      double *vals, double *vals_tmp, int n_m, const int *m_array,
+                      double *val_out, double *norm_out, void *stream) {
+  if (!sh || !op || !apply_key || n <= 0 || !cfg || !s_cfg || !s_cfg_tmp || !s_parents ||
+      !s_log_w || !s_e_loc || !vals || !vals_tmp || !m_array || !val_out || !norm_out ||
+      (parents_valid && !parents))
+    return fail(GFMC_ERR_INVALID, "gfmc_forward_walk: bad argument");
+  if (cfg == s_cfg || cfg == s_cfg_tmp || s_cfg == s_cfg_tmp || vals == vals_tmp)
+    return fail(GFMC_ERR_INVALID, "gfmc_forward_walk: the shadow buffers must be distinct from "
+                                  "each other and from the main population");
+  if (n_m < 1 || n_m > GFMC_FW_MAX_P)
+    return fail(GFMC_ERR_INVALID, "gfmc_forward_walk: 1 <= n_m <= %d", GFMC_FW_MAX_P);
+  for (int j = 0; j < n_m; ++j)
+    if (m_array[j] < 0 || (j && m_array[j] < m_array[j - 1]))
+      return fail(GFMC_ERR_INVALID, "m_array must be sorted and non-negative");
+  if (sh->precision != op->precision || sh->family != op->family || sh->N != op->N)
+    return fail(GFMC_ERR_INVALID, "operator and shadow handles differ in precision, model family "
+                                  "or site count");
+  const int m_max = m_array[n_m - 1];
+  if (m_max > 0) {
+    if (!shadow_keys) return fail(GFMC_ERR_INVALID, "gfmc_forward_walk: shadow_keys missing");
+    int rc = check_method(method, step);
+    if (rc) return rc;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  const int nb = fw_blocks(n);
+  const int rows = m_max + 1;
+  if (rows > sh->fw_cap_rows || nb > sh->fw_cap_nb) {
+    cudaFree(sh->fw_partial); cudaFree(sh->fw_logG); cudaFree(sh->fw_E);
+    sh->fw_partial = sh->fw_logG = sh->fw_E = nullptr;
+    sh->fw_cap_rows = sh->fw_cap_nb = 0;
+    GFMC_CUDA(cudaMalloc(&sh->fw_partial, sizeof(double) * (size_t)rows * nb));
+    GFMC_CUDA(cudaMalloc(&sh->fw_logG, sizeof(double) * rows));
+    GFMC_CUDA(cudaMalloc(&sh->fw_E, sizeof(double) * rows));
+    sh->fw_cap_rows = rows;
+    sh->fw_cap_nb = nb;
+  }
+  // 1. the operator on the main population (apply_operator_one, vmapped)
+  int rc = single_launch(op, APPLY, Key{apply_key[0], apply_key[1]}, n, cfg,
+                         parents_valid ? parents : nullptr, s_cfg, vals, s);
+  if (rc) return rc;
+  // 2. depth 0: the un-propagated values
+  std::vector<char> rec(rows, 0);
+  for (int j = 0; j < n_m; ++j) rec[m_array[j]] = 1;
+  cudaError_t e = cudaSuccess;
+  if (rec[0]) {
+    e = launch_fw_remap(n, nullptr, vals, nullptr, sh->fw_partial, s);
+    if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "forward-walk sum: %s", cudaGetErrorString(e));
+  }
+  // 3. the shadow chain, the values following every parent map
+  if (m_max > 0) {
+    FwHook hook{{vals, vals_tmp}, 0, rec.data(), sh->fw_partial, nb};
+    double *saved_diag = sh->diag_out;
+    sh->diag_out = nullptr;
+    sh->fw = &hook;
+    rc = gfmc_run_steps(sh, method, step, lam, alw, m_max, shadow_keys, n, s_cfg, s_cfg_tmp,
+                        s_parents, 0, s_log_w, s_e_loc, sh->fw_logG, sh->fw_E, nullptr, stream);
+    sh->fw = nullptr;
+    sh->diag_out = saved_diag;
+    if (rc) return rc;
+  }
+  // 4. means and accumulated log norms at the recorded depths
+  FwRows r{};
+  r.n_m = n_m;
+  for (int j = 0; j < n_m; ++j) r.m[j] = m_array[j];
+  e = launch_fw_finish(sh->fw_partial, nb, n, sh->fw_logG, r, val_out, norm_out, s);
+  if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "forward-walk finish: %s", cudaGetErrorString(e));
   return GFMC_OK;
 }
 

@@ -435,14 +435,22 @@ template <typename T> struct Eval {
   int C;     // slots per lane
 };
 
-// One rate evaluation.  lamform (single_step): slot 0 is the diagonal and
-// the scanned values are the rates, cdf = lam - cumsum(rates); otherwise the
-// slots are the off-diagonal moves and the scanned values their weights
-// -rates, cdf = cumsum(weights).
+// Slot layouts of a rate evaluation:
+//  MODE_OFF (cont_time, multi_step): the off-diagonal moves, scanned values
+//    their weights -rates, cdf = cumsum(weights);
+//  MODE_LAM (single_step): slot 0 the diagonal, scanned values the rates,
+//    cdf = lam - cumsum(rates), weights (lam - H_xx, -rates);
+//  MODE_POS (applying a measurement operator, apply_operator_one:849-888):
+//    slot 0 the diagonal, scanned values and weights the (non-negative)
+//    rates, cdf = cumsum(rates).
+enum SlotMode { MODE_OFF = 0, MODE_LAM = 1, MODE_POS = 2 };
+
+// One rate evaluation in slot layout `mode`.
 template <typename T, int FAM, int FAST>
 __device__ __forceinline__ Eval<T> evaluate(const DevModel<T> &m, const DevGuide<T> &g,
                                             const uint8_t *occ, const T *SF, int n_slots,
-                                            bool lamform, int lane) {
+                                            int mode, int lane) {
+  const bool lamform = mode != MODE_OFF;   // slot 0 is the diagonal
   Eval<T> ev;
   const int C = chunk_of(n_slots);
   ev.C = C;
@@ -511,11 +519,19 @@ __device__ __forceinline__ Eval<T> evaluate(const DevModel<T> &m, const DevGuide
 // Scanned value and weight of slot s (valid slots only).
 template <typename T, int FAM, int FAST>
 __device__ __forceinline__ T slot_q(const DevModel<T> &m, const DevGuide<T> &g, const uint8_t *occ,
-                                    const T *SF, int s, bool lamform, T diag) {
+                                    const T *SF, int s, int mode, T diag) {
+  const bool lamform = mode != MODE_OFF;
   if (lamform && s == 0) return diag;
   int anti;
   const T v = offdiag<T, FAM, FAST>(m, g, occ, SF, lamform ? s - 1 : s, &anti);
   return lamform ? v : -v;
+}
+
+// Weight of slot s with scanned value q.
+template <typename T>
+__device__ __forceinline__ T slot_w(int mode, int s, T q, T lam) {
+  if (mode == MODE_LAM) return s == 0 ? (-q + lam) : -q;
+  return q;
 }
 
 // evolution.sample_index: the first slot whose cdf exceeds u, stepped back to
@@ -527,29 +543,30 @@ __device__ __forceinline__ T slot_q(const DevModel<T> &m, const DevGuide<T> &g, 
 template <typename T, int FAM, int FAST>
 __device__ __forceinline__ int sample_slot(const DevModel<T> &m, const DevGuide<T> &g,
                                            const uint8_t *occ, const T *SF, const Eval<T> &ev,
-                                           int n_slots, bool lamform, T lam, T u, int lane) {
+                                           int n_slots, int mode, T lam, T u, int lane) {
   const int C = ev.C;
   const int last_lane = (n_slots - 1) / C;
-  const T cend = lamform ? lam - ev.end : ev.end;
+  const bool lamc = mode == MODE_LAM;   // cdf = lam - cumsum
+  const T cend = lamc ? lam - ev.end : ev.end;
   const unsigned bal = __ballot_sync(FULL, lane <= last_lane && cend > u);
   const int L = bal ? __ffs(bal) - 1 : last_lane;
   const T exclL = __shfl_sync(FULL, ev.excl, L);
   int s = L * C + lane;
   bool valid = lane < C && s < n_slots;
-  T qv = valid ? slot_q<T, FAM, FAST>(m, g, occ, SF, s, lamform, ev.diag) : T(0);
+  T qv = valid ? slot_q<T, FAM, FAST>(m, g, occ, SF, s, mode, ev.diag) : T(0);
   const T pre = warp_inclusive_scan(qv, lane);
-  const T c = lamform ? lam - (exclL + pre) : exclL + pre;
+  const T c = lamc ? lam - (exclL + pre) : exclL + pre;
   const unsigned hit = __ballot_sync(FULL, valid && c > u);
   const int nvalid = (n_slots - L * C) < C ? (n_slots - L * C) : C;
   const int jh = hit ? __ffs(hit) - 1 : nvalid - 1;
-  T w = lamform ? (s == 0 ? (-qv + lam) : -qv) : qv;
+  T w = slot_w(mode, s, qv, lam);
   unsigned bk = __ballot_sync(FULL, valid && lane <= jh && w > T(0));
   if (bk) return L * C + 31 - __clz(bk);
   for (int L2 = L - 1; L2 >= 0; --L2) {
     s = L2 * C + lane;
     valid = lane < C && s < n_slots;
-    qv = valid ? slot_q<T, FAM, FAST>(m, g, occ, SF, s, lamform, ev.diag) : T(0);
-    w = lamform ? (s == 0 ? (-qv + lam) : -qv) : qv;
+    qv = valid ? slot_q<T, FAM, FAST>(m, g, occ, SF, s, mode, ev.diag) : T(0);
+    w = slot_w(mode, s, qv, lam);
     bk = __ballot_sync(FULL, valid && w > T(0));
     if (bk) return L2 * C + 31 - __clz(bk);
   }
@@ -626,7 +643,7 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta
       T t = T(0);
       uint32_t it = 0;
       while (t < beta) {
-        const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.n_off, false, lane);
+        const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.n_off, MODE_OFF, lane);
         const T R = ev.total;
         const T eL = ev.diag - R;
         if ((it & 15u) == 0) draws = uniform<T>(fold(kw, 2u * it + (uint32_t)lane));
@@ -635,7 +652,7 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta
         int si = 0;
         if (R > T(0)) {
           const T u = U1 * R, cap = next_below(R);
-          si = sample_slot<T, FAM, FAST>(m, g, occ, SF, ev, m.n_off, false, lam,
+          si = sample_slot<T, FAM, FAST>(m, g, occ, SF, ev, m.n_off, MODE_OFF, lam,
                                          u < cap ? u : cap, lane);
         }
         const T tau_raw = (R > T(0)) ? -math_log1p(-psi) / R : pos_inf<T>();
@@ -657,12 +674,12 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta
     } else if (method == SINGLE_STEP) {
       const int n_bra = (int)a.step;
       for (int sidx = 0; sidx < n_bra; ++sidx) {
-        const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.M, true, lane);
+        const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.M, MODE_LAM, lane);
         const T bx = lam - ev.total;
         if ((sidx & 31) == 0) draws = uniform<T>(fold(kw, (uint32_t)(sidx + lane)));
         const T U = __shfl_sync(FULL, draws, sidx & 31);
         const T u = U * bx, cap = next_below(bx);
-        const int idx = sample_slot<T, FAM, FAST>(m, g, occ, SF, ev, m.M, true, lam,
+        const int idx = sample_slot<T, FAM, FAST>(m, g, occ, SF, ev, m.M, MODE_LAM, lam,
                                                   u < cap ? u : cap, lane);
         if (idx != 0) {
           apply_move<T, FAM>(m, g, occ, SF, idx - 1, lane);
@@ -670,7 +687,7 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta
         }
         lw = lw + (double)math_log(bx);
       }
-      const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.n_off, false, lane);
+      const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.n_off, MODE_OFF, lane);
       eloc = ev.diag - ev.total;
       lw -= a.alw * (double)n_bra;
     } else if (method == MULTI_STEP) {
@@ -678,7 +695,7 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta
       int used = 0;
       uint32_t it = 0;
       while (used < n_bra) {
-        const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.n_off, false, lane);
+        const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.n_off, MODE_OFF, lane);
         const T R = ev.total;
         const T bx = lam - ev.diag + R;
         if ((it & 15u) == 0) draws = uniform<T>(fold(kw, 2u * it + (uint32_t)lane));
@@ -687,7 +704,7 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta
         int si = 0;
         if (R > T(0)) {
           const T u = U1 * R, cap = next_below(R);
-          si = sample_slot<T, FAM, FAST>(m, g, occ, SF, ev, m.n_off, false, lam,
+          si = sample_slot<T, FAM, FAST>(m, g, occ, SF, ev, m.n_off, MODE_OFF, lam,
                                          u < cap ? u : cap, lane);
         }
         const int remaining = n_bra - used;
@@ -710,11 +727,48 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta
           break;
         }
       }
-      const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.n_off, false, lane);
+      const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.n_off, MODE_OFF, lane);
       eloc = ev.diag - ev.total;
       lw -= a.alw * (double)n_bra;
+    } else if (method == APPLY) {
+      // apply_operator_one:849-888: draw the successor in proportion to the
+      // operator's guided rates (slot 0 the diagonal, i.e. stay); the value
+      // is their sum, 0 when it is not positive; a purely diagonal operator
+      // keeps the configuration and returns its diagonal element
+      if (m.M == 1) {
+        const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, 0, MODE_OFF, lane);
+        eloc = ev.diag;
+      } else {
+        const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.M, MODE_POS, lane);
+        const T total = ev.total;
+        if (total <= T(0)) {
+          eloc = T(0);
+        } else {
+          const T U = uniform<T>(kw);
+          const T u = U * total, cap = next_below(total);
+          const int idx = sample_slot<T, FAM, FAST>(m, g, occ, SF, ev, m.M, MODE_POS, lam,
+                                                    u < cap ? u : cap, lane);
+          if (idx != 0) apply_move<T, FAM>(m, g, occ, SF, idx - 1, lane);
+          eloc = total;
+        }
+      }
+    } else if (method == MIN_RATE) {
+      // check_off_diag_operator_positivity (engine/estimators.py:631-681):
+      // the smallest guide-transformed rate over all M_total slots, NaN when
+      // one is not finite (the full evaluation gives the diagonal element)
+      const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.M, MODE_POS, lane);
+      T mn = ev.diag;
+      bool bad = !isfinite(ev.diag);
+      for (int o = lane; o < m.n_off; o += 32) {
+        int anti;
+        const T v = offdiag<T, FAM, FAST>(m, g, occ, SF, o, &anti);
+        mn = v < mn ? v : mn;
+        bad = bad || !isfinite(v);
+      }
+      mn = -warp_max(-mn);
+      eloc = __any_sync(FULL, bad) ? T(NAN) : mn;
     } else {  // EVALUATE: local energy of the loaded configuration
-      const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.n_off, false, lane);
+      const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.n_off, MODE_OFF, lane);
       eloc = ev.diag - ev.total;
     }
 
@@ -740,10 +794,10 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta
       for (int k = lane; k < m.N; k += 32) fout[k] = SF[k];
     }
     if (lane == 0) {
-      if (method != EVALUATE) a.log_w[walker] = lw;
+      if (method <= MULTI_STEP) a.log_w[walker] = lw;
       a.e_loc[walker] = (double)eloc;
     }
-    wmax = lw > wmax ? lw : wmax;
+    if (method <= MULTI_STEP) wmax = lw > wmax ? lw : wmax;
     hop_acc += (unsigned long long)hops;
     __syncwarp();
   }

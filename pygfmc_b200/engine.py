@@ -25,8 +25,8 @@ from . import random as _rnd
 from .hamiltonian import BoseHubbard, SpinHalf
 from .walkers import Walker
 from .wavefunction import JastrowBoseHubbard, JastrowSpinHalf
-from .estimators import (autocorrelation_stats, diagonal_estimates, validated_p_array,
-                         windowed_energy_host)
+from .estimators import (autocorrelation_stats, diagonal_estimates, off_diagonal_estimates,
+                         validated_p_array, windowed_energy_host)
 
 __all__ = ["run", "run_gfmc", "GFMCEngine", "DEFAULT_WARMUP_STEPS"]
 
@@ -392,6 +392,40 @@ class GFMCEngine:
         _lib.check(self.L.gfmc_set_diag_output(self.h, self._ptr(out) if out is not None
                                                else ctypes.c_void_p(0)), "gfmc_set_diag_output")
 
+    def copy_population_from(self, other):
+        """This engine's population := other's current population (gathered
+        through its parent map); weights and local energies restart."""
+        par = other.parents if other.parents_valid else self.torch.arange(
+            self.n, dtype=self.torch.int32, device=self.device)
+        _lib.check(self.L.gfmc_gather(self.h, self.n, self._ptr(par), self._ptr(other.cfg),
+                                      self._ptr(self.cfg), self._ptr(other.e_loc), self._ptr(self.e_loc),
+                                      self._ptr(self.log_w), self._stream()), "gfmc_gather")
+        self.parents_valid = 0
+
+    def forward_walk(self, op, main, method, step, lam, alw, apply_key, shadow_keys, m_array,
+                     val_out, norm_out):
+        """One forward walk of operator handle ``op`` from ``main``'s current
+        population with this engine as the shadow chain (gfmc_forward_walk);
+        writes mean values and log norms at the depths m_array into the
+        float64 device views val_out, norm_out (n_p each)."""
+        torch = self.torch
+        if getattr(self, "_fw_vals", None) is None:
+            self._fw_vals = torch.empty(self.n, dtype=torch.float64, device=self.device)
+            self._fw_vals_tmp = torch.empty_like(self._fw_vals)
+        apply_key = np.ascontiguousarray(apply_key, dtype=np.uint32)
+        sk = np.ascontiguousarray(shadow_keys, dtype=np.uint32)
+        m = np.ascontiguousarray(m_array, dtype=np.int32)
+        P = ctypes.POINTER(ctypes.c_uint32)
+        _lib.check(self.L.gfmc_forward_walk(
+            self.h, op.h, _lib.METHODS[method], float(step), float(lam if lam is not None else 0.0),
+            float(alw), apply_key.ctypes.data_as(P), sk.ctypes.data_as(P) if sk.size else None,
+            self.n, self._ptr(main.cfg), self._ptr(main.parents), int(main.parents_valid),
+            self._ptr(self.cfg), self._ptr(self.cfg_tmp), self._ptr(self.parents),
+            self._ptr(self.log_w), self._ptr(self.e_loc), self._ptr(self._fw_vals),
+            self._ptr(self._fw_vals_tmp), len(m), m.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+            self._ptr(val_out), self._ptr(norm_out), self._stream()), "gfmc_forward_walk")
+        self.parents_valid = 1
+
     def windowed_energy(self, logG, E, p_array):
         p = np.ascontiguousarray(p_array, dtype=np.int32)
         out = np.zeros(len(p), dtype=np.float64)
@@ -401,6 +435,56 @@ class GFMCEngine:
             out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), self._stream()),
             "gfmc_windowed_energy")
         return dict(zip([int(v) for v in p], out.tolist()))
+
+
+class OperatorHandle:
+    """Device tables of a measurement operator under the run's guide -- the
+    analogue of ``guide.build_cache(op)`` (engine/driver.py:1476-1477) --
+    for gfmc_apply_operator / gfmc_forward_walk / gfmc_operator_min_rate."""
+
+    def __init__(self, op, guide, precision):
+        L = _lib.load()
+        self.L = L
+        keep = _Keep()
+        md = model_desc(op, keep)
+        gd = guide_desc(guide, op, keep)
+        h = ctypes.c_void_p()
+        _lib.check(L.gfmc_create(ctypes.byref(md), ctypes.byref(gd),
+                                 {"fp64": _lib.PRECISION_FP64, "mixed": _lib.PRECISION_MIXED}[precision],
+                                 ctypes.byref(h)), "gfmc_create (operator)")
+        self.h = h
+        self.M = L.gfmc_n_transitions(h)
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None) is not None and self.h.value:
+                self.L.gfmc_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    def min_rates(self, eng, count):
+        """Smallest rate per walker of the first ``count`` walkers of
+        ``eng``'s population (host float64; NaN where a rate is not finite)."""
+        torch = eng.torch
+        out = torch.empty(eng.n, dtype=torch.float64, device=eng.device)
+        _lib.check(self.L.gfmc_operator_min_rate(self.h, eng.n, eng._ptr(eng.cfg), eng._ptr(eng.parents),
+                                                 int(eng.parents_valid), eng._ptr(out), eng._stream()),
+                   "gfmc_operator_min_rate")
+        return out[:count].cpu().numpy()
+
+    def apply(self, eng, key):
+        """apply_operator_one over ``eng``'s population: (packed successor
+        configurations, values) as device tensors."""
+        torch = eng.torch
+        cfg_out = torch.empty_like(eng.cfg)
+        vals = torch.empty(eng.n, dtype=torch.float64, device=eng.device)
+        key = np.ascontiguousarray(key, dtype=np.uint32)
+        _lib.check(self.L.gfmc_apply_operator(self.h, key.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+                                              eng.n, eng._ptr(eng.cfg), eng._ptr(eng.parents),
+                                              int(eng.parents_valid), eng._ptr(cfg_out), eng._ptr(vals),
+                                              eng._stream()), "gfmc_apply_operator")
+        return cfg_out, vals
 
 
 def _is_vector_op(op):
@@ -417,6 +501,70 @@ def key_schedule(key, n_steps):
     P = ctypes.POINTER(ctypes.c_uint32)
     _lib.check(L.gfmc_key_schedule(key.ctypes.data_as(P), int(n_steps), out.ctypes.data_as(P),
                                    nxt.ctypes.data_as(P)), "gfmc_key_schedule")
+    return out, nxt
+
+
+_AUX_POSITIVITY = 10_001
+_POSITIVITY_PROBE_STEPS = 100
+_N_POSITIVITY_CHECK = 100
+
+
+def measurement_plan(n_steps, p_array, n_off_ops, off_diag_stride, return_raw):
+    """Window grid and off-diagonal measurement grid of one call
+    (engine/driver.py _measurement_plan:478-551).  Off-diagonal rows are
+    measured at the steps t with (t + 1) % stride == 0; without raw series
+    (return_raw False) only in the band every window can use, so every p
+    rests on the same measurements."""
+    p = list(p_array)
+    m = [v // 2 for v in p]
+    equal = not bool(return_raw)
+    p_max = p[-1] if p else 0
+    m_od = p_max // 2
+    if p_max >= n_steps:
+        raise ValueError(f"every p value must be smaller than n_steps: got n_steps={n_steps} and "
+                         f"max(p)={p_max}")
+    if n_off_ops > 0 and n_steps <= p_max + m_od:
+        raise ValueError(f"off-diagonal operators need n_steps > 1.5*max(p) (max(p) + max(p)//2 = "
+                         f"{p_max + m_od}: every window p needs p past and p//2 future steps in this "
+                         f"call), got n_steps={n_steps}")
+    gate = n_off_ops > 0 and (off_diag_stride > 1 or equal)
+    if equal and n_off_ops > 0:
+        offset = next((k for k in range(p_max, p_max + off_diag_stride)
+                       if (k + 1) % off_diag_stride == 0), p_max)
+        if not any((k + 1) % off_diag_stride == 0 for k in range(p_max, n_steps - m_od)):
+            raise ValueError(
+                f"equal off-diagonal windows (return_raw=False) measure only the steps "
+                f"{p_max}..{n_steps - m_od - 1} (n_steps={n_steps} minus the lead-in max(p)={p_max} "
+                f"and the tail max(p)//2={m_od}), and none of them is a multiple of "
+                f"off_diag_stride={off_diag_stride} (counted from 1); raise n_steps or lower the stride")
+    else:
+        offset = off_diag_stride - 1
+    return SimpleNamespace(p_array=p, m_array=m, p_max=p_max, m_max=max(m) if m else 0,
+                           n_off_ops=n_off_ops, off_diag_stride=off_diag_stride,
+                           equal_windows=equal, gate_off_diag=gate, off_diag_offset=offset)
+
+
+def measured_steps(n_steps, plan):
+    """The 0-based production steps that measure the off-diagonal operators
+    (engine/driver.py _measured_steps:554-564)."""
+    t = np.arange(n_steps)
+    meas = (t + 1) % plan.off_diag_stride == 0
+    if plan.equal_windows and plan.n_off_ops > 0:
+        meas &= (t >= plan.p_max) & (t <= n_steps - plan.p_max // 2 - 1)
+    return t[meas]
+
+
+def key_schedule_ex(key, n_steps, n_sub):
+    """(n_steps, n_sub, 2) sub-keys fold_in(rng_s, j) of the production key
+    recurrence and the key after n_steps (gfmc_key_schedule_ex)."""
+    L = _lib.load()
+    key = np.ascontiguousarray(_rnd.as_key(key))
+    out = np.zeros((n_steps, n_sub, 2), dtype=np.uint32)
+    nxt = np.zeros(2, dtype=np.uint32)
+    P = ctypes.POINTER(ctypes.c_uint32)
+    _lib.check(L.gfmc_key_schedule_ex(key.ctypes.data_as(P), int(n_steps), int(n_sub),
+                                      out.ctypes.data_as(P), nxt.ctypes.data_as(P)),
+               "gfmc_key_schedule_ex")
     return out, nxt
 
 
@@ -535,14 +683,22 @@ def run_gfmc(walkers, n_steps, hamiltonian, step_size, guide, p_array, *, method
     if len(p_array) != p_in:
         _emit(f"[gfmc.run_gfmc] dedup'd p_array: {p_in - len(p_array)} duplicate value(s) "
               f"dropped, using {p_array}", verbosity)
-    if off_diag_operators:
-        raise NotImplementedError(
-            "off-diagonal forward-walking operators are not built into the B200 engine yet")
+    off_names = list(off_diag_operators.keys()) if off_diag_operators else []
     diag_names = list(diag_operators.keys()) if diag_operators else []
-    m_array = [p // 2 for p in p_array]
-    if p_array[-1] >= n_steps:
-        raise ValueError(f"every p value must be smaller than n_steps: got n_steps={n_steps} and "
-                         f"max(p)={p_array[-1]}")
+    collisions = set(diag_names) & set(off_names)
+    if collisions:
+        raise ValueError(
+            f"diag_operators and off_diag_operators share name(s) {sorted(collisions)}; the returned "
+            "obs dict is keyed by name, so colliding entries would silently overwrite each other.")
+    if off_diag_operators is not None:
+        # the shadow chain is m = p // 2 steps deep (driver.py:1453-1463)
+        if any(int(op.M_total) > 1 for op in off_diag_operators.values()):
+            bad = [p for p in p_array if p % 2 != 0]
+            if bad:
+                raise ValueError("All p values must be divisible by 2 when off_diag_operators have "
+                                 f"off-diagonal elements (M_total > 1); got {bad}")
+    plan = measurement_plan(n_steps, p_array, len(off_names), off_diag_stride, return_raw)
+    m_array = plan.m_array
     if avg_log_weight is None and warmup_steps == 0:
         raise ValueError(
             "warmup_steps=0 needs an avg_log_weight: without a warm-up nothing measures it. Pass "
@@ -599,6 +755,30 @@ def run_gfmc(walkers, n_steps, hamiltonian, step_size, guide, p_array, *, method
     if not stages:
         _emit(f"[gfmc] - [run_gfmc] - no warmup (warmup_steps=0), avg_log_weight={alw:.6f}", verbosity, 8)
 
+    # ---- off-diagonal operators: device tables, shadow chain, positivity
+    #      probe on a side-stream (driver.py _positivity_probe:791-807)
+    op_handles, shadow = [], None
+    if off_names:
+        op_handles = [OperatorHandle(off_diag_operators[nm], guide, precision) for nm in off_names]
+        shadow = GFMCEngine(hamiltonian, guide, N_walker, precision=precision)
+        if max_hops_per_step is not None:
+            shadow.set_max_iters(int(max_hops_per_step))
+        shadow.copy_population_from(eng)
+        rngs = _rnd.split(_rnd.fold_in(aux_root, _AUX_POSITIVITY), _POSITIVITY_PROBE_STEPS)
+        lgp = torch.empty(_POSITIVITY_PROBE_STEPS, dtype=torch.float64, device=dev)
+        Ep = torch.empty_like(lgp)
+        shadow.steps(method, step_f, lam, alw, _warmup_keys(rngs), lgp, Ep)
+        n_check = min(_N_POSITIVITY_CHECK, N_walker)
+        for nm, oh in zip(off_names, op_handles):
+            if oh.M == 1:
+                continue
+            mins = oh.min_rates(shadow, n_check)
+            if not np.all(np.isfinite(mins) & (mins >= 0)):
+                raise ValueError(f"Operator '{nm}': negative rate detected (min = {float(np.min(mins)):.6f}). "
+                                 "All rates must be >= 0.")
+        _emit("[estimators] - [check_off_diag_operator_positivity] - all operators passed positivity "
+              f"check ({n_check} configs, {len(off_names)} operators)", verbosity, 1)
+
     # ---- diagonal forward walking: ring buffers start after the warm-up
     #      (driver.py _diag_ring_buffers:810-838, called after _warmup)
     n_p = len(p_array)
@@ -621,13 +801,50 @@ def run_gfmc(walkers, n_steps, hamiltonian, step_size, guide, p_array, *, method
     pending = []
     step0 = 0
     last_print_t, last_print_step = prod_start, 0
-    while step0 < n_steps:
-        cs = min(chunk, n_steps - step0)
-        keys, key = key_schedule(key, cs)
-        sl = slice(step0, step0 + cs)
+    meas = measured_steps(n_steps, plan) if off_names else np.zeros(0, dtype=np.int64)
+    n_meas = len(meas)
+    od_d = on_d = None
+    if off_names:
+        od_d = torch.full((n_meas, len(off_names), n_p), float("nan"), dtype=torch.float64, device=dev)
+        on_d = torch.full_like(od_d, float("nan"))
+    m_max_od = plan.m_max if off_names else 0
+    row = 0
+
+    def run_range(a, b, keys, step0):
+        """Main-chain steps step0+a .. step0+b-1 of the chunk."""
+        sl = slice(step0 + a, step0 + b)
         if diag_d is not None:
             eng.set_diag_output(diag_d[sl])
-        eng.steps(method, step_f, lam, alw, keys, logG_d[sl], E_d[sl], hops_d[sl])
+        eng.steps(method, step_f, lam, alw, keys[a:b], logG_d[sl], E_d[sl], hops_d[sl])
+
+    while step0 < n_steps:
+        cs = min(chunk, n_steps - step0)
+        keys, key_after = key_schedule(key, cs)
+        sl = slice(step0, step0 + cs)
+        if not off_names:
+            run_range(0, cs, keys, step0)
+        else:
+            # forward walks right after each measured step's reconfiguration;
+            # the shadow replays the main chain's next m_max steps' keys
+            # (driver.py:291-316): the chunk's schedule runs m_max further
+            kx, _ = key_schedule_ex(key, cs + m_max_od, 3)
+            a = 0
+            for t in meas[(meas >= step0) & (meas < step0 + cs)] - step0:
+                t = int(t)
+                run_range(a, t + 1, keys, step0)
+                a = t + 1
+                k3 = kx[t, 2]
+                ak0, ak1 = _rnd.threefry2x32(k3[0], k3[1], np.zeros(len(off_names), np.uint32),
+                                              np.arange(len(off_names), dtype=np.uint32))
+                sk = np.ascontiguousarray(kx[t + 1:t + 1 + m_max_od, :2].reshape(m_max_od, 4))
+                for i, oh in enumerate(op_handles):
+                    shadow.forward_walk(oh, eng, method, step_f, lam, alw,
+                                        np.array([ak0[i], ak1[i]], dtype=np.uint32), sk, m_array,
+                                        od_d[row, i], on_d[row, i])
+                row += 1
+            if a < cs:
+                run_range(a, cs, keys, step0)
+        key = key_after
         logG_h[sl].copy_(logG_d[sl], non_blocking=True)
         E_h[sl].copy_(E_d[sl], non_blocking=True)
         ev = torch.cuda.Event()
@@ -709,6 +926,10 @@ def run_gfmc(walkers, n_steps, hamiltonian, step_size, guide, p_array, *, method
         "parameters/verbosity": int(verbosity),
         "parameters/number_of_outputs": int(number_of_outputs),
         "parameters/off_diag_stride": int(off_diag_stride),
+        "parameters/off_diag_offset": int(plan.off_diag_offset),
+        "parameters/off_diag_equal_windows": int(bool(plan.equal_windows)),
+        "parameters/n_off_diag_operators": len(off_names),
+        "parameters/off_diag_operators": np.asarray(off_names, dtype="S64"),
         "parameters/method": np.asarray(str(method), dtype="S32"),
         "parameters/guide": np.asarray(type(guide).__name__ if guide is not None else "none", dtype="S32"),
         "parameters/hamiltonian": np.asarray(type(hamiltonian).__name__, dtype="S32"),
@@ -717,15 +938,31 @@ def run_gfmc(walkers, n_steps, hamiltonian, step_size, guide, p_array, *, method
         "parameters/rng_key": rng_key_in,
         "parameters/rng_key_next": key,
     }
-    stats.update(autocorrelation_stats(E_np, weights_np, diag_np=diag_np))
+    off_np = off_norm_np = off_steps_np = None
+    if off_names:
+        od = od_d.cpu().numpy()
+        on = on_d.cpu().numpy()
+        off_np = {nm: od[:, i].copy() for i, nm in enumerate(off_names)}
+        off_norm_np = {nm: on[:, i].copy() for i, nm in enumerate(off_names)}
+        off_steps_np = meas.astype(np.int64)
+    stats.update(autocorrelation_stats(E_np, weights_np, diag_np=diag_np, off_diag_np=off_np,
+                                       off_diag_stride=off_diag_stride))
     stats["parameters/diag_operators"] = np.asarray(diag_names, dtype="S64")
     stats["parameters/n_diag_operators"] = len(diag_names)
-    obs = diagonal_estimates(p_array, weights_np, diag_np) if diag_np else {}
+    # with both kinds measured, every window starts at i >= max(m)
+    # (engine/estimators.py:596-619)
+    m_common = max(m_array) if (diag_np and off_names) else 0
+    obs = diagonal_estimates(p_array, weights_np, diag_np, m_common) if diag_np else {}
+    if off_names:
+        obs.update(off_diagonal_estimates(p_array, m_array, weights_np, off_np, off_norm_np,
+                                          off_steps_np, m_common))
     if return_raw:
-        raw = dict(log_weights=weights_np, energy=E_np, diag=diag_np, off_diag=None,
-                   off_diag_norm=None, off_diag_steps=None, additional_diag=additional_diag_np,
+        raw = dict(log_weights=weights_np, energy=E_np, diag=diag_np, off_diag=off_np,
+                   off_diag_norm=off_norm_np, off_diag_steps=off_steps_np,
+                   additional_diag=additional_diag_np,
                    p_array=list(p_array), m_array=list(m_array),
-                   diag_operators=list(diag_names) or None, off_diag_operators=None)
+                   diag_operators=list(diag_names) or None,
+                   off_diag_operators=list(off_names) or None)
         return out_w, energy, obs, stats, raw
     return out_w, energy, obs, stats
 

@@ -9,7 +9,8 @@ progress lines (:268-305; the final estimate runs on the device),
 """
 import numpy as np
 
-__all__ = ["validated_p_array", "windowed_energy_host", "diagonal_estimates", "autocorrelation",
+__all__ = ["validated_p_array", "windowed_energy_host", "diagonal_estimates",
+           "off_diagonal_estimates", "autocorrelation",
            "autocorrelation_stats", "jackknife_energy", "evaluate_observables"]
 
 
@@ -57,6 +58,49 @@ def diagonal_estimates(p_array, log_weights, diag_by_name, m_max_common=0):
                 out[name][p] = float(np.sum(G * a[:, j][p:][m_max_common:])) / gs
             else:
                 out[name][p] = np.sum(G[:, None] * a[:, :, j][p:][m_max_common:], axis=0) / gs
+    return out
+
+
+def off_diagonal_estimates(p_array, m_array, log_weights, off_diag, off_diag_norm, off_diag_steps,
+                           m_max_common=0):
+    """Forward-walking pure estimates {name: {p: value}} of the off-diagonal
+    operators (engine/estimators.py _off_diagonal_estimates:308-355).
+
+    A row measured at main-chain step k = p + i carries the mean operator
+    value after m = p // 2 shadow steps and the shadow's log weight product;
+    with L the cumulative main-chain log weights (L[0] = 0),
+        numerator   sum_k exp(L[k+1] - L[k-m+1] + norm_k) val_k
+        denominator sum_k exp(L[k+m+1] - L[k-m+1]),
+    both shifted by one common maximum before exponentiating, over the rows
+    with p + max(0, m_max_common - m) <= k < n - m."""
+    lw = np.asarray(log_weights, dtype=np.float64)
+    n = len(lw)
+    L = np.concatenate([[0.0], np.cumsum(lw)])
+    k_all = np.asarray(off_diag_steps, dtype=np.int64)
+    names = list(off_diag)
+    vals = {nm: np.asarray(off_diag[nm], dtype=np.float64) for nm in names}
+    norms = {nm: np.asarray(off_diag_norm[nm], dtype=np.float64) for nm in names}
+    for nm in names:
+        if not (np.all(np.isfinite(vals[nm])) and np.all(np.isfinite(norms[nm]))):
+            raise ValueError("off_diag_np and off_diag_norm_np must contain only finite values.")
+    out = {nm: {} for nm in names}
+    for j, (p, m) in enumerate(zip(validated_p_array(p_array), m_array)):
+        if n - m - p <= 0:
+            raise ValueError(f"Insufficient samples for off-diagonal windows [{p}]; each requires "
+                             "n_samples > p + m.")
+        lo, hi = np.searchsorted(k_all, [p + max(0, m_max_common - m), n - m])
+        i = k_all[lo:hi] - p
+        if len(i) == 0:
+            raise ValueError(f"No stored off-diagonal measurement is usable for p={p}, m={m}.")
+        log_num = L[p + 1 + i] - L[p - m + 1 + i]
+        log_den = L[p + m + 1 + i] - L[p - m + 1 + i]
+        for nm in names:
+            lt = log_num + norms[nm][lo:hi, j]
+            fin = np.isfinite(lt)
+            shift = max(np.max(lt[fin]), np.max(log_den)) if fin.any() else np.max(log_den)
+            num = float(np.sum(np.exp(lt - shift) * vals[nm][lo:hi, j]))
+            den = float(np.sum(np.exp(log_den - shift)))
+            out[nm][p] = num / den
     return out
 
 

@@ -48,6 +48,43 @@ def engine_diag_ops(P, name):
     return {"nn": P.BoseHubbard.create(P.chain(6).edges, U=2.0, n_max=2, dtype=np.float64)}
 
 
+def oracle_off_ops(O, name):
+    """The off-diagonal operators of the golden systems as oracle models, each
+    with the case's guide built against the operator (guide.build_cache(op)):
+    [(name, op_model, op_guide)] (test_golden_outputs.py:180-193, 206-209,
+    236-237)."""
+    jas = "_jastrow_" in name
+    if name.startswith("spinhalf"):
+        e = O.chain_edges(8)
+        W = 1.0 + np.cos(np.ones(len(e)) * np.pi / 2)
+        ops = [("spsm", O.spin_half(e, J_x=2.0, J_y=2.0, J_z=0.0)),
+               ("sx", O.spin_half(e, h_x=-1.0)),
+               ("sfx", O.spin_half(e, J_x=4.0 * W, J_y=0.0 * W, J_z=0.0, N=8))]
+        return [(nm, m, O.jastrow_spin_half(8, e, 0.3, 0.05, m) if jas else O.no_guide())
+                for nm, m in ops]
+    e = O.chain_edges(6)
+    ops = [("hop", O.bose_hubbard(e, t=-1.0, n_max=2)),
+           ("pair", O.bose_hubbard(e, eta=-0.3, n_max=2))]
+    return [(nm, m, O.jastrow_bose_hubbard(6, e, 0.05, m, h=0.1, d=0.3) if jas else O.no_guide())
+            for nm, m in ops]
+
+
+def engine_off_ops(P, name):
+    """The off-diagonal operators of the golden systems for the engine
+    (test_golden_outputs.py:180-193, 206-209, 236-237)."""
+    if name.startswith("spinhalf"):
+        e = P.chain(8).edges
+        W = 1.0 + np.cos(np.ones(len(e)) * np.pi / 2)
+        return {"spsm": P.SpinHalf.create(e, J_x=2.0, J_y=2.0, J_z=0.0, sign_check=False,
+                                          dtype=np.float64),
+                "sx": P.SpinHalf.create(e, h_x=-1.0, sign_check=False, dtype=np.float64),
+                "sfx": P.SpinHalf.create(np.asarray(e, dtype=np.int32), J_x=4.0 * W, J_y=0.0 * W,
+                                         J_z=0.0, N=8, dtype=np.float64, sign_check=False)}
+    e = P.chain(6).edges
+    return {"hop": P.BoseHubbard.create(e, t=-1.0, n_max=2, sign_check=False, dtype=np.float64),
+            "pair": P.BoseHubbard.create(e, eta=-0.3, n_max=2, sign_check=False, dtype=np.float64)}
+
+
 def _crc(s):
     import zlib
     return zlib.crc32(s.encode())

@@ -45,6 +45,20 @@ def test_key_schedule_matches_the_reference_recurrence(lib, oracle):
     assert np.array_equal(nxt, [4201513499, 1131088919])
 
 
+def test_key_schedule_ex_sub_keys(lib, oracle):
+    """fold_in(rng, j) for j < n_sub per step; the (k1, k2) columns equal
+    gfmc_key_schedule's, and the measurement key is fold_in(rng, 2)."""
+    from pygfmc_b200.engine import key_schedule, key_schedule_ex
+    key = oracle.case_key("bose_none_cont_time")
+    kx, nxt = key_schedule_ex(key, 40, 3)
+    k4, nxt4 = key_schedule(key, 40)
+    assert np.array_equal(kx[:, :2].reshape(40, 4), k4) and np.array_equal(nxt, nxt4)
+    k = key.copy()
+    for s in range(40):
+        k, r = oracle.split(k, 2)
+        assert np.array_equal(kx[s, 2], oracle.fold_in(r, 2))
+
+
 def test_last_error_and_invalid_arguments(lib):
     from pygfmc_b200 import _lib
     rc = lib.gfmc_key_schedule(None, 3, None, None)

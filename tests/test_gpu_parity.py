@@ -7,7 +7,8 @@ import ctypes
 import numpy as np
 import pytest
 
-from golden_cases import CASES, engine_diag_ops, engine_system, method_of, oracle_system
+from golden_cases import (CASES, engine_diag_ops, engine_off_ops, engine_system, method_of,
+                          oracle_off_ops, oracle_system)
 
 pytestmark = pytest.mark.gpu
 
@@ -28,8 +29,18 @@ def test_engine_reproduces_golden_run(P, golden, name):
     walkers, energy, obs, stats, raw = P.run(
         w, 300, H, step, g, [2, 4], method=method, rng_key=key,
         lam=None if method == "cont_time" else lam, warmup_steps=8, verbosity=0,
-        diag_operators=engine_diag_ops(P, name))
+        diag_operators=engine_diag_ops(P, name), off_diag_operators=engine_off_ops(P, name))
     p = name + "/"
+    for on in engine_off_ops(P, name):
+        np.testing.assert_allclose(raw["off_diag"][on], golden[p + f"raw/off_diag/{on}"], rtol=1e-10,
+                                   atol=1e-12, err_msg=on)
+        np.testing.assert_allclose(raw["off_diag_norm"][on], golden[p + f"raw/off_diag_norm/{on}"],
+                                   rtol=1e-10, atol=1e-12, err_msg=on)
+    assert np.array_equal(raw["off_diag_steps"], np.arange(300))
+    for nm in list(engine_diag_ops(P, name)) + list(engine_off_ops(P, name)):
+        for pp in (2, 4):
+            np.testing.assert_allclose(obs[nm][pp], golden[p + f"obs/{nm}/{pp}"], rtol=1e-10,
+                                       atol=1e-12, err_msg=f"{nm} p={pp}")
     for dn in engine_diag_ops(P, name):
         np.testing.assert_allclose(raw["diag"][dn], golden[p + f"raw/diag/{dn}"], rtol=1e-10,
                                    atol=1e-12, err_msg=dn)

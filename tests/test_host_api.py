@@ -121,3 +121,49 @@ def test_run_validation_errors_before_any_work():
         P.run(w, 10, H, 0.1, None, [2], warmup_steps=0, rng_key=P.PRNGKey(1))
     with pytest.raises(TypeError):
         P.run(w, 10, object(), 0.1, None, [2], rng_key=P.PRNGKey(1))
+    # off-diagonal operators: name collisions, odd p, too short a run,
+    # an empty equal-window band (engine/driver.py:1444-1466, 478-551)
+    op = P.SpinHalf.create(P.chain(6).edges, J_x=2.0, J_y=2.0, sign_check=False)
+    with pytest.raises(ValueError, match="share name"):
+        P.run(w, 40, H, 0.1, None, [2], diag_operators={"a": H}, off_diag_operators={"a": op},
+              rng_key=P.PRNGKey(1))
+    with pytest.raises(ValueError, match="divisible by 2"):
+        P.run(w, 40, H, 0.1, None, [2, 3], off_diag_operators={"a": op}, rng_key=P.PRNGKey(1))
+    with pytest.raises(ValueError, match="n_steps > 1.5"):
+        P.run(w, 12, H, 0.1, None, [8], off_diag_operators={"a": op}, rng_key=P.PRNGKey(1))
+    with pytest.raises(ValueError, match="equal off-diagonal windows"):
+        P.run(w, 14, H, 0.1, None, [8], off_diag_operators={"a": op}, rng_key=P.PRNGKey(1),
+              return_raw=False, off_diag_stride=7)
+
+
+def test_measurement_plan_grid():
+    """Stride grid, equal-window band and offset (engine/driver.py:478-564)."""
+    from pygfmc_b200.engine import measured_steps, measurement_plan
+    pl = measurement_plan(100, [2, 8], 2, 1, True)
+    assert not pl.gate_off_diag and pl.off_diag_offset == 0
+    assert np.array_equal(measured_steps(100, pl), np.arange(100))
+    pl = measurement_plan(100, [2, 8], 2, 3, True)
+    assert pl.gate_off_diag and np.array_equal(measured_steps(100, pl), np.arange(2, 100, 3))
+    pl = measurement_plan(100, [2, 8], 2, 3, False)
+    assert pl.equal_windows and pl.off_diag_offset == 8
+    assert np.array_equal(measured_steps(100, pl), np.arange(8, 96, 3))
+
+
+@pytest.mark.parametrize("name", ["spinhalf_jastrow_cont_time", "bose_none_single_step",
+                                  "spinhalf_none_multi_step", "bose_jastrow_cont_time"])
+def test_estimators_reproduce_golden_observables(golden, name):
+    """The host estimators on the golden raw series give the golden obs:
+    diagonal and off-diagonal windows both restricted to i >= max(m)."""
+    from pygfmc_b200.estimators import diagonal_estimates, off_diagonal_estimates
+    p = name + "/"
+    lw = golden[p + "raw/log_weights"]
+    diag = {k.split("/")[-1]: golden[k] for k in golden.files if k.startswith(p + "raw/diag/")}
+    off = {k.split("/")[-1]: golden[k] for k in golden.files if k.startswith(p + "raw/off_diag/")}
+    norm = {nm: golden[p + f"raw/off_diag_norm/{nm}"] for nm in off}
+    assert diag and off
+    obs = diagonal_estimates([2, 4], lw, diag, 2)
+    obs.update(off_diagonal_estimates([2, 4], [1, 2], lw, off, norm, np.arange(len(lw)), 2))
+    for nm in list(diag) + list(off):
+        for pp in (2, 4):
+            np.testing.assert_allclose(obs[nm][pp], golden[p + f"obs/{nm}/{pp}"], rtol=1e-10,
+                                       atol=1e-12, err_msg=f"{nm} p={pp}")

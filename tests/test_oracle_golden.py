@@ -3,7 +3,7 @@ key chains, walker initialisers, and whole 300-step trajectories."""
 import numpy as np
 import pytest
 
-from golden_cases import CASES, method_of, oracle_system
+from golden_cases import CASES, method_of, oracle_off_ops, oracle_system
 
 
 def test_threefry_key_chain_kats(golden, oracle):
@@ -37,6 +37,33 @@ def test_oracle_reproduces_golden_run(golden, oracle, name):
     for pp in (2, 4):
         np.testing.assert_allclose(r.energy[pp], golden[p + f"energy/{pp}"], rtol=1e-10, atol=1e-12)
     assert np.array_equal(r.rng_key_next, golden[p + "stats/parameters/rng_key_next"])
+
+
+@pytest.mark.parametrize("name", [c for c in CASES if c.endswith(("cont_time", "single_step"))]
+                         + ["bose_jastrow_multi_step"])
+def test_oracle_off_diagonal_forward_walk_golden(golden, oracle, name):
+    """Forward-walking rows of every off-diagonal operator (operator applied
+    after each step's reconfiguration, shadow chain on the main chain's future
+    keys) against raw['off_diag'] / raw['off_diag_norm'] of the golden run."""
+    m, cfg, g, dt, lam = oracle_system(oracle, name)
+    method = method_of(name)
+    step = dt if method == "cont_time" else 2
+    ops = oracle_off_ops(oracle, name)
+    r = oracle.run(cfg, 300, m, step, g, [2, 4], method=method, rng_key=oracle.case_key(name),
+                   lam=None if method == "cont_time" else lam, warmup_steps=8,
+                   off_diag_operators=ops)
+    p = name + "/"
+    for nm, _, _ in ops:
+        np.testing.assert_allclose(r.off_diag[nm], golden[p + f"raw/off_diag/{nm}"],
+                                   rtol=1e-10, atol=1e-12, err_msg=nm)
+        np.testing.assert_allclose(r.off_diag_norm[nm], golden[p + f"raw/off_diag_norm/{nm}"],
+                                   rtol=1e-10, atol=1e-12, err_msg=nm)
+        # the pure estimate, windows restricted to i >= max(m) as with the
+        # diagonal operators of the same call
+        est = oracle.off_diagonal_estimates([2, 4], r.m_array, r.log_weights, r.off_diag[nm],
+                                            r.off_diag_norm[nm], np.arange(300), max(r.m_array))
+        for pp in (2, 4):
+            np.testing.assert_allclose(est[pp], golden[p + f"obs/{nm}/{pp}"], rtol=1e-10, atol=1e-12)
 
 
 def test_sample_index_edge_cases(oracle):
