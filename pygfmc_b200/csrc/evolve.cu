@@ -575,7 +575,10 @@ __device__ __forceinline__ int sample_slot(const DevModel<T> &m, const DevGuide<
 
 // 256 threads and 4 blocks per SM: 64 registers, 32 resident warps per SM
 // (a warp's shared state is ~2 KB, so registers bound the occupancy).
-template <typename T, int FAM, int FAST>
+// OPK selects the instantiation: 0 the propagators and EVALUATE, 1 the
+// measurement-operator modes APPLY and MIN_RATE (kept apart so that their
+// code does not weigh on the step kernel's register allocation).
+template <typename T, int FAM, int FAST, int OPK>
 __global__ void __launch_bounds__(256, FAM == SPIN_HALF ? 4 : 2)
 evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta_bytes) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -638,7 +641,7 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta
     int hops = 0;
     T draws = T(0);   // uniforms of 16 holds (cont/multi) or 32 sub-steps (single)
 
-    if (method == CONT_TIME) {
+    if (!OPK && method == CONT_TIME) {
       const T beta = T(a.step);
       T t = T(0);
       uint32_t it = 0;
@@ -671,7 +674,7 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta
         }
       }
       lw -= a.alw * a.step;
-    } else if (method == SINGLE_STEP) {
+    } else if (!OPK && method == SINGLE_STEP) {
       const int n_bra = (int)a.step;
       for (int sidx = 0; sidx < n_bra; ++sidx) {
         const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.M, MODE_LAM, lane);
@@ -690,7 +693,7 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta
       const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.n_off, MODE_OFF, lane);
       eloc = ev.diag - ev.total;
       lw -= a.alw * (double)n_bra;
-    } else if (method == MULTI_STEP) {
+    } else if (!OPK && method == MULTI_STEP) {
       const int n_bra = (int)a.step;
       int used = 0;
       uint32_t it = 0;
@@ -730,7 +733,7 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta
       const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.n_off, MODE_OFF, lane);
       eloc = ev.diag - ev.total;
       lw -= a.alw * (double)n_bra;
-    } else if (method == APPLY) {
+    } else if (OPK && method == APPLY) {
       // apply_operator_one:849-888: draw the successor in proportion to the
       // operator's guided rates (slot 0 the diagonal, i.e. stay); the value
       // is their sum, 0 when it is not positive; a purely diagonal operator
@@ -752,7 +755,7 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta
           eloc = total;
         }
       }
-    } else if (method == MIN_RATE) {
+    } else if (OPK && method == MIN_RATE) {
       // check_off_diag_operator_positivity (engine/estimators.py:631-681):
       // the smallest guide-transformed rate over all M_total slots, NaN when
       // one is not finite (the full evaluation gives the diagonal element)
@@ -824,9 +827,12 @@ void staging_plan(const DevModel<T> &m, const DevGuide<T> &g, int *stage_nbr, si
 template <typename T>
 using KernelFn = void (*)(DevModel<T>, DevGuide<T>, EvolveArgs, int, int);
 
-template <typename T> KernelFn<T> pick_kernel(const DevModel<T> &m) {
-  if (m.family == SPIN_HALF) return m.fast ? evolve_kernel<T, SPIN_HALF, 1> : evolve_kernel<T, SPIN_HALF, 0>;
-  return evolve_kernel<T, BOSE_HUBBARD, 0>;
+template <typename T> KernelFn<T> pick_kernel(const DevModel<T> &m, bool opk) {
+  if (m.family == SPIN_HALF) {
+    if (opk) return m.fast ? evolve_kernel<T, SPIN_HALF, 1, 1> : evolve_kernel<T, SPIN_HALF, 0, 1>;
+    return m.fast ? evolve_kernel<T, SPIN_HALF, 1, 0> : evolve_kernel<T, SPIN_HALF, 0, 0>;
+  }
+  return opk ? evolve_kernel<T, BOSE_HUBBARD, 0, 1> : evolve_kernel<T, BOSE_HUBBARD, 0, 0>;
 }
 
 }  // namespace
@@ -843,8 +849,11 @@ cudaError_t plan_evolve(const DevModel<T> &m, const DevGuide<T> &g, int n_slots_
   size_t cta;
   staging_plan(m, g, &stage_nbr, &cta);
   const size_t warp_bytes = warp_layout(m, g).bytes;
-  KernelFn<T> kern = pick_kernel(m);
+  KernelFn<T> kern = pick_kernel(m, false);
   cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+  if (err != cudaSuccess) return err;
+  err = cudaFuncSetAttribute(pick_kernel(m, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             max_smem);
   if (err != cudaSuccess) return err;
   // the warps-per-block choice with the most resident warps per SM
   int best_w = 0, best = -1;
@@ -874,7 +883,8 @@ cudaError_t launch_evolve(const DevModel<T> &m, const DevGuide<T> &g, const Laun
   int need = (a.n_walkers + plan.wpb - 1) / plan.wpb;
   if (grid > need) grid = need;
   if (grid < 1) grid = 1;
-  pick_kernel(m)<<<grid, plan.block, plan.smem, s>>>(m, g, a, stage_nbr, (int)cta);
+  pick_kernel(m, a.method >= APPLY)<<<grid, plan.block, plan.smem, s>>>(m, g, a, stage_nbr,
+                                                                        (int)cta);
   return cudaGetLastError();
 }
 
