@@ -39,6 +39,7 @@ extern "C" {
 #define GFMC_GUIDE_NONE 0
 #define GFMC_GUIDE_JASTROW_SPIN_HALF 1
 #define GFMC_GUIDE_JASTROW_BOSE_HUBBARD 2
+#define GFMC_GUIDE_RBM_SPIN_HALF 3        /* no counterpart in PyGFMC */
 
 #define GFMC_METHOD_CONT_TIME 0
 #define GFMC_METHOD_SINGLE_STEP 1
@@ -90,6 +91,12 @@ typedef struct {
   int d_mode;
   double d0;
   const double *d;
+  /* RBM (GFMC_GUIDE_RBM_SPIN_HALF; no PyGFMC counterpart): log psi(s) =
+   * sum_h log cosh(b_h + sum_i W_hi s_i) + a.s over spins s = +-1; rbm_W
+   * (n_hidden, n_sites) row-major, rounded to bfloat16 on the device;
+   * rbm_b (n_hidden), rbm_a (n_sites); n_hidden <= 1024. */
+  int n_hidden;
+  const float *rbm_W, *rbm_b, *rbm_a;
 } gfmc_guide_desc;
 
 typedef struct gfmc_handle gfmc_handle;

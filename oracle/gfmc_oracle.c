@@ -98,7 +98,51 @@ typedef struct {
   int beta_tied; double beta0;
   int h_mode;  double h0;   /* 0 none, 1 tied (h0), 2 array (h) */
   int d_mode;  double d0; const double *d;
+  /* RBM (no PyGFMC counterpart): log psi = sum_h log cosh(b_h + sum_i W_hi s_i) + a.s,
+   * W (n_hidden, N) row-major with bfloat16-representable values. */
+  int n_hidden; const double *rbm_W, *rbm_b, *rbm_a;
 } om_guide;
+
+/* Extra scratch doubles om_rates needs for a guide (theta and theta'). */
+static inline int om_guide_scratch(const om_guide *g) {
+  return (g && g->kind == 3) ? 2 * g->n_hidden : 0;
+}
+
+/* log cosh(x) - log 2, the RBM hidden-unit term (the constant cancels in
+ * every ratio). */
+static inline double om_lncosh(double x) {
+  double y = fabs(x);
+  return y + log1p(exp(-2.0 * y)) - 0.6931471805599453;
+}
+
+/* RBM: theta = b + W x (W row-major (H, N)) and sum_h lncosh(theta_h). */
+static double rbm_theta(const om_guide *g, int N, const double *x, double *theta) {
+  double lcs = 0.0;
+  for (int h = 0; h < g->n_hidden; ++h) {
+    double t = g->rbm_b[h];
+    const double *w = g->rbm_W + (size_t)h * N;
+    for (int k = 0; k < N; ++k) t += w[k] * x[k];
+    theta[h] = t;
+    lcs += om_lncosh(t);
+  }
+  return lcs;
+}
+
+/* RBM log ratio psi(x')/psi(x) for flipping site i and, when j >= 0, site j:
+ * theta'_h = theta_h - 2 x_i W_hi - 2 x_j W_hj. */
+static double rbm_log_diff(const om_guide *g, int N, const double *x, const double *theta,
+                           double lcsum, int i, int j) {
+  double s = 0.0;
+  for (int h = 0; h < g->n_hidden; ++h) {
+    const double *w = g->rbm_W + (size_t)h * N;
+    double t = theta[h] - 2.0 * x[i] * w[i];
+    if (j >= 0) t -= 2.0 * x[j] * w[j];
+    s += om_lncosh(t);
+  }
+  double d = s - lcsum - 2.0 * g->rbm_a[i] * x[i];
+  if (j >= 0) d -= 2.0 * g->rbm_a[j] * x[j];
+  return d;
+}
 
 static inline int om_M(const om_model *m) {
   if (m->kind == 0) return 1 + m->n_hx + m->n_jpm;
@@ -227,6 +271,15 @@ static void om_rates(const om_model *m, const om_guide *g, const double *x,
       for (int e = 0; e < m->n_jpm; ++e) {
         double *re = &r[1 + m->n_hx + e];
         if (*re != 0.0) *re *= exp(jsh_edge_ld(g, m, x, e));
+      }
+    } else if (g && g->kind == 3) {
+      double *theta = scratch + M;   /* om_guide_scratch doubles past the M-slot area */
+      double lcs = rbm_theta(g, m->N, x, theta);
+      for (int k = 0; k < m->n_hx; ++k)
+        if (r[1 + k] != 0.0) r[1 + k] *= exp(rbm_log_diff(g, m->N, x, theta, lcs, k, -1));
+      for (int e = 0; e < m->n_jpm; ++e) {
+        double *re = &r[1 + m->n_hx + e];
+        if (*re != 0.0) *re *= exp(rbm_log_diff(g, m->N, x, theta, lcs, m->ei[e], m->ej[e]));
       }
     }
   } else {
@@ -408,7 +461,7 @@ int om_evolve(const om_model *m, const om_guide *g, int method, double step, dou
 #pragma omp parallel
   {
     om_ws ws;
-    size_t S = (size_t)(4 * M + 2 * N + 8);
+    size_t S = (size_t)(4 * M + 2 * N + 8 + om_guide_scratch(gg));
     double *buf = (double *)malloc(sizeof(double) * S);
     ws.r = buf; ws.cdf = buf + M; ws.w = buf + 2 * M; ws.scratch = buf + 3 * M; ws.xn = NULL;
 #pragma omp for schedule(dynamic, 16)
@@ -430,7 +483,7 @@ int om_rates_batch(const om_model *m, const om_guide *g, int n_walkers, const do
                    double *rates_out) {
   int M = om_M(m), N = m->N;
   const om_guide *gg = (g && g->kind) ? g : NULL;
-  double *scratch = (double *)malloc(sizeof(double) * (size_t)(M + N + 8));
+  double *scratch = (double *)malloc(sizeof(double) * (size_t)(M + N + 8 + om_guide_scratch(gg)));
   for (int w = 0; w < n_walkers; ++w)
     om_rates(m, gg, cfg + (size_t)w * N, rates_out + (size_t)w * M, scratch);
   free(scratch);
@@ -442,7 +495,7 @@ double om_initial_alw(const om_model *m, const om_guide *g, int method, double l
                       int n_walkers, const double *cfg) {
   int M = om_M(m), N = m->N;
   const om_guide *gg = (g && g->kind) ? g : NULL;
-  double *r = (double *)malloc(sizeof(double) * (size_t)(2 * M + N + 8));
+  double *r = (double *)malloc(sizeof(double) * (size_t)(2 * M + N + 8 + om_guide_scratch(gg)));
   double s = 0.0;
   for (int w = 0; w < n_walkers; ++w) {
     om_rates(m, gg, cfg + (size_t)w * N, r, r + M);
@@ -502,7 +555,7 @@ int om_apply_operator(const om_model *m, const om_guide *g, const uint32_t key[2
                       double *cfg, double *vals) {
   int M = om_M(m), N = m->N;
   const om_guide *gg = (g && g->kind) ? g : NULL;
-  double *buf = (double *)malloc(sizeof(double) * (size_t)(3 * M + N + 8));
+  double *buf = (double *)malloc(sizeof(double) * (size_t)(3 * M + N + 8 + om_guide_scratch(gg)));
   double *r = buf, *cdf = buf + M, *scratch = buf + 2 * M;
   om_key k = {key[0], key[1]};
   for (int w = 0; w < n_walkers; ++w) {

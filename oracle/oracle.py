@@ -61,7 +61,8 @@ class _Guide(ctypes.Structure):
                 ("n_pairs", ctypes.c_int), ("pair_i", _ip), ("pair_j", _ip), ("pair_wt", _dp),
                 ("trans_pw", _dp), ("beta_tied", ctypes.c_int), ("beta0", ctypes.c_double),
                 ("h_mode", ctypes.c_int), ("h0", ctypes.c_double),
-                ("d_mode", ctypes.c_int), ("d0", ctypes.c_double), ("d", _dp)]
+                ("d_mode", ctypes.c_int), ("d0", ctypes.c_double), ("d", _dp),
+                ("n_hidden", ctypes.c_int), ("rbm_W", _dp), ("rbm_b", _dp), ("rbm_a", _dp)]
 
 
 def build():
@@ -372,6 +373,21 @@ def jastrow_spin_half(N, pairs, beta, h, model):
     s.edge_other = _p(g._arr(edge_other, np.int32), _ip)
     s.edge_J = _p(g._arr(edge_J))
     s.h = _p(g._arr(hh))
+    g.s = s
+    return g
+
+
+def rbm_spin_half(W, b, a):
+    """RBM guide (no reference counterpart): log psi = sum_h log cosh(b_h +
+    sum_i W_hi s_i) + a.s on the given (bf16-valued) parameters, float64."""
+    W = np.asarray(W, np.float64); H, N = W.shape
+    g = OracleModel()
+    s = _Guide()
+    s.kind = 3
+    s.n_hidden = H
+    s.rbm_W = _p(g._arr(W.ravel()))
+    s.rbm_b = _p(g._arr(np.broadcast_to(np.asarray(b, np.float64), (H,))))
+    s.rbm_a = _p(g._arr(np.broadcast_to(np.asarray(a, np.float64), (N,))))
     g.s = s
     return g
 

@@ -22,6 +22,7 @@ MODEL_BOSE_HUBBARD = 1
 GUIDE_NONE = 0
 GUIDE_JASTROW_SPIN_HALF = 1
 GUIDE_JASTROW_BOSE_HUBBARD = 2
+GUIDE_RBM_SPIN_HALF = 3
 METHODS = {"cont_time": 0, "single_step": 1, "multi_step": 2}
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
@@ -33,6 +34,7 @@ _dp = ctypes.POINTER(ctypes.c_double)
 _i32p = ctypes.POINTER(ctypes.c_int32)
 _u32p = ctypes.POINTER(ctypes.c_uint32)
 _vp = ctypes.c_void_p
+_fp = ctypes.POINTER(ctypes.c_float)
 
 
 class ModelDesc(ctypes.Structure):
@@ -51,7 +53,8 @@ class GuideDesc(ctypes.Structure):
                 ("pair_i", _i32p), ("pair_j", _i32p), ("pair_w", _dp), ("h", _dp),
                 ("beta_tied", ctypes.c_int), ("beta0", ctypes.c_double),
                 ("h_mode", ctypes.c_int), ("h0", ctypes.c_double),
-                ("d_mode", ctypes.c_int), ("d0", ctypes.c_double), ("d", _dp)]
+                ("d_mode", ctypes.c_int), ("d0", ctypes.c_double), ("d", _dp),
+                ("n_hidden", ctypes.c_int), ("rbm_W", _fp), ("rbm_b", _fp), ("rbm_a", _fp)]
 
 
 class DiagDesc(ctypes.Structure):

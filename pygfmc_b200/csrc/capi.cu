@@ -1,5 +1,6 @@
 // C ABI of the engine (include/gfmc_b200.h): table construction, the host
 // loop of a chunk of branching steps, and the small helpers around it.
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -11,6 +12,7 @@
 #include "../../include/gfmc_b200.h"
 #include "diag.cuh"
 #include "fw.cuh"
+#include "rbm.cuh"
 #include "engine.cuh"
 
 using namespace gfmc;
@@ -94,6 +96,12 @@ struct gfmc_handle {
   int diag_cap_n = 0, diag_slot = 0, diag_ready = 0;
   double *diag_partial = nullptr;
   double *diag_out = nullptr;
+  // RBM guide: bf16 weights (both layouts), biases; theta is the carried state
+  int rbm_on = 0;
+  RbmTables rbm{};
+  void *d_rbm = nullptr;
+  int rbm_grid = 0;
+  int state_len = 0;     // carried state values per walker (N, or Hp for the RBM)
   // off-diagonal forward walking through this handle as the shadow chain
   FwHook *fw = nullptr;              // installed for the length of one walk
   int *ctr1 = nullptr;               // work counter of single launches (apply, min rate)
@@ -102,6 +110,58 @@ struct gfmc_handle {
 };
 
 namespace {
+
+uint16_t bf16_bits(float x) {
+  uint32_t u;
+  memcpy(&u, &x, 4);
+  if ((u & 0x7F800000u) == 0x7F800000u) return (uint16_t)(u >> 16);   // inf / nan kept
+  return (uint16_t)((u + 0x7FFFu + ((u >> 16) & 1u)) >> 16);          // nearest, ties to even
+}
+
+// RBM tables: W rounded to bf16 in the site-major (N, Hp) and hidden-major
+// (Hp, N) layouts, b and a in float; the hidden axis padded with zeros to a
+// multiple of 256 (32 lanes x 8-element vector loads).
+int build_rbm(gfmc_handle *h, const gfmc_guide_desc *gd, int N) {
+  const int H = gd->n_hidden;
+  if (H < 1 || H > 1024) return fail(GFMC_ERR_INVALID, "n_hidden must be in [1, 1024], got %d", H);
+  if (!gd->rbm_W || !gd->rbm_b || !gd->rbm_a)
+    return fail(GFMC_ERR_INVALID, "RBM guide: rbm_W, rbm_b and rbm_a are required");
+  const int Hp = ((H + 255) / 256) * 256;
+  std::vector<uint16_t> WT((size_t)N * Hp, 0), W((size_t)Hp * N, 0);
+  std::vector<float> b(Hp, 0.0f), a(N);
+  for (int hh = 0; hh < H; ++hh) {
+    for (int i = 0; i < N; ++i) {
+      const float w = gd->rbm_W[(size_t)hh * N + i];
+      if (!std::isfinite(w)) return fail(GFMC_ERR_INVALID, "RBM weight (%d, %d) is not finite", hh, i);
+      const uint16_t v = bf16_bits(w);
+      WT[(size_t)i * Hp + hh] = v;
+      W[(size_t)hh * N + i] = v;
+    }
+    b[hh] = gd->rbm_b[hh];
+  }
+  for (int i = 0; i < N; ++i) a[i] = gd->rbm_a[i];
+  const size_t sWT = WT.size() * 2, sW = W.size() * 2, sb = (size_t)Hp * 4, sa = (size_t)N * 4;
+  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  const size_t oW = al(sWT), ob = oW + al(sW), oa = ob + al(sb), tot = oa + al(sa);
+  std::vector<unsigned char> host(tot, 0);
+  memcpy(host.data(), WT.data(), sWT);
+  memcpy(host.data() + oW, W.data(), sW);
+  memcpy(host.data() + ob, b.data(), sb);
+  memcpy(host.data() + oa, a.data(), sa);
+  GFMC_CUDA(cudaMalloc(&h->d_rbm, tot));
+  GFMC_CUDA(cudaMemcpy(h->d_rbm, host.data(), tot, cudaMemcpyHostToDevice));
+  unsigned char *base = (unsigned char *)h->d_rbm;
+  h->rbm.WT = (const __nv_bfloat16 *)base;
+  h->rbm.W = (const __nv_bfloat16 *)(base + oW);
+  h->rbm.b = (const float *)(base + ob);
+  h->rbm.a = (const float *)(base + oa);
+  h->rbm.H = H;
+  h->rbm.Hp = Hp;
+  h->rbm_on = 1;
+  h->carry = 1;
+  h->state_len = Hp;
+  return GFMC_OK;
+}
 
 template <typename T>
 int build_tables(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_desc *gd,
@@ -179,6 +239,11 @@ int build_tables(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_des
 
   // ---- guide
   int gk = gd ? gd->kind : GFMC_GUIDE_NONE;
+  if (gk == GFMC_GUIDE_RBM_SPIN_HALF) {
+    if (md->kind != GFMC_MODEL_SPIN_HALF)
+      return fail(GFMC_ERR_INVALID, "the RBM guide needs a SpinHalf model");
+    gk = GFMC_GUIDE_NONE;   // the Jastrow tables stay empty; rbm.cu evaluates the ratios
+  }
   if (gk == GFMC_GUIDE_JASTROW_SPIN_HALF && md->kind != GFMC_MODEL_SPIN_HALF)
     return fail(GFMC_ERR_INVALID, "JastrowSpinHalf needs the SpinHalf transition layout");
   if (gk == GFMC_GUIDE_JASTROW_BOSE_HUBBARD && md->kind != GFMC_MODEL_BOSE_HUBBARD)
@@ -406,15 +471,17 @@ int ensure_scratch(gfmc_handle *h, int n, int n_steps) {
     GFMC_CUDA(cudaMalloc(&h->hops, sizeof(unsigned long long) * n_steps));
     h->cap_steps = n_steps;
   }
-  if (!h->pmax)
-    GFMC_CUDA(cudaMalloc(&h->pmax, sizeof(double) * (size_t)(h->plan.grid > 0 ? h->plan.grid : 1) *
-                                       (h->plan.wpb > 0 ? h->plan.wpb : 1)));
+  if (!h->pmax) {
+    size_t np = (size_t)(h->plan.grid > 0 ? h->plan.grid : 1) * (h->plan.wpb > 0 ? h->plan.wpb : 1);
+    if (h->rbm_on) np = std::max(np, (size_t)rbm_partials(h->rbm_grid, h->rbm_grid * 4));
+    GFMC_CUDA(cudaMalloc(&h->pmax, sizeof(double) * np));
+  }
   if (h->carry && n > h->cap_field) {
     size_t tsz = h->precision == GFMC_PRECISION_FP64 ? sizeof(double) : sizeof(float);
     cudaFree(h->fbuf[0]); cudaFree(h->fbuf[1]);
     h->fbuf[0] = h->fbuf[1] = nullptr;
-    GFMC_CUDA(cudaMalloc(&h->fbuf[0], tsz * (size_t)n * h->N));
-    GFMC_CUDA(cudaMalloc(&h->fbuf[1], tsz * (size_t)n * h->N));
+    GFMC_CUDA(cudaMalloc(&h->fbuf[0], tsz * (size_t)n * h->state_len));
+    GFMC_CUDA(cudaMalloc(&h->fbuf[1], tsz * (size_t)n * h->state_len));
     h->cap_field = n;
     h->field_valid = 0;
   }
@@ -440,7 +507,7 @@ int run_steps_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, int 
   GFMC_CUDA(cudaMemsetAsync(h->ctr, 0, sizeof(int) * n_steps, s));
   unsigned long long *hops = hops_out ? (unsigned long long *)hops_out : h->hops;
   GFMC_CUDA(cudaMemsetAsync(hops, 0, sizeof(unsigned long long) * n_steps, s));
-  const int n_partials = evolve_partials(h->plan, n);
+  const int n_partials = h->rbm_on ? rbm_partials(h->rbm_grid, n) : evolve_partials(h->plan, n);
   void *cur = cfg, *nxt = cfg_tmp;
   for (int st = 0; st < n_steps; ++st) {
     EvolveArgs a{};
@@ -470,7 +537,8 @@ int run_steps_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, int 
       h->field_cfg = cfg;
       h->since_refresh = fresh ? 1 : h->since_refresh + 1;
     }
-    cudaError_t e = launch_evolve<T>(m, g, h->plan, a, s);
+    cudaError_t e = h->rbm_on ? launch_rbm_evolve<T>(m, h->rbm, a, h->rbm_grid, s)
+                              : launch_evolve<T>(m, g, h->plan, a, s);
     if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "evolve launch: %s", cudaGetErrorString(e));
     ReconArgs r{};
     r.n = n;
@@ -547,6 +615,8 @@ int single_launch_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, 
 
 int single_launch(gfmc_handle *h, int method, Key key, int n, const void *cfg,
                   const int32_t *parents, void *cfg_out, double *out, cudaStream_t s) {
+  if (h->rbm_on)
+    return fail(GFMC_ERR_UNSUPPORTED, "measurement operators under an RBM guide are not built");
   if (h->precision == GFMC_PRECISION_FP64)
     return single_launch_t<double>(h, h->m64, h->g64, method, key, n, cfg, parents, cfg_out, out, s);
   return single_launch_t<float>(h, h->m32, h->g32, method, key, n, cfg, parents, cfg_out, out, s);
@@ -579,7 +649,8 @@ int local_energy_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, i
   a.partial_max = nullptr;
   a.status = h->status;
   a.max_iters = 1;
-  cudaError_t e = launch_evolve<T>(m, g, h->plan, a, s);
+  cudaError_t e = h->rbm_on ? launch_rbm_evolve<T>(m, h->rbm, a, h->rbm_grid, s)
+                            : launch_evolve<T>(m, g, h->plan, a, s);
   if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "local energy launch: %s", cudaGetErrorString(e));
   return GFMC_OK;
 }
@@ -608,6 +679,17 @@ int gfmc_create(const gfmc_model_desc *model, const gfmc_guide_desc *guide, int 
     return rc;
   }
   h->M = precision == GFMC_PRECISION_FP64 ? h->m64.M : h->m32.M;
+  h->state_len = h->N;
+  if (guide && guide->kind == GFMC_GUIDE_RBM_SPIN_HALF) {
+    rc = build_rbm(h, guide, h->N);
+    if (rc == GFMC_OK)
+      h->rbm_grid = precision == GFMC_PRECISION_FP64 ? rbm_grid<double>(h->m64, h->rbm)
+                                                     : rbm_grid<float>(h->m32, h->rbm);
+    if (rc) {
+      gfmc_destroy(h);
+      return rc;
+    }
+  }
   // float32 factors drift faster under the multiplicative updates
   h->refresh_every = precision == GFMC_PRECISION_FP64 ? 100 : 50;
   *out = h;
@@ -624,6 +706,7 @@ int gfmc_destroy(gfmc_handle *h) {
   cudaFree(h->d_ops); cudaFree(h->d_diag_tables); cudaFree(h->diag.ring_parents);
   cudaFree(h->diag.ring_vals); cudaFree(h->diag_partial);
   cudaFree(h->fw_partial); cudaFree(h->fw_logG); cudaFree(h->fw_E); cudaFree(h->ctr1);
+  cudaFree(h->d_rbm);
   delete h;
   return GFMC_OK;
 }

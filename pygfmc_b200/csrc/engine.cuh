@@ -10,7 +10,7 @@ namespace gfmc {
 
 enum Family { SPIN_HALF = 0, BOSE_HUBBARD = 1 };
 enum Method { CONT_TIME = 0, SINGLE_STEP = 1, MULTI_STEP = 2, EVALUATE = 3, APPLY = 4, MIN_RATE = 5 };
-enum GuideKind { GUIDE_NONE = 0, GUIDE_JASTROW_SPIN = 1, GUIDE_JASTROW_BOSE = 2 };
+enum GuideKind { GUIDE_NONE = 0, GUIDE_JASTROW_SPIN = 1, GUIDE_JASTROW_BOSE = 2, GUIDE_RBM_SPIN = 3 };
 
 // Status bits the kernels raise (atomicOr into a device word).
 enum StatusBits {

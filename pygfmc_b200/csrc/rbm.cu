@@ -1,0 +1,480 @@
+// The GFMC step with an RBM guide: one warp per walker.
+//
+// Each lane owns HPL = Hp / 32 consecutive hidden units and keeps their
+// theta in registers.  A rate evaluation loops over the move slots (site
+// flips, then edges): for a slot with a nonzero coupling the warp loads the
+// flipped sites' weight rows W[:, i], W[:, j] (bf16, 16-byte vector loads of
+// the lane's HPL units, read-only cache), sums log cosh(theta' ) over its
+// units with theta' = theta - 2 s_i W_i - 2 s_j W_j, and reduces over the
+// warp; rate = coupling * exp(sum - sum_h log cosh(theta_h) - 2 a_i s_i -
+// 2 a_j s_j).  Zero couplings (parallel spins without J_pmpm) are skipped,
+// as the reference masks zero rates (engine/evolution.py:260).  The rates go
+// to the warp's shared-memory row; the draw scans lane chunks of it and
+// steps back off zero weights exactly as sample_index
+// (engine/evolution.py:30-59).  A move updates theta in registers with the
+// same expression the rate used, so the state and the ratios agree bit for
+// bit.  The propagators are those of the Jastrow kernel (evolve.cu), with the
+// same per-walker Threefry streams.
+//
+// Roofline: special-function bound.  Per evaluation and slot: HPL log cosh
+// per lane (two MUFU ops each in float: ex2, lg2), against 2 x 2 Hp bytes of
+// weight rows from L1/L2.
+#include <cfloat>
+
+#include "rbm.cuh"
+
+namespace gfmc {
+namespace {
+
+constexpr unsigned FULLM = 0xffffffffu;
+constexpr int RB_WARPS = 4;   // warps per block
+
+__host__ __device__ inline int rb_words(int N) { return (N + 63) / 64; }
+
+__host__ __device__ inline int rb_chunk(int n_slots) {
+  int c = (n_slots + 31) / 32;
+  if (c < 1) c = 1;
+  return c | 1;
+}
+
+enum RbMode { RB_OFF = 0, RB_LAM = 1 };
+
+template <typename T> __device__ __forceinline__ T lncosh(T x);
+// log cosh x - log 2 = |x| + log1p(exp(-2|x|)) - log 2
+template <> __device__ __forceinline__ double lncosh<double>(double x) {
+  const double y = fabs(x);
+  return y + log1p(exp(-2.0 * y)) - 0.6931471805599453;
+}
+template <> __device__ __forceinline__ float lncosh<float>(float x) {
+  const float y = fabsf(x);
+  return y + __logf(1.0f + __expf(-2.0f * y)) - 0.69314718f;
+}
+
+__device__ __forceinline__ int spin_bit(const uint64_t *bits, int k) {
+  return (int)((bits[k >> 6] >> (k & 63)) & 1ull);
+}
+
+// The lane's HPL weights of one row of WT (bf16 -> float, exact).
+template <int HPL>
+__device__ __forceinline__ void load_row(const __nv_bfloat16 *row, float (&w)[HPL]) {
+  const uint4 *p = reinterpret_cast<const uint4 *>(row);
+#pragma unroll
+  for (int c = 0; c < HPL / 8; ++c) {
+    const uint4 u = __ldg(p + c);
+    const uint32_t v[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      w[8 * c + 2 * q] = __uint_as_float(v[q] << 16);
+      w[8 * c + 2 * q + 1] = __uint_as_float(v[q] & 0xFFFF0000u);
+    }
+  }
+}
+
+// Coupling of off-diagonal slot o (site flips first, then edges) at the
+// current spins, and the flipped sites (j = -1 for a site flip).
+template <typename T>
+__device__ __forceinline__ T slot_coupling(const DevModel<T> &m, const uint64_t *bits, int o,
+                                           int *i, int *j) {
+  if (o < m.n_hx) {
+    *i = o;
+    *j = -1;
+    return m.hx_half[o];
+  }
+  const int e = o - m.n_hx;
+  const uint32_t pe = m.edge[e];
+  *i = (int)(pe & 0xFFFF);
+  *j = (int)(pe >> 16);
+  const bool anti = spin_bit(bits, *i) != spin_bit(bits, *j);
+  return m.uniform_pm ? (anti ? m.jpm0 : m.jpmpm0) : (anti ? m.jpm[e] : m.jpmpm[e]);
+}
+
+// q[0] = H_xx, q[1 + o] = guide-transformed rate of slot o.
+template <typename T, int HPL>
+__device__ void rbm_rates(const DevModel<T> &m, const RbmTables &r, const uint64_t *bits,
+                          const T (&th)[HPL], T *q, int lane) {
+  T l = T(0);
+#pragma unroll
+  for (int k = 0; k < HPL; ++k) l += lncosh<T>(th[k]);
+  const T lcs = warp_sum(l);
+  const int hoff = lane * HPL;
+  for (int o = 0; o < m.n_off; ++o) {
+    int i, j;
+    const T c = slot_coupling(m, bits, o, &i, &j);
+    T rate = c;
+    if (c != T(0)) {
+      const T si = spin_bit(bits, i) ? T(1) : T(-1);
+      float wi[HPL];
+      load_row<HPL>(r.WT + (size_t)i * r.Hp + hoff, wi);
+      T acc = T(0);
+      T d;
+      if (j >= 0) {
+        const T sj = spin_bit(bits, j) ? T(1) : T(-1);
+        float wj[HPL];
+        load_row<HPL>(r.WT + (size_t)j * r.Hp + hoff, wj);
+#pragma unroll
+        for (int k = 0; k < HPL; ++k)
+          acc += lncosh<T>(th[k] - T(2) * si * T(wi[k]) - T(2) * sj * T(wj[k]));
+        d = warp_sum(acc) - lcs - T(2) * T(r.a[i]) * si - T(2) * T(r.a[j]) * sj;
+      } else {
+#pragma unroll
+        for (int k = 0; k < HPL; ++k) acc += lncosh<T>(th[k] - T(2) * si * T(wi[k]));
+        d = warp_sum(acc) - lcs - T(2) * T(r.a[i]) * si;
+      }
+      rate = c * math_exp<T>(d);
+    }
+    if (lane == 0) q[1 + o] = rate;
+  }
+  // diagonal element: SpinHalf.diagonal_weight:291-314
+  T dg = T(0);
+  if (m.has_jz) {
+    int na = 0;
+    T jzs = T(0);
+    for (int e = lane; e < m.E; e += 32) {
+      const uint32_t pe = m.edge[e];
+      const bool anti = spin_bit(bits, (int)(pe & 0xFFFF)) != spin_bit(bits, (int)(pe >> 16));
+      if (m.uniform_jz) na += anti;
+      else jzs += anti ? -m.jz[e] / T(4) : m.jz[e] / T(4);
+    }
+    if (m.uniform_jz) dg = (m.jz[0] / T(4)) * T(m.E - 2 * warp_sum(na));
+    else dg = warp_sum(jzs);
+  }
+  if (m.has_hz) {
+    T hzs = T(0);
+    for (int k = lane; k < m.N; k += 32) hzs += m.hz[k] * (spin_bit(bits, k) ? T(1) : T(-1));
+    dg = dg + warp_sum(hzs) / T(2);
+  }
+  if (lane == 0) q[0] = dg;
+  __syncwarp();
+}
+
+// Scanned value of slot s: RB_OFF the weights -rates of the off-diagonal
+// slots; RB_LAM slot 0 = H_xx and the rates (cdf = lam - cumsum).
+template <typename T>
+__device__ __forceinline__ T slot_val(const T *q, int mode, int s) {
+  return mode == RB_LAM ? q[s] : -q[1 + s];
+}
+template <typename T>
+__device__ __forceinline__ T slot_weight(const T *q, int mode, int s, T lam) {
+  if (mode == RB_LAM) return s == 0 ? lam - q[0] : -q[s];
+  return -q[1 + s];
+}
+
+template <typename T> struct RScan {
+  T excl, end, total;
+  int C, n_slots;
+};
+
+template <typename T>
+__device__ __forceinline__ RScan<T> rbm_scan(const T *q, int n_off, int mode, int lane) {
+  RScan<T> sc;
+  sc.n_slots = mode == RB_LAM ? n_off + 1 : n_off;
+  sc.C = rb_chunk(sc.n_slots);
+  const int s0 = lane * sc.C;
+  T acc = T(0);
+  for (int j = 0; j < sc.C; ++j) {
+    const int s = s0 + j;
+    if (s < sc.n_slots) acc += slot_val(q, mode, s);
+  }
+  const T inc = warp_inclusive_scan(acc, lane);
+  T ex = __shfl_up_sync(FULLM, inc, 1);
+  if (lane == 0) ex = T(0);
+  sc.excl = ex;
+  sc.end = ex + acc;
+  const int last = sc.n_slots > 0 ? (sc.n_slots - 1) / sc.C : 0;
+  sc.total = __shfl_sync(FULLM, sc.end, last);
+  return sc;
+}
+
+// sample_index over the scanned slots: the first slot whose cdf exceeds u,
+// clamped to the last slot, stepped back to the nearest positive weight.
+template <typename T>
+__device__ __forceinline__ int rbm_pick(const T *q, const RScan<T> &sc, int mode, T lam, T u,
+                                        int lane) {
+  const int C = sc.C, n = sc.n_slots;
+  const int last = (n - 1) / C;
+  const bool lamc = mode == RB_LAM;
+  const T cend = lamc ? lam - sc.end : sc.end;
+  const unsigned bal = __ballot_sync(FULLM, lane <= last && cend > u);
+  const int L = bal ? __ffs(bal) - 1 : last;
+  int res = 0;
+  if (lane == L) {
+    const int s0 = L * C;
+    const int s1 = (s0 + C < n) ? s0 + C : n;
+    T c = sc.excl;
+    int hit = s1 - 1;
+    for (int s = s0; s < s1; ++s) {
+      c += slot_val(q, mode, s);
+      if ((lamc ? lam - c : c) > u) {
+        hit = s;
+        break;
+      }
+    }
+    res = hit;
+    for (int s = hit; s >= 0; --s)
+      if (slot_weight(q, mode, s, lam) > T(0)) {
+        res = s;
+        break;
+      }
+  }
+  return __shfl_sync(FULLM, res, L);
+}
+
+// Off-diagonal move o: theta -= 2 s_i W_i (+ 2 s_j W_j), then the flips.
+template <typename T, int HPL>
+__device__ __forceinline__ void rbm_move(const DevModel<T> &m, const RbmTables &r,
+                                         uint64_t *bits, T (&th)[HPL], int o, int lane) {
+  int i, j;
+  (void)slot_coupling(m, bits, o, &i, &j);
+  const int hoff = lane * HPL;
+  const T si = spin_bit(bits, i) ? T(1) : T(-1);
+  float wi[HPL];
+  load_row<HPL>(r.WT + (size_t)i * r.Hp + hoff, wi);
+  if (j >= 0) {
+    const T sj = spin_bit(bits, j) ? T(1) : T(-1);
+    float wj[HPL];
+    load_row<HPL>(r.WT + (size_t)j * r.Hp + hoff, wj);
+#pragma unroll
+    for (int k = 0; k < HPL; ++k) th[k] = th[k] - T(2) * si * T(wi[k]) - T(2) * sj * T(wj[k]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < HPL; ++k) th[k] = th[k] - T(2) * si * T(wi[k]);
+  }
+  __syncwarp();
+  if (lane == 0) {
+    bits[i >> 6] ^= 1ull << (i & 63);
+    if (j >= 0) bits[j >> 6] ^= 1ull << (j & 63);
+  }
+  __syncwarp();
+}
+
+template <typename T>
+__host__ __device__ inline size_t rb_warp_bytes(int N, int M) {
+  return (((size_t)rb_words(N) * 8 + (size_t)M * sizeof(T)) + 15) & ~(size_t)15;
+}
+
+template <typename T, int HPL>
+__global__ void __launch_bounds__(RB_WARPS * 32)
+rbm_evolve_kernel(DevModel<T> m, RbmTables r, EvolveArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int NW = rb_words(m.N);
+  unsigned char *wb = smem + (size_t)wib * rb_warp_bytes<T>(m.N, m.M);
+  uint64_t *bits = reinterpret_cast<uint64_t *>(wb);
+  T *q = reinterpret_cast<T *>(wb + (size_t)NW * 8);
+  const int method = a.method;
+  const T lam = T(a.lam);
+  const int hoff = lane * HPL;
+  double wmax = -DBL_MAX;
+  unsigned long long hop_acc = 0;
+
+  for (;;) {
+    int walker = 0;
+    if (lane == 0) walker = atomicAdd(a.work_ctr, 1);
+    walker = __shfl_sync(FULLM, walker, 0);
+    if (walker >= a.n_walkers) break;
+
+    // ---- load: configuration (through the parent map) and theta
+    const int src = a.parents ? a.parents[walker] : walker;
+    const uint64_t *in = reinterpret_cast<const uint64_t *>(a.cfg_in) + (size_t)src * NW;
+    for (int k = lane; k < NW; k += 32) bits[k] = in[k];
+    __syncwarp();
+    T th[HPL];
+    if (a.field_in) {
+      const T *fin = reinterpret_cast<const T *>(a.field_in) + (size_t)src * r.Hp + hoff;
+#pragma unroll
+      for (int k = 0; k < HPL; ++k) th[k] = fin[k];
+    } else {
+#pragma unroll
+      for (int k = 0; k < HPL; ++k) th[k] = T(r.b[hoff + k]);
+      for (int i = 0; i < m.N; ++i) {
+        const T si = spin_bit(bits, i) ? T(1) : T(-1);
+        float w[HPL];
+        load_row<HPL>(r.WT + (size_t)i * r.Hp + hoff, w);
+#pragma unroll
+        for (int k = 0; k < HPL; ++k) th[k] = th[k] + si * T(w[k]);
+      }
+    }
+
+    const Key kw = fold(a.key, (uint32_t)walker);
+    double lw = 0.0;
+    T eloc = T(0);
+    int hops = 0;
+    T draws = T(0);
+
+    if (method == CONT_TIME) {
+      const T beta = T(a.step);
+      T t = T(0);
+      uint32_t it = 0;
+      while (t < beta) {
+        rbm_rates<T, HPL>(m, r, bits, th, q, lane);
+        const RScan<T> sc = rbm_scan(q, m.n_off, RB_OFF, lane);
+        const T R = sc.total;
+        const T eL = q[0] - R;
+        if ((it & 15u) == 0) draws = uniform<T>(fold(kw, 2u * it + (uint32_t)lane));
+        const T U1 = __shfl_sync(FULLM, draws, (int)(2u * (it & 15u)));
+        const T psi = __shfl_sync(FULLM, draws, (int)(2u * (it & 15u) + 1u));
+        int si = 0;
+        if (R > T(0)) {
+          const T u = U1 * R, cap = next_below(R);
+          si = rbm_pick(q, sc, RB_OFF, lam, u < cap ? u : cap, lane);
+        }
+        const T tau_raw = (R > T(0)) ? -math_log1p(-psi) / R : pos_inf<T>();
+        const T rem = beta - t;
+        const T tau = tau_raw < rem ? tau_raw : rem;
+        lw = lw - (double)eL * (double)tau;
+        t = t + tau;
+        if (tau_raw < rem) {
+          rbm_move<T, HPL>(m, r, bits, th, si, lane);
+          ++hops;
+        }
+        eloc = eL;
+        if (++it >= (uint32_t)a.max_iters) {
+          if (lane == 0) atomicOr(a.status, ST_HOP_CAP);
+          break;
+        }
+      }
+      lw -= a.alw * a.step;
+    } else if (method == SINGLE_STEP) {
+      const int n_bra = (int)a.step;
+      for (int sidx = 0; sidx < n_bra; ++sidx) {
+        rbm_rates<T, HPL>(m, r, bits, th, q, lane);
+        const RScan<T> sc = rbm_scan(q, m.n_off, RB_LAM, lane);
+        const T bx = lam - sc.total;
+        if ((sidx & 31) == 0) draws = uniform<T>(fold(kw, (uint32_t)(sidx + lane)));
+        const T U = __shfl_sync(FULLM, draws, sidx & 31);
+        const T u = U * bx, cap = next_below(bx);
+        const int idx = rbm_pick(q, sc, RB_LAM, lam, u < cap ? u : cap, lane);
+        if (idx != 0) {
+          rbm_move<T, HPL>(m, r, bits, th, idx - 1, lane);
+          ++hops;
+        }
+        lw = lw + (double)math_log(bx);
+      }
+      rbm_rates<T, HPL>(m, r, bits, th, q, lane);
+      const RScan<T> sc = rbm_scan(q, m.n_off, RB_OFF, lane);
+      eloc = q[0] - sc.total;
+      lw -= a.alw * (double)n_bra;
+    } else if (method == MULTI_STEP) {
+      const int n_bra = (int)a.step;
+      int used = 0;
+      uint32_t it = 0;
+      while (used < n_bra) {
+        rbm_rates<T, HPL>(m, r, bits, th, q, lane);
+        const RScan<T> sc = rbm_scan(q, m.n_off, RB_OFF, lane);
+        const T R = sc.total;
+        const T bx = lam - q[0] + R;
+        if ((it & 15u) == 0) draws = uniform<T>(fold(kw, 2u * it + (uint32_t)lane));
+        const T U1 = __shfl_sync(FULLM, draws, (int)(2u * (it & 15u)));
+        const T psi = __shfl_sync(FULLM, draws, (int)(2u * (it & 15u) + 1u));
+        int si = 0;
+        if (R > T(0)) {
+          const T u = U1 * R, cap = next_below(R);
+          si = rbm_pick(q, sc, RB_OFF, lam, u < cap ? u : cap, lane);
+        }
+        const int remaining = n_bra - used;
+        const T hp = R / bx;
+        const bool can_hop = hp > T(0);
+        const T log_pd = can_hop ? math_log1p(-hp) : T(-1);
+        const T hold = floor(math_log1p(-psi) / log_pd) + T(1);
+        const T capk = T(remaining + 1);
+        const T hm = hold < capk ? hold : capk;
+        const int k_raw = can_hop ? (int)hm : remaining + 1;
+        const int k = k_raw < remaining ? k_raw : remaining;
+        lw = lw + (double)math_log(bx) * (double)k;
+        used += k;
+        if (k_raw <= remaining) {
+          rbm_move<T, HPL>(m, r, bits, th, si, lane);
+          ++hops;
+        }
+        if (++it >= (uint32_t)a.max_iters) {
+          if (lane == 0) atomicOr(a.status, ST_HOP_CAP);
+          break;
+        }
+      }
+      rbm_rates<T, HPL>(m, r, bits, th, q, lane);
+      const RScan<T> sc = rbm_scan(q, m.n_off, RB_OFF, lane);
+      eloc = q[0] - sc.total;
+      lw -= a.alw * (double)n_bra;
+    } else {  // EVALUATE
+      rbm_rates<T, HPL>(m, r, bits, th, q, lane);
+      const RScan<T> sc = rbm_scan(q, m.n_off, RB_OFF, lane);
+      eloc = q[0] - sc.total;
+    }
+
+    // ---- store
+    if (a.cfg_out) {
+      uint64_t *out = reinterpret_cast<uint64_t *>(a.cfg_out) + (size_t)walker * NW;
+      for (int k = lane; k < NW; k += 32) out[k] = bits[k];
+    }
+    if (a.field_out) {
+      T *fout = reinterpret_cast<T *>(a.field_out) + (size_t)walker * r.Hp + hoff;
+#pragma unroll
+      for (int k = 0; k < HPL; ++k) fout[k] = th[k];
+    }
+    if (lane == 0) {
+      if (method <= MULTI_STEP) a.log_w[walker] = lw;
+      a.e_loc[walker] = (double)eloc;
+    }
+    if (method <= MULTI_STEP) wmax = lw > wmax ? lw : wmax;
+    hop_acc += (unsigned long long)hops;
+    __syncwarp();
+  }
+  if (lane == 0) {
+    if (a.partial_max) a.partial_max[(size_t)blockIdx.x * RB_WARPS + wib] = wmax;
+    if (a.hops && hop_acc) atomicAdd(a.hops, hop_acc);
+  }
+}
+
+template <typename T>
+using RbmKernel = void (*)(DevModel<T>, RbmTables, EvolveArgs);
+
+template <typename T> RbmKernel<T> pick_rbm(int hpl) {
+  switch (hpl) {
+    case 8: return rbm_evolve_kernel<T, 8>;
+    case 16: return rbm_evolve_kernel<T, 16>;
+    case 24: return rbm_evolve_kernel<T, 24>;
+    default: return rbm_evolve_kernel<T, 32>;
+  }
+}
+
+}  // namespace
+
+template <typename T> int rbm_grid(const DevModel<T> &m, const RbmTables &r) {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const size_t smem = RB_WARPS * rb_warp_bytes<T>(m.N, m.M);
+  RbmKernel<T> k = pick_rbm<T>(rbm_hpl(r.Hp));
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, RB_WARPS * 32, smem);
+  if (per_sm < 1) per_sm = 1;
+  return sms * per_sm;
+}
+
+template <typename T>
+cudaError_t launch_rbm_evolve(const DevModel<T> &m, const RbmTables &r, const EvolveArgs &a,
+                              int grid, cudaStream_t s) {
+  const size_t smem = RB_WARPS * rb_warp_bytes<T>(m.N, m.M);
+  int need = (a.n_walkers + RB_WARPS - 1) / RB_WARPS;
+  if (grid > need) grid = need;
+  if (grid < 1) grid = 1;
+  pick_rbm<T>(rbm_hpl(r.Hp))<<<grid, RB_WARPS * 32, smem, s>>>(m, r, a);
+  return cudaGetLastError();
+}
+
+// per-warp partial maxima a launch over n walkers writes
+int rbm_partials(int grid, int n_walkers) {
+  int need = (n_walkers + RB_WARPS - 1) / RB_WARPS;
+  if (grid > need) grid = need;
+  if (grid < 1) grid = 1;
+  return grid * RB_WARPS;
+}
+
+template int rbm_grid<double>(const DevModel<double> &, const RbmTables &);
+template int rbm_grid<float>(const DevModel<float> &, const RbmTables &);
+template cudaError_t launch_rbm_evolve<double>(const DevModel<double> &, const RbmTables &,
+                                               const EvolveArgs &, int, cudaStream_t);
+template cudaError_t launch_rbm_evolve<float>(const DevModel<float> &, const RbmTables &,
+                                              const EvolveArgs &, int, cudaStream_t);
+
+}  // namespace gfmc

@@ -24,7 +24,7 @@ from . import _lib
 from . import random as _rnd
 from .hamiltonian import BoseHubbard, SpinHalf
 from .walkers import Walker
-from .wavefunction import JastrowBoseHubbard, JastrowSpinHalf
+from .wavefunction import JastrowBoseHubbard, JastrowSpinHalf, RBMSpinHalf
 from .estimators import (autocorrelation_stats, diagonal_estimates, off_diagonal_estimates,
                          validated_p_array, windowed_energy_host)
 
@@ -105,6 +105,11 @@ class _Keep:
         self.arrays.append(a)
         return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
 
+    def f32(self, a):
+        a = np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+        self.arrays.append(a)
+        return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
 
 def _is_spin_half(op):
     return all(hasattr(op, a) for a in ("n_hx_static", "n_jpm_static", "edge_i", "edge_j",
@@ -135,10 +140,10 @@ def require_guide_protocol(guide):
         raise TypeError(f"Guide {type(guide).__name__!r} must implement at least one of "
                         "log_diff_from_operator, log_diff_from_configs, or log_psi "
                         "(the guide protocol, pygfmc.Guide).")
-    if not isinstance(guide, (JastrowSpinHalf, JastrowBoseHubbard)) and \
+    if not isinstance(guide, (JastrowSpinHalf, JastrowBoseHubbard, RBMSpinHalf)) and \
             not hasattr(guide, "_gfmc_guide_desc"):
         raise TypeError(f"Guide {type(guide).__name__!r} has no device implementation in the B200 "
-                        "engine (supported: JastrowSpinHalf, JastrowBoseHubbard).")
+                        "engine (supported: JastrowSpinHalf, JastrowBoseHubbard, RBMSpinHalf).")
 
 
 def model_desc(op, keep):
@@ -246,6 +251,15 @@ def guide_desc(guide, op, keep):
                 setattr(g, name + "0", float(v))
             elif mode == 2:
                 setattr(g, name, keep.f64(v))
+        return g
+    if isinstance(guide, RBMSpinHalf):
+        if not _is_spin_half(op):
+            raise TypeError(f"RBMSpinHalf needs a SpinHalf operator; got {type(op).__name__}")
+        if guide.N != int(op.N):
+            raise ValueError(f"RBMSpinHalf has {guide.N} visible units for {int(op.N)} sites")
+        g.kind = _lib.GUIDE_RBM_SPIN_HALF
+        g.n_hidden = guide.n_hidden
+        g.rbm_W, g.rbm_b, g.rbm_a = keep.f32(guide.W), keep.f32(guide.b), keep.f32(guide.a)
         return g
     raise TypeError(f"Guide {type(guide).__name__!r} has no device implementation")
 

@@ -14,7 +14,7 @@ import numpy as np
 
 from .hamiltonian import BoseHubbard, edges_array
 
-__all__ = ["JastrowSpinHalf", "JastrowBoseHubbard"]
+__all__ = ["JastrowSpinHalf", "JastrowBoseHubbard", "RBMSpinHalf", "round_bf16"]
 
 LAYOUT_ATTRS = ("n_hx_static", "n_jpm_static", "edge_i", "edge_j")
 
@@ -149,3 +149,83 @@ class JastrowBoseHubbard:
 
     def build_cache(self, op):
         return None
+
+
+def round_bf16(x):
+    """Round float values to the nearest bfloat16 (ties to even); returned as
+    float32 arrays whose values are exactly representable in bf16."""
+    a = np.ascontiguousarray(np.asarray(x, dtype=np.float32))
+    u = a.view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    out = r.astype(np.uint32).view(np.float32)
+    return np.where(np.isnan(a), a, out).astype(np.float32)
+
+
+class RBMSpinHalf:
+    """Restricted Boltzmann machine guide for spin-1/2 configurations:
+
+        log psi(s) = sum_h log cosh(theta_h) + a . s,   theta = b + W s,
+
+    s in {+-1}^N, W of shape (n_hidden, N) with bfloat16 values (stored as
+    float32 arrays holding bf16-representable numbers), b (n_hidden,) and
+    a (N,) float32.  A positive-amplitude guide; PyGFMC has no counterpart
+    (its learned guides are the NetKet-trained cluster models).  The engine
+    evaluates ratios on the device from theta, updated incrementally per move
+    (theta' = theta - 2 s_i W[:, i] - 2 s_j W[:, j] for an edge flip)."""
+
+    def __init__(self, N, n_hidden, W=None, b=None, a=None, seed=0, sigma=0.01, dtype=np.float32):
+        N, H = int(N), int(n_hidden)
+        if N <= 0 or H <= 0:
+            raise ValueError("N and n_hidden must be positive")
+        if H > 1024:
+            raise ValueError(f"n_hidden={H} exceeds the engine's limit of 1024")
+        rng = np.random.default_rng(seed)
+        W = rng.normal(0.0, sigma, size=(H, N)) if W is None else np.asarray(W, dtype=np.float64)
+        if W.shape != (H, N):
+            raise ValueError(f"W must have shape ({H}, {N}), got {W.shape}")
+        b = np.zeros(H) if b is None else np.broadcast_to(np.asarray(b, dtype=np.float64), (H,))
+        a = np.zeros(N) if a is None else np.broadcast_to(np.asarray(a, dtype=np.float64), (N,))
+        self.N, self.n_hidden = N, H
+        self.dtype = np.dtype(dtype)
+        self.W = round_bf16(W)
+        self.b = np.asarray(b, dtype=np.float32).copy()
+        self.a = np.asarray(a, dtype=np.float32).copy()
+
+    def parameters(self):
+        return {"W": self.W, "b": self.b, "a": self.a}
+
+    def set_parameters(self, W=None, b=None, a=None):
+        if W is not None:
+            self.W = round_bf16(np.asarray(W).reshape(self.n_hidden, self.N))
+        if b is not None:
+            self.b = np.asarray(b, dtype=np.float32).reshape(self.n_hidden).copy()
+        if a is not None:
+            self.a = np.asarray(a, dtype=np.float32).reshape(self.N).copy()
+
+    def theta(self, config):
+        s = np.asarray(config, dtype=np.float64)
+        return s @ self.W.astype(np.float64).T + self.b.astype(np.float64)
+
+    def log_psi(self, config):
+        s = np.asarray(config, dtype=np.float64)
+        t = self.theta(s)
+        lc = np.abs(t) + np.log1p(np.exp(-2.0 * np.abs(t))) - np.log(2.0)
+        return lc.sum(-1) + s @ self.a.astype(np.float64)
+
+    def log_diff_from_configs(self, config, new_configs):
+        return self.log_psi(new_configs) - self.log_psi(config)
+
+    def log_diff_from_operator(self, config, op, cache=None):
+        """Host log-ratios in the SpinHalf rate layout (slot 0 = 0)."""
+        require_spin_half_layout(op, type(self).__name__)
+        x = np.asarray(config, dtype=np.float64)
+        M = 1 + op.n_hx_static + op.n_jpm_static
+        out = np.zeros(M)
+        for k in range(op.n_hx_static):
+            y = x.copy(); y[k] = -y[k]
+            out[1 + k] = self.log_psi(y) - self.log_psi(x)
+        for e in range(op.n_jpm_static):
+            y = x.copy(); i, j = int(op.edge_i[e]), int(op.edge_j[e])
+            y[i], y[j] = -y[i], -y[j]
+            out[1 + op.n_hx_static + e] = self.log_psi(y) - self.log_psi(x)
+        return out
