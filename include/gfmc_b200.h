@@ -53,6 +53,7 @@ extern "C" {
 #define GFMC_STATUS_HOP_CAP 1     /* a walker hit the per-step iteration cap */
 #define GFMC_STATUS_BAD_CONFIG 2  /* a configuration value outside the model's basis */
 #define GFMC_STATUS_NONFINITE 4   /* non-finite mean branch weight (extinct population) */
+#define GFMC_STATUS_TIMEOUT 8     /* a bounded wait on the tensor-core pipeline ran out */
 
 /* Model description (host arrays, float64, read during gfmc_create only).
  * SpinHalf: the stored-sign fields of hamiltonian/SpinHalf.py:101-117
@@ -196,6 +197,16 @@ int gfmc_reset_diag(gfmc_handle *h, int n_walkers, void *stream);
  * float64, the mean over walkers of each value traced m steps back; NULL
  * stops the measurement. */
 int gfmc_set_diag_output(gfmc_handle *h, double *out);
+
+/* ---- RBM guide ---------------------------------------------------------- */
+/* Hidden pre-activations theta = b + W s (float32, row-major (n_walkers, Hp))
+ * of the configurations cfg[parents[i]] (parents read when parents_valid)
+ * on the tensor cores (bf16 inputs, float32 accumulation); Hp is
+ * gfmc_rbm_hidden_padded(h) >= n_hidden (padding rows are zero).  No
+ * counterpart in PyGFMC. */
+int gfmc_rbm_theta(gfmc_handle *h, int n_walkers, const void *cfg, const int32_t *parents,
+                   int parents_valid, float *theta_out, void *stream);
+int gfmc_rbm_hidden_padded(const gfmc_handle *h);
 
 /* ---- off-diagonal observables with forward walking ---------------------- */
 /* At most this many windows per forward walk. */

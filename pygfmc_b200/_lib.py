@@ -29,6 +29,7 @@ PRECISION_MIXED = 1
 STATUS_HOP_CAP = 1
 STATUS_BAD_CONFIG = 2
 STATUS_NONFINITE = 4
+STATUS_TIMEOUT = 8
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _i32p = ctypes.POINTER(ctypes.c_int32)
@@ -98,6 +99,8 @@ SIGNATURES = {
                                          ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                          ctypes.c_int, _i32p, _vp, _vp, _vp]),
     "gfmc_operator_min_rate": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp, _vp]),
+    "gfmc_rbm_theta": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp, _vp]),
+    "gfmc_rbm_hidden_padded": (ctypes.c_int, [_vp]),
     "gfmc_reconfigure_noalloc": (ctypes.c_int, [ctypes.c_int, _vp, _vp, _u32p, _vp, _vp, _vp, _vp]),
     "gfmc_read_status": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int), _vp]),
     "gfmc_key_schedule": (ctypes.c_int, [_u32p, ctypes.c_int, _u32p, _u32p]),

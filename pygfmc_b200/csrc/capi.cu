@@ -127,7 +127,8 @@ int build_rbm(gfmc_handle *h, const gfmc_guide_desc *gd, int N) {
   if (!gd->rbm_W || !gd->rbm_b || !gd->rbm_a)
     return fail(GFMC_ERR_INVALID, "RBM guide: rbm_W, rbm_b and rbm_a are required");
   const int Hp = ((H + 255) / 256) * 256;
-  std::vector<uint16_t> WT((size_t)N * Hp, 0), W((size_t)Hp * N, 0);
+  const int Np = ((N + 63) / 64) * 64;
+  std::vector<uint16_t> WT((size_t)N * Hp, 0), W((size_t)Hp * Np, 0);
   std::vector<float> b(Hp, 0.0f), a(N);
   for (int hh = 0; hh < H; ++hh) {
     for (int i = 0; i < N; ++i) {
@@ -135,7 +136,7 @@ int build_rbm(gfmc_handle *h, const gfmc_guide_desc *gd, int N) {
       if (!std::isfinite(w)) return fail(GFMC_ERR_INVALID, "RBM weight (%d, %d) is not finite", hh, i);
       const uint16_t v = bf16_bits(w);
       WT[(size_t)i * Hp + hh] = v;
-      W[(size_t)hh * N + i] = v;
+      W[(size_t)hh * Np + i] = v;
     }
     b[hh] = gd->rbm_b[hh];
   }
@@ -157,6 +158,7 @@ int build_rbm(gfmc_handle *h, const gfmc_guide_desc *gd, int N) {
   h->rbm.a = (const float *)(base + oa);
   h->rbm.H = H;
   h->rbm.Hp = Hp;
+  h->rbm.Np = Np;
   h->rbm_on = 1;
   h->carry = 1;
   h->state_len = Hp;
@@ -531,6 +533,15 @@ int run_steps_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, int 
       const bool fresh = (st == 0 && !parents_valid) || !h->field_valid || h->field_cfg != cfg ||
                          h->since_refresh >= h->refresh_every;
       a.field_in = fresh ? nullptr : h->fbuf[h->fcur];
+      if (fresh && h->rbm_on && h->precision == GFMC_PRECISION_MIXED) {
+        // the float32 build rebuilds theta for the whole population on the
+        // tensor cores (rows indexed like cfg_in; the step reads them
+        // through the parent map)
+        cudaError_t eg = launch_rbm_theta(h->rbm, n, cur, nullptr, (h->N + 63) / 64,
+                                          (float *)h->fbuf[h->fcur], h->status, s);
+        if (eg != cudaSuccess) return fail(GFMC_ERR_CUDA, "theta GEMM: %s", cudaGetErrorString(eg));
+        a.field_in = h->fbuf[h->fcur];
+      }
       a.field_out = h->fbuf[1 - h->fcur];
       h->fcur = 1 - h->fcur;
       h->field_valid = 1;
@@ -945,6 +956,25 @@ int gfmc_key_schedule(const uint32_t key[2], int n_steps, uint32_t *keys_out, ui
   key_next[0] = k.a;
   key_next[1] = k.b;
   return GFMC_OK;
+}
+
+int gfmc_rbm_theta(gfmc_handle *h, int n, const void *cfg, const int32_t *parents,
+                   int parents_valid, float *theta_out, void *stream) {
+  if (!h || n <= 0 || !cfg || !theta_out || (parents_valid && !parents))
+    return fail(GFMC_ERR_INVALID, "gfmc_rbm_theta: bad argument");
+  if (!h->rbm_on) return fail(GFMC_ERR_INVALID, "gfmc_rbm_theta: the handle has no RBM guide");
+  if (!h->status) {
+    GFMC_CUDA(cudaMalloc(&h->status, sizeof(int)));
+    GFMC_CUDA(cudaMemset(h->status, 0, sizeof(int)));
+  }
+  cudaError_t e = launch_rbm_theta(h->rbm, n, cfg, parents_valid ? parents : nullptr,
+                                   (h->N + 63) / 64, theta_out, h->status, (cudaStream_t)stream);
+  if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "theta GEMM: %s", cudaGetErrorString(e));
+  return GFMC_OK;
+}
+
+int gfmc_rbm_hidden_padded(const gfmc_handle *h) {
+  return (h && h->rbm_on) ? h->rbm.Hp : GFMC_ERR_INVALID;
 }
 
 int gfmc_key_schedule_ex(const uint32_t key[2], int n_steps, int n_sub, uint32_t *keys_out,

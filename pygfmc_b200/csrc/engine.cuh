@@ -17,6 +17,7 @@ enum StatusBits {
   ST_HOP_CAP = 1,        // a walker hit the per-step iteration cap
   ST_BAD_CONFIG = 2,     // an occupation outside [0, n_max] (Bose-Hubbard)
   ST_NONFINITE = 4,      // non-finite population weight in reconfiguration
+  ST_TIMEOUT = 8,        // a bounded wait on the tensor-core pipeline ran out
 };
 
 // Model tables (device pointers).  Couplings follow the stored-sign

@@ -13,10 +13,11 @@ namespace gfmc {
 
 struct RbmTables {
   const __nv_bfloat16 *WT;   // (N, Hp) site-major: row i = W[:, i]
-  const __nv_bfloat16 *W;    // (Hp, N) hidden-major (the GEMM's K-major operand)
+  const __nv_bfloat16 *W;    // (Hp, Np) hidden-major, Np = N rounded up to 64 (the GEMM's
+                             // K-major operand; padding zero)
   const float *b;            // (Hp,)
   const float *a;            // (N,)
-  int H, Hp;
+  int H, Hp, Np;
 };
 
 // Hidden units per lane of the step kernel's warp (Hp / 32).
@@ -32,5 +33,11 @@ cudaError_t launch_rbm_evolve(const DevModel<T> &m, const RbmTables &r, const Ev
 template <typename T> int rbm_grid(const DevModel<T> &m, const RbmTables &r);
 // Per-warp partial maxima of log_w a launch over n_walkers writes.
 int rbm_partials(int grid, int n_walkers);
+
+// theta (float32, (n, Hp)) of the packed spin configurations cfg[parents[w]]
+// (parents nullable) on the tensor cores (rbm_gemm.cu); status bit 8 when a
+// bounded wait ran out.
+cudaError_t launch_rbm_theta(const RbmTables &r, int n, const void *cfg, const int *parents,
+                             int NW, float *theta, int *status, cudaStream_t s);
 
 }  // namespace gfmc

@@ -406,6 +406,17 @@ class GFMCEngine:
         _lib.check(self.L.gfmc_set_diag_output(self.h, self._ptr(out) if out is not None
                                                else ctypes.c_void_p(0)), "gfmc_set_diag_output")
 
+    def rbm_theta(self):
+        """theta = b + W s of the current population on the tensor cores
+        (float32 device tensor (n, Hp), Hp = n_hidden padded to 256)."""
+        Hp = self.L.gfmc_rbm_hidden_padded(self.h)
+        _lib.check(Hp if Hp < 0 else 0, "gfmc_rbm_hidden_padded")
+        out = self.torch.empty((self.n, Hp), dtype=self.torch.float32, device=self.device)
+        _lib.check(self.L.gfmc_rbm_theta(self.h, self.n, self._ptr(self.cfg), self._ptr(self.parents),
+                                         int(self.parents_valid), self._ptr(out), self._stream()),
+                   "gfmc_rbm_theta")
+        return out
+
     def copy_population_from(self, other):
         """This engine's population := other's current population (gathered
         through its parent map); weights and local energies restart."""
@@ -638,6 +649,9 @@ def _device_status_check(eng):
         raise _lib.GFMCError("a walker exceeded the per-step iteration cap (max_hops_per_step, "
                              "default 2**22 holds): the escape rate times the step size is far "
                              "too large for this model")
+    if st & _lib.STATUS_TIMEOUT:
+        raise _lib.GFMCError("a bounded wait on the tensor-core pipeline ran out (theta GEMM); "
+                             "the results of this call are not valid")
 
 
 def _weight_dtype(lw):

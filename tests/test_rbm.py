@@ -166,3 +166,31 @@ def test_rbm_mixed_run_matches_exact_energy():
                              verbosity=0, precision="mixed")
     Ej, err = P.estimators.jackknife_energy([32], raw["log_weights"], raw["energy"], 15)
     assert abs(Ej[32] / 16 - (-0.4463935)) < max(5e-3, 4 * err[32] / 16)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("N,H,n", [(16, 40, 300), (256, 512, 1024), (100, 700, 257)])
+def test_rbm_theta_gemm_on_tensor_cores(N, H, n):
+    """theta = b + W s from the tcgen05 kernel (bf16 inputs, f32 accumulation)
+    equals the float64 product of the same bf16 weights to float32 rounding;
+    padded hidden units are exactly zero; the parent map is honoured."""
+    import torch
+    P._lib.load()
+    e = P.chain(N).edges
+    Hm = P.SpinHalf.create(e, J_x=-1.0, J_y=-1.0, J_z=1.0, dtype=np.float64)
+    G = P.RBMSpinHalf(N, H, seed=N + H, sigma=0.05, b=np.linspace(-0.3, 0.3, H))
+    cfg = P.prepare_walkers_random(n, N, P.PRNGKey(H)).config
+    eng = P.GFMCEngine(Hm, G, n, precision="mixed")
+    eng.load(cfg)
+    th = eng.rbm_theta().cpu().numpy()
+    ref = G.theta(cfg)
+    assert th.shape[1] % 256 == 0 and th.shape[1] >= H
+    np.testing.assert_allclose(th[:, :H], ref, rtol=0, atol=2e-6 * np.sqrt(N))
+    assert np.all(th[:, H:] == 0.0)
+    # through a parent map
+    par = torch.as_tensor(np.random.default_rng(1).integers(0, n, n).astype(np.int32), device=eng.device)
+    eng.parents.copy_(par)
+    eng.parents_valid = 1
+    th2 = eng.rbm_theta().cpu().numpy()
+    np.testing.assert_allclose(th2[:, :H], ref[par.cpu().numpy()], rtol=0, atol=2e-6 * np.sqrt(N))
+    assert eng.status() == 0
