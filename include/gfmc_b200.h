@@ -208,6 +208,27 @@ int gfmc_rbm_theta(gfmc_handle *h, int n_walkers, const void *cfg, const int32_t
                    int parents_valid, float *theta_out, void *stream);
 int gfmc_rbm_hidden_padded(const gfmc_handle *h);
 
+/* Local-energy variance loss of the RBM guide over the walkers cfg[parents[i]]
+ * with weights omega (device float64, NULL: all 1):
+ *   L = sum omega (e_L - E)^2 / sum omega,  E = sum omega e_L / sum omega.
+ * gfmc_rbm_gradient writes dL/dW (n_hidden, n_sites), dL/db, dL/da (device
+ * float32, each nullable) and stats = (E, L) (host); the dW contraction over
+ * every walker's connected configurations runs on the tensor cores (bf16
+ * inputs, float32 accumulation).  gfmc_rbm_train_step takes one Adam step
+ * (beta1 0.9, beta2 0.999, eps 1e-8) of rate lr on float32 master parameters
+ * and writes them back to the guide rounded to bf16; stats are those before
+ * the step.  Float32 (mixed) handles, at most 256 sites.  No counterpart in
+ * PyGFMC (it trains guides by NetKet VMC). */
+int gfmc_rbm_gradient(gfmc_handle *h, int n_walkers, const void *cfg, const int32_t *parents,
+                      int parents_valid, const double *omega, float *grad_W, float *grad_b,
+                      float *grad_a, double stats[2], void *stream);
+int gfmc_rbm_train_step(gfmc_handle *h, int n_walkers, const void *cfg, const int32_t *parents,
+                        int parents_valid, const double *omega, double lr, double stats[2],
+                        void *stream);
+/* The guide's current parameters (host float32: W (n_hidden, n_sites) as
+ * used, i.e. bf16 values; b; a). */
+int gfmc_rbm_get_params(gfmc_handle *h, float *W, float *b, float *a);
+
 /* ---- off-diagonal observables with forward walking ---------------------- */
 /* At most this many windows per forward walk. */
 #define GFMC_FW_MAX_P 16

@@ -5,7 +5,7 @@ step_size, guide, p_array, *, method, rng_key, lam, warmup_steps, ...)`` with
 PyGFMC's SpinHalf / BoseHubbard Hamiltonians and Jastrow guides, executed by
 hand-written CUDA kernels behind a C ABI (``include/gfmc_b200.h``).
 """
-from . import hamiltonian, random, walkers, wavefunction
+from . import hamiltonian, learn, random, walkers, wavefunction
 from .engine import GFMCEngine, run, run_gfmc
 from .estimators import evaluate_observables
 from .hamiltonian import BoseHubbard, SpinHalf, chain, kagome, square

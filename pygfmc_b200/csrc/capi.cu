@@ -102,6 +102,15 @@ struct gfmc_handle {
   void *d_rbm = nullptr;
   int rbm_grid = 0;
   int state_len = 0;     // carried state values per walker (N, or Hp for the RBM)
+  // RBM variance-minimisation scratch (sized for train_cap walkers) and the
+  // float32 master parameters with their Adam moments
+  int train_cap = 0;
+  uint64_t *tr_cfg = nullptr;
+  float *tr_theta = nullptr, *tr_rates = nullptr, *tr_rsum = nullptr, *tr_gw = nullptr;
+  double *tr_e = nullptr, *tr_stats = nullptr;
+  float *tr_gW = nullptr, *tr_gb = nullptr, *tr_ga = nullptr;
+  float *ms_W = nullptr, *ms_b = nullptr, *ms_a = nullptr, *ad_m = nullptr, *ad_v = nullptr;
+  int adam_step = 0;
   // off-diagonal forward walking through this handle as the shadow chain
   FwHook *fw = nullptr;              // installed for the length of one walk
   int *ctr1 = nullptr;               // work counter of single launches (apply, min rate)
@@ -641,6 +650,93 @@ int check_method(int method, double step) {
   return GFMC_OK;
 }
 
+// The variance-loss gradient of the RBM guide over the population
+// cfg[parents[i]] (float32 build): gather, theta on the tensor cores, the
+// EVALUATE pass with per-slot rates, coefficients, the fused gradient kernel.
+// Leaves grad_W (Hp, Np), grad_b, grad_a and (E, var) in the handle's scratch.
+int rbm_gradient_t(gfmc_handle *h, int n, const void *cfg, const int32_t *parents,
+                   int parents_valid, const double *omega, cudaStream_t s) {
+  const RbmTables &r = h->rbm;
+  const int NW = (h->N + 63) / 64, n_off = h->M - 1;
+  if (h->precision != GFMC_PRECISION_MIXED)
+    return fail(GFMC_ERR_UNSUPPORTED, "RBM training runs in the float32 (mixed) build");
+  if (r.Np > 256) return fail(GFMC_ERR_UNSUPPORTED, "RBM training supports at most 256 sites");
+  if (n > h->train_cap) {
+    cudaFree(h->tr_cfg); cudaFree(h->tr_theta); cudaFree(h->tr_rates); cudaFree(h->tr_rsum);
+    cudaFree(h->tr_gw); cudaFree(h->tr_e);
+    h->tr_cfg = nullptr; h->tr_theta = h->tr_rates = h->tr_rsum = h->tr_gw = nullptr;
+    h->tr_e = nullptr;
+    h->train_cap = 0;
+    GFMC_CUDA(cudaMalloc(&h->tr_cfg, sizeof(uint64_t) * (size_t)n * NW));
+    GFMC_CUDA(cudaMalloc(&h->tr_theta, sizeof(float) * (size_t)n * r.Hp));
+    GFMC_CUDA(cudaMalloc(&h->tr_rates, sizeof(float) * (size_t)n * (n_off > 0 ? n_off : 1)));
+    GFMC_CUDA(cudaMalloc(&h->tr_rsum, sizeof(float) * (size_t)n));
+    GFMC_CUDA(cudaMalloc(&h->tr_gw, sizeof(float) * (size_t)n));
+    GFMC_CUDA(cudaMalloc(&h->tr_e, sizeof(double) * (size_t)n));
+    h->train_cap = n;
+  }
+  if (!h->tr_stats) {
+    GFMC_CUDA(cudaMalloc(&h->tr_stats, sizeof(double) * 2));
+    GFMC_CUDA(cudaMalloc(&h->tr_gW, sizeof(float) * (size_t)r.Hp * r.Np));
+    GFMC_CUDA(cudaMalloc(&h->tr_gb, sizeof(float) * (size_t)r.Hp));
+    GFMC_CUDA(cudaMalloc(&h->tr_ga, sizeof(float) * (size_t)r.Np));
+  }
+  if (!h->ctr1) GFMC_CUDA(cudaMalloc(&h->ctr1, sizeof(int)));
+  if (!h->status) {
+    GFMC_CUDA(cudaMalloc(&h->status, sizeof(int)));
+    GFMC_CUDA(cudaMemset(h->status, 0, sizeof(int)));
+  }
+  cudaError_t e = launch_gather(n, h->cfg_bytes, parents_valid ? parents : nullptr, cfg, h->tr_cfg,
+                                nullptr, nullptr, nullptr, s);
+  if (e == cudaSuccess) e = launch_rbm_theta(r, n, h->tr_cfg, nullptr, NW, h->tr_theta, h->status, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->ctr1, 0, sizeof(int), s);
+  if (e == cudaSuccess) {
+    EvolveArgs a{};
+    a.method = EVALUATE;
+    a.n_walkers = n;
+    a.cfg_in = h->tr_cfg;
+    a.e_loc = h->tr_e;
+    a.work_ctr = h->ctr1;
+    a.status = h->status;
+    a.max_iters = 1;
+    a.field_in = h->tr_theta;
+    a.rates_out = h->tr_rates;
+    a.rsum_out = h->tr_rsum;
+    e = launch_rbm_evolve<float>(h->m32, r, a, h->rbm_grid, s);
+  }
+  if (e == cudaSuccess) e = launch_train_coeff(n, h->tr_e, omega, h->tr_gw, h->tr_stats, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->tr_gW, 0, sizeof(float) * (size_t)r.Hp * r.Np, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->tr_gb, 0, sizeof(float) * (size_t)r.Hp, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->tr_ga, 0, sizeof(float) * (size_t)r.Np, s);
+  if (e == cudaSuccess) {
+    GradArgs g{};
+    g.cfg = h->tr_cfg;
+    g.NW = NW;
+    g.n = n;
+    g.N = h->N;
+    g.Np = r.Np;
+    g.Hp = r.Hp;
+    g.n_off = n_off;
+    g.n_hx = h->m32.n_hx;
+    g.edge = h->m32.edge;
+    g.WT = r.WT;
+    g.theta = h->tr_theta;
+    g.rates = h->tr_rates;
+    g.rsum = h->tr_rsum;
+    g.gw = h->tr_gw;
+    g.grad_W = h->tr_gW;
+    g.grad_b = h->tr_gb;
+    g.grad_a = h->tr_ga;
+    g.status = h->status;
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    e = launch_rbm_grad(g, sms, s);
+  }
+  if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "RBM gradient: %s", cudaGetErrorString(e));
+  return GFMC_OK;
+}
+
 template <typename T>
 int local_energy_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, int n,
                    const void *cfg, const int32_t *parents, double *e_loc, cudaStream_t s) {
@@ -718,6 +814,10 @@ int gfmc_destroy(gfmc_handle *h) {
   cudaFree(h->diag.ring_vals); cudaFree(h->diag_partial);
   cudaFree(h->fw_partial); cudaFree(h->fw_logG); cudaFree(h->fw_E); cudaFree(h->ctr1);
   cudaFree(h->d_rbm);
+  cudaFree(h->tr_cfg); cudaFree(h->tr_theta); cudaFree(h->tr_rates); cudaFree(h->tr_rsum);
+  cudaFree(h->tr_gw); cudaFree(h->tr_e); cudaFree(h->tr_stats); cudaFree(h->tr_gW);
+  cudaFree(h->tr_gb); cudaFree(h->tr_ga); cudaFree(h->ms_W); cudaFree(h->ms_b); cudaFree(h->ms_a);
+  cudaFree(h->ad_m); cudaFree(h->ad_v);
   delete h;
   return GFMC_OK;
 }
@@ -970,6 +1070,79 @@ int gfmc_rbm_theta(gfmc_handle *h, int n, const void *cfg, const int32_t *parent
   cudaError_t e = launch_rbm_theta(h->rbm, n, cfg, parents_valid ? parents : nullptr,
                                    (h->N + 63) / 64, theta_out, h->status, (cudaStream_t)stream);
   if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "theta GEMM: %s", cudaGetErrorString(e));
+  return GFMC_OK;
+}
+
+int gfmc_rbm_gradient(gfmc_handle *h, int n, const void *cfg, const int32_t *parents,
+                      int parents_valid, const double *omega, float *grad_W, float *grad_b,
+                      float *grad_a, double stats[2], void *stream) {
+  if (!h || n <= 0 || !cfg || !stats || (parents_valid && !parents))
+    return fail(GFMC_ERR_INVALID, "gfmc_rbm_gradient: bad argument");
+  if (!h->rbm_on) return fail(GFMC_ERR_INVALID, "gfmc_rbm_gradient: the handle has no RBM guide");
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc = rbm_gradient_t(h, n, cfg, parents, parents_valid, omega, s);
+  if (rc) return rc;
+  const RbmTables &r = h->rbm;
+  if (grad_W)
+    GFMC_CUDA(cudaMemcpy2DAsync(grad_W, sizeof(float) * h->N, h->tr_gW, sizeof(float) * r.Np,
+                                sizeof(float) * h->N, r.H, cudaMemcpyDeviceToDevice, s));
+  if (grad_b)
+    GFMC_CUDA(cudaMemcpyAsync(grad_b, h->tr_gb, sizeof(float) * r.H, cudaMemcpyDeviceToDevice, s));
+  if (grad_a)
+    GFMC_CUDA(cudaMemcpyAsync(grad_a, h->tr_ga, sizeof(float) * h->N, cudaMemcpyDeviceToDevice, s));
+  GFMC_CUDA(cudaMemcpyAsync(stats, h->tr_stats, sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
+  GFMC_CUDA(cudaStreamSynchronize(s));
+  return GFMC_OK;
+}
+
+int gfmc_rbm_train_step(gfmc_handle *h, int n, const void *cfg, const int32_t *parents,
+                        int parents_valid, const double *omega, double lr, double stats[2],
+                        void *stream) {
+  if (!h || n <= 0 || !cfg || !stats || (parents_valid && !parents) || !(lr > 0.0))
+    return fail(GFMC_ERR_INVALID, "gfmc_rbm_train_step: bad argument");
+  if (!h->rbm_on) return fail(GFMC_ERR_INVALID, "gfmc_rbm_train_step: the handle has no RBM guide");
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc = rbm_gradient_t(h, n, cfg, parents, parents_valid, omega, s);
+  if (rc) return rc;
+  RbmTables &r = h->rbm;
+  const size_t P = (size_t)r.H * h->N + r.H + h->N;
+  if (!h->ms_W) {
+    GFMC_CUDA(cudaMalloc(&h->ms_W, sizeof(float) * (size_t)r.H * h->N));
+    GFMC_CUDA(cudaMalloc(&h->ms_b, sizeof(float) * r.H));
+    GFMC_CUDA(cudaMalloc(&h->ms_a, sizeof(float) * h->N));
+    GFMC_CUDA(cudaMalloc(&h->ad_m, sizeof(float) * P));
+    GFMC_CUDA(cudaMalloc(&h->ad_v, sizeof(float) * P));
+    GFMC_CUDA(cudaMemsetAsync(h->ad_m, 0, sizeof(float) * P, s));
+    GFMC_CUDA(cudaMemsetAsync(h->ad_v, 0, sizeof(float) * P, s));
+    cudaError_t e = launch_rbm_master_init(r, h->N, h->ms_W, h->ms_b, h->ms_a, s);
+    if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "master init: %s", cudaGetErrorString(e));
+    h->adam_step = 0;
+  }
+  h->adam_step += 1;
+  cudaError_t e = launch_adam(r.H, h->N, r.Hp, r.Np, h->ms_W, h->ms_b, h->ms_a, h->tr_gW, h->tr_gb,
+                              h->tr_ga, h->ad_m, h->ad_v, (float)lr, 0.9f, 0.999f, 1e-8f,
+                              h->adam_step, (__nv_bfloat16 *)r.WT, (__nv_bfloat16 *)r.W,
+                              (float *)r.b, (float *)r.a, s);
+  if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "Adam step: %s", cudaGetErrorString(e));
+  // the guide changed: carried theta is stale
+  h->field_valid = 0;
+  GFMC_CUDA(cudaMemcpyAsync(stats, h->tr_stats, sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
+  GFMC_CUDA(cudaStreamSynchronize(s));
+  return GFMC_OK;
+}
+
+int gfmc_rbm_get_params(gfmc_handle *h, float *W, float *b, float *a) {
+  if (!h || !h->rbm_on || !W || !b || !a) return fail(GFMC_ERR_INVALID, "gfmc_rbm_get_params: bad argument");
+  const RbmTables &r = h->rbm;
+  std::vector<uint16_t> Wt((size_t)r.Hp * r.Np);
+  GFMC_CUDA(cudaMemcpy(Wt.data(), r.W, Wt.size() * 2, cudaMemcpyDeviceToHost));
+  for (int hh = 0; hh < r.H; ++hh)
+    for (int i = 0; i < h->N; ++i) {
+      const uint32_t u = (uint32_t)Wt[(size_t)hh * r.Np + i] << 16;
+      memcpy(&W[(size_t)hh * h->N + i], &u, 4);
+    }
+  GFMC_CUDA(cudaMemcpy(b, r.b, sizeof(float) * r.H, cudaMemcpyDeviceToHost));
+  GFMC_CUDA(cudaMemcpy(a, r.a, sizeof(float) * h->N, cudaMemcpyDeviceToHost));
   return GFMC_OK;
 }
 

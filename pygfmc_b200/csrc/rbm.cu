@@ -399,6 +399,10 @@ rbm_evolve_kernel(DevModel<T> m, RbmTables r, EvolveArgs a) {
       rbm_rates<T, HPL>(m, r, bits, th, q, lane);
       const RScan<T> sc = rbm_scan(q, m.n_off, RB_OFF, lane);
       eloc = q[0] - sc.total;
+      if (a.rates_out)
+        for (int o = lane; o < m.n_off; o += 32)
+          a.rates_out[(size_t)walker * m.n_off + o] = (float)q[1 + o];
+      if (a.rsum_out && lane == 0) a.rsum_out[walker] = (float)(-sc.total);
     }
 
     // ---- store

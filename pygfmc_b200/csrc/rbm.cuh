@@ -40,4 +40,39 @@ int rbm_partials(int grid, int n_walkers);
 cudaError_t launch_rbm_theta(const RbmTables &r, int n, const void *cfg, const int *parents,
                              int NW, float *theta, int *status, cudaStream_t s);
 
+// Arguments of the gradient kernel of the variance loss (rbm_train.cu); the
+// population is gathered (cfg row w is walker w), theta / rates / rsum come
+// from the tensor-core GEMM and the EVALUATE pass, gw from launch_train_coeff.
+struct GradArgs {
+  const uint64_t *cfg;       // (n, NW) population (already gathered)
+  int NW, n, N, Np, Hp, n_off, n_hx;
+  const uint32_t *edge;      // (E,) packed sites
+  const __nv_bfloat16 *WT;   // (N, Hp)
+  const float *theta;        // (n, Hp)
+  const float *rates;        // (n, n_off)
+  const float *rsum;         // (n,)
+  const float *gw;           // (n,)
+  float *grad_W;             // (Hp, Np)
+  float *grad_b;             // (Hp,)
+  float *grad_a;             // (Np,)
+  int walkers_per_cta;
+  int *status;
+};
+
+// Gradient of the variance loss into grad_W (Hp, Np), grad_b (Hp), grad_a
+// (Np) (accumulated: zero them first).  Np <= 256.
+cudaError_t launch_rbm_grad(const GradArgs &a, int sms, cudaStream_t s);
+// gw[w] = 2 omega_w (e_w - E) / sum omega; stats = (E, variance) (device).
+cudaError_t launch_train_coeff(int n, const double *e, const double *omega, float *gw,
+                               double *stats, cudaStream_t s);
+// One Adam step (bias corrections of step `step`) on the float32 master
+// parameters, writing the guide's bf16 / float tables.
+cudaError_t launch_adam(int H, int N, int Hp, int Np, float *W, float *b, float *a, const float *gW,
+                        const float *gb, const float *ga, float *m, float *v, float lr, float b1,
+                        float b2, float eps, int step, __nv_bfloat16 *WT_t, __nv_bfloat16 *W_t,
+                        float *b_t, float *a_t, cudaStream_t s);
+// Float32 master parameters (W (H, N), b, a) from the guide's tables.
+cudaError_t launch_rbm_master_init(const RbmTables &r, int N, float *W, float *b, float *a,
+                                   cudaStream_t s);
+
 }  // namespace gfmc

@@ -53,6 +53,16 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
   return false;
 }
 
+// CTA-uniform bounded wait: thread 0 waits, every thread gets its verdict
+// (so all threads leave or stay in the loops together).
+__device__ __forceinline__ bool cta_wait(uint64_t *bar, uint32_t parity, volatile int *flag) {
+  if (threadIdx.x == 0) *flag = mbar_wait(bar, parity) ? 1 : 0;
+  __syncthreads();
+  const bool r = *flag != 0;
+  __syncthreads();
+  return r;
+}
+
 // Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
 // 1024 bytes apart (SBO), version 1 (sm_100).
 __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
@@ -114,6 +124,7 @@ rbm_theta_kernel(const uint64_t *cfg, const int *parents, int NW, int n, int Np,
   unsigned char *B = base + GT * 128;            // up to 512 x 64 bf16 = 64 KB
   uint64_t *bar = reinterpret_cast<uint64_t *>(B + MAXN * 128);
   uint32_t *slot = reinterpret_cast<uint32_t *>(bar + 1);
+  volatile int *flag = reinterpret_cast<volatile int *>(slot + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int ncols = Hp < MAXN ? Hp : MAXN;       // 256 or 512 (a power of two)
 
@@ -182,12 +193,11 @@ rbm_theta_kernel(const uint64_t *cfg, const int *parents, int NW, int n, int Np,
         mma_commit(bar);
       }
       // the tiles may be overwritten once the MMAs have read them
-      if (!mbar_wait(bar, phase)) {
+      if (!cta_wait(bar, phase, flag)) {
         if (tid == 0) atomicOr(status, 8);
         ok = false;
       }
       phase ^= 1u;
-      __syncthreads();
     }
     if (!ok) break;
     // epilogue: warp owns TMEM lanes 32 warp .. 32 warp + 31

@@ -417,6 +417,44 @@ class GFMCEngine:
                    "gfmc_rbm_theta")
         return out
 
+    def rbm_gradient(self, omega=None):
+        """Variance-loss gradient of the RBM guide over the current population:
+        (dW (H, N), db (H,), da (N,)) float32 device tensors and (E, var)."""
+        torch = self.torch
+        g = self.guide
+        gW = torch.empty((g.n_hidden, self.N), dtype=torch.float32, device=self.device)
+        gb = torch.empty(g.n_hidden, dtype=torch.float32, device=self.device)
+        ga = torch.empty(self.N, dtype=torch.float32, device=self.device)
+        st = np.zeros(2, dtype=np.float64)
+        om = self._ptr(omega) if omega is not None else ctypes.c_void_p(0)
+        _lib.check(self.L.gfmc_rbm_gradient(
+            self.h, self.n, self._ptr(self.cfg), self._ptr(self.parents), int(self.parents_valid), om,
+            self._ptr(gW), self._ptr(gb), self._ptr(ga),
+            st.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), self._stream()), "gfmc_rbm_gradient")
+        return gW, gb, ga, (float(st[0]), float(st[1]))
+
+    def rbm_train_step(self, lr, omega=None):
+        """One Adam step of the RBM guide on the current population; returns
+        (E, var) of the population before the step."""
+        st = np.zeros(2, dtype=np.float64)
+        om = self._ptr(omega) if omega is not None else ctypes.c_void_p(0)
+        _lib.check(self.L.gfmc_rbm_train_step(
+            self.h, self.n, self._ptr(self.cfg), self._ptr(self.parents), int(self.parents_valid), om,
+            float(lr), st.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), self._stream()),
+            "gfmc_rbm_train_step")
+        return float(st[0]), float(st[1])
+
+    def rbm_parameters(self):
+        """The guide's current (W, b, a) as host float32 arrays."""
+        g = self.guide
+        W = np.zeros((g.n_hidden, self.N), dtype=np.float32)
+        b = np.zeros(g.n_hidden, dtype=np.float32)
+        a = np.zeros(self.N, dtype=np.float32)
+        P = ctypes.POINTER(ctypes.c_float)
+        _lib.check(self.L.gfmc_rbm_get_params(self.h, W.ctypes.data_as(P), b.ctypes.data_as(P),
+                                              a.ctypes.data_as(P)), "gfmc_rbm_get_params")
+        return W, b, a
+
     def copy_population_from(self, other):
         """This engine's population := other's current population (gathered
         through its parent map); weights and local energies restart."""

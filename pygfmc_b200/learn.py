@@ -1,0 +1,77 @@
+"""Training the RBM guide on the walkers of a GFMC run (no PyGFMC
+counterpart; PyGFMC trains its learned guides by NetKet VMC).
+
+``train_rbm_guide`` alternates GFMC steps under the current guide with Adam
+steps on the local-energy variance of the current population, so the guide
+is fitted on the mixed distribution the GFMC run itself samples.  Every step
+runs on the device: the branching steps in the RBM step kernel, theta on the
+tensor cores, the loss gradient in the fused tanh + tcgen05 kernel
+(``gfmc_rbm_train_step``)."""
+import math
+import time
+
+import numpy as np
+
+from . import random as _rnd
+from .engine import GFMCEngine, _device_status_check, _emit, key_schedule
+from .wavefunction import RBMSpinHalf
+
+__all__ = ["train_rbm_guide"]
+
+
+def train_rbm_guide(walkers, hamiltonian, guide, *, n_iterations=200, steps_per_iteration=5,
+                    step_size=0.05, method="cont_time", lam=None, rng_key=None, lr=3e-3,
+                    warmup_steps=100, verbosity=1):
+    """Variance-minimisation training of an ``RBMSpinHalf`` guide.
+
+    Returns ``(trained_guide, history)``: a new ``RBMSpinHalf`` with the
+    trained (bf16-valued) parameters, and a dict of per-iteration arrays
+    ``energy`` (population mean local energy), ``variance`` (the loss) and
+    the total ``seconds``.  The walkers are evolved in the float32 build;
+    ``walkers.config`` is the starting population."""
+    if not isinstance(guide, RBMSpinHalf):
+        raise TypeError("train_rbm_guide needs an RBMSpinHalf guide")
+    n_iterations = int(n_iterations)
+    steps_per_iteration = int(steps_per_iteration)
+    if n_iterations < 1 or steps_per_iteration < 1:
+        raise ValueError("n_iterations and steps_per_iteration must be positive")
+    if not lr > 0:
+        raise ValueError("lr must be positive")
+    if method != "cont_time" and lam is None:
+        raise ValueError(f"method={method!r} needs the GFMC shift lam")
+    config = np.asarray(walkers.config)
+    n = config.shape[0]
+    key = _rnd.as_key(rng_key if rng_key is not None else _rnd.PRNGKey(0))
+    t0 = time.time()
+    eng = GFMCEngine(hamiltonian, guide, n, precision="mixed")
+    eng.load(config)
+    torch = eng.torch
+    e = eng.local_energy().cpu().numpy()
+    alw = float(np.mean(-e)) if method == "cont_time" else float(np.mean(np.log(lam - e)))
+    lg = torch.empty(max(warmup_steps, steps_per_iteration, 1), dtype=torch.float64,
+                     device=eng.device)
+    E = torch.empty_like(lg)
+    if warmup_steps > 0:
+        keys, key = key_schedule(key, warmup_steps)
+        eng.steps(method, step_size, lam, alw, keys, lg[:warmup_steps], E[:warmup_steps])
+    hist_e, hist_v = [], []
+    for it in range(n_iterations):
+        keys, key = key_schedule(key, steps_per_iteration)
+        eng.steps(method, step_size, lam, alw, keys, lg[:steps_per_iteration],
+                  E[:steps_per_iteration])
+        em, var = eng.rbm_train_step(lr)
+        hist_e.append(em)
+        hist_v.append(var)
+        if not (math.isfinite(em) and math.isfinite(var)):
+            raise ValueError(f"training diverged at iteration {it}: E={em}, var={var}")
+        if verbosity >= 2 or (verbosity >= 1 and (it % max(1, n_iterations // 10) == 0
+                                                  or it == n_iterations - 1)):
+            _emit(f"[learn] - [train_rbm_guide] - iteration {it + 1}/{n_iterations}: "
+                  f"E/N = {em / hamiltonian.N:.6f}, var(e_L)/N = {var / hamiltonian.N:.6f}",
+                  verbosity)
+    _device_status_check(eng)
+    W, b, a = eng.rbm_parameters()
+    trained = RBMSpinHalf(guide.N, guide.n_hidden, W=W, b=b, a=a, dtype=guide.dtype)
+    torch.cuda.current_stream().synchronize()
+    return trained, {"energy": np.asarray(hist_e), "variance": np.asarray(hist_v),
+                     "seconds": time.time() - t0}
