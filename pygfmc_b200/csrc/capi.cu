@@ -109,6 +109,7 @@ struct gfmc_handle {
   float *tr_theta = nullptr, *tr_rates = nullptr, *tr_rsum = nullptr, *tr_gw = nullptr;
   double *tr_e = nullptr, *tr_stats = nullptr;
   float *tr_gW = nullptr, *tr_gb = nullptr, *tr_ga = nullptr;
+  void *tr_recs = nullptr;
   float *ms_W = nullptr, *ms_b = nullptr, *ms_a = nullptr, *ad_m = nullptr, *ad_v = nullptr;
   int adam_step = 0;
   // off-diagonal forward walking through this handle as the shadow chain
@@ -663,9 +664,10 @@ int rbm_gradient_t(gfmc_handle *h, int n, const void *cfg, const int32_t *parent
   if (r.Np > 256) return fail(GFMC_ERR_UNSUPPORTED, "RBM training supports at most 256 sites");
   if (n > h->train_cap) {
     cudaFree(h->tr_cfg); cudaFree(h->tr_theta); cudaFree(h->tr_rates); cudaFree(h->tr_rsum);
-    cudaFree(h->tr_gw); cudaFree(h->tr_e);
+    cudaFree(h->tr_gw); cudaFree(h->tr_e); cudaFree(h->tr_recs);
     h->tr_cfg = nullptr; h->tr_theta = h->tr_rates = h->tr_rsum = h->tr_gw = nullptr;
     h->tr_e = nullptr;
+    h->tr_recs = nullptr;
     h->train_cap = 0;
     GFMC_CUDA(cudaMalloc(&h->tr_cfg, sizeof(uint64_t) * (size_t)n * NW));
     GFMC_CUDA(cudaMalloc(&h->tr_theta, sizeof(float) * (size_t)n * r.Hp));
@@ -673,6 +675,7 @@ int rbm_gradient_t(gfmc_handle *h, int n, const void *cfg, const int32_t *parent
     GFMC_CUDA(cudaMalloc(&h->tr_rsum, sizeof(float) * (size_t)n));
     GFMC_CUDA(cudaMalloc(&h->tr_gw, sizeof(float) * (size_t)n));
     GFMC_CUDA(cudaMalloc(&h->tr_e, sizeof(double) * (size_t)n));
+    GFMC_CUDA(cudaMalloc(&h->tr_recs, 16 * (size_t)n * (size_t)(n_off + 1)));
     h->train_cap = n;
   }
   if (!h->tr_stats) {
@@ -731,7 +734,7 @@ int rbm_gradient_t(gfmc_handle *h, int n, const void *cfg, const int32_t *parent
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    e = launch_rbm_grad(g, sms, s);
+    e = launch_rbm_grad(g, h->tr_recs, sms, s);
   }
   if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "RBM gradient: %s", cudaGetErrorString(e));
   return GFMC_OK;
@@ -817,7 +820,7 @@ int gfmc_destroy(gfmc_handle *h) {
   cudaFree(h->tr_cfg); cudaFree(h->tr_theta); cudaFree(h->tr_rates); cudaFree(h->tr_rsum);
   cudaFree(h->tr_gw); cudaFree(h->tr_e); cudaFree(h->tr_stats); cudaFree(h->tr_gW);
   cudaFree(h->tr_gb); cudaFree(h->tr_ga); cudaFree(h->ms_W); cudaFree(h->ms_b); cudaFree(h->ms_a);
-  cudaFree(h->ad_m); cudaFree(h->ad_v);
+  cudaFree(h->ad_m); cudaFree(h->ad_v); cudaFree(h->tr_recs);
   delete h;
   return GFMC_OK;
 }

@@ -60,8 +60,9 @@ struct GradArgs {
 };
 
 // Gradient of the variance loss into grad_W (Hp, Np), grad_b (Hp), grad_a
-// (Np) (accumulated: zero them first).  Np <= 256.
-cudaError_t launch_rbm_grad(const GradArgs &a, int sms, cudaStream_t s);
+// (Np) (accumulated: zero them first).  Np <= 256.  recs: scratch of
+// n (n_off + 1) x 16 bytes for the row records.
+cudaError_t launch_rbm_grad(const GradArgs &a, void *recs, int sms, cudaStream_t s);
 // gw[w] = 2 omega_w (e_w - E) / sum omega; stats = (E, variance) (device).
 cudaError_t launch_train_coeff(int n, const double *e, const double *omega, float *gw,
                                double *stats, cudaStream_t s);

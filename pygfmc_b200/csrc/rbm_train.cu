@@ -129,26 +129,137 @@ __device__ __forceinline__ uint32_t bf16_pair(float lo, float hi) {
 
 namespace {
 
-__global__ void __launch_bounds__(TT, 1) rbm_grad_kernel(GradArgs g) {
+// Row records of the gradient contraction, one per (walker, slot) and one
+// base row per walker, in row order r = w (n_off + 1) + s:
+//   x: coefficient c (slot: g_w r_ws; base: -g_w R_w; 0 for a zero rate)
+//   y, z: -2 s_i, -2 s_j of the flipped sites (0 when absent)
+//   w: code = i | j << 9 | (walker & 0x3FFF) << 18, absent sites = Np (a
+//      zero row of the staged weight tile)
+// rbm_records_kernel also accumulates dL/da (per-block shared sums, then one
+// global atomic per site and block).
+__global__ void rbm_records_kernel(GradArgs g, float4 *recs) {
+  extern __shared__ float acc[];   // (Np,)
+  const int rows_per_w = g.n_off + 1;
+  for (int i = threadIdx.x; i < g.Np; i += blockDim.x) acc[i] = 0.0f;
+  __syncthreads();
+  const int wb0 = blockIdx.x * 16;
+  int wb1 = wb0 + 16;
+  if (wb1 > g.n) wb1 = g.n;
+  const long long r0 = (long long)wb0 * rows_per_w, r1 = (long long)wb1 * rows_per_w;
+  for (long long r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+    const int w = (int)(r / rows_per_w);
+    const int s = (int)(r - (long long)w * rows_per_w);
+    int i = g.Np, j = g.Np;
+    float c, m2si = 0.0f, m2sj = 0.0f;
+    if (s < g.n_off) {
+      c = g.gw[w] * g.rates[(size_t)w * g.n_off + s];
+      if (c != 0.0f) {
+        if (s < g.n_hx) {
+          i = s;
+        } else {
+          const uint32_t pe = g.edge[s - g.n_hx];
+          i = (int)(pe & 0xFFFF);
+          j = (int)(pe >> 16);
+        }
+        const uint64_t *x = g.cfg + (size_t)w * g.NW;
+        const float si = ((x[i >> 6] >> (i & 63)) & 1ull) ? 1.0f : -1.0f;
+        m2si = -2.0f * si;
+        atomicAdd(&acc[i], c * m2si);
+        if (j < g.Np) {
+          const float sj = ((x[j >> 6] >> (j & 63)) & 1ull) ? 1.0f : -1.0f;
+          m2sj = -2.0f * sj;
+          atomicAdd(&acc[j], c * m2sj);
+        }
+      }
+    } else {
+      c = -g.gw[w] * g.rsum[w];
+    }
+    const uint32_t code = (uint32_t)i | ((uint32_t)j << 9) | (((uint32_t)w & 0x3FFFu) << 18);
+    recs[r] = make_float4(c, m2si, m2sj, __uint_as_float(code));
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < g.Np; i += blockDim.x)
+    if (acc[i] != 0.0f) atomicAdd(&g.grad_a[i], acc[i]);
+}
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void cp_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void bgroup_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+
+// Shared-memory plan of the gradient kernel (offsets from a 1024-aligned base).
+struct GradSmem {
+  size_t A0, A1, B0, B1, WTs, recs, th, wd, bar, total;
+  int maxw;
+};
+
+__host__ __device__ inline GradSmem grad_smem_plan(int Np, int n_off, int NW) {
+  GradSmem p;
+  const int rows_per_w = n_off + 1;
+  p.maxw = (KR - 1) / rows_per_w + 2;
+  size_t o = 0;
+  p.A0 = o; o += 16384;
+  p.A1 = o; o += 16384;
+  p.B0 = o; o += (size_t)Np * 128;
+  p.B1 = o; o += (size_t)Np * 128;
+  p.WTs = o; o += (size_t)(Np + 1) * TT * 2;                 // + one zero row
+  o = (o + 15) & ~(size_t)15;
+  p.recs = o; o += 3 * (size_t)KR * 16;                      // three chunks in flight
+  p.th = o; o += 3 * (size_t)p.maxw * TT * 4;
+  p.wd = o; o += 3 * (size_t)p.maxw * NW * 8;
+  o = (o + 7) & ~(size_t)7;
+  p.bar = o; o += 32;
+  p.total = o;
+  return p;
+}
+
+// The copies of chunk ch into buffer b (run by the 128 B-group threads): its
+// 64 row records, and the theta rows (this tile's units) and spin words of
+// the walkers it spans.  Rows past the end get zero records.
+__device__ __forceinline__ void issue_chunk(const GradArgs &g, const float4 *recs_g,
+                                            unsigned char *base, const GradSmem &P, int b,
+                                            long long R0, long long R1, int ch, int h0, int t) {
+  const int rows_per_w = g.n_off + 1;
+  const long long r0 = R0 + (long long)ch * KR;
+  float4 *rs = reinterpret_cast<float4 *>(base + P.recs) + (size_t)b * KR;
+  if (t < KR) {
+    if (r0 + t < R1) cp_async16(rs + t, recs_g + r0 + t);
+    else rs[t] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(0u));
+  }
+  const int wbase = (int)(r0 / rows_per_w);
+  long long rl = r0 + KR - 1;
+  if (rl > R1 - 1) rl = R1 - 1;
+  const int nw = (int)(rl / rows_per_w) - wbase + 1;
+  float *th = reinterpret_cast<float *>(base + P.th) + (size_t)b * P.maxw * TT;
+  for (int k = t; k < nw * (TT / 4); k += 128) {
+    const int wi = k / (TT / 4), c4 = k % (TT / 4);
+    cp_async16(th + (size_t)wi * TT + 4 * c4, g.theta + (size_t)(wbase + wi) * g.Hp + h0 + 4 * c4);
+  }
+  uint64_t *wd = reinterpret_cast<uint64_t *>(base + P.wd) + (size_t)b * P.maxw * g.NW;
+  for (int k = t; k < nw * g.NW; k += 128)
+    cp_async8(wd + k, g.cfg + (size_t)(wbase + k / g.NW) * g.NW + (k % g.NW));
+}
+
+__global__ void __launch_bounds__(3 * TT, 1) rbm_grad_kernel(GradArgs g, const float4 *recs_g) {
   extern __shared__ unsigned char dsm[];
   unsigned char *base = (unsigned char *)(((uintptr_t)dsm + 1023) & ~(uintptr_t)1023);
   const int Np = g.Np;
-  unsigned char *Ast[2], *Bst[2];
-  Ast[0] = base;                                  // 128 x 64 bf16 = 16 KB
-  Ast[1] = base + 16384;
-  Bst[0] = base + 32768;                          // Np x 64 bf16
-  Bst[1] = Bst[0] + (size_t)Np * 128;
-  __nv_bfloat16 *WTs = reinterpret_cast<__nv_bfloat16 *>(Bst[1] + (size_t)Np * 128);  // (Np, 128)
-  float *acc_a = reinterpret_cast<float *>(WTs + (size_t)Np * TT);                      // (Np,)
-  int *m_w = reinterpret_cast<int *>(acc_a + Np);                                      // rows
-  int *m_i = m_w + KR;
-  int *m_j = m_i + KR;
-  float *m_c = reinterpret_cast<float *>(m_j + KR);
-  uint64_t *bar = reinterpret_cast<uint64_t *>(((uintptr_t)(m_c + KR) + 7) & ~(uintptr_t)7);
+  const GradSmem P = grad_smem_plan(Np, g.n_off, g.NW);
+  __nv_bfloat16 *WTs = reinterpret_cast<__nv_bfloat16 *>(base + P.WTs);   // (Np + 1, 128)
+  uint64_t *bar = reinterpret_cast<uint64_t *>(base + P.bar);
   uint32_t *slot = reinterpret_cast<uint32_t *>(bar + 2);
   volatile int *flag = reinterpret_cast<volatile int *>(slot + 1);
 
   const int tid = threadIdx.x, warp = tid >> 5;
+  const bool groupA = tid < 2 * TT;       // A producers: two threads per hidden unit
+  const int hl = tid & (TT - 1), half = (tid >> 7) & 1;
+  const int tb = tid - 2 * TT;            // B group: sites and the copies
   const int h0 = blockIdx.x * TT;
   const int w0 = blockIdx.y * g.walkers_per_cta;
   int w1 = w0 + g.walkers_per_cta;
@@ -156,17 +267,14 @@ __global__ void __launch_bounds__(TT, 1) rbm_grad_kernel(GradArgs g) {
   const int rows_per_w = g.n_off + 1;
   const long long R0 = (long long)w0 * rows_per_w, R1 = (long long)w1 * rows_per_w;
   const int nchunks = R1 > R0 ? (int)((R1 - R0 + KR - 1) / KR) : 0;
-  const uint32_t ncols = Np <= 32 ? 32u : (Np <= 64 ? 64u : (Np <= 128 ? 128u : (Np <= 256 ? 256u : 512u)));
-  const bool do_a = blockIdx.x == 0;
+  const uint32_t ncols = Np <= 32 ? 32u : (Np <= 64 ? 64u : (Np <= 128 ? 128u : 256u));
 
-  // stage the W^T tile (sites x 128 hidden) and clear the a accumulator
-  for (int idx = tid; idx < Np * (TT / 8); idx += TT) {
+  for (int idx = tid; idx < (Np + 1) * (TT / 8); idx += 3 * TT) {
     const int i = idx / (TT / 8), c = idx % (TT / 8);
     uint4 v = make_uint4(0u, 0u, 0u, 0u);
     if (i < g.N) v = __ldg(reinterpret_cast<const uint4 *>(g.WT + (size_t)i * g.Hp + h0) + c);
     reinterpret_cast<uint4 *>(WTs + (size_t)i * TT)[c] = v;
   }
-  for (int i = tid; i < Np; i += TT) acc_a[i] = 0.0f;
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(slot)),
@@ -179,172 +287,163 @@ __global__ void __launch_bounds__(TT, 1) rbm_grad_kernel(GradArgs g) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar[1])) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
+  if (!groupA) {
+    if (nchunks > 0) issue_chunk(g, recs_g, base, P, 0, R0, R1, 0, h0, tb);
+    cp_commit();
+    if (nchunks > 1) issue_chunk(g, recs_g, base, P, 1, R0, R1, 1, h0, tb);
+    cp_commit();
+    cp_wait1();
+  }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *slot;
 
-  const int h = h0 + tid;   // this thread's hidden unit
   float acc_b = 0.0f;
-  uint32_t cnt[2] = {0u, 0u};
+  uint32_t cnt0 = 0u, cnt1 = 0u;
   bool ok = true;
-  int th_w = -1;
-  float th_v = 0.0f;
 
   for (int ch = 0; ch < nchunks && ok; ++ch) {
-    const int st = ch & 1;
-    // the stage's previous MMAs must have read it
-    if (cnt[st] > 0 && !cta_wait(&bar[st], (cnt[st] - 1u) & 1u, flag)) {
+    const int st = ch & 1, b = ch % 3;
+    const uint32_t cst = st ? cnt1 : cnt0;
+    if (cst > 0 && !cta_wait(&bar[st], (cst - 1u) & 1u, flag)) {
       if (tid == 0) atomicOr(g.status, 8);
       ok = false;
       break;
     }
-    // ---- decode the chunk's rows
-    if (tid < KR) {
-      const long long r = R0 + (long long)ch * KR + tid;
-      int w = -1, i = -1, j = -1;
-      float c = 0.0f;
-      if (r < R1) {
-        w = (int)(r / rows_per_w);
-        const int s = (int)(r - (long long)w * rows_per_w);
-        if (s < g.n_off) {
-          c = g.gw[w] * g.rates[(size_t)w * g.n_off + s];
-          if (s < g.n_hx) {
-            i = s;
-          } else {
-            const uint32_t pe = g.edge[s - g.n_hx];
-            i = (int)(pe & 0xFFFF);
-            j = (int)(pe >> 16);
-          }
-          if (do_a && c != 0.0f) {
-            const uint64_t *x = g.cfg + (size_t)w * g.NW;
-            const float si = ((x[i >> 6] >> (i & 63)) & 1ull) ? 1.0f : -1.0f;
-            atomicAdd(&acc_a[i], -2.0f * c * si);
-            if (j >= 0) {
-              const float sj = ((x[j >> 6] >> (j & 63)) & 1ull) ? 1.0f : -1.0f;
-              atomicAdd(&acc_a[j], -2.0f * c * sj);
-            }
-          }
-        } else {
-          c = -g.gw[w] * g.rsum[w];   // base row
-        }
-      }
-      m_w[tid] = w;
-      m_i[tid] = i;
-      m_j[tid] = j;
-      m_c[tid] = c;
-    }
-    __syncthreads();
-    // ---- A: U[h, r] = c_r tanh(theta'_r,h), this thread's hidden row
-    unsigned char *A = Ast[st];
+    const long long r0 = R0 + (long long)ch * KR;
+    const int wbase_lo = (int)((r0 / rows_per_w) & 0x3FFF);
+    const float4 *rs = reinterpret_cast<const float4 *>(base + P.recs) + (size_t)b * KR;
+    if (groupA) {
+      // U[h, r] = c_r tanh(theta_w,h - 2 s_i W[h, i] - 2 s_j W[h, j]), rows 32 half ..
+      const float *th = reinterpret_cast<const float *>(base + P.th) + (size_t)b * P.maxw * TT;
+      unsigned char *A = base + (st ? P.A1 : P.A0);
 #pragma unroll 1
-    for (int cc = 0; cc < KR / 8; ++cc) {
-      uint32_t q[4];
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        float u2[2];
-#pragma unroll
-        for (int t2 = 0; t2 < 2; ++t2) {
-          const int rr = 8 * cc + 2 * e + t2;
-          const int w = m_w[rr];
-          const float c = m_c[rr];
-          float u = 0.0f;
-          if (w >= 0 && c != 0.0f) {
-            if (w != th_w) {
-              th_v = g.theta[(size_t)w * g.Hp + h];
-              th_w = w;
-            }
-            float t = th_v;
-            const int i = m_i[rr], j = m_j[rr];
-            if (i >= 0) {
-              const uint64_t *x = g.cfg + (size_t)w * g.NW;
-              const float si = ((x[i >> 6] >> (i & 63)) & 1ull) ? 1.0f : -1.0f;
-              t = t - 2.0f * si * __bfloat162float(WTs[(size_t)i * TT + tid]);
-              if (j >= 0) {
-                const float sj = ((x[j >> 6] >> (j & 63)) & 1ull) ? 1.0f : -1.0f;
-                t = t - 2.0f * sj * __bfloat162float(WTs[(size_t)j * TT + tid]);
-              }
-            }
-            u = c * tanh_approx(t);
-            acc_b += u;
-          }
-          u2[t2] = u;
-        }
-        q[e] = bf16_pair(u2[0], u2[1]);
-      }
-      *reinterpret_cast<uint4 *>(sw_chunk(A, tid, cc)) = make_uint4(q[0], q[1], q[2], q[3]);
-    }
-    // ---- B: V[i, r] = s'_r,i for the sites i = tid, tid + 128, ...
-    unsigned char *B = Bst[st];
-    for (int i = tid; i < Np; i += TT) {
-      int lw = -1;
-      uint64_t word = 0;
-#pragma unroll 1
-      for (int cc = 0; cc < KR / 8; ++cc) {
+      for (int cc = 4 * half; cc < 4 * half + 4; ++cc) {
         uint32_t q[4];
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
-          uint32_t hv[2];
+          float u2[2];
 #pragma unroll
           for (int t2 = 0; t2 < 2; ++t2) {
-            const int rr = 8 * cc + 2 * e + t2;
-            const int w = m_w[rr];
-            uint32_t v = 0u;
-            if (w >= 0 && i < g.N) {
-              if (w != lw) {
-                word = g.cfg[(size_t)w * g.NW + (i >> 6)];
-                lw = w;
-              }
-              bool up = ((word >> (i & 63)) & 1ull) != 0ull;
-              if (i == m_i[rr] || i == m_j[rr]) up = !up;
-              v = up ? 0x3F80u : 0xBF80u;
+            const float4 rec = rs[8 * cc + 2 * e + t2];
+            float u = 0.0f;
+            if (rec.x != 0.0f) {
+              const uint32_t code = __float_as_uint(rec.w);
+              const int i = (int)(code & 0x1FFu), j = (int)((code >> 9) & 0x1FFu);
+              const int wr = (int)(((code >> 18) - (uint32_t)wbase_lo) & 0x3FFFu);
+              float t = th[(size_t)wr * TT + hl];
+              t = fmaf(rec.y, __bfloat162float(WTs[(size_t)i * TT + hl]), t);
+              t = fmaf(rec.z, __bfloat162float(WTs[(size_t)j * TT + hl]), t);
+              u = rec.x * tanh_approx(t);
+              acc_b += u;
             }
-            hv[t2] = v;
+            u2[t2] = u;
           }
-          q[e] = hv[0] | (hv[1] << 16);
+          q[e] = bf16_pair(u2[0], u2[1]);
         }
-        *reinterpret_cast<uint4 *>(sw_chunk(B, i, cc)) = make_uint4(q[0], q[1], q[2], q[3]);
+        *reinterpret_cast<uint4 *>(sw_chunk(A, hl, cc)) = make_uint4(q[0], q[1], q[2], q[3]);
       }
+    } else {
+      // copies of chunk ch + 2 (its buffer held chunk ch - 1, consumed)
+      if (ch + 2 < nchunks) issue_chunk(g, recs_g, base, P, (ch + 2) % 3, R0, R1, ch + 2, h0, tb);
+      cp_commit();
+      // V: each site row holds the spin of the row's walker (one run per
+      // walker), then the moves' flips are patched in
+      unsigned char *B = base + (st ? P.B1 : P.B0);
+      const uint64_t *wd = reinterpret_cast<const uint64_t *>(base + P.wd) + (size_t)b * P.maxw * g.NW;
+      const long long rend = R1 - r0;                 // valid rows of this chunk
+      const int first = (int)(r0 % rows_per_w);       // row offset inside the first walker
+      for (int i = tb; i < Np; i += TT) {
+        const bool real = i < g.N;
+        // walker segments: row rr belongs to walker wr; the next one starts at nextb
+        int wr = 0, nextb = rows_per_w - first;
+        uint32_t val = real ? (((wd[i >> 6] >> (i & 63)) & 1ull) ? 0x3F80u : 0xBF80u) : 0u;
+#pragma unroll 1
+        for (int cc = 0; cc < KR / 8; ++cc) {
+          uint32_t q[4];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            uint32_t hv[2];
+#pragma unroll
+            for (int t2 = 0; t2 < 2; ++t2) {
+              const int rr = 8 * cc + 2 * e + t2;
+              if (rr == nextb) {
+                ++wr;
+                nextb += rows_per_w;
+                val = (real && rr < rend)
+                          ? (((wd[(size_t)wr * g.NW + (i >> 6)] >> (i & 63)) & 1ull) ? 0x3F80u : 0xBF80u)
+                          : 0u;
+              }
+              hv[t2] = rr < rend ? val : 0u;
+            }
+            q[e] = hv[0] | (hv[1] << 16);
+          }
+          *reinterpret_cast<uint4 *>(sw_chunk(B, i, cc)) = make_uint4(q[0], q[1], q[2], q[3]);
+        }
+      }
+      bgroup_sync();
+      if (tb < KR) {
+        const float4 rec = rs[tb];
+        if (rec.x != 0.0f) {
+          const uint32_t code = __float_as_uint(rec.w);
+          const int i = (int)(code & 0x1FFu), j = (int)((code >> 9) & 0x1FFu);
+          // the flipped spin -s = m2s / 2
+          const int cc = tb >> 3, e = tb & 7;
+          if (i < Np) {
+            unsigned short *p = reinterpret_cast<unsigned short *>(sw_chunk(B, i, cc)) + e;
+            *p = rec.y > 0.0f ? 0x3F80u : 0xBF80u;
+          }
+          if (j < Np) {
+            unsigned short *p = reinterpret_cast<unsigned short *>(sw_chunk(B, j, cc)) + e;
+            *p = rec.z > 0.0f ? 0x3F80u : 0xBF80u;
+          }
+        }
+      }
+      cp_wait1();   // chunk ch + 1 has landed (this thread's copies)
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t a0 = smem_u32(A), b0 = smem_u32(B);
-      for (int sub = 0; sub * 256 < Np; ++sub) {
-        const int nn = (Np - sub * 256) < 256 ? (Np - sub * 256) : 256;
-        const uint32_t id = idesc_n((uint32_t)nn);
+      const uint32_t a0 = smem_u32(base + (st ? P.A1 : P.A0));
+      const uint32_t b0 = smem_u32(base + (st ? P.B1 : P.B0));
+      const uint32_t id = idesc_n((uint32_t)Np);
 #pragma unroll
-        for (int kk = 0; kk < KR / 16; ++kk)
-          mma_bf16(tmem + (uint32_t)sub * 256u, sw128_desc(a0 + 32u * kk),
-                   sw128_desc(b0 + (uint32_t)sub * 256u * 128u + 32u * kk), id,
-                   (ch > 0 || kk > 0) ? 1u : 0u);
-      }
+      for (int kk = 0; kk < KR / 16; ++kk)
+        mma_bf16(tmem, sw128_desc(a0 + 32u * kk), sw128_desc(b0 + 32u * kk), id,
+                 (ch > 0 || kk > 0) ? 1u : 0u);
       mma_commit(&bar[st]);
     }
-    cnt[st] += 1u;
+    if (st) ++cnt1; else ++cnt0;
   }
-  // ---- the outstanding commits
-  for (int st = 0; st < 2; ++st)
-    if (ok && cnt[st] > 0 && !cta_wait(&bar[st], (cnt[st] - 1u) & 1u, flag)) {
-      if (tid == 0) atomicOr(g.status, 8);
-      ok = false;
-    }
+  if (!groupA) cp_wait0();
+  if (ok && cnt0 > 0 && !cta_wait(&bar[0], (cnt0 - 1u) & 1u, flag)) {
+    if (tid == 0) atomicOr(g.status, 8);
+    ok = false;
+  }
+  if (ok && cnt1 > 0 && !cta_wait(&bar[1], (cnt1 - 1u) & 1u, flag)) {
+    if (tid == 0) atomicOr(g.status, 8);
+    ok = false;
+  }
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (ok && nchunks > 0) {
-    for (int c0 = 0; c0 < Np; c0 += 16) {
+    // warp w reads TMEM lanes 32 (w % 4) ..; the three warps of a lane
+    // quarter split the columns
+    const int q4 = warp & 3, part = warp >> 2;
+    const int per = ((Np / 16 + 2) / 3) * 16;
+    const int cbeg = part * per;
+    const int cend = cbeg + per < Np ? cbeg + per : Np;
+    for (int c0 = cbeg; c0 < cend; c0 += 16) {
       float v[16];
-      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-      float *out = g.grad_W + (size_t)(h0 + warp * 32 + (tid & 31)) * Np + c0;
+      tmem_ld16(tmem + ((uint32_t)(q4 * 32) << 16) + (uint32_t)c0, v);
+      float *out = g.grad_W + (size_t)(h0 + q4 * 32 + (tid & 31)) * Np + c0;
 #pragma unroll
       for (int k = 0; k < 16; ++k)
         if (v[k] != 0.0f) atomicAdd(out + k, v[k]);
     }
-    atomicAdd(&g.grad_b[h], acc_b);
-    if (do_a)
-      for (int i = tid; i < Np; i += TT)
-        if (acc_a[i] != 0.0f) atomicAdd(&g.grad_a[i], acc_a[i]);
+    if (groupA && acc_b != 0.0f) atomicAdd(&g.grad_b[h0 + hl], acc_b);
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -460,15 +559,14 @@ cudaError_t launch_rbm_master_init(const RbmTables &r, int N, float *W, float *b
   return cudaGetLastError();
 }
 
-size_t rbm_grad_smem(int Np) {
-  return 1024 + 32768 + 2 * (size_t)Np * 128 + (size_t)Np * TT * 2 + (size_t)Np * 4 + 4 * KR * 4 +
-         64;
-}
-
-cudaError_t launch_rbm_grad(const GradArgs &a, int sms, cudaStream_t s) {
-  const size_t smem = rbm_grad_smem(a.Np);
-  cudaError_t e = cudaFuncSetAttribute(rbm_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
+cudaError_t launch_rbm_grad(const GradArgs &a, void *recs, int sms, cudaStream_t s) {
+  const size_t smem = 1024 + grad_smem_plan(a.Np, a.n_off, a.NW).total;
+  if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
+  // the row records (and dL/da)
+  rbm_records_kernel<<<(a.n + 15) / 16, 256, sizeof(float) * a.Np, s>>>(a, (float4 *)recs);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(rbm_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const int tiles = a.Hp / TT;
   int blocks = (2 * sms + tiles - 1) / tiles;
@@ -477,7 +575,7 @@ cudaError_t launch_rbm_grad(const GradArgs &a, int sms, cudaStream_t s) {
   GradArgs g = a;
   g.walkers_per_cta = (a.n + blocks - 1) / blocks;
   blocks = (a.n + g.walkers_per_cta - 1) / g.walkers_per_cta;
-  rbm_grad_kernel<<<dim3(tiles, blocks), TT, smem, s>>>(g);
+  rbm_grad_kernel<<<dim3(tiles, blocks), 3 * TT, smem, s>>>(g, (const float4 *)recs);
   return cudaGetLastError();
 }
 
