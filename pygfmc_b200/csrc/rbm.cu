@@ -88,14 +88,38 @@ __device__ __forceinline__ T slot_coupling(const DevModel<T> &m, const uint64_t 
   return m.uniform_pm ? (anti ? m.jpm0 : m.jpmpm0) : (anti ? m.jpm[e] : m.jpmpm[e]);
 }
 
+__device__ __forceinline__ float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 // q[0] = H_xx, q[1 + o] = guide-transformed rate of slot o.
+//
+// float64: sum_h lncosh(theta') - sum_h lncosh(theta) term by term (the
+// reference form).  float32: the same difference as
+//   sum_h (|theta'_h| - |theta_h|) + log prod_h (1 + e'_h) / (1 + e_h),
+//   e = exp(-2 |x|),
+// with 1 / (1 + e_h) computed once per evaluation, so a (slot, unit) pair
+// costs one ex2 instead of an ex2 and a lg2; each factor lies in (1/2, 2),
+// so the lane's product of HPL factors stays in range, and one lg2 per
+// lane and slot closes it.
 template <typename T, int HPL>
 __device__ void rbm_rates(const DevModel<T> &m, const RbmTables &r, const uint64_t *bits,
                           const T (&th)[HPL], T *q, int lane) {
-  T l = T(0);
+  constexpr bool F32 = sizeof(T) == 4;
+  T lcs = T(0);
+  float binv[F32 ? HPL : 1];
+  if constexpr (F32) {
 #pragma unroll
-  for (int k = 0; k < HPL; ++k) l += lncosh<T>(th[k]);
-  const T lcs = warp_sum(l);
+    for (int k = 0; k < HPL; ++k)
+      binv[k] = __fdividef(1.0f, 1.0f + ex2_approx(-2.8853900817779268f * fabsf((float)th[k])));
+  } else {
+    T l = T(0);
+#pragma unroll
+    for (int k = 0; k < HPL; ++k) l += lncosh<T>(th[k]);
+    lcs = warp_sum(l);
+  }
   const int hoff = lane * HPL;
   for (int o = 0; o < m.n_off; ++o) {
     int i, j;
@@ -103,23 +127,35 @@ __device__ void rbm_rates(const DevModel<T> &m, const RbmTables &r, const uint64
     T rate = c;
     if (c != T(0)) {
       const T si = spin_bit(bits, i) ? T(1) : T(-1);
-      float wi[HPL];
+      const T sj = j >= 0 ? (spin_bit(bits, j) ? T(1) : T(-1)) : T(0);
+      float wi[HPL], wj[HPL];
       load_row<HPL>(r.WT + (size_t)i * r.Hp + hoff, wi);
-      T acc = T(0);
-      T d;
       if (j >= 0) {
-        const T sj = spin_bit(bits, j) ? T(1) : T(-1);
-        float wj[HPL];
         load_row<HPL>(r.WT + (size_t)j * r.Hp + hoff, wj);
+      } else {
+#pragma unroll
+        for (int k = 0; k < HPL; ++k) wj[k] = 0.0f;
+      }
+      T d;
+      if constexpr (F32) {
+        float sd = 0.0f, pr = 1.0f;
+#pragma unroll
+        for (int k = 0; k < HPL; ++k) {
+          const float t = th[k] - 2.0f * si * wi[k] - 2.0f * sj * wj[k];
+          const float y = fabsf(t);
+          sd += y - fabsf(th[k]);
+          pr *= (1.0f + ex2_approx(-2.8853900817779268f * y)) * binv[k];
+        }
+        d = warp_sum(sd + 0.69314718f * __log2f(pr));
+      } else {
+        T acc = T(0);
 #pragma unroll
         for (int k = 0; k < HPL; ++k)
           acc += lncosh<T>(th[k] - T(2) * si * T(wi[k]) - T(2) * sj * T(wj[k]));
-        d = warp_sum(acc) - lcs - T(2) * T(r.a[i]) * si - T(2) * T(r.a[j]) * sj;
-      } else {
-#pragma unroll
-        for (int k = 0; k < HPL; ++k) acc += lncosh<T>(th[k] - T(2) * si * T(wi[k]));
-        d = warp_sum(acc) - lcs - T(2) * T(r.a[i]) * si;
+        d = warp_sum(acc) - lcs;
       }
+      d = d - T(2) * T(r.a[i]) * si;
+      if (j >= 0) d = d - T(2) * T(r.a[j]) * sj;
       rate = c * math_exp<T>(d);
     }
     if (lane == 0) q[1 + o] = rate;
