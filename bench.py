@@ -118,6 +118,61 @@ def cpu_reference(P, cfg_sample, alw, steps, warmup, seed_key):
     return len(cfg) * steps / sum(times), threads, sum(times)
 
 
+def sigma_study(P, args):
+    """GPU seconds to sigma(E/N) = 1e-5 on the 16x16 Heisenberg lattice: the
+    plain float64 long-range-Jastrow engine against the float32/bf16 RBM
+    guide (H = 512) trained on the run's own walkers by variance
+    minimisation.  Each method runs warm-up + production through run(); the
+    blocked jackknife error at the largest window gives sigma(E/N); the time
+    to the target is the production GPU time x (sigma / 1e-5)^2 (errors fall
+    as 1/sqrt(steps)).  The RBM's training time is reported beside it."""
+    import torch
+    lat, H, G, pairs, beta = build_system(P, "fp64")
+    out = {}
+    p_arr = [8, 32, 128]
+
+    def measure(name, guide, n, steps, warm, precision):
+        w = P.prepare_walkers_sz(n, 256, P.PRNGKey(11), sz=0)
+        torch.cuda.synchronize()
+        wf, E, _, st, raw = P.run(w, steps, H, TAU, guide, p_arr, rng_key=P.PRNGKey(12),
+                                  warmup_steps=warm, verbosity=0, precision=precision)
+        Ej, err = P.estimators.jackknife_energy([128], raw["log_weights"], raw["energy"], 20)
+        sig = err[128] / 256
+        t = st["runtime"]
+        out[name] = {"E_per_site": Ej[128] / 256, "sigma_per_site": sig, "n_walkers": n,
+                     "steps": steps, "warmup": warm, "precision": precision,
+                     "production_gpu_s": t, "gpu_s_to_1e-5": t * (sig / 1e-5) ** 2,
+                     "walker_steps_per_s": n * steps / t,
+                     "local_energy_var_per_site": float(np.var(wf.e_loc) / 256)}
+
+    measure("jastrow_fp64", G, N_WALKERS, args.study_steps, 2000, "fp64")
+    measure("jastrow_mixed", G, N_WALKERS, args.study_steps, 2000, "mixed")
+    G0 = P.RBMSpinHalf(256, 512, seed=0, sigma=0.01)
+    w = P.prepare_walkers_sz(65536, 256, P.PRNGKey(13), sz=0)
+    trained, hist = P.learn.train_rbm_guide(w, H, G0, n_iterations=args.train_iters,
+                                            steps_per_iteration=3, step_size=TAU, lr=args.train_lr,
+                                            rng_key=P.PRNGKey(14), warmup_steps=100, verbosity=0)
+    measure("rbm_h512_mixed", trained, 65536, args.rbm_steps, 500, "mixed")
+    out["rbm_h512_mixed"]["training_gpu_s"] = hist["seconds"]
+    out["rbm_h512_mixed"]["train_var_per_site_first_last"] = [float(hist["variance"][0] / 256),
+                                                              float(hist["variance"][-1] / 256)]
+    out["rbm_h512_mixed"]["train_iterations"] = len(hist["variance"])
+    out["rbm_h512_mixed"]["train_lr"] = args.train_lr
+    out["rbm_h512_mixed"]["train_collapsed"] = bool(hist["collapsed"])
+    out["rbm_h512_mixed"]["gpu_s_to_1e-5_with_training"] = (
+        out["rbm_h512_mixed"]["gpu_s_to_1e-5"] + hist["seconds"])
+    j, r = out["jastrow_fp64"], out["rbm_h512_mixed"]
+    diff = abs(j["E_per_site"] - r["E_per_site"]) / np.hypot(j["sigma_per_site"], r["sigma_per_site"])
+    line = {"metric": "GPU-s to sigma(E/N)=1e-5", "value": r["gpu_s_to_1e-5"], "unit": "s",
+            "higher_is_better": False, "n_gpus": 1, "data": "synthetic",
+            "config": {"workload": "heisenberg_16x16_rbm_h512_vs_longrange_jastrow", "tau": TAU,
+                       "p": 128, "jackknife_blocks": 20},
+            "methods": out,
+            "learned_over_jastrow_fp64_time_ratio": r["gpu_s_to_1e-5"] / j["gpu_s_to_1e-5"],
+            "energy_difference_in_sigma": diff}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -128,10 +183,21 @@ def main():
     ap.add_argument("--walkers", type=int, default=N_WALKERS)
     ap.add_argument("--cpu-sample", type=int, default=512)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--study", default=None, choices=["sigma"],
+                    help="sigma: GPU seconds to sigma(E/N)=1e-5, RBM vs Jastrow (minutes)")
+    ap.add_argument("--study-steps", type=int, default=4000)
+    ap.add_argument("--rbm-steps", type=int, default=1000)
+    ap.add_argument("--train-iters", type=int, default=600)
+    ap.add_argument("--train-lr", type=float, default=3e-4)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     import pygfmc_b200 as P
+
+    if args.study == "sigma":
+        if rank == 0:
+            sigma_study(P, args)
+        return
 
     if args.impl == "reference":
         if rank != 0:

@@ -144,6 +144,11 @@ int gfmc_run_steps(gfmc_handle *h, int method, double step, double lam, double a
  * cfg[parents[i]] (parents nullable). */
 int gfmc_local_energy(gfmc_handle *h, int n_walkers, const void *cfg, const int32_t *parents,
                       double *e_loc, void *stream);
+/* The same with the diagonal element H_xx of each configuration (device,
+ * float64, n_walkers): the sampler-health probes of engine/estimators.py
+ * statistics:1139 (escape rate diag - e_L, stay probability). */
+int gfmc_local_energy_parts(gfmc_handle *h, int n_walkers, const void *cfg,
+                            const int32_t *parents, double *e_loc, double *diag, void *stream);
 
 /* Applies a parent map: cfg_out[i] = cfg_in[parents[i]], e_out[i] = e_in[parents[i]],
  * log_w[i] = 0 (any output nullable except cfg_out). */

@@ -5,7 +5,8 @@ step_size, guide, p_array, *, method, rng_key, lam, warmup_steps, ...)`` with
 PyGFMC's SpinHalf / BoseHubbard Hamiltonians and Jastrow guides, executed by
 hand-written CUDA kernels behind a C ABI (``include/gfmc_b200.h``).
 """
-from . import hamiltonian, learn, random, walkers, wavefunction
+from . import diagnostics, hamiltonian, learn, random, walkers, wavefunction
+from .diagnostics import statistics
 from .engine import GFMCEngine, run, run_gfmc
 from .estimators import evaluate_observables
 from .hamiltonian import BoseHubbard, SpinHalf, chain, kagome, square
@@ -16,7 +17,7 @@ from .wavefunction import JastrowBoseHubbard, JastrowSpinHalf, RBMSpinHalf
 
 __version__ = "0.1.0"
 
-__all__ = ["run", "run_gfmc", "GFMCEngine", "evaluate_observables", "SpinHalf", "BoseHubbard",
+__all__ = ["run", "run_gfmc", "statistics", "GFMCEngine", "evaluate_observables", "SpinHalf", "BoseHubbard",
            "chain", "square", "kagome", "PRNGKey", "Walker", "prepare_walkers_random",
            "prepare_walkers_sz", "prepare_walkers_from_configs", "prepare_walkers_occupations",
            "JastrowSpinHalf", "JastrowBoseHubbard", "RBMSpinHalf", "hamiltonian", "random", "walkers",

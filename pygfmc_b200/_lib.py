@@ -84,6 +84,7 @@ SIGNATURES = {
                                       ctypes.c_double, ctypes.c_int, _u32p, ctypes.c_int,
                                       _vp, _vp, _vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gfmc_local_energy": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, _vp]),
+    "gfmc_local_energy_parts": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp]),
     "gfmc_gather": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gfmc_windowed_energy": (ctypes.c_int, [ctypes.c_int, _vp, _vp, ctypes.c_int, _i32p, _dp, _vp]),
     "gfmc_set_max_iters": (ctypes.c_int, [_vp, ctypes.c_int]),

@@ -742,7 +742,8 @@ int rbm_gradient_t(gfmc_handle *h, int n, const void *cfg, const int32_t *parent
 
 template <typename T>
 int local_energy_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, int n,
-                   const void *cfg, const int32_t *parents, double *e_loc, cudaStream_t s) {
+                   const void *cfg, const int32_t *parents, double *e_loc, cudaStream_t s,
+                   double *diag_out = nullptr) {
   int rc = ensure_scratch(h, n, 1);
   if (rc) return rc;
   GFMC_CUDA(cudaMemsetAsync(h->ctr, 0, sizeof(int), s));
@@ -754,6 +755,7 @@ int local_energy_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, i
   a.cfg_out = nullptr;
   a.log_w = nullptr;
   a.e_loc = e_loc;
+  a.diag_out = diag_out;
   a.hops = nullptr;
   a.work_ctr = h->ctr;
   a.partial_max = nullptr;
@@ -879,6 +881,16 @@ int gfmc_local_energy(gfmc_handle *h, int n, const void *cfg, const int32_t *par
   if (h->precision == GFMC_PRECISION_FP64)
     return local_energy_t<double>(h, h->m64, h->g64, n, cfg, parents, e_loc, s);
   return local_energy_t<float>(h, h->m32, h->g32, n, cfg, parents, e_loc, s);
+}
+
+int gfmc_local_energy_parts(gfmc_handle *h, int n, const void *cfg, const int32_t *parents,
+                            double *e_loc, double *diag, void *stream) {
+  if (!h || n <= 0 || !cfg || !e_loc || !diag)
+    return fail(GFMC_ERR_INVALID, "gfmc_local_energy_parts: bad argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (h->precision == GFMC_PRECISION_FP64)
+    return local_energy_t<double>(h, h->m64, h->g64, n, cfg, parents, e_loc, s, diag);
+  return local_energy_t<float>(h, h->m32, h->g32, n, cfg, parents, e_loc, s, diag);
 }
 
 int gfmc_gather(gfmc_handle *h, int n, const int32_t *parents, const void *cfg_in, void *cfg_out,

@@ -106,6 +106,7 @@ struct EvolveArgs {
   void *field_out;        // guide fields after the step (N per walker); nullable
   float *rates_out;       // EVALUATE, RBM guide: (n_walkers, M - 1) guided rates; nullable
   float *rsum_out;        // EVALUATE, RBM guide: (n_walkers,) sum of those rates; nullable
+  double *diag_out;       // EVALUATE: (n_walkers,) diagonal element H_xx; nullable
 };
 
 struct LaunchPlan {

@@ -773,6 +773,7 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta
     } else {  // EVALUATE: local energy of the loaded configuration
       const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.n_off, MODE_OFF, lane);
       eloc = ev.diag - ev.total;
+      if (a.diag_out && lane == 0) a.diag_out[walker] = (double)ev.diag;
     }
 
     // ---- store

@@ -439,6 +439,7 @@ rbm_evolve_kernel(DevModel<T> m, RbmTables r, EvolveArgs a) {
         for (int o = lane; o < m.n_off; o += 32)
           a.rates_out[(size_t)walker * m.n_off + o] = (float)q[1 + o];
       if (a.rsum_out && lane == 0) a.rsum_out[walker] = (float)(-sc.total);
+      if (a.diag_out && lane == 0) a.diag_out[walker] = (double)q[0];
     }
 
     // ---- store

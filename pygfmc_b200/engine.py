@@ -349,6 +349,26 @@ class GFMCEngine:
                                             self._stream()), "gfmc_local_energy")
         return out
 
+    def local_energy_parts(self):
+        """(e_L, H_xx) of the current population (float64 device tensors)."""
+        e = self.torch.empty(self.n, dtype=self.torch.float64, device=self.device)
+        d = self.torch.empty_like(e)
+        par = self._ptr(self.parents) if self.parents_valid else ctypes.c_void_p(0)
+        _lib.check(self.L.gfmc_local_energy_parts(self.h, self.n, self._ptr(self.cfg), par,
+                                                  self._ptr(e), self._ptr(d), self._stream()),
+                   "gfmc_local_energy_parts")
+        return e, d
+
+    def packed_population(self):
+        """The current population's packed configurations (host uint8 (n, bytes))."""
+        cfg = self.cfg
+        if self.parents_valid:
+            cfg = self.torch.empty_like(self.cfg)
+            _lib.check(self.L.gfmc_gather(self.h, self.n, self._ptr(self.parents), self._ptr(self.cfg),
+                                          self._ptr(cfg), ctypes.c_void_p(0), ctypes.c_void_p(0),
+                                          ctypes.c_void_p(0), self._stream()), "gfmc_gather")
+        return cfg.view(self.n, self.cfg_bytes).cpu().numpy()
+
     def steps(self, method, step, lam, alw, keys, logG, E, hops=None):
         """len(keys) branching steps; keys is a (n_steps, 4) uint32 host array."""
         keys = np.ascontiguousarray(keys, dtype=np.uint32)
@@ -568,6 +588,7 @@ def key_schedule(key, n_steps):
 
 
 _AUX_POSITIVITY = 10_001
+_AUX_STATISTICS = 10_002
 _POSITIVITY_PROBE_STEPS = 100
 _N_POSITIVITY_CHECK = 100
 
@@ -974,13 +995,20 @@ def run_gfmc(walkers, n_steps, hamiltonian, step_size, guide, p_array, *, method
                    e_loc=e_d.cpu().numpy().astype(weight_dtype))
     hops_np = hops_d.cpu().numpy()
 
-    stats = {
+    # the end-of-run statistics pass from the production-final walkers, on
+    # its own side-stream (driver.py _run_stats:627-660)
+    from .diagnostics import statistics as _statistics
+    _, end_stats = _statistics(out_w, hamiltonian, step_f, guide, method,
+                               _rnd.fold_in(aux_root, _AUX_STATISTICS), alw, lam=lam,
+                               quiet=verbosity < 1, m_array=m_array, precision=precision)
+    stats = dict(end_stats)
+    stats.update({
         "avg_log_weight": float(alw),
         "it_per_sec": n_steps / runtime,
         "runtime": runtime,
         "total_wall_time": time.time() - wall_start,
         "number_of_devices": 1,
-        "hops_per_step_mean": hops_np / float(N_walker),
+        "moves_per_walker_step": hops_np / float(N_walker),
         "parameters/n_steps": int(n_steps),
         "parameters/n_walkers": N_walker,
         "parameters/n_sites": int(np.shape(config)[1]),
@@ -1003,7 +1031,7 @@ def run_gfmc(walkers, n_steps, hamiltonian, step_size, guide, p_array, *, method
         "parameters/precision": np.asarray(precision, dtype="S32"),
         "parameters/rng_key": rng_key_in,
         "parameters/rng_key_next": key,
-    }
+    })
     off_np = off_norm_np = off_steps_np = None
     if off_names:
         od = od_d.cpu().numpy()

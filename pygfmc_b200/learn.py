@@ -20,15 +20,23 @@ __all__ = ["train_rbm_guide"]
 
 
 def train_rbm_guide(walkers, hamiltonian, guide, *, n_iterations=200, steps_per_iteration=5,
-                    step_size=0.05, method="cont_time", lam=None, rng_key=None, lr=3e-3,
-                    warmup_steps=100, verbosity=1):
+                    step_size=0.05, method="cont_time", lam=None, rng_key=None, lr=3e-4,
+                    warmup_steps=100, verbosity=1, collapse_tol=0.05, snapshot_every=10):
     """Variance-minimisation training of an ``RBMSpinHalf`` guide.
 
     Returns ``(trained_guide, history)``: a new ``RBMSpinHalf`` with the
     trained (bf16-valued) parameters, and a dict of per-iteration arrays
-    ``energy`` (population mean local energy), ``variance`` (the loss) and
-    the total ``seconds``.  The walkers are evolved in the float32 build;
-    ``walkers.config`` is the starting population."""
+    ``energy`` (population mean local energy), ``variance`` (the loss), the
+    total ``seconds`` and ``collapsed`` (see below).  The walkers are evolved
+    in the float32 build; ``walkers.config`` is the starting population.
+
+    Collapse guard: the population's mean local energy estimates the ground
+    energy whatever the guide, so a jump of more than ``collapse_tol`` (relative)
+    away from its running mean over the last 20 iterations means the guide has
+    switched the moves off (the zero-variance degenerate solution of variance
+    minimisation on walkers the guide itself steers).  Training then stops and
+    the parameters of the last snapshot (every ``snapshot_every`` iterations)
+    are returned."""
     if not isinstance(guide, RBMSpinHalf):
         raise TypeError("train_rbm_guide needs an RBMSpinHalf guide")
     n_iterations = int(n_iterations)
@@ -55,6 +63,8 @@ def train_rbm_guide(walkers, hamiltonian, guide, *, n_iterations=200, steps_per_
         keys, key = key_schedule(key, warmup_steps)
         eng.steps(method, step_size, lam, alw, keys, lg[:warmup_steps], E[:warmup_steps])
     hist_e, hist_v = [], []
+    snapshot = eng.rbm_parameters()
+    collapsed = False
     for it in range(n_iterations):
         keys, key = key_schedule(key, steps_per_iteration)
         eng.steps(method, step_size, lam, alw, keys, lg[:steps_per_iteration],
@@ -62,16 +72,23 @@ def train_rbm_guide(walkers, hamiltonian, guide, *, n_iterations=200, steps_per_
         em, var = eng.rbm_train_step(lr)
         hist_e.append(em)
         hist_v.append(var)
-        if not (math.isfinite(em) and math.isfinite(var)):
-            raise ValueError(f"training diverged at iteration {it}: E={em}, var={var}")
+        recent = hist_e[-21:-1]
+        if (not (math.isfinite(em) and math.isfinite(var))) or (
+                len(recent) >= 20 and abs(em - np.mean(recent)) > collapse_tol * abs(np.mean(recent))):
+            collapsed = True
+            _emit(f"[learn] - [train_rbm_guide] - collapse at iteration {it + 1} (E = {em:.6g}); "
+                  "returning the last snapshot", verbosity)
+            break
+        if (it + 1) % snapshot_every == 0:
+            snapshot = eng.rbm_parameters()
         if verbosity >= 2 or (verbosity >= 1 and (it % max(1, n_iterations // 10) == 0
                                                   or it == n_iterations - 1)):
             _emit(f"[learn] - [train_rbm_guide] - iteration {it + 1}/{n_iterations}: "
                   f"E/N = {em / hamiltonian.N:.6f}, var(e_L)/N = {var / hamiltonian.N:.6f}",
                   verbosity)
     _device_status_check(eng)
-    W, b, a = eng.rbm_parameters()
+    W, b, a = snapshot if collapsed else eng.rbm_parameters()
     trained = RBMSpinHalf(guide.N, guide.n_hidden, W=W, b=b, a=a, dtype=guide.dtype)
     torch.cuda.current_stream().synchronize()
     return trained, {"energy": np.asarray(hist_e), "variance": np.asarray(hist_v),
-                     "seconds": time.time() - t0}
+                     "seconds": time.time() - t0, "collapsed": collapsed}

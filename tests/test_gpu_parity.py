@@ -54,6 +54,11 @@ def test_engine_reproduces_golden_run(P, golden, name):
     for pp in (2, 4):
         np.testing.assert_allclose(energy[pp], golden[p + f"energy/{pp}"], rtol=1e-10, atol=1e-12)
     assert np.array_equal(stats["parameters/rng_key_next"], golden[p + "stats/parameters/rng_key_next"])
+    # the end-of-run statistics pass (engine/estimators.py statistics:1139)
+    np.testing.assert_allclose(stats["offspring_k0"], golden[p + "stats/offspring_k0"], rtol=0, atol=1e-12)
+    if method == "cont_time":
+        np.testing.assert_allclose(stats["hops_per_step_mean"], golden[p + "stats/hops_per_step_mean"],
+                                   rtol=2e-6)
 
 
 def _systems(P, O):
