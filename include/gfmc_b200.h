@@ -284,6 +284,41 @@ int gfmc_forward_walk(gfmc_handle *shadow, gfmc_handle *op, int method, double s
 int gfmc_operator_min_rate(gfmc_handle *op, int n_walkers, const void *cfg, const int32_t *parents,
                            int parents_valid, double *min_out, void *stream);
 
+/* ---- walkers sharded over GPUs ---------------------------------------- */
+/* The evolve half of a branching step alone (no resampling): walkers
+ * cfg[parents[i]] (parents read when parents_valid) propagated with key
+ * into cfg_out, with their log weights and local energies.  Walker i draws
+ * from fold_in(key, walker_offset + i): a rank holding global walkers
+ * [offset, offset + n) of a sharded population reproduces the streams of the
+ * unsharded one.  Carried guide state is rebuilt. */
+int gfmc_evolve(gfmc_handle *h, int method, double step, double lam, double alw,
+                const uint32_t key[2], long long walker_offset, int n_walkers, const void *cfg,
+                const int32_t *parents, int parents_valid, void *cfg_out, double *log_w,
+                double *e_loc, uint64_t *hops, void *stream);
+/* Systematic resampling of a population sharded over ranks in contiguous
+ * blocks (walkers/reconfiguration.py:9-62 applied to the concatenated
+ * population):
+ * 1. gfmc_dist_local_max: the rank's max log weight (host); the caller takes
+ *    the max over ranks as the common shift.
+ * 2. gfmc_dist_local_sums: (S_r, sum_r w e_loc, last positive index) of the
+ *    rank's weights w = exp(log_w - shift) (host).  Over ranks: S = sum S_r,
+ *    E_n = sum (sum w e) / S, log G_n = log S + shift - log N.
+ * 3. gfmc_dist_parents: the rank's local parents of the global output slots
+ *    [slot_lo, slot_lo + count), the slots whose point U_i = (i + psi) / N S
+ *    lies in [offset, offset + S_r) (offset = the earlier ranks' S sum);
+ *    psi = uniform(reconfiguration key), N = N_total.  The caller sends each
+ *    slot's walker to the rank that owns the slot (contiguous blocks).
+ * PyGFMC's multi-device path all-gathers every configuration instead
+ * (engine/multi_gpu.py:91-155). */
+int gfmc_dist_local_max(gfmc_handle *h, int n_walkers, const double *log_w, double *max_out,
+                        void *stream);
+int gfmc_dist_local_sums(gfmc_handle *h, int n_walkers, const double *log_w,
+                         const double *e_loc, double shift, double out[3], void *stream);
+int gfmc_dist_parents(gfmc_handle *h, int n_walkers, const double *log_w, double shift,
+                      double offset, double S_total, double psi, long long N_total,
+                      long long slot_lo, int count, int last_pos, int32_t *parents_out,
+                      void *stream);
+
 /* Largest population gfmc_reconfigure_noalloc accepts. */
 #define GFMC_NOALLOC_MAX_WALKERS 131072
 

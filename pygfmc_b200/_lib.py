@@ -107,6 +107,15 @@ SIGNATURES = {
     "gfmc_rbm_train_step": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp,
                                            ctypes.c_double, _dp, _vp]),
     "gfmc_rbm_get_params": (ctypes.c_int, [_vp, _fp, _fp, _fp]),
+    "gfmc_evolve": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                   ctypes.c_double, _u32p, ctypes.c_longlong, ctypes.c_int, _vp,
+                                   _vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp]),
+    "gfmc_dist_local_max": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _dp, _vp]),
+    "gfmc_dist_local_sums": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_double, _dp,
+                                            _vp]),
+    "gfmc_dist_parents": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_double, ctypes.c_double,
+                                         ctypes.c_double, ctypes.c_double, ctypes.c_longlong,
+                                         ctypes.c_longlong, ctypes.c_int, ctypes.c_int, _vp, _vp]),
     "gfmc_reconfigure_noalloc": (ctypes.c_int, [ctypes.c_int, _vp, _vp, _u32p, _vp, _vp, _vp, _vp]),
     "gfmc_read_status": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int), _vp]),
     "gfmc_key_schedule": (ctypes.c_int, [_u32p, ctypes.c_int, _u32p, _u32p]),

@@ -110,6 +110,8 @@ struct gfmc_handle {
   double *tr_e = nullptr, *tr_stats = nullptr;
   float *tr_gW = nullptr, *tr_gb = nullptr, *tr_ga = nullptr;
   void *tr_recs = nullptr;
+  // sharded reconfiguration: (max | S, S_e, last positive) on the device
+  double *dist_out = nullptr;
   float *ms_W = nullptr, *ms_b = nullptr, *ms_a = nullptr, *ad_m = nullptr, *ad_v = nullptr;
   int adam_step = 0;
   // off-diagonal forward walking through this handle as the shadow chain
@@ -822,7 +824,7 @@ int gfmc_destroy(gfmc_handle *h) {
   cudaFree(h->tr_cfg); cudaFree(h->tr_theta); cudaFree(h->tr_rates); cudaFree(h->tr_rsum);
   cudaFree(h->tr_gw); cudaFree(h->tr_e); cudaFree(h->tr_stats); cudaFree(h->tr_gW);
   cudaFree(h->tr_gb); cudaFree(h->tr_ga); cudaFree(h->ms_W); cudaFree(h->ms_b); cudaFree(h->ms_a);
-  cudaFree(h->ad_m); cudaFree(h->ad_v); cudaFree(h->tr_recs);
+  cudaFree(h->ad_m); cudaFree(h->ad_v); cudaFree(h->tr_recs); cudaFree(h->dist_out);
   delete h;
   return GFMC_OK;
 }
@@ -1163,6 +1165,108 @@ int gfmc_rbm_get_params(gfmc_handle *h, float *W, float *b, float *a) {
 
 int gfmc_rbm_hidden_padded(const gfmc_handle *h) {
   return (h && h->rbm_on) ? h->rbm.Hp : GFMC_ERR_INVALID;
+}
+
+int gfmc_evolve(gfmc_handle *h, int method, double step, double lam, double alw,
+                const uint32_t key[2], long long walker_offset, int n, const void *cfg,
+                const int32_t *parents, int parents_valid, void *cfg_out, double *log_w,
+                double *e_loc, uint64_t *hops, void *stream) {
+  if (!h || !key || n <= 0 || !cfg || !cfg_out || cfg == cfg_out || !log_w || !e_loc ||
+      (parents_valid && !parents) || walker_offset < 0)
+    return fail(GFMC_ERR_INVALID, "gfmc_evolve: bad argument");
+  int rc = check_method(method, step);
+  if (rc) return rc;
+  rc = ensure_scratch(h, n, 1);
+  if (rc) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  GFMC_CUDA(cudaMemsetAsync(h->ctr, 0, sizeof(int), s));
+  if (hops) GFMC_CUDA(cudaMemsetAsync(hops, 0, sizeof(uint64_t), s));
+  EvolveArgs a{};
+  a.method = method;
+  a.step = step;
+  a.lam = lam;
+  a.alw = alw;
+  a.key = Key{key[0], key[1]};
+  a.walker_offset = walker_offset;
+  a.n_walkers = n;
+  a.parents = parents_valid ? parents : nullptr;
+  a.cfg_in = cfg;
+  a.cfg_out = cfg_out;
+  a.log_w = log_w;
+  a.e_loc = e_loc;
+  a.hops = (unsigned long long *)hops;
+  a.work_ctr = h->ctr;
+  a.status = h->status;
+  a.max_iters = h->max_iters;
+  h->field_valid = 0;   // carried state is not kept across a sharded step
+  cudaError_t e;
+  if (h->precision == GFMC_PRECISION_FP64)
+    e = h->rbm_on ? launch_rbm_evolve<double>(h->m64, h->rbm, a, h->rbm_grid, s)
+                  : launch_evolve<double>(h->m64, h->g64, h->plan, a, s);
+  else
+    e = h->rbm_on ? launch_rbm_evolve<float>(h->m32, h->rbm, a, h->rbm_grid, s)
+                  : launch_evolve<float>(h->m32, h->g32, h->plan, a, s);
+  if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "evolve launch: %s", cudaGetErrorString(e));
+  return GFMC_OK;
+}
+
+static int dist_prepare(gfmc_handle *h, int n) {
+  int rc = ensure_scratch(h, n, 1);
+  if (rc) return rc;
+  if (!h->dist_out) GFMC_CUDA(cudaMalloc(&h->dist_out, sizeof(double) * 4));
+  return GFMC_OK;
+}
+
+int gfmc_dist_local_max(gfmc_handle *h, int n, const double *log_w, double *max_out,
+                        void *stream) {
+  if (!h || n <= 0 || !log_w || !max_out)
+    return fail(GFMC_ERR_INVALID, "gfmc_dist_local_max: bad argument");
+  int rc = dist_prepare(h, n);
+  if (rc) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = launch_dist_max(n, log_w, h->psum, h->dist_out, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(max_out, h->dist_out, sizeof(double), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "dist max: %s", cudaGetErrorString(e));
+  return GFMC_OK;
+}
+
+int gfmc_dist_local_sums(gfmc_handle *h, int n, const double *log_w, const double *e_loc,
+                         double shift, double out[3], void *stream) {
+  if (!h || n <= 0 || !log_w || !e_loc || !out)
+    return fail(GFMC_ERR_INVALID, "gfmc_dist_local_sums: bad argument");
+  int rc = dist_prepare(h, n);
+  if (rc) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = launch_dist_sums(n, log_w, e_loc, shift, h->psum, h->pE, h->plp, h->dist_out, s);
+  double tmp[4];
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(tmp, h->dist_out, sizeof(double) * 4, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "dist sums: %s", cudaGetErrorString(e));
+  out[0] = tmp[1];
+  out[1] = tmp[2];
+  out[2] = tmp[3];
+  return GFMC_OK;
+}
+
+int gfmc_dist_parents(gfmc_handle *h, int n, const double *log_w, double shift, double offset,
+                      double S_total, double psi, long long N_total, long long slot_lo, int count,
+                      int last_pos, int32_t *parents_out, void *stream) {
+  if (!h || n <= 0 || !log_w || count < 0 || (count && !parents_out) || N_total <= 0 ||
+      last_pos < 0 || last_pos >= n || slot_lo < 0 || slot_lo + count > N_total)
+    return fail(GFMC_ERR_INVALID, "gfmc_dist_parents: bad argument");
+  int rc = dist_prepare(h, n);
+  if (rc) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  // the tile sums of this shift (the weighted-energy partials are not used)
+  cudaError_t e = launch_dist_sums(n, log_w, log_w, shift, h->psum, h->pE, h->plp, h->dist_out, s);
+  if (e == cudaSuccess)
+    e = launch_dist_parents(n, log_w, shift, offset, h->psum, h->cdf, h->wbuf, psi, S_total,
+                            N_total, slot_lo, count, last_pos, parents_out, s);
+  if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "dist parents: %s", cudaGetErrorString(e));
+  return GFMC_OK;
 }
 
 int gfmc_key_schedule_ex(const uint32_t key[2], int n_steps, int n_sub, uint32_t *keys_out,

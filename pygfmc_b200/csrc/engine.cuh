@@ -107,6 +107,7 @@ struct EvolveArgs {
   float *rates_out;       // EVALUATE, RBM guide: (n_walkers, M - 1) guided rates; nullable
   float *rsum_out;        // EVALUATE, RBM guide: (n_walkers,) sum of those rates; nullable
   double *diag_out;       // EVALUATE: (n_walkers,) diagonal element H_xx; nullable
+  long long walker_offset;  // global index of walker 0 (streams fold_in(key, offset + i))
 };
 
 struct LaunchPlan {
@@ -123,6 +124,17 @@ cudaError_t plan_evolve(const DevModel<T> &m, const DevGuide<T> &g, int n_slots_
                         LaunchPlan *plan);
 // Number of per-warp partial maxima an evolve launch over n_walkers writes.
 int evolve_partials(const LaunchPlan &plan, int n_walkers);
+
+// Sharded reconfiguration pieces (recon_dist.cu), float64.  out: (max, S,
+// sum w e, last positive index).
+int dist_tiles(int n);
+cudaError_t launch_dist_max(int n, const double *lw, double *tmax, double *out, cudaStream_t s);
+cudaError_t launch_dist_sums(int n, const double *lw, const double *e, double shift, double *tS,
+                             double *tE, int *tlp, double *out, cudaStream_t s);
+cudaError_t launch_dist_parents(int n, const double *lw, double shift, double offset,
+                                const double *tS, double *cdf, double *wbuf, double psi,
+                                double S_total, long long N_total, long long i_lo, int count,
+                                int last_pos, int *parents, cudaStream_t s);
 
 // Reconfiguration (reconfig.cu), always float64.
 struct ReconArgs {

@@ -635,7 +635,7 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta
       }
     }
 
-    const Key kw = fold(a.key, (uint32_t)walker);
+    const Key kw = fold(a.key, (uint32_t)(a.walker_offset + walker));
     double lw = 0.0;
     T eloc = T(0);
     int hops = 0;
