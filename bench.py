@@ -173,6 +173,80 @@ def sigma_study(P, args):
     print(json.dumps(line))
 
 
+def rbm_bench(P, args):
+    """Learned-guide workload: 16x16 Heisenberg, RBM guide H = 512 (bf16
+    weights, N(0, 0.01^2)), float32 build, cont_time tau = 0.05.  Times the
+    branching step (L2 flushed before each), one training step
+    (gfmc_rbm_train_step) and the tensor-core theta GEMM."""
+    import torch
+    lat = P.square(L)
+    H = P.SpinHalf.create(lat.edges, J_x=-1.0, J_y=-1.0, J_z=1.0, dtype=np.float64)
+    G = P.RBMSpinHalf(L * L, args.hidden, seed=0, sigma=0.01)
+    n = args.walkers
+    w = P.prepare_walkers_sz(n, L * L, P.PRNGKey(0), sz=0)
+    eng = P.GFMCEngine(H, G, n, precision="mixed")
+    eng.load(w.config)
+    dev = eng.device
+    alw = float((-eng.local_energy()).mean().item())
+    key = P.PRNGKey(1000)
+    wk = max(args.warmup, 3)
+    keys, key = P.engine.key_schedule(key, wk)
+    lg = torch.empty(wk, dtype=torch.float64, device=dev)
+    Ew = torch.empty_like(lg)
+    eng.steps("cont_time", TAU, None, alw, keys, lg, Ew)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    keys, key = P.engine.key_schedule(key, args.steps)
+    logG = torch.empty(1, dtype=torch.float64, device=dev)
+    Es = torch.empty_like(logG)
+    hops = torch.zeros(1, dtype=torch.int64, device=dev)
+    stream = torch.cuda.current_stream()
+    ms, tot_hops = [], 0
+    for st in range(args.steps):
+        flush.fill_(float(st))
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        eng.steps("cont_time", TAU, None, alw, keys[st:st + 1], logG, Es, hops)
+        b.record(stream)
+        b.synchronize()
+        ms.append(a.elapsed_time(b))
+        tot_hops += int(hops.item())
+    step_ms = float(np.mean(ms))
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    eng.rbm_theta()
+    a.record(stream)
+    eng.rbm_theta()
+    b.record(stream)
+    b.synchronize()
+    gemm_ms = a.elapsed_time(b)
+    eng.rbm_train_step(1e-4)
+    torch.cuda.synchronize()
+    a.record(stream)
+    eng.rbm_train_step(1e-4)
+    b.record(stream)
+    b.synchronize()
+    train_ms = a.elapsed_time(b)
+    pk, pk_kind = peaks()
+    Hp = ((args.hidden + 255) // 256) * 256
+    gemm_tflops = 2.0 * n * Hp * 256 / (gemm_ms / 1e3) / 1e12
+    line = {"metric": "walker-steps/s", "value": n / (step_ms / 1e3), "unit": "walker-steps/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": wk, "ms_per_step": step_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+bf16",
+            "data": "synthetic",
+            "config": {"workload": f"heisenberg_16x16_rbm_h{args.hidden}_cont_time", "n_walkers": n,
+                       "tau": TAU, "l2": "flushed (256 MB write) before every timed step",
+                       "hops_per_walker_step": tot_hops / (n * args.steps)},
+            "train_step_ms": train_ms,
+            "roofline": {"bound": "tensor", "kernel": "rbm_theta_kernel", "achieved": gemm_tflops,
+                         "peak": pk["bf16_tflops"], "unit": "TFLOP/s",
+                         "frac": gemm_tflops / pk["bf16_tflops"], "traffic": None,
+                         "peak_source": pk_kind,
+                         "note": "the branching step itself is bound by the log-cosh work and the "
+                                 "weight-row traffic through L1/L2 (see profiles/)"}}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -189,6 +263,9 @@ def main():
     ap.add_argument("--rbm-steps", type=int, default=1000)
     ap.add_argument("--train-iters", type=int, default=600)
     ap.add_argument("--train-lr", type=float, default=3e-4)
+    ap.add_argument("--guide", default="jastrow", choices=["jastrow", "rbm"],
+                    help="rbm: the learned-guide workload (RBM, float32)")
+    ap.add_argument("--hidden", type=int, default=512)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -197,6 +274,12 @@ def main():
     if args.study == "sigma":
         if rank == 0:
             sigma_study(P, args)
+        return
+    if args.guide == "rbm":
+        if args.walkers == N_WALKERS:
+            args.walkers = 65536
+        if rank == 0:
+            rbm_bench(P, args)
         return
 
     if args.impl == "reference":
