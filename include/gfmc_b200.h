@@ -40,6 +40,7 @@ extern "C" {
 #define GFMC_GUIDE_JASTROW_SPIN_HALF 1
 #define GFMC_GUIDE_JASTROW_BOSE_HUBBARD 2
 #define GFMC_GUIDE_RBM_SPIN_HALF 3        /* no counterpart in PyGFMC */
+#define GFMC_GUIDE_MLP_BOSE_HUBBARD 4     /* no counterpart in PyGFMC */
 
 #define GFMC_METHOD_CONT_TIME 0
 #define GFMC_METHOD_SINGLE_STEP 1
@@ -98,6 +99,16 @@ typedef struct {
    * rbm_b (n_hidden), rbm_a (n_sites); n_hidden <= 1024. */
   int n_hidden;
   const float *rbm_W, *rbm_b, *rbm_a;
+  /* MLP (GFMC_GUIDE_MLP_BOSE_HUBBARD; no PyGFMC counterpart; float32 build
+   * only, methods cont_time and the local energy): over the one-hot
+   * occupations x (input k (n_max + 1) + n_k), h1 = tanh(W1 x + b1) rounded
+   * to bfloat16, log psi = w3 . tanh(W2 h1 + b2) + b3.  mlp_W1 (mlp_H1,
+   * n_sites (n_max + 1)) and mlp_W2 (mlp_H2, mlp_H1) row-major, rounded to
+   * bfloat16 on the device, as are mlp_w3 (mlp_H2); mlp_b1, mlp_b2 float32.
+   * mlp_H1 in {64, 128, 192, 256}; mlp_H2 a multiple of 16 in [16, 256]. */
+  int mlp_H1, mlp_H2;
+  const float *mlp_W1, *mlp_b1, *mlp_W2, *mlp_b2, *mlp_w3;
+  double mlp_b3;
 } gfmc_guide_desc;
 
 typedef struct gfmc_handle gfmc_handle;

@@ -101,11 +101,44 @@ typedef struct {
   /* RBM (no PyGFMC counterpart): log psi = sum_h log cosh(b_h + sum_i W_hi s_i) + a.s,
    * W (n_hidden, N) row-major with bfloat16-representable values. */
   int n_hidden; const double *rbm_W, *rbm_b, *rbm_a;
+  /* Bose-Hubbard MLP (no PyGFMC counterpart): one-hot occupations ->
+   * H1 tanh -> (bf16) -> H2 tanh -> w3 . h2 + b3; W1 (H1, N np1), W2 (H2, H1). */
+  int mlp_H1, mlp_H2, mlp_np1;
+  const double *mlp_W1, *mlp_b1, *mlp_W2, *mlp_b2, *mlp_w3;
+  double mlp_b3;
 } om_guide;
 
 /* Extra scratch doubles om_rates needs for a guide (theta and theta'). */
 static inline int om_guide_scratch(const om_guide *g) {
-  return (g && g->kind == 3) ? 2 * g->n_hidden : 0;
+  if (g && g->kind == 3) return 2 * g->n_hidden;
+  if (g && g->kind == 4) return 2 * g->mlp_H1 + 4096;
+  return 0;
+}
+
+/* float64 -> nearest bfloat16 (through float32, ties to even) */
+static double om_bf16(double v) {
+  float f = (float)v;
+  uint32_t u; memcpy(&u, &f, 4);
+  if ((u & 0x7F800000u) != 0x7F800000u) u = (u + 0x7FFFu + ((u >> 16) & 1u)) & 0xFFFF0000u;
+  memcpy(&f, &u, 4);
+  return (double)f;
+}
+
+/* MLP log amplitude of occupations n (length N) */
+static double mlp_logpsi(const om_guide *g, int N, const double *n, double *z1) {
+  const int H1 = g->mlp_H1, H2 = g->mlp_H2, D = N * g->mlp_np1;
+  for (int h = 0; h < H1; ++h) {
+    double z = g->mlp_b1[h];
+    for (int k = 0; k < N; ++k) z += g->mlp_W1[(size_t)h * D + k * g->mlp_np1 + (int)n[k]];
+    z1[h] = om_bf16(tanh(z));
+  }
+  double lp = g->mlp_b3;
+  for (int j = 0; j < H2; ++j) {
+    double z = g->mlp_b2[j];
+    for (int h = 0; h < H1; ++h) z += g->mlp_W2[(size_t)j * H1 + h] * z1[h];
+    lp += g->mlp_w3[j] * tanh(z);
+  }
+  return lp;
 }
 
 /* log cosh(x) - log 2, the RBM hidden-unit term (the constant cancels in
@@ -313,6 +346,18 @@ static void om_rates(const om_model *m, const om_guide *g, const double *x,
       jbh_log_diff(g, m, x, S, ld);
       for (int t = 1; t < M; ++t)
         if (r[t] != 0.0) r[t] *= exp(ld[t]);
+    } else if (g && g->kind == 4) {
+      double *z1 = scratch + M, *y = z1 + g->mlp_H1;
+      const double lp0 = mlp_logpsi(g, m->N, x, z1);
+      for (int t = 1; t < M; ++t) {
+        if (r[t] == 0.0) continue;
+        memcpy(y, x, sizeof(double) * m->N);
+        int a, b, da, db;
+        bose_move(m, t, &a, &b, &da, &db);
+        y[a] += (double)da;
+        y[b] += (double)db;
+        r[t] *= exp(mlp_logpsi(g, m->N, y, z1) - lp0);
+      }
     }
   }
 }

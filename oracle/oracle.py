@@ -62,7 +62,10 @@ class _Guide(ctypes.Structure):
                 ("trans_pw", _dp), ("beta_tied", ctypes.c_int), ("beta0", ctypes.c_double),
                 ("h_mode", ctypes.c_int), ("h0", ctypes.c_double),
                 ("d_mode", ctypes.c_int), ("d0", ctypes.c_double), ("d", _dp),
-                ("n_hidden", ctypes.c_int), ("rbm_W", _dp), ("rbm_b", _dp), ("rbm_a", _dp)]
+                ("n_hidden", ctypes.c_int), ("rbm_W", _dp), ("rbm_b", _dp), ("rbm_a", _dp),
+                ("mlp_H1", ctypes.c_int), ("mlp_H2", ctypes.c_int), ("mlp_np1", ctypes.c_int),
+                ("mlp_W1", _dp), ("mlp_b1", _dp), ("mlp_W2", _dp), ("mlp_b2", _dp), ("mlp_w3", _dp),
+                ("mlp_b3", ctypes.c_double)]
 
 
 def build():
@@ -388,6 +391,22 @@ def rbm_spin_half(W, b, a):
     s.rbm_W = _p(g._arr(W.ravel()))
     s.rbm_b = _p(g._arr(np.broadcast_to(np.asarray(b, np.float64), (H,))))
     s.rbm_a = _p(g._arr(np.broadcast_to(np.asarray(a, np.float64), (N,))))
+    g.s = s
+    return g
+
+
+def mlp_bose_hubbard(W1, b1, W2, b2, w3, b3, n_max):
+    """Bose-Hubbard MLP guide (no reference counterpart): one-hot occupations ->
+    tanh -> bf16 -> tanh -> w3 . h2 + b3, float64 on the given (bf16-valued)
+    weights."""
+    W1 = np.asarray(W1, np.float64); W2 = np.asarray(W2, np.float64)
+    g = OracleModel()
+    s = _Guide()
+    s.kind = 4
+    s.mlp_H1, s.mlp_H2, s.mlp_np1 = W1.shape[0], W2.shape[0], int(n_max) + 1
+    s.mlp_W1 = _p(g._arr(W1.ravel())); s.mlp_b1 = _p(g._arr(b1))
+    s.mlp_W2 = _p(g._arr(W2.ravel())); s.mlp_b2 = _p(g._arr(b2)); s.mlp_w3 = _p(g._arr(w3))
+    s.mlp_b3 = float(b3)
     g.s = s
     return g
 

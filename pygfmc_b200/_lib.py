@@ -23,6 +23,7 @@ GUIDE_NONE = 0
 GUIDE_JASTROW_SPIN_HALF = 1
 GUIDE_JASTROW_BOSE_HUBBARD = 2
 GUIDE_RBM_SPIN_HALF = 3
+GUIDE_MLP_BOSE_HUBBARD = 4
 METHODS = {"cont_time": 0, "single_step": 1, "multi_step": 2}
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
@@ -55,7 +56,10 @@ class GuideDesc(ctypes.Structure):
                 ("beta_tied", ctypes.c_int), ("beta0", ctypes.c_double),
                 ("h_mode", ctypes.c_int), ("h0", ctypes.c_double),
                 ("d_mode", ctypes.c_int), ("d0", ctypes.c_double), ("d", _dp),
-                ("n_hidden", ctypes.c_int), ("rbm_W", _fp), ("rbm_b", _fp), ("rbm_a", _fp)]
+                ("n_hidden", ctypes.c_int), ("rbm_W", _fp), ("rbm_b", _fp), ("rbm_a", _fp),
+                ("mlp_H1", ctypes.c_int), ("mlp_H2", ctypes.c_int), ("mlp_W1", _fp),
+                ("mlp_b1", _fp), ("mlp_W2", _fp), ("mlp_b2", _fp), ("mlp_w3", _fp),
+                ("mlp_b3", ctypes.c_double)]
 
 
 class DiagDesc(ctypes.Structure):

@@ -7,11 +7,13 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/gfmc_b200.h"
 #include "diag.cuh"
 #include "fw.cuh"
+#include "mlp.cuh"
 #include "rbm.cuh"
 #include "engine.cuh"
 
@@ -102,6 +104,11 @@ struct gfmc_handle {
   void *d_rbm = nullptr;
   int rbm_grid = 0;
   int state_len = 0;     // carried state values per walker (N, or Hp for the RBM)
+  // MLP guide (Bose-Hubbard, float32 build): bf16 layer weights, biases
+  int mlp_on = 0;
+  MlpTables mlp{};
+  void *d_mlp = nullptr;
+  int mlp_grid = 0;
   // RBM variance-minimisation scratch (sized for train_cap walkers) and the
   // float32 master parameters with their Adam moments
   int train_cap = 0;
@@ -175,6 +182,84 @@ int build_rbm(gfmc_handle *h, const gfmc_guide_desc *gd, int N) {
   h->carry = 1;
   h->state_len = Hp;
   return GFMC_OK;
+}
+
+// MLP tables: W1 transposed to input-major (D, H1) and W2 (H2, H1), both
+// rounded to bf16; b1, b2 and w3 (rounded to bf16 values) in float.
+int build_mlp(gfmc_handle *h, const gfmc_guide_desc *gd, int N, int n_max) {
+  const int H1 = gd->mlp_H1, H2 = gd->mlp_H2;
+  if (H1 != 64 && H1 != 128 && H1 != 192 && H1 != 256)
+    return fail(GFMC_ERR_INVALID, "mlp_H1 must be 64, 128, 192 or 256, got %d", H1);
+  if (H2 < 16 || H2 > 256 || H2 % 16)
+    return fail(GFMC_ERR_INVALID, "mlp_H2 must be a multiple of 16 in [16, 256], got %d", H2);
+  if (!gd->mlp_W1 || !gd->mlp_b1 || !gd->mlp_W2 || !gd->mlp_b2 || !gd->mlp_w3)
+    return fail(GFMC_ERR_INVALID, "MLP guide: mlp_W1, mlp_b1, mlp_W2, mlp_b2 and mlp_w3 are required");
+  if (n_max < 1 || n_max > 254) return fail(GFMC_ERR_INVALID, "MLP guide: n_max must be in [1, 254]");
+  const int np1 = n_max + 1;
+  const size_t D = (size_t)N * np1;
+  std::vector<uint16_t> W1T(D * H1), W2((size_t)H2 * H1);
+  std::vector<float> b1(H1), b2(H2), w3(H2);
+  for (int j = 0; j < H1; ++j) {
+    for (size_t c = 0; c < D; ++c) {
+      const float w = gd->mlp_W1[(size_t)j * D + c];
+      if (!std::isfinite(w)) return fail(GFMC_ERR_INVALID, "MLP W1 (%d, %zu) is not finite", j, c);
+      W1T[c * H1 + j] = bf16_bits(w);
+    }
+    b1[j] = gd->mlp_b1[j];
+  }
+  for (int i = 0; i < H2; ++i) {
+    for (int j = 0; j < H1; ++j) {
+      const float w = gd->mlp_W2[(size_t)i * H1 + j];
+      if (!std::isfinite(w)) return fail(GFMC_ERR_INVALID, "MLP W2 (%d, %d) is not finite", i, j);
+      W2[(size_t)i * H1 + j] = bf16_bits(w);
+    }
+    b2[i] = gd->mlp_b2[i];
+    const uint32_t u = (uint32_t)bf16_bits(gd->mlp_w3[i]) << 16;
+    memcpy(&w3[i], &u, 4);
+  }
+  const size_t s1 = W1T.size() * 2, s2 = W2.size() * 2;
+  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  const size_t o2 = al(s1), ob1 = o2 + al(s2), ob2 = ob1 + al((size_t)H1 * 4),
+               ow3 = ob2 + al((size_t)H2 * 4), tot = ow3 + al((size_t)H2 * 4);
+  std::vector<unsigned char> host(tot, 0);
+  memcpy(host.data(), W1T.data(), s1);
+  memcpy(host.data() + o2, W2.data(), s2);
+  memcpy(host.data() + ob1, b1.data(), (size_t)H1 * 4);
+  memcpy(host.data() + ob2, b2.data(), (size_t)H2 * 4);
+  memcpy(host.data() + ow3, w3.data(), (size_t)H2 * 4);
+  GFMC_CUDA(cudaMalloc(&h->d_mlp, tot));
+  GFMC_CUDA(cudaMemcpy(h->d_mlp, host.data(), tot, cudaMemcpyHostToDevice));
+  unsigned char *base = (unsigned char *)h->d_mlp;
+  h->mlp.W1T = (const __nv_bfloat16 *)base;
+  h->mlp.W2 = (const __nv_bfloat16 *)(base + o2);
+  h->mlp.b1 = (const float *)(base + ob1);
+  h->mlp.b2 = (const float *)(base + ob2);
+  h->mlp.w3 = (const float *)(base + ow3);
+  h->mlp.b3 = (float)gd->mlp_b3;
+  h->mlp.H1 = H1;
+  h->mlp.H2 = H2;
+  h->mlp.np1 = np1;
+  h->mlp_on = 1;
+  h->mlp_grid = mlp_grid();
+  return GFMC_OK;
+}
+
+// The per-walker step kernel of the handle's guide.
+template <typename T>
+cudaError_t launch_step(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g,
+                        const EvolveArgs &a, cudaStream_t s) {
+  if (h->rbm_on) return launch_rbm_evolve<T>(m, h->rbm, a, h->rbm_grid, s);
+  if constexpr (std::is_same<T, float>::value) {
+    if (h->mlp_on) return launch_mlp_evolve(m, h->mlp, a, h->mlp_grid, s);
+  }
+  return launch_evolve<T>(m, g, h->plan, a, s);
+}
+
+// Per-block partial maxima of log_w a step launch over n walkers writes.
+int step_partials(const gfmc_handle *h, int n) {
+  if (h->rbm_on) return rbm_partials(h->rbm_grid, n);
+  if (h->mlp_on) return std::max(1, std::min(h->mlp_grid, n));
+  return evolve_partials(h->plan, n);
 }
 
 template <typename T>
@@ -257,6 +342,13 @@ int build_tables(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_des
     if (md->kind != GFMC_MODEL_SPIN_HALF)
       return fail(GFMC_ERR_INVALID, "the RBM guide needs a SpinHalf model");
     gk = GFMC_GUIDE_NONE;   // the Jastrow tables stay empty; rbm.cu evaluates the ratios
+  }
+  if (gk == GFMC_GUIDE_MLP_BOSE_HUBBARD) {
+    if (md->kind != GFMC_MODEL_BOSE_HUBBARD)
+      return fail(GFMC_ERR_INVALID, "the MLP guide needs a BoseHubbard model");
+    if (h->precision != GFMC_PRECISION_MIXED)
+      return fail(GFMC_ERR_UNSUPPORTED, "the MLP guide runs in the float32 (mixed) build");
+    gk = GFMC_GUIDE_NONE;   // mlp.cu evaluates the ratios
   }
   if (gk == GFMC_GUIDE_JASTROW_SPIN_HALF && md->kind != GFMC_MODEL_SPIN_HALF)
     return fail(GFMC_ERR_INVALID, "JastrowSpinHalf needs the SpinHalf transition layout");
@@ -488,6 +580,7 @@ int ensure_scratch(gfmc_handle *h, int n, int n_steps) {
   if (!h->pmax) {
     size_t np = (size_t)(h->plan.grid > 0 ? h->plan.grid : 1) * (h->plan.wpb > 0 ? h->plan.wpb : 1);
     if (h->rbm_on) np = std::max(np, (size_t)rbm_partials(h->rbm_grid, h->rbm_grid * 4));
+    if (h->mlp_on) np = std::max(np, (size_t)h->mlp_grid);
     GFMC_CUDA(cudaMalloc(&h->pmax, sizeof(double) * np));
   }
   if (h->carry && n > h->cap_field) {
@@ -521,7 +614,9 @@ int run_steps_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, int 
   GFMC_CUDA(cudaMemsetAsync(h->ctr, 0, sizeof(int) * n_steps, s));
   unsigned long long *hops = hops_out ? (unsigned long long *)hops_out : h->hops;
   GFMC_CUDA(cudaMemsetAsync(hops, 0, sizeof(unsigned long long) * n_steps, s));
-  const int n_partials = h->rbm_on ? rbm_partials(h->rbm_grid, n) : evolve_partials(h->plan, n);
+  if (h->mlp_on && method != CONT_TIME)
+    return fail(GFMC_ERR_UNSUPPORTED, "the MLP guide propagates with cont_time only");
+  const int n_partials = step_partials(h, n);
   void *cur = cfg, *nxt = cfg_tmp;
   for (int st = 0; st < n_steps; ++st) {
     EvolveArgs a{};
@@ -560,8 +655,7 @@ int run_steps_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, int 
       h->field_cfg = cfg;
       h->since_refresh = fresh ? 1 : h->since_refresh + 1;
     }
-    cudaError_t e = h->rbm_on ? launch_rbm_evolve<T>(m, h->rbm, a, h->rbm_grid, s)
-                              : launch_evolve<T>(m, g, h->plan, a, s);
+    cudaError_t e = launch_step<T>(h, m, g, a, s);
     if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "evolve launch: %s", cudaGetErrorString(e));
     ReconArgs r{};
     r.n = n;
@@ -638,8 +732,8 @@ int single_launch_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, 
 
 int single_launch(gfmc_handle *h, int method, Key key, int n, const void *cfg,
                   const int32_t *parents, void *cfg_out, double *out, cudaStream_t s) {
-  if (h->rbm_on)
-    return fail(GFMC_ERR_UNSUPPORTED, "measurement operators under an RBM guide are not built");
+  if (h->rbm_on || h->mlp_on)
+    return fail(GFMC_ERR_UNSUPPORTED, "measurement operators under a learned guide are not built");
   if (h->precision == GFMC_PRECISION_FP64)
     return single_launch_t<double>(h, h->m64, h->g64, method, key, n, cfg, parents, cfg_out, out, s);
   return single_launch_t<float>(h, h->m32, h->g32, method, key, n, cfg, parents, cfg_out, out, s);
@@ -763,8 +857,7 @@ int local_energy_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, i
   a.partial_max = nullptr;
   a.status = h->status;
   a.max_iters = 1;
-  cudaError_t e = h->rbm_on ? launch_rbm_evolve<T>(m, h->rbm, a, h->rbm_grid, s)
-                            : launch_evolve<T>(m, g, h->plan, a, s);
+  cudaError_t e = launch_step<T>(h, m, g, a, s);
   if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "local energy launch: %s", cudaGetErrorString(e));
   return GFMC_OK;
 }
@@ -804,6 +897,17 @@ int gfmc_create(const gfmc_model_desc *model, const gfmc_guide_desc *guide, int 
       return rc;
     }
   }
+  if (guide && guide->kind == GFMC_GUIDE_MLP_BOSE_HUBBARD) {
+    rc = build_mlp(h, guide, h->N, h->n_max);
+    if (rc == GFMC_OK &&
+        mlp_smem_bytes(h->mlp.H1, h->mlp.H2, h->M - 1, h->N) > (size_t)227 * 1024)
+      rc = fail(GFMC_ERR_UNSUPPORTED, "MLP guide: %d moves with (%d, %d) hidden units exceed "
+                "the shared memory of one SM", h->M - 1, h->mlp.H1, h->mlp.H2);
+    if (rc) {
+      gfmc_destroy(h);
+      return rc;
+    }
+  }
   // float32 factors drift faster under the multiplicative updates
   h->refresh_every = precision == GFMC_PRECISION_FP64 ? 100 : 50;
   *out = h;
@@ -821,6 +925,7 @@ int gfmc_destroy(gfmc_handle *h) {
   cudaFree(h->diag.ring_vals); cudaFree(h->diag_partial);
   cudaFree(h->fw_partial); cudaFree(h->fw_logG); cudaFree(h->fw_E); cudaFree(h->ctr1);
   cudaFree(h->d_rbm);
+  cudaFree(h->d_mlp);
   cudaFree(h->tr_cfg); cudaFree(h->tr_theta); cudaFree(h->tr_rates); cudaFree(h->tr_rsum);
   cudaFree(h->tr_gw); cudaFree(h->tr_e); cudaFree(h->tr_stats); cudaFree(h->tr_gW);
   cudaFree(h->tr_gb); cudaFree(h->tr_ga); cudaFree(h->ms_W); cudaFree(h->ms_b); cudaFree(h->ms_a);
@@ -1176,6 +1281,8 @@ int gfmc_evolve(gfmc_handle *h, int method, double step, double lam, double alw,
     return fail(GFMC_ERR_INVALID, "gfmc_evolve: bad argument");
   int rc = check_method(method, step);
   if (rc) return rc;
+  if (h->mlp_on && method != CONT_TIME)
+    return fail(GFMC_ERR_UNSUPPORTED, "the MLP guide propagates with cont_time only");
   rc = ensure_scratch(h, n, 1);
   if (rc) return rc;
   cudaStream_t s = (cudaStream_t)stream;
@@ -1201,11 +1308,9 @@ int gfmc_evolve(gfmc_handle *h, int method, double step, double lam, double alw,
   h->field_valid = 0;   // carried state is not kept across a sharded step
   cudaError_t e;
   if (h->precision == GFMC_PRECISION_FP64)
-    e = h->rbm_on ? launch_rbm_evolve<double>(h->m64, h->rbm, a, h->rbm_grid, s)
-                  : launch_evolve<double>(h->m64, h->g64, h->plan, a, s);
+    e = launch_step<double>(h, h->m64, h->g64, a, s);
   else
-    e = h->rbm_on ? launch_rbm_evolve<float>(h->m32, h->rbm, a, h->rbm_grid, s)
-                  : launch_evolve<float>(h->m32, h->g32, h->plan, a, s);
+    e = launch_step<float>(h, h->m32, h->g32, a, s);
   if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "evolve launch: %s", cudaGetErrorString(e));
   return GFMC_OK;
 }

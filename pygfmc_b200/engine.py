@@ -24,7 +24,7 @@ from . import _lib
 from . import random as _rnd
 from .hamiltonian import BoseHubbard, SpinHalf
 from .walkers import Walker
-from .wavefunction import JastrowBoseHubbard, JastrowSpinHalf, RBMSpinHalf
+from .wavefunction import JastrowBoseHubbard, JastrowSpinHalf, MLPBoseHubbard, RBMSpinHalf
 from .estimators import (autocorrelation_stats, diagonal_estimates, off_diagonal_estimates,
                          validated_p_array, windowed_energy_host)
 
@@ -140,10 +140,11 @@ def require_guide_protocol(guide):
         raise TypeError(f"Guide {type(guide).__name__!r} must implement at least one of "
                         "log_diff_from_operator, log_diff_from_configs, or log_psi "
                         "(the guide protocol, pygfmc.Guide).")
-    if not isinstance(guide, (JastrowSpinHalf, JastrowBoseHubbard, RBMSpinHalf)) and \
+    if not isinstance(guide, (JastrowSpinHalf, JastrowBoseHubbard, RBMSpinHalf, MLPBoseHubbard)) and \
             not hasattr(guide, "_gfmc_guide_desc"):
         raise TypeError(f"Guide {type(guide).__name__!r} has no device implementation in the B200 "
-                        "engine (supported: JastrowSpinHalf, JastrowBoseHubbard, RBMSpinHalf).")
+                        "engine (supported: JastrowSpinHalf, JastrowBoseHubbard, RBMSpinHalf, "
+                        "MLPBoseHubbard).")
 
 
 def model_desc(op, keep):
@@ -260,6 +261,18 @@ def guide_desc(guide, op, keep):
         g.kind = _lib.GUIDE_RBM_SPIN_HALF
         g.n_hidden = guide.n_hidden
         g.rbm_W, g.rbm_b, g.rbm_a = keep.f32(guide.W), keep.f32(guide.b), keep.f32(guide.a)
+        return g
+    if isinstance(guide, MLPBoseHubbard):
+        if not _is_bose(op):
+            raise TypeError(f"MLPBoseHubbard needs a BoseHubbard operator; got {type(op).__name__}")
+        if guide.N != int(op.N) or guide.n_max != int(op.n_max):
+            raise ValueError(f"MLPBoseHubbard is built for {guide.N} sites with n_max {guide.n_max}; "
+                             f"the operator has {int(op.N)} sites with n_max {int(op.n_max)}")
+        g.kind = _lib.GUIDE_MLP_BOSE_HUBBARD
+        g.mlp_H1, g.mlp_H2 = guide.H1, guide.H2
+        g.mlp_W1, g.mlp_b1 = keep.f32(guide.W1), keep.f32(guide.b1)
+        g.mlp_W2, g.mlp_b2 = keep.f32(guide.W2), keep.f32(guide.b2)
+        g.mlp_w3, g.mlp_b3 = keep.f32(guide.w3), float(guide.b3)
         return g
     raise TypeError(f"Guide {type(guide).__name__!r} has no device implementation")
 
@@ -792,7 +805,9 @@ def run_gfmc(walkers, n_steps, hamiltonian, step_size, guide, p_array, *, method
             "avg_log_weight=stats['avg_log_weight'] of the run being continued (run_from_HDF5 does "
             f"this), or leave warmup_steps unset for the default warm-up of {DEFAULT_WARMUP_STEPS} steps.")
     if precision is None:
-        precision = "fp64" if weight_dtype == np.float64 else "mixed"
+        # the MLP guide's kernel exists in the float32 build only
+        precision = "fp64" if weight_dtype == np.float64 and not isinstance(guide, MLPBoseHubbard) \
+            else "mixed"
     step_f = float(step_size)
 
     torch = _torch()

@@ -14,7 +14,7 @@ import numpy as np
 
 from .hamiltonian import BoseHubbard, edges_array
 
-__all__ = ["JastrowSpinHalf", "JastrowBoseHubbard", "RBMSpinHalf", "round_bf16"]
+__all__ = ["JastrowSpinHalf", "JastrowBoseHubbard", "RBMSpinHalf", "MLPBoseHubbard", "round_bf16"]
 
 LAYOUT_ATTRS = ("n_hx_static", "n_jpm_static", "edge_i", "edge_j")
 
@@ -229,3 +229,57 @@ class RBMSpinHalf:
             y[i], y[j] = -y[i], -y[j]
             out[1 + op.n_hx_static + e] = self.log_psi(y) - self.log_psi(x)
         return out
+
+
+def _bf16_round64(x):
+    """float64 values rounded through float32 to the nearest bfloat16."""
+    return round_bf16(np.asarray(x, dtype=np.float32)).astype(np.float64)
+
+
+class MLPBoseHubbard:
+    """Dense log-amplitude MLP guide for Bose-Hubbard occupations:
+
+        x = one-hot occupations (site k, occupation n -> input k (n_max + 1) + n)
+        h1 = tanh(W1 x + b1),  h2 = tanh(W2 bf16(h1) + b2),  log psi = w3 . h2 + b3
+
+    W1 (H1, N (n_max + 1)), W2 (H2, H1) and w3 (H2,) hold bfloat16 values; the
+    biases are float32.  The first layer's activations enter the second as
+    bf16, as the tensor-core kernel consumes them.  No PyGFMC counterpart (its
+    learned guides are NetKet-trained cluster models).  H1 in {64, 128, 192,
+    256}, H2 a multiple of 16 up to 256."""
+
+    def __init__(self, N, n_max, hidden=(256, 256), W1=None, b1=None, W2=None, b2=None, w3=None,
+                 b3=0.0, seed=0, sigma=0.05, dtype=np.float32):
+        N, n_max = int(N), int(n_max)
+        H1, H2 = (int(hidden), int(hidden)) if np.ndim(hidden) == 0 else (int(hidden[0]), int(hidden[1]))
+        if H1 not in (64, 128, 192, 256) or H2 < 16 or H2 > 256 or H2 % 16:
+            raise ValueError(f"hidden sizes ({H1}, {H2}): H1 must be 64, 128, 192 or 256 and H2 a "
+                             "multiple of 16 up to 256")
+        if n_max < 1 or N < 1:
+            raise ValueError("N and n_max must be positive")
+        D = N * (n_max + 1)
+        rng = np.random.default_rng(seed)
+        W1 = rng.normal(0.0, sigma, (H1, D)) if W1 is None else np.asarray(W1, np.float64)
+        W2 = rng.normal(0.0, sigma, (H2, H1)) if W2 is None else np.asarray(W2, np.float64)
+        w3 = rng.normal(0.0, sigma, H2) if w3 is None else np.asarray(w3, np.float64)
+        if W1.shape != (H1, D) or W2.shape != (H2, H1) or w3.shape != (H2,):
+            raise ValueError("W1, W2, w3 shapes do not match (H1, N (n_max + 1)), (H2, H1), (H2,)")
+        self.N, self.n_max, self.H1, self.H2 = N, n_max, H1, H2
+        self.dtype = np.dtype(dtype)
+        self.W1, self.W2, self.w3 = round_bf16(W1), round_bf16(W2), round_bf16(w3)
+        self.b1 = np.broadcast_to(np.asarray(0.0 if b1 is None else b1, np.float32), (H1,)).copy()
+        self.b2 = np.broadcast_to(np.asarray(0.0 if b2 is None else b2, np.float32), (H2,)).copy()
+        self.b3 = float(np.float32(b3))
+
+    def log_psi(self, config):
+        n = np.asarray(config, dtype=np.float64)
+        idx = np.arange(self.N) * (self.n_max + 1) + n.astype(np.int64)
+        z1 = self.W1.astype(np.float64)[:, idx].sum(-1).T if n.ndim > 1 else \
+            self.W1.astype(np.float64)[:, idx].sum(-1)
+        z1 = z1 + self.b1.astype(np.float64)
+        h1 = _bf16_round64(np.tanh(z1))
+        h2 = np.tanh(h1 @ self.W2.astype(np.float64).T + self.b2.astype(np.float64))
+        return h2 @ self.w3.astype(np.float64) + self.b3
+
+    def log_diff_from_configs(self, config, new_configs):
+        return self.log_psi(new_configs) - self.log_psi(config)
