@@ -247,6 +247,95 @@ def rbm_bench(P, args):
     print(json.dumps(line))
 
 
+def bose_chain(P):
+    """Bose-Hubbard ring of 64 sites, 64 bosons, n_max = 4, t = 1, U = 3
+    (M = 129), with the Gutzwiller + density-Jastrow guide."""
+    e = P.chain(64).edges
+    H = P.BoseHubbard.create(e, t=1.0, U=3.0, n_max=4, dtype=np.float64)
+    GJ = P.JastrowBoseHubbard(64, e, beta=0.05, d=0.3)
+    return e, H, GJ
+
+
+def timed_steps(P, eng, alw, tau, steps, warmup, key):
+    """Mean CUDA-event time of one cont_time branching step (L2 flushed by a
+    256 MB write before each) and the hops per walker-step."""
+    import torch
+    dev = eng.device
+    keys, key = P.engine.key_schedule(key, warmup)
+    lg = torch.empty(warmup, dtype=torch.float64, device=dev)
+    eng.steps("cont_time", tau, None, alw, keys, lg, torch.empty_like(lg))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    keys, key = P.engine.key_schedule(key, steps)
+    logG = torch.empty(1, dtype=torch.float64, device=dev)
+    Es = torch.empty_like(logG)
+    hops = torch.zeros(1, dtype=torch.int64, device=dev)
+    stream = torch.cuda.current_stream()
+    ms, tot_hops = [], 0
+    for st in range(steps):
+        flush.fill_(float(st))
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        eng.steps("cont_time", tau, None, alw, keys[st:st + 1], logG, Es, hops)
+        b.record(stream)
+        b.synchronize()
+        ms.append(a.elapsed_time(b))
+        tot_hops += int(hops.item())
+    return float(np.mean(ms)), tot_hops / (eng.n * steps)
+
+
+def mlp_bench(P, args):
+    """Learned-guide workload for bosons: the 64-site Bose-Hubbard ring with
+    64 bosons (n_max = 4, t = 1, U = 3; M = 129), dense MLP guide
+    320 -> 256 -> 256 -> 1 (tanh, bf16 weights N(0, 0.01^2)), float32 build,
+    32768 walkers drawn uniformly with sum n = 64, cont_time tau = 0.02.
+    Times the MLP-guided branching step and, beside it, the same step under
+    the Gutzwiller + density-Jastrow guide (float64 and float32 builds)."""
+    import torch
+    e, H, GJ = bose_chain(P)
+    hid = min(args.hidden, 256)
+    G = P.MLPBoseHubbard(64, 4, hidden=(hid, hid), seed=0, sigma=0.01)
+    n = args.walkers
+    w = P.prepare_walkers_occupations(n, 64, 64, 4, P.PRNGKey(0))
+    tau = 0.02
+    wk = max(args.warmup, 3)
+    out = {}
+    for name, guide, prec in (("mlp", G, "mixed"), ("jastrow_fp64", GJ, "fp64"),
+                              ("jastrow_mixed", GJ, "mixed")):
+        eng = P.GFMCEngine(H, guide, n, precision=prec)
+        eng.load(w.config)
+        alw = float((-eng.local_energy()).mean().item())
+        ms, hpw = timed_steps(P, eng, alw, tau, args.steps, wk, P.PRNGKey(1000))
+        out[name] = (ms, hpw)
+        del eng
+        torch.cuda.synchronize()
+    ms, hpw = out["mlp"]
+    # tiles of 128 moves per walker-step: the walker's own amplitude, then one
+    # rate evaluation per hop and one for the final hold (M - 1 = 128 moves)
+    tiles = n * (2.0 + hpw)
+    tflops = 2.0 * 128 * hid * hid * tiles / (ms / 1e3) / 1e12
+    pk, pk_kind = peaks()
+    line = {"metric": "walker-steps/s", "value": n / (ms / 1e3), "unit": "walker-steps/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": wk, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+bf16",
+            "data": "synthetic",
+            "config": {"workload": f"bose_hubbard_ring64_mlp_{hid}x{hid}_cont_time", "n_walkers": n,
+                       "tau": tau, "l2": "flushed (256 MB write) before every timed step",
+                       "hops_per_walker_step": hpw},
+            "jastrow_fp64": {"value": n / (out["jastrow_fp64"][0] / 1e3),
+                             "ms_per_step": out["jastrow_fp64"][0]},
+            "jastrow_mixed": {"value": n / (out["jastrow_mixed"][0] / 1e3),
+                              "ms_per_step": out["jastrow_mixed"][0]},
+            "roofline": {"bound": "tensor", "kernel": "mlp_evolve_kernel", "achieved": tflops,
+                         "peak": pk["bf16_tflops"], "unit": "TFLOP/s",
+                         "frac": tflops / pk["bf16_tflops"], "traffic": None,
+                         "peak_source": pk_kind,
+                         "note": "second-layer MMA flops (128 x H x H per tile) over the whole step; "
+                                 "the step is bound by the first-layer rows and tanh on the CUDA "
+                                 "cores (see profiles/)"}}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -263,8 +352,9 @@ def main():
     ap.add_argument("--rbm-steps", type=int, default=1000)
     ap.add_argument("--train-iters", type=int, default=600)
     ap.add_argument("--train-lr", type=float, default=3e-4)
-    ap.add_argument("--guide", default="jastrow", choices=["jastrow", "rbm"],
-                    help="rbm: the learned-guide workload (RBM, float32)")
+    ap.add_argument("--guide", default="jastrow", choices=["jastrow", "rbm", "mlp"],
+                    help="rbm: the learned-guide workload (RBM, float32); mlp: the Bose-Hubbard "
+                         "ring with the dense MLP guide")
     ap.add_argument("--hidden", type=int, default=512)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -280,6 +370,10 @@ def main():
             args.walkers = 65536
         if rank == 0:
             rbm_bench(P, args)
+        return
+    if args.guide == "mlp":
+        if rank == 0:
+            mlp_bench(P, args)
         return
 
     if args.impl == "reference":

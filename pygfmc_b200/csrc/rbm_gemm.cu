@@ -17,6 +17,7 @@
 #include <cuda_bf16.h>
 
 #include "rbm.cuh"
+#include "tc05.cuh"
 
 namespace gfmc {
 namespace {
@@ -24,96 +25,10 @@ namespace {
 constexpr int GT = 128;            // threads = walkers per CTA = UMMA M
 constexpr int KC = 64;             // visible sites per chunk (one 128-byte swizzle row)
 constexpr int MAXN = 512;          // TMEM columns per pass
-constexpr uint32_t WAIT_LIMIT = 1u << 26;
+using namespace tc;
 
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}\n"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// Bounded wait on the mbarrier phase; false when the limit ran out.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-  for (uint32_t it = 0; it < WAIT_LIMIT; ++it)
-    if (mbar_try_wait(bar, parity)) return true;
-  return false;
-}
-
-// CTA-uniform bounded wait: thread 0 waits, every thread gets its verdict
-// (so all threads leave or stay in the loops together).
-__device__ __forceinline__ bool cta_wait(uint64_t *bar, uint32_t parity, volatile int *flag) {
-  if (threadIdx.x == 0) *flag = mbar_wait(bar, parity) ? 1 : 0;
-  __syncthreads();
-  const bool r = *flag != 0;
-  __syncthreads();
-  return r;
-}
-
-// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
-// 1024 bytes apart (SBO), version 1 (sm_100).
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
-  d |= (uint64_t)1u << 16;                 // LBO (unused by swizzled K-major)
-  d |= (uint64_t)(1024u >> 4) << 32;       // SBO
-  d |= (uint64_t)1u << 46;                 // version
-  d |= (uint64_t)2u << 61;                 // SWIZZLE_128B
-  return d;
-}
-
-// Instruction descriptor: D f32, A and B bf16, both K-major, M = 128, N = 256.
-constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((256u >> 3) << 17) |
-                           ((128u >> 4) << 24);
-
-__device__ __forceinline__ void mma_bf16(uint32_t dtmem, uint64_t adesc, uint64_t bdesc,
-                                         uint32_t accum) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dtmem),
-      "l"(adesc), "l"(bdesc), "r"(IDESC), "r"(accum));
-}
-
-__device__ __forceinline__ void mma_commit(uint64_t *bar) {
-  asm volatile(
-      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-          smem_u32(bar))
-      : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
-        "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-// Row r of a 128-byte-swizzled K-major tile: logical 16-byte chunk c lives
-// at chunk c ^ (r & 7).
-__device__ __forceinline__ unsigned char *sw_chunk(unsigned char *tile, int r, int c) {
-  return tile + (size_t)r * 128 + (size_t)((c ^ (r & 7)) * 16);
-}
+// D f32, A and B bf16, both K-major, M = 128, N = 256.
+constexpr uint32_t IDESC = idesc_m128(256u);
 
 __global__ void __launch_bounds__(GT, 1)
 rbm_theta_kernel(const uint64_t *cfg, const int *parents, int NW, int n, int Np,
@@ -187,7 +102,7 @@ rbm_theta_kernel(const uint64_t *cfg, const int *parents, int NW, int n, int Np,
           for (int kk = 0; kk < KC / 16; ++kk) {
             const uint64_t ad = sw128_desc(a0 + 32u * kk);
             const uint64_t bd = sw128_desc(b0 + (uint32_t)sub * 256u * 128u + 32u * kk);
-            mma_bf16(tmem + (uint32_t)sub * 256u, ad, bd, (kc > 0 || kk > 0) ? 1u : 0u);
+            mma_bf16(tmem + (uint32_t)sub * 256u, ad, bd, IDESC, (kc > 0 || kk > 0) ? 1u : 0u);
           }
         }
         mma_commit(bar);

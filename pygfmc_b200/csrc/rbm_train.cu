@@ -23,99 +23,19 @@
 #include <cuda_bf16.h>
 
 #include "rbm.cuh"
+#include "tc05.cuh"
 
 namespace gfmc {
 namespace {
 
 constexpr int TT = 128;     // threads = hidden units per tile = UMMA M
 constexpr int KR = 64;      // rows per chunk = UMMA K per chunk
-constexpr uint32_t WAIT_LIMIT = 1u << 26;
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}\n"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-  for (uint32_t it = 0; it < WAIT_LIMIT; ++it)
-    if (mbar_try_wait(bar, parity)) return true;
-  return false;
-}
-
-// CTA-uniform bounded wait: thread 0 waits, every thread gets its verdict
-// (so all threads leave or stay in the loops together).
-__device__ __forceinline__ bool cta_wait(uint64_t *bar, uint32_t parity, volatile int *flag) {
-  if (threadIdx.x == 0) *flag = mbar_wait(bar, parity) ? 1 : 0;
-  __syncthreads();
-  const bool r = *flag != 0;
-  __syncthreads();
-  return r;
-}
-
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
-  d |= (uint64_t)1u << 16;
-  d |= (uint64_t)(1024u >> 4) << 32;
-  d |= (uint64_t)1u << 46;
-  d |= (uint64_t)2u << 61;
-  return d;
-}
-
-// D f32, A and B bf16, K-major, M = 128, N = n (multiple of 16, <= 256).
-__device__ __forceinline__ uint32_t idesc_n(uint32_t n) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((128u >> 4) << 24);
-}
-
-__device__ __forceinline__ void mma_bf16(uint32_t dtmem, uint64_t adesc, uint64_t bdesc,
-                                         uint32_t idesc, uint32_t accum) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dtmem),
-      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum));
-}
-
-__device__ __forceinline__ void mma_commit(uint64_t *bar) {
-  asm volatile(
-      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-          smem_u32(bar))
-      : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
-        "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
+using namespace tc;
 
 __device__ __forceinline__ float tanh_approx(float x) {
   float y;
   asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
-}
-
-__device__ __forceinline__ unsigned char *sw_chunk(unsigned char *tile, int r, int c) {
-  return tile + (size_t)r * 128 + (size_t)((c ^ (r & 7)) * 16);
 }
 
 __device__ __forceinline__ uint32_t bf16_pair(float lo, float hi) {
@@ -408,7 +328,7 @@ __global__ void __launch_bounds__(3 * TT, 1) rbm_grad_kernel(GradArgs g, const f
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const uint32_t a0 = smem_u32(base + (st ? P.A1 : P.A0));
       const uint32_t b0 = smem_u32(base + (st ? P.B1 : P.B0));
-      const uint32_t id = idesc_n((uint32_t)Np);
+      const uint32_t id = idesc_m128((uint32_t)Np);
 #pragma unroll
       for (int kk = 0; kk < KR / 16; ++kk)
         mma_bf16(tmem, sw128_desc(a0 + 32u * kk), sw128_desc(b0 + 32u * kk), id,
