@@ -310,9 +310,11 @@ def mlp_bench(P, args):
         del eng
         torch.cuda.synchronize()
     ms, hpw = out["mlp"]
-    # tiles of 128 moves per walker-step: the walker's own amplitude, then one
-    # rate evaluation per hop and one for the final hold (M - 1 = 128 moves)
-    tiles = n * (2.0 + hpw)
+    # tiles of 128 moves per walker-step: one rate evaluation per hop and one
+    # for the final hold (M - 1 = 128 moves); the walker's own amplitude is
+    # carried (its tile on the steps that rebuild the carried state, every
+    # 50th, is not counted)
+    tiles = n * (1.0 + hpw)
     tflops = 2.0 * 128 * hid * hid * tiles / (ms / 1e3) / 1e12
     pk, pk_kind = peaks()
     line = {"metric": "walker-steps/s", "value": n / (ms / 1e3), "unit": "walker-steps/s",

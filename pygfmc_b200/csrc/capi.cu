@@ -241,6 +241,8 @@ int build_mlp(gfmc_handle *h, const gfmc_guide_desc *gd, int N, int n_max) {
   h->mlp.np1 = np1;
   h->mlp_on = 1;
   h->mlp_grid = mlp_grid();
+  h->carry = 1;            // z1 and log psi per walker (float32)
+  h->state_len = H1 + 1;
   return GFMC_OK;
 }
 
@@ -258,7 +260,7 @@ cudaError_t launch_step(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> 
 // Per-block partial maxima of log_w a step launch over n walkers writes.
 int step_partials(const gfmc_handle *h, int n) {
   if (h->rbm_on) return rbm_partials(h->rbm_grid, n);
-  if (h->mlp_on) return std::max(1, std::min(h->mlp_grid, n));
+  if (h->mlp_on) return mlp_partials(h->mlp_grid, n);
   return evolve_partials(h->plan, n);
 }
 
@@ -580,7 +582,7 @@ int ensure_scratch(gfmc_handle *h, int n, int n_steps) {
   if (!h->pmax) {
     size_t np = (size_t)(h->plan.grid > 0 ? h->plan.grid : 1) * (h->plan.wpb > 0 ? h->plan.wpb : 1);
     if (h->rbm_on) np = std::max(np, (size_t)rbm_partials(h->rbm_grid, h->rbm_grid * 4));
-    if (h->mlp_on) np = std::max(np, (size_t)h->mlp_grid);
+    if (h->mlp_on) np = std::max(np, (size_t)mlp_partials(h->mlp_grid, h->mlp_grid));
     GFMC_CUDA(cudaMalloc(&h->pmax, sizeof(double) * np));
   }
   if (h->carry && n > h->cap_field) {

@@ -4,23 +4,40 @@
 //   x = one-hot occupations, z1 = W1 x + b1, h1 = tanh(z1),
 //   log psi = w3 . tanh(W2 bf16(h1) + b2) + b3
 //
-// One CTA (4 warps) per SM, persistent over walkers (atomic work counter).
-// W2 (H2 x H1, bf16) is staged once per CTA in shared memory in the 128-byte
-// swizzled K-major layout (the MMA's B operand).  For a walker, z1 is built
-// from the W1 columns of its occupations and updated per move.  A rate
-// evaluation takes the moves in tiles of 128: the moves' first-layer
-// activations h1' = tanh(z1 + W1[:, new] - W1[:, old]) (two sites, four
-// columns) are written as bf16 rows of the A tile, one tcgen05.mma
-// (kind::f16, M = 128 moves, N = H2, K = H1) per tile computes every
-// successor's second-layer pre-activations into TMEM, and the epilogue
-// (tcgen05.ld, thread = move) forms log psi(x') and the guided rate
-// coupling * exp(log psi(x') - log psi(x)).  The walker's own log psi comes
-// from the same path (a tile whose row 0 is the current configuration), so
-// every ratio is a ratio of one function.  The draw and the hold follow the
-// cont_time propagator of evolve.cu (same per-walker Threefry streams).
+// One CTA per SM, persistent over walkers (atomic work counter), running two
+// independent walker pipelines of 8 warps each (named barriers), so that one
+// pipeline computes while the other waits on its tensor-core work or draws
+// its move.  W2 (H2 x H1, bf16) is staged once per CTA in shared memory in
+// the 128-byte swizzled K-major layout (the MMA's B operand, shared by both
+// pipelines).  For a walker, z1 is carried from step to step through the
+// parent map (field_in / field_out, with log psi: H1 + 1 floats per walker;
+// rebuilt from the W1 columns of the occupations when the engine refreshes
+// the carried state) and updated per move.  A rate evaluation takes the
+// moves in tiles of 128 rows, two threads per row (warps w and w + 4 of the
+// pipeline share TMEM lanes 32 (w % 4)):
+//   1. one thread per row decodes its move (sites, W1 columns, unguided
+//      element);
+//   2. per chunk of 64 inputs, the two threads write half the row of the A
+//      chunk each,
+//      the activations h1' = tanh(z1 + W1[:, new] - W1[:, old]) as bf16
+//      (four W1 columns for a two-site move, read as 16-byte vectors); the
+//      chunks go through a ring of two buffers, and the pipeline's leader
+//      issues tcgen05.mma (kind::f16, M = 128 moves, N = H2, K = 64) on a
+//      chunk while the next one is built;
+//   3. the epilogue (tcgen05.ld, each thread half the columns of its row)
+//      forms log psi(x') = w3 . tanh(v + b2) (up to the constant b3 + sum w3,
+//      which cancels in
+//      every ratio) and the guided element coupling * exp(log psi(x') -
+//      log psi(x)).
+// Rows of moves with no element are neither built nor read.  The walker's
+// own log psi comes from the same path (a tile whose row 0 is the current
+// configuration), so every ratio is a ratio of one function.  The
+// pipeline's first warp then forms the diagonal element, scans the rates
+// and draws the move and the hold as the cont_time propagator of evolve.cu
+// does (the same per-walker Threefry streams).
 //
-// Roofline: tensor + special-function bound: 2 * 128 * H1 * H2 flops and
-// 128 (H1 + H2) tanh per tile, W1 columns (4 x H1 bf16 per move) from L1/L2.
+// Roofline: per tile 2 * 128 * H1 * H2 tensor flops, 128 (H1 + H2) tanh (two
+// MUFU operations each) and 128 x 4 W1 columns (2 H1 bytes each) from L2.
 #include <cfloat>
 #include <cuda_bf16.h>
 
@@ -32,7 +49,33 @@ namespace {
 
 using namespace tc;
 
-constexpr int MT = 128;                 // threads = moves per tile = UMMA M
+constexpr int ROWS = 128;               // moves per tile = UMMA M = TMEM lanes
+constexpr int PT = 2 * ROWS;            // threads per pipeline: two per row
+constexpr int NP = 2;                   // walker pipelines per CTA
+constexpr int MT = PT * NP;
+constexpr int KC = 64;                  // inputs per A chunk (one 128-byte swizzle row)
+constexpr int NBUF = 2;                 // A chunk buffers per pipeline
+constexpr unsigned FULLW = 0xffffffffu;
+
+// tanh y = 1 - 2 / (1 + e^{2y}) with e^{2y} = 2^{K y}, K = 2 log2(e): one
+// ex2 and one rcp (absolute error about 1e-7; e^{2y} overflowing to inf
+// gives 1, underflowing to 0 gives -1).
+constexpr float KT = 2.8853900817779268f;
+
+__device__ __forceinline__ float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+__device__ __forceinline__ float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// 1 / (1 + e^{2y}) from Ky = K y: tanh y = 1 - 2 of it.
+__device__ __forceinline__ float sig2(float Ky) { return rcp_approx(1.0f + ex2_approx(Ky)); }
 
 // Moves of the Bose-Hubbard layout (bose_hubbard.py; _common.two_site_move):
 // sites a, b, occupation changes da, db (b == a, db = 0 for the single-site
@@ -85,45 +128,98 @@ __device__ __forceinline__ Mv mlp_move(const DevModel<float> &m, const uint8_t *
   return mv;
 }
 
-// z1 after move mv for the units j, j + 1 (the same expression as the rows
-// of the A tile, so state and ratios agree bit for bit)
-__device__ __forceinline__ float2 z1_moved(const MlpTables &t, const uint8_t *occ, const Mv &mv,
-                                           int np1, float2 z, int j) {
-  const int ca0 = mv.a * np1 + occ[mv.a], ca1 = ca0 + mv.da;
-  const __nv_bfloat162 wa1 = *reinterpret_cast<const __nv_bfloat162 *>(t.W1T + (size_t)ca1 * t.H1 + j);
-  const __nv_bfloat162 wa0 = *reinterpret_cast<const __nv_bfloat162 *>(t.W1T + (size_t)ca0 * t.H1 + j);
-  z.x = (z.x + __low2float(wa1)) - __low2float(wa0);
-  z.y = (z.y + __high2float(wa1)) - __high2float(wa0);
+// W1 columns a move exchanges: (old a, new a, old b, new b); x < 0 for none
+// (the current configuration), z < 0 for a single-site move.
+__device__ __forceinline__ int4 move_cols(const Mv &mv, const uint8_t *occ, int np1) {
+  const int ca0 = mv.a * np1 + occ[mv.a];
+  int4 c = make_int4(ca0, ca0 + mv.da, -1, -1);
   if (mv.b != mv.a) {
-    const int cb0 = mv.b * np1 + occ[mv.b], cb1 = cb0 + mv.db;
-    const __nv_bfloat162 wb1 = *reinterpret_cast<const __nv_bfloat162 *>(t.W1T + (size_t)cb1 * t.H1 + j);
-    const __nv_bfloat162 wb0 = *reinterpret_cast<const __nv_bfloat162 *>(t.W1T + (size_t)cb0 * t.H1 + j);
-    z.x = (z.x + __low2float(wb1)) - __low2float(wb0);
-    z.y = (z.y + __high2float(wb1)) - __high2float(wb0);
+    const int cb0 = mv.b * np1 + occ[mv.b];
+    c.z = cb0;
+    c.w = cb0 + mv.db;
   }
-  return z;
+  return c;
 }
 
+__device__ __forceinline__ void bf8(const uint4 &u, float (&f)[8]) {
+  const __nv_bfloat162 *p = reinterpret_cast<const __nv_bfloat162 *>(&u);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    f[2 * i] = __low2float(p[i]);
+    f[2 * i + 1] = __high2float(p[i]);
+  }
+}
+
+// acc + sum_i wm_i / (1 + 2^{K v_i + bk_i}) over 32 accumulator columns.
+__device__ __forceinline__ float reduce32(const uint32_t (&r)[32], const float *bk, const float *wm,
+                                          float acc) {
+#pragma unroll
+  for (int i = 0; i < 32; i += 4) {
+    const float4 b = *reinterpret_cast<const float4 *>(bk + i);
+    const float4 w = *reinterpret_cast<const float4 *>(wm + i);
+    acc = fmaf(w.x, sig2(fmaf(__uint_as_float(r[i]), KT, b.x)), acc);
+    acc = fmaf(w.y, sig2(fmaf(__uint_as_float(r[i + 1]), KT, b.y)), acc);
+    acc = fmaf(w.z, sig2(fmaf(__uint_as_float(r[i + 2]), KT, b.z)), acc);
+    acc = fmaf(w.w, sig2(fmaf(__uint_as_float(r[i + 3]), KT, b.w)), acc);
+  }
+  return acc;
+}
+
+// Shared memory: W2 and the epilogue constants (CTA), then one region per
+// pipeline: the A chunk ring, z1, the tile's row records, the rates and
+// log amplitudes of the moves, the occupations and the pipeline's
+// mbarriers and broadcast words.
+struct PipeSmem {
+  size_t A, z1, rc, rv, part, rates, lps, occ, misc, bytes;
+};
 struct MlpSmem {
-  size_t W2s, As, z1, b2, w3, rates, lps, rv, occ, misc, total;
+  size_t W2s, b2, w3, pipe0;
+  PipeSmem p;
+  size_t total;
 };
 
 __host__ __device__ inline MlpSmem mlp_plan(int H1, int H2, int n_off, int N) {
-  MlpSmem p;
+  MlpSmem s;
   size_t o = 0;
-  p.W2s = o; o += (size_t)H2 * H1 * 2;
-  p.As = o; o += (size_t)MT * H1 * 2;
-  p.z1 = o; o += (size_t)H1 * 4;
-  p.b2 = o; o += (size_t)H2 * 4;
-  p.w3 = o; o += (size_t)H2 * 4;
-  p.rates = o; o += (size_t)(n_off + 1) * 4;
-  p.lps = o; o += (size_t)(n_off + 1) * 4;
-  p.rv = o; o += (size_t)MT * 4;
-  p.occ = o; o += (size_t)((N + 15) / 16) * 16;
-  o = (o + 15) & ~(size_t)15;
-  p.misc = o; o += 128;
-  p.total = o;
-  return p;
+  s.W2s = o; o += (size_t)H2 * H1 * 2;
+  s.b2 = o; o += (size_t)H2 * 4;
+  s.w3 = o; o += (size_t)H2 * 4;
+  o = (o + 1023) & ~(size_t)1023;
+  s.pipe0 = o;
+  PipeSmem &p = s.p;
+  size_t q = 0;
+  p.A = q; q += (size_t)NBUF * ROWS * 128;
+  p.z1 = q; q += (size_t)H1 * 4;
+  p.rc = q; q += (size_t)ROWS * 16;
+  p.rv = q; q += (size_t)ROWS * 4;
+  p.part = q; q += (size_t)2 * ROWS * 4;
+  p.rates = q; q += (size_t)(n_off + 1) * 4;
+  p.lps = q; q += (size_t)(n_off + 1) * 4;
+  p.occ = q; q += (size_t)((N + 15) / 16) * 16;
+  q = (q + 15) & ~(size_t)15;
+  p.misc = q; q += 128;
+  p.bytes = (q + 1023) & ~(size_t)1023;
+  s.total = o + NP * p.bytes;
+  return s;
+}
+
+__device__ __forceinline__ void pipe_sync(int s) {
+  asm volatile("bar.sync %0, %1;" ::"r"(1 + s), "r"(PT) : "memory");
+}
+
+// Pipeline-uniform bounded wait on an mbarrier phase: the leader waits, the
+// pipeline's threads get the verdict (false when the limit ran out).
+__device__ __forceinline__ bool pipe_wait(uint64_t *bar, uint32_t parity, volatile int *flag, int s,
+                                          bool leader) {
+  if (leader) {
+    int ok = 0;
+    for (uint32_t it = 0; it < WAIT_LIMIT && !ok; ++it) ok = mbar_try_wait(bar, parity) ? 1 : 0;
+    *flag = ok;
+  }
+  pipe_sync(s);
+  const bool r = *flag != 0;
+  pipe_sync(s);
+  return r;
 }
 
 __global__ void __launch_bounds__(MT, 1) mlp_evolve_kernel(DevModel<float> m, MlpTables t,
@@ -131,169 +227,256 @@ __global__ void __launch_bounds__(MT, 1) mlp_evolve_kernel(DevModel<float> m, Ml
   extern __shared__ unsigned char dsm[];
   unsigned char *base = (unsigned char *)(((uintptr_t)dsm + 1023) & ~(uintptr_t)1023);
   const int H1 = t.H1, H2 = t.H2, np1 = t.np1;
-  const MlpSmem P = mlp_plan(H1, H2, m.n_off, m.N);
-  unsigned char *W2s = base + P.W2s;
-  unsigned char *As = base + P.As;
-  float *z1 = reinterpret_cast<float *>(base + P.z1);
-  float *b2s = reinterpret_cast<float *>(base + P.b2);
-  float *w3s = reinterpret_cast<float *>(base + P.w3);
-  float *rates = reinterpret_cast<float *>(base + P.rates);
-  float *lps = reinterpret_cast<float *>(base + P.lps);
-  float *rv = reinterpret_cast<float *>(base + P.rv);
-  uint8_t *occ = base + P.occ;
-  uint64_t *bar = reinterpret_cast<uint64_t *>(base + P.misc);
-  uint32_t *slot = reinterpret_cast<uint32_t *>(base + P.misc + 8);
-  volatile int *flag = reinterpret_cast<volatile int *>(base + P.misc + 12);
-  volatile int *bi = reinterpret_cast<volatile int *>(base + P.misc + 16);      // 4 ints
-  volatile float *bf = reinterpret_cast<volatile float *>(base + P.misc + 32);  // 4 floats
+  const MlpSmem S = mlp_plan(H1, H2, m.n_off, m.N);
+  unsigned char *W2s = base + S.W2s;
+  float *b2s = reinterpret_cast<float *>(base + S.b2);
+  float *w3s = reinterpret_cast<float *>(base + S.w3);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const uint32_t ncols = H2 <= 32 ? 32u : (H2 <= 64 ? 64u : (H2 <= 128 ? 128u : 256u));
+  const int s = tid / PT, tp = tid % PT;             // pipeline, thread in it
+  const int ridx = tp & (ROWS - 1), half = tp / ROWS; // row (TMEM lane), row half
+  const bool leader = tp == 0;
+  unsigned char *pb = base + S.pipe0 + (size_t)s * S.p.bytes;
+  unsigned char *Ar = pb + S.p.A;
+  float *z1 = reinterpret_cast<float *>(pb + S.p.z1);
+  int4 *rc = reinterpret_cast<int4 *>(pb + S.p.rc);
+  float *rv = reinterpret_cast<float *>(pb + S.p.rv);
+  float *part = reinterpret_cast<float *>(pb + S.p.part);
+  float *rates = reinterpret_cast<float *>(pb + S.p.rates);
+  float *lps = reinterpret_cast<float *>(pb + S.p.lps);
+  uint8_t *occ = pb + S.p.occ;
+  uint64_t *freeb = reinterpret_cast<uint64_t *>(pb + S.p.misc);       // NBUF
+  uint64_t *done = freeb + NBUF;
+  volatile int *flag = reinterpret_cast<volatile int *>(pb + S.p.misc + 32);
+  volatile int *bi = reinterpret_cast<volatile int *>(pb + S.p.misc + 48);      // 4 ints
+  volatile float *bf = reinterpret_cast<volatile float *>(pb + S.p.misc + 64);  // 4 floats
+  uint32_t *slot = reinterpret_cast<uint32_t *>(base + S.pipe0 + S.p.misc + 96);
+  const uint32_t dcols = H2 <= 32 ? 32u : (H2 <= 64 ? 64u : (H2 <= 128 ? 128u : 256u));
+  const uint32_t ncols = NP * dcols;
 
   // W2 into the swizzled K-major B layout: K chunk kc (64 inputs) holds the
-  // H2 rows, 128 bytes each
+  // H2 rows, 128 bytes each.  log psi = b3 + sum_j w3_j tanh(v_j + b2_j) =
+  // const + sum_j (-2 w3_j) / (1 + 2^{K v_j + K b2_j}).
   for (int idx = tid; idx < H2 * (H1 / 8); idx += MT) {
     const int j = idx / (H1 / 8), c8 = idx % (H1 / 8);
     const uint4 v = __ldg(reinterpret_cast<const uint4 *>(t.W2 + (size_t)j * H1) + c8);
     *reinterpret_cast<uint4 *>(sw_chunk(W2s + (size_t)(c8 / 8) * H2 * 128, j, c8 % 8)) = v;
   }
   for (int j = tid; j < H2; j += MT) {
-    b2s[j] = t.b2[j];
-    w3s[j] = t.w3[j];
+    b2s[j] = KT * t.b2[j];
+    w3s[j] = -2.0f * t.w3[j];
   }
   if (warp == 0) tmem_alloc(slot, ncols);
-  if (tid == 0) {
-    mbar_init(bar, 1);
+  if (leader) {
+    for (int b = 0; b < NBUF; ++b) mbar_init(freeb + b, 1);
+    mbar_init(done, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   fence_before();
   __syncthreads();
   fence_after();
   const uint32_t tmem = *slot;
+  const uint32_t tD = tmem + (uint32_t)s * dcols;                    // this pipeline's accumulator
+  const uint32_t tl = tD + ((uint32_t)(32 * (warp & 3)) << 16);     // this warp's lanes
   const uint32_t idesc = idesc_m128((uint32_t)H2);
   const int CB = ((m.N + 15) / 16) * 16;
-  uint32_t phase = 0;
+  const int C = (m.n_off + 31) / 32;   // rate slots per lane of the sampling warp
+  const bool sampler = tp < 32;
+  uint32_t use[NBUF] = {0u, 0u};       // commits per A buffer
+  uint32_t dphase = 0;
   bool ok = true;
   double wmax = -DBL_MAX;
   unsigned long long hop_acc = 0;
-  const int j2 = 2 * tid;            // this thread's unit pair (j2, j2 + 1) when j2 < H1
 
-  // One tile of 128 rows, the moves tb .. tb + 127 (current: row 0 is the
-  // configuration itself).  Writes rates[o] / lps[o] of the moves, or
-  // bf[0] = log psi(x) for the current-configuration tile.
+  // One tile: the moves tb .. tb + 127 (current: row 0 is the configuration
+  // itself).  Writes rates[o] / lps[o] of the moves, or bf[0] = log psi(x)
+  // for the current-configuration tile.
   auto tile = [&](int tb, bool current, float lpx) -> bool {
-    {
-      const int o = tb + tid;
+    if (half == 0) {
+      const int o = tb + ridx;
       float v = 0.0f;
-      if (current) v = tid == 0 ? 1.0f : 0.0f;
-      else if (o < m.n_off) v = mlp_move(m, occ, o).v;
-      rv[tid] = v;
-    }
-    __syncthreads();
-    if (j2 < H1) {
-      const float2 zc = make_float2(z1[j2], z1[j2 + 1]);
-      unsigned char *Ac = As + (size_t)(j2 / 64) * MT * 128;
-      const int c16 = (j2 % 64) / 8, e2 = (j2 % 8) * 2;
-      for (int r = 0; r < MT; ++r) {
-        uint32_t q = 0u;
-        if (rv[r] != 0.0f) {
-          float2 z = zc;
-          if (!current) z = z1_moved(t, occ, mlp_move(m, occ, tb + r), np1, zc, j2);
-          const __nv_bfloat162 h = __floats2bfloat162_rn(tanhf(z.x), tanhf(z.y));
-          q = *reinterpret_cast<const uint32_t *>(&h);
-        }
-        *reinterpret_cast<uint32_t *>(sw_chunk(Ac, r, c16) + e2) = q;
+      int4 c = make_int4(-1, -1, -1, -1);
+      if (current) {
+        v = ridx == 0 ? 1.0f : 0.0f;
+      } else if (o < m.n_off) {
+        const Mv mv = mlp_move(m, occ, o);
+        v = mv.v;
+        if (v != 0.0f) c = move_cols(mv, occ, np1);
       }
+      rv[ridx] = v;
+      rc[ridx] = c;
     }
-    fence_async_smem();
-    __syncthreads();
-    if (tid == 0) {
-      fence_after();
-      for (int kc = 0; kc < H1 / 64; ++kc)
+    pipe_sync(s);
+    const bool act = rv[ridx] != 0.0f;
+    const int4 c = rc[ridx];
+    const uint4 *W = reinterpret_cast<const uint4 *>(t.W1T);
+    const int rs = H1 / 8;             // uint4 per W1 column
+    for (int kc = 0; kc < H1 / KC; ++kc) {
+      const int b = kc & (NBUF - 1);
+      if (use[b] > 0 && !pipe_wait(freeb + b, (use[b] - 1) & 1u, flag, s, leader)) return false;
+      unsigned char *Ab = Ar + (size_t)b * ROWS * 128;
+      if (act) {
+#pragma unroll 2
+        for (int pc = 4 * half; pc < 4 * half + 4; ++pc) {
+          const int q = kc * 8 + pc;   // 8-input piece of the row
+          float z[8];
+          const float4 z0 = *reinterpret_cast<const float4 *>(z1 + 8 * q);
+          const float4 z4 = *reinterpret_cast<const float4 *>(z1 + 8 * q + 4);
+          z[0] = z0.x; z[1] = z0.y; z[2] = z0.z; z[3] = z0.w;
+          z[4] = z4.x; z[5] = z4.y; z[6] = z4.z; z[7] = z4.w;
+          if (c.x >= 0) {
+            const uint4 pa = __ldg(W + (size_t)c.y * rs + q), qa = __ldg(W + (size_t)c.x * rs + q);
+            uint4 pb4 = make_uint4(0, 0, 0, 0), qb4 = make_uint4(0, 0, 0, 0);
+            if (c.z >= 0) {
+              pb4 = __ldg(W + (size_t)c.w * rs + q);
+              qb4 = __ldg(W + (size_t)c.z * rs + q);
+            }
+            float p8[8], q8[8];
+            bf8(pa, p8);
+            bf8(qa, q8);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) z[i] = (z[i] + p8[i]) - q8[i];
+            if (c.z >= 0) {
+              bf8(pb4, p8);
+              bf8(qb4, q8);
+#pragma unroll
+              for (int i = 0; i < 8; ++i) z[i] = (z[i] + p8[i]) - q8[i];
+            }
+          }
+          uint4 o4;
+          uint32_t *ow = reinterpret_cast<uint32_t *>(&o4);
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const __nv_bfloat162 h = __floats2bfloat162_rn(fmaf(-2.0f, sig2(KT * z[2 * i]), 1.0f),
+                                                           fmaf(-2.0f, sig2(KT * z[2 * i + 1]), 1.0f));
+            ow[i] = *reinterpret_cast<const uint32_t *>(&h);
+          }
+          *reinterpret_cast<uint4 *>(sw_chunk(Ab, ridx, pc)) = o4;
+        }
+      }
+      fence_async_smem();
+      pipe_sync(s);
+      if (leader) {
+        fence_after();
 #pragma unroll
         for (int kk = 0; kk < 4; ++kk)
-          mma_bf16(tmem, sw128_desc(smem_u32(As + (size_t)kc * MT * 128) + 32u * kk),
+          mma_bf16(tD, sw128_desc(smem_u32(Ab) + 32u * kk),
                    sw128_desc(smem_u32(W2s + (size_t)kc * H2 * 128) + 32u * kk), idesc,
                    (kc > 0 || kk > 0) ? 1u : 0u);
-      mma_commit(bar);
+        mma_commit(freeb + b);
+        if (kc == H1 / KC - 1) mma_commit(done);
+      }
+      ++use[b];
     }
-    const bool done = cta_wait(bar, phase, flag);
-    phase ^= 1u;
-    if (!done) return false;
+    if (!pipe_wait(done, dphase, flag, s, leader)) return false;
+    dphase ^= 1u;
     fence_after();
     float acc = 0.0f;
-    for (int c0 = 0; c0 < H2; c0 += 16) {
-      float v[16];
-      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+    if (__any_sync(FULLW, rv[ridx] != 0.0f)) {
+      if ((H2 & 63) == 0) {
+        // this thread's column half in loads of 32 columns
+        const int cb = half * (H2 / 2);
+        for (int cc = cb; cc < cb + H2 / 2; cc += 32) {
+          uint32_t ra[32];
+          tmem_ld32_async(tl + (uint32_t)cc, ra);
+          tmem_ld_wait(ra);
+          acc = reduce32(ra, b2s + cc, w3s + cc, acc);
+        }
+      } else {
+        for (int c0 = 16 * half; c0 < H2; c0 += 32) {
+          float v[16];
+          tmem_ld16(tl + (uint32_t)c0, v);
 #pragma unroll
-      for (int i = 0; i < 16; ++i) acc = fmaf(w3s[c0 + i], tanhf(v[i] + b2s[c0 + i]), acc);
+          for (int i = 0; i < 16; ++i) acc = fmaf(w3s[c0 + i], sig2(fmaf(v[i], KT, b2s[c0 + i])), acc);
+        }
+      }
     }
-    const float lp = t.b3 + acc;
-    if (current) {
-      if (tid == 0) bf[0] = lp;
-    } else {
-      const int o = tb + tid;
-      if (o < m.n_off) {
-        const float v = rv[tid];
-        lps[o] = lp;
-        rates[o] = v != 0.0f ? v * __expf(lp - lpx) : 0.0f;
+    part[half * ROWS + ridx] = acc;
+    fence_before();
+    pipe_sync(s);
+    if (half == 0) {
+      const float lp = part[ridx] + part[ROWS + ridx];
+      if (current) {
+        if (ridx == 0) bf[0] = lp;
+      } else {
+        const int o = tb + ridx;
+        if (o < m.n_off) {
+          const float v = rv[ridx];
+          lps[o] = lp;
+          rates[o] = v != 0.0f ? v * __expf(lp - lpx) : 0.0f;
+        }
       }
     }
     fence_before();
-    __syncthreads();
+    pipe_sync(s);
     return true;
   };
 
-  // H_xx (BoseHubbard diagonal, bose_hubbard.py:271-281) by warp 0 in the
-  // step kernel's lane order, into bf[3]
-  auto diag = [&]() {
-    if (warp == 0) {
-      float su = 0.0f, sm = 0.0f;
-      for (int k = lane; k < m.N; k += 32) {
-        const float n = (float)occ[k];
-        if (m.has_U) su += m.U[k] * n * (n - 1.0f);
-        if (m.has_mu) sm += m.mu[k] * n;
-      }
-      float d = 0.0f;
-      if (m.has_U) d = d + 0.5f * warp_sum(su);
-      if (m.has_mu) d = d - warp_sum(sm);
-      if (lane == 0) bf[3] = d;
+  // H_xx (BoseHubbard diagonal, bose_hubbard.py:271-281) in the step
+  // kernel's lane order, by the sampling warp
+  auto diag0 = [&]() -> float {
+    float su = 0.0f, sm = 0.0f;
+    for (int k = lane; k < m.N; k += 32) {
+      const float n = (float)occ[k];
+      if (m.has_U) su += m.U[k] * n * (n - 1.0f);
+      if (m.has_mu) sm += m.mu[k] * n;
     }
+    float d = 0.0f;
+    if (m.has_U) d = d + 0.5f * warp_sum(su);
+    if (m.has_mu) d = d - warp_sum(sm);
+    return d;
+  };
+
+  // Sampling warp: this lane's chunk sum of the weights -rates (C slots per
+  // lane) into *own; returns its inclusive scan over the lanes.
+  auto scan0 = [&](float *own) -> float {
+    float sum = 0.0f;
+    const int lo = lane * C, hi = min(lo + C, m.n_off);
+    for (int o = lo; o < hi; ++o) sum += -rates[o];
+    *own = sum;
+    return warp_inclusive_scan(sum, lane);
   };
 
   for (;;) {
-    if (tid == 0) bi[0] = atomicAdd(a.work_ctr, 1);
-    __syncthreads();
+    if (leader) bi[0] = atomicAdd(a.work_ctr, 1);
+    pipe_sync(s);
     const int walker = bi[0];
-    __syncthreads();
+    pipe_sync(s);
     if (walker >= a.n_walkers) break;
     const int src = a.parents ? a.parents[walker] : walker;
     const uint32_t *in = reinterpret_cast<const uint32_t *>(
         reinterpret_cast<const uint8_t *>(a.cfg_in) + (size_t)src * CB);
-    for (int k = tid; k < CB / 4; k += MT) reinterpret_cast<uint32_t *>(occ)[k] = in[k];
-    __syncthreads();
+    for (int k = tp; k < CB / 4; k += PT) reinterpret_cast<uint32_t *>(occ)[k] = in[k];
+    pipe_sync(s);
     // an occupation above n_max is flagged and clamped (W1 has n_max + 1
     // columns per site)
-    for (int k = tid; k < m.N; k += MT)
+    for (int k = tp; k < m.N; k += PT)
       if (occ[k] > m.n_max) {
         atomicOr(a.status, ST_BAD_CONFIG);
         occ[k] = (uint8_t)m.n_max;
       }
-    __syncthreads();
-    // z1 of the configuration: b1 + the W1 columns of its occupations
-    if (j2 < H1) {
-      float zx = t.b1[j2], zy = t.b1[j2 + 1];
-      for (int k = 0; k < m.N; ++k) {
-        const __nv_bfloat162 w = *reinterpret_cast<const __nv_bfloat162 *>(
-            t.W1T + (size_t)(k * np1 + occ[k]) * H1 + j2);
-        zx += __low2float(w);
-        zy += __high2float(w);
+    pipe_sync(s);
+    // z1 and log psi: carried from the parent (H1 + 1 floats per walker), or
+    // z1 = b1 + the W1 columns of the occupations and log psi through a tile
+    const float *fin =
+        a.field_in ? reinterpret_cast<const float *>(a.field_in) + (size_t)src * (H1 + 1) : nullptr;
+    for (int j = tp; j < H1; j += PT) {
+      float z;
+      if (fin) {
+        z = fin[j];
+      } else {
+        z = t.b1[j];
+        for (int k = 0; k < m.N; ++k) z += __bfloat162float(t.W1T[(size_t)(k * np1 + occ[k]) * H1 + j]);
       }
-      z1[j2] = zx;
-      z1[j2 + 1] = zy;
+      z1[j] = z;
     }
-    __syncthreads();
-    if (!tile(0, true, 0.0f)) { ok = false; break; }
-    float lpx = bf[0];
+    pipe_sync(s);
+    float lpx;
+    if (fin) {
+      lpx = fin[H1];
+    } else {
+      if (!tile(0, true, 0.0f)) { ok = false; break; }
+      lpx = bf[0];
+    }
 
     const Key kw = fold(a.key, (uint32_t)(a.walker_offset + walker));
     double lw = 0.0;
@@ -304,97 +487,121 @@ __global__ void __launch_bounds__(MT, 1) mlp_evolve_kernel(DevModel<float> m, Ml
       float tcur = 0.0f;
       uint32_t it = 0;
       while (tcur < beta) {
-        for (int tb = 0; tb < m.n_off && ok; tb += MT) ok = tile(tb, false, lpx);
+        for (int tb = 0; tb < m.n_off && ok; tb += ROWS) ok = tile(tb, false, lpx);
         if (!ok) break;
-        diag();
-        __syncthreads();
-        if (tid == 0) {
-          // cumulative weights -rates in move order; evolution.sample_index:30-59
-          float R = 0.0f;
-          for (int o = 0; o < m.n_off; ++o) R += -rates[o];
+        if (sampler) {
+          // evolution.sample_index:30-59: the first slot whose cdf exceeds u,
+          // stepped back to the nearest slot at or before it with positive
+          // weight
+          const float d = diag0();
+          float own;
+          const float cum = scan0(&own);
+          const float R = __shfl_sync(FULLW, cum, 31);
           const float U1 = uniform<float>(fold(kw, 2u * it));
           const float psi = uniform<float>(fold(kw, 2u * it + 1u));
           int si = 0;
-          if (R > 0.0f) {
+          if (R > 0.0f) {   // (R is the same in every lane)
             float u = U1 * R;
             const float cap = nextafterf(R, 0.0f);
             u = u < cap ? u : cap;
-            float c = 0.0f;
-            int hit = m.n_off - 1;
-            for (int o = 0; o < m.n_off; ++o) {
-              c += -rates[o];
-              if (c > u) { hit = o; break; }
+            const unsigned bal = __ballot_sync(FULLW, cum > u);
+            const int Lh = bal ? __ffs(bal) - 1 : 31;
+            if (lane == Lh) {
+              int hit = m.n_off - 1;
+              if (bal) {
+                float cu = cum - own;
+                const int lo = Lh * C, hi = min(lo + C, m.n_off);
+                for (int o = lo; o < hi; ++o) {
+                  cu += -rates[o];
+                  if (cu > u) { hit = o; break; }
+                }
+              }
+              si = hit;
+              for (int o = hit; o >= 0; --o)
+                if (-rates[o] > 0.0f) { si = o; break; }
             }
-            si = hit;
-            for (int o = hit; o >= 0; --o)
-              if (-rates[o] > 0.0f) { si = o; break; }
+            si = __shfl_sync(FULLW, si, Lh);
           }
-          const float tau_raw = R > 0.0f ? -log1pf(-psi) / R : __int_as_float(0x7F800000);
-          const float rem = beta - tcur;
-          bi[1] = (tau_raw < rem) ? 1 : 0;
-          bi[2] = si;
-          bf[1] = tau_raw < rem ? tau_raw : rem;
-          bf[0] = bf[3] - R;
+          if (lane == 0) {
+            const float tau_raw = R > 0.0f ? -log1pf(-psi) / R : __int_as_float(0x7F800000);
+            const float rem = beta - tcur;
+            bi[2] = si;
+            bi[1] = (tau_raw < rem) ? 1 : 0;
+            bf[1] = tau_raw < rem ? tau_raw : rem;
+            bf[0] = d - R;
+          }
         }
-        __syncthreads();
+        pipe_sync(s);
         const float tau = bf[1], eL = bf[0];
         const int hop = bi[1], si = bi[2];
         lw = lw - (double)eL * (double)tau;
         tcur = tcur + tau;
         if (hop) {
           const Mv mv = mlp_move(m, occ, si);
-          if (j2 < H1) {
-            const float2 zn = z1_moved(t, occ, mv, np1, make_float2(z1[j2], z1[j2 + 1]), j2);
-            z1[j2] = zn.x;
-            z1[j2 + 1] = zn.y;
+          const int4 c = move_cols(mv, occ, np1);
+          for (int j = tp; j < H1; j += PT) {
+            float z = z1[j];
+            z = (z + __bfloat162float(t.W1T[(size_t)c.y * H1 + j])) -
+                __bfloat162float(t.W1T[(size_t)c.x * H1 + j]);
+            if (c.z >= 0)
+              z = (z + __bfloat162float(t.W1T[(size_t)c.w * H1 + j])) -
+                  __bfloat162float(t.W1T[(size_t)c.z * H1 + j]);
+            z1[j] = z;
           }
           lpx = lps[si];
-          __syncthreads();
-          if (tid == 0) {
+          pipe_sync(s);
+          if (leader) {
             occ[mv.a] = (uint8_t)(occ[mv.a] + mv.da);
             if (mv.b != mv.a) occ[mv.b] = (uint8_t)(occ[mv.b] + mv.db);
           }
           ++hops;
         }
         eloc = eL;
-        __syncthreads();
+        pipe_sync(s);
         if (++it >= (uint32_t)a.max_iters) {
-          if (tid == 0) atomicOr(a.status, ST_HOP_CAP);
+          if (leader) atomicOr(a.status, ST_HOP_CAP);
           break;
         }
       }
       lw -= a.alw * a.step;
     } else {   // EVALUATE: E_L = H_xx + sum of the guided off-diagonal elements
-      for (int tb = 0; tb < m.n_off && ok; tb += MT) ok = tile(tb, false, lpx);
+      for (int tb = 0; tb < m.n_off && ok; tb += ROWS) ok = tile(tb, false, lpx);
       if (!ok) break;
-      diag();
-      __syncthreads();
-      if (tid == 0) {
-        float s = 0.0f;
-        for (int o = 0; o < m.n_off; ++o) s += rates[o];
-        bf[0] = bf[3] + s;
+      if (sampler) {
+        const float d = diag0();
+        float own;
+        const float R = __shfl_sync(FULLW, scan0(&own), 31);
+        if (lane == 0) {
+          bf[0] = d - R;
+          bf[3] = d;
+        }
       }
-      __syncthreads();
+      pipe_sync(s);
       eloc = bf[0];
-      if (tid == 0 && a.diag_out) a.diag_out[walker] = (double)bf[3];
+      if (leader && a.diag_out) a.diag_out[walker] = (double)bf[3];
     }
     if (!ok) break;
     if (a.cfg_out) {
       uint32_t *out = reinterpret_cast<uint32_t *>(reinterpret_cast<uint8_t *>(a.cfg_out) +
                                                    (size_t)walker * CB);
-      for (int k = tid; k < CB / 4; k += MT) out[k] = reinterpret_cast<const uint32_t *>(occ)[k];
+      for (int k = tp; k < CB / 4; k += PT) out[k] = reinterpret_cast<const uint32_t *>(occ)[k];
     }
-    if (tid == 0) {
+    if (a.field_out) {
+      float *fo = reinterpret_cast<float *>(a.field_out) + (size_t)walker * (H1 + 1);
+      for (int j = tp; j < H1; j += PT) fo[j] = z1[j];
+      if (leader) fo[H1] = lpx;
+    }
+    if (leader) {
       if (a.method == CONT_TIME) a.log_w[walker] = lw;
       a.e_loc[walker] = (double)eloc;
     }
     if (a.method == CONT_TIME) wmax = lw > wmax ? lw : wmax;
     hop_acc += (unsigned long long)hops;
-    __syncthreads();
+    pipe_sync(s);
   }
-  if (!ok && tid == 0) atomicOr(a.status, ST_TIMEOUT);
-  if (tid == 0) {
-    if (a.partial_max) a.partial_max[blockIdx.x] = wmax;
+  if (!ok && leader) atomicOr(a.status, ST_TIMEOUT);
+  if (leader) {
+    if (a.partial_max) a.partial_max[(size_t)blockIdx.x * NP + s] = wmax;
     if (a.hops && hop_acc) atomicAdd(a.hops, hop_acc);
   }
   fence_before();
@@ -406,6 +613,10 @@ __global__ void __launch_bounds__(MT, 1) mlp_evolve_kernel(DevModel<float> m, Ml
 
 size_t mlp_smem_bytes(int H1, int H2, int n_off, int N) {
   return 1024 + mlp_plan(H1, H2, n_off, N).total;
+}
+
+int mlp_partials(int grid, int n_walkers) {
+  return NP * (grid < n_walkers ? grid : (n_walkers > 0 ? n_walkers : 1));
 }
 
 int mlp_grid() {

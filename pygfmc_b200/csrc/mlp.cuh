@@ -27,6 +27,8 @@ struct MlpTables {
 size_t mlp_smem_bytes(int H1, int H2, int n_off, int N);
 // Persistent grid: one CTA per SM.
 int mlp_grid();
+// Partial maxima of log_w a launch over n_walkers writes (one per pipeline).
+int mlp_partials(int grid, int n_walkers);
 // One launch of the MLP step kernel (methods CONT_TIME and EVALUATE, float).
 cudaError_t launch_mlp_evolve(const DevModel<float> &m, const MlpTables &t, const EvolveArgs &a,
                               int grid, cudaStream_t s);

@@ -199,6 +199,33 @@ def test_mlp_local_energy_matches_oracle(oracle):
 
 
 @pytest.mark.gpu
+def test_mlp_carried_state_matches_the_oracle(oracle):
+    """60 cont_time steps with z1 and log psi carried through the parent maps
+    (rebuilt every 50 steps): the local energies the last step wrote for its
+    configurations agree with the oracle's fresh evaluation of them."""
+    import ctypes
+    import torch
+    O = oracle
+    P._lib.load()
+    name, H, G, m, g, cfg = _mlp_systems(O)[1]
+    n = cfg.shape[0]
+    eng = P.GFMCEngine(H, G, n, precision="mixed")
+    eng.load(cfg)
+    keys, _ = P.engine.key_schedule(P.PRNGKey(5), 60)
+    lg = torch.empty(60, dtype=torch.float64, device=eng.device)
+    alw = float((-eng.local_energy()).mean().item())
+    eng.steps("cont_time", 0.1, None, alw, keys, lg, torch.empty_like(lg))
+    out = torch.empty((n, eng.N), dtype=torch.float64, device=eng.device)
+    eng.L.gfmc_unpack(eng.h, n, ctypes.c_void_p(eng.cfg.data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                      eng._stream())
+    c = out.cpu().numpy()
+    r = O.rates(m, g, c)
+    err = np.abs(eng.e_loc.cpu().numpy() - r.sum(axis=1)) / np.abs(r).sum(axis=1)
+    assert np.all(err <= 2e-3) and err.mean() <= 1e-4, (err.max(), err.mean())
+    assert eng.status() == 0
+
+
+@pytest.mark.gpu
 def test_mlp_requires_the_float32_build_and_cont_time():
     P._lib.load()
     H = _bh(6, 2)
