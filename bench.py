@@ -119,99 +119,103 @@ def cpu_reference(P, cfg_sample, alw, steps, warmup, seed_key):
 
 
 def sigma_study(P, args):
-    """GPU seconds to sigma(E/N) = 1e-5 on the 16x16 Heisenberg lattice: the
-    plain float64 long-range-Jastrow engine against the float32/bf16 RBM
-    guide (H = 512) trained on the run's own walkers by variance
-    minimisation.  Each method runs warm-up + production through run(); the
-    blocked jackknife error at the largest window gives sigma(E/N); the time
-    to the target is the production GPU time x (sigma / 1e-5)^2 (errors fall
-    as 1/sqrt(steps)).  The RBM's training time is reported beside it."""
+    """GPU seconds to sigma(E/N) = 1e-5: the plain float64 Jastrow engine
+    against the float32/bf16 RBM guide trained on the run's own walkers by
+    variance minimisation, on the 16x16 Heisenberg lattice (long-range
+    Jastrow; RBM H = 512, 65536 walkers, tau = 0.05, p = 128) or the 432-site
+    kagome XXZ lattice (nearest-neighbour Jastrow; RBM H = 432, 131072
+    walkers, tau = 0.02, p = 256).  Each method runs warm-up + production
+    through run(); the blocked jackknife error at the largest window gives
+    sigma(E/N); the time to the target is the production GPU time x
+    (sigma / 1e-5)^2 (errors fall as 1/sqrt(steps)).  The RBM's training time
+    is reported beside it."""
     import torch
-    lat, H, G, pairs, beta = build_system(P, "fp64")
+    lat, H, G, hid, tau, n_rbm, name = rbm_system(P, args.lattice)
+    N = lat.N
     out = {}
-    p_arr = [8, 32, 128]
+    p_arr = [8, 32, 128] if args.lattice == "square16" else [16, 64, 256]
+    pm = p_arr[-1]
 
-    def measure(name, guide, n, steps, warm, precision):
-        w = P.prepare_walkers_sz(n, 256, P.PRNGKey(11), sz=0)
+    def measure(key, guide, n, steps, warm, precision):
+        w = P.prepare_walkers_sz(n, N, P.PRNGKey(11), sz=0)
         torch.cuda.synchronize()
-        wf, E, _, st, raw = P.run(w, steps, H, TAU, guide, p_arr, rng_key=P.PRNGKey(12),
+        wf, E, _, st, raw = P.run(w, steps, H, tau, guide, p_arr, rng_key=P.PRNGKey(12),
                                   warmup_steps=warm, verbosity=0, precision=precision)
-        Ej, err = P.estimators.jackknife_energy([128], raw["log_weights"], raw["energy"], 20)
-        sig = err[128] / 256
+        Ej, err = P.estimators.jackknife_energy([pm], raw["log_weights"], raw["energy"], 20)
+        sig = err[pm] / N
         t = st["runtime"]
-        out[name] = {"E_per_site": Ej[128] / 256, "sigma_per_site": sig, "n_walkers": n,
-                     "steps": steps, "warmup": warm, "precision": precision,
-                     "production_gpu_s": t, "gpu_s_to_1e-5": t * (sig / 1e-5) ** 2,
-                     "walker_steps_per_s": n * steps / t,
-                     "local_energy_var_per_site": float(np.var(wf.e_loc) / 256)}
+        out[key] = {"E_per_site": Ej[pm] / N, "sigma_per_site": sig, "n_walkers": n,
+                    "steps": steps, "warmup": warm, "precision": precision,
+                    "production_gpu_s": t, "gpu_s_to_1e-5": t * (sig / 1e-5) ** 2,
+                    "walker_steps_per_s": n * steps / t,
+                    "local_energy_var_per_site": float(np.var(wf.e_loc) / N)}
 
     measure("jastrow_fp64", G, N_WALKERS, args.study_steps, 2000, "fp64")
     measure("jastrow_mixed", G, N_WALKERS, args.study_steps, 2000, "mixed")
-    G0 = P.RBMSpinHalf(256, 512, seed=0, sigma=0.01)
-    w = P.prepare_walkers_sz(65536, 256, P.PRNGKey(13), sz=0)
+    G0 = P.RBMSpinHalf(N, hid, seed=0, sigma=0.01)
+    w = P.prepare_walkers_sz(n_rbm, N, P.PRNGKey(13), sz=0)
     trained, hist = P.learn.train_rbm_guide(w, H, G0, n_iterations=args.train_iters,
-                                            steps_per_iteration=3, step_size=TAU, lr=args.train_lr,
+                                            steps_per_iteration=3, step_size=tau, lr=args.train_lr,
                                             rng_key=P.PRNGKey(14), warmup_steps=100, verbosity=0)
-    measure("rbm_h512_mixed", trained, 65536, args.rbm_steps, 500, "mixed")
-    out["rbm_h512_mixed"]["training_gpu_s"] = hist["seconds"]
-    out["rbm_h512_mixed"]["train_var_per_site_first_last"] = [float(hist["variance"][0] / 256),
-                                                              float(hist["variance"][-1] / 256)]
-    out["rbm_h512_mixed"]["train_iterations"] = len(hist["variance"])
-    out["rbm_h512_mixed"]["train_lr"] = args.train_lr
-    out["rbm_h512_mixed"]["train_collapsed"] = bool(hist["collapsed"])
-    out["rbm_h512_mixed"]["gpu_s_to_1e-5_with_training"] = (
-        out["rbm_h512_mixed"]["gpu_s_to_1e-5"] + hist["seconds"])
-    j, r = out["jastrow_fp64"], out["rbm_h512_mixed"]
+    rk = f"rbm_h{hid}_mixed"
+    measure(rk, trained, n_rbm, args.rbm_steps, 500, "mixed")
+    r = out[rk]
+    r["training_gpu_s"] = hist["seconds"]
+    r["train_var_per_site_first_last"] = [float(hist["variance"][0] / N),
+                                          float(hist["variance"][-1] / N)]
+    r["train_iterations"] = len(hist["variance"])
+    r["train_lr"] = args.train_lr
+    r["train_collapsed"] = bool(hist["collapsed"])
+    r["gpu_s_to_1e-5_with_training"] = r["gpu_s_to_1e-5"] + hist["seconds"]
+    j = out["jastrow_fp64"]
     diff = abs(j["E_per_site"] - r["E_per_site"]) / np.hypot(j["sigma_per_site"], r["sigma_per_site"])
+    plain = "longrange_jastrow" if args.lattice == "square16" else "nn_jastrow"
     line = {"metric": "GPU-s to sigma(E/N)=1e-5", "value": r["gpu_s_to_1e-5"], "unit": "s",
             "higher_is_better": False, "n_gpus": 1, "data": "synthetic",
-            "config": {"workload": "heisenberg_16x16_rbm_h512_vs_longrange_jastrow", "tau": TAU,
-                       "p": 128, "jackknife_blocks": 20},
+            "config": {"workload": f"{name}_rbm_h{hid}_vs_{plain}", "tau": tau, "p": pm,
+                       "jackknife_blocks": 20},
             "methods": out,
             "learned_over_jastrow_fp64_time_ratio": r["gpu_s_to_1e-5"] / j["gpu_s_to_1e-5"],
             "energy_difference_in_sigma": diff}
     print(json.dumps(line))
 
 
+def rbm_system(P, lattice):
+    """The RBM workloads: the periodic 16x16 Heisenberg lattice (H = 512,
+    tau = 0.05, 65536 walkers) or the 12x12 kagome XXZ lattice (432 sites,
+    864 bonds, J_x = J_y = -1, J_z = 1; H = 432, tau = 0.02, 131072 walkers),
+    each with the plain guide it is compared with (long-range Jastrow v(r) =
+    0.3 / r on the square lattice, nearest-neighbour Jastrow beta = 0.3 on
+    kagome)."""
+    if lattice == "kagome12":
+        lat = P.kagome(12, 12)
+        H = P.SpinHalf.create(lat.edges, J_x=-1.0, J_y=-1.0, J_z=1.0, dtype=np.float64)
+        GJ = P.JastrowSpinHalf(lat.N, lat.edges, beta=0.3)
+        return lat, H, GJ, 432, 0.02, 131072, "kagome_12x12_xxz"
+    lat, H, GJ, pairs, beta = build_system(P, "fp64")
+    return lat, H, GJ, 512, TAU, 65536, "heisenberg_16x16"
+
+
 def rbm_bench(P, args):
-    """Learned-guide workload: 16x16 Heisenberg, RBM guide H = 512 (bf16
-    weights, N(0, 0.01^2)), float32 build, cont_time tau = 0.05.  Times the
-    branching step (L2 flushed before each), one training step
-    (gfmc_rbm_train_step) and the tensor-core theta GEMM."""
+    """Learned-guide workload: an RBM guide (bf16 weights N(0, 0.01^2)),
+    float32 build, cont_time.  Times the branching step (L2 flushed before
+    each), one training step (gfmc_rbm_train_step), the tensor-core theta
+    GEMM and, beside them, the plain Jastrow-guided step on the same lattice
+    (float64 and float32)."""
     import torch
-    lat = P.square(L)
-    H = P.SpinHalf.create(lat.edges, J_x=-1.0, J_y=-1.0, J_z=1.0, dtype=np.float64)
-    G = P.RBMSpinHalf(L * L, args.hidden, seed=0, sigma=0.01)
-    n = args.walkers
-    w = P.prepare_walkers_sz(n, L * L, P.PRNGKey(0), sz=0)
+    lat, H, GJ, hid, tau, n_def, name = rbm_system(P, args.lattice)
+    if args.hidden_set:
+        hid = args.hidden
+    N = lat.N
+    G = P.RBMSpinHalf(N, hid, seed=0, sigma=0.01)
+    n = args.walkers if args.walkers_set else n_def
+    w = P.prepare_walkers_sz(n, N, P.PRNGKey(0), sz=0)
     eng = P.GFMCEngine(H, G, n, precision="mixed")
     eng.load(w.config)
-    dev = eng.device
-    alw = float((-eng.local_energy()).mean().item())
-    key = P.PRNGKey(1000)
-    wk = max(args.warmup, 3)
-    keys, key = P.engine.key_schedule(key, wk)
-    lg = torch.empty(wk, dtype=torch.float64, device=dev)
-    Ew = torch.empty_like(lg)
-    eng.steps("cont_time", TAU, None, alw, keys, lg, Ew)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    keys, key = P.engine.key_schedule(key, args.steps)
-    logG = torch.empty(1, dtype=torch.float64, device=dev)
-    Es = torch.empty_like(logG)
-    hops = torch.zeros(1, dtype=torch.int64, device=dev)
     stream = torch.cuda.current_stream()
-    ms, tot_hops = [], 0
-    for st in range(args.steps):
-        flush.fill_(float(st))
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        eng.steps("cont_time", TAU, None, alw, keys[st:st + 1], logG, Es, hops)
-        b.record(stream)
-        b.synchronize()
-        ms.append(a.elapsed_time(b))
-        tot_hops += int(hops.item())
-    step_ms = float(np.mean(ms))
+    alw = float((-eng.local_energy()).mean().item())
+    wk = max(args.warmup, 3)
+    step_ms, hpw = timed_steps(P, eng, alw, tau, args.steps, wk, P.PRNGKey(1000))
     a = torch.cuda.Event(enable_timing=True)
     b = torch.cuda.Event(enable_timing=True)
     eng.rbm_theta()
@@ -227,17 +231,28 @@ def rbm_bench(P, args):
     b.record(stream)
     b.synchronize()
     train_ms = a.elapsed_time(b)
+    del eng
+    plain = {}
+    for prec in ("fp64", "mixed"):
+        ej = P.GFMCEngine(H, GJ, n, precision=prec)
+        ej.load(w.config)
+        alw_j = float((-ej.local_energy()).mean().item())
+        ms_j, _ = timed_steps(P, ej, alw_j, tau, args.steps, wk, P.PRNGKey(1000))
+        plain[prec] = {"value": n / (ms_j / 1e3), "ms_per_step": ms_j}
+        del ej
     pk, pk_kind = peaks()
-    Hp = ((args.hidden + 255) // 256) * 256
-    gemm_tflops = 2.0 * n * Hp * 256 / (gemm_ms / 1e3) / 1e12
+    Hp = ((hid + 255) // 256) * 256
+    Np = ((N + 63) // 64) * 64
+    gemm_tflops = 2.0 * n * Hp * Np / (gemm_ms / 1e3) / 1e12
     line = {"metric": "walker-steps/s", "value": n / (step_ms / 1e3), "unit": "walker-steps/s",
             "n_gpus": 1, "steps": args.steps, "warmup": wk, "ms_per_step": step_ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+bf16",
             "data": "synthetic",
-            "config": {"workload": f"heisenberg_16x16_rbm_h{args.hidden}_cont_time", "n_walkers": n,
-                       "tau": TAU, "l2": "flushed (256 MB write) before every timed step",
-                       "hops_per_walker_step": tot_hops / (n * args.steps)},
+            "config": {"workload": f"{name}_rbm_h{hid}_cont_time", "n_walkers": n, "n_sites": N,
+                       "tau": tau, "l2": "flushed (256 MB write) before every timed step",
+                       "hops_per_walker_step": hpw},
             "train_step_ms": train_ms,
+            "jastrow_fp64": plain["fp64"], "jastrow_mixed": plain["mixed"],
             "roofline": {"bound": "tensor", "kernel": "rbm_theta_kernel", "achieved": gemm_tflops,
                          "peak": pk["bf16_tflops"], "unit": "TFLOP/s",
                          "frac": gemm_tflops / pk["bf16_tflops"], "traffic": None,
@@ -357,7 +372,10 @@ def main():
     ap.add_argument("--guide", default="jastrow", choices=["jastrow", "rbm", "mlp"],
                     help="rbm: the learned-guide workload (RBM, float32); mlp: the Bose-Hubbard "
                          "ring with the dense MLP guide")
-    ap.add_argument("--hidden", type=int, default=512)
+    ap.add_argument("--hidden", type=int, default=None,
+                    help="hidden units of the learned guide (default: the workload's)")
+    ap.add_argument("--lattice", default="square16", choices=["square16", "kagome12"],
+                    help="--guide rbm: the 16x16 Heisenberg or the 432-site kagome XXZ workload")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -367,9 +385,11 @@ def main():
         if rank == 0:
             sigma_study(P, args)
         return
+    args.hidden_set = args.hidden is not None
+    args.walkers_set = args.walkers != N_WALKERS
+    if args.hidden is None:
+        args.hidden = 256 if args.guide == "mlp" else 512
     if args.guide == "rbm":
-        if args.walkers == N_WALKERS:
-            args.walkers = 65536
         if rank == 0:
             rbm_bench(P, args)
         return

@@ -233,7 +233,7 @@ int gfmc_rbm_hidden_padded(const gfmc_handle *h);
  * inputs, float32 accumulation).  gfmc_rbm_train_step takes one Adam step
  * (beta1 0.9, beta2 0.999, eps 1e-8) of rate lr on float32 master parameters
  * and writes them back to the guide rounded to bf16; stats are those before
- * the step.  Float32 (mixed) handles, at most 256 sites.  No counterpart in
+ * the step.  Float32 (mixed) handles, at most 448 sites.  No counterpart in
  * PyGFMC (it trains guides by NetKet VMC). */
 int gfmc_rbm_gradient(gfmc_handle *h, int n_walkers, const void *cfg, const int32_t *parents,
                       int parents_valid, const double *omega, float *grad_W, float *grad_b,

@@ -759,7 +759,7 @@ int rbm_gradient_t(gfmc_handle *h, int n, const void *cfg, const int32_t *parent
   const int NW = (h->N + 63) / 64, n_off = h->M - 1;
   if (h->precision != GFMC_PRECISION_MIXED)
     return fail(GFMC_ERR_UNSUPPORTED, "RBM training runs in the float32 (mixed) build");
-  if (r.Np > 256) return fail(GFMC_ERR_UNSUPPORTED, "RBM training supports at most 256 sites");
+  if (r.Np > 448) return fail(GFMC_ERR_UNSUPPORTED, "RBM training supports at most 448 sites");
   if (n > h->train_cap) {
     cudaFree(h->tr_cfg); cudaFree(h->tr_theta); cudaFree(h->tr_rates); cudaFree(h->tr_rsum);
     cudaFree(h->tr_gw); cudaFree(h->tr_e); cudaFree(h->tr_recs);

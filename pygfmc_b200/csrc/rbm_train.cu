@@ -18,8 +18,12 @@
 // swizzled K-major A tile, and two site rows of V (+-1 as bf16) into the B
 // tile; thread 0 issues tcgen05.mma (M = 128 hidden, N = sites, K = 64 rows)
 // accumulating dL/dW of the tile in TMEM.  Two stages: the MMAs of one chunk
-// run while the next is produced.  The epilogue adds the tile into the global
-// float32 gradient (atomics; one CTA per walker block and tile).
+// run while the next is produced.  Up to 256 sites both tiles are double
+// buffered; above (at most 448 padded sites) the B tile has one buffer, which
+// its producers refill once the previous chunk's MMAs are done, and each K
+// step is two MMAs (sites 0..255 and 256..Np-1 into TMEM columns of their
+// own, 512 in all).  The epilogue adds the tile into the global float32
+// gradient (atomics; one CTA per walker block and tile).
 #include <cuda_bf16.h>
 
 #include "rbm.cuh"
@@ -127,7 +131,8 @@ __host__ __device__ inline GradSmem grad_smem_plan(int Np, int n_off, int NW) {
   p.A0 = o; o += 16384;
   p.A1 = o; o += 16384;
   p.B0 = o; o += (size_t)Np * 128;
-  p.B1 = o; o += (size_t)Np * 128;
+  p.B1 = p.B0;
+  if (Np <= 256) { p.B1 = o; o += (size_t)Np * 128; }     // wider tiles: one B buffer
   p.WTs = o; o += (size_t)(Np + 1) * TT * 2;                 // + one zero row
   o = (o + 15) & ~(size_t)15;
   p.recs = o; o += 3 * (size_t)KR * 16;                      // three chunks in flight
@@ -187,7 +192,9 @@ __global__ void __launch_bounds__(3 * TT, 1) rbm_grad_kernel(GradArgs g, const f
   const int rows_per_w = g.n_off + 1;
   const long long R0 = (long long)w0 * rows_per_w, R1 = (long long)w1 * rows_per_w;
   const int nchunks = R1 > R0 ? (int)((R1 - R0 + KR - 1) / KR) : 0;
-  const uint32_t ncols = Np <= 32 ? 32u : (Np <= 64 ? 64u : (Np <= 128 ? 128u : 256u));
+  const uint32_t ncols =
+      Np <= 32 ? 32u : (Np <= 64 ? 64u : (Np <= 128 ? 128u : (Np <= 256 ? 256u : 512u)));
+  const bool oneB = Np > 256;
 
   for (int idx = tid; idx < (Np + 1) * (TT / 8); idx += 3 * TT) {
     const int i = idx / (TT / 8), c = idx % (TT / 8);
@@ -203,6 +210,7 @@ __global__ void __launch_bounds__(3 * TT, 1) rbm_grad_kernel(GradArgs g, const f
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (tid == 0) {
+    flag[2] = 0;
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar[0])) : "memory");
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar[1])) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -271,10 +279,33 @@ __global__ void __launch_bounds__(3 * TT, 1) rbm_grad_kernel(GradArgs g, const f
       // V: each site row holds the spin of the row's walker (one run per
       // walker), then the moves' flips are patched in
       unsigned char *B = base + (st ? P.B1 : P.B0);
+      bool writeB = true;
+      if (oneB && ch > 0) {
+        // the single B buffer still feeds chunk ch - 1's MMAs (stage 1 - st,
+        // its commit number (ch + 1) / 2 on that barrier)
+        const uint32_t prev = (uint32_t)((ch + 1) / 2);
+        if (tb == 0) {
+          int okw = 0;
+          for (uint32_t it = 0; it < WAIT_LIMIT && !okw; ++it)
+            okw = mbar_try_wait(&bar[1 - st], (prev - 1u) & 1u) ? 1 : 0;
+          flag[1] = okw;
+        }
+        bgroup_sync();
+        const bool okb = flag[1] != 0;
+        bgroup_sync();
+        if (!okb) {
+          // the whole CTA leaves after the barrier below; B is not touched
+          if (tb == 0) {
+            atomicOr(g.status, 8);
+            flag[2] = 1;
+          }
+          writeB = false;
+        }
+      }
       const uint64_t *wd = reinterpret_cast<const uint64_t *>(base + P.wd) + (size_t)b * P.maxw * g.NW;
       const long long rend = R1 - r0;                 // valid rows of this chunk
       const int first = (int)(r0 % rows_per_w);       // row offset inside the first walker
-      for (int i = tb; i < Np; i += TT) {
+      for (int i = tb; writeB && i < Np; i += TT) {
         const bool real = i < g.N;
         // walker segments: row rr belongs to walker wr; the next one starts at nextb
         int wr = 0, nextb = rows_per_w - first;
@@ -303,7 +334,7 @@ __global__ void __launch_bounds__(3 * TT, 1) rbm_grad_kernel(GradArgs g, const f
         }
       }
       bgroup_sync();
-      if (tb < KR) {
+      if (writeB && tb < KR) {
         const float4 rec = rs[tb];
         if (rec.x != 0.0f) {
           const uint32_t code = __float_as_uint(rec.w);
@@ -324,15 +355,26 @@ __global__ void __launch_bounds__(3 * TT, 1) rbm_grad_kernel(GradArgs g, const f
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
+    if (flag[2]) {
+      ok = false;
+      break;
+    }
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const uint32_t a0 = smem_u32(base + (st ? P.A1 : P.A0));
       const uint32_t b0 = smem_u32(base + (st ? P.B1 : P.B0));
-      const uint32_t id = idesc_m128((uint32_t)Np);
+      // sites 0..255 into TMEM columns 0..255, the rest into 256..Np-1
+      const int n0 = Np < 256 ? Np : 256;
+      const uint32_t id0 = idesc_m128((uint32_t)n0);
+      const uint32_t id1 = idesc_m128((uint32_t)(Np > 256 ? Np - 256 : 16));
 #pragma unroll
-      for (int kk = 0; kk < KR / 16; ++kk)
-        mma_bf16(tmem, sw128_desc(a0 + 32u * kk), sw128_desc(b0 + 32u * kk), id,
+      for (int kk = 0; kk < KR / 16; ++kk) {
+        mma_bf16(tmem, sw128_desc(a0 + 32u * kk), sw128_desc(b0 + 32u * kk), id0,
                  (ch > 0 || kk > 0) ? 1u : 0u);
+        if (Np > 256)
+          mma_bf16(tmem + 256u, sw128_desc(a0 + 32u * kk), sw128_desc(b0 + 256u * 128u + 32u * kk),
+                   id1, (ch > 0 || kk > 0) ? 1u : 0u);
+      }
       mma_commit(&bar[st]);
     }
     if (st) ++cnt1; else ++cnt0;

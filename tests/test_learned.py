@@ -12,8 +12,12 @@ E0_4X4 = -11.228483   # periodic 4x4 Heisenberg antiferromagnet, J = 1
 
 
 def _system(N=16, H=32, seed=3, sigma=0.2):
-    sq = P.square(4) if N == 16 else None
-    edges = sq.edges if sq is not None else P.chain(N).edges
+    if N == 16:
+        edges = P.square(4).edges
+    elif N == 432:
+        edges = P.kagome(12, 12).edges     # 12 x 12 unit cells, 864 bonds
+    else:
+        edges = P.chain(N).edges
     Hm = P.SpinHalf.create(edges, J_x=-1.0, J_y=-1.0, J_z=1.0, dtype=np.float64)
     rng = np.random.default_rng(seed)
     G = P.RBMSpinHalf(N, H, seed=seed, sigma=sigma, b=rng.normal(0, 0.1, H), a=rng.normal(0, 0.05, N))
@@ -39,8 +43,11 @@ def test_oracle_gradient_matches_finite_differences():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("N,H,n", [(16, 32, 256), (64, 200, 384)])
+@pytest.mark.parametrize("N,H,n", [(16, 32, 256), (64, 200, 384), (300, 96, 128), (432, 64, 96)])
 def test_device_gradient_matches_oracle(N, H, n):
+    """Up to 256 sites the gradient tile is double buffered in both operands;
+    above, one site buffer and two MMAs per K step (sites 0..255 and the
+    rest) -- the 300-site chain and the 432-site kagome lattice."""
     from oracle import learned
     P._lib.load()
     Hm, G = _system(N, H)
