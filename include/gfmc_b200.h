@@ -245,6 +245,30 @@ int gfmc_rbm_train_step(gfmc_handle *h, int n_walkers, const void *cfg, const in
  * used, i.e. bf16 values; b; a). */
 int gfmc_rbm_get_params(gfmc_handle *h, float *W, float *b, float *a);
 
+/* ---- MLP guide trainer ---------------------------------------------------- */
+/* The same variance loss for the MLP guide (float32 handles; mlp_H2 a
+ * multiple of 64; at most 800 one-hot inputs n_sites (n_max + 1)).  The
+ * parameters, and the gradient, are one float32 array of
+ * gfmc_mlp_param_count(h) values: W1 (mlp_H1, n_sites (n_max + 1)), b1
+ * (mlp_H1), W2 (mlp_H2, mlp_H1), b2 (mlp_H2), w3 (mlp_H2) (b3 cancels in
+ * every ratio and is not trained).  gfmc_mlp_gradient writes dL/dp (device,
+ * nullable) and stats = (E, L) (host); the second layer forward, its
+ * backward into the first layer and dL/dW2 run on the tensor cores (bf16
+ * inputs, float32 accumulation), dL/dW1 by one-hot accumulation.
+ * gfmc_mlp_train_step takes one Adam step (beta1 0.9, beta2 0.999, eps 1e-8)
+ * of rate lr on float32 master parameters and writes them back to the guide
+ * (weights rounded to bf16).  gfmc_mlp_get_params copies the guide's
+ * parameters as used (bf16 values) to host memory.  No counterpart in
+ * PyGFMC. */
+long long gfmc_mlp_param_count(const gfmc_handle *h);
+int gfmc_mlp_gradient(gfmc_handle *h, int n_walkers, const void *cfg, const int32_t *parents,
+                      int parents_valid, const double *omega, float *grad, double stats[2],
+                      void *stream);
+int gfmc_mlp_train_step(gfmc_handle *h, int n_walkers, const void *cfg, const int32_t *parents,
+                        int parents_valid, const double *omega, double lr, double stats[2],
+                        void *stream);
+int gfmc_mlp_get_params(gfmc_handle *h, float *params);
+
 /* ---- off-diagonal observables with forward walking ---------------------- */
 /* At most this many windows per forward walk. */
 #define GFMC_FW_MAX_P 16

@@ -1,6 +1,6 @@
-"""CPU oracle of the learned guide -- TEST INFRASTRUCTURE ONLY.
+"""CPU oracle of the learned guides -- TEST INFRASTRUCTURE ONLY.
 
-The RBM guide and its variance-minimisation trainer have no counterpart in
+The RBM and MLP guides and their variance-minimisation trainer have no counterpart in
 the reference (PyGFMC trains its guides by NetKet VMC), so the checker is a
 direct float64 statement of the definitions with torch's CPU autograd for
 the derivatives:
@@ -10,8 +10,13 @@ the derivatives:
   L          = sum_w omega_w (e_L(x_w) - E)^2 / sum_w omega_w
 
 over every walker's connected configurations x'_s (the SpinHalf slots: site
-flips, then edges, with their couplings c_s(x) before the guide).  Only
-tests use it.
+flips, then edges; the BoseHubbard moves: hops, pair terms, b+ / b-; with
+their couplings c_s(x) before the guide).  The MLP guide,
+
+  log psi(x) = w3 . tanh(W2 bf16(tanh(W1 onehot(x) + b1)) + b2) + b3,
+
+passes its bf16 rounding straight through the derivative.  Only tests use
+it.
 """
 import numpy as np
 import torch
@@ -69,3 +74,53 @@ def variance_loss_and_grads(model, W, b, a, x, omega=None):
     Em, L = Em.detach(), L.detach()
     return (Em.item(), L.item(), Wt.grad.numpy().copy(), bt.grad.numpy().copy(),
             at.grad.numpy().copy())
+
+
+def _bose_moves(model, x):
+    """Couplings (n, n_off), successor occupations (n, n_off, N) (clipped to
+    [0, n_max] where a move has no element) and the diagonal (n,) of the
+    BoseHubbard moves (hamiltonian/bose_hubbard.py get_rates:285-393)."""
+    x = np.asarray(x, dtype=np.float64)
+    a, b, da, db = model.moves()
+    coup = np.stack([model.get_rates(xi)[0] for xi in x])
+    succ = np.repeat(x[:, None, :], len(a), axis=1)
+    k = np.arange(len(a))
+    succ[:, k, a] += da
+    succ[:, k, b] += db
+    succ = np.clip(succ, 0, model.n_max)
+    return coup[:, 1:], succ[:, 1:], coup[:, 0]
+
+
+def mlp_variance_loss_and_grads(model, W1, b1, W2, b2, w3, b3, x, omega=None, round_h1=True):
+    """(E, L, grads) in float64 for MLP parameters on the occupations x (n, N);
+    grads is a dict W1, b1, W2, b2, w3.  round_h1=False drops the bf16
+    rounding of the first layer (the loss is then smooth, for finite
+    differences)."""
+    c, xs, diag = _bose_moves(model, x)
+    N, nm = int(model.N), int(model.n_max)
+    T = {k: torch.tensor(np.asarray(v, np.float64), requires_grad=True)
+         for k, v in (("W1", W1), ("b1", b1), ("W2", W2), ("b2", b2), ("w3", w3))}
+
+    def logpsi(nconf):
+        nconf = np.asarray(nconf, np.int64)
+        onehot = np.zeros(nconf.shape[:-1] + (N * (nm + 1),))
+        np.put_along_axis(onehot, np.arange(N) * (nm + 1) + nconf, 1.0, axis=-1)
+        z1 = torch.tensor(onehot) @ T["W1"].T + T["b1"]
+        h1 = torch.tanh(z1)
+        if not round_h1:
+            h1b = h1
+        else:
+            h1r = h1.detach().float().bfloat16().double()
+            h1b = h1 + (h1r - h1).detach()
+        h2 = torch.tanh(h1b @ T["W2"].T + T["b2"])
+        return h2 @ T["w3"] + float(b3)
+
+    lp = logpsi(x)
+    lps = logpsi(xs)
+    C = torch.tensor(c)
+    e = torch.tensor(diag) + (C * torch.exp(lps - lp[:, None])).sum(1)
+    om = torch.ones_like(e) if omega is None else torch.tensor(np.asarray(omega, np.float64))
+    Em = (om * e).sum() / om.sum()
+    L = (om * (e - Em) ** 2).sum() / om.sum()
+    L.backward()
+    return (Em.item(), L.item(), {k: v.grad.numpy().copy() for k, v in T.items()})

@@ -111,6 +111,12 @@ SIGNATURES = {
     "gfmc_rbm_train_step": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp,
                                            ctypes.c_double, _dp, _vp]),
     "gfmc_rbm_get_params": (ctypes.c_int, [_vp, _fp, _fp, _fp]),
+    "gfmc_mlp_param_count": (ctypes.c_longlong, [_vp]),
+    "gfmc_mlp_gradient": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp, _vp, _dp,
+                                         _vp]),
+    "gfmc_mlp_train_step": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp,
+                                           ctypes.c_double, _dp, _vp]),
+    "gfmc_mlp_get_params": (ctypes.c_int, [_vp, _fp]),
     "gfmc_evolve": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                    ctypes.c_double, _u32p, ctypes.c_longlong, ctypes.c_int, _vp,
                                    _vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp]),

@@ -109,6 +109,18 @@ struct gfmc_handle {
   MlpTables mlp{};
   void *d_mlp = nullptr;
   int mlp_grid = 0;
+  // MLP trainer: scratch sized for mtr_cap walkers / mtr_rows rows, float32
+  // master parameters with their Adam moments, one gradient array
+  int mtr_cap = 0;
+  long long mtr_rows = 0;
+  void *mtr_cfg = nullptr;
+  float *mtr_rates = nullptr, *mtr_rsum = nullptr, *mtr_gw = nullptr, *mtr_coef = nullptr;
+  double *mtr_e = nullptr, *mtr_stats = nullptr;
+  __nv_bfloat16 *mtr_h1 = nullptr, *mtr_h1lo = nullptr, *mtr_h1T = nullptr, *mtr_d2 = nullptr,
+                *mtr_d2T = nullptr;
+  float *mtr_d1 = nullptr, *mtr_grad = nullptr, *mtr_p = nullptr, *mtr_m1 = nullptr,
+        *mtr_m2 = nullptr;
+  int mtr_step = 0;
   // RBM variance-minimisation scratch (sized for train_cap walkers) and the
   // float32 master parameters with their Adam moments
   int train_cap = 0;
@@ -197,7 +209,7 @@ int build_mlp(gfmc_handle *h, const gfmc_guide_desc *gd, int N, int n_max) {
   if (n_max < 1 || n_max > 254) return fail(GFMC_ERR_INVALID, "MLP guide: n_max must be in [1, 254]");
   const int np1 = n_max + 1;
   const size_t D = (size_t)N * np1;
-  std::vector<uint16_t> W1T(D * H1), W2((size_t)H2 * H1);
+  std::vector<uint16_t> W1T(D * H1), W2((size_t)H2 * H1), W2T((size_t)H1 * H2);
   std::vector<float> b1(H1), b2(H2), w3(H2);
   for (int j = 0; j < H1; ++j) {
     for (size_t c = 0; c < D; ++c) {
@@ -212,6 +224,7 @@ int build_mlp(gfmc_handle *h, const gfmc_guide_desc *gd, int N, int n_max) {
       const float w = gd->mlp_W2[(size_t)i * H1 + j];
       if (!std::isfinite(w)) return fail(GFMC_ERR_INVALID, "MLP W2 (%d, %d) is not finite", i, j);
       W2[(size_t)i * H1 + j] = bf16_bits(w);
+      W2T[(size_t)j * H2 + i] = bf16_bits(w);
     }
     b2[i] = gd->mlp_b2[i];
     const uint32_t u = (uint32_t)bf16_bits(gd->mlp_w3[i]) << 16;
@@ -219,11 +232,12 @@ int build_mlp(gfmc_handle *h, const gfmc_guide_desc *gd, int N, int n_max) {
   }
   const size_t s1 = W1T.size() * 2, s2 = W2.size() * 2;
   auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
-  const size_t o2 = al(s1), ob1 = o2 + al(s2), ob2 = ob1 + al((size_t)H1 * 4),
+  const size_t o2 = al(s1), o2t = o2 + al(s2), ob1 = o2t + al(s2), ob2 = ob1 + al((size_t)H1 * 4),
                ow3 = ob2 + al((size_t)H2 * 4), tot = ow3 + al((size_t)H2 * 4);
   std::vector<unsigned char> host(tot, 0);
   memcpy(host.data(), W1T.data(), s1);
   memcpy(host.data() + o2, W2.data(), s2);
+  memcpy(host.data() + o2t, W2T.data(), s2);
   memcpy(host.data() + ob1, b1.data(), (size_t)H1 * 4);
   memcpy(host.data() + ob2, b2.data(), (size_t)H2 * 4);
   memcpy(host.data() + ow3, w3.data(), (size_t)H2 * 4);
@@ -232,6 +246,7 @@ int build_mlp(gfmc_handle *h, const gfmc_guide_desc *gd, int N, int n_max) {
   unsigned char *base = (unsigned char *)h->d_mlp;
   h->mlp.W1T = (const __nv_bfloat16 *)base;
   h->mlp.W2 = (const __nv_bfloat16 *)(base + o2);
+  h->mlp.W2T = (const __nv_bfloat16 *)(base + o2t);
   h->mlp.b1 = (const float *)(base + ob1);
   h->mlp.b2 = (const float *)(base + ob2);
   h->mlp.w3 = (const float *)(base + ow3);
@@ -838,6 +853,117 @@ int rbm_gradient_t(gfmc_handle *h, int n, const void *cfg, const int32_t *parent
   return GFMC_OK;
 }
 
+// The variance-loss gradient of the MLP guide over the population
+// cfg[parents[i]] (float32 build): gather, the EVALUATE pass with per-move
+// rates, coefficients, the training rows, the three tensor-core GEMMs and the
+// one-hot layer.  Leaves the gradient (master-parameter order) in
+// mtr_grad and (E, var) in mtr_stats.
+int mlp_gradient_t(gfmc_handle *h, int n, const void *cfg, const int32_t *parents,
+                   int parents_valid, const double *omega, cudaStream_t s) {
+  const MlpTables &t = h->mlp;
+  if (t.H2 % 64)
+    return fail(GFMC_ERR_UNSUPPORTED, "MLP training needs mlp_H2 a multiple of 64, got %d", t.H2);
+  const int n_off = h->M - 1, rpw = n_off + 1, D = h->N * t.np1, CB = h->cfg_bytes;
+  if ((size_t)D * 64 * 4 > 200 * 1024)
+    return fail(GFMC_ERR_UNSUPPORTED, "MLP training supports at most 800 one-hot inputs, got %d", D);
+  const long long R = (long long)n * rpw, Mpad = (R + 127) / 128 * 128;
+  const size_t per_row = (size_t)t.H1 * 2 * 3 + (size_t)t.H2 * 2 * 4 + (size_t)t.H1 * 4 + 4;
+  if ((double)Mpad * per_row > 64e9)
+    return fail(GFMC_ERR_UNSUPPORTED, "MLP training scratch for %d walkers exceeds 64 GB", n);
+  const long long np = mlp_param_count(t.H1, t.H2, D);
+  if (n > h->mtr_cap || Mpad > h->mtr_rows) {
+    cudaFree(h->mtr_cfg); cudaFree(h->mtr_rates); cudaFree(h->mtr_rsum); cudaFree(h->mtr_gw);
+    cudaFree(h->mtr_e); cudaFree(h->mtr_coef); cudaFree(h->mtr_h1); cudaFree(h->mtr_h1T);
+    cudaFree(h->mtr_h1lo); cudaFree(h->mtr_d2); cudaFree(h->mtr_d2T); cudaFree(h->mtr_d1);
+    h->mtr_cfg = nullptr; h->mtr_rates = h->mtr_rsum = h->mtr_gw = h->mtr_coef = h->mtr_d1 = nullptr;
+    h->mtr_e = nullptr;
+    h->mtr_h1 = h->mtr_h1lo = h->mtr_h1T = h->mtr_d2 = h->mtr_d2T = nullptr;
+    h->mtr_cap = 0;
+    h->mtr_rows = 0;
+    GFMC_CUDA(cudaMalloc(&h->mtr_cfg, (size_t)n * CB));
+    GFMC_CUDA(cudaMalloc(&h->mtr_rates, sizeof(float) * (size_t)n * (n_off > 0 ? n_off : 1)));
+    GFMC_CUDA(cudaMalloc(&h->mtr_rsum, sizeof(float) * (size_t)n));
+    GFMC_CUDA(cudaMalloc(&h->mtr_gw, sizeof(float) * (size_t)n));
+    GFMC_CUDA(cudaMalloc(&h->mtr_e, sizeof(double) * (size_t)n));
+    GFMC_CUDA(cudaMalloc(&h->mtr_coef, sizeof(float) * (size_t)Mpad));
+    GFMC_CUDA(cudaMalloc(&h->mtr_h1, 2 * (size_t)Mpad * t.H1));
+    GFMC_CUDA(cudaMalloc(&h->mtr_h1T, 2 * (size_t)Mpad * t.H1));
+    GFMC_CUDA(cudaMalloc(&h->mtr_h1lo, 2 * (size_t)Mpad * t.H1));
+    GFMC_CUDA(cudaMalloc(&h->mtr_d2, 4 * (size_t)Mpad * t.H2));     // hi | lo
+    GFMC_CUDA(cudaMalloc(&h->mtr_d2T, 4 * (size_t)Mpad * t.H2));
+    GFMC_CUDA(cudaMalloc(&h->mtr_d1, 4 * (size_t)Mpad * t.H1));
+    h->mtr_cap = n;
+    h->mtr_rows = Mpad;
+  }
+  if (!h->mtr_stats) {
+    GFMC_CUDA(cudaMalloc(&h->mtr_stats, sizeof(double) * 2));
+    GFMC_CUDA(cudaMalloc(&h->mtr_grad, sizeof(float) * (size_t)np));
+  }
+  if (!h->ctr1) GFMC_CUDA(cudaMalloc(&h->ctr1, sizeof(int)));
+  if (!h->status) {
+    GFMC_CUDA(cudaMalloc(&h->status, sizeof(int)));
+    GFMC_CUDA(cudaMemset(h->status, 0, sizeof(int)));
+  }
+  cudaError_t e = launch_gather(n, CB, parents_valid ? parents : nullptr, cfg, h->mtr_cfg, nullptr,
+                                nullptr, nullptr, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->ctr1, 0, sizeof(int), s);
+  if (e == cudaSuccess) {
+    EvolveArgs a{};
+    a.method = EVALUATE;
+    a.n_walkers = n;
+    a.cfg_in = h->mtr_cfg;
+    a.e_loc = h->mtr_e;
+    a.work_ctr = h->ctr1;
+    a.status = h->status;
+    a.max_iters = 1;
+    a.rates_out = h->mtr_rates;
+    a.rsum_out = h->mtr_rsum;
+    e = launch_mlp_evolve(h->m32, t, a, h->mlp_grid, s);
+  }
+  if (e == cudaSuccess) e = launch_train_coeff(n, h->mtr_e, omega, h->mtr_gw, h->mtr_stats, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->mtr_grad, 0, sizeof(float) * (size_t)np, s);
+  if (e == cudaSuccess)
+    e = launch_mlp_rows(h->m32, t, h->mtr_cfg, CB, n, Mpad, h->mtr_rates, h->mtr_rsum, h->mtr_gw,
+                        h->mtr_coef, h->mtr_h1, h->mtr_h1lo, h->mtr_h1T, s);
+  float *gW1 = h->mtr_grad, *gb1 = gW1 + (size_t)t.H1 * D, *gW2 = gb1 + t.H1,
+        *gb2 = gW2 + (size_t)t.H2 * t.H1, *gw3 = gb2 + t.H2;
+  if (e == cudaSuccess) {
+    MlpGemmArgs g{};
+    g.mode = MLP_EPI_FWD;
+    g.A = h->mtr_h1; g.lda = t.H1;
+    g.B = t.W2; g.ldb = t.H1;
+    g.M = (int)Mpad; g.N = t.H2; g.K = t.H1;
+    g.coef = h->mtr_coef; g.b2 = t.b2; g.w3 = t.w3;
+    g.d2 = h->mtr_d2; g.d2T = h->mtr_d2T; g.ldT = 2 * Mpad;
+    g.g_w3 = gw3; g.g_b2 = gb2;
+    g.status = h->status;
+    e = launch_mlp_gemm(g, s);
+  }
+  if (e == cudaSuccess) {
+    MlpGemmArgs g{};
+    g.mode = MLP_EPI_BWD;
+    g.A = h->mtr_d2; g.lda = 2 * t.H2;          // [hi | lo] against W2^T twice
+    g.B = t.W2T; g.ldb = t.H2;
+    g.M = (int)Mpad; g.N = t.H1; g.K = 2 * t.H2; g.kb = t.H2;
+    g.h1 = h->mtr_h1; g.h1lo = h->mtr_h1lo; g.d1 = h->mtr_d1; g.g_b1 = gb1;
+    g.status = h->status;
+    e = launch_mlp_gemm(g, s);
+  }
+  if (e == cudaSuccess) {
+    MlpGemmArgs g{};
+    g.mode = MLP_EPI_ACC;
+    g.A = h->mtr_d2T; g.lda = 2 * Mpad;         // [hi^T | lo^T] against h1^T twice
+    g.B = h->mtr_h1T; g.ldb = Mpad;
+    g.M = t.H2; g.N = t.H1; g.K = (int)(2 * Mpad); g.kb = (int)Mpad;
+    g.C = gW2; g.ldc = t.H1;
+    g.status = h->status;
+    e = launch_mlp_gemm(g, s);
+  }
+  if (e == cudaSuccess) e = launch_mlp_dw1(h->m32, t, h->mtr_cfg, CB, n, h->mtr_d1, gW1, s);
+  if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "MLP gradient: %s", cudaGetErrorString(e));
+  return GFMC_OK;
+}
+
 template <typename T>
 int local_energy_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, int n,
                    const void *cfg, const int32_t *parents, double *e_loc, cudaStream_t s,
@@ -928,6 +1054,10 @@ int gfmc_destroy(gfmc_handle *h) {
   cudaFree(h->fw_partial); cudaFree(h->fw_logG); cudaFree(h->fw_E); cudaFree(h->ctr1);
   cudaFree(h->d_rbm);
   cudaFree(h->d_mlp);
+  cudaFree(h->mtr_cfg); cudaFree(h->mtr_rates); cudaFree(h->mtr_rsum); cudaFree(h->mtr_gw);
+  cudaFree(h->mtr_e); cudaFree(h->mtr_coef); cudaFree(h->mtr_h1); cudaFree(h->mtr_h1T);
+  cudaFree(h->mtr_h1lo); cudaFree(h->mtr_d2); cudaFree(h->mtr_d2T); cudaFree(h->mtr_d1); cudaFree(h->mtr_stats);
+  cudaFree(h->mtr_grad); cudaFree(h->mtr_p); cudaFree(h->mtr_m1); cudaFree(h->mtr_m2);
   cudaFree(h->tr_cfg); cudaFree(h->tr_theta); cudaFree(h->tr_rates); cudaFree(h->tr_rsum);
   cudaFree(h->tr_gw); cudaFree(h->tr_e); cudaFree(h->tr_stats); cudaFree(h->tr_gW);
   cudaFree(h->tr_gb); cudaFree(h->tr_ga); cudaFree(h->ms_W); cudaFree(h->ms_b); cudaFree(h->ms_a);
@@ -1267,6 +1397,80 @@ int gfmc_rbm_get_params(gfmc_handle *h, float *W, float *b, float *a) {
     }
   GFMC_CUDA(cudaMemcpy(b, r.b, sizeof(float) * r.H, cudaMemcpyDeviceToHost));
   GFMC_CUDA(cudaMemcpy(a, r.a, sizeof(float) * h->N, cudaMemcpyDeviceToHost));
+  return GFMC_OK;
+}
+
+long long gfmc_mlp_param_count(const gfmc_handle *h) {
+  if (!h || !h->mlp_on) return GFMC_ERR_INVALID;
+  return mlp_param_count(h->mlp.H1, h->mlp.H2, h->N * h->mlp.np1);
+}
+
+int gfmc_mlp_gradient(gfmc_handle *h, int n, const void *cfg, const int32_t *parents,
+                      int parents_valid, const double *omega, float *grad, double stats[2],
+                      void *stream) {
+  if (!h || n <= 0 || !cfg || !stats || (parents_valid && !parents))
+    return fail(GFMC_ERR_INVALID, "gfmc_mlp_gradient: bad argument");
+  if (!h->mlp_on) return fail(GFMC_ERR_INVALID, "gfmc_mlp_gradient: the handle has no MLP guide");
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc = mlp_gradient_t(h, n, cfg, parents, parents_valid, omega, s);
+  if (rc) return rc;
+  const long long np = mlp_param_count(h->mlp.H1, h->mlp.H2, h->N * h->mlp.np1);
+  if (grad)
+    GFMC_CUDA(cudaMemcpyAsync(grad, h->mtr_grad, sizeof(float) * (size_t)np,
+                              cudaMemcpyDeviceToDevice, s));
+  GFMC_CUDA(cudaMemcpyAsync(stats, h->mtr_stats, sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
+  GFMC_CUDA(cudaStreamSynchronize(s));
+  return GFMC_OK;
+}
+
+int gfmc_mlp_train_step(gfmc_handle *h, int n, const void *cfg, const int32_t *parents,
+                        int parents_valid, const double *omega, double lr, double stats[2],
+                        void *stream) {
+  if (!h || n <= 0 || !cfg || !stats || (parents_valid && !parents) || !(lr > 0.0))
+    return fail(GFMC_ERR_INVALID, "gfmc_mlp_train_step: bad argument");
+  if (!h->mlp_on) return fail(GFMC_ERR_INVALID, "gfmc_mlp_train_step: the handle has no MLP guide");
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc = mlp_gradient_t(h, n, cfg, parents, parents_valid, omega, s);
+  if (rc) return rc;
+  const MlpTables &t = h->mlp;
+  const int D = h->N * t.np1;
+  const long long np = mlp_param_count(t.H1, t.H2, D);
+  if (!h->mtr_p) {
+    GFMC_CUDA(cudaMalloc(&h->mtr_p, sizeof(float) * (size_t)np));
+    GFMC_CUDA(cudaMalloc(&h->mtr_m1, sizeof(float) * (size_t)np));
+    GFMC_CUDA(cudaMalloc(&h->mtr_m2, sizeof(float) * (size_t)np));
+    GFMC_CUDA(cudaMemsetAsync(h->mtr_m1, 0, sizeof(float) * (size_t)np, s));
+    GFMC_CUDA(cudaMemsetAsync(h->mtr_m2, 0, sizeof(float) * (size_t)np, s));
+    cudaError_t e = launch_mlp_master_init(t, D, h->mtr_p, s);
+    if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "MLP master init: %s", cudaGetErrorString(e));
+    h->mtr_step = 0;
+  }
+  h->mtr_step += 1;
+  cudaError_t e = launch_mlp_adam(np, h->mtr_p, h->mtr_grad, h->mtr_m1, h->mtr_m2, (float)lr,
+                                  h->mtr_step, s);
+  if (e == cudaSuccess)
+    e = launch_mlp_tables(t, D, h->mtr_p, (__nv_bfloat16 *)t.W1T, (float *)t.b1,
+                          (__nv_bfloat16 *)t.W2, (__nv_bfloat16 *)t.W2T, (float *)t.b2,
+                          (float *)t.w3, s);
+  if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "MLP Adam step: %s", cudaGetErrorString(e));
+  // the guide changed: the carried z1 and log psi are stale
+  h->field_valid = 0;
+  GFMC_CUDA(cudaMemcpyAsync(stats, h->mtr_stats, sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
+  GFMC_CUDA(cudaStreamSynchronize(s));
+  return GFMC_OK;
+}
+
+int gfmc_mlp_get_params(gfmc_handle *h, float *params) {
+  if (!h || !h->mlp_on || !params) return fail(GFMC_ERR_INVALID, "gfmc_mlp_get_params: bad argument");
+  const MlpTables &t = h->mlp;
+  const int D = h->N * t.np1;
+  const long long np = mlp_param_count(t.H1, t.H2, D);
+  float *tmp = nullptr;
+  GFMC_CUDA(cudaMalloc(&tmp, sizeof(float) * (size_t)np));
+  cudaError_t e = launch_mlp_master_init(t, D, tmp, 0);
+  if (e == cudaSuccess) e = cudaMemcpy(params, tmp, sizeof(float) * (size_t)np, cudaMemcpyDeviceToHost);
+  cudaFree(tmp);
+  if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "gfmc_mlp_get_params: %s", cudaGetErrorString(e));
   return GFMC_OK;
 }
 

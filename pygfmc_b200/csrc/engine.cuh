@@ -104,8 +104,8 @@ struct EvolveArgs {
   int max_iters;          // per-walker hop cap
   const void *field_in;   // carried guide fields (N per walker), read at parents[w]; nullable
   void *field_out;        // guide fields after the step (N per walker); nullable
-  float *rates_out;       // EVALUATE, RBM guide: (n_walkers, M - 1) guided rates; nullable
-  float *rsum_out;        // EVALUATE, RBM guide: (n_walkers,) sum of those rates; nullable
+  float *rates_out;       // EVALUATE, learned guides: (n_walkers, M - 1) guided rates; nullable
+  float *rsum_out;        // EVALUATE, learned guides: (n_walkers,) sum of those rates; nullable
   double *diag_out;       // EVALUATE: (n_walkers,) diagonal element H_xx; nullable
   long long walker_offset;  // global index of walker 0 (streams fold_in(key, offset + i))
 };

@@ -42,12 +42,14 @@
 #include <cuda_bf16.h>
 
 #include "mlp.cuh"
+#include "mlp_dev.cuh"
 #include "tc05.cuh"
 
 namespace gfmc {
 namespace {
 
 using namespace tc;
+using namespace mlpdev;
 
 constexpr int ROWS = 128;               // moves per tile = UMMA M = TMEM lanes
 constexpr int PT = 2 * ROWS;            // threads per pipeline: two per row
@@ -56,99 +58,6 @@ constexpr int MT = PT * NP;
 constexpr int KC = 64;                  // inputs per A chunk (one 128-byte swizzle row)
 constexpr int NBUF = 2;                 // A chunk buffers per pipeline
 constexpr unsigned FULLW = 0xffffffffu;
-
-// tanh y = 1 - 2 / (1 + e^{2y}) with e^{2y} = 2^{K y}, K = 2 log2(e): one
-// ex2 and one rcp (absolute error about 1e-7; e^{2y} overflowing to inf
-// gives 1, underflowing to 0 gives -1).
-constexpr float KT = 2.8853900817779268f;
-
-__device__ __forceinline__ float ex2_approx(float x) {
-  float y;
-  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
-
-__device__ __forceinline__ float rcp_approx(float x) {
-  float y;
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
-
-// 1 / (1 + e^{2y}) from Ky = K y: tanh y = 1 - 2 of it.
-__device__ __forceinline__ float sig2(float Ky) { return rcp_approx(1.0f + ex2_approx(Ky)); }
-
-// Moves of the Bose-Hubbard layout (bose_hubbard.py; _common.two_site_move):
-// sites a, b, occupation changes da, db (b == a, db = 0 for the single-site
-// h_pm moves) and the unguided off-diagonal element.
-struct Mv {
-  int a, b, da, db;
-  float v;
-};
-
-__device__ __forceinline__ Mv mlp_move(const DevModel<float> &m, const uint8_t *occ, int o) {
-  Mv mv;
-  const int E = m.E;
-  const float nmax = (float)m.n_max;
-  int blk;
-  int idx;
-  if (m.n_hop && o < 2 * E) {
-    const int e = o < E ? o : o - E;
-    const uint32_t pe = m.edge[e];
-    mv.a = pe & 0xFFFF; mv.b = pe >> 16; idx = e;
-    if (o < E) { mv.da = -1; mv.db = 1; blk = 0; } else { mv.da = 1; mv.db = -1; blk = 1; }
-  } else {
-    if (m.n_hop) o -= 2 * E;
-    if (m.n_eta && o < 2 * E) {
-      const int e = o < E ? o : o - E;
-      const uint32_t pe = m.edge[e];
-      mv.a = pe & 0xFFFF; mv.b = pe >> 16; idx = e;
-      if (o < E) { mv.da = 1; mv.db = 1; blk = 2; } else { mv.da = -1; mv.db = -1; blk = 3; }
-    } else {
-      if (m.n_eta) o -= 2 * E;
-      const int k = o < m.N ? o : o - m.N;
-      mv.a = mv.b = k; idx = k; mv.db = 0;
-      if (o < m.N) { mv.da = 1; blk = 4; } else { mv.da = -1; blk = 5; }
-    }
-  }
-  const float na = (float)occ[mv.a], nb = (float)occ[mv.b];
-  switch (blk) {
-    case 0: mv.v = -m.t[idx] * sqrtf(na * (nb + 1.0f)) * (nb < nmax ? 1.0f : 0.0f); break;
-    case 1: mv.v = -m.t[idx] * sqrtf((na + 1.0f) * nb) * (na < nmax ? 1.0f : 0.0f); break;
-    case 2:
-      mv.v = -m.eta[idx] * sqrtf((na + 1.0f) * (nb + 1.0f)) * ((na < nmax && nb < nmax) ? 1.0f : 0.0f);
-      break;
-    case 3: mv.v = -m.eta[idx] * sqrtf(na * nb); break;
-    case 4: mv.v = m.hpm[idx] * sqrtf(na + 1.0f) * (na < nmax ? 1.0f : 0.0f); break;
-    default: mv.v = m.hpm[idx] * sqrtf(na); break;
-  }
-  // a move that leaves [0, n_max] has no element (and reads no W1 column),
-  // whatever the couplings hold
-  const int a1 = (int)occ[mv.a] + mv.da, b1 = (int)occ[mv.b] + mv.db;
-  if (a1 < 0 || a1 > m.n_max || b1 < 0 || b1 > m.n_max) mv.v = 0.0f;
-  return mv;
-}
-
-// W1 columns a move exchanges: (old a, new a, old b, new b); x < 0 for none
-// (the current configuration), z < 0 for a single-site move.
-__device__ __forceinline__ int4 move_cols(const Mv &mv, const uint8_t *occ, int np1) {
-  const int ca0 = mv.a * np1 + occ[mv.a];
-  int4 c = make_int4(ca0, ca0 + mv.da, -1, -1);
-  if (mv.b != mv.a) {
-    const int cb0 = mv.b * np1 + occ[mv.b];
-    c.z = cb0;
-    c.w = cb0 + mv.db;
-  }
-  return c;
-}
-
-__device__ __forceinline__ void bf8(const uint4 &u, float (&f)[8]) {
-  const __nv_bfloat162 *p = reinterpret_cast<const __nv_bfloat162 *>(&u);
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    f[2 * i] = __low2float(p[i]);
-    f[2 * i + 1] = __high2float(p[i]);
-  }
-}
 
 // acc + sum_i wm_i / (1 + 2^{K v_i + bk_i}) over 32 accumulator columns.
 __device__ __forceinline__ float reduce32(const uint32_t (&r)[32], const float *bk, const float *wm,
@@ -574,11 +483,15 @@ __global__ void __launch_bounds__(MT, 1) mlp_evolve_kernel(DevModel<float> m, Ml
         if (lane == 0) {
           bf[0] = d - R;
           bf[3] = d;
+          if (a.rsum_out) a.rsum_out[walker] = -R;
         }
       }
       pipe_sync(s);
       eloc = bf[0];
       if (leader && a.diag_out) a.diag_out[walker] = (double)bf[3];
+      // the guided elements of every move (the trainer's row coefficients)
+      if (a.rates_out)
+        for (int o = tp; o < m.n_off; o += PT) a.rates_out[(size_t)walker * m.n_off + o] = rates[o];
     }
     if (!ok) break;
     if (a.cfg_out) {

@@ -488,6 +488,54 @@ class GFMCEngine:
                                               a.ctypes.data_as(P)), "gfmc_rbm_get_params")
         return W, b, a
 
+    def _mlp_split(self, flat):
+        """The MLP parameter order W1 (H1, D), b1, W2 (H2, H1), b2, w3 as views."""
+        g = self.guide
+        H1, H2, D = g.H1, g.H2, g.N * (g.n_max + 1)
+        sizes = [("W1", (H1, D)), ("b1", (H1,)), ("W2", (H2, H1)), ("b2", (H2,)), ("w3", (H2,))]
+        out, o = {}, 0
+        for name, shp in sizes:
+            k = int(np.prod(shp))
+            out[name] = flat[o:o + k].reshape(shp)
+            o += k
+        return out
+
+    def mlp_gradient(self, omega=None):
+        """Variance-loss gradient of the MLP guide over the current population:
+        a dict of float32 device tensors (W1, b1, W2, b2, w3) and (E, var)."""
+        torch = self.torch
+        np_ = int(self.L.gfmc_mlp_param_count(self.h))
+        _lib.check(np_ if np_ < 0 else 0, "gfmc_mlp_param_count")
+        grad = torch.empty(np_, dtype=torch.float32, device=self.device)
+        st = np.zeros(2, dtype=np.float64)
+        om = self._ptr(omega) if omega is not None else ctypes.c_void_p(0)
+        _lib.check(self.L.gfmc_mlp_gradient(
+            self.h, self.n, self._ptr(self.cfg), self._ptr(self.parents), int(self.parents_valid), om,
+            self._ptr(grad), st.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), self._stream()),
+            "gfmc_mlp_gradient")
+        return self._mlp_split(grad), (float(st[0]), float(st[1]))
+
+    def mlp_train_step(self, lr, omega=None):
+        """One Adam step of the MLP guide on the current population; returns
+        (E, var) of the population before the step."""
+        st = np.zeros(2, dtype=np.float64)
+        om = self._ptr(omega) if omega is not None else ctypes.c_void_p(0)
+        _lib.check(self.L.gfmc_mlp_train_step(
+            self.h, self.n, self._ptr(self.cfg), self._ptr(self.parents), int(self.parents_valid), om,
+            float(lr), st.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), self._stream()),
+            "gfmc_mlp_train_step")
+        return float(st[0]), float(st[1])
+
+    def mlp_parameters(self):
+        """The guide's current parameters as used (bf16 weight values): a dict
+        of host float32 arrays W1, b1, W2, b2, w3."""
+        np_ = int(self.L.gfmc_mlp_param_count(self.h))
+        _lib.check(np_ if np_ < 0 else 0, "gfmc_mlp_param_count")
+        flat = np.zeros(np_, dtype=np.float32)
+        _lib.check(self.L.gfmc_mlp_get_params(self.h, flat.ctypes.data_as(ctypes.POINTER(ctypes.c_float))),
+                   "gfmc_mlp_get_params")
+        return {k: v.copy() for k, v in self._mlp_split(flat).items()}
+
     def copy_population_from(self, other):
         """This engine's population := other's current population (gathered
         through its parent map); weights and local energies restart."""

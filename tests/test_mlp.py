@@ -255,3 +255,91 @@ def test_mlp_guided_run_matches_exact_energy():
     Ej, err = P.estimators.jackknife_energy([32], raw["log_weights"], raw["energy"], 15)
     E0 = _exact_ground_energy(L, n_max, **BH)
     assert abs(Ej[32] - E0) < max(3e-3 * abs(E0), 4 * err[32]), (Ej[32], err[32], E0)
+
+
+# ---- trainer ----------------------------------------------------------------
+
+def test_mlp_oracle_gradient_matches_finite_differences():
+    """The float64 autograd statement of the variance loss (without the bf16
+    rounding of h1, which makes the loss piecewise constant in W1, b1)."""
+    from oracle import learned
+    H = _bh(6, 2)
+    G = P.MLPBoseHubbard(6, 2, hidden=(64, 64), seed=3, sigma=0.3, b1=0.05, b2=-0.05, b3=0.2)
+    x = _occupations(10, 6, 2, 1)
+    base = {"W1": G.W1, "b1": G.b1, "W2": G.W2, "b2": G.b2, "w3": G.w3}
+    base = {k: np.asarray(v, np.float64) for k, v in base.items()}
+    order = ("W1", "b1", "W2", "b2", "w3")
+    _, _, g = learned.mlp_variance_loss_and_grads(H, *[base[k] for k in order], G.b3, x,
+                                                  round_h1=False)
+    eps = 1e-6
+    for name, idx in (("W1", (1, 5)), ("W1", (7, 0)), ("b1", (4,)), ("W2", (2, 7)), ("b2", (5,)),
+                      ("w3", (3,))):
+        p = {k: v.copy() for k, v in base.items()}
+        q = {k: v.copy() for k, v in base.items()}
+        p[name][idx] += eps
+        q[name][idx] -= eps
+        Lp = learned.mlp_variance_loss_and_grads(H, *[p[k] for k in order], G.b3, x, round_h1=False)[1]
+        Lq = learned.mlp_variance_loss_and_grads(H, *[q[k] for k in order], G.b3, x, round_h1=False)[1]
+        fd = (Lp - Lq) / (2 * eps)
+        assert abs(fd - g[name][idx]) < 1e-6 * max(1.0, abs(fd)), (name, idx, fd, g[name][idx])
+
+
+def _trainer_systems():
+    out = []
+    for (L, n_max, hidden, sigma, n, kw) in ((6, 2, (64, 64), 0.2, 96, {}),
+                                             (16, 3, (128, 128), 0.1, 128, {"eta": 0.0}),
+                                             (64, 4, (256, 256), 0.05, 48, {"eta": 0.0, "h_pm": None,
+                                                                            "mu": 0.0, "U": 3.0})):
+        H = _bh(L, n_max, **kw)
+        rng = np.random.default_rng(L + 1)
+        G = P.MLPBoseHubbard(L, n_max, hidden=hidden, seed=L, sigma=sigma,
+                             b1=rng.normal(0, 0.1, hidden[0]), b2=rng.normal(0, 0.1, hidden[1]))
+        x = _occupations(n, L, n_max, 3 * L)
+        out.append((f"L{L}_h{hidden[0]}", H, G, x))
+    return out
+
+
+@pytest.mark.gpu
+def test_mlp_device_gradient_matches_oracle():
+    """gfmc_mlp_gradient (second layer forward, its backward and dW2 on the
+    tensor cores, one-hot first layer accumulated) against float64 autograd
+    with the same straight-through bf16 rounding: E and L to float32
+    accuracy, each gradient block to 3e-2 in relative norm."""
+    from oracle import learned
+    P._lib.load()
+    for name, H, G, x in _trainer_systems():
+        eng = P.GFMCEngine(H, G, x.shape[0], precision="mixed")
+        eng.load(x)
+        grads, (E, L) = eng.mlp_gradient()
+        rE, rL, rg = learned.mlp_variance_loss_and_grads(H, G.W1, G.b1, G.W2, G.b2, G.w3, G.b3, x)
+        assert abs(E - rE) < 1e-4 * abs(rE) + 1e-6 and abs(L - rL) < 3e-3 * rL + 1e-6, (name, E, rE, L, rL)
+        for k, ref in rg.items():
+            got = grads[k].cpu().numpy().astype(np.float64)
+            err = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+            assert err < 3e-2, (name, k, err)
+        assert eng.status() == 0, name
+
+
+@pytest.mark.gpu
+def test_mlp_training_lowers_variance_and_keeps_the_exact_energy():
+    """6-site Bose-Hubbard chain: training on GFMC walkers lowers the
+    local-energy variance well below the untrained guide's, and a production
+    run with the trained guide gives the exact ground-state energy within its
+    error bar."""
+    P._lib.load()
+    L, n_max = 6, 2
+    H = _bh(L, n_max)
+    G0 = P.MLPBoseHubbard(L, n_max, hidden=(64, 64), seed=0, sigma=0.01)
+    w = P.prepare_walkers_random(1024, L, P.PRNGKey(0), states=(0.0, 1.0, 2.0))
+    trained, hist = P.learn.train_mlp_guide(w, H, G0, n_iterations=150, steps_per_iteration=4,
+                                            step_size=0.1, lr=3e-3, rng_key=P.PRNGKey(1),
+                                            warmup_steps=50, verbosity=0)
+    v0, v1 = hist["variance"][:5].mean(), hist["variance"][-10:].mean()
+    assert not hist["collapsed"]
+    assert v1 < 0.5 * v0, (v0, v1)
+    _, E, _, st, raw = P.run(P.prepare_walkers_random(2048, L, P.PRNGKey(5), states=(0.0, 1.0, 2.0)),
+                             1500, H, 0.1, trained, [8, 32], rng_key=P.PRNGKey(6), warmup_steps=200,
+                             verbosity=0)
+    Ej, err = P.estimators.jackknife_energy([32], raw["log_weights"], raw["energy"], 15)
+    E0 = _exact_ground_energy(L, n_max, **BH)
+    assert abs(Ej[32] - E0) < max(4 * err[32], 3e-3 * abs(E0)), (Ej[32], err[32], E0)
