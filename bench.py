@@ -118,26 +118,60 @@ def cpu_reference(P, cfg_sample, alw, steps, warmup, seed_key):
     return len(cfg) * steps / sum(times), threads, sum(times)
 
 
-def sigma_study(P, args):
-    """GPU seconds to sigma(E/N) = 1e-5: the plain float64 Jastrow engine
-    against the float32/bf16 RBM guide trained on the run's own walkers by
-    variance minimisation, on the 16x16 Heisenberg lattice (long-range
-    Jastrow; RBM H = 512, 65536 walkers, tau = 0.05, p = 128) or the 432-site
-    kagome XXZ lattice (nearest-neighbour Jastrow; RBM H = 432, 131072
-    walkers, tau = 0.02, p = 256).  Each method runs warm-up + production
-    through run(); the blocked jackknife error at the largest window gives
-    sigma(E/N); the time to the target is the production GPU time x
-    (sigma / 1e-5)^2 (errors fall as 1/sqrt(steps)).  The RBM's training time
-    is reported beside it."""
-    import torch
+def study_system(P, args):
+    """The learned-vs-plain workloads of the sigma study: the RBM on the 16x16
+    Heisenberg or the kagome lattice (see rbm_system), or the dense MLP
+    (320 -> 256 -> 256 -> 1) on the 64-site Bose-Hubbard ring against the
+    Gutzwiller + density-Jastrow guide (32768 walkers, tau = 0.02,
+    p = [16, 64])."""
+    if args.lattice == "bose64":
+        e, H, GJ = bose_chain(P)
+        G0 = P.MLPBoseHubbard(64, 4, hidden=(256, 256), seed=0, sigma=0.01)
+
+        def walk(n, key):
+            return P.prepare_walkers_occupations(n, 64, 64, 4, key)
+
+        def train(w, G):
+            return P.learn.train_mlp_guide(w, H, G, n_iterations=args.train_iters,
+                                           steps_per_iteration=3, step_size=0.02, lr=args.train_lr,
+                                           rng_key=P.PRNGKey(14), warmup_steps=100, verbosity=0)
+        return {"name": "bose_hubbard_ring64", "H": H, "plain": GJ, "G0": G0, "N": 64,
+                "learned": "mlp_256x256_mixed", "n_learned": N_WALKERS, "tau": 0.02,
+                "p": [16, 64], "walk": walk, "train": train,
+                "plain_name": "gutzwiller_density_jastrow"}
     lat, H, G, hid, tau, n_rbm, name = rbm_system(P, args.lattice)
     N = lat.N
-    out = {}
-    p_arr = [8, 32, 128] if args.lattice == "square16" else [16, 64, 256]
+
+    def walk(n, key):
+        return P.prepare_walkers_sz(n, N, key, sz=0)
+
+    def train(w, G0):
+        return P.learn.train_rbm_guide(w, H, G0, n_iterations=args.train_iters,
+                                       steps_per_iteration=3, step_size=tau, lr=args.train_lr,
+                                       rng_key=P.PRNGKey(14), warmup_steps=100, verbosity=0)
+    return {"name": name, "H": H, "plain": G, "G0": P.RBMSpinHalf(N, hid, seed=0, sigma=0.01),
+            "N": N, "learned": f"rbm_h{hid}_mixed", "n_learned": n_rbm, "tau": tau,
+            "p": [8, 32, 128] if args.lattice == "square16" else [16, 64, 256], "walk": walk,
+            "train": train,
+            "plain_name": "longrange_jastrow" if args.lattice == "square16" else "nn_jastrow"}
+
+
+def sigma_study(P, args):
+    """GPU seconds to sigma(E/N) = 1e-5: the plain Jastrow engine (float64 and
+    float32) against a learned guide trained on the run's own walkers by
+    variance minimisation, on the workload of study_system.  Each method runs
+    warm-up + production through run(); the blocked jackknife error at the
+    largest window gives sigma(E/N); the time to the target is the production
+    GPU time x (sigma / 1e-5)^2 (errors fall as 1/sqrt(steps)).  The learned
+    guide's training time is reported beside it."""
+    import torch
+    S = study_system(P, args)
+    H, N, tau, p_arr = S["H"], S["N"], S["tau"], S["p"]
     pm = p_arr[-1]
+    out = {}
 
     def measure(key, guide, n, steps, warm, precision):
-        w = P.prepare_walkers_sz(n, N, P.PRNGKey(11), sz=0)
+        w = S["walk"](n, P.PRNGKey(11))
         torch.cuda.synchronize()
         wf, E, _, st, raw = P.run(w, steps, H, tau, guide, p_arr, rng_key=P.PRNGKey(12),
                                   warmup_steps=warm, verbosity=0, precision=precision)
@@ -150,15 +184,11 @@ def sigma_study(P, args):
                     "walker_steps_per_s": n * steps / t,
                     "local_energy_var_per_site": float(np.var(wf.e_loc) / N)}
 
-    measure("jastrow_fp64", G, N_WALKERS, args.study_steps, 2000, "fp64")
-    measure("jastrow_mixed", G, N_WALKERS, args.study_steps, 2000, "mixed")
-    G0 = P.RBMSpinHalf(N, hid, seed=0, sigma=0.01)
-    w = P.prepare_walkers_sz(n_rbm, N, P.PRNGKey(13), sz=0)
-    trained, hist = P.learn.train_rbm_guide(w, H, G0, n_iterations=args.train_iters,
-                                            steps_per_iteration=3, step_size=tau, lr=args.train_lr,
-                                            rng_key=P.PRNGKey(14), warmup_steps=100, verbosity=0)
-    rk = f"rbm_h{hid}_mixed"
-    measure(rk, trained, n_rbm, args.rbm_steps, 500, "mixed")
+    measure("jastrow_fp64", S["plain"], N_WALKERS, args.study_steps, 2000, "fp64")
+    measure("jastrow_mixed", S["plain"], N_WALKERS, args.study_steps, 2000, "mixed")
+    trained, hist = S["train"](S["walk"](S["n_learned"], P.PRNGKey(13)), S["G0"])
+    rk = S["learned"]
+    measure(rk, trained, S["n_learned"], args.rbm_steps, 500, "mixed")
     r = out[rk]
     r["training_gpu_s"] = hist["seconds"]
     r["train_var_per_site_first_last"] = [float(hist["variance"][0] / N),
@@ -169,10 +199,9 @@ def sigma_study(P, args):
     r["gpu_s_to_1e-5_with_training"] = r["gpu_s_to_1e-5"] + hist["seconds"]
     j = out["jastrow_fp64"]
     diff = abs(j["E_per_site"] - r["E_per_site"]) / np.hypot(j["sigma_per_site"], r["sigma_per_site"])
-    plain = "longrange_jastrow" if args.lattice == "square16" else "nn_jastrow"
     line = {"metric": "GPU-s to sigma(E/N)=1e-5", "value": r["gpu_s_to_1e-5"], "unit": "s",
             "higher_is_better": False, "n_gpus": 1, "data": "synthetic",
-            "config": {"workload": f"{name}_rbm_h{hid}_vs_{plain}", "tau": tau, "p": pm,
+            "config": {"workload": f"{S['name']}_{rk}_vs_{S['plain_name']}", "tau": tau, "p": pm,
                        "jackknife_blocks": 20},
             "methods": out,
             "learned_over_jastrow_fp64_time_ratio": r["gpu_s_to_1e-5"] / j["gpu_s_to_1e-5"],
@@ -304,8 +333,9 @@ def mlp_bench(P, args):
     64 bosons (n_max = 4, t = 1, U = 3; M = 129), dense MLP guide
     320 -> 256 -> 256 -> 1 (tanh, bf16 weights N(0, 0.01^2)), float32 build,
     32768 walkers drawn uniformly with sum n = 64, cont_time tau = 0.02.
-    Times the MLP-guided branching step and, beside it, the same step under
-    the Gutzwiller + density-Jastrow guide (float64 and float32 builds)."""
+    Times the MLP-guided branching step, one training step
+    (gfmc_mlp_train_step) and, beside them, the same branching step under the
+    Gutzwiller + density-Jastrow guide (float64 and float32 builds)."""
     import torch
     e, H, GJ = bose_chain(P)
     hid = min(args.hidden, 256)
@@ -315,6 +345,7 @@ def mlp_bench(P, args):
     tau = 0.02
     wk = max(args.warmup, 3)
     out = {}
+    train_ms = None
     for name, guide, prec in (("mlp", G, "mixed"), ("jastrow_fp64", GJ, "fp64"),
                               ("jastrow_mixed", GJ, "mixed")):
         eng = P.GFMCEngine(H, guide, n, precision=prec)
@@ -322,6 +353,17 @@ def mlp_bench(P, args):
         alw = float((-eng.local_energy()).mean().item())
         ms, hpw = timed_steps(P, eng, alw, tau, args.steps, wk, P.PRNGKey(1000))
         out[name] = (ms, hpw)
+        if name == "mlp" and hid % 64 == 0:
+            # one variance-minimisation step (gfmc_mlp_train_step) on this population
+            stream = torch.cuda.current_stream()
+            eng.mlp_train_step(1e-4)
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            eng.mlp_train_step(1e-4)
+            b.record(stream)
+            b.synchronize()
+            train_ms = a.elapsed_time(b)
         del eng
         torch.cuda.synchronize()
     ms, hpw = out["mlp"]
@@ -339,6 +381,7 @@ def mlp_bench(P, args):
             "config": {"workload": f"bose_hubbard_ring64_mlp_{hid}x{hid}_cont_time", "n_walkers": n,
                        "tau": tau, "l2": "flushed (256 MB write) before every timed step",
                        "hops_per_walker_step": hpw},
+            "train_step_ms": train_ms,
             "jastrow_fp64": {"value": n / (out["jastrow_fp64"][0] / 1e3),
                              "ms_per_step": out["jastrow_fp64"][0]},
             "jastrow_mixed": {"value": n / (out["jastrow_mixed"][0] / 1e3),
@@ -366,7 +409,8 @@ def main():
     ap.add_argument("--study", default=None, choices=["sigma"],
                     help="sigma: GPU seconds to sigma(E/N)=1e-5, RBM vs Jastrow (minutes)")
     ap.add_argument("--study-steps", type=int, default=4000)
-    ap.add_argument("--rbm-steps", type=int, default=1000)
+    ap.add_argument("--rbm-steps", type=int, default=1000,
+                    help="--study sigma: production steps of the learned guide")
     ap.add_argument("--train-iters", type=int, default=600)
     ap.add_argument("--train-lr", type=float, default=3e-4)
     ap.add_argument("--guide", default="jastrow", choices=["jastrow", "rbm", "mlp"],
@@ -374,8 +418,10 @@ def main():
                          "ring with the dense MLP guide")
     ap.add_argument("--hidden", type=int, default=None,
                     help="hidden units of the learned guide (default: the workload's)")
-    ap.add_argument("--lattice", default="square16", choices=["square16", "kagome12"],
-                    help="--guide rbm: the 16x16 Heisenberg or the 432-site kagome XXZ workload")
+    ap.add_argument("--lattice", default="square16", choices=["square16", "kagome12", "bose64"],
+                    help="--guide rbm / --study sigma: the 16x16 Heisenberg, the 432-site kagome "
+                         "XXZ workload, or (--study sigma) the 64-site Bose-Hubbard ring with the "
+                         "MLP guide")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -389,6 +435,8 @@ def main():
     args.walkers_set = args.walkers != N_WALKERS
     if args.hidden is None:
         args.hidden = 256 if args.guide == "mlp" else 512
+    if args.guide == "rbm" and args.lattice == "bose64":
+        ap.error("--guide rbm runs on --lattice square16 or kagome12")
     if args.guide == "rbm":
         if rank == 0:
             rbm_bench(P, args)
