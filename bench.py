@@ -40,6 +40,14 @@ L = 16
 TAU = 0.05
 
 
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one
+# evolve_kernel launch of this workload, from a one-pass ncu capture of
+# `bench.py --steps 20 --warmup 3 --no-cpu-baseline` (32768 walkers, float64):
+# 61 MB read + 20 MB written; part of the carried fields stays in L2 across
+# the step, so DRAM sees less than the algorithmic bytes.
+EVOLVE_TRAFFIC_BYTES = {("fp64", 32768): 81.0e6}
+
+
 def build_system(P, precision):
     lat = P.square(L)
     H = P.SpinHalf.create(lat.edges, J_x=-1.0, J_y=-1.0, J_z=1.0, dtype=np.float64)
@@ -54,19 +62,63 @@ def build_system(P, precision):
     return lat, H, G, pairs, 0.3 / r
 
 
-def sample_clocks(stop, out):
-    cmd = ["nvidia-smi", "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,"
-           "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-           "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-           "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits"]
-    while not stop.is_set():
+CLOCK_FIELDS = ("uuid,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+
+class ClockSampler:
+    """nvidia-smi sampling this process's GPU every 50 ms while it runs (one
+    nvidia-smi process, stopped through its own handle).  start() returns once
+    the first sample has arrived, so the samples cover what runs after it."""
+
+    def __init__(self, uuid):
+        self.uuid = (uuid or "").lower()
+        self.lines, self.proc, self.th = [], None, None
+
+    def start(self):
         try:
-            r = subprocess.run(cmd, capture_output=True, text=True, timeout=5)
-            if r.returncode == 0 and r.stdout.strip():
-                out.append(r.stdout.strip().splitlines()[0])
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={CLOCK_FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
-            pass
-        stop.wait(0.2)
+            self.proc = None
+            return self
+
+        def read():
+            for ln in self.proc.stdout:
+                ln = ln.strip()
+                if ln and (not self.uuid or self.uuid in ln.split(",")[0].strip().lower()):
+                    self.lines.append(ln)
+
+        self.th = threading.Thread(target=read, daemon=True)
+        self.th.start()
+        t0 = time.time()
+        while not self.lines and time.time() - t0 < 10 and self.proc.poll() is None:
+            time.sleep(0.01)
+        self.n0 = len(self.lines)
+        return self
+
+    def stop(self):
+        """The samples taken between start() and now."""
+        if self.proc is None:
+            return []
+        n1 = len(self.lines)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.th.join(timeout=2)
+        return self.lines[max(self.n0 - 1, 0):n1]
+
+
+def gpu_uuid(torch, dev):
+    try:
+        u = str(torch.cuda.get_device_properties(dev).uuid)
+        return u if u.startswith("GPU-") else "GPU-" + u
+    except Exception:
+        return ""
 
 
 def summarize_clocks(lines):
@@ -74,14 +126,14 @@ def summarize_clocks(lines):
     names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
     for ln in lines:
         f = [x.strip() for x in ln.split(",")]
-        if len(f) < 9:
+        if len(f) < 10:
             continue
         try:
-            sm.append(float(f[1]))
-            mx = float(f[2])
+            sm.append(float(f[2]))
+            mx = float(f[3])
         except ValueError:
             continue
-        for nm, v in zip(names, f[5:9]):
+        for nm, v in zip(names, f[6:10]):
             if v.lower() == "active":
                 reasons.add(nm)
     return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
@@ -399,7 +451,7 @@ def mlp_bench(P, args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
@@ -505,13 +557,10 @@ def main():
     hops = torch.zeros(1, dtype=torch.int64, device=dev)
     keys, key = P.engine.key_schedule(key, args.steps)
 
-    stop = threading.Event()
-    clock_lines = []
-    th = threading.Thread(target=sample_clocks, args=(stop, clock_lines), daemon=True)
+    sampler = ClockSampler(gpu_uuid(torch, dev)).start()
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-    th.start()
     step_ms = []
     evolve_ms = []
     total_hops = 0
@@ -526,10 +575,9 @@ def main():
         step_ms.append(a.elapsed_time(b))
         total_hops += int(hops.item())
     torch.cuda.synchronize()
+    clock_lines = sampler.stop()
     if world > 1:
         torch.distributed.barrier()
-    stop.set()
-    th.join(timeout=5)
     t_step = float(np.sum(step_ms)) / 1e3
     if world > 1:
         t = torch.tensor([t_step], device=dev)
@@ -565,7 +613,10 @@ def main():
     pk, pk_kind = peaks()
     clocks = summarize_clocks(clock_lines)
     C = eng.cfg_bytes
-    alg_bytes = 4 + 2 * C + 16 + (2 * C + 36)   # evolve (gather fused) + reconfiguration
+    # evolve (gather fused) + reconfiguration, and the carried guide fields
+    # (N values per walker, read through the parent map and written back)
+    fbytes = 2 * (L * L) * (8 if args.precision == "fp64" else 4)
+    alg_bytes = 4 + 2 * C + 16 + (2 * C + 36) + fbytes
     achieved_gbs = alg_bytes * n / (ms_per_step / 1e3) / 1e9
     line = {
         "metric": "walker-steps/s", "value": value, "unit": "walker-steps/s", "n_gpus": world,
@@ -581,11 +632,14 @@ def main():
                 "d2h_bytes_per_step": n * C + 4 * n + 16},
         "gpu_launches": 5 * args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": pk["hbm_gbs"],
-                     "unit": "GB/s", "frac": achieved_gbs / pk["hbm_gbs"], "traffic": None,
+                     "unit": "GB/s", "frac": achieved_gbs / pk["hbm_gbs"],
+                     "traffic": EVOLVE_TRAFFIC_BYTES.get((args.precision, n)),
+                     "algorithmic_bytes_per_launch": alg_bytes * n,
                      "peak_source": pk_kind,
                      "note": f"algorithmic bytes per walker-step {alg_bytes} (packed configs "
-                             "in/out, parent index, weights, resampling); the step is "
-                             "compute-bound (float64 exp + guide-ratio arithmetic), see profiles/"},
+                             "in/out, parent index, weights, resampling, carried guide fields "
+                             "in/out); the step is compute-bound (guide-ratio arithmetic over "
+                             "512 bonds per rate evaluation), see profiles/"},
         "clocks": clocks,
     }
     if rank == 0 and not args.no_cpu_baseline:
