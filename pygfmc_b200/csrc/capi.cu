@@ -665,6 +665,12 @@ int run_steps_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, int 
                                           (float *)h->fbuf[h->fcur], h->status, s);
         if (eg != cudaSuccess) return fail(GFMC_ERR_CUDA, "theta GEMM: %s", cudaGetErrorString(eg));
         a.field_in = h->fbuf[h->fcur];
+      } else if (fresh && !h->rbm_on && !h->mlp_on && g.dense && g.Jd) {
+        // dense Jastrow couplings: the population's state as one product
+        // (same values as the step kernel's per-walker rebuild)
+        cudaError_t eg = launch_fields<T>(m, g, n, cur, (T *)h->fbuf[h->fcur], s);
+        if (eg != cudaSuccess) return fail(GFMC_ERR_CUDA, "guide fields: %s", cudaGetErrorString(eg));
+        a.field_in = h->fbuf[h->fcur];
       }
       a.field_out = h->fbuf[1 - h->fcur];
       h->fcur = 1 - h->fcur;

@@ -125,6 +125,13 @@ cudaError_t plan_evolve(const DevModel<T> &m, const DevGuide<T> &g, int n_slots_
 // Number of per-warp partial maxima an evolve launch over n_walkers writes.
 int evolve_partials(const LaunchPlan &plan, int n_walkers);
 
+// Guide state of n configurations at once for a dense coupling matrix
+// (fields.cu): spin-1/2 the signed ratio factors, Bose-Hubbard the fields,
+// (n, N) values of T, bit-identical to the step kernel's own rebuild.
+template <typename T>
+cudaError_t launch_fields(const DevModel<T> &m, const DevGuide<T> &g, int n, const void *cfg, T *out,
+                          cudaStream_t s);
+
 // Sharded reconfiguration pieces (recon_dist.cu), float64.  out: (max, S,
 // sum w e, last positive index).
 int dist_tiles(int n);

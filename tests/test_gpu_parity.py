@@ -109,6 +109,12 @@ def _systems(P, O):
     GBt = P.JastrowBoseHubbard(12, eb, beta=0.1, d=0.2)
     gbt = O.jastrow_bose_hubbard(12, eb, 0.1, mb, d=0.2)
     out.append(("bose12_jastrow_tied", B, GBt, mb, gbt, occ))
+    # all-pairs density Jastrow: the dense path (population fields as one product)
+    pb = np.array([(i, j) for i in range(12) for j in range(i + 1, 12)])
+    bpd = rng.uniform(0.01, 0.1, len(pb))
+    GBd = P.JastrowBoseHubbard(12, pb, beta=bpd, d=0.2)
+    gbd = O.jastrow_bose_hubbard(12, pb, bpd, mb, d=0.2)
+    out.append(("bose12_jastrow_dense", B, GBd, mb, gbd, occ))
     return out
 
 
@@ -179,6 +185,29 @@ def test_mixed_precision_agrees_with_fp64(P):
     assert abs(a - b) < 4 * np.hypot(ea, eb) + 1e-6, res
     # exact ground state of the periodic 16-site Heisenberg chain
     assert abs(a / 16 - (-0.4463935)) < 5e-3
+
+
+def test_mixed_precision_dense_guide_agrees_with_fp64(P):
+    """The long-range (all-pairs) Jastrow on the 4x4 torus, whose fresh guide
+    state is built for the whole population as one product: the float32 and
+    float64 builds agree with each other and with the exact ground state."""
+    sq = P.square(4)
+    H = P.SpinHalf.create(sq.edges, J_x=-1.0, J_y=-1.0, J_z=1.0, dtype=np.float64)
+    pairs = np.array([(i, j) for i in range(16) for j in range(i + 1, 16)])
+    pos = sq.extras["positions"]
+    d = np.abs(pos[pairs[:, 0]] - pos[pairs[:, 1]])
+    d = np.minimum(d, 4 - d)
+    G = P.JastrowSpinHalf(16, pairs, beta=0.3 / np.sqrt((d ** 2).sum(1)))
+    w = P.prepare_walkers_sz(2048, 16, P.PRNGKey(0), sz=0)
+    res = {}
+    for prec in ("fp64", "mixed"):
+        _, E, _, st, raw = P.run(w, 1500, H, 0.1, G, [8, 32], rng_key=P.PRNGKey(1), warmup_steps=200,
+                                 verbosity=0, precision=prec)
+        Ej, err = P.estimators.jackknife_energy([32], raw["log_weights"], raw["energy"], 20)
+        res[prec] = (Ej[32], err[32])
+    (a, ea), (b, eb) = res["fp64"], res["mixed"]
+    assert abs(a - b) < 4 * np.hypot(ea, eb) + 1e-6, res
+    assert abs(a - (-11.228483)) < max(4 * ea, 2e-3 * 11.228483), res
 
 
 def test_hop_cap_is_reported_not_hung(P):
