@@ -991,6 +991,17 @@ int local_energy_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, i
   a.partial_max = nullptr;
   a.status = h->status;
   a.max_iters = 1;
+  if (h->carry && !h->rbm_on && !h->mlp_on && g.dense && g.Jd) {
+    // dense couplings: the carried state when it belongs to cfg, else the
+    // population's state as one product into the spare carried buffer
+    if (h->field_valid && h->field_cfg == cfg) {
+      a.field_in = h->fbuf[h->fcur];
+    } else {
+      cudaError_t eg = launch_fields<T>(m, g, n, cfg, (T *)h->fbuf[1 - h->fcur], s);
+      if (eg != cudaSuccess) return fail(GFMC_ERR_CUDA, "guide fields: %s", cudaGetErrorString(eg));
+      a.field_in = h->fbuf[1 - h->fcur];
+    }
+  }
   cudaError_t e = launch_step<T>(h, m, g, a, s);
   if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "local energy launch: %s", cudaGetErrorString(e));
   return GFMC_OK;
@@ -1518,11 +1529,20 @@ int gfmc_evolve(gfmc_handle *h, int method, double step, double lam, double alw,
   a.status = h->status;
   a.max_iters = h->max_iters;
   h->field_valid = 0;   // carried state is not kept across a sharded step
-  cudaError_t e;
-  if (h->precision == GFMC_PRECISION_FP64)
-    e = launch_step<double>(h, h->m64, h->g64, a, s);
-  else
-    e = launch_step<float>(h, h->m32, h->g32, a, s);
+  cudaError_t e = cudaSuccess;
+  const bool dense_state = h->carry && !h->rbm_on && !h->mlp_on &&
+                           (h->precision == GFMC_PRECISION_FP64 ? h->g64.dense && h->g64.Jd
+                                                                : h->g32.dense && h->g32.Jd);
+  if (dense_state) {
+    // the guide state of cfg's rows as one product (read through the parents)
+    e = h->precision == GFMC_PRECISION_FP64
+            ? launch_fields<double>(h->m64, h->g64, n, cfg, (double *)h->fbuf[h->fcur], s)
+            : launch_fields<float>(h->m32, h->g32, n, cfg, (float *)h->fbuf[h->fcur], s);
+    a.field_in = h->fbuf[h->fcur];
+  }
+  if (e == cudaSuccess)
+    e = h->precision == GFMC_PRECISION_FP64 ? launch_step<double>(h, h->m64, h->g64, a, s)
+                                            : launch_step<float>(h, h->m32, h->g32, a, s);
   if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "evolve launch: %s", cudaGetErrorString(e));
   return GFMC_OK;
 }

@@ -100,8 +100,8 @@ def test_gloo_sharded_resampling_equals_the_concatenated_one(oracle, world, n, s
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("R", [1, 3])
-def test_sharded_steps_follow_the_unsharded_run(R):
+@pytest.mark.parametrize("R,guide", [(1, "nn"), (3, "nn"), (3, "dense")])
+def test_sharded_steps_follow_the_unsharded_run(R, guide):
     """R emulated ranks on one GPU (evolve with global walker offsets, the
     device resampling pieces, the exchange plan applied by copies) against
     one engine over the whole population: identical configurations after
@@ -114,7 +114,13 @@ def test_sharded_steps_follow_the_unsharded_run(R):
     from pygfmc_b200.distributed import evolve_shard
     e = P.chain(24).edges
     H = P.SpinHalf.create(e, J_x=-1.0, J_y=-1.0, J_z=1.0, h_x=0.2, dtype=np.float64)
-    G = P.JastrowSpinHalf(24, e, beta=0.3)
+    if guide == "dense":
+        # all pairs: the shards' guide state is built as one product per call
+        pairs = np.array([(i, j) for i in range(24) for j in range(i + 1, 24)])
+        r = np.minimum(pairs[:, 1] - pairs[:, 0], 24 - (pairs[:, 1] - pairs[:, 0]))
+        G = P.JastrowSpinHalf(24, pairs, beta=0.3 / r)
+    else:
+        G = P.JastrowSpinHalf(24, e, beta=0.3)
     n = 200
     N = n * R
     cfg = P.prepare_walkers_random(N, 24, P.PRNGKey(3)).config
