@@ -25,6 +25,7 @@
 #include <cfloat>
 
 #include "engine.cuh"
+#include "bose_moves.cuh"
 
 namespace gfmc {
 namespace {
@@ -135,64 +136,14 @@ __device__ __forceinline__ T site_val(const uint64_t *bits, const uint8_t *occ, 
   return T(occ[k]);
 }
 
-// ---- Bose-Hubbard transition layout (bose_hubbard.py module docstring;
-//      _common.two_site_move:34-72) -------------------------------------------
-struct BoseMove {
-  int a, b, da, db, blk, idx;  // blk: 0 hop fwd, 1 hop bwd, 2 pair up, 3 pair dn, 4 b+, 5 b
-};
-
-template <typename T>
-__device__ __forceinline__ BoseMove bose_decode(const DevModel<T> &m, int o) {
-  BoseMove mv;
-  int E = m.E;
-  if (m.n_hop) {
-    if (o < 2 * E) {
-      int e = o < E ? o : o - E;
-      uint32_t pe = m.edge[e];
-      mv.a = pe & 0xFFFF; mv.b = pe >> 16; mv.idx = e;
-      if (o < E) { mv.da = -1; mv.db = +1; mv.blk = 0; }
-      else { mv.da = +1; mv.db = -1; mv.blk = 1; }
-      return mv;
-    }
-    o -= 2 * E;
-  }
-  if (m.n_eta) {
-    if (o < 2 * E) {
-      int e = o < E ? o : o - E;
-      uint32_t pe = m.edge[e];
-      mv.a = pe & 0xFFFF; mv.b = pe >> 16; mv.idx = e;
-      if (o < E) { mv.da = +1; mv.db = +1; mv.blk = 2; }
-      else { mv.da = -1; mv.db = -1; mv.blk = 3; }
-      return mv;
-    }
-    o -= 2 * E;
-  }
-  int k = o < m.N ? o : o - m.N;
-  mv.a = mv.b = k; mv.idx = k; mv.db = 0;
-  if (o < m.N) { mv.da = +1; mv.blk = 4; } else { mv.da = -1; mv.blk = 5; }
-  return mv;
-}
-
 // Off-diagonal element of Bose-Hubbard move o (<= 0), guide ratio folded in:
 // BoseHubbard.get_rates:285-393, JastrowBoseHubbard.log_diff_from_operator:253-286.
 template <typename T>
 __device__ __forceinline__ T bose_offdiag(const DevModel<T> &m, const DevGuide<T> &g,
                                           const uint8_t *occ, const T *F, int o) {
   BoseMove mv = bose_decode(m, o);
-  T na = T(occ[mv.a]), nb = T(occ[mv.b]);
-  T nmax = T(m.n_max);
-  T v;
-  switch (mv.blk) {
-    case 0: v = -m.t[mv.idx] * math_sqrt(na * (nb + T(1))) * (nb < nmax ? T(1) : T(0)); break;
-    case 1: v = -m.t[mv.idx] * math_sqrt((na + T(1)) * nb) * (na < nmax ? T(1) : T(0)); break;
-    case 2:
-      v = -m.eta[mv.idx] * math_sqrt((na + T(1)) * (nb + T(1))) *
-          ((na < nmax && nb < nmax) ? T(1) : T(0));
-      break;
-    case 3: v = -m.eta[mv.idx] * math_sqrt(na * nb); break;
-    case 4: v = m.hpm[mv.idx] * math_sqrt(na + T(1)) * (na < nmax ? T(1) : T(0)); break;
-    default: v = m.hpm[mv.idx] * math_sqrt(na); break;
-  }
+  const T na = T(occ[mv.a]), nb = T(occ[mv.b]);
+  T v = bose_element<T>(m, occ, mv);
   if (g.kind && v != T(0)) {
     T da = T(mv.da), db = T(mv.db);
     T out = T(0);

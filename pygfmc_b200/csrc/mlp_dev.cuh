@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <cuda_bf16.h>
 
+#include "bose_moves.cuh"
 #include "engine.cuh"
 
 namespace gfmc {
@@ -30,50 +31,18 @@ __device__ __forceinline__ float rcp_approx(float x) {
 // 1 / (1 + e^{2y}) from Ky = K y: tanh y = 1 - 2 of it.
 __device__ __forceinline__ float sig2(float Ky) { return rcp_approx(1.0f + ex2_approx(Ky)); }
 
-// Moves of the Bose-Hubbard layout (bose_hubbard.py; _common.two_site_move):
-// sites a, b, occupation changes da, db (b == a, db = 0 for the single-site
-// h_pm moves) and the unguided off-diagonal element.
+// A move of the Bose-Hubbard layout (bose_decode) with its unguided element
+// (bose_element); b == a, db = 0 for the single-site h_pm moves.
 struct Mv {
   int a, b, da, db;
   float v;
 };
 
 __device__ __forceinline__ Mv mlp_move(const DevModel<float> &m, const uint8_t *occ, int o) {
+  const BoseMove bm = bose_decode(m, o);
   Mv mv;
-  const int E = m.E;
-  const float nmax = (float)m.n_max;
-  int blk;
-  int idx;
-  if (m.n_hop && o < 2 * E) {
-    const int e = o < E ? o : o - E;
-    const uint32_t pe = m.edge[e];
-    mv.a = pe & 0xFFFF; mv.b = pe >> 16; idx = e;
-    if (o < E) { mv.da = -1; mv.db = 1; blk = 0; } else { mv.da = 1; mv.db = -1; blk = 1; }
-  } else {
-    if (m.n_hop) o -= 2 * E;
-    if (m.n_eta && o < 2 * E) {
-      const int e = o < E ? o : o - E;
-      const uint32_t pe = m.edge[e];
-      mv.a = pe & 0xFFFF; mv.b = pe >> 16; idx = e;
-      if (o < E) { mv.da = 1; mv.db = 1; blk = 2; } else { mv.da = -1; mv.db = -1; blk = 3; }
-    } else {
-      if (m.n_eta) o -= 2 * E;
-      const int k = o < m.N ? o : o - m.N;
-      mv.a = mv.b = k; idx = k; mv.db = 0;
-      if (o < m.N) { mv.da = 1; blk = 4; } else { mv.da = -1; blk = 5; }
-    }
-  }
-  const float na = (float)occ[mv.a], nb = (float)occ[mv.b];
-  switch (blk) {
-    case 0: mv.v = -m.t[idx] * sqrtf(na * (nb + 1.0f)) * (nb < nmax ? 1.0f : 0.0f); break;
-    case 1: mv.v = -m.t[idx] * sqrtf((na + 1.0f) * nb) * (na < nmax ? 1.0f : 0.0f); break;
-    case 2:
-      mv.v = -m.eta[idx] * sqrtf((na + 1.0f) * (nb + 1.0f)) * ((na < nmax && nb < nmax) ? 1.0f : 0.0f);
-      break;
-    case 3: mv.v = -m.eta[idx] * sqrtf(na * nb); break;
-    case 4: mv.v = m.hpm[idx] * sqrtf(na + 1.0f) * (na < nmax ? 1.0f : 0.0f); break;
-    default: mv.v = m.hpm[idx] * sqrtf(na); break;
-  }
+  mv.a = bm.a; mv.b = bm.b; mv.da = bm.da; mv.db = bm.db;
+  mv.v = bose_element<float>(m, occ, bm);
   // a move that leaves [0, n_max] has no element (and reads no W1 column),
   // whatever the couplings hold
   const int a1 = (int)occ[mv.a] + mv.da, b1 = (int)occ[mv.b] + mv.db;
