@@ -188,7 +188,8 @@ def study_system(P, args):
                                            steps_per_iteration=3, step_size=0.02, lr=args.train_lr,
                                            rng_key=P.PRNGKey(14), warmup_steps=100, verbosity=0)
         return {"name": "bose_hubbard_ring64", "H": H, "plain": GJ, "G0": G0, "N": 64,
-                "learned": "mlp_256x256_mixed", "n_learned": N_WALKERS, "tau": 0.02,
+                "learned": "mlp_256x256_mixed", "n_learned": N_WALKERS, "n_plain": N_WALKERS,
+                "tau": 0.02,
                 "p": [16, 64], "walk": walk, "train": train,
                 "plain_name": "gutzwiller_density_jastrow"}
     lat, H, G, hid, tau, n_rbm, name = rbm_system(P, args.lattice)
@@ -202,7 +203,8 @@ def study_system(P, args):
                                        steps_per_iteration=3, step_size=tau, lr=args.train_lr,
                                        rng_key=P.PRNGKey(14), warmup_steps=100, verbosity=0)
     return {"name": name, "H": H, "plain": G, "G0": P.RBMSpinHalf(N, hid, seed=0, sigma=0.01),
-            "N": N, "learned": f"rbm_h{hid}_mixed", "n_learned": n_rbm, "tau": tau,
+            "N": N, "learned": f"rbm_h{hid}_mixed", "n_learned": n_rbm,
+            "n_plain": N_WALKERS if args.lattice == "square16" else n_rbm, "tau": tau,
             "p": [8, 32, 128] if args.lattice == "square16" else [16, 64, 256], "walk": walk,
             "train": train,
             "plain_name": "longrange_jastrow" if args.lattice == "square16" else "nn_jastrow"}
@@ -236,8 +238,8 @@ def sigma_study(P, args):
                     "walker_steps_per_s": n * steps / t,
                     "local_energy_var_per_site": float(np.var(wf.e_loc) / N)}
 
-    measure("jastrow_fp64", S["plain"], N_WALKERS, args.study_steps, 2000, "fp64")
-    measure("jastrow_mixed", S["plain"], N_WALKERS, args.study_steps, 2000, "mixed")
+    measure("jastrow_fp64", S["plain"], S["n_plain"], args.study_steps, 2000, "fp64")
+    measure("jastrow_mixed", S["plain"], S["n_plain"], args.study_steps, 2000, "mixed")
     trained, hist = S["train"](S["walk"](S["n_learned"], P.PRNGKey(13)), S["G0"])
     rk = S["learned"]
     measure(rk, trained, S["n_learned"], args.rbm_steps, 500, "mixed")
