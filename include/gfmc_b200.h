@@ -247,7 +247,8 @@ int gfmc_rbm_get_params(gfmc_handle *h, float *W, float *b, float *a);
 
 /* ---- MLP guide trainer ---------------------------------------------------- */
 /* The same variance loss for the MLP guide (float32 handles; mlp_H2 a
- * multiple of 64; at most 800 one-hot inputs n_sites (n_max + 1)).  The
+ * multiple of 64; at most 800 one-hot inputs n_sites (n_max + 1); at
+ * least 9 moves per configuration).  The
  * parameters, and the gradient, are one float32 array of
  * gfmc_mlp_param_count(h) values: W1 (mlp_H1, n_sites (n_max + 1)), b1
  * (mlp_H1), W2 (mlp_H2, mlp_H1), b2 (mlp_H2), w3 (mlp_H2) (b3 cancels in

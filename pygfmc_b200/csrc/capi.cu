@@ -120,6 +120,7 @@ struct gfmc_handle {
                 *mtr_d2T = nullptr;
   float *mtr_d1 = nullptr, *mtr_grad = nullptr, *mtr_p = nullptr, *mtr_m1 = nullptr,
         *mtr_m2 = nullptr;
+  int4 *mtr_rowcols = nullptr;
   int mtr_step = 0;
   // RBM variance-minimisation scratch (sized for train_cap walkers) and the
   // float32 master parameters with their Adam moments
@@ -872,15 +873,19 @@ int mlp_gradient_t(gfmc_handle *h, int n, const void *cfg, const int32_t *parent
   const int n_off = h->M - 1, rpw = n_off + 1, D = h->N * t.np1, CB = h->cfg_bytes;
   if ((size_t)D * 64 * 4 > 200 * 1024)
     return fail(GFMC_ERR_UNSUPPORTED, "MLP training supports at most 800 one-hot inputs, got %d", D);
+  if (rpw < 10)
+    return fail(GFMC_ERR_UNSUPPORTED, "MLP training needs at least 9 moves per configuration");
   const long long R = (long long)n * rpw, Mpad = (R + 127) / 128 * 128;
-  const size_t per_row = (size_t)t.H1 * 2 * 3 + (size_t)t.H2 * 2 * 4 + (size_t)t.H1 * 4 + 4;
+  const size_t per_row = (size_t)t.H1 * 2 * 3 + (size_t)t.H2 * 2 * 4 + (size_t)t.H1 * 4 + 4 + 16;
   if ((double)Mpad * per_row > 64e9)
     return fail(GFMC_ERR_UNSUPPORTED, "MLP training scratch for %d walkers exceeds 64 GB", n);
   const long long np = mlp_param_count(t.H1, t.H2, D);
   if (n > h->mtr_cap || Mpad > h->mtr_rows) {
     cudaFree(h->mtr_cfg); cudaFree(h->mtr_rates); cudaFree(h->mtr_rsum); cudaFree(h->mtr_gw);
     cudaFree(h->mtr_e); cudaFree(h->mtr_coef); cudaFree(h->mtr_h1); cudaFree(h->mtr_h1T);
-    cudaFree(h->mtr_h1lo); cudaFree(h->mtr_d2); cudaFree(h->mtr_d2T); cudaFree(h->mtr_d1);
+    cudaFree(h->mtr_h1lo); cudaFree(h->mtr_rowcols); cudaFree(h->mtr_d2); cudaFree(h->mtr_d2T); cudaFree(h->mtr_d1);
+    cudaFree(h->mtr_rowcols);
+    h->mtr_rowcols = nullptr;
     h->mtr_cfg = nullptr; h->mtr_rates = h->mtr_rsum = h->mtr_gw = h->mtr_coef = h->mtr_d1 = nullptr;
     h->mtr_e = nullptr;
     h->mtr_h1 = h->mtr_h1lo = h->mtr_h1T = h->mtr_d2 = h->mtr_d2T = nullptr;
@@ -898,6 +903,7 @@ int mlp_gradient_t(gfmc_handle *h, int n, const void *cfg, const int32_t *parent
     GFMC_CUDA(cudaMalloc(&h->mtr_d2, 4 * (size_t)Mpad * t.H2));     // hi | lo
     GFMC_CUDA(cudaMalloc(&h->mtr_d2T, 4 * (size_t)Mpad * t.H2));
     GFMC_CUDA(cudaMalloc(&h->mtr_d1, 4 * (size_t)Mpad * t.H1));
+    GFMC_CUDA(cudaMalloc(&h->mtr_rowcols, sizeof(int4) * (size_t)Mpad));
     h->mtr_cap = n;
     h->mtr_rows = Mpad;
   }
@@ -930,7 +936,7 @@ int mlp_gradient_t(gfmc_handle *h, int n, const void *cfg, const int32_t *parent
   if (e == cudaSuccess) e = cudaMemsetAsync(h->mtr_grad, 0, sizeof(float) * (size_t)np, s);
   if (e == cudaSuccess)
     e = launch_mlp_rows(h->m32, t, h->mtr_cfg, CB, n, Mpad, h->mtr_rates, h->mtr_rsum, h->mtr_gw,
-                        h->mtr_coef, h->mtr_h1, h->mtr_h1lo, h->mtr_h1T, s);
+                        h->mtr_coef, h->mtr_rowcols, h->mtr_h1, h->mtr_h1lo, h->mtr_h1T, s);
   float *gW1 = h->mtr_grad, *gb1 = gW1 + (size_t)t.H1 * D, *gW2 = gb1 + t.H1,
         *gb2 = gW2 + (size_t)t.H2 * t.H1, *gw3 = gb2 + t.H2;
   if (e == cudaSuccess) {
@@ -965,7 +971,8 @@ int mlp_gradient_t(gfmc_handle *h, int n, const void *cfg, const int32_t *parent
     g.status = h->status;
     e = launch_mlp_gemm(g, s);
   }
-  if (e == cudaSuccess) e = launch_mlp_dw1(h->m32, t, h->mtr_cfg, CB, n, h->mtr_d1, gW1, s);
+  if (e == cudaSuccess)
+    e = launch_mlp_dw1(h->m32, t, h->mtr_cfg, CB, n, h->mtr_d1, h->mtr_rowcols, gW1, s);
   if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "MLP gradient: %s", cudaGetErrorString(e));
   return GFMC_OK;
 }

@@ -41,13 +41,14 @@ cudaError_t launch_mlp_evolve(const DevModel<float> &m, const MlpTables &t, cons
 // W1 (H1, D), b1 (H1), W2 (H2, H1), b2 (H2), w3 (H2), D = N (n_max + 1).
 long long mlp_param_count(int H1, int H2, int D);
 // Row coefficients (g_w r_ws for a move, -g_w R_w for the walker itself, 0
-// for rows without an element) and first-layer activations h1 (Mpad, H1),
-// their bf16 rounding residuals h1lo (Mpad, H1) and h1 transposed (H1, Mpad),
-// bf16.
+// for rows without an element), the W1 columns each move row exchanges
+// (rowcols: old a, new a, old b, new b; x < 0 for none), first-layer
+// activations h1 (Mpad, H1), their bf16 rounding residuals h1lo (Mpad, H1)
+// and h1 transposed (H1, Mpad), bf16.  At least 10 rows per walker.
 cudaError_t launch_mlp_rows(const DevModel<float> &m, const MlpTables &t, const void *cfg, int CB,
                             int n, long long Mpad, const float *rates, const float *rsum,
-                            const float *gw, float *coef, __nv_bfloat16 *h1, __nv_bfloat16 *h1lo,
-                            __nv_bfloat16 *h1T, cudaStream_t s);
+                            const float *gw, float *coef, int4 *rowcols, __nv_bfloat16 *h1,
+                            __nv_bfloat16 *h1lo, __nv_bfloat16 *h1T, cudaStream_t s);
 
 enum MlpEpilogue { MLP_EPI_FWD = 0, MLP_EPI_BWD = 1, MLP_EPI_ACC = 2 };
 
@@ -83,9 +84,10 @@ struct MlpGemmArgs {
   int *status;
 };
 cudaError_t launch_mlp_gemm(const MlpGemmArgs &g, cudaStream_t s);
-// dW1 (H1, D) += sum over rows of d1 x^T (x one-hot), d1 (rows, H1) float32.
+// dW1 (H1, D) += sum over rows of d1 x^T (x one-hot), d1 (rows, H1) float32,
+// the move rows' columns from launch_mlp_rows.
 cudaError_t launch_mlp_dw1(const DevModel<float> &m, const MlpTables &t, const void *cfg, int CB,
-                           int n, const float *d1, float *gW1, cudaStream_t s);
+                           int n, const float *d1, const int4 *rowcols, float *gW1, cudaStream_t s);
 // Adam (beta 0.9 / 0.999, eps 1e-8, bias corrections of step `step`).
 cudaError_t launch_mlp_adam(long long np, float *p, const float *g, float *m1, float *m2, float lr,
                             int step, cudaStream_t s);

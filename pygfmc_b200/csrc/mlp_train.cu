@@ -79,21 +79,30 @@ __device__ __forceinline__ float reduce_scatter32(float (&v)[32], int lane) {
 // ---- rows: coefficients and first-layer activations ------------------------
 // Row r = w (n_off + 1) + s: s < n_off the move s of walker w, s = n_off the
 // walker itself; rows past n (n_off + 1) up to Mpad are zero.  One block of
-// 256 threads per 64 rows; thread i < H1 owns hidden unit i.
+// 256 threads per 64 rows: threads 0..63 decode the rows (coefficient, the
+// W1 columns the move exchanges, also written to rowcols for the one-hot
+// layer); the z1 of each walker the block spans is built once in shared
+// memory (thread i < H1 owns hidden unit i); the rows then go four at a
+// time, their column loads issued together.
+constexpr int RWMAX = 8;         // walkers one 64-row block can span (rows per walker >= 9)
+
 __global__ void __launch_bounds__(256) mlp_rows_kernel(DevModel<float> m, MlpTables t,
                                                        const uint8_t *cfg, int CB, int n,
                                                        long long Mpad, const float *rates,
                                                        const float *rsum, const float *gw,
-                                                       float *coef, __nv_bfloat16 *h1,
-                                                       __nv_bfloat16 *h1lo, __nv_bfloat16 *h1T) {
+                                                       float *coef, int4 *rowcols,
+                                                       __nv_bfloat16 *h1, __nv_bfloat16 *h1lo,
+                                                       __nv_bfloat16 *h1T) {
   extern __shared__ unsigned char rsm[];
   __nv_bfloat16 *T = reinterpret_cast<__nv_bfloat16 *>(rsm);              // (H1, RB)
-  int4 *rcol = reinterpret_cast<int4 *>(rsm + (size_t)t.H1 * RB * 2);     // (RB,)
-  int *rw = reinterpret_cast<int *>(rcol + RB);                           // (RB,) walker or -1
+  float *zs = reinterpret_cast<float *>(rsm + (size_t)t.H1 * RB * 2);     // (RWMAX, H1)
+  int4 *rcol = reinterpret_cast<int4 *>(zs + (size_t)RWMAX * t.H1);       // (RB,)
+  int *rw = reinterpret_cast<int *>(rcol + RB);                           // (RB,) walker slot or -1
   const int H1 = t.H1, np1 = t.np1, rpw = m.n_off + 1;
   const long long r0 = (long long)blockIdx.x * RB;
   const long long R = (long long)n * rpw;
   const int tid = threadIdx.x;
+  const int wfirst = (int)(r0 / rpw);
   if (tid < RB) {
     const long long r = r0 + tid;
     int w = -1;
@@ -116,43 +125,57 @@ __global__ void __launch_bounds__(256) mlp_rows_kernel(DevModel<float> m, MlpTab
       }
     }
     coef[r] = co;
+    rowcols[r] = c;
     rcol[tid] = c;
-    rw[tid] = w;
+    rw[tid] = w >= 0 ? w - wfirst : -1;
+  }
+  // z1 of the walkers this block spans
+  long long rl = r0 + RB - 1;
+  if (rl > R - 1) rl = R - 1;
+  const int nwb = r0 < R ? (int)(rl / rpw) - wfirst + 1 : 0;
+  if (tid < H1) {
+    for (int wi = 0; wi < nwb; ++wi) {
+      const uint8_t *occ = cfg + (size_t)(wfirst + wi) * CB;
+      float z = t.b1[tid];
+#pragma unroll 8
+      for (int k = 0; k < m.N; ++k) {
+        const int o = occ[k] <= m.n_max ? occ[k] : m.n_max;   // (packed occupations are checked)
+        z += __bfloat162float(t.W1T[(size_t)(k * np1 + o) * H1 + tid]);
+      }
+      zs[(size_t)wi * H1 + tid] = z;
+    }
   }
   __syncthreads();
   if (tid < H1) {
-    int cw = -1;
-    float z1 = 0.0f;
-    for (int rr = 0; rr < RB; ++rr) {
-      const int w = rw[rr];
-      __nv_bfloat16 hv = __float2bfloat16_rn(0.0f), lv = hv;
-      if (w >= 0) {
-        if (w != cw) {
-          const uint8_t *occ = cfg + (size_t)w * CB;
-          float z = t.b1[tid];
-          for (int k = 0; k < m.N; ++k) {
-            const int o = occ[k] <= m.n_max ? occ[k] : m.n_max;   // (packed occupations are checked)
-            z += __bfloat162float(t.W1T[(size_t)(k * np1 + o) * H1 + tid]);
-          }
-          z1 = z;
-          cw = w;
-        }
-        float z = z1;
-        const int4 c = rcol[rr];
-        if (c.x >= 0) {
-          z = (z + __bfloat162float(t.W1T[(size_t)c.y * H1 + tid])) -
-              __bfloat162float(t.W1T[(size_t)c.x * H1 + tid]);
-          if (c.z >= 0)
-            z = (z + __bfloat162float(t.W1T[(size_t)c.w * H1 + tid])) -
-                __bfloat162float(t.W1T[(size_t)c.z * H1 + tid]);
-        }
-        const float th = tanh_k(z);
-        hv = __float2bfloat16_rn(th);
-        lv = __float2bfloat16_rn(th - __bfloat162float(hv));
+    for (int rr0 = 0; rr0 < RB; rr0 += 4) {
+      float w1v[4][4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int4 c = rcol[rr0 + u];
+        const bool on = rw[rr0 + u] >= 0 && c.x >= 0;
+        w1v[u][0] = on ? __bfloat162float(t.W1T[(size_t)c.y * H1 + tid]) : 0.0f;
+        w1v[u][1] = on ? __bfloat162float(t.W1T[(size_t)c.x * H1 + tid]) : 0.0f;
+        const bool onb = on && c.z >= 0;
+        w1v[u][2] = onb ? __bfloat162float(t.W1T[(size_t)c.w * H1 + tid]) : 0.0f;
+        w1v[u][3] = onb ? __bfloat162float(t.W1T[(size_t)c.z * H1 + tid]) : 0.0f;
       }
-      h1[(size_t)(r0 + rr) * H1 + tid] = hv;
-      h1lo[(size_t)(r0 + rr) * H1 + tid] = lv;
-      T[(size_t)tid * RB + rr] = hv;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int rr = rr0 + u, wi = rw[rr];
+        __nv_bfloat16 hv = __float2bfloat16_rn(0.0f), lv = hv;
+        if (wi >= 0) {
+          float z = zs[(size_t)wi * H1 + tid];
+          // ((z + new a) - old a), then b: the step kernel's order
+          z = (z + w1v[u][0]) - w1v[u][1];
+          z = (z + w1v[u][2]) - w1v[u][3];
+          const float th = tanh_k(z);
+          hv = __float2bfloat16_rn(th);
+          lv = __float2bfloat16_rn(th - __bfloat162float(hv));
+        }
+        h1[(size_t)(r0 + rr) * H1 + tid] = hv;
+        h1lo[(size_t)(r0 + rr) * H1 + tid] = lv;
+        T[(size_t)tid * RB + rr] = hv;
+      }
     }
   }
   __syncthreads();
@@ -424,7 +447,7 @@ __global__ void __launch_bounds__(GT, 1) mlp_gemm_kernel(MlpGemmArgs g) {
 __global__ void __launch_bounds__(256) mlp_dw1_kernel(DevModel<float> m, MlpTables t,
                                                       const uint8_t *cfg, int CB, int n,
                                                       int walkers_per_block, const float *d1,
-                                                      float *gW1) {
+                                                      const int4 *rowcols, float *gW1) {
   extern __shared__ float dacc[];   // (D, 64)
   const int H1 = t.H1, np1 = t.np1, D = m.N * np1, rpw = m.n_off + 1;
   const int tid = threadIdx.x, grp = tid >> 6, tt = tid & 63;
@@ -441,9 +464,8 @@ __global__ void __launch_bounds__(256) mlp_dw1_kernel(DevModel<float> m, MlpTabl
       const float d = dr[(size_t)sl * H1];
       S += d;
       if (sl < m.n_off && d != 0.0f) {
-        const Mv mv = mlp_move(m, occ, sl);
-        if (mv.v == 0.0f) continue;      // no element: its columns may not exist
-        const int4 c = move_cols(mv, occ, np1);
+        const int4 c = rowcols[(size_t)w * rpw + sl];   // the rows kernel's decode
+        if (c.x < 0) continue;           // no element: its columns may not exist
         atomicAdd(dacc + (size_t)c.y * 64 + tt, d);
         atomicAdd(dacc + (size_t)c.x * 64 + tt, -d);
         if (c.z >= 0) {
@@ -548,13 +570,14 @@ long long mlp_param_count(int H1, int H2, int D) {
 
 cudaError_t launch_mlp_rows(const DevModel<float> &m, const MlpTables &t, const void *cfg, int CB,
                             int n, long long Mpad, const float *rates, const float *rsum,
-                            const float *gw, float *coef, __nv_bfloat16 *h1, __nv_bfloat16 *h1lo,
-                            __nv_bfloat16 *h1T, cudaStream_t s) {
-  const size_t smem = (size_t)t.H1 * RB * 2 + RB * 16 + RB * 4;
+                            const float *gw, float *coef, int4 *rowcols, __nv_bfloat16 *h1,
+                            __nv_bfloat16 *h1lo, __nv_bfloat16 *h1T, cudaStream_t s) {
+  if (m.n_off + 1 < (RB + RWMAX - 2) / (RWMAX - 1)) return cudaErrorInvalidValue;
+  const size_t smem = (size_t)t.H1 * RB * 2 + (size_t)RWMAX * t.H1 * 4 + RB * 16 + RB * 4;
   const long long blocks = Mpad / RB;
   mlp_rows_kernel<<<(unsigned)blocks, 256, smem, s>>>(m, t, reinterpret_cast<const uint8_t *>(cfg),
-                                                      CB, n, Mpad, rates, rsum, gw, coef, h1, h1lo,
-                                                      h1T);
+                                                      CB, n, Mpad, rates, rsum, gw, coef, rowcols,
+                                                      h1, h1lo, h1T);
   return cudaGetLastError();
 }
 
@@ -588,7 +611,7 @@ cudaError_t launch_mlp_gemm(const MlpGemmArgs &g, cudaStream_t s) {
 }
 
 cudaError_t launch_mlp_dw1(const DevModel<float> &m, const MlpTables &t, const void *cfg, int CB,
-                           int n, const float *d1, float *gW1, cudaStream_t s) {
+                           int n, const float *d1, const int4 *rowcols, float *gW1, cudaStream_t s) {
   const int D = m.N * t.np1;
   const size_t smem = (size_t)D * 64 * 4;
   if (smem > 200 * 1024) return cudaErrorInvalidConfiguration;
@@ -600,7 +623,7 @@ cudaError_t launch_mlp_dw1(const DevModel<float> &m, const MlpTables &t, const v
   if (wpb < 4) wpb = 4;
   const int blocks = (n + wpb - 1) / wpb;
   mlp_dw1_kernel<<<dim3(blocks, quarters), 256, smem, s>>>(
-      m, t, reinterpret_cast<const uint8_t *>(cfg), CB, n, wpb, d1, gW1);
+      m, t, reinterpret_cast<const uint8_t *>(cfg), CB, n, wpb, d1, rowcols, gW1);
   return cudaGetLastError();
 }
 
