@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(MT, 1) mlp_evolve_kernel(DevModel<float> m, Ml
   const int CB = ((m.N + 15) / 16) * 16;
   const int C = (m.n_off + 31) / 32;   // rate slots per lane of the sampling warp
   const bool sampler = tp < 32;
-  uint32_t use[NBUF] = {0u, 0u};       // commits per A buffer
+  uint32_t use[NBUF] = {};             // commits per A buffer
   uint32_t dphase = 0;
   bool ok = true;
   double wmax = -DBL_MAX;
