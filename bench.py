@@ -610,6 +610,10 @@ def main():
         out_h[1:2].copy_(Es, non_blocking=True)
         stream.synchronize()
     t_e2e = time.perf_counter() - t0
+    if world > 1:
+        te = torch.tensor([t_e2e], device=dev)
+        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
+        t_e2e = float(te.item())
     e2e_val = n * e2e_steps / t_e2e * world
 
     pk, pk_kind = peaks()
