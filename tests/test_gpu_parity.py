@@ -115,6 +115,18 @@ def _systems(P, O):
     GBd = P.JastrowBoseHubbard(12, pb, beta=bpd, d=0.2)
     gbd = O.jastrow_bose_hubbard(12, pb, bpd, mb, d=0.2)
     out.append(("bose12_jastrow_dense", B, GBd, mb, gbd, occ))
+    # translation-invariant long-range couplings on a 6 x 6 torus (36 sites:
+    # two lanes' strides per row, a displacement table wider than one warp)
+    s6 = P.square(6)
+    H6 = P.SpinHalf.create(s6.edges, J_x=-1.0, J_y=-1.0, J_z=1.0, dtype=np.float64)
+    m6 = O.spin_half(s6.edges, J_x=-1.0, J_y=-1.0, J_z=1.0)
+    p6 = np.array([(i, j) for i in range(36) for j in range(i + 1, 36)])
+    d6 = np.abs(s6.extras["positions"][p6[:, 0]] - s6.extras["positions"][p6[:, 1]])
+    d6 = np.minimum(d6, 6 - d6)
+    b6 = 0.25 / np.sqrt((d6 ** 2).sum(1))
+    G6 = P.JastrowSpinHalf(36, p6, beta=b6)
+    cfg6 = P.prepare_walkers_sz(512, 36, P.PRNGKey(15), sz=0).config
+    out.append(("square6_longrange", H6, G6, m6, O.jastrow_spin_half(36, p6, b6, None, m6), cfg6))
     return out
 
 
