@@ -377,7 +377,7 @@ int build_tables(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_des
     return fail(GFMC_ERR_UNSUPPORTED, "unknown guide kind %d", gk);
   g.kind = gk;
   size_t o_nbr = 0, o_nbrw = 0, o_cnt = 0, o_tpw = 0, o_jd = 0, o_ep = 0, o_em = 0, o_tep = 0,
-           o_tem = 0, o_xy = 0;
+           o_xy = 0;
   if (gk != GFMC_GUIDE_NONE) {
     // per-site partner lists, duplicates merged (each partner once per site)
     std::vector<std::map<int, double>> lists(N);
@@ -412,7 +412,9 @@ int build_tables(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_des
       o_jd = A.add(Jd.data(), Jd.size() * sizeof(T));
       if (gk == GFMC_GUIDE_JASTROW_SPIN_HALF) {
         // translation invariance on an Lx x Ly torus: J_ak = J_0[d(a, k)]
-        for (int Lx = 1; Lx <= N && !g.ti; ++Lx) {
+        // (its factor table, 8 N entries, is staged in shared memory: at most 48 KB)
+        const bool ti_fits = (size_t)8 * N * sizeof(T) <= 48 * 1024;
+        for (int Lx = 1; ti_fits && Lx <= N && !g.ti; ++Lx) {
           if (N % Lx) continue;
           const int Ly = N / Lx;
           bool ok = true;
@@ -430,16 +432,20 @@ int build_tables(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_des
           }
         }
         if (g.ti) {
-          std::vector<T> tp(N), tm(N);
-          std::vector<uint32_t> xy(N);
-          for (int d = 0; d < N; ++d) {
-            tp[d] = (T)std::exp(4.0 * (double)Jd[d]);
-            tm[d] = (T)std::exp(-4.0 * (double)Jd[d]);
-            xy[d] = (uint32_t)(d % g.Lx) | ((uint32_t)(d / g.Lx) << 16);
-          }
-          o_tep = A.add(tp.data(), N * sizeof(T));
-          o_tem = A.add(tm.data(), N * sizeof(T));
-          o_xy = A.add(xy.data(), N * 4);
+          const int Lx = g.Lx, Ly = g.Ly;
+          std::vector<T> te((size_t)8 * N);
+          std::vector<int> tq(N);
+          for (int uy = 0; uy < 2 * Ly; ++uy)
+            for (int ux = 0; ux < 2 * Lx; ++ux) {
+              const int d = (ux % Lx) + Lx * (uy % Ly);   // (ux - Lx) mod Lx, (uy - Ly) mod Ly
+              const size_t i = 2 * ((size_t)ux + 2 * (size_t)Lx * uy);
+              te[i] = (T)std::exp(4.0 * (double)Jd[d]);
+              te[i + 1] = (T)std::exp(-4.0 * (double)Jd[d]);
+            }
+          for (int k = 0; k < N; ++k) tq[k] = 2 * (k % Lx + 2 * Lx * (k / Lx));
+          g.tE_off = 2 * (Lx + 2 * Lx * Ly);
+          o_tep = A.add(te.data(), te.size() * sizeof(T));
+          o_xy = A.add(tq.data(), N * sizeof(int));
         }
         // multiplicative factor updates exp(+-4 J_kp) (1 where no pair)
         std::vector<T> ep((size_t)N * N, T(1)), em((size_t)N * N, T(1));
@@ -545,9 +551,8 @@ int build_tables(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_des
         g.Ep = (const T *)(base + o_ep);
         g.Em = (const T *)(base + o_em);
         if (g.ti) {
-          g.tEp = (const T *)(base + o_tep);
-          g.tEm = (const T *)(base + o_tem);
-          g.xy = (const uint32_t *)(base + o_xy);
+          g.tE = (const T *)(base + o_tep);
+          g.tq = (const int *)(base + o_xy);
         }
       } else {
         g.nbr_ep = (const T *)(base + o_ep);

@@ -74,13 +74,16 @@ template <typename T> struct DevGuide {
   const T *Ep, *Em;       // dense: (N, N)
   const T *nbr_ep, *nbr_em;   // sparse: (N, deg), aligned with nbr
   // Translation-invariant dense couplings on an Lx x Ly torus (site
-  // x + Lx y): J_ak = J_0[d(a, k)] with d the displacement index
-  // ((x_k - x_a) mod Lx) + Lx ((y_k - y_a) mod Ly); the factor rows are then
-  // the N-entry tables tEp = exp(4 J_0), tEm = exp(-4 J_0), staged in shared
-  // memory, and xy[k] = x_k | y_k << 16.
-  int ti, Lx, Ly;
-  const T *tEp, *tEm;
-  const uint32_t *xy;
+  // x + Lx y): J_ak = J_0[d(a, k)], d the displacement ((x_k - x_a) mod Lx) +
+  // Lx ((y_k - y_a) mod Ly).  The factor of site k after a flip of a is then
+  // tE[tq[k] - tq[a] + tE_off + (x_k != x_a)], tq[k] = 2 (x_k + 2 Lx y_k),
+  // tE_off = 2 (Lx + 2 Lx Ly): tE runs over the unwrapped displacements
+  // (dx + Lx) + 2 Lx (dy + Ly), two entries each, exp(4 J_0[d]) for parallel
+  // spins and exp(-4 J_0[d]) for anti-parallel ones (8 N entries, staged in
+  // shared memory with tq).
+  int ti, Lx, Ly, tE_off;
+  const T *tE;
+  const int *tq;
   int dense;              // couplings as a dense symmetric (N, N) matrix Jd
   const T *Jd;            // (N, N) row-major, zero diagonal (dense == 1)
 };

@@ -80,9 +80,8 @@ __host__ __device__ inline size_t stage_tables(DevModel<T> &m, DevGuide<T> &g, i
     }
   }
   if (g.kind == GUIDE_JASTROW_SPIN && g.ti) {
-    g.tEp = stage_arr(g.tEp, m.N, base, off, copy);
-    g.tEm = stage_arr(g.tEm, m.N, base, off, copy);
-    g.xy = stage_arr(g.xy, m.N, base, off, copy);
+    g.tE = stage_arr(g.tE, 8 * m.N, base, off, copy);
+    g.tq = stage_arr(g.tq, m.N, base, off, copy);
   }
   if (g.kind != GUIDE_NONE && stage_nbr && !g.dense) {
     g.nbr = stage_arr(g.nbr, m.N * g.deg, base, off, copy);
@@ -208,15 +207,6 @@ __device__ __forceinline__ void signed_init(const DevModel<T> &m, const DevGuide
   __syncwarp();
 }
 
-// Displacement index of site k (packed xy) from (xa, ya) on the torus.
-template <typename T>
-__device__ __forceinline__ int ti_disp(const DevGuide<T> &g, uint32_t pk, int xa, int ya) {
-  int dx = (int)(pk & 0xFFFF) - xa, dy = (int)(pk >> 16) - ya;
-  dx += dx < 0 ? g.Lx : 0;
-  dy += dy < 0 ? g.Ly : 0;
-  return dx + g.Lx * dy;
-}
-
 // Flip of spin a (the sequential update of one flip): its partners k get
 // A_k *= exp(4 x_k x_a J_ak) (x_a before the flip), then s_a -> -1 / s_a.
 template <typename T>
@@ -226,12 +216,10 @@ __device__ __forceinline__ void flip_one(const DevModel<T> &m, const DevGuide<T>
   if (g.kind != GUIDE_NONE) {
     const bool ua = sa > T(0);
     if (g.ti) {
-      const uint32_t pa = g.xy[a];
-      const int xa = pa & 0xFFFF, ya = pa >> 16;
+      const int ca = g.tE_off - g.tq[a];
       for (int k = lane; k < m.N; k += 32) {
         const T sk = S[k];
-        const int d = ti_disp(g, g.xy[k], xa, ya);
-        S[k] = sk * (((sk > T(0)) == ua) ? g.tEp[d] : g.tEm[d]);
+        S[k] = sk * g.tE[g.tq[k] + ca + ((sk > T(0)) != ua)];
       }
     } else if (g.dense) {
       const T *ep = g.Ep + (size_t)a * m.N, *em = g.Em + (size_t)a * m.N;
@@ -250,7 +238,7 @@ __device__ __forceinline__ void flip_one(const DevModel<T> &m, const DevGuide<T>
       }
     }
     __syncwarp();
-    if (lane == 0) S[a] = T(-1) / sa;
+    if (lane == 0) S[a] = -math_rcp(sa);
   } else {
     if (lane == 0) S[a] = -sa;
   }
@@ -271,24 +259,22 @@ __device__ __forceinline__ void flip_pair(const DevModel<T> &m, const DevGuide<T
   const T sa = S[a], sb = S[b];
   const bool ua = sa > T(0), ub = sb > T(0);
   if (g.ti) {
-    const uint32_t pa = g.xy[a], pb = g.xy[b];
-    const int xa = pa & 0xFFFF, ya = pa >> 16, xb = pb & 0xFFFF, yb = pb >> 16;
+    const int qa = g.tq[a], qb = g.tq[b];
+    const int ca = g.tE_off - qa, cb = g.tE_off - qb;
     for (int k = lane; k < m.N; k += 32) {
       const T sk = S[k];
       const bool uk = sk > T(0);
-      const uint32_t pk = g.xy[k];
-      const int da = ti_disp(g, pk, xa, ya), db = ti_disp(g, pk, xb, yb);
-      const T fa = (uk == ua) ? g.tEp[da] : g.tEm[da];
-      const T fb = (uk == ub) ? g.tEp[db] : g.tEm[db];
+      const int qk = g.tq[k];
+      const T fa = g.tE[qk + ca + (uk != ua)];
+      const T fb = g.tE[qk + cb + (uk != ub)];
       S[k] = sk * fa * fb;
     }
     __syncwarp();
     if (lane == 0) {
-      const int dba = ti_disp(g, pa, xb, yb), dab = ti_disp(g, pb, xa, ya);
-      const T fba = ((!ua) == ub) ? g.tEp[dba] : g.tEm[dba];
-      const T fab = (ub == ua) ? g.tEp[dab] : g.tEm[dab];
-      S[a] = (T(-1) / sa) * fba;
-      S[b] = T(-1) / (sb * fab);
+      const T fba = g.tE[qa + cb + ((!ua) != ub)];   // row b at a, x_a after its flip
+      const T fab = g.tE[qb + ca + (ub != ua)];      // row a at b, x_b before its flip
+      S[a] = -math_rcp(sa) * fba;
+      S[b] = -math_rcp(sb * fab);
     }
     __syncwarp();
     return;
@@ -306,8 +292,8 @@ __device__ __forceinline__ void flip_pair(const DevModel<T> &m, const DevGuide<T
   if (lane == 0) {
     const T fba = ((!ua) == ub) ? epb[a] : emb[a];   // row b at a, x_a after its flip
     const T fab = (ub == ua) ? epa[b] : ema[b];      // row a at b, x_b before its flip
-    S[a] = (T(-1) / sa) * fba;
-    S[b] = T(-1) / (sb * fab);
+    S[a] = -math_rcp(sa) * fba;
+    S[b] = -math_rcp(sb * fab);
   }
   __syncwarp();
 }
@@ -366,7 +352,9 @@ __device__ __forceinline__ T offdiag(const DevModel<T> &m, const DevGuide<T> &g,
     const T p = SF[pe & 0xFFFF] * SF[pe >> 16];
     const bool anti = p < T(0);
     *anti_out = anti;
-    if (FAST) return anti ? m.k_anti * (-p) : m.k_par * p;
+    // (k_anti (-p) and k_par p as one product: negation and the order of a
+    // product's factors do not change its rounding)
+    if (FAST) return (anti ? -m.k_anti : m.k_par) * p;
     const T b = m.uniform_pm ? (anti ? m.jpm0 : m.jpmpm0) : (anti ? m.jpm[e] : m.jpmpm[e]);
     if (g.kind != GUIDE_NONE && b != T(0)) {
       const T c = g.uniform_c ? (anti ? g.c_anti0 : g.c_par0) : (anti ? g.c_anti[e] : g.c_par[e]);
@@ -415,7 +403,7 @@ __device__ __forceinline__ Eval<T> evaluate(const DevModel<T> &m, const DevGuide
   jmax = jmax < 0 ? 0 : (jmax > C ? C : jmax);
   for (int j = 0; j < jmax; ++j) {
     const int o = lamform ? s0 + j - 1 : s0 + j;
-    if (o >= 0) {
+    if (!lamform || o >= 0) {
       int anti = -1;
       const T v = offdiag<T, FAM, FAST>(m, g, occ, SF, o, &anti);
       if (fused_diag && anti >= 0) {
@@ -526,10 +514,11 @@ __device__ __forceinline__ int sample_slot(const DevModel<T> &m, const DevGuide<
 
 // 256 threads and 4 blocks per SM: 64 registers, 32 resident warps per SM
 // (a warp's shared state is ~2 KB, so registers bound the occupancy).
-// OPK selects the instantiation: 0 the propagators and EVALUATE, 1 the
-// measurement-operator modes APPLY and MIN_RATE (kept apart so that their
-// code does not weigh on the step kernel's register allocation).
-template <typename T, int FAM, int FAST, int OPK>
+// KIND selects the instantiation: 0 cont_time and EVALUATE, 1 the discrete
+// propagators single_step and multi_step, 2 the measurement-operator modes
+// APPLY and MIN_RATE (kept apart so that the code of one does not weigh on
+// another's register allocation).
+template <typename T, int FAM, int FAST, int KIND>
 __global__ void __launch_bounds__(256, FAM == SPIN_HALF ? 4 : 2)
 evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta_bytes) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -590,9 +579,9 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta
     double lw = 0.0;
     T eloc = T(0);
     int hops = 0;
-    T draws = T(0);   // uniforms of 16 holds (cont/multi) or 32 sub-steps (single)
+    T draws = T(0);   // draws of 16 holds (cont/multi) or uniforms of 32 sub-steps (single)
 
-    if (!OPK && method == CONT_TIME) {
+    if (KIND == 0 && method == CONT_TIME) {
       const T beta = T(a.step);
       T t = T(0);
       uint32_t it = 0;
@@ -600,16 +589,22 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta
         const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.n_off, MODE_OFF, lane);
         const T R = ev.total;
         const T eL = ev.diag - R;
-        if ((it & 15u) == 0) draws = uniform<T>(fold(kw, 2u * it + (uint32_t)lane));
+        if ((it & 15u) == 0) {
+          // even lanes keep the move uniform, odd lanes turn the hold uniform
+          // psi into the exponential variate -log1p(-psi) for its hold
+          const T d = uniform<T>(fold(kw, 2u * it + (uint32_t)lane));
+          const T ex = -math_log1p(-d);
+          draws = (lane & 1) ? ex : d;
+        }
         const T U1 = __shfl_sync(FULL, draws, (int)(2u * (it & 15u)));
-        const T psi = __shfl_sync(FULL, draws, (int)(2u * (it & 15u) + 1u));
+        const T ex = __shfl_sync(FULL, draws, (int)(2u * (it & 15u) + 1u));
         int si = 0;
         if (R > T(0)) {
           const T u = U1 * R, cap = next_below(R);
           si = sample_slot<T, FAM, FAST>(m, g, occ, SF, ev, m.n_off, MODE_OFF, lam,
                                          u < cap ? u : cap, lane);
         }
-        const T tau_raw = (R > T(0)) ? -math_log1p(-psi) / R : pos_inf<T>();
+        const T tau_raw = (R > T(0)) ? ex / R : pos_inf<T>();
         const T rem = beta - t;
         const T tau = tau_raw < rem ? tau_raw : rem;
         lw = lw - (double)eL * (double)tau;
@@ -625,7 +620,7 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta
         }
       }
       lw -= a.alw * a.step;
-    } else if (!OPK && method == SINGLE_STEP) {
+    } else if (KIND == 1 && method == SINGLE_STEP) {
       const int n_bra = (int)a.step;
       for (int sidx = 0; sidx < n_bra; ++sidx) {
         const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.M, MODE_LAM, lane);
@@ -644,7 +639,7 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta
       const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.n_off, MODE_OFF, lane);
       eloc = ev.diag - ev.total;
       lw -= a.alw * (double)n_bra;
-    } else if (!OPK && method == MULTI_STEP) {
+    } else if (KIND == 1 && method == MULTI_STEP) {
       const int n_bra = (int)a.step;
       int used = 0;
       uint32_t it = 0;
@@ -652,9 +647,14 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta
         const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.n_off, MODE_OFF, lane);
         const T R = ev.total;
         const T bx = lam - ev.diag + R;
-        if ((it & 15u) == 0) draws = uniform<T>(fold(kw, 2u * it + (uint32_t)lane));
+        if ((it & 15u) == 0) {
+          // odd lanes hold log1p(-psi) of their hold uniform
+          const T d = uniform<T>(fold(kw, 2u * it + (uint32_t)lane));
+          const T lp = math_log1p(-d);
+          draws = (lane & 1) ? lp : d;
+        }
         const T U1 = __shfl_sync(FULL, draws, (int)(2u * (it & 15u)));
-        const T psi = __shfl_sync(FULL, draws, (int)(2u * (it & 15u) + 1u));
+        const T lpsi = __shfl_sync(FULL, draws, (int)(2u * (it & 15u) + 1u));
         int si = 0;
         if (R > T(0)) {
           const T u = U1 * R, cap = next_below(R);
@@ -665,7 +665,7 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta
         const T hp = R / bx;
         const bool can_hop = hp > T(0);
         const T log_pd = can_hop ? math_log1p(-hp) : T(-1);
-        const T hold = floor(math_log1p(-psi) / log_pd) + T(1);
+        const T hold = floor(lpsi / log_pd) + T(1);
         const T capk = T(remaining + 1);
         const T hm = hold < capk ? hold : capk;
         const int k_raw = can_hop ? (int)hm : remaining + 1;
@@ -684,7 +684,7 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta
       const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.n_off, MODE_OFF, lane);
       eloc = ev.diag - ev.total;
       lw -= a.alw * (double)n_bra;
-    } else if (OPK && method == APPLY) {
+    } else if (KIND == 2 && method == APPLY) {
       // apply_operator_one:849-888: draw the successor in proportion to the
       // operator's guided rates (slot 0 the diagonal, i.e. stay); the value
       // is their sum, 0 when it is not positive; a purely diagonal operator
@@ -706,7 +706,7 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta
           eloc = total;
         }
       }
-    } else if (OPK && method == MIN_RATE) {
+    } else if (KIND == 2 && method == MIN_RATE) {
       // check_off_diag_operator_positivity (engine/estimators.py:631-681):
       // the smallest guide-transformed rate over all M_total slots, NaN when
       // one is not finite (the full evaluation gives the diagonal element)
@@ -779,12 +779,19 @@ void staging_plan(const DevModel<T> &m, const DevGuide<T> &g, int *stage_nbr, si
 template <typename T>
 using KernelFn = void (*)(DevModel<T>, DevGuide<T>, EvolveArgs, int, int);
 
-template <typename T> KernelFn<T> pick_kernel(const DevModel<T> &m, bool opk) {
-  if (m.family == SPIN_HALF) {
-    if (opk) return m.fast ? evolve_kernel<T, SPIN_HALF, 1, 1> : evolve_kernel<T, SPIN_HALF, 0, 1>;
-    return m.fast ? evolve_kernel<T, SPIN_HALF, 1, 0> : evolve_kernel<T, SPIN_HALF, 0, 0>;
-  }
-  return opk ? evolve_kernel<T, BOSE_HUBBARD, 0, 1> : evolve_kernel<T, BOSE_HUBBARD, 0, 0>;
+// Instantiation of a method (the KIND parameter of evolve_kernel).
+inline int kind_of(int method) {
+  return (method == CONT_TIME || method == EVALUATE) ? 0 : (method <= MULTI_STEP ? 1 : 2);
+}
+
+template <typename T, int KIND> KernelFn<T> pick_kind(const DevModel<T> &m) {
+  if (m.family == SPIN_HALF)
+    return m.fast ? evolve_kernel<T, SPIN_HALF, 1, KIND> : evolve_kernel<T, SPIN_HALF, 0, KIND>;
+  return evolve_kernel<T, BOSE_HUBBARD, 0, KIND>;
+}
+
+template <typename T> KernelFn<T> pick_kernel(const DevModel<T> &m, int kind) {
+  return kind == 0 ? pick_kind<T, 0>(m) : (kind == 1 ? pick_kind<T, 1>(m) : pick_kind<T, 2>(m));
 }
 
 }  // namespace
@@ -801,12 +808,13 @@ cudaError_t plan_evolve(const DevModel<T> &m, const DevGuide<T> &g, int n_slots_
   size_t cta;
   staging_plan(m, g, &stage_nbr, &cta);
   const size_t warp_bytes = warp_layout(m, g).bytes;
-  KernelFn<T> kern = pick_kernel(m, false);
-  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
-  if (err != cudaSuccess) return err;
-  err = cudaFuncSetAttribute(pick_kernel(m, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             max_smem);
-  if (err != cudaSuccess) return err;
+  KernelFn<T> kern = pick_kernel(m, 0);
+  cudaError_t err = cudaSuccess;
+  for (int kind = 0; kind < 3; ++kind) {
+    err = cudaFuncSetAttribute(pick_kernel(m, kind), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               max_smem);
+    if (err != cudaSuccess) return err;
+  }
   // the warps-per-block choice with the most resident warps per SM
   int best_w = 0, best = -1;
   for (int wpb = 8; wpb >= 1; wpb >>= 1) {
@@ -835,8 +843,8 @@ cudaError_t launch_evolve(const DevModel<T> &m, const DevGuide<T> &g, const Laun
   int need = (a.n_walkers + plan.wpb - 1) / plan.wpb;
   if (grid > need) grid = need;
   if (grid < 1) grid = 1;
-  pick_kernel(m, a.method >= APPLY)<<<grid, plan.block, plan.smem, s>>>(m, g, a, stage_nbr,
-                                                                        (int)cta);
+  pick_kernel(m, kind_of(a.method))<<<grid, plan.block, plan.smem, s>>>(m, g, a, stage_nbr,
+                                                                         (int)cta);
   return cudaGetLastError();
 }
 

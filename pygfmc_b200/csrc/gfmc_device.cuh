@@ -114,6 +114,11 @@ template <typename T> __device__ __forceinline__ T math_log(T x);
 template <> __device__ __forceinline__ double math_log<double>(double x) { return log(x); }
 template <> __device__ __forceinline__ float math_log<float>(float x) { return __logf(x); }
 
+// Correctly rounded reciprocal: the value of 1 / x under IEEE division.
+template <typename T> __device__ __forceinline__ T math_rcp(T x);
+template <> __device__ __forceinline__ double math_rcp<double>(double x) { return __drcp_rn(x); }
+template <> __device__ __forceinline__ float math_rcp<float>(float x) { return __frcp_rn(x); }
+
 template <typename T> __device__ __forceinline__ T math_log1p(T x);
 template <> __device__ __forceinline__ double math_log1p<double>(double x) { return log1p(x); }
 template <> __device__ __forceinline__ float math_log1p<float>(float x) { return log1pf(x); }
