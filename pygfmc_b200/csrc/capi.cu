@@ -569,6 +569,9 @@ int build_tables(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_des
       const bool gd_on = gk == GFMC_GUIDE_JASTROW_SPIN_HALF;
       m.k_anti = m.jpm0 * (gd_on ? g.c_anti0 : T(1));
       m.k_par = m.jpmpm0 * (gd_on ? g.c_par0 : T(1));
+      // the min form of k_par = 0 measured faster in float32 and slower in
+      // float64 than the coefficient select
+      m.fast = (m.k_par == T(0) && sizeof(T) == 4) ? 1 : 2;
     }
   }
   cudaError_t e = plan_evolve<T>(m, g, m.M, &h->plan);

@@ -37,7 +37,7 @@ template <typename T> struct DevModel {
   // guide edge constants), no h_z.  Edge rate = k_anti |s_i s_j| for
   // anti-parallel spins, k_par |s_i s_j| for parallel ones, where
   // s_k = x_k A_k are the signed ratio factors (A = 1 without a guide).
-  int fast;
+  int fast;               // 0 general; 1 fast with k_par = 0 (float32 only); 2 other fast
   T k_anti, k_par;
   // BoseHubbard
   int n_max, n_hop, n_eta, n_hpm, has_U, has_mu;

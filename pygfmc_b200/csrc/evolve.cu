@@ -48,6 +48,14 @@ __host__ __device__ inline X *stage_arr(const X *src, int n, unsigned char *base
   return const_cast<X *>(src);
 }
 
+// A pointer into this block's dynamic shared memory rebuilt from the shared
+// array, so that the compiler addresses it as shared memory.
+template <typename X>
+__device__ __forceinline__ const X *as_shared(const X *p, const unsigned char *smem) {
+  const size_t o = __cvta_generic_to_shared(p) - __cvta_generic_to_shared(smem);
+  return reinterpret_cast<const X *>(smem + o);
+}
+
 // Stages the CTA-shared tables (in a fixed order) and rewrites the pointers
 // to their shared copies.  The host runs the same function with copy=false
 // to size the region.
@@ -353,8 +361,10 @@ __device__ __forceinline__ T offdiag(const DevModel<T> &m, const DevGuide<T> &g,
     const bool anti = p < T(0);
     *anti_out = anti;
     // (k_anti (-p) and k_par p as one product: negation and the order of a
-    // product's factors do not change its rounding)
-    if (FAST) return (anti ? -m.k_anti : m.k_par) * p;
+    // product's factors do not change its rounding; with k_par = 0 the
+    // parallel edges' +0 comes from min(p, 0) instead of a select)
+    if (FAST == 1) return (-m.k_anti) * math_min(p, T(0));
+    if (FAST == 2) return (anti ? -m.k_anti : m.k_par) * p;
     const T b = m.uniform_pm ? (anti ? m.jpm0 : m.jpmpm0) : (anti ? m.jpm[e] : m.jpmpm[e]);
     if (g.kind != GUIDE_NONE && b != T(0)) {
       const T c = g.uniform_c ? (anti ? g.c_anti0 : g.c_par0) : (anti ? g.c_anti[e] : g.c_par[e]);
@@ -401,6 +411,7 @@ __device__ __forceinline__ Eval<T> evaluate(const DevModel<T> &m, const DevGuide
   const int s0 = lane * C;
   int jmax = n_slots - s0;
   jmax = jmax < 0 ? 0 : (jmax > C ? C : jmax);
+#pragma unroll 4
   for (int j = 0; j < jmax; ++j) {
     const int o = lamform ? s0 + j - 1 : s0 + j;
     if (!lamform || o >= 0) {
@@ -523,6 +534,12 @@ __global__ void __launch_bounds__(256, FAM == SPIN_HALF ? 4 : 2)
 evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta_bytes) {
   extern __shared__ __align__(16) unsigned char smem[];
   stage_tables(m, g, stage_nbr, smem, true);
+  // the tables every staging copies, as pointers derived from the shared
+  // array itself (shared-memory loads, 32-bit addresses); absent tables stay
+  // unused
+  m.edge = as_shared(m.edge, smem);
+  g.tE = as_shared(g.tE, smem);
+  g.tq = as_shared(g.tq, smem);
   __syncthreads();
 
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -785,8 +802,13 @@ inline int kind_of(int method) {
 }
 
 template <typename T, int KIND> KernelFn<T> pick_kind(const DevModel<T> &m) {
-  if (m.family == SPIN_HALF)
-    return m.fast ? evolve_kernel<T, SPIN_HALF, 1, KIND> : evolve_kernel<T, SPIN_HALF, 0, KIND>;
+  if (m.family == SPIN_HALF) {
+    if constexpr (sizeof(T) == 4) {   // (float64 builds use fast = 2 only)
+      if (m.fast == 1) return evolve_kernel<T, SPIN_HALF, 1, KIND>;
+    }
+    if (m.fast == 2) return evolve_kernel<T, SPIN_HALF, 2, KIND>;
+    return evolve_kernel<T, SPIN_HALF, 0, KIND>;
+  }
   return evolve_kernel<T, BOSE_HUBBARD, 0, KIND>;
 }
 

@@ -114,6 +114,10 @@ template <typename T> __device__ __forceinline__ T math_log(T x);
 template <> __device__ __forceinline__ double math_log<double>(double x) { return log(x); }
 template <> __device__ __forceinline__ float math_log<float>(float x) { return __logf(x); }
 
+template <typename T> __device__ __forceinline__ T math_min(T x, T y);
+template <> __device__ __forceinline__ double math_min<double>(double x, double y) { return fmin(x, y); }
+template <> __device__ __forceinline__ float math_min<float>(float x, float y) { return fminf(x, y); }
+
 // Correctly rounded reciprocal: the value of 1 / x under IEEE division.
 template <typename T> __device__ __forceinline__ T math_rcp(T x);
 template <> __device__ __forceinline__ double math_rcp<double>(double x) { return __drcp_rn(x); }
