@@ -147,8 +147,10 @@ def peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
-def cpu_reference(P, cfg_sample, alw, steps, warmup, seed_key):
-    """The oracle (C, OpenMP) on a sample of walkers: walker-steps/s."""
+def cpu_reference(P, cfg_sample, alw, steps, warmup, seed_key, min_seconds=0.0, max_steps=1000):
+    """The oracle (C, OpenMP) on a sample of walkers: walker-steps/s, the
+    threads used, the timed seconds and the timed steps (at least `steps`,
+    more until `min_seconds` of timed work or `max_steps`)."""
     from oracle import oracle as O
     O.build()
     lat, H, G, pairs, beta = build_system(P, "fp64")
@@ -159,7 +161,8 @@ def cpu_reference(P, cfg_sample, alw, steps, warmup, seed_key):
     key = np.asarray(seed_key, np.uint32)
     threads = O.lib().om_threads()
     times = []
-    for s in range(warmup + steps):
+    s = 0
+    while s < warmup + steps or (sum(times) < min_seconds and len(times) < max_steps):
         key, r = O.split(key, 2)
         k1, k2 = O.fold_in(r, 0), O.fold_in(r, 1)
         t0 = time.perf_counter()
@@ -167,7 +170,8 @@ def cpu_reference(P, cfg_sample, alw, steps, warmup, seed_key):
         O.reconfigure(k2, cfg, lw, el)
         if s >= warmup:
             times.append(time.perf_counter() - t0)
-    return len(cfg) * steps / sum(times), threads, sum(times)
+        s += 1
+    return len(cfg) * len(times) / sum(times), threads, sum(times), len(times)
 
 
 def study_system(P, args):
@@ -512,7 +516,8 @@ def main():
         g = O.jastrow_spin_half(lat.N, pairs, beta, None, m)
         alw = O.initial_alw(m, g, "cont_time", None, w.config)
         steps = max(1, args.steps)
-        val, threads, secs = cpu_reference(P, w.config, alw, steps, min(args.warmup, 1), P.PRNGKey(7))
+        val, threads, secs, _ = cpu_reference(P, w.config, alw, steps, min(args.warmup, 1),
+                                              P.PRNGKey(7))
         line = {"metric": "walker-steps/s", "value": val, "unit": "walker-steps/s", "n_gpus": 0,
                 "steps": steps, "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * secs / steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -654,10 +659,10 @@ def main():
     if rank == 0 and not args.no_cpu_baseline:
         cfg_d, _ = eng.population()
         sample = cfg_d[: args.cpu_sample].cpu().numpy()
-        val, threads, secs = cpu_reference(P, sample, alw, 2, 0, P.PRNGKey(7))
+        val, threads, secs, nst = cpu_reference(P, sample, alw, 2, 0, P.PRNGKey(7), min_seconds=10.0)
         line["cpu_baseline"] = {"value": val, "unit": "walker-steps/s", "cores": threads,
                                 "kind": "port",
-                                "sample": f"{args.cpu_sample} equilibrated walkers x 2 steps "
+                                "sample": f"{args.cpu_sample} equilibrated walkers x {nst} steps "
                                           f"({secs:.1f} s), C+OpenMP restatement of the reference"}
     if world > 1:
         torch.distributed.barrier()
