@@ -376,6 +376,7 @@ int build_tables(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_des
       gk != GFMC_GUIDE_JASTROW_BOSE_HUBBARD)
     return fail(GFMC_ERR_UNSUPPORTED, "unknown guide kind %d", gk);
   g.kind = gk;
+  size_t o_jdig = 0;
   size_t o_nbr = 0, o_nbrw = 0, o_cnt = 0, o_tpw = 0, o_jd = 0, o_ep = 0, o_em = 0, o_tep = 0,
            o_xy = 0;
   if (gk != GFMC_GUIDE_NONE) {
@@ -410,6 +411,32 @@ int build_tables(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_des
       for (int k = 0; k < N; ++k)
         for (auto &kv : lists[k]) Jd[(size_t)k * N + kv.first] = (T)kv.second;
       o_jd = A.add(Jd.data(), Jd.size() * sizeof(T));
+      // the population product's int8 digits of Jd (occupations must fit an int8)
+      if (md->kind == GFMC_MODEL_SPIN_HALF || md->n_max <= 127) {
+        const int D = fields_digits<T>(), NT = 256 / D;
+        const int Kp = ((N + 127) / 128) * 128, ny = (N + NT - 1) / NT;
+        double amax = 0.0;
+        for (const T v : Jd) amax = std::max(amax, std::fabs((double)v));
+        int ex = 0;
+        if (amax > 0.0) std::frexp(amax, &ex);            // amax < 2^ex
+        const double S = std::ldexp(1.0, ex + 1);         // |Jd| / S < 1/2
+        std::vector<int8_t> dig((size_t)ny * 256 * Kp, 0);
+        for (int k = 0; k < N; ++k) {
+          const size_t row = (size_t)(k / NT) * 256 + (size_t)(k % NT);
+          for (int p = 0; p < N; ++p) {
+            double v = (double)Jd[(size_t)p * N + k] / S;   // exact: S is a power of two
+            for (int d = 0; d < D; ++d) {
+              const double t = v * 128.0, jd = std::nearbyint(t);   // |t| <= 64
+              v = t - jd;                                           // exact, |v| <= 1/2
+              dig[(row + (size_t)d * NT) * Kp + p] = (int8_t)jd;
+            }
+          }
+        }
+        o_jdig = A.add(dig.data(), dig.size());
+        g.jdig_scale = S / 128.0;
+        g.jdig_kp = Kp;
+        g.jdig_d = D;
+      }
       if (gk == GFMC_GUIDE_JASTROW_SPIN_HALF) {
         // translation invariance on an Lx x Ly torus: J_ak = J_0[d(a, k)]
         // (its factor table, 8 N entries, is staged in shared memory: at most 48 KB)
@@ -546,6 +573,7 @@ int build_tables(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_des
       g.trans_pw = (const T *)(base + o_tpw);
     }
     if (g.dense) g.Jd = (const T *)(base + o_jd);
+    if (g.dense && g.jdig_d) g.jdig = (const int8_t *)(base + o_jdig);
     if (gk == GFMC_GUIDE_JASTROW_SPIN_HALF) {
       if (g.dense) {
         g.Ep = (const T *)(base + o_ep);
@@ -674,10 +702,9 @@ int run_steps_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, int 
                                           (float *)h->fbuf[h->fcur], h->status, s);
         if (eg != cudaSuccess) return fail(GFMC_ERR_CUDA, "theta GEMM: %s", cudaGetErrorString(eg));
         a.field_in = h->fbuf[h->fcur];
-      } else if (fresh && !h->rbm_on && !h->mlp_on && g.dense && g.Jd) {
+      } else if (fresh && !h->rbm_on && !h->mlp_on && g.dense && g.jdig) {
         // dense Jastrow couplings: the population's state as one product
-        // (same values as the step kernel's per-walker rebuild)
-        cudaError_t eg = launch_fields<T>(m, g, n, cur, (T *)h->fbuf[h->fcur], s);
+        cudaError_t eg = launch_fields<T>(m, g, n, cur, (T *)h->fbuf[h->fcur], h->status, s);
         if (eg != cudaSuccess) return fail(GFMC_ERR_CUDA, "guide fields: %s", cudaGetErrorString(eg));
         a.field_in = h->fbuf[h->fcur];
       }
@@ -1006,13 +1033,13 @@ int local_energy_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, i
   a.partial_max = nullptr;
   a.status = h->status;
   a.max_iters = 1;
-  if (h->carry && !h->rbm_on && !h->mlp_on && g.dense && g.Jd) {
+  if (h->carry && !h->rbm_on && !h->mlp_on && g.dense && g.jdig) {
     // dense couplings: the carried state when it belongs to cfg, else the
     // population's state as one product into the spare carried buffer
     if (h->field_valid && h->field_cfg == cfg) {
       a.field_in = h->fbuf[h->fcur];
     } else {
-      cudaError_t eg = launch_fields<T>(m, g, n, cfg, (T *)h->fbuf[1 - h->fcur], s);
+      cudaError_t eg = launch_fields<T>(m, g, n, cfg, (T *)h->fbuf[1 - h->fcur], h->status, s);
       if (eg != cudaSuccess) return fail(GFMC_ERR_CUDA, "guide fields: %s", cudaGetErrorString(eg));
       a.field_in = h->fbuf[1 - h->fcur];
     }
@@ -1546,13 +1573,13 @@ int gfmc_evolve(gfmc_handle *h, int method, double step, double lam, double alw,
   h->field_valid = 0;   // carried state is not kept across a sharded step
   cudaError_t e = cudaSuccess;
   const bool dense_state = h->carry && !h->rbm_on && !h->mlp_on &&
-                           (h->precision == GFMC_PRECISION_FP64 ? h->g64.dense && h->g64.Jd
-                                                                : h->g32.dense && h->g32.Jd);
+                           (h->precision == GFMC_PRECISION_FP64 ? h->g64.dense && h->g64.jdig
+                                                                : h->g32.dense && h->g32.jdig);
   if (dense_state) {
     // the guide state of cfg's rows as one product (read through the parents)
     e = h->precision == GFMC_PRECISION_FP64
-            ? launch_fields<double>(h->m64, h->g64, n, cfg, (double *)h->fbuf[h->fcur], s)
-            : launch_fields<float>(h->m32, h->g32, n, cfg, (float *)h->fbuf[h->fcur], s);
+            ? launch_fields<double>(h->m64, h->g64, n, cfg, (double *)h->fbuf[h->fcur], h->status, s)
+            : launch_fields<float>(h->m32, h->g32, n, cfg, (float *)h->fbuf[h->fcur], h->status, s);
     a.field_in = h->fbuf[h->fcur];
   }
   if (e == cudaSuccess)

@@ -86,7 +86,20 @@ template <typename T> struct DevGuide {
   const int *tq;
   int dense;              // couplings as a dense symmetric (N, N) matrix Jd
   const T *Jd;            // (N, N) row-major, zero diagonal (dense == 1)
+  // Jd as jdig_d balanced base-128 int8 digits for the population product
+  // (fields.cu): jdig[(t 256 + d (256 / jdig_d) + j) jdig_kp + p] is digit d of
+  // Jd[p, 256 t / jdig_d + j], Jd = 128 jdig_scale sum_d digit_d 128^-(d+1);
+  // jdig_kp = N rounded up to 128 (zero padding); nullptr when absent
+  const int8_t *jdig;
+  double jdig_scale;
+  int jdig_kp, jdig_d;
 };
+
+// Digits of the couplings in the population product: 8 (56 bits) for the
+// float64 build, 4 (28 bits) for the float32 build.
+template <typename T> __host__ __device__ constexpr int fields_digits() {
+  return sizeof(T) == 8 ? 8 : 4;
+}
 
 struct EvolveArgs {
   int method;
@@ -129,11 +142,12 @@ cudaError_t plan_evolve(const DevModel<T> &m, const DevGuide<T> &g, int n_slots_
 int evolve_partials(const LaunchPlan &plan, int n_walkers);
 
 // Guide state of n configurations at once for a dense coupling matrix
-// (fields.cu): spin-1/2 the signed ratio factors, Bose-Hubbard the fields,
-// (n, N) values of T, bit-identical to the step kernel's own rebuild.
+// (fields.cu, int8 tensor cores on the coupling digits): spin-1/2 the signed
+// ratio factors, Bose-Hubbard the fields, (n, N) values of T.  Needs g.jdig;
+// a bounded wait that runs out sets ST_TIMEOUT in *status.
 template <typename T>
 cudaError_t launch_fields(const DevModel<T> &m, const DevGuide<T> &g, int n, const void *cfg, T *out,
-                          cudaStream_t s);
+                          int *status, cudaStream_t s);
 
 // Sharded reconfiguration pieces (recon_dist.cu), float64.  out: (max, S,
 // sum w e, last positive index).

@@ -3,187 +3,244 @@
 // and, for spin-1/2, the signed ratio factors s_k = x_k exp(-2 x_k (F_k + h_k))
 // the step kernel carries (JastrowSpinHalf; jastrow_spin_half.py:290-353).
 //
-// The step kernel rebuilds this state per walker when it has none to carry
-// (a fresh population, every refresh); with a dense coupling matrix that is
-// N^2 multiply-adds per walker through L2.  Here the population's fields are
-// one (walkers x N) x (N x N) product.  A block takes 64 walkers and 128
-// output sites (blockIdx.y picks the sites): the walkers' configurations are
-// staged in shared memory once, J comes in chunks of 16 rows x 128 columns
-// through a two-stage cp.async ring (the next chunk lands while the current
-// one is used), and each thread accumulates 4 walkers x 8 sites in
-// registers, adding the sites p = 0 .. N-1 in order with one fused
-// multiply-add each -- the order and rounding of the step kernel's own
-// rebuild, so the carried state is bit-identical to it.  Rows are indexed
-// like the configurations (the step reads them through the parent map).
+// The step kernel would otherwise rebuild this state per walker (a fresh
+// population, every refresh): N^2 multiply-adds per walker through L2.  Here
+// it is one (walkers x N) x (N x N) product on the 5th-generation tensor
+// cores with exact integer arithmetic:
+//
+// * the couplings are split once, on the host, into D balanced base-128
+//   digits, Jd[p, k] = S sum_d j_d[k, p] 128^-(d+1) + r, j_d in [-64, 64],
+//   S a power of two with |Jd| <= S / 2, |r| <= S 2^-(7D+1) (D = 8 in the
+//   float64 build, 56 bits; D = 4 in the float32 build);
+// * x (+-1, or an occupation 0..n_max) is an int8, so every digit's product
+//   I_d[w, k] = sum_p x_p j_d[k, p] is exact in int32 (tcgen05.mma
+//   kind::i8, s8 x s8 -> s32);
+// * the epilogue combines the digits from the least significant one,
+//   acc = I_d + acc / 128 in float64 (each step exact until the bits run
+//   past 53; about 1.5 ulp in all), F = acc S / 128 -- closer to the exact
+//   sum than a sequential float64 accumulation of the N terms.
+//
+// A CTA (8 warps) takes 128 walkers (TMEM lanes) and 256 / D output sites;
+// the B operand holds all D digits of those sites (row d (256 / D) + j), so
+// one MMA of N = 256 covers every digit and the accumulator is 256 int32
+// columns.  K runs in chunks of 128 sites (one 128-byte swizzled row of
+// int8) through a two-stage ring: the CTA expands its walkers'
+// configurations into the int8 A tile (128 x 128) and copies the digit rows
+// into the B tile (256 x 128); thread 0 issues four MMAs of K = 32 per chunk
+// and commits to the stage's mbarrier.  Every wait is bounded: one that runs
+// out sets status bit ST_TIMEOUT, and the CTA still frees its TMEM.
+#include <cstdint>
+
 #include "engine.cuh"
+#include "tc05.cuh"
 
 namespace gfmc {
 namespace {
 
-constexpr int FW = 64;    // walkers per block
-constexpr int FS = 128;   // output sites per block
-constexpr int FK = 16;    // sites p per chunk of J
-constexpr int CFG_STAGE_MAX = 64 * 1024;   // staged configuration bytes per block at most
+using namespace tc;
 
-__device__ __forceinline__ uint32_t sh_addr(const void *p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+constexpr int MT = 128;     // walkers per CTA = UMMA M = TMEM lanes
+constexpr int KCH = 128;    // sites per K chunk (128 int8 = one swizzled row)
+constexpr int BN = 256;     // B rows = UMMA N = TMEM columns
+constexpr int FT = 256;     // threads per CTA
+constexpr int STAGE = MT * KCH + BN * KCH;   // A + B bytes per stage (48 KB)
+
+// D s32, A and B s8, both K-major, M = 128, N = 256.
+constexpr uint32_t IDESC_I8 =
+    (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ void mma_i8(uint32_t dtmem, uint64_t adesc, uint64_t bdesc,
+                                       uint32_t accum) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dtmem),
+      "l"(adesc), "l"(bdesc), "r"(IDESC_I8), "r"(accum));
 }
 
-// One element of J into shared memory (zero-filled when it lies outside J).
-template <int SZ>
-__device__ __forceinline__ void cp_el(void *dst, const void *src, bool valid) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(sh_addr(dst)), "l"(src),
-               "n"(SZ), "r"(valid ? SZ : 0)
-               : "memory");
-}
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int NPEND> __device__ __forceinline__ void cp_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(NPEND) : "memory");
+// Four TMEM columns of this warp's 32 lanes (no wait).
+__device__ __forceinline__ void tmem_ld4_async(uint32_t taddr, int32_t (&r)[4]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(taddr));
 }
 
-// +-1 from bit b of a spin word.
-template <typename T> __device__ __forceinline__ T spin_of(uint32_t word, int b) {
-  return ((word >> b) & 1u) ? T(1) : T(-1);
-}
-
-template <typename T, int FAM>
-__global__ void __launch_bounds__(256) fields_kernel(DevModel<T> m, DevGuide<T> g, int n,
-                                                     const void *cfg, T *out, int stage_cfg) {
-  extern __shared__ __align__(16) unsigned char fsm[];
-  T *Js = reinterpret_cast<T *>(fsm);                                    // [2][FK][FS]
-  unsigned char *cs = fsm + (size_t)2 * FK * FS * sizeof(T);             // [FW][cfgb]
-  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-  const int N = m.N, NW = (N + 63) / 64, CB = ((N + 15) / 16) * 16;
-  const int cfgb = FAM == SPIN_HALF ? NW * 8 : CB;
-  const int w0 = blockIdx.x * FW, s0 = blockIdx.y * FS;
-  const int nwb = n - w0 < FW ? n - w0 : FW;
-  const unsigned char *cg = reinterpret_cast<const unsigned char *>(cfg) + (size_t)w0 * cfgb;
-  if (stage_cfg) {
-    const uint64_t *src = reinterpret_cast<const uint64_t *>(cg);
-    uint64_t *dst = reinterpret_cast<uint64_t *>(cs);
-    for (int i = tid; i < nwb * cfgb / 8; i += 256) dst[i] = src[i];
+// 16 sites p0 .. p0+15 of walker row w as int8 x (0 past N or past the
+// population).
+template <int FAM>
+__device__ __forceinline__ uint4 x_chunk(const unsigned char *cfg, int cfgb, int N, int n, int w,
+                                         int p0) {
+  if (w >= n || p0 >= N) return make_uint4(0u, 0u, 0u, 0u);
+  uint32_t q[4];
+  if (FAM == SPIN_HALF) {
+    const uint64_t wd = reinterpret_cast<const uint64_t *>(cfg + (size_t)w * cfgb)[p0 >> 6];
+    const uint32_t bits = (uint32_t)(wd >> (p0 & 63)) & 0xFFFFu;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      uint32_t v = 0;
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const int i = 4 * e + b;
+        const uint32_t byte = (p0 + i < N) ? (((bits >> i) & 1u) ? 0x01u : 0xFFu) : 0u;
+        v |= byte << (8 * b);
+      }
+      q[e] = v;
+    }
+  } else {
+    const uint4 o = *reinterpret_cast<const uint4 *>(cfg + (size_t)w * cfgb + p0);
+    q[0] = o.x; q[1] = o.y; q[2] = o.z; q[3] = o.w;
+#pragma unroll
+    for (int e = 0; e < 4; ++e)
+#pragma unroll
+      for (int b = 0; b < 4; ++b)
+        if (p0 + 4 * e + b >= N) q[e] &= ~(0xFFu << (8 * b));
   }
-  const unsigned char *cw = stage_cfg ? cs : cg;   // the block's configurations
+  return make_uint4(q[0], q[1], q[2], q[3]);
+}
 
-  T acc[4][8];
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 8; ++b) acc[a][b] = T(0);
+template <typename T, int FAM, int D>
+__global__ void __launch_bounds__(FT, 1) fields_i8_kernel(DevModel<T> m, DevGuide<T> g, int n,
+                                                           const void *cfg_v, T *out, int *status) {
+  constexpr int NT = BN / D;   // output sites per CTA
+  extern __shared__ unsigned char dsm[];
+  unsigned char *base = (unsigned char *)(((uintptr_t)dsm + 1023) & ~(uintptr_t)1023);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(base + 2 * STAGE);   // [2]
+  uint32_t *slot = reinterpret_cast<uint32_t *>(bar + 2);
+  volatile int *flag = reinterpret_cast<volatile int *>(slot + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int N = m.N, Kp = g.jdig_kp, nk = Kp / KCH;
+  const int cfgb = FAM == SPIN_HALF ? ((N + 63) / 64) * 8 : ((N + 15) / 16) * 16;
+  const unsigned char *cfg = reinterpret_cast<const unsigned char *>(cfg_v);
+  const int w0 = blockIdx.x * MT, k0 = blockIdx.y * NT;
+  const int8_t *Bg = g.jdig + (size_t)blockIdx.y * BN * Kp;
 
-  const int nch = (N + FK - 1) / FK;
-  auto load_chunk = [&](int c) {
-    T *dst = Js + (c & 1) * FK * FS;
-    const int p0 = c * FK;
-    for (int i = tid; i < FK * FS; i += 256) {
-      const int p = p0 + i / FS, k = s0 + i % FS;
-      const bool ok = p < N && k < N;
-      cp_el<sizeof(T)>(dst + i, ok ? g.Jd + (size_t)p * N + k : g.Jd, ok);
+  if (warp == 0) tmem_alloc(slot, BN);
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = *slot;
+
+  bool ok = true;
+  int last = -1;   // last chunk whose MMAs were committed
+  for (int kc = 0; kc < nk && ok; ++kc) {
+    const int st = kc & 1;
+    unsigned char *A = base + st * STAGE;
+    unsigned char *B = A + MT * KCH;
+    if (kc >= 2) {
+      // the MMAs of chunk kc - 2 have read this stage
+      if (!cta_wait(&bar[st], (uint32_t)(((kc - 2) >> 1) & 1), flag)) {
+        if (tid == 0) atomicOr(status, ST_TIMEOUT);
+        ok = false;
+        break;
+      }
     }
-    cp_commit();
-  };
-  load_chunk(0);
-  for (int c = 0; c < nch; ++c) {
-    if (c + 1 < nch) {
-      load_chunk(c + 1);
-      cp_wait<1>();
-    } else {
-      cp_wait<0>();
+    // A: row r = walker w0 + r, four 16-site pieces per thread
+    {
+      const int r = tid & (MT - 1), c0 = (tid >> 7) * 4;
+#pragma unroll
+      for (int c = c0; c < c0 + 4; ++c)
+        *reinterpret_cast<uint4 *>(sw_chunk(A, r, c)) =
+            x_chunk<FAM>(cfg, cfgb, N, n, w0 + r, kc * KCH + 16 * c);
     }
+    // B: the 256 digit rows of this CTA's sites, chunk kc
+#pragma unroll
+    for (int q = 0; q < (BN * 8) / FT; ++q) {
+      const int i = tid + FT * q, r = i >> 3, c = i & 7;
+      const uint4 v = __ldg(reinterpret_cast<const uint4 *>(Bg + (size_t)r * Kp + kc * KCH + 16 * c));
+      *reinterpret_cast<uint4 *>(sw_chunk(B, r, c)) = v;
+    }
+    fence_async_smem();
     __syncthreads();
-    const T *J = Js + (c & 1) * FK * FS;
-    const int p0 = c * FK;
-    const int kmax = N - p0 < FK ? N - p0 : FK;
-    if (FAM == SPIN_HALF) {
-      // the 16 spins p0 .. p0+15 of each of the thread's walkers (0 past n)
-      uint32_t xb[4];
-      bool xv_ok[4];
+    if (tid == 0) {
+      fence_after();
+      const uint32_t a0 = smem_u32(A), b0 = smem_u32(B);
 #pragma unroll
-      for (int a = 0; a < 4; ++a) {
-        const int wl = 4 * ty + a;
-        xv_ok[a] = wl < nwb;
-        const uint64_t wd =
-            xv_ok[a] ? reinterpret_cast<const uint64_t *>(cw + (size_t)wl * cfgb)[p0 >> 6] : 0ull;
-        xb[a] = (uint32_t)(wd >> (p0 & 63));
-      }
-#pragma unroll
-      for (int kk = 0; kk < FK; ++kk) {
-        if (kk < kmax) {
-          T xv[4], jv[8];
-#pragma unroll
-          for (int a = 0; a < 4; ++a) xv[a] = xv_ok[a] ? spin_of<T>(xb[a], kk) : T(0);
-#pragma unroll
-          for (int b = 0; b < 8; ++b) jv[b] = J[kk * FS + tx + 16 * b];
-#pragma unroll
-          for (int a = 0; a < 4; ++a)
-#pragma unroll
-            for (int b = 0; b < 8; ++b) acc[a][b] = fma(jv[b], xv[a], acc[a][b]);
-        }
-      }
-    } else {
-#pragma unroll 4
-      for (int kk = 0; kk < kmax; ++kk) {
-        T xv[4], jv[8];
-#pragma unroll
-        for (int a = 0; a < 4; ++a) {
-          const int wl = 4 * ty + a;
-          xv[a] = wl < nwb ? T(cw[(size_t)wl * cfgb + p0 + kk]) : T(0);
-        }
-#pragma unroll
-        for (int b = 0; b < 8; ++b) jv[b] = J[kk * FS + tx + 16 * b];
-#pragma unroll
-        for (int a = 0; a < 4; ++a)
-#pragma unroll
-          for (int b = 0; b < 8; ++b) acc[a][b] = fma(jv[b], xv[a], acc[a][b]);
-      }
+      for (int kk = 0; kk < KCH / 32; ++kk)
+        mma_i8(tmem, sw128_desc(a0 + 32u * kk), sw128_desc(b0 + 32u * kk), (kc > 0 || kk > 0) ? 1u : 0u);
+      mma_commit(&bar[st]);
     }
-    __syncthreads();   // the next iteration's prefetch overwrites this buffer
+    last = kc;
+    __syncthreads();
+  }
+  // every MMA done: the last commit arrives after all earlier ones complete
+  if (ok && !cta_wait(&bar[(nk - 1) & 1], (uint32_t)(((nk - 1) >> 1) & 1), flag)) {
+    if (tid == 0) atomicOr(status, ST_TIMEOUT);
+    ok = false;
+  } else if (!ok && last >= 0 && tid == 0) {
+    // a wait ran out: give the committed MMAs one more bounded wait before
+    // the accumulator is freed
+    for (uint32_t it = 0; it < WAIT_LIMIT; ++it)
+      if (mbar_try_wait(&bar[last & 1], (uint32_t)((last >> 1) & 1))) break;
   }
 
+  if (ok) {
+    fence_after();
+    const int q = warp & 3, half = warp >> 2;
+    const int wl = 32 * q + lane, w = w0 + wl;
+    const uint32_t trow = tmem + ((uint32_t)(32 * q) << 16);
+    const double scale = g.jdig_scale;   // S / 128
+    const uint64_t *wbits =
+        FAM == SPIN_HALF ? reinterpret_cast<const uint64_t *>(cfg + (size_t)(w < n ? w : 0) * cfgb) : nullptr;
+    for (int j0 = half * (NT / 2); j0 < (half + 1) * (NT / 2); j0 += 4) {
+      int32_t I[D][4];
 #pragma unroll
-  for (int a = 0; a < 4; ++a) {
-    const int wl = 4 * ty + a;
-    if (wl >= nwb) continue;
-    const int w = w0 + wl;
+      for (int d = 0; d < D; ++d) tmem_ld4_async(trow + (uint32_t)(d * NT + j0), I[d]);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-    for (int b = 0; b < 8; ++b) {
-      const int k = s0 + tx + 16 * b;
-      if (k >= N) continue;
-      T v = acc[a][b];
-      if (FAM == SPIN_HALF) {
-        const uint64_t wd = reinterpret_cast<const uint64_t *>(cw + (size_t)wl * cfgb)[k >> 6];
-        const T x = ((wd >> (k & 63)) & 1ull) ? T(1) : T(-1);
-        v = x * math_exp(T(-2) * x * (g.has_h ? v + g.h[k] : v));
+      for (int e = 0; e < 4; ++e) {
+        double acc = (double)I[D - 1][e];
+#pragma unroll
+        for (int d = D - 2; d >= 0; --d) acc = (double)I[d][e] + acc * (1.0 / 128.0);
+        const int k = k0 + j0 + e;
+        if (w < n && k < N) {
+          T v = (T)(acc * scale);
+          if (FAM == SPIN_HALF) {
+            const T x = ((wbits[k >> 6] >> (k & 63)) & 1ull) ? T(1) : T(-1);
+            v = x * math_exp(T(-2) * x * (g.has_h ? v + g.h[k] : v));
+          }
+          out[(size_t)w * N + k] = v;
+        }
       }
-      out[(size_t)w * N + k] = v;
     }
   }
+  fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, BN);
+}
+
+constexpr size_t I8_SMEM = 1024 + 2 * (size_t)STAGE + 32;
+
+template <typename T, int D>
+cudaError_t launch_d(const DevModel<T> &m, const DevGuide<T> &g, int n, const void *cfg, T *out,
+                     int *status, cudaStream_t s) {
+  auto kern = m.family == SPIN_HALF ? fields_i8_kernel<T, SPIN_HALF, D>
+                                    : fields_i8_kernel<T, BOSE_HUBBARD, D>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)I8_SMEM);
+  if (e != cudaSuccess) return e;
+  const dim3 grid((n + MT - 1) / MT, (m.N + BN / D - 1) / (BN / D));
+  kern<<<grid, FT, I8_SMEM, s>>>(m, g, n, cfg, out, status);
+  return cudaGetLastError();
 }
 
 }  // namespace
 
 template <typename T>
 cudaError_t launch_fields(const DevModel<T> &m, const DevGuide<T> &g, int n, const void *cfg,
-                          T *out, cudaStream_t s) {
-  if (!g.dense || !g.Jd || g.kind == GUIDE_NONE) return cudaErrorInvalidValue;
+                          T *out, int *status, cudaStream_t s) {
+  if (!g.dense || !g.Jd || !g.jdig || g.kind == GUIDE_NONE) return cudaErrorInvalidValue;
+  if (g.jdig_d != fields_digits<T>()) return cudaErrorInvalidValue;
   if (n <= 0) return cudaSuccess;
-  const int N = m.N;
-  const size_t cfgb = m.family == SPIN_HALF ? (size_t)((N + 63) / 64) * 8 : (size_t)((N + 15) / 16) * 16;
-  const int stage_cfg = FW * cfgb <= (size_t)CFG_STAGE_MAX;
-  const size_t smem = (size_t)2 * FK * FS * sizeof(T) + (stage_cfg ? FW * cfgb : 0);
-  const dim3 grid((n + FW - 1) / FW, (N + FS - 1) / FS);
-  auto kern = m.family == SPIN_HALF ? fields_kernel<T, SPIN_HALF> : fields_kernel<T, BOSE_HUBBARD>;
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-  }
-  kern<<<grid, 256, smem, s>>>(m, g, n, cfg, out, stage_cfg);
-  return cudaGetLastError();
+  return launch_d<T, fields_digits<T>()>(m, g, n, cfg, out, status, s);
 }
 
 template cudaError_t launch_fields<double>(const DevModel<double> &, const DevGuide<double> &, int,
-                                           const void *, double *, cudaStream_t);
+                                           const void *, double *, int *, cudaStream_t);
 template cudaError_t launch_fields<float>(const DevModel<float> &, const DevGuide<float> &, int,
-                                          const void *, float *, cudaStream_t);
+                                          const void *, float *, int *, cudaStream_t);
 
 }  // namespace gfmc
