@@ -65,30 +65,37 @@ __device__ __forceinline__ void tmem_ld4_async(uint32_t taddr, int32_t (&r)[4]) 
                : "r"(taddr));
 }
 
-// 16 sites p0 .. p0+15 of walker row w as int8 x (0 past N or past the
-// population).
+__device__ __forceinline__ void cp16(void *dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int NPEND> __device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(NPEND) : "memory");
+}
+
+// Spins (bits b0..b3 of b4) as four int8 bytes, 1 for up and -1 for down:
+// the multiply spreads bit i to bit 8 i, the mask keeps those, and each
+// byte becomes ~(bit * 0xFE).
+__device__ __forceinline__ uint32_t spin_bytes4(uint32_t b4) {
+  return ~(((b4 * 0x00204081u) & 0x01010101u) * 0xFEu);
+}
+
+// 16 sites p0 .. p0+15 of a walker (row pointer crow, nullptr past the
+// population) as int8 x, 0 past N.  Spin-1/2: wd is the walker's 64-bit
+// word holding p0.
 template <int FAM>
-__device__ __forceinline__ uint4 x_chunk(const unsigned char *cfg, int cfgb, int N, int n, int w,
-                                         int p0) {
-  if (w >= n || p0 >= N) return make_uint4(0u, 0u, 0u, 0u);
+__device__ __forceinline__ uint4 x_chunk(const unsigned char *crow, uint64_t wd, int N, int p0) {
+  if (crow == nullptr || p0 >= N) return make_uint4(0u, 0u, 0u, 0u);
   uint32_t q[4];
   if (FAM == SPIN_HALF) {
-    const uint64_t wd = reinterpret_cast<const uint64_t *>(cfg + (size_t)w * cfgb)[p0 >> 6];
-    const uint32_t bits = (uint32_t)(wd >> (p0 & 63)) & 0xFFFFu;
+    const uint32_t bits = (uint32_t)(wd >> (p0 & 63));
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      uint32_t v = 0;
-#pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        const int i = 4 * e + b;
-        const uint32_t byte = (p0 + i < N) ? (((bits >> i) & 1u) ? 0x01u : 0xFFu) : 0u;
-        v |= byte << (8 * b);
-      }
-      q[e] = v;
-    }
+    for (int e = 0; e < 4; ++e) q[e] = spin_bytes4((bits >> (4 * e)) & 0xFu);
   } else {
-    const uint4 o = *reinterpret_cast<const uint4 *>(cfg + (size_t)w * cfgb + p0);
+    const uint4 o = *reinterpret_cast<const uint4 *>(crow + p0);
     q[0] = o.x; q[1] = o.y; q[2] = o.z; q[3] = o.w;
+  }
+  if (p0 + 16 > N) {
 #pragma unroll
     for (int e = 0; e < 4; ++e)
 #pragma unroll
@@ -125,6 +132,23 @@ __global__ void __launch_bounds__(FT, 1) fields_i8_kernel(DevModel<T> m, DevGuid
   fence_after();
   const uint32_t tmem = *slot;
 
+  // B: the CTA's 256 digit rows of chunk kc into its stage (the digit
+  // buffer is padded to whole chunks and tiles)
+  auto issue_b = [&](int kc) {
+    unsigned char *B = base + (kc & 1) * STAGE + MT * KCH;
+    const int8_t *src = Bg + (size_t)kc * KCH;
+#pragma unroll
+    for (int q = 0; q < (BN * 8) / FT; ++q) {
+      const int i = tid + FT * q, r = i >> 3, c = i & 7;
+      cp16(sw_chunk(B, r, c), src + (size_t)r * Kp + 16 * c);
+    }
+    cp_commit();
+  };
+  issue_b(0);
+  if (nk > 1) issue_b(1);
+
+  const int ar = tid & (MT - 1), ac0 = (tid >> 7) * 4;     // A row and first 16-site piece
+  const unsigned char *crow = w0 + ar < n ? cfg + (size_t)(w0 + ar) * cfgb : nullptr;
   bool ok = true;
   int last = -1;   // last chunk whose MMAs were committed
   for (int kc = 0; kc < nk && ok; ++kc) {
@@ -138,22 +162,24 @@ __global__ void __launch_bounds__(FT, 1) fields_i8_kernel(DevModel<T> m, DevGuid
         ok = false;
         break;
       }
+      issue_b(kc);
     }
-    // A: row r = walker w0 + r, four 16-site pieces per thread
+    // A: row ar = walker w0 + ar, four 16-site pieces (64 sites) per thread
     {
-      const int r = tid & (MT - 1), c0 = (tid >> 7) * 4;
+      const int p0 = kc * KCH + 16 * ac0;
+      uint64_t wd = 0;
+      if (FAM == SPIN_HALF && crow != nullptr && p0 < N)
+        wd = reinterpret_cast<const uint64_t *>(crow)[p0 >> 6];
 #pragma unroll
-      for (int c = c0; c < c0 + 4; ++c)
-        *reinterpret_cast<uint4 *>(sw_chunk(A, r, c)) =
-            x_chunk<FAM>(cfg, cfgb, N, n, w0 + r, kc * KCH + 16 * c);
+      for (int c = 0; c < 4; ++c)
+        *reinterpret_cast<uint4 *>(sw_chunk(A, ar, ac0 + c)) = x_chunk<FAM>(crow, wd, N, p0 + 16 * c);
     }
-    // B: the 256 digit rows of this CTA's sites, chunk kc
-#pragma unroll
-    for (int q = 0; q < (BN * 8) / FT; ++q) {
-      const int i = tid + FT * q, r = i >> 3, c = i & 7;
-      const uint4 v = __ldg(reinterpret_cast<const uint4 *>(Bg + (size_t)r * Kp + kc * KCH + 16 * c));
-      *reinterpret_cast<uint4 *>(sw_chunk(B, r, c)) = v;
-    }
+    // this chunk's B has landed (the newest group, B of chunk 1, may still be
+    // in flight while chunk 0 is used)
+    if (kc == 0 && nk > 1)
+      cp_wait<1>();
+    else
+      cp_wait<0>();
     fence_async_smem();
     __syncthreads();
     if (tid == 0) {
@@ -165,7 +191,6 @@ __global__ void __launch_bounds__(FT, 1) fields_i8_kernel(DevModel<T> m, DevGuid
       mma_commit(&bar[st]);
     }
     last = kc;
-    __syncthreads();
   }
   // every MMA done: the last commit arrives after all earlier ones complete
   if (ok && !cta_wait(&bar[(nk - 1) & 1], (uint32_t)(((nk - 1) >> 1) & 1), flag)) {
@@ -177,6 +202,7 @@ __global__ void __launch_bounds__(FT, 1) fields_i8_kernel(DevModel<T> m, DevGuid
     for (uint32_t it = 0; it < WAIT_LIMIT; ++it)
       if (mbar_try_wait(&bar[last & 1], (uint32_t)((last >> 1) & 1))) break;
   }
+  cp_wait<0>();
 
   if (ok) {
     fence_after();
@@ -184,26 +210,44 @@ __global__ void __launch_bounds__(FT, 1) fields_i8_kernel(DevModel<T> m, DevGuid
     const int wl = 32 * q + lane, w = w0 + wl;
     const uint32_t trow = tmem + ((uint32_t)(32 * q) << 16);
     const double scale = g.jdig_scale;   // S / 128
-    const uint64_t *wbits =
-        FAM == SPIN_HALF ? reinterpret_cast<const uint64_t *>(cfg + (size_t)(w < n ? w : 0) * cfgb) : nullptr;
+    // the tile's NT sites lie in one 64-bit spin word
+    uint64_t wb = 0;
+    if (FAM == SPIN_HALF && w < n && k0 < N)
+      wb = reinterpret_cast<const uint64_t *>(cfg + (size_t)w * cfgb)[k0 >> 6];
+    const bool vec = (N % 4) == 0;
     for (int j0 = half * (NT / 2); j0 < (half + 1) * (NT / 2); j0 += 4) {
       int32_t I[D][4];
 #pragma unroll
       for (int d = 0; d < D; ++d) tmem_ld4_async(trow + (uint32_t)(d * NT + j0), I[d]);
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      T v[4];
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         double acc = (double)I[D - 1][e];
 #pragma unroll
         for (int d = D - 2; d >= 0; --d) acc = (double)I[d][e] + acc * (1.0 / 128.0);
         const int k = k0 + j0 + e;
-        if (w < n && k < N) {
-          T v = (T)(acc * scale);
-          if (FAM == SPIN_HALF) {
-            const T x = ((wbits[k >> 6] >> (k & 63)) & 1ull) ? T(1) : T(-1);
-            v = x * math_exp(T(-2) * x * (g.has_h ? v + g.h[k] : v));
+        v[e] = (T)(acc * scale);
+        if (FAM == SPIN_HALF) {
+          const T x = ((wb >> (k & 63)) & 1ull) ? T(1) : T(-1);
+          const T hk = (g.has_h && k < N) ? g.h[k] : T(0);
+          v[e] = x * math_exp(T(-2) * x * (v[e] + hk));
+        }
+      }
+      const int kb = k0 + j0;
+      if (w < n) {
+        T *o = out + (size_t)w * N + kb;
+        if (vec && kb + 3 < N) {
+          if (sizeof(T) == 8) {
+            reinterpret_cast<double2 *>(o)[0] = make_double2((double)v[0], (double)v[1]);
+            reinterpret_cast<double2 *>(o)[1] = make_double2((double)v[2], (double)v[3]);
+          } else {
+            *reinterpret_cast<float4 *>(o) = make_float4((float)v[0], (float)v[1], (float)v[2], (float)v[3]);
           }
-          out[(size_t)w * N + k] = v;
+        } else {
+#pragma unroll
+          for (int e = 0; e < 4; ++e)
+            if (kb + e < N) o[e] = v[e];
         }
       }
     }
