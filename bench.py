@@ -599,17 +599,22 @@ def main():
     packed_h.copy_(eng.cfg)
     par_h = torch.empty(n, dtype=torch.int32, pin_memory=True)
     out_h = torch.empty(2, dtype=torch.float64, pin_memory=True)
-    ident = torch.arange(n, dtype=torch.int32, device=dev)
     e2e_steps = max(1, min(args.steps, 10))
     keys2, key = P.engine.key_schedule(key, e2e_steps)
+    null = ctypes.c_void_p(0)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for s in range(e2e_steps):
+        # the host population in, one step (evolve + resampling), the resampled
+        # population (configurations gathered through the parents), the
+        # parents and log G, E out
         eng.cfg.copy_(packed_h, non_blocking=True)
-        eng.parents.copy_(ident)
         eng.parents_valid = 0
         eng.steps("cont_time", TAU, None, alw, keys2[s:s + 1], logG, Es)
-        packed_h.copy_(eng.cfg, non_blocking=True)
+        P._lib.check(eng.L.gfmc_gather(eng.h, n, eng._ptr(eng.parents), eng._ptr(eng.cfg),
+                                       eng._ptr(eng.cfg_tmp), null, null, null, eng._stream()),
+                     "gfmc_gather")
+        packed_h.copy_(eng.cfg_tmp, non_blocking=True)
         par_h.copy_(eng.parents, non_blocking=True)
         out_h[0:1].copy_(logG, non_blocking=True)
         out_h[1:2].copy_(Es, non_blocking=True)
