@@ -80,6 +80,11 @@ struct gfmc_handle {
   // scratch
   int cap_n = 0, cap_steps = 0;
   double *pmax = nullptr, *psum = nullptr, *pE = nullptr, *cdf = nullptr, *wbuf = nullptr;
+  // grid-barrier counter of the one-launch resampling (grows by 2 tiles per
+  // launch; rbase mirrors it) and the most tiles such a launch can hold
+  unsigned *rctr = nullptr;
+  unsigned rbase = 0;
+  int fused_tiles = -1;
   int *plp = nullptr, *ctr = nullptr, *status = nullptr;
   unsigned long long *hops = nullptr;
   // carried guide fields (W / S per walker), double-buffered through the
@@ -631,6 +636,12 @@ int ensure_scratch(gfmc_handle *h, int n, int n_steps) {
     GFMC_CUDA(cudaMalloc(&h->hops, sizeof(unsigned long long) * n_steps));
     h->cap_steps = n_steps;
   }
+  if (!h->rctr) {
+    GFMC_CUDA(cudaMalloc(&h->rctr, sizeof(unsigned)));
+    GFMC_CUDA(cudaMemset(h->rctr, 0, sizeof(unsigned)));
+    h->rbase = 0;
+    h->fused_tiles = recon_fused_max_tiles();
+  }
   if (!h->pmax) {
     size_t np = (size_t)(h->plan.grid > 0 ? h->plan.grid : 1) * (h->plan.wpb > 0 ? h->plan.wpb : 1);
     if (h->rbm_on) np = std::max(np, (size_t)rbm_partials(h->rbm_grid, h->rbm_grid * 4));
@@ -731,7 +742,13 @@ int run_steps_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, int 
     r.parents = parents;
     r.logG_out = logG_out + st;
     r.status = h->status;
-    e = launch_reconfigure(r, s);
+    if (nb <= h->fused_tiles) {
+      // one cooperative launch (all tiles resident); each block adds 2 to the counter
+      e = launch_reconfigure_fused(r, h->rctr, h->rbase, s);
+      if (e == cudaSuccess) h->rbase += 2u * (unsigned)nb;
+    } else {
+      e = launch_reconfigure(r, s);
+    }
     if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "reconfigure launch: %s", cudaGetErrorString(e));
     if (h->fw) {
       FwHook &f = *h->fw;
@@ -1105,6 +1122,7 @@ int gfmc_create(const gfmc_model_desc *model, const gfmc_guide_desc *guide, int 
 int gfmc_destroy(gfmc_handle *h) {
   if (!h) return GFMC_OK;
   cudaFree(h->d_tables);
+  cudaFree(h->rctr);
   cudaFree(h->pmax); cudaFree(h->psum); cudaFree(h->pE); cudaFree(h->cdf); cudaFree(h->wbuf);
   cudaFree(h->plp); cudaFree(h->ctr); cudaFree(h->status); cudaFree(h->hops);
   cudaFree(h->fbuf[0]); cudaFree(h->fbuf[1]);

@@ -179,6 +179,13 @@ struct ReconArgs {
 };
 int recon_tiles(int n);
 cudaError_t launch_reconfigure(const ReconArgs &a, cudaStream_t s);
+// The same resampling as one cooperative launch of recon_tiles(a.n) blocks
+// with two grid barriers on *ctr (a counter only this launch family touches,
+// zero when allocated; bar_base = its value before the launch, which then
+// adds 2 recon_tiles(a.n)).  Needs recon_tiles(a.n) <= recon_fused_max_tiles().
+cudaError_t launch_reconfigure_fused(const ReconArgs &a, unsigned *ctr, unsigned bar_base,
+                                     cudaStream_t s);
+int recon_fused_max_tiles();
 cudaError_t launch_series_reduce(const double *pE, int nb, int n_steps, double *E_out,
                                  cudaStream_t s);
 cudaError_t launch_gather(int n, int cfg_bytes, const int *parents, const void *cfg_in,

@@ -169,6 +169,130 @@ __global__ void __launch_bounds__(RT) recon_parents(ReconArgs a, int nb) {
   a.parents[i] = k;
 }
 
+// ---- the three phases in one cooperative launch ----------------------------
+// One block of TILE threads per tile (one walker or output slot per thread);
+// the phases are separated by grid barriers on a counter that only grows
+// (the host passes its value at launch, bar_base): barrier k of the launch
+// waits until every block has arrived, i.e. the counter reaches
+// bar_base + k nb.  Each wait is bounded; one that runs out sets ST_TIMEOUT
+// (the host then reports the error) and the block carries on.  The
+// arithmetic is that of the three launches with one walker per thread.
+constexpr int FT = TILE;                 // threads per block of the fused launch
+constexpr uint32_t BAR_LIMIT = 1u << 22;
+
+__device__ __forceinline__ void grid_barrier(unsigned *ctr, unsigned target, int *status) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(ctr, 1u);
+    uint32_t it = 0;
+    while ((int)(*(volatile unsigned *)ctr - target) < 0 && ++it < BAR_LIMIT) __nanosleep(32);
+    if (it >= BAR_LIMIT) atomicOr(status, ST_TIMEOUT);
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ double block_sum_f(double v, double *sh) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  v = warp_sum(v);
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < FT / 32; ++i) r += sh[i];
+    sh[32] = r;
+  }
+  __syncthreads();
+  r = sh[32];
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(FT) recon_fused(ReconArgs a, int nb, unsigned *ctr,
+                                                  unsigned bar_base) {
+  __shared__ double sh[33];
+  __shared__ double s_scan[FT / 32];
+  __shared__ int s_lp[FT / 32];
+  __shared__ double s_tot[3];
+  __shared__ int s_last;
+  __shared__ double s_psi;
+  const int tid = threadIdx.x, lane = tid & 31, wi = tid >> 5;
+  const int k = blockIdx.x * FT + tid;
+  const double gmax = global_max(a.partial_max, a.n_partial_max, sh);
+  const double shift = lse_shift(gmax);
+  const double lwk = k < a.n ? a.log_w[k] : 0.0;
+  // phase 1: the tile's sum of exp(log_w - shift)
+  const double s = block_sum_f(k < a.n ? exp(lwk - shift) : 0.0, sh);
+  if (tid == 0) a.psum[blockIdx.x] = s;
+  grid_barrier(ctr, bar_base + (unsigned)nb, a.status);
+  // phase 2: log G, the weights and the cdf (canonical prefix of the tile sums)
+  if (tid == 0) {
+    double S = 0.0, pre = 0.0;
+    for (int b = 0; b < nb; ++b) {   // (other blocks' values: L2 loads)
+      if (b == (int)blockIdx.x) pre = S;
+      S += __ldcg(a.psum + b);
+    }
+    s_tot[0] = S;
+    s_tot[1] = log(S) + shift;
+    s_tot[2] = pre / S;
+  }
+  __syncthreads();
+  const double lG = s_tot[1], off = s_tot[2];
+  if (blockIdx.x == 0 && tid == 0) {
+    *a.logG_out = lG - log((double)a.n);
+    if (!(lG > -DBL_MAX && lG < DBL_MAX)) atomicOr(a.status, ST_NONFINITE);
+  }
+  double wk = 0.0, ek = 0.0;
+  int lp = -1;
+  if (k < a.n) {
+    wk = exp(lwk - lG);
+    ek = a.e_loc[k] * wk;
+    if (wk > 0.0) lp = k;
+  }
+  const double inc = warp_inclusive_scan(wk, lane);
+  if (lane == 31) s_scan[wi] = inc;
+  const int lpw = warp_max(lp);
+  if (lane == 0) s_lp[wi] = lpw;
+  __syncthreads();
+  double wpre = 0.0;
+  for (int i = 0; i < wi; ++i) wpre += s_scan[i];
+  if (k < a.n) {
+    a.cdf[k] = off + (wpre + inc);
+    a.wbuf[k] = wk;
+  }
+  const double e = block_sum_f(ek, sh);
+  if (tid == 0) {
+    a.pE[blockIdx.x] = e;
+    int l = -1;
+    for (int i = 0; i < FT / 32; ++i) l = s_lp[i] > l ? s_lp[i] : l;
+    a.plp[blockIdx.x] = l;
+  }
+  grid_barrier(ctr, bar_base + 2u * (unsigned)nb, a.status);
+  // phase 3: the parent of output slot k
+  if (tid == 0) {
+    int l = -1;
+    for (int b = 0; b < nb; ++b) {
+      const int pl = __ldcg(a.plp + b);
+      l = pl > l ? pl : l;
+    }
+    s_last = l < 0 ? 0 : l;
+    s_psi = uniform_f64(a.key);
+  }
+  __syncthreads();
+  if (k >= a.n) return;
+  const double u = ((double)k + s_psi) / (double)a.n;
+  int lo = 0, hi = a.n;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (__ldcg(a.cdf + mid) <= u) lo = mid + 1;
+    else hi = mid;
+  }
+  int q = lo < s_last ? lo : s_last;
+  while (q > 0 && !(__ldcg(a.wbuf + q) > 0.0)) --q;
+  a.parents[k] = q;
+}
+
 __global__ void series_reduce(const double *pE, int nb, int n_steps, double *E_out) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n_steps) return;
@@ -292,6 +416,23 @@ cudaError_t launch_reconfigure(const ReconArgs &a, cudaStream_t s) {
   recon_cdf<<<nb, RT, 0, s>>>(a, nb);
   recon_parents<<<(a.n + RT - 1) / RT, RT, 0, s>>>(a, nb);
   return cudaGetLastError();
+}
+
+int recon_fused_max_tiles() {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, recon_fused, FT, 0) != cudaSuccess)
+    return 0;
+  return sms * per_sm;
+}
+
+cudaError_t launch_reconfigure_fused(const ReconArgs &a, unsigned *ctr, unsigned bar_base,
+                                     cudaStream_t s) {
+  int nb = recon_tiles(a.n);
+  ReconArgs aa = a;
+  void *args[] = {&aa, &nb, &ctr, &bar_base};
+  return cudaLaunchCooperativeKernel((const void *)recon_fused, dim3(nb), dim3(FT), args, 0, s);
 }
 
 cudaError_t launch_series_reduce(const double *pE, int nb, int n_steps, double *E_out,
