@@ -411,7 +411,7 @@ __device__ __forceinline__ Eval<T> evaluate(const DevModel<T> &m, const DevGuide
   const int s0 = lane * C;
   int jmax = n_slots - s0;
   jmax = jmax < 0 ? 0 : (jmax > C ? C : jmax);
-#pragma unroll 4
+#pragma unroll 8
   for (int j = 0; j < jmax; ++j) {
     const int o = lamform ? s0 + j - 1 : s0 + j;
     if (!lamform || o >= 0) {
