@@ -646,10 +646,11 @@ def main():
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e_val, "unit": "walker-steps/s", "h2d_bytes_per_step": n * C,
                 "d2h_bytes_per_step": n * C + 4 * n + 16},
-        # per step: evolve, the one-launch resampling, the series reduction;
-        # plus the population guide-state product on each refresh of the
-        # carried state (every 100 steps in float64, 50 in float32)
-        "gpu_launches": 3 * args.steps + args.steps // (100 if args.precision == "fp64" else 50),
+        # per step: evolve and the one-launch resampling (which also sums the
+        # step's E_n); plus the population guide-state product on each
+        # refresh of the carried state (every 100 steps in float64, 50 in
+        # float32)
+        "gpu_launches": 2 * args.steps + args.steps // (100 if args.precision == "fp64" else 50),
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": pk["hbm_gbs"],
                      "unit": "GB/s", "frac": achieved_gbs / pk["hbm_gbs"],
                      "traffic": EVOLVE_TRAFFIC_BYTES.get((args.precision, n)),

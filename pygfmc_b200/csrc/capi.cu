@@ -743,7 +743,9 @@ int run_steps_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, int 
     r.logG_out = logG_out + st;
     r.status = h->status;
     if (nb <= h->fused_tiles) {
-      // one cooperative launch (all tiles resident); each block adds 2 to the counter
+      // one cooperative launch (all tiles resident, E_n summed in it); each
+      // block adds 2 to the counter
+      r.E_step = E_out ? E_out + st : nullptr;
       e = launch_reconfigure_fused(r, h->rctr, h->rbase, s);
       if (e == cudaSuccess) h->rbase += 2u * (unsigned)nb;
     } else {
@@ -768,8 +770,10 @@ int run_steps_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, int 
     void *t = cur; cur = nxt; nxt = t;
   }
   (void)nbc;
-  cudaError_t e = launch_series_reduce(h->pE, nb, n_steps, E_out, s);
-  if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "series reduce: %s", cudaGetErrorString(e));
+  if (nb > h->fused_tiles && E_out) {   // (the one-launch resampling wrote E_n itself)
+    cudaError_t e = launch_series_reduce(h->pE, nb, n_steps, E_out, s);
+    if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "series reduce: %s", cudaGetErrorString(e));
+  }
   if (cur != cfg)
     GFMC_CUDA(cudaMemcpyAsync(cfg, cur, (size_t)n * h->cfg_bytes, cudaMemcpyDeviceToDevice, s));
   return GFMC_OK;

@@ -176,6 +176,8 @@ struct ReconArgs {
   int *parents;           // (n,) output
   double *logG_out;       // scalar slot of this step
   int *status;
+  double *E_step;         // the one-launch resampling only: the step's E_n (sum of
+                          // pE in tile order), or nullptr
 };
 int recon_tiles(int n);
 cudaError_t launch_reconfigure(const ReconArgs &a, cudaStream_t s);

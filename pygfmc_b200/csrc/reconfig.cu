@@ -269,6 +269,12 @@ __global__ void __launch_bounds__(FT) recon_fused(ReconArgs a, int nb, unsigned 
     a.plp[blockIdx.x] = l;
   }
   grid_barrier(ctr, bar_base + 2u * (unsigned)nb, a.status);
+  // the step's E_n: the tile partials in tile order (series_reduce's sum)
+  if (a.E_step && blockIdx.x == 0 && tid == 0) {
+    double es = 0.0;
+    for (int b = 0; b < nb; ++b) es += __ldcg(a.pE + b);
+    *a.E_step = es;
+  }
   // phase 3: the parent of output slot k
   if (tid == 0) {
     int l = -1;
