@@ -231,3 +231,39 @@ def test_hop_cap_is_reported_not_hung(P):
     with pytest.raises(P._lib.GFMCError, match="iteration cap"):
         P.run(w, 4, H, 500.0, None, [2], rng_key=P.PRNGKey(1), warmup_steps=4, verbosity=0,
               max_hops_per_step=64)
+
+
+@pytest.mark.parametrize("n", [100_000, 310_000])
+def test_resampling_at_scale_matches_oracle(P, oracle, n):
+    """One cont_time step of 100 k walkers (the resampling as one cooperative
+    launch, E_n summed inside it) and of 310 k walkers (more tiles than can be
+    resident at once on a B200: the three-launch path and the series
+    reduction) on the 16-site Heisenberg chain with a nearest-neighbour
+    Jastrow guide: identical configurations and parents, log G and E_n to
+    1e-12, against the oracle's evolve and reconfiguration."""
+    import torch
+    O = oracle
+    e = P.chain(16).edges
+    H = P.SpinHalf.create(e, J_x=-1.0, J_y=-1.0, J_z=1.0, dtype=np.float64)
+    G = P.JastrowSpinHalf(16, e, beta=0.3)
+    m = O.spin_half(e, J_x=-1.0, J_y=-1.0, J_z=1.0)
+    g = O.jastrow_spin_half(16, e, 0.3, None, m)
+    cfg = P.prepare_walkers_sz(n, 16, P.PRNGKey(21), sz=0).config
+    eng = P.GFMCEngine(H, G, n, precision="fp64")
+    eng.load(cfg)
+    keys, _ = P.engine.key_schedule(P.PRNGKey(22), 1)
+    lg = torch.empty(1, dtype=torch.float64, device=eng.device)
+    En = torch.empty(1, dtype=torch.float64, device=eng.device)
+    alw = 0.45
+    eng.steps("cont_time", 0.2, None, alw, keys, lg, En)
+    c_gpu = _raw_cfg(eng, torch)
+    par_gpu = eng.parents.cpu().numpy()
+    c = np.array(cfg, dtype=np.float64, copy=True)
+    lw = np.zeros(n); el = np.zeros(n)
+    O.evolve(m, g, "cont_time", 0.2, None, alw, keys[0, :2], c, lw, el)
+    assert np.array_equal(c_gpu, c), "configurations differ"
+    par, lG, E = O.reconfigure(keys[0, 2:], c, lw, el)
+    assert np.array_equal(par_gpu, par), "parents differ"
+    np.testing.assert_allclose(lg.item(), lG, rtol=1e-12, atol=1e-13)
+    np.testing.assert_allclose(En.item(), E, rtol=1e-12, atol=1e-12)
+    assert eng.status() == 0
