@@ -386,6 +386,95 @@ def timed_steps(P, eng, alw, tau, steps, warmup, key):
     return float(np.mean(ms)), tot_hops / (eng.n * steps)
 
 
+# The reference's published throughput (paper/images/Fig3/data.csv, 1 H200,
+# iterations/s x walkers): walker-steps/s by population.
+FIG3_H200 = {1024: 1.16e6, 32768: 2.68e7, 65536: 3.63e7, 131072: 4.68e7, 1 << 20: 5.67e7,
+             1 << 24: 5.69e7}
+
+
+def fig3_bench(P, args):
+    """The reference's own throughput workload (its paper's Fig. 3): periodic
+    Heisenberg chain L = 100 (J_xy = -1, J_z = 1), no guide, single_step with
+    n_bra = 6 and lam = n_edges J_z / 4 = 25, every walker starting from the
+    Neel state, a branching step = 6 sub-steps + resampling.  Same timing
+    rules as the headline line (W warm-up steps, CUDA events per step on the
+    launching stream, L2 flushed before each, clocks sampled); the line adds
+    the published H200 number at the same population where there is one, and
+    the oracle on the host cores (C + OpenMP, ~10 s) beside it."""
+    import torch
+    L_ = 100
+    e = P.chain(L_).edges
+    H = P.SpinHalf.create(e, J_x=-1.0, J_y=-1.0, J_z=1.0, dtype=np.float64)
+    n = args.walkers
+    neel = np.where(np.arange(L_) % 2 == 0, 1.0, -1.0)
+    eng = P.GFMCEngine(H, None, n, precision=args.precision)
+    dev = eng.device
+    # one Neel row expanded on the device (no n x L host array)
+    eng.load(torch.as_tensor(neel, dtype=torch.float64, device=dev).expand(n, L_))
+    n_bra, lam = 6, 25.0
+    e0 = eng.local_energy()
+    alw = float(torch.log(lam - e0).mean().item())
+    wk = max(args.warmup, 3)
+    keys, key = P.engine.key_schedule(P.PRNGKey(1), wk)
+    lgw = torch.empty(wk, dtype=torch.float64, device=dev)
+    eng.steps("single_step", n_bra, lam, alw, keys, lgw, torch.empty_like(lgw))
+    torch.cuda.synchronize()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    logG = torch.empty(1, dtype=torch.float64, device=dev)
+    Es = torch.empty_like(logG)
+    keys, key = P.engine.key_schedule(key, args.steps)
+    stream = torch.cuda.current_stream()
+    sampler = ClockSampler(gpu_uuid(torch, dev)).start()
+    torch.cuda.synchronize()
+    ms = []
+    for st in range(args.steps):
+        flush.fill_(float(st))
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        eng.steps("single_step", n_bra, lam, alw, keys[st:st + 1], logG, Es)
+        b.record(stream)
+        b.synchronize()
+        ms.append(a.elapsed_time(b))
+    torch.cuda.synchronize()
+    clocks = summarize_clocks(sampler.stop())
+    t = float(np.sum(ms)) / 1e3
+    value = n * args.steps / t
+    ref = FIG3_H200.get(n)
+    line = {"metric": "walker-steps/s", "value": value, "unit": "walker-steps/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": wk, "ms_per_step": 1e3 * t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
+            "config": {"workload": "heisenberg_chain100_noguide_single_step_nbra6_lam25",
+                       "n_walkers": n, "precision": args.precision, "init": "neel",
+                       "l2": "flushed (256 MB write) before every timed step"},
+            "published_h200_walker_steps_per_s": ref,
+            "vs_published_h200": (value / ref) if ref else None,
+            "clocks": clocks}
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        O.build()
+        m = O.spin_half(e, J_x=-1.0, J_y=-1.0, J_z=1.0)
+        g = O.no_guide()
+        c = np.tile(neel, (args.cpu_sample, 1))
+        lw = np.zeros(len(c)); el = np.zeros(len(c))
+        k = np.asarray(P.PRNGKey(7), np.uint32)
+        times = []
+        while sum(times) < 10.0 and len(times) < 1000:
+            k, r = O.split(k, 2)
+            k1, k2 = O.fold_in(r, 0), O.fold_in(r, 1)
+            t0 = time.perf_counter()
+            O.evolve(m, g, "single_step", n_bra, lam, alw, k1, c, lw, el)
+            O.reconfigure(k2, c, lw, el)
+            times.append(time.perf_counter() - t0)
+        line["cpu_baseline"] = {"value": len(c) * len(times) / sum(times), "unit": "walker-steps/s",
+                                "cores": O.lib().om_threads(), "kind": "port",
+                                "sample": f"{args.cpu_sample} walkers x {len(times)} steps "
+                                          f"({sum(times):.1f} s), C+OpenMP restatement of the "
+                                          "reference"}
+    print(json.dumps(line))
+
+
 def mlp_bench(P, args):
     """Learned-guide workload for bosons: the 64-site Bose-Hubbard ring with
     64 bosons (n_max = 4, t = 1, U = 3; M = 129), dense MLP guide
@@ -476,6 +565,10 @@ def main():
                          "ring with the dense MLP guide")
     ap.add_argument("--hidden", type=int, default=None,
                     help="hidden units of the learned guide (default: the workload's)")
+    ap.add_argument("--workload", default="headline", choices=["headline", "fig3"],
+                    help="fig3: the reference's published throughput workload (Heisenberg chain "
+                         "L = 100, no guide, single_step n_bra = 6, lam = 25; --walkers, "
+                         "--precision)")
     ap.add_argument("--lattice", default="square16", choices=["square16", "kagome12", "bose64"],
                     help="--guide rbm / --study sigma: the 16x16 Heisenberg, the 432-site kagome "
                          "XXZ workload, or (--study sigma) the 64-site Bose-Hubbard ring with the "
@@ -488,6 +581,10 @@ def main():
     if args.study == "sigma":
         if rank == 0:
             sigma_study(P, args)
+        return
+    if args.workload == "fig3":
+        if rank == 0:
+            fig3_bench(P, args)
         return
     args.hidden_set = args.hidden is not None
     args.walkers_set = args.walkers != N_WALKERS
