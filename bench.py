@@ -443,7 +443,8 @@ def fig3_bench(P, args):
     ref = FIG3_H200.get(n)
     line = {"metric": "walker-steps/s", "value": value, "unit": "walker-steps/s", "n_gpus": 1,
             "steps": args.steps, "warmup": wk, "ms_per_step": 1e3 * t / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": (value / ref) if ref else None,   # the published 1-H200 number
             "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
             "config": {"workload": "heisenberg_chain100_noguide_single_step_nbra6_lam25",
                        "n_walkers": n, "precision": args.precision, "init": "neel",
