@@ -460,17 +460,31 @@ __global__ void __launch_bounds__(256) mlp_dw1_kernel(DevModel<float> m, MlpTabl
     const uint8_t *occ = cfg + (size_t)w * CB;
     const float *dr = d1 + (size_t)w * rpw * H1 + unit;
     float S = 0.0f;
-    for (int sl = 0; sl < rpw; ++sl) {
-      const float d = dr[(size_t)sl * H1];
-      S += d;
-      if (sl < m.n_off && d != 0.0f) {
-        const int4 c = rowcols[(size_t)w * rpw + sl];   // the rows kernel's decode
-        if (c.x < 0) continue;           // no element: its columns may not exist
-        atomicAdd(dacc + (size_t)c.y * 64 + tt, d);
-        atomicAdd(dacc + (size_t)c.x * 64 + tt, -d);
-        if (c.z >= 0) {
-          atomicAdd(dacc + (size_t)c.w * 64 + tt, d);
-          atomicAdd(dacc + (size_t)c.z * 64 + tt, -d);
+    // four rows per pass: their d1 values and decoded columns are loaded
+    // together before they are used (S still adds the rows in order)
+    for (int sl0 = 0; sl0 < rpw; sl0 += 4) {
+      float d4[4];
+      int4 c4[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int sl = sl0 + q;
+        d4[q] = sl < rpw ? dr[(size_t)sl * H1] : 0.0f;
+        c4[q] = sl < m.n_off ? rowcols[(size_t)w * rpw + sl]   // the rows kernel's decode
+                             : make_int4(-1, -1, -1, -1);
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const float d = d4[q];
+        const int4 c = c4[q];
+        S += d;
+        // (c.x < 0: no element, its columns may not exist)
+        if (d != 0.0f && c.x >= 0) {
+          atomicAdd(dacc + (size_t)c.y * 64 + tt, d);
+          atomicAdd(dacc + (size_t)c.x * 64 + tt, -d);
+          if (c.z >= 0) {
+            atomicAdd(dacc + (size_t)c.w * 64 + tt, d);
+            atomicAdd(dacc + (size_t)c.z * 64 + tt, -d);
+          }
         }
       }
     }
