@@ -375,19 +375,44 @@ __global__ void __launch_bounds__(GT, 1) mlp_gemm_kernel(MlpGemmArgs g) {
         atomicAdd(red1 + j0 + lane, sq);
       }
     } else if (g.mode == MLP_EPI_BWD) {
+      // the row's h1 and residual of the next 32 columns load while this
+      // chunk is formed (the loads are the epilogue's latency)
+      uint4 hn[4], ln[4];
+      if (valid) {
+        const uint4 *hs = reinterpret_cast<const uint4 *>(g.h1 + (size_t)row * N);
+        const uint4 *ls = reinterpret_cast<const uint4 *>(g.h1lo + (size_t)row * N);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          hn[k] = hs[k];
+          ln[k] = ls[k];
+        }
+      }
       for (int j0 = 0; j0 < N; j0 += 32) {
         uint32_t v[32];
         tmem_ld32_async(tl + (uint32_t)j0, v);
+        uint4 hc[4], lc[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          hc[k] = hn[k];
+          lc[k] = ln[k];
+        }
+        if (valid && j0 + 32 < N) {
+          const uint4 *hs = reinterpret_cast<const uint4 *>(g.h1 + (size_t)row * N + j0 + 32);
+          const uint4 *ls = reinterpret_cast<const uint4 *>(g.h1lo + (size_t)row * N + j0 + 32);
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            hn[k] = hs[k];
+            ln[k] = ls[k];
+          }
+        }
         tmem_ld_wait(v);
         float d[32];
         if (valid) {
-          const uint4 *hs = reinterpret_cast<const uint4 *>(g.h1 + (size_t)row * N + j0);
-          const uint4 *ls = reinterpret_cast<const uint4 *>(g.h1lo + (size_t)row * N + j0);
 #pragma unroll
           for (int k = 0; k < 4; ++k) {
             float f[8], fl[8];
-            bf8(hs[k], f);
-            bf8(ls[k], fl);
+            bf8(hc[k], f);
+            bf8(lc[k], fl);
 #pragma unroll
             for (int e = 0; e < 8; ++e) {
               const float t1 = f[e] + fl[e];
