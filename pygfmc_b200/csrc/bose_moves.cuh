@@ -47,20 +47,22 @@ __device__ __forceinline__ BoseMove bose_decode(const DevModel<T> &m, int o) {
 
 // Unguided off-diagonal element of a decoded move (BoseHubbard.get_rates:
 // 285-393): zero where the cutoff n_max forbids it.
+// The square roots of the occupation products (integers up to
+// (n_max + 1)^2) come from m.sqrt_tab, filled on the host with the same
+// correctly rounded square root.
 template <typename T>
 __device__ __forceinline__ T bose_element(const DevModel<T> &m, const uint8_t *occ,
                                           const BoseMove &mv) {
-  const T na = T(occ[mv.a]), nb = T(occ[mv.b]);
-  const T nmax = T(m.n_max);
+  const int na = occ[mv.a], nb = occ[mv.b], nmax = m.n_max;
   switch (mv.blk) {
-    case 0: return -m.t[mv.idx] * math_sqrt(na * (nb + T(1))) * (nb < nmax ? T(1) : T(0));
-    case 1: return -m.t[mv.idx] * math_sqrt((na + T(1)) * nb) * (na < nmax ? T(1) : T(0));
+    case 0: return -m.t[mv.idx] * m.sqrt_tab[na * (nb + 1)] * (nb < nmax ? T(1) : T(0));
+    case 1: return -m.t[mv.idx] * m.sqrt_tab[(na + 1) * nb] * (na < nmax ? T(1) : T(0));
     case 2:
-      return -m.eta[mv.idx] * math_sqrt((na + T(1)) * (nb + T(1))) *
+      return -m.eta[mv.idx] * m.sqrt_tab[(na + 1) * (nb + 1)] *
              ((na < nmax && nb < nmax) ? T(1) : T(0));
-    case 3: return -m.eta[mv.idx] * math_sqrt(na * nb);
-    case 4: return m.hpm[mv.idx] * math_sqrt(na + T(1)) * (na < nmax ? T(1) : T(0));
-    default: return m.hpm[mv.idx] * math_sqrt(na);
+    case 3: return -m.eta[mv.idx] * m.sqrt_tab[na * nb];
+    case 4: return m.hpm[mv.idx] * m.sqrt_tab[na + 1] * (na < nmax ? T(1) : T(0));
+    default: return m.hpm[mv.idx] * m.sqrt_tab[na];
   }
 }
 

@@ -353,6 +353,11 @@ int build_tables(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_des
     put("U", md->U, m.has_U ? N : 0);
     put("mu", md->mu, m.has_mu ? N : 0);
     put("hpm", md->hpm, m.n_hpm ? N : 0);
+    {
+      std::vector<T> sq((size_t)(m.n_max + 1) * (m.n_max + 1) + 1);
+      for (size_t k = 0; k < sq.size(); ++k) sq[k] = std::sqrt((T)k);   // correctly rounded
+      off["sqrt"] = A.add(sq.data(), sq.size() * sizeof(T));
+    }
     h->cfg_bytes = ((N + 15) / 16) * 16;
   } else {
     return fail(GFMC_ERR_UNSUPPORTED, "unknown model kind %d", md->kind);
@@ -565,6 +570,7 @@ int build_tables(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_des
   m.jpm = ptr("jpm"); m.jpmpm = ptr("jpmpm"); m.jz = ptr("jz"); m.hz = ptr("hz");
   m.hx_half = ptr("hx_half");
   m.t = ptr("t"); m.eta = ptr("eta"); m.U = ptr("U"); m.mu = ptr("mu"); m.hpm = ptr("hpm");
+  m.sqrt_tab = ptr("sqrt");
   if (gk != GFMC_GUIDE_NONE) {
     g.nbr = (const uint32_t *)(base + o_nbr);
     g.nbr_w = (const T *)(base + o_nbrw);

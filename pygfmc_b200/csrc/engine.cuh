@@ -41,6 +41,7 @@ template <typename T> struct DevModel {
   T k_anti, k_par;
   // BoseHubbard
   int n_max, n_hop, n_eta, n_hpm, has_U, has_mu;
+  const T *sqrt_tab;      // sqrt(k), k = 0 .. (n_max + 1)^2: the elements' square roots
   const T *t, *eta, *U, *mu, *hpm;
 };
 

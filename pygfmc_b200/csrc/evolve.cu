@@ -81,6 +81,10 @@ __host__ __device__ inline size_t stage_tables(DevModel<T> &m, DevGuide<T> &g, i
     m.U = stage_arr(m.U, m.has_U ? m.N : 0, base, off, copy);
     m.mu = stage_arr(m.mu, m.has_mu ? m.N : 0, base, off, copy);
     m.hpm = stage_arr(m.hpm, m.n_hpm ? m.N : 0, base, off, copy);
+    {
+      const int nsq = (m.n_max + 1) * (m.n_max + 1) + 1;   // staged when small (n_max <= 21)
+      m.sqrt_tab = stage_arr(m.sqrt_tab, nsq <= 513 ? nsq : 0, base, off, copy);
+    }
     if (g.kind == GUIDE_JASTROW_BOSE) {
       g.trans_pw = stage_arr(g.trans_pw, m.M, base, off, copy);
       g.h = stage_arr(g.h, g.h_mode == 2 ? m.N : 0, base, off, copy);
