@@ -53,7 +53,9 @@ __device__ __forceinline__ BoseMove bose_decode(const DevModel<T> &m, int o) {
 template <typename T>
 __device__ __forceinline__ T bose_element(const DevModel<T> &m, const uint8_t *occ,
                                           const BoseMove &mv) {
-  const int na = occ[mv.a], nb = occ[mv.b], nmax = m.n_max;
+  // (occupations clamped to n_max: the table bounds hold even for unchecked input)
+  const int nmax = m.n_max;
+  const int na = occ[mv.a] < nmax ? occ[mv.a] : nmax, nb = occ[mv.b] < nmax ? occ[mv.b] : nmax;
   switch (mv.blk) {
     case 0: return -m.t[mv.idx] * m.sqrt_tab[na * (nb + 1)] * (nb < nmax ? T(1) : T(0));
     case 1: return -m.t[mv.idx] * m.sqrt_tab[(na + 1) * nb] * (na < nmax ? T(1) : T(0));

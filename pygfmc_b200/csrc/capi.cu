@@ -386,7 +386,7 @@ int build_tables(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_des
       gk != GFMC_GUIDE_JASTROW_BOSE_HUBBARD)
     return fail(GFMC_ERR_UNSUPPORTED, "unknown guide kind %d", gk);
   g.kind = gk;
-  size_t o_jdig = 0;
+  size_t o_jdig = 0, o_slq = 0, o_sit = 0;
   size_t o_nbr = 0, o_nbrw = 0, o_cnt = 0, o_tpw = 0, o_jd = 0, o_ep = 0, o_em = 0, o_tep = 0,
            o_xy = 0;
   if (gk != GFMC_GUIDE_NONE) {
@@ -555,6 +555,29 @@ int build_tables(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_des
         if (!gd->d) return fail(GFMC_ERR_INVALID, "d array missing");
         put("gd", gd->d, N);
       }
+      // the ratio's static factors (see DevGuide::slot_q, site_t)
+      {
+        const double bs = (double)g.beta_scale;
+        std::vector<T> q(m.M, T(1));
+        int o = 1;
+        const int hop = m.n_hop ? 2 * E : 0, eta = m.n_eta ? 2 * E : 0;
+        for (int i = 0; i < hop; ++i, ++o) q[o] = (T)std::exp(-bs * (double)tpw[o]);   // da db = -1
+        for (int i = 0; i < eta; ++i, ++o) q[o] = (T)std::exp(bs * (double)tpw[o]);    // da db = +1
+        o_slq = A.add(q.data(), q.size() * sizeof(T));
+        const int nm = m.n_max;
+        std::vector<T> st((size_t)N * (nm + 1) * 2);
+        for (int k = 0; k < N; ++k) {
+          const double dk = g.d_mode == 2 ? gd->d[k] : (g.d_mode == 1 ? gd->d0 : 0.0);
+          const double hk = g.h_mode == 2 ? gd->h[k] : (g.h_mode == 1 ? gd->h0 : 0.0);
+          for (int n = 0; n <= nm; ++n)
+            for (int si = 0; si < 2; ++si) {
+              const double sv = si ? 1.0 : -1.0;
+              const double ds = (n + sv) * (n + sv) - (double)n * n;
+              st[((size_t)k * (nm + 1) + n) * 2 + si] = (T)std::exp(-dk * ds + hk * sv);
+            }
+        }
+        o_sit = A.add(st.data(), st.size() * sizeof(T));
+      }
     }
   }
 
@@ -582,6 +605,8 @@ int build_tables(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_des
       g.c_par = ptr("c_par");
     } else {
       g.trans_pw = (const T *)(base + o_tpw);
+      g.slot_q = (const T *)(base + o_slq);
+      g.site_t = (const T *)(base + o_sit);
     }
     if (g.dense) g.Jd = (const T *)(base + o_jd);
     if (g.dense && g.jdig_d) g.jdig = (const int8_t *)(base + o_jdig);

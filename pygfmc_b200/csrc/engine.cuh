@@ -57,6 +57,14 @@ template <typename T> struct DevGuide {
   const int *nbr_cnt;     // (N,) partners per site
   const T *h;             // (N,) one-body field (spin: JastrowSpinHalf.h)
   const T *trans_pw;      // (M,) bose: summed pair weight joining each transition's sites
+  // Bose: the guide ratio as a product, exp(out) = Gs_a(da) Gs_b(db) slot_q[o + 1]
+  // site_t[a][n_a][da] site_t[b][n_b][db], with the walker's carried factors
+  // Gs_k(+-1) = exp(+-beta_scale F_k) (per-warp shared memory, beside F),
+  // slot_q = exp(beta_scale da db pw) per transition (index o + 1 like
+  // trans_pw) and site_t[(k (n_max + 1) + n) 2 + (s > 0)] =
+  // exp(-d_k ((n + s)^2 - n^2) + h_k s) for s = -1, +1
+  const T *slot_q;
+  const T *site_t;
   T beta_scale;           // bose: -beta for a tied beta, else 1
   int h_mode;             // bose: 0 none, 1 tied (h0), 2 array (h)
   T h0;

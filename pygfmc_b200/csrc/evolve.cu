@@ -86,7 +86,11 @@ __host__ __device__ inline size_t stage_tables(DevModel<T> &m, DevGuide<T> &g, i
       m.sqrt_tab = stage_arr(m.sqrt_tab, nsq <= 513 ? nsq : 0, base, off, copy);
     }
     if (g.kind == GUIDE_JASTROW_BOSE) {
-      g.trans_pw = stage_arr(g.trans_pw, m.M, base, off, copy);
+      g.slot_q = stage_arr(g.slot_q, m.M, base, off, copy);
+      {
+        const int nst = m.N * (m.n_max + 1) * 2;   // staged when small
+        g.site_t = stage_arr(g.site_t, nst <= 1024 ? nst : 0, base, off, copy);
+      }
       g.h = stage_arr(g.h, g.h_mode == 2 ? m.N : 0, base, off, copy);
       g.d = stage_arr(g.d, g.d_mode == 2 ? m.N : 0, base, off, copy);
     }
@@ -132,6 +136,8 @@ __host__ __device__ inline WarpLayout warp_layout(const DevModel<T> &m, const De
   off = (off + 15) & ~size_t(15);
   L.fa = off;
   if (m.family == SPIN_HALF || g.kind != GUIDE_NONE) off += (size_t)m.N * sizeof(T);
+  // Bose-Hubbard guide: the factors exp(+beta_scale F_k), exp(-beta_scale F_k)
+  if (m.family != SPIN_HALF && g.kind != GUIDE_NONE) off += 2 * (size_t)m.N * sizeof(T);
   L.bytes = (off + 15) & ~size_t(15);
   return L;
 }
@@ -156,19 +162,21 @@ __device__ __forceinline__ T bose_offdiag(const DevModel<T> &m, const DevGuide<T
   const T na = T(occ[mv.a]), nb = T(occ[mv.b]);
   T v = bose_element<T>(m, occ, mv);
   if (g.kind && v != T(0)) {
-    T da = T(mv.da), db = T(mv.db);
-    T out = T(0);
-    if (g.d_mode) {
-      T dsa = (na + da) * (na + da) - na * na, dsb = (nb + db) * (nb + db) - nb * nb;
-      out = (g.d_mode == 2) ? -(g.d[mv.a] * dsa + g.d[mv.b] * dsb) : -g.d0 * (dsa + dsb);
-    }
-    T pw = g.trans_pw[o + 1];
-    if (g.beta_scale == T(1)) out = out + da * F[mv.a] + db * F[mv.b] + da * db * pw;
-    else out = out + g.beta_scale * (da * F[mv.a] + db * F[mv.b] + da * db * pw);
-    if (g.h_mode == 2) out = out + (g.h[mv.a] * da + g.h[mv.b] * db);
-    else if (g.h_mode == 1) out = out + g.h0 * (da + db);
-    v *= math_exp(out);
+    // exp(out) of JastrowBoseHubbard.log_diff_from_operator as the product of
+    // its factors (DevGuide::slot_q, site_t and the walker's Gs)
+    const T *Gp = F + m.N, *Gm = F + 2 * m.N;
+    const int np1 = m.n_max + 1;
+    const int oa = occ[mv.a] < m.n_max ? occ[mv.a] : m.n_max;   // (clamped: table bounds)
+    const int ob = occ[mv.b] < m.n_max ? occ[mv.b] : m.n_max;
+    T f = g.slot_q[o + 1] * (mv.da > 0 ? Gp[mv.a] : Gm[mv.a]) *
+          g.site_t[((size_t)mv.a * np1 + oa) * 2 + (mv.da > 0)];
+    if (mv.db != 0)
+      f = f * (mv.db > 0 ? Gp[mv.b] : Gm[mv.b]) *
+          g.site_t[((size_t)mv.b * np1 + ob) * 2 + (mv.db > 0)];
+    v *= f;
   }
+  (void)na;
+  (void)nb;
   return v;
 }
 
@@ -312,11 +320,28 @@ __device__ __forceinline__ void flip_pair(const DevModel<T> &m, const DevGuide<T
 
 // Bose-Hubbard Jastrow field update after site k changed by delta.
 template <typename T>
-__device__ __forceinline__ void field_update(const DevGuide<T> &g, T *F, int k, T delta, int lane) {
+__device__ __forceinline__ void field_update(const DevGuide<T> &g, T *F, int N, int k, T delta,
+                                             int lane) {
   const int c = g.nbr_cnt[k];
   const uint32_t *nb = g.nbr + (size_t)k * g.deg;
   const T *nw = g.nbr_w + (size_t)k * g.deg;
-  for (int d = lane; d < c; d += 32) F[nb[d]] += nw[d] * delta;
+  for (int d = lane; d < c; d += 32) {
+    const int q = (int)nb[d];
+    const T fq = F[q] + nw[d] * delta;
+    F[q] = fq;
+    F[N + q] = math_exp(g.beta_scale * fq);       // the partner's ratio factors
+    F[2 * N + q] = math_exp(-g.beta_scale * fq);
+  }
+  __syncwarp();
+}
+
+// The Bose-Hubbard ratio factors exp(+-beta_scale F_k) of every site from F.
+template <typename T>
+__device__ __forceinline__ void bose_factors(const DevGuide<T> &g, T *F, int N, int lane) {
+  for (int k = lane; k < N; k += 32) {
+    F[N + k] = math_exp(g.beta_scale * F[k]);
+    F[2 * N + k] = math_exp(-g.beta_scale * F[k]);
+  }
   __syncwarp();
 }
 
@@ -340,8 +365,8 @@ __device__ __forceinline__ void apply_move(const DevModel<T> &m, const DevGuide<
     }
     __syncwarp();
     if (g.kind != GUIDE_NONE) {
-      field_update(g, SF, mv.a, T(mv.da), lane);
-      if (mv.db != 0) field_update(g, SF, mv.b, T(mv.db), lane);
+      field_update(g, SF, m.N, mv.a, T(mv.da), lane);
+      if (mv.db != 0) field_update(g, SF, m.N, mv.b, T(mv.db), lane);
     }
   }
 }
@@ -595,6 +620,7 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta
         __syncwarp();
       }
     }
+    if (FAM != SPIN_HALF && guided) bose_factors(g, SF, m.N, lane);
 
     const Key kw = fold(a.key, (uint32_t)(a.walker_offset + walker));
     double lw = 0.0;
