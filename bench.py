@@ -441,7 +441,13 @@ def fig3_bench(P, args):
     t = float(np.sum(ms)) / 1e3
     value = n * args.steps / t
     ref = FIG3_H200.get(n)
+    # per step: evolve + the one-launch resampling when every 1024-walker tile
+    # fits on the GPU at once (2 per SM), else evolve + three resampling
+    # launches + the series reduction
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    per_step = 2 if (n + 1023) // 1024 <= 2 * sms else 5
     line = {"metric": "walker-steps/s", "value": value, "unit": "walker-steps/s", "n_gpus": 1,
+            "gpu_launches": per_step * args.steps,
             "steps": args.steps, "warmup": wk, "ms_per_step": 1e3 * t / args.steps,
             "higher_is_better": True, "scaling": "weak",
             "vs_baseline": (value / ref) if ref else None,   # the published 1-H200 number
