@@ -701,7 +701,6 @@ def main():
     import ctypes
     packed_h = torch.empty(n * eng.cfg_bytes, dtype=torch.uint8, pin_memory=True)
     packed_h.copy_(eng.cfg)
-    par_h = torch.empty(n, dtype=torch.int32, pin_memory=True)
     out_h = torch.empty(2, dtype=torch.float64, pin_memory=True)
     e2e_steps = max(1, min(args.steps, 10))
     keys2, key = P.engine.key_schedule(key, e2e_steps)
@@ -710,8 +709,8 @@ def main():
     t0 = time.perf_counter()
     for s in range(e2e_steps):
         # the host population in, one step (evolve + resampling), the resampled
-        # population (configurations gathered through the parents), the
-        # parents and log G, E out
+        # population (configurations gathered through the parents) and
+        # log G, E out
         eng.cfg.copy_(packed_h, non_blocking=True)
         eng.parents_valid = 0
         eng.steps("cont_time", TAU, None, alw, keys2[s:s + 1], logG, Es)
@@ -719,7 +718,6 @@ def main():
                                        eng._ptr(eng.cfg_tmp), null, null, null, eng._stream()),
                      "gfmc_gather")
         packed_h.copy_(eng.cfg_tmp, non_blocking=True)
-        par_h.copy_(eng.parents, non_blocking=True)
         out_h[0:1].copy_(logG, non_blocking=True)
         out_h[1:2].copy_(Es, non_blocking=True)
         stream.synchronize()
@@ -749,7 +747,7 @@ def main():
                    "hops_per_walker_step": total_hops / (n * args.steps),
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e_val, "unit": "walker-steps/s", "h2d_bytes_per_step": n * C,
-                "d2h_bytes_per_step": n * C + 4 * n + 16},
+                "d2h_bytes_per_step": n * C + 16},
         # per step: evolve and the one-launch resampling (which also sums the
         # step's E_n); plus the population guide-state product on each
         # refresh of the carried state (every 100 steps in float64, 50 in
