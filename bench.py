@@ -731,9 +731,11 @@ def main():
     pk, pk_kind = peaks()
     clocks = summarize_clocks(clock_lines)
     C = eng.cfg_bytes
-    # evolve (gather fused) + reconfiguration, and the carried guide fields
-    # (N values per walker, read through the parent map and written back)
-    fbytes = 2 * (L * L) * (8 if args.precision == "fp64" else 4)
+    # evolve (gather fused) + reconfiguration, the carried guide fields (N
+    # values per walker, read through the parent map and written back) and
+    # the carried evaluation record (68 values per walker, the same way)
+    tsz = 8 if args.precision == "fp64" else 4
+    fbytes = 2 * (L * L) * tsz + 2 * 68 * tsz
     alg_bytes = 4 + 2 * C + 16 + (2 * C + 36) + fbytes
     achieved_gbs = alg_bytes * n / (ms_per_step / 1e3) / 1e9
     line = {
@@ -760,8 +762,9 @@ def main():
                      "peak_source": pk_kind,
                      "note": f"algorithmic bytes per walker-step {alg_bytes} (packed configs "
                              "in/out, parent index, weights, resampling, carried guide fields "
-                             "in/out); the step is compute-bound (guide-ratio arithmetic over "
-                             "512 bonds per rate evaluation), see profiles/"},
+                             "and evaluation record in/out); the step is compute-bound "
+                             "(guide-ratio arithmetic over 512 bonds per rate evaluation), "
+                             "see profiles/"},
         "clocks": clocks,
     }
     if rank == 0 and not args.no_cpu_baseline:

@@ -94,6 +94,11 @@ struct gfmc_handle {
   int refresh_every = 100;
   void *fbuf[2] = {nullptr, nullptr};
   int fcur = 0, field_valid = 0, since_refresh = 0;
+  // evaluation records beside the carried fields (EvolveArgs::eval_in), plain
+  // and Jastrow guides; eval_valid: ebuf[fcur] holds the last cont_time
+  // step's records
+  void *ebuf[2] = {nullptr, nullptr};
+  int eval_valid = 0;
   const void *field_cfg = nullptr;
   int cap_field = 0;
   // diagonal observables (forward walking)
@@ -682,11 +687,19 @@ int ensure_scratch(gfmc_handle *h, int n, int n_steps) {
   if (h->carry && n > h->cap_field) {
     size_t tsz = h->precision == GFMC_PRECISION_FP64 ? sizeof(double) : sizeof(float);
     cudaFree(h->fbuf[0]); cudaFree(h->fbuf[1]);
+  cudaFree(h->ebuf[0]); cudaFree(h->ebuf[1]);
     h->fbuf[0] = h->fbuf[1] = nullptr;
     GFMC_CUDA(cudaMalloc(&h->fbuf[0], tsz * (size_t)n * h->state_len));
     GFMC_CUDA(cudaMalloc(&h->fbuf[1], tsz * (size_t)n * h->state_len));
+    cudaFree(h->ebuf[0]); cudaFree(h->ebuf[1]);
+    h->ebuf[0] = h->ebuf[1] = nullptr;
+    if (!h->rbm_on && !h->mlp_on) {
+      GFMC_CUDA(cudaMalloc(&h->ebuf[0], tsz * (size_t)n * EVAL_REC));
+      GFMC_CUDA(cudaMalloc(&h->ebuf[1], tsz * (size_t)n * EVAL_REC));
+    }
     h->cap_field = n;
     h->field_valid = 0;
+    h->eval_valid = 0;
   }
   if (!h->status) {
     GFMC_CUDA(cudaMalloc(&h->status, sizeof(int)));
@@ -751,6 +764,13 @@ int run_steps_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, int 
         a.field_in = h->fbuf[h->fcur];
       }
       a.field_out = h->fbuf[1 - h->fcur];
+      if (h->ebuf[0] && method == CONT_TIME) {
+        // carried fields and the last step's records: reuse its final evaluation
+        a.eval_in = (!fresh && a.field_in == h->fbuf[h->fcur] && h->eval_valid) ? h->ebuf[h->fcur]
+                                                                                : nullptr;
+        a.eval_out = h->ebuf[1 - h->fcur];
+      }
+      h->eval_valid = a.eval_out != nullptr;
       h->fcur = 1 - h->fcur;
       h->field_valid = 1;
       h->field_cfg = cfg;
@@ -1161,6 +1181,7 @@ int gfmc_destroy(gfmc_handle *h) {
   cudaFree(h->pmax); cudaFree(h->psum); cudaFree(h->pE); cudaFree(h->cdf); cudaFree(h->wbuf);
   cudaFree(h->plp); cudaFree(h->ctr); cudaFree(h->status); cudaFree(h->hops);
   cudaFree(h->fbuf[0]); cudaFree(h->fbuf[1]);
+  cudaFree(h->ebuf[0]); cudaFree(h->ebuf[1]);
   cudaFree(h->d_ops); cudaFree(h->d_diag_tables); cudaFree(h->diag.ring_parents);
   cudaFree(h->diag.ring_vals); cudaFree(h->diag_partial);
   cudaFree(h->fw_partial); cudaFree(h->fw_logG); cudaFree(h->fw_E); cudaFree(h->ctr1);

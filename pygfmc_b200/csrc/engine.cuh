@@ -133,7 +133,15 @@ struct EvolveArgs {
   float *rsum_out;        // EVALUATE, learned guides: (n_walkers,) sum of those rates; nullable
   double *diag_out;       // EVALUATE: (n_walkers,) diagonal element H_xx; nullable
   long long walker_offset;  // global index of walker 0 (streams fold_in(key, offset + i))
+  // cont_time, Jastrow and plain kernels: the rate evaluation of each
+  // walker's final configuration (EVAL_REC values of T: the 32 lanes' scan
+  // prefixes, their chunk ends, H_xx, the total, a valid flag), written at
+  // the end of the step and read through the parent map by the next step,
+  // whose first evaluation is then that record; nullable
+  const void *eval_in;
+  void *eval_out;
 };
+constexpr int EVAL_REC = 68;
 
 struct LaunchPlan {
   int grid, block, wpb;   // blocks, threads per block, warps per block

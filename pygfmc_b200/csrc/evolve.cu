@@ -634,8 +634,22 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta
       const T beta = T(a.step);
       T t = T(0);
       uint32_t it = 0;
+      // the previous step's evaluation of this configuration, when carried
+      const T *rec = a.eval_in ? reinterpret_cast<const T *>(a.eval_in) + (size_t)src * EVAL_REC
+                               : nullptr;
+      bool carried = rec != nullptr && rec[66] != T(0);
       while (t < beta) {
-        const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.n_off, MODE_OFF, lane);
+        Eval<T> ev;
+        if (carried) {
+          ev.excl = rec[lane];
+          ev.end = rec[32 + lane];
+          ev.diag = rec[64];
+          ev.total = rec[65];
+          ev.C = chunk_of(m.n_off);
+          carried = false;
+        } else {
+          ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.n_off, MODE_OFF, lane);
+        }
         const T R = ev.total;
         const T eL = ev.diag - R;
         if ((it & 15u) == 0) {
@@ -661,10 +675,22 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta
         if (tau_raw < rem) {
           apply_move<T, FAM>(m, g, occ, SF, si, lane);
           ++hops;
+        } else if (a.eval_out) {
+          // the final configuration's evaluation, for the next step
+          T *out = reinterpret_cast<T *>(a.eval_out) + (size_t)walker * EVAL_REC;
+          out[lane] = ev.excl;
+          out[32 + lane] = ev.end;
+          if (lane == 0) {
+            out[64] = ev.diag;
+            out[65] = ev.total;
+            out[66] = T(1);
+          }
         }
         eloc = eL;
         if (++it >= (uint32_t)a.max_iters) {
           if (lane == 0) atomicOr(a.status, ST_HOP_CAP);
+          if (a.eval_out && lane == 0)   // (the configuration moved after ev)
+            reinterpret_cast<T *>(a.eval_out)[(size_t)walker * EVAL_REC + 66] = T(0);
           break;
         }
       }
