@@ -515,7 +515,14 @@ int build_tables(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_des
     o_nbr = A.add(nbr.data(), nbr.size() * 4);
     o_nbrw = A.add(nbrw.data(), nbrw.size() * sizeof(T));
     o_cnt = A.add(cnt.data(), cnt.size() * 4);
-    h->carry = (g.dense || deg >= 16) ? 1 : 0;
+    // carried guide state: for dense or high-degree guides, and in the
+    // float64 build for every guide (the per-walker rebuild, N exps, costs
+    // more than 2 N values of traffic even at degree 4: the 432-site kagome
+    // guide ran 39 % faster carried).  Sparse float32 guides keep the
+    // rebuild: the float32 multiplicative updates drift by ~1e-7 per flip
+    // between refreshes, which biased the 100-site chain's energy by 4.6
+    // sigma when carried.
+    h->carry = (g.dense || deg >= 16 || h->precision == GFMC_PRECISION_FP64) ? 1 : 0;
     auto pair_sum = [&](int a, int b) -> double {
       if (a == b) return 0.0;
       auto it = lists[a].find(b);
