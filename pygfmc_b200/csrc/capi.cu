@@ -805,7 +805,17 @@ int run_steps_t(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> &g, int 
       // block adds 2 to the counter
       r.E_step = E_out ? E_out + st : nullptr;
       e = launch_reconfigure_fused(r, h->rctr, h->rbase, s);
-      if (e == cudaSuccess) h->rbase += 2u * (unsigned)nb;
+      if (e == cudaSuccess) {
+        h->rbase += 2u * (unsigned)nb;
+      } else {
+        // the cooperative launch was refused (nothing ran): the three
+        // launches from now on; the chunk's series reduction then writes
+        // every E_n (the tile partials are written on both paths)
+        (void)cudaGetLastError();
+        h->fused_tiles = 0;
+        r.E_step = nullptr;
+        e = launch_reconfigure(r, s);
+      }
     } else {
       e = launch_reconfigure(r, s);
     }
