@@ -255,8 +255,7 @@ __global__ void __launch_bounds__(MT, 1) mlp_evolve_kernel(DevModel<float> m, Ml
           uint32_t *ow = reinterpret_cast<uint32_t *>(&o4);
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
-            const __nv_bfloat162 h = __floats2bfloat162_rn(fmaf(-2.0f, sig2(KT * z[2 * i]), 1.0f),
-                                                           fmaf(-2.0f, sig2(KT * z[2 * i + 1]), 1.0f));
+            const __nv_bfloat162 h = __floats2bfloat162_rn(tanh_h1(z[2 * i]), tanh_h1(z[2 * i + 1]));
             ow[i] = *reinterpret_cast<const uint32_t *>(&h);
           }
           *reinterpret_cast<uint4 *>(sw_chunk(Ab, ridx, pc)) = o4;

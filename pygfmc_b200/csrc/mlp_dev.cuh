@@ -30,6 +30,13 @@ __device__ __forceinline__ float rcp_approx(float x) {
 
 // 1 / (1 + e^{2y}) from Ky = K y: tanh y = 1 - 2 of it.
 __device__ __forceinline__ float sig2(float Ky) { return rcp_approx(1.0f + ex2_approx(Ky)); }
+// First-layer activation before its bf16 rounding: the hardware tanh (one
+// special-function operation; its error is below the bf16 step).
+__device__ __forceinline__ float tanh_h1(float z) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(z));
+  return y;
+}
 
 // A move of the Bose-Hubbard layout (bose_decode) with its unguided element
 // (bose_element); b == a, db = 0 for the single-site h_pm moves.

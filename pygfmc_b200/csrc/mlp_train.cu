@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(256) mlp_rows_kernel(DevModel<float> m, MlpTab
           // ((z + new a) - old a), then b: the step kernel's order
           z = (z + w1v[u][0]) - w1v[u][1];
           z = (z + w1v[u][2]) - w1v[u][3];
-          const float th = tanh_k(z);
+          const float th = tanh_h1(z);   // the step kernel's first-layer activation
           hv = __float2bfloat16_rn(th);
           lv = __float2bfloat16_rn(th - __bfloat162float(hv));
         }
