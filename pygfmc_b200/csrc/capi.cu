@@ -99,6 +99,7 @@ struct gfmc_handle {
   // step's records
   void *ebuf[2] = {nullptr, nullptr};
   int eval_valid = 0;
+  int carry_optional = 0;   // carry chosen for speed only (the step can rebuild instead)
   const void *field_cfg = nullptr;
   int cap_field = 0;
   // diagonal observables (forward walking)
@@ -523,6 +524,7 @@ int build_tables(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_des
     // between refreshes, which biased the 100-site chain's energy by 4.6
     // sigma when carried.
     h->carry = (g.dense || deg >= 16 || h->precision == GFMC_PRECISION_FP64) ? 1 : 0;
+    h->carry_optional = (!g.dense && deg < 16) ? 1 : 0;   // the rebuild also works
     auto pair_sum = [&](int a, int b) -> double {
       if (a == b) return 0.0;
       auto it = lists[a].find(b);
@@ -690,6 +692,19 @@ int ensure_scratch(gfmc_handle *h, int n, int n_steps) {
     if (h->rbm_on) np = std::max(np, (size_t)rbm_partials(h->rbm_grid, h->rbm_grid * 4));
     if (h->mlp_on) np = std::max(np, (size_t)mlp_partials(h->mlp_grid, h->mlp_grid));
     GFMC_CUDA(cudaMalloc(&h->pmax, sizeof(double) * np));
+  }
+  if (h->carry && h->carry_optional && n > h->cap_field) {
+    // the optional carried state only while it takes at most half the free memory
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+      const size_t tsz = h->precision == GFMC_PRECISION_FP64 ? 8 : 4;
+      const size_t need = 2 * tsz * (size_t)n * ((size_t)h->state_len + EVAL_REC);
+      if (need > free_b / 2) {
+        h->carry = 0;
+        h->field_valid = 0;
+        h->eval_valid = 0;
+      }
+    }
   }
   if (h->carry && n > h->cap_field) {
     size_t tsz = h->precision == GFMC_PRECISION_FP64 ? sizeof(double) : sizeof(float);
