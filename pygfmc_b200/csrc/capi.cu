@@ -353,6 +353,11 @@ int build_tables(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_des
     if ((m.n_hop != 0 && m.n_hop != 2 * E) || (m.n_eta != 0 && m.n_eta != 2 * E) ||
         (m.n_hpm != 0 && m.n_hpm != N))
       return fail(GFMC_ERR_INVALID, "BoseHubbard layout sizes inconsistent");
+    if (m.n_hop && !md->t) return fail(GFMC_ERR_INVALID, "t missing");
+    if (m.n_eta && !md->eta) return fail(GFMC_ERR_INVALID, "eta missing");
+    if (m.has_U && !md->U) return fail(GFMC_ERR_INVALID, "U missing");
+    if (m.has_mu && !md->mu) return fail(GFMC_ERR_INVALID, "mu missing");
+    if (m.n_hpm && !md->hpm) return fail(GFMC_ERR_INVALID, "hpm missing");
     m.M = 1 + m.n_hop + m.n_eta + 2 * m.n_hpm;
     put("t", md->t, m.n_hop ? E : 0);
     put("eta", md->eta, m.n_eta ? E : 0);
@@ -708,13 +713,17 @@ int ensure_scratch(gfmc_handle *h, int n, int n_steps) {
   }
   if (h->carry && n > h->cap_field) {
     size_t tsz = h->precision == GFMC_PRECISION_FP64 ? sizeof(double) : sizeof(float);
+    // every old buffer is released (and forgotten) before any new one is
+    // allocated, so none is freed twice
     cudaFree(h->fbuf[0]); cudaFree(h->fbuf[1]);
-  cudaFree(h->ebuf[0]); cudaFree(h->ebuf[1]);
+    cudaFree(h->ebuf[0]); cudaFree(h->ebuf[1]);
     h->fbuf[0] = h->fbuf[1] = nullptr;
+    h->ebuf[0] = h->ebuf[1] = nullptr;
+    h->cap_field = 0;
+    h->field_valid = 0;
+    h->eval_valid = 0;
     GFMC_CUDA(cudaMalloc(&h->fbuf[0], tsz * (size_t)n * h->state_len));
     GFMC_CUDA(cudaMalloc(&h->fbuf[1], tsz * (size_t)n * h->state_len));
-    cudaFree(h->ebuf[0]); cudaFree(h->ebuf[1]);
-    h->ebuf[0] = h->ebuf[1] = nullptr;
     if (!h->rbm_on && !h->mlp_on) {
       GFMC_CUDA(cudaMalloc(&h->ebuf[0], tsz * (size_t)n * EVAL_REC));
       GFMC_CUDA(cudaMalloc(&h->ebuf[1], tsz * (size_t)n * EVAL_REC));
@@ -1162,6 +1171,8 @@ int gfmc_create(const gfmc_model_desc *model, const gfmc_guide_desc *guide, int 
   if (!model || !out) return fail(GFMC_ERR_INVALID, "null argument");
   if (model->n_sites <= 0) return fail(GFMC_ERR_INVALID, "n_sites must be positive");
   if (model->n_sites > 65535) return fail(GFMC_ERR_UNSUPPORTED, "at most 65535 sites");
+  if (model->n_edges < 0 || (model->n_edges && (!model->edge_i || !model->edge_j)))
+    return fail(GFMC_ERR_INVALID, "n_edges must be >= 0, with edge_i and edge_j given");
   if (precision != GFMC_PRECISION_FP64 && precision != GFMC_PRECISION_MIXED)
     return fail(GFMC_ERR_INVALID, "unknown precision %d", precision);
   gfmc_handle *h = new gfmc_handle();
@@ -1301,6 +1312,7 @@ int gfmc_gather(gfmc_handle *h, int n, const int32_t *parents, const void *cfg_i
                 const double *e_in, double *e_out, double *log_w, void *stream) {
   if (!h || n <= 0 || !cfg_in || !cfg_out || cfg_in == cfg_out)
     return fail(GFMC_ERR_INVALID, "gfmc_gather: bad argument");
+  if (e_out && !e_in) return fail(GFMC_ERR_INVALID, "gfmc_gather: e_out given without e_in");
   cudaError_t e = launch_gather(n, h->cfg_bytes, parents, cfg_in, cfg_out, e_in, e_out, log_w,
                                 (cudaStream_t)stream);
   if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "gather: %s", cudaGetErrorString(e));
@@ -1355,6 +1367,12 @@ int gfmc_set_diag_operators(gfmc_handle *h, int n_ops, const gfmc_diag_desc *ops
     op.N = d.n_sites;
     op.E = d.n_edges;
     if (d.n_sites != h->N) return fail(GFMC_ERR_INVALID, "diagonal operator %d: n_sites %d != %d", o, d.n_sites, h->N);
+    // every table a flag announces must be given (the kernels read it unchecked)
+    if ((d.kind == GFMC_DIAG_SPIN_HALF &&
+         (d.n_edges < 0 || (d.n_edges && (!d.edge_i || !d.edge_j)) ||
+          (d.has_jz && !d.jz) || (d.has_hz && !d.hz))) ||
+        (d.kind == GFMC_DIAG_BOSE_HUBBARD && ((d.has_U && !d.U) || (d.has_mu && !d.mu))))
+      return fail(GFMC_ERR_INVALID, "diagonal operator %d: a table its flags announce is missing", o);
     auto addd = [&](const char *nm, const double *p, size_t cnt) {
       if (p && cnt) offs[o][nm] = A.add(p, cnt * sizeof(double));
     };
@@ -1423,6 +1441,7 @@ int gfmc_reset_diag(gfmc_handle *h, int n, void *stream) {
   if (!h || n <= 0 || !h->d_ops) return fail(GFMC_ERR_INVALID, "gfmc_reset_diag: no operators set");
   cudaFree(h->diag.ring_parents); cudaFree(h->diag.ring_vals); cudaFree(h->diag_partial);
   h->diag.ring_parents = nullptr; h->diag.ring_vals = nullptr; h->diag_partial = nullptr;
+  h->diag_ready = 0;   // until the rings below exist
   const size_t size = (size_t)(h->diag.m_max + 1);
   GFMC_CUDA(cudaMalloc(&h->diag.ring_parents, sizeof(int) * size * n));
   GFMC_CUDA(cudaMalloc(&h->diag.ring_vals, sizeof(double) * size * n * (h->diag.width ? h->diag.width : 1)));
@@ -1525,7 +1544,10 @@ int gfmc_rbm_train_step(gfmc_handle *h, int n, const void *cfg, const int32_t *p
   if (rc) return rc;
   RbmTables &r = h->rbm;
   const size_t P = (size_t)r.H * h->N + r.H + h->N;
-  if (!h->ms_W) {
+  if (!h->ad_v) {
+    // (a first call that failed part-way may have left some of them)
+    cudaFree(h->ms_W); cudaFree(h->ms_b); cudaFree(h->ms_a); cudaFree(h->ad_m);
+    h->ms_W = h->ms_b = h->ms_a = h->ad_m = nullptr;
     GFMC_CUDA(cudaMalloc(&h->ms_W, sizeof(float) * (size_t)r.H * h->N));
     GFMC_CUDA(cudaMalloc(&h->ms_b, sizeof(float) * r.H));
     GFMC_CUDA(cudaMalloc(&h->ms_a, sizeof(float) * h->N));
@@ -1600,7 +1622,10 @@ int gfmc_mlp_train_step(gfmc_handle *h, int n, const void *cfg, const int32_t *p
   const MlpTables &t = h->mlp;
   const int D = h->N * t.np1;
   const long long np = mlp_param_count(t.H1, t.H2, D);
-  if (!h->mtr_p) {
+  if (!h->mtr_m2) {
+    // (a first call that failed part-way may have left some of them)
+    cudaFree(h->mtr_p); cudaFree(h->mtr_m1);
+    h->mtr_p = h->mtr_m1 = nullptr;
     GFMC_CUDA(cudaMalloc(&h->mtr_p, sizeof(float) * (size_t)np));
     GFMC_CUDA(cudaMalloc(&h->mtr_m1, sizeof(float) * (size_t)np));
     GFMC_CUDA(cudaMalloc(&h->mtr_m2, sizeof(float) * (size_t)np));

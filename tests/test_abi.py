@@ -66,3 +66,20 @@ def test_last_error_and_invalid_arguments(lib):
     assert "gfmc_key_schedule" in _lib.last_error()
     with pytest.raises(ValueError):
         _lib.check(rc, "gfmc_key_schedule")
+
+
+def test_create_rejects_edges_without_arrays(lib):
+    """gfmc_create checks the edge list before touching the device: a
+    positive n_edges without edge_i / edge_j, or a negative n_edges, is an
+    invalid argument (no GPU needed)."""
+    from pygfmc_b200 import _lib
+    for n_edges in (4, -1):
+        md = _lib.ModelDesc()
+        md.kind = _lib.MODEL_SPIN_HALF
+        md.n_sites = 4
+        md.n_edges = n_edges
+        h = ctypes.c_void_p()
+        rc = lib.gfmc_create(ctypes.byref(md), None, _lib.PRECISION_FP64, ctypes.byref(h))
+        assert rc == _lib.ERR_INVALID
+        assert "edge_i" in _lib.last_error()
+        assert not h.value
