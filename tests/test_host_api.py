@@ -167,3 +167,65 @@ def test_estimators_reproduce_golden_observables(golden, name):
         for pp in (2, 4):
             np.testing.assert_allclose(obs[nm][pp], golden[p + f"obs/{nm}/{pp}"], rtol=1e-10,
                                        atol=1e-12, err_msg=f"{nm} p={pp}")
+
+
+_N4 = 4
+
+
+def _run_table():
+    """(label, overrides, exception, message) in the form of the reference's
+    validation table (tests/core/test_validation_messages.py:62-96, engine
+    part); each must raise before any device work (none is possible on a CPU
+    host)."""
+    XX = P.SpinHalf.create(P.chain(_N4).edges, J_x=-1.0, J_y=-1.0, sign_check=False)
+
+    class NoRatios:
+        pass
+
+    rows = [(f"nonfinite step {v}", dict(step_size=v), ValueError, "step_size must be finite")
+            for v in (np.nan, np.inf, -np.inf)]
+    rows += [(f"nonfinite shift {m} {v}", dict(method=m, step_size=2, lam=v), ValueError,
+              "lam must be finite") for m in ("single_step", "multi_step")
+             for v in (np.nan, np.inf, -np.inf)]
+    rows += [
+        ("zero walkers", dict(walkers=P.prepare_walkers_from_configs(np.zeros((0, _N4)))),
+         ValueError, "At least one walker is required"),
+        ("step_size zero", dict(step_size=0.0), ValueError, "step_size must be > 0"),
+        ("step_size negative", dict(step_size=-1.0), ValueError, "step_size must be > 0"),
+        ("non-integer discrete step", dict(step_size=2.5, method="multi_step", lam=3.0), ValueError,
+         "method='multi_step' requires an integer step_size"),
+        ("hamiltonian without get_rates", dict(hamiltonian=type("Bare", (), {"M_total": 2})()),
+         TypeError, "hamiltonian 'Bare' is missing required attribute(s) get_rates"),
+        ("off-diagonal operator without get_rates",
+         dict(off_diag_operators={"bad": type("Bare", (), {"M_total": 1})()}), TypeError,
+         "off-diagonal operator 'bad' 'Bare' is missing required attribute(s) get_rates"),
+        ("guide without ratio routines", dict(guide=NoRatios()), TypeError,
+         "Guide 'NoRatios' must implement at least one of log_diff_from_operator"),
+        ("batch size not dividing the walkers", dict(off_diag_batch_size=3), ValueError,
+         "off_diag_batch_size=3 must divide N_walkers=8"),
+        ("max(p) not below n_steps", dict(n_steps=8, p_array=[8]), ValueError,
+         "every p value must be smaller than n_steps: got n_steps=8 and max(p)=8"),
+        ("off-diagonal run too short", dict(n_steps=10, p_array=[8], off_diag_operators={"xx": XX}),
+         ValueError, "off-diagonal operators need n_steps > 1.5*max(p)"),
+        ("equal windows hold no stride step",
+         dict(n_steps=13, p_array=[8], off_diag_stride=4, return_raw=False,
+              off_diag_operators={"xx": XX}),
+         ValueError, "measure only the steps 8..8 (n_steps=13"),
+        ("odd p with an off-diagonal operator", dict(p_array=[3], off_diag_operators={"xx": XX}),
+         ValueError, "All p values must be divisible by 2 when off_diag_operators have "
+                     "off-diagonal elements (M_total > 1); got [3]"),
+    ]
+    return rows
+
+
+@pytest.mark.parametrize("row", range(len(_run_table())))
+def test_run_messages_match_the_reference_table(row):
+    import re
+    label, overrides, exc, message = _run_table()[row]
+    kw = dict(walkers=P.prepare_walkers_sz(8, _N4, P.PRNGKey(0), sz=0), n_steps=20,
+              hamiltonian=P.SpinHalf.create(P.chain(_N4).edges, J_x=-1.0, J_y=-1.0, J_z=1.0),
+              step_size=0.1, guide=None, p_array=[2], rng_key=P.PRNGKey(1), warmup_steps=8,
+              verbosity=0)
+    kw.update(overrides)
+    with pytest.raises(exc, match=re.escape(message)):
+        P.run(**kw)
