@@ -229,3 +229,28 @@ def test_run_messages_match_the_reference_table(row):
     kw.update(overrides)
     with pytest.raises(exc, match=re.escape(message)):
         P.run(**kw)
+
+
+def test_require_lam_contract():
+    """engine/evolution.py require_lam:724-741: cont_time takes no shift
+    (any lam is dropped), the discrete methods need a finite one."""
+    from pygfmc_b200.engine import require_lam
+    assert require_lam("cont_time", None) is None
+    assert require_lam("cont_time", 5.0) is None
+    assert require_lam("multi_step", 4) == 4.0 and isinstance(require_lam("single_step", 4.5), float)
+    for m in ("single_step", "multi_step"):
+        with pytest.raises(ValueError, match="needs the GFMC shift"):
+            require_lam(m, None)
+    with pytest.raises(ValueError, match="Unknown method"):
+        require_lam("exact", 1.0)
+
+
+def test_lam_stays_a_keyword():
+    """lam comes after rng_key: a shift placed positionally after the
+    Hamiltonian lands in the step_size slot and the call is rejected
+    (engine/multi_gpu.py run:822)."""
+    w = P.prepare_walkers_sz(64, 8, P.PRNGKey(0), sz=0)
+    H = P.SpinHalf.create(P.chain(8).edges, J_x=-1.0, J_y=-1.0, J_z=1.0)
+    with pytest.raises(TypeError, match="got multiple values for argument 'step_size'"):
+        P.run(w, 30, H, 4.0, step_size=2, guide=None, p_array=[2], method="multi_step",
+              rng_key=P.PRNGKey(0), verbosity=0)
