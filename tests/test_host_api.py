@@ -254,3 +254,45 @@ def test_lam_stays_a_keyword():
     with pytest.raises(TypeError, match="got multiple values for argument 'step_size'"):
         P.run(w, 30, H, 4.0, step_size=2, guide=None, p_array=[2], method="multi_step",
               rng_key=P.PRNGKey(0), verbosity=0)
+
+
+@pytest.mark.parametrize("model", ["SpinHalf", "BoseHubbard"])
+@pytest.mark.parametrize("edges", [[0, 1], [[0, 1, 2]], [[-1, 0]], [[0, 1.5]], [[0, np.nan]],
+                                   [[0, np.inf]], np.empty((0, 3)), [[0, 2**63]]],
+                         ids=["flat", "three-column", "negative", "fractional", "nan", "inf",
+                              "empty-three-column", "overflow"])
+def test_models_reject_invalid_edges(model, edges):
+    """Invalid connectivity raises instead of changing the Hamiltonian
+    (hamiltonian/_common.py edges_array; the reference's
+    tests/core/test_hamiltonian_fixes.py:23-31 cases)."""
+    with pytest.raises(ValueError, match="edge"):
+        getattr(P, model).create(edges, N=3)
+
+
+@pytest.mark.parametrize("edges", [[], np.empty((0, 2)), [[0., 1.]],
+                                   np.array([[0, 1]], dtype=np.uint64)])
+def test_valid_edge_inputs_are_kept(edges):
+    H = P.SpinHalf.create(edges, N=3)
+    assert np.asarray(H.edges).shape == (len(edges), 2)
+
+
+def test_spinhalf_sign_checks_name_the_remedy():
+    """A wrong-sign J_pmpm or J_pm raises with the fix in the message, per
+    edge too; the caller-side J_x <-> J_y swap is accepted; sign_check=False
+    builds measurement operators as given (hamiltonian/SpinHalf.py create)."""
+    edges = P.chain(8).edges
+    with pytest.raises(ValueError, match="sign-problem-free"):
+        P.SpinHalf.create(edges, J_x=-0.3, J_y=-1.1, J_z=0.5, h_x=0.7)
+    with pytest.raises(ValueError, match="swap"):
+        P.SpinHalf.create(edges, J_x=-0.3, J_y=-1.1, J_z=0.5)
+    with pytest.raises(ValueError, match="J_pm"):
+        P.SpinHalf.create(edges, J_x=1.0, J_y=1.0, J_z=0.5)
+    Jx, Jy = -np.ones(len(edges)), -np.ones(len(edges))
+    Jx[3] = -0.2
+    with pytest.raises(ValueError, match="Offending edges"):
+        P.SpinHalf.create(edges, J_x=Jx, J_y=Jy, J_z=0.5)
+    ok = P.SpinHalf.create(edges, J_x=-1.1, J_y=-0.3, J_z=0.5, h_x=0.7)
+    assert float(np.ravel(ok.J_pmpm)[0]) == pytest.approx(-0.2)
+    assert float(np.ravel(ok.J_pm)[0]) == pytest.approx(-0.35)
+    meas = P.SpinHalf.create(edges, J_x=-0.3, J_y=-1.1, J_z=0.5, sign_check=False)
+    assert float(np.ravel(meas.J_pmpm)[0]) == pytest.approx(0.2)
