@@ -60,7 +60,8 @@ def build_system(P, precision):
     d = np.minimum(d, L - d)
     r = np.sqrt((d ** 2).sum(1))
     G = P.JastrowSpinHalf(n, pairs, beta=0.3 / r)
-    return lat, H, G, pairs, 0.3 / r
+    # the couplings as the guide stores them (rounded to its float32 dtype)
+    return lat, H, G, pairs, np.asarray(G.beta, np.float64)
 
 
 CLOCK_FIELDS = ("uuid,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"

@@ -133,6 +133,22 @@ def require_operator_protocol(op, role="hamiltonian"):
                         "the B200 engine has device kernels for those two transition layouts only.")
 
 
+# The attributes a guide is lowered from: those PyGFMC's own guide classes
+# store (wavefunction/jastrow_spin_half.py:79-157 and its beta / h
+# properties:162-186; wavefunction/jastrow_bose_hubbard.py:97-125).  A guide
+# carrying them -- PyGFMC's object or this package's -- lowers the same way.
+SPIN_JASTROW_ATTRS = ("N", "site_other", "_pair_site", "_pair_slot", "beta", "h")
+BOSE_JASTROW_ATTRS = ("N", "pair_i", "pair_j", "_beta", "_h", "_d")
+
+
+def _is_spin_jastrow(guide):
+    return all(hasattr(guide, a) for a in SPIN_JASTROW_ATTRS)
+
+
+def _is_bose_jastrow(guide):
+    return all(hasattr(guide, a) for a in BOSE_JASTROW_ATTRS) and not _is_spin_jastrow(guide)
+
+
 def require_guide_protocol(guide):
     if guide is None:
         return
@@ -140,11 +156,29 @@ def require_guide_protocol(guide):
         raise TypeError(f"Guide {type(guide).__name__!r} must implement at least one of "
                         "log_diff_from_operator, log_diff_from_configs, or log_psi "
                         "(the guide protocol, pygfmc.Guide).")
-    if not isinstance(guide, (JastrowSpinHalf, JastrowBoseHubbard, RBMSpinHalf, MLPBoseHubbard)) and \
-            not hasattr(guide, "_gfmc_guide_desc"):
+    if not (_is_spin_jastrow(guide) or _is_bose_jastrow(guide)
+            or isinstance(guide, (RBMSpinHalf, MLPBoseHubbard)) or hasattr(guide, "_gfmc_guide_desc")):
         raise TypeError(f"Guide {type(guide).__name__!r} has no device implementation in the B200 "
-                        "engine (supported: JastrowSpinHalf, JastrowBoseHubbard, RBMSpinHalf, "
-                        "MLPBoseHubbard).")
+                        "engine (supported: JastrowSpinHalf, JastrowBoseHubbard -- PyGFMC's or "
+                        "this package's -- RBMSpinHalf, MLPBoseHubbard).")
+
+
+def spin_jastrow_tables(guide):
+    """(pairs (n_pairs, 2) int32 in constructor order, J = -beta per pair,
+    h per site) of a spin-1/2 Jastrow guide, read from the attributes PyGFMC's
+    JastrowSpinHalf stores (its ``save``, jastrow_spin_half.py:205-210,
+    recovers the pairs the same way).  The values are the guide's own,
+    already rounded to its dtype; they are widened to float64 exactly."""
+    a = np.asarray(guide._pair_site, dtype=np.int64)
+    slot = np.asarray(guide._pair_slot, dtype=np.int64)
+    b = np.asarray(guide.site_other)[a, slot]
+    pairs = np.stack([a, b], axis=1).astype(np.int32)
+    J = -np.asarray(guide.beta, dtype=np.float64).reshape(-1)
+    N = int(guide.N)
+    h = np.broadcast_to(np.asarray(guide.h, dtype=np.float64), (N,))
+    if J.shape != (len(pairs),):
+        raise ValueError(f"JastrowSpinHalf guide has {J.shape[0]} couplings for {len(pairs)} pairs")
+    return pairs, J, h
 
 
 def model_desc(op, keep):
@@ -223,17 +257,20 @@ def guide_desc(guide, op, keep):
         return g
     if hasattr(guide, "_gfmc_guide_desc"):
         return guide._gfmc_guide_desc(op, keep)
-    if isinstance(guide, JastrowSpinHalf):
+    if _is_spin_jastrow(guide):
         if not _is_spin_half(op):
             raise TypeError(f"JastrowSpinHalf needs an operator with the SpinHalf transition layout "
                             f"(n_hx_static, n_jpm_static, edge_i, edge_j); got {type(op).__name__}")
+        if int(guide.N) != int(op.N):
+            raise ValueError(f"JastrowSpinHalf guide has N={int(guide.N)} for {int(op.N)} sites")
+        pairs, J, h = spin_jastrow_tables(guide)
         g.kind = _lib.GUIDE_JASTROW_SPIN_HALF
-        g.n_pairs = len(guide.pairs)
-        g.pair_i, g.pair_j = keep.i32(guide.pairs[:, 0]), keep.i32(guide.pairs[:, 1])
-        g.pair_w = keep.f64(guide.J_pairs)
-        g.h = keep.f64(guide.h)
+        g.n_pairs = len(pairs)
+        g.pair_i, g.pair_j = keep.i32(pairs[:, 0]), keep.i32(pairs[:, 1])
+        g.pair_w = keep.f64(J)
+        g.h = keep.f64(h)
         return g
-    if isinstance(guide, JastrowBoseHubbard):
+    if _is_bose_jastrow(guide):
         if not _is_bose(op):
             raise TypeError(f"JastrowBoseHubbard needs a BoseHubbard operator; got {type(op).__name__}")
         g.kind = _lib.GUIDE_JASTROW_BOSE_HUBBARD
@@ -242,16 +279,16 @@ def guide_desc(guide, op, keep):
         g.pair_i, g.pair_j = keep.i32(guide.pair_i), keep.i32(guide.pair_j)
         tied = np.ndim(guide._beta) == 0
         g.beta_tied = int(tied)
-        g.beta0 = float(guide._beta) if tied else 0.0
+        g.beta0 = float(np.asarray(guide._beta)) if tied else 0.0
         g.pair_w = keep.f64(np.ones(P) if tied else -np.asarray(guide._beta, np.float64))
         for name in ("h", "d"):
             v = getattr(guide, "_" + name)
             mode = 0 if v is None else (1 if np.ndim(v) == 0 else 2)
             setattr(g, name + "_mode", mode)
             if mode == 1:
-                setattr(g, name + "0", float(v))
+                setattr(g, name + "0", float(np.asarray(v)))
             elif mode == 2:
-                setattr(g, name, keep.f64(v))
+                setattr(g, name, keep.f64(np.asarray(v, np.float64)))
         return g
     if isinstance(guide, RBMSpinHalf):
         if not _is_spin_half(op):
@@ -348,6 +385,14 @@ class GFMCEngine:
 
     def set_max_iters(self, max_iters):
         _lib.check(self.L.gfmc_set_max_iters(self.h, int(max_iters)), "gfmc_set_max_iters")
+
+    def carry_mode(self, mode=-1):
+        """Sets the carried-guide-state mode of a sparse Jastrow guide (1: carry
+        while it fits, 0: rebuild per walker every step; -1: unchanged) and
+        returns whether the handle carries guide state (gfmc_carry_mode)."""
+        v = ctypes.c_int(0)
+        _lib.check(self.L.gfmc_carry_mode(self.h, int(mode), ctypes.byref(v)), "gfmc_carry_mode")
+        return bool(v.value)
 
     def status(self):
         v = ctypes.c_int(0)
@@ -1057,6 +1102,10 @@ def run_gfmc(walkers, n_steps, hamiltonian, step_size, guide, p_array, *, method
     out_w = Walker(config=cfg_np, log_weight=np.zeros(N_walker, dtype=weight_dtype),
                    e_loc=e_d.cpu().numpy().astype(weight_dtype))
     hops_np = hops_d.cpu().numpy()
+    # whether the steps carried guide state through the parent maps (a sparse
+    # guide's optional state is rebuilt per step when it does not fit; the
+    # float64 results then differ from a carried run in the last bits only)
+    carried = eng.carry_mode()
 
     # the end-of-run statistics pass from the production-final walkers, on
     # its own side-stream (driver.py _run_stats:627-660)
@@ -1071,6 +1120,7 @@ def run_gfmc(walkers, n_steps, hamiltonian, step_size, guide, p_array, *, method
         "runtime": runtime,
         "total_wall_time": time.time() - wall_start,
         "number_of_devices": 1,
+        "guide_state_carried": int(carried),
         "moves_per_walker_step": hops_np / float(N_walker),
         "parameters/n_steps": int(n_steps),
         "parameters/n_walkers": N_walker,

@@ -27,7 +27,17 @@ def require_spin_half_layout(op, guide_name):
 
 
 class JastrowSpinHalf:
-    """psi_T(x) = exp(sum_{(i,j) in pairs} J_ij x_i x_j + sum_i h_i x_i), J = -beta."""
+    """psi_T(x) = exp(sum_{(i,j) in pairs} J_ij x_i x_j + sum_i h_i x_i), J = -beta.
+
+    Stores what PyGFMC's ``JastrowSpinHalf`` stores
+    (``wavefunction/jastrow_spin_half.py:79-157``): the parameters in the
+    form they were given and rounded to ``dtype`` (``_J`` 0-d for a tied
+    coupling or one per pair, ``_h`` None / 0-d / per site), the per-site
+    partner tables ``site_other`` / ``site_valid_mask`` / ``_site_pair`` and
+    the constructor order of the pairs (``_pair_site``, ``_pair_slot``).  The
+    engine lowers a guide from exactly these attributes, so PyGFMC's own
+    guide objects and this class are interchangeable.
+    """
 
     def __init__(self, N, pairs, beta, h=None, dtype=np.float32):
         N = int(N)
@@ -38,38 +48,79 @@ class JastrowSpinHalf:
             raise ValueError(f"pair indices must lie in [0, {N}).")
         pairs_np = np.sort(pairs_np.astype(np.int32), axis=1)
         n_pairs = pairs_np.shape[0]
-        J = -np.broadcast_to(np.asarray(beta, dtype=np.float64), (n_pairs,))
-        if h is None:
-            h_np = np.zeros(N)
-        else:
-            h_in = np.asarray(h, dtype=np.float64)
+        dtype = np.dtype(dtype)
+        # the broadcast rejects a beta of any other length than n_pairs
+        J_np = -np.broadcast_to(np.asarray(beta, dtype=dtype), (n_pairs,))
+        if h is not None:
+            h_in = np.asarray(h, dtype=dtype)
             if h_in.ndim > 1 or (h_in.ndim == 1 and h_in.shape != (N,)):
                 raise ValueError(f"h must be a scalar or have shape ({N},), got {h_in.shape}")
-            h_np = np.broadcast_to(h_in, (N,)).copy()
-        self.dtype = np.dtype(dtype)
+        partners = [[] for _ in range(N)]
+        pair_site = np.zeros(n_pairs, dtype=np.int32)
+        pair_slot = np.zeros(n_pairs, dtype=np.int32)
+        for p, (a, b) in enumerate(pairs_np):
+            pair_site[p] = a
+            pair_slot[p] = len(partners[a])
+            partners[a].append((int(b), p))
+            partners[b].append((int(a), p))
+        max_deg = max((len(s) for s in partners), default=0) or 1
+        other = -np.ones((N, max_deg), dtype=np.int32)
+        site_pair = np.zeros((N, max_deg), dtype=np.int32)
+        for k in range(N):
+            for slot, (o, p) in enumerate(partners[k]):
+                other[k, slot] = o
+                site_pair[k, slot] = p
+        self.dtype = dtype
         self.N = N
-        self.pairs = pairs_np
-        self._J = J.copy()
-        self.tied_beta = np.ndim(beta) == 0
-        self._h_given = h
-        self._h = h_np
+        self.site_other = np.clip(other, 0, None)
+        self.site_valid_mask = other >= 0
+        self._pair_site = pair_site
+        self._pair_slot = pair_slot
+        self._site_pair = site_pair
+        if np.ndim(beta) == 0:
+            self._J = np.asarray(-float(np.asarray(beta)), dtype=dtype)
+        else:
+            self._J = np.array(J_np, dtype=dtype)
+        if h is None:
+            self._h = None
+        elif np.ndim(h) == 0:
+            self._h = np.asarray(float(np.asarray(h)), dtype=dtype)
+        else:
+            self._h = np.array(h_in, dtype=dtype)
 
     @property
-    def beta(self):
-        return -self._J
+    def tied_beta(self):
+        return self._J.ndim == 0
+
+    @property
+    def site_J(self):
+        """Couplings J = -beta per site and partner slot, (N, max_deg)."""
+        J = self._J if self._J.ndim == 0 else self._J[self._site_pair]
+        return np.where(self.site_valid_mask, J, 0).astype(self.dtype)
 
     @property
     def h(self):
-        return self._h
+        """One-body field per site, (N,) (zeros without a field)."""
+        if self._h is None:
+            return np.zeros(self.N, dtype=self.dtype)
+        return np.broadcast_to(self._h, (self.N,))
 
     @property
-    def J_pairs(self):
-        return self._J
+    def beta(self):
+        """Per-pair coupling beta = -J in constructor order."""
+        return -np.broadcast_to(self._J, self._pair_site.shape)
+
+    @property
+    def pairs(self):
+        """(n_pairs, 2) pairs (min, max) in constructor order."""
+        return np.stack([self._pair_site, self.site_other[self._pair_site, self._pair_slot]], axis=1)
 
     def log_psi(self, config):
         x = np.asarray(config, dtype=np.float64)
-        pair = (self._J * x[..., self.pairs[:, 0]] * x[..., self.pairs[:, 1]]).sum(-1)
-        return pair + (self._h * x).sum(-1)
+        pr = self.pairs
+        J = -self.beta.astype(np.float64)
+        pair = (J * x[..., pr[:, 0]] * x[..., pr[:, 1]]).sum(-1)
+        return pair + (self.h.astype(np.float64) * x).sum(-1)
 
     def log_diff_from_configs(self, config, new_configs):
         return self.log_psi(new_configs) - self.log_psi(config)
@@ -91,7 +142,14 @@ class JastrowSpinHalf:
 
 
 class JastrowBoseHubbard:
-    """log psi_T(x) = -sum_pairs beta_ij x_i x_j + sum_i h_i x_i - sum_i d_i x_i^2."""
+    """log psi_T(x) = -sum_pairs beta_ij x_i x_j + sum_i h_i x_i - sum_i d_i x_i^2.
+
+    Stores what PyGFMC's ``JastrowBoseHubbard`` stores
+    (``wavefunction/jastrow_bose_hubbard.py:97-125``): ``pair_i``, ``pair_j``
+    and the parameters ``_beta``, ``_h``, ``_d`` in the form they were given
+    (None, a 0-d tied value or one per pair / site), rounded to ``dtype``.
+    The engine lowers a guide from exactly these attributes.
+    """
 
     def __init__(self, N, pairs, beta, h=None, d=None, dtype=np.float32, incremental=False):
         pairs, _, n_min = edges_array(pairs)
@@ -105,14 +163,15 @@ class JastrowBoseHubbard:
         self.pair_j = pairs[:, 1].astype(np.int32)
 
         def param(v, n, name):
+            # jastrow_bose_hubbard.py _param:36-45: the form given, rounded to dtype
             if v is None:
                 return None
             a = np.asarray(v, dtype=np.float64)
             if a.ndim == 0:
-                return float(a)
+                return np.asarray(float(a), dtype=self.dtype)
             if a.shape != (n,):
                 raise ValueError(f"{name} must be a scalar or have shape ({n},), got {a.shape}")
-            return a
+            return np.asarray(a, dtype=self.dtype)
         self._beta = param(beta, len(pairs), "beta")
         self._h = param(h, self.N, "h")
         self._d = param(d, self.N, "d")
@@ -120,21 +179,22 @@ class JastrowBoseHubbard:
 
     @property
     def beta(self):
-        return np.broadcast_to(np.asarray(self._beta, np.float64), self.pair_i.shape)
+        return np.broadcast_to(self._beta, self.pair_i.shape)
 
     @property
     def h(self):
-        return np.zeros(self.N) if self._h is None else np.broadcast_to(np.asarray(self._h), (self.N,))
+        return np.zeros(self.N, self.dtype) if self._h is None else np.broadcast_to(self._h, (self.N,))
 
     @property
     def d(self):
-        return np.zeros(self.N) if self._d is None else np.broadcast_to(np.asarray(self._d), (self.N,))
+        return np.zeros(self.N, self.dtype) if self._d is None else np.broadcast_to(self._d, (self.N,))
 
     def log_psi(self, config):
         n = np.asarray(config, dtype=np.float64)
-        out = -(self.d * n * n).sum(-1)
-        out = out - (self.beta * n[..., self.pair_i] * n[..., self.pair_j]).sum(-1)
-        return out + (self.h * n).sum(-1)
+        d, beta, h = (np.asarray(v, np.float64) for v in (self.d, self.beta, self.h))
+        out = -(d * n * n).sum(-1)
+        out = out - (beta * n[..., self.pair_i] * n[..., self.pair_j]).sum(-1)
+        return out + (h * n).sum(-1)
 
     def log_diff_from_operator(self, config, op, cache=None, state=None):
         if not isinstance(op, BoseHubbard):

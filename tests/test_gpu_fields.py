@@ -13,6 +13,7 @@ import numpy as np
 import pytest
 
 import pygfmc_b200 as P
+from oracle_guides import oracle_guide
 
 pytestmark = pytest.mark.gpu
 
@@ -32,7 +33,7 @@ def _spin_cases(O):
         H = P.SpinHalf.create(lat.edges, J_x=-1.0, J_y=-1.0, J_z=1.0, dtype=np.float64)
         m = O.spin_half(lat.edges, J_x=-1.0, J_y=-1.0, J_z=1.0)
         G = P.JastrowSpinHalf(lat.N, pairs, beta=beta)
-        g = O.jastrow_spin_half(lat.N, pairs, beta, None, m)
+        g = oracle_guide(O, G, m)
         cfg = P.prepare_walkers_sz(n, lat.N, P.PRNGKey(L), sz=0).config
         out.append((f"square{L}_longrange", H, G, m, g, cfg))
     N = 300
@@ -44,7 +45,7 @@ def _spin_cases(O):
     H = P.SpinHalf.create(e, J_x=-1.0, J_y=-1.0, J_z=1.0, dtype=np.float64)
     m = O.spin_half(e, J_x=-1.0, J_y=-1.0, J_z=1.0)
     G = P.JastrowSpinHalf(N, pairs, beta=beta, h=h)
-    g = O.jastrow_spin_half(N, pairs, beta, h, m)
+    g = oracle_guide(O, G, m)
     cfg = P.prepare_walkers_random(130, N, P.PRNGKey(4)).config
     out.append(("chain300_dense_random_field", H, G, m, g, cfg))
     return out
@@ -59,7 +60,7 @@ def _bose_case(O):
     H = P.BoseHubbard.create(e, t=1.0, U=3.0, mu=0.2, n_max=2, dtype=np.float64)
     m = O.bose_hubbard(e, t=1.0, U=3.0, mu=0.2, n_max=2)
     G = P.JastrowBoseHubbard(N, pairs, beta=beta, d=0.2)
-    g = O.jastrow_bose_hubbard(N, pairs, beta, m, d=0.2)
+    g = oracle_guide(O, G, m)
     cfg = rng.integers(0, 3, (70, N)).astype(np.float64)
     return ("chain1040_bose_dense", H, G, m, g, cfg)
 

@@ -9,6 +9,7 @@ import pytest
 
 from golden_cases import (CASES, engine_diag_ops, engine_off_ops, engine_system, method_of,
                           oracle_off_ops, oracle_system)
+from oracle_guides import oracle_guide
 
 pytestmark = pytest.mark.gpu
 
@@ -70,7 +71,7 @@ def _systems(P, O):
     cfg = P.prepare_walkers_random(512, 32, P.PRNGKey(11)).config
     out.append(("chain32_hx_none", H, None, m, O.no_guide(), cfg))
     G = P.JastrowSpinHalf(32, e, beta=0.3, h=0.05)
-    out.append(("chain32_hx_jastrow", H, G, m, O.jastrow_spin_half(32, e, 0.3, 0.05, m), cfg))
+    out.append(("chain32_hx_jastrow", H, G, m, oracle_guide(O, G, m), cfg))
     sq = P.square(4)
     Hs = P.SpinHalf.create(sq.edges, J_x=-1.0, J_y=-1.0, J_z=1.0, dtype=np.float64)
     ms = O.spin_half(sq.edges, J_x=-1.0, J_y=-1.0, J_z=1.0)
@@ -81,13 +82,13 @@ def _systems(P, O):
     beta = 0.3 / r
     Gs = P.JastrowSpinHalf(16, pairs, beta=beta)
     cfgs = P.prepare_walkers_sz(512, 16, P.PRNGKey(12), sz=0).config
-    out.append(("square4_longrange", Hs, Gs, ms, O.jastrow_spin_half(16, pairs, beta, None, ms), cfgs))
+    out.append(("square4_longrange", Hs, Gs, ms, oracle_guide(O, Gs, ms), cfgs))
     # dense couplings without translation invariance, with a field
     rng = np.random.default_rng(21)
     bd = rng.uniform(0.05, 0.4, len(pairs))
     hd = rng.uniform(-0.1, 0.1, 16)
     Gd = P.JastrowSpinHalf(16, pairs, beta=bd, h=hd)
-    out.append(("square4_dense_random", Hs, Gd, ms, O.jastrow_spin_half(16, pairs, bd, hd, ms), cfgs))
+    out.append(("square4_dense_random", Hs, Gd, ms, oracle_guide(O, Gd, ms), cfgs))
     # non-uniform couplings and both fields (general spin path)
     e12 = P.chain(12).edges
     jx = -rng.uniform(0.5, 1.5, 12)
@@ -97,23 +98,23 @@ def _systems(P, O):
     mg = O.spin_half(e12, J_x=jx, J_y=jy, J_z=jz, h_z=0.3, h_x=0.2)
     Gg = P.JastrowSpinHalf(12, e12, beta=0.2, h=0.03)
     cfgg = P.prepare_walkers_random(512, 12, P.PRNGKey(14)).config
-    out.append(("chain12_xyz_fields", Hg, Gg, mg, O.jastrow_spin_half(12, e12, 0.2, 0.03, mg), cfgg))
+    out.append(("chain12_xyz_fields", Hg, Gg, mg, oracle_guide(O, Gg, mg), cfgg))
     eb = P.chain(12).edges
     B = P.BoseHubbard.create(eb, t=1.0, eta=0.2, U=3.0, mu=0.4, h_pm=0.1, n_max=3, dtype=np.float64)
     mb = O.bose_hubbard(eb, t=1.0, eta=0.2, U=3.0, mu=0.4, h_pm=0.1, n_max=3)
     betas = np.linspace(0.02, 0.2, 12)
     GB = P.JastrowBoseHubbard(12, eb, beta=betas, h=0.1, d=np.linspace(0.1, 0.3, 12))
-    gb = O.jastrow_bose_hubbard(12, eb, betas, mb, h=0.1, d=np.linspace(0.1, 0.3, 12))
+    gb = oracle_guide(O, GB, mb)
     occ = P.prepare_walkers_sz(512, 12, P.PRNGKey(13), sz=12, states=(0.0, 1.0, 2.0, 3.0)).config
     out.append(("bose12_jastrow", B, GB, mb, gb, occ))
     GBt = P.JastrowBoseHubbard(12, eb, beta=0.1, d=0.2)
-    gbt = O.jastrow_bose_hubbard(12, eb, 0.1, mb, d=0.2)
+    gbt = oracle_guide(O, GBt, mb)
     out.append(("bose12_jastrow_tied", B, GBt, mb, gbt, occ))
     # all-pairs density Jastrow: the dense path (population fields as one product)
     pb = np.array([(i, j) for i in range(12) for j in range(i + 1, 12)])
     bpd = rng.uniform(0.01, 0.1, len(pb))
     GBd = P.JastrowBoseHubbard(12, pb, beta=bpd, d=0.2)
-    gbd = O.jastrow_bose_hubbard(12, pb, bpd, mb, d=0.2)
+    gbd = oracle_guide(O, GBd, mb)
     out.append(("bose12_jastrow_dense", B, GBd, mb, gbd, occ))
     # translation-invariant long-range couplings on a 6 x 6 torus (36 sites:
     # two lanes' strides per row, a displacement table wider than one warp)
@@ -126,7 +127,7 @@ def _systems(P, O):
     b6 = 0.25 / np.sqrt((d6 ** 2).sum(1))
     G6 = P.JastrowSpinHalf(36, p6, beta=b6)
     cfg6 = P.prepare_walkers_sz(512, 36, P.PRNGKey(15), sz=0).config
-    out.append(("square6_longrange", H6, G6, m6, O.jastrow_spin_half(36, p6, b6, None, m6), cfg6))
+    out.append(("square6_longrange", H6, G6, m6, oracle_guide(O, G6, m6), cfg6))
     return out
 
 
@@ -247,7 +248,7 @@ def test_resampling_at_scale_matches_oracle(P, oracle, n):
     H = P.SpinHalf.create(e, J_x=-1.0, J_y=-1.0, J_z=1.0, dtype=np.float64)
     G = P.JastrowSpinHalf(16, e, beta=0.3)
     m = O.spin_half(e, J_x=-1.0, J_y=-1.0, J_z=1.0)
-    g = O.jastrow_spin_half(16, e, 0.3, None, m)
+    g = oracle_guide(O, G, m)
     cfg = P.prepare_walkers_sz(n, 16, P.PRNGKey(21), sz=0).config
     eng = P.GFMCEngine(H, G, n, precision="fp64")
     eng.load(cfg)

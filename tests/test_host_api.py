@@ -4,6 +4,7 @@ import numpy as np
 import pytest
 
 import pygfmc_b200 as P
+from oracle_guides import oracle_guide
 
 
 def test_spinhalf_create_conventions_and_errors():
@@ -57,7 +58,7 @@ def test_guide_ratios_match_log_psi_differences(oracle):
     H = P.SpinHalf.create(e, J_x=-1.0, J_y=-1.0, J_z=1.0, h_x=0.5)
     G = P.JastrowSpinHalf(8, e, beta=0.3, h=0.05)
     m = oracle.spin_half(e, J_x=-1.0, J_y=-1.0, J_z=1.0, h_x=0.5)
-    g = oracle.jastrow_spin_half(8, e, 0.3, 0.05, m)
+    g = oracle_guide(oracle, G, m)
     cfg = P.prepare_walkers_random(8, 8, P.PRNGKey(5)).config
     guided = oracle.rates(m, g, cfg)
     bare = oracle.rates(m, oracle.no_guide(), cfg)
@@ -69,8 +70,7 @@ def test_guide_ratios_match_log_psi_differences(oracle):
     GB = P.JastrowBoseHubbard(6, P.chain(6).edges, beta=[0.05, 0.1, 0.02, 0.3, 0.07, 0.01],
                               h=0.1, d=np.linspace(0.1, 0.4, 6))
     mb = oracle.bose_hubbard(P.chain(6).edges, t=1.0, eta=0.3, U=2.0, mu=0.5, h_pm=0.2, n_max=2)
-    gb = oracle.jastrow_bose_hubbard(6, P.chain(6).edges, np.array([0.05, 0.1, 0.02, 0.3, 0.07, 0.01]),
-                                     mb, h=0.1, d=np.linspace(0.1, 0.4, 6))
+    gb = oracle_guide(oracle, GB, mb)
     occ = P.prepare_walkers_sz(8, 6, P.PRNGKey(6), sz=6, states=(0.0, 1.0, 2.0)).config
     guided = oracle.rates(mb, gb, occ)
     bare = oracle.rates(mb, oracle.no_guide(), occ)
