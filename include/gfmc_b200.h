@@ -178,6 +178,20 @@ int gfmc_windowed_energy(int n_steps, const double *logG, const double *E, int n
  * unbounded). */
 int gfmc_set_max_iters(gfmc_handle *h, int max_iters);
 
+/* Carried guide state of sparse Jastrow guides (degree < 16; the float64
+ * build carries it by default, the float32 build rebuilds).  mode 1 (the
+ * default): carry each walker's guide fields and last rate evaluation
+ * through the parent map, while their buffers fit in half of the device
+ * memory free at the call that sizes them; mode 0: rebuild them per walker
+ * every step; mode < 0: leave the mode as it is.  Carried and rebuilt runs
+ * agree to the last bits in float64 (identical moves on every tested case).
+ * Dense guides and the learned guides always carry.  *carrying_out (host,
+ * may be NULL): 1 when the handle carries guide state (as decided by the
+ * last gfmc_run_steps call, or the mode just set).  No counterpart in
+ * PyGFMC; its JastrowBoseHubbard(incremental=True) neighbour sums
+ * (wavefunction/jastrow_bose_hubbard.py:87-92) are the nearest analogue. */
+int gfmc_carry_mode(gfmc_handle *h, int mode, int *carrying_out);
+
 /* ---- diagonal observables with forward walking ------------------------- */
 #define GFMC_DIAG_SPIN_HALF 0   /* SpinHalf.diagonal_weight (J_z edges, h_z)     */
 #define GFMC_DIAG_BOSE_HUBBARD 1 /* BoseHubbard.diagonal_weight (U, mu)          */
@@ -371,7 +385,11 @@ int gfmc_dist_parents(gfmc_handle *h, int n_walkers, const double *log_w, double
  * counts return GFMC_ERR_INVALID); all calls on a device share it, so calls
  * that overlap on the GPU race.  The first call on a device looks up the
  * array's address on that (current) device; make it before any stream
- * capture. */
+ * capture.  The return code covers the arguments and the launches only:
+ * the call does not wait for the GPU and reports no status word.  A
+ * population whose weights sum to zero or overflow is signalled by a
+ * non-finite *logG_out (and *E_out) alone -- check that it is finite; the
+ * parents are then in range but meaningless. */
 int gfmc_reconfigure_noalloc(int n_walkers, const double *log_w, const double *e_loc,
                              const uint32_t key[2], int32_t *parents_out, double *logG_out,
                              double *E_out, void *stream);

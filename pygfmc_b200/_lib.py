@@ -92,6 +92,7 @@ SIGNATURES = {
     "gfmc_gather": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gfmc_windowed_energy": (ctypes.c_int, [ctypes.c_int, _vp, _vp, ctypes.c_int, _i32p, _dp, _vp]),
     "gfmc_set_max_iters": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "gfmc_carry_mode": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     "gfmc_set_diag_operators": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(DiagDesc),
                                                ctypes.c_int, _i32p]),
     "gfmc_diag_width": (ctypes.c_int, [_vp]),

@@ -100,6 +100,8 @@ struct gfmc_handle {
   void *ebuf[2] = {nullptr, nullptr};
   int eval_valid = 0;
   int carry_optional = 0;   // carry chosen for speed only (the step can rebuild instead)
+  int carry_pref = 0;       // the carry decision made at create
+  int carry_mode = 1;       // gfmc_carry_mode: 1 carry the optional state when it fits, 0 rebuild
   const void *field_cfg = nullptr;
   int cap_field = 0;
   // diagonal observables (forward walking)
@@ -133,6 +135,7 @@ struct gfmc_handle {
         *mtr_m2 = nullptr;
   int4 *mtr_rowcols = nullptr;
   int mtr_step = 0;
+  int mtr_ready = 0;   // MLP masters and Adam moments allocated and initialised
   // RBM variance-minimisation scratch (sized for train_cap walkers) and the
   // float32 master parameters with their Adam moments
   int train_cap = 0;
@@ -145,6 +148,7 @@ struct gfmc_handle {
   double *dist_out = nullptr;
   float *ms_W = nullptr, *ms_b = nullptr, *ms_a = nullptr, *ad_m = nullptr, *ad_v = nullptr;
   int adam_step = 0;
+  int adam_ready = 0;  // RBM masters and Adam moments allocated and initialised
   // off-diagonal forward walking through this handle as the shadow chain
   FwHook *fw = nullptr;              // installed for the length of one walk
   int *ctr1 = nullptr;               // work counter of single launches (apply, min rate)
@@ -530,6 +534,7 @@ int build_tables(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_des
     // sigma when carried.
     h->carry = (g.dense || deg >= 16 || h->precision == GFMC_PRECISION_FP64) ? 1 : 0;
     h->carry_optional = (!g.dense && deg < 16) ? 1 : 0;   // the rebuild also works
+    h->carry_pref = h->carry;
     auto pair_sum = [&](int a, int b) -> double {
       if (a == b) return 0.0;
       auto it = lists[a].find(b);
@@ -698,17 +703,24 @@ int ensure_scratch(gfmc_handle *h, int n, int n_steps) {
     if (h->mlp_on) np = std::max(np, (size_t)mlp_partials(h->mlp_grid, h->mlp_grid));
     GFMC_CUDA(cudaMalloc(&h->pmax, sizeof(double) * np));
   }
-  if (h->carry && h->carry_optional && n > h->cap_field) {
-    // the optional carried state only while it takes at most half the free memory
-    size_t free_b = 0, total_b = 0;
-    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
-      const size_t tsz = h->precision == GFMC_PRECISION_FP64 ? 8 : 4;
-      const size_t need = 2 * tsz * (size_t)n * ((size_t)h->state_len + EVAL_REC);
-      if (need > free_b / 2) {
-        h->carry = 0;
-        h->field_valid = 0;
-        h->eval_valid = 0;
+  if (h->carry_optional) {
+    // the optional carried state (sparse guides): only when chosen at create
+    // and by gfmc_carry_mode, and while its buffers take at most half the
+    // free memory at the call that sizes them; otherwise the step rebuilds
+    // every walker's state (the same values up to the last bits in float64)
+    int want = h->carry_pref && h->carry_mode;
+    if (want && n > h->cap_field) {
+      size_t free_b = 0, total_b = 0;
+      if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+        const size_t tsz = h->precision == GFMC_PRECISION_FP64 ? 8 : 4;
+        const size_t need = 2 * tsz * (size_t)n * ((size_t)h->state_len + EVAL_REC);
+        if (need > free_b / 2) want = 0;
       }
+    }
+    if (want != h->carry) {
+      h->carry = want;
+      h->field_valid = 0;
+      h->eval_valid = 0;
     }
   }
   if (h->carry && n > h->cap_field) {
@@ -1467,6 +1479,21 @@ int gfmc_set_max_iters(gfmc_handle *h, int max_iters) {
   return GFMC_OK;
 }
 
+int gfmc_carry_mode(gfmc_handle *h, int mode, int *carrying_out) {
+  if (!h || mode > 1) return fail(GFMC_ERR_INVALID, "gfmc_carry_mode: bad argument");
+  if (mode >= 0 && mode != h->carry_mode) {
+    h->carry_mode = mode;
+    if (h->carry_optional) {
+      // takes effect at the next call that sizes the buffers
+      h->carry = h->carry_pref && mode;
+      h->field_valid = 0;
+      h->eval_valid = 0;
+    }
+  }
+  if (carrying_out) *carrying_out = h->carry;
+  return GFMC_OK;
+}
+
 int gfmc_read_status(gfmc_handle *h, int *status_out, void *stream) {
   if (!h || !status_out) return fail(GFMC_ERR_INVALID, "gfmc_read_status: bad argument");
   *status_out = 0;
@@ -1544,10 +1571,10 @@ int gfmc_rbm_train_step(gfmc_handle *h, int n, const void *cfg, const int32_t *p
   if (rc) return rc;
   RbmTables &r = h->rbm;
   const size_t P = (size_t)r.H * h->N + r.H + h->N;
-  if (!h->ad_v) {
+  if (!h->adam_ready) {
     // (a first call that failed part-way may have left some of them)
-    cudaFree(h->ms_W); cudaFree(h->ms_b); cudaFree(h->ms_a); cudaFree(h->ad_m);
-    h->ms_W = h->ms_b = h->ms_a = h->ad_m = nullptr;
+    cudaFree(h->ms_W); cudaFree(h->ms_b); cudaFree(h->ms_a); cudaFree(h->ad_m); cudaFree(h->ad_v);
+    h->ms_W = h->ms_b = h->ms_a = h->ad_m = h->ad_v = nullptr;
     GFMC_CUDA(cudaMalloc(&h->ms_W, sizeof(float) * (size_t)r.H * h->N));
     GFMC_CUDA(cudaMalloc(&h->ms_b, sizeof(float) * r.H));
     GFMC_CUDA(cudaMalloc(&h->ms_a, sizeof(float) * h->N));
@@ -1558,6 +1585,7 @@ int gfmc_rbm_train_step(gfmc_handle *h, int n, const void *cfg, const int32_t *p
     cudaError_t e = launch_rbm_master_init(r, h->N, h->ms_W, h->ms_b, h->ms_a, s);
     if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "master init: %s", cudaGetErrorString(e));
     h->adam_step = 0;
+    h->adam_ready = 1;
   }
   h->adam_step += 1;
   cudaError_t e = launch_adam(r.H, h->N, r.Hp, r.Np, h->ms_W, h->ms_b, h->ms_a, h->tr_gW, h->tr_gb,
@@ -1622,10 +1650,10 @@ int gfmc_mlp_train_step(gfmc_handle *h, int n, const void *cfg, const int32_t *p
   const MlpTables &t = h->mlp;
   const int D = h->N * t.np1;
   const long long np = mlp_param_count(t.H1, t.H2, D);
-  if (!h->mtr_m2) {
+  if (!h->mtr_ready) {
     // (a first call that failed part-way may have left some of them)
-    cudaFree(h->mtr_p); cudaFree(h->mtr_m1);
-    h->mtr_p = h->mtr_m1 = nullptr;
+    cudaFree(h->mtr_p); cudaFree(h->mtr_m1); cudaFree(h->mtr_m2);
+    h->mtr_p = h->mtr_m1 = h->mtr_m2 = nullptr;
     GFMC_CUDA(cudaMalloc(&h->mtr_p, sizeof(float) * (size_t)np));
     GFMC_CUDA(cudaMalloc(&h->mtr_m1, sizeof(float) * (size_t)np));
     GFMC_CUDA(cudaMalloc(&h->mtr_m2, sizeof(float) * (size_t)np));
@@ -1634,6 +1662,7 @@ int gfmc_mlp_train_step(gfmc_handle *h, int n, const void *cfg, const int32_t *p
     cudaError_t e = launch_mlp_master_init(t, D, h->mtr_p, s);
     if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "MLP master init: %s", cudaGetErrorString(e));
     h->mtr_step = 0;
+    h->mtr_ready = 1;
   }
   h->mtr_step += 1;
   cudaError_t e = launch_mlp_adam(np, h->mtr_p, h->mtr_grad, h->mtr_m1, h->mtr_m2, (float)lr,

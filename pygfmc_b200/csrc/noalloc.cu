@@ -19,7 +19,11 @@
 //    start at zero: each pass writes every entry the next pass reads;
 //  * the first call on a device looks up the array's device address
 //    (cudaGetSymbolAddress, with that device current) and caches it; make
-//    that first call before any stream capture.
+//    that first call before any stream capture;
+//  * the call does not wait for the GPU and returns no status: the status
+//    word the resampling kernels write lives in the array and is never read.
+//    The one condition it records (weights that sum to zero or overflow) is
+//    exactly a non-finite *logG_out, which is the caller's signal.
 #include <cfloat>
 #include <mutex>
 

@@ -5,9 +5,9 @@ Source: PyGFMC's own golden-output file
 its ``tests/core/test_golden_outputs.py`` writes and checks.  Only the cases
 of the hot path are kept (SpinHalf and BoseHubbard, without a guide and with
 their Jastrow guides, for the three propagators), plus the Threefry key chain
-of every case.  Run from the repository root when the reference is present:
+of every case.  Run from the repository root with the path of PyGFMC's file:
 
-    python tests/golden/make_golden.py [path/to/golden_cpu.npz]
+    python tests/golden/make_golden.py <PyGFMC>/tests/core/reference_data/golden_cpu.npz
 
 Writes ``tests/golden/golden_subset.npz``.
 """
@@ -16,7 +16,6 @@ import sys
 
 import numpy as np
 
-DEFAULT_SRC = "/root/reference/tests/core/reference_data/golden_cpu.npz"
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden_subset.npz")
 
 CASES = [f"{sys_}_{g}_{m}" for sys_ in ("spinhalf", "bose") for g in ("none", "jastrow")
@@ -29,7 +28,7 @@ KEEP = ("config", "log_weight", "e_loc", "energy/", "obs/", "raw/log_weights", "
         "stats/hops_per_step_mean", "stats/offspring_k0")
 
 
-def main(src=DEFAULT_SRC):
+def main(src):
     g = np.load(src, allow_pickle=False)
     out = {"__jax_version__": g["__jax_version__"]}
     for k in g.files:
@@ -48,4 +47,6 @@ def main(src=DEFAULT_SRC):
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <PyGFMC>/tests/core/reference_data/golden_cpu.npz")
+    main(sys.argv[1])

@@ -66,6 +66,8 @@ def test_last_error_and_invalid_arguments(lib):
     assert "gfmc_key_schedule" in _lib.last_error()
     with pytest.raises(ValueError):
         _lib.check(rc, "gfmc_key_schedule")
+    assert lib.gfmc_carry_mode(None, 1, None) == _lib.ERR_INVALID
+    assert "gfmc_carry_mode" in _lib.last_error()
 
 
 def test_create_rejects_edges_without_arrays(lib):
