@@ -368,6 +368,18 @@ int gfmc_dist_parents(gfmc_handle *h, int n_walkers, const double *log_w, double
                       double offset, double S_total, double psi, long long N_total,
                       long long slot_lo, int count, int last_pos, int32_t *parents_out,
                       void *stream);
+/* Steps 1 and 2 with their results left in device memory and no wait on the
+ * stream, for callers whose collectives run on device buffers (NCCL):
+ * gfmc_dist_local_max_dev writes the rank's max log weight to max_out
+ * (device, 1 double); after the caller's max-reduction over ranks into
+ * shift (device, 1 double), gfmc_dist_local_sums_dev writes out (device, 4
+ * doubles) = (the shift used -- 0 when the max is not finite --, S_r,
+ * sum_r w e_loc, last positive index).  One gather of the 4-double rows
+ * then gives every rank the slot partition and log G_n, E_n. */
+int gfmc_dist_local_max_dev(gfmc_handle *h, int n_walkers, const double *log_w, double *max_out,
+                            void *stream);
+int gfmc_dist_local_sums_dev(gfmc_handle *h, int n_walkers, const double *log_w,
+                             const double *e_loc, const double *shift, double *out, void *stream);
 
 /* Largest population gfmc_reconfigure_noalloc accepts. */
 #define GFMC_NOALLOC_MAX_WALKERS 131072

@@ -124,6 +124,8 @@ SIGNATURES = {
     "gfmc_dist_local_max": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _dp, _vp]),
     "gfmc_dist_local_sums": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_double, _dp,
                                             _vp]),
+    "gfmc_dist_local_max_dev": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp]),
+    "gfmc_dist_local_sums_dev": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp]),
     "gfmc_dist_parents": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_double, ctypes.c_double,
                                          ctypes.c_double, ctypes.c_double, ctypes.c_longlong,
                                          ctypes.c_longlong, ctypes.c_int, ctypes.c_int, _vp, _vp]),

@@ -1778,7 +1778,8 @@ int gfmc_dist_local_sums(gfmc_handle *h, int n, const double *log_w, const doubl
   int rc = dist_prepare(h, n);
   if (rc) return rc;
   cudaStream_t s = (cudaStream_t)stream;
-  cudaError_t e = launch_dist_sums(n, log_w, e_loc, shift, h->psum, h->pE, h->plp, h->dist_out, s);
+  cudaError_t e = launch_dist_sums(n, log_w, e_loc, shift, nullptr, h->psum, h->pE, h->plp,
+                                   h->dist_out, s);
   double tmp[4];
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(tmp, h->dist_out, sizeof(double) * 4, cudaMemcpyDeviceToHost, s);
@@ -1787,6 +1788,29 @@ int gfmc_dist_local_sums(gfmc_handle *h, int n, const double *log_w, const doubl
   out[0] = tmp[1];
   out[1] = tmp[2];
   out[2] = tmp[3];
+  return GFMC_OK;
+}
+
+int gfmc_dist_local_max_dev(gfmc_handle *h, int n, const double *log_w, double *max_out,
+                            void *stream) {
+  if (!h || n <= 0 || !log_w || !max_out)
+    return fail(GFMC_ERR_INVALID, "gfmc_dist_local_max_dev: bad argument");
+  int rc = dist_prepare(h, n);
+  if (rc) return rc;
+  cudaError_t e = launch_dist_max(n, log_w, h->psum, max_out, (cudaStream_t)stream);
+  if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "dist max: %s", cudaGetErrorString(e));
+  return GFMC_OK;
+}
+
+int gfmc_dist_local_sums_dev(gfmc_handle *h, int n, const double *log_w, const double *e_loc,
+                             const double *shift, double *out, void *stream) {
+  if (!h || n <= 0 || !log_w || !e_loc || !shift || !out)
+    return fail(GFMC_ERR_INVALID, "gfmc_dist_local_sums_dev: bad argument");
+  int rc = dist_prepare(h, n);
+  if (rc) return rc;
+  cudaError_t e = launch_dist_sums(n, log_w, e_loc, 0.0, shift, h->psum, h->pE, h->plp, out,
+                                   (cudaStream_t)stream);
+  if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "dist sums: %s", cudaGetErrorString(e));
   return GFMC_OK;
 }
 
@@ -1800,7 +1824,8 @@ int gfmc_dist_parents(gfmc_handle *h, int n, const double *log_w, double shift, 
   if (rc) return rc;
   cudaStream_t s = (cudaStream_t)stream;
   // the tile sums of this shift (the weighted-energy partials are not used)
-  cudaError_t e = launch_dist_sums(n, log_w, log_w, shift, h->psum, h->pE, h->plp, h->dist_out, s);
+  cudaError_t e = launch_dist_sums(n, log_w, log_w, shift, nullptr, h->psum, h->pE, h->plp,
+                                   h->dist_out, s);
   if (e == cudaSuccess)
     e = launch_dist_parents(n, log_w, shift, offset, h->psum, h->cdf, h->wbuf, psi, S_total,
                             N_total, slot_lo, count, last_pos, parents_out, s);

@@ -170,8 +170,10 @@ cudaError_t launch_fields(const DevModel<T> &m, const DevGuide<T> &g, int n, con
 // sum w e, last positive index).
 int dist_tiles(int n);
 cudaError_t launch_dist_max(int n, const double *lw, double *tmax, double *out, cudaStream_t s);
-cudaError_t launch_dist_sums(int n, const double *lw, const double *e, double shift, double *tS,
-                             double *tE, int *tlp, double *out, cudaStream_t s);
+// shift_dev (nullable): the shift in device memory, used instead of shift
+cudaError_t launch_dist_sums(int n, const double *lw, const double *e, double shift,
+                             const double *shift_dev, double *tS, double *tE, int *tlp,
+                             double *out, cudaStream_t s);
 cudaError_t launch_dist_parents(int n, const double *lw, double shift, double offset,
                                 const double *tS, double *cdf, double *wbuf, double psi,
                                 double S_total, long long N_total, long long i_lo, int count,

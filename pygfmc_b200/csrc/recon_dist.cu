@@ -40,11 +40,19 @@ __global__ void dist_tile_max(int n, const double *lw, double *tmax) {
   }
 }
 
+// the common shift: the host value, or the one in device memory when given
+// (the max over ranks reduced there); a non-finite max (no live walker) is 0
+__device__ __forceinline__ double dist_shift(double shift, const double *shift_p) {
+  const double v = shift_p ? *shift_p : shift;
+  return (v > -DBL_MAX && v < DBL_MAX) ? v : 0.0;
+}
+
 // per tile: sum w, sum w e, last positive index (w = exp(lw - shift))
-__global__ void dist_tile_sums(int n, const double *lw, const double *e, double shift,
-                               double *tS, double *tE, int *tlp) {
+__global__ void dist_tile_sums(int n, const double *lw, const double *e, double shift_h,
+                               const double *shift_p, double *tS, double *tE, int *tlp) {
   __shared__ double s1[DT / 32], s2[DT / 32];
   __shared__ int s3[DT / 32];
+  const double shift = dist_shift(shift_h, shift_p);
   double a = 0.0, b = 0.0;
   int lp = -1;
   const int base = blockIdx.x * DTILE + threadIdx.x * DPT;
@@ -80,9 +88,10 @@ __global__ void dist_tile_sums(int n, const double *lw, const double *e, double 
   }
 }
 
-// out = (max, S, sum w e, last positive index) over the tiles
+// over the tiles: out[0] = max (tmax given) or the shift the sums used;
+// out[1..3] = (S, sum w e, last positive index) (tS given)
 __global__ void dist_combine(int nb, const double *tmax, const double *tS, const double *tE,
-                             const int *tlp, double *out) {
+                             const int *tlp, double shift_h, const double *shift_p, double *out) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   double m = -DBL_MAX, S = 0.0, SE = 0.0;
   int l = -1;
@@ -94,7 +103,11 @@ __global__ void dist_combine(int nb, const double *tmax, const double *tS, const
       l = tlp[b] > l ? tlp[b] : l;
     }
   }
-  out[0] = m;
+  if (tmax) {
+    out[0] = m;
+    return;
+  }
+  out[0] = dist_shift(shift_h, shift_p);
   out[1] = S;
   out[2] = SE;
   out[3] = (double)l;
@@ -162,15 +175,16 @@ int dist_tiles(int n) { return (n + DTILE - 1) / DTILE; }
 cudaError_t launch_dist_max(int n, const double *lw, double *tmax, double *out, cudaStream_t s) {
   const int nb = dist_tiles(n);
   dist_tile_max<<<nb, DT, 0, s>>>(n, lw, tmax);
-  dist_combine<<<1, 32, 0, s>>>(nb, tmax, nullptr, nullptr, nullptr, out);
+  dist_combine<<<1, 32, 0, s>>>(nb, tmax, nullptr, nullptr, nullptr, 0.0, nullptr, out);
   return cudaGetLastError();
 }
 
-cudaError_t launch_dist_sums(int n, const double *lw, const double *e, double shift, double *tS,
-                             double *tE, int *tlp, double *out, cudaStream_t s) {
+cudaError_t launch_dist_sums(int n, const double *lw, const double *e, double shift,
+                             const double *shift_dev, double *tS, double *tE, int *tlp,
+                             double *out, cudaStream_t s) {
   const int nb = dist_tiles(n);
-  dist_tile_sums<<<nb, DT, 0, s>>>(n, lw, e, shift, tS, tE, tlp);
-  dist_combine<<<1, 32, 0, s>>>(nb, nullptr, tS, tE, tlp, out);
+  dist_tile_sums<<<nb, DT, 0, s>>>(n, lw, e, shift, shift_dev, tS, tE, tlp);
+  dist_combine<<<1, 32, 0, s>>>(nb, nullptr, tS, tE, tlp, shift, shift_dev, out);
   return cudaGetLastError();
 }
 

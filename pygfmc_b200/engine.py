@@ -831,7 +831,7 @@ def run_gfmc(walkers, n_steps, hamiltonian, step_size, guide, p_array, *, method
              rng_key=None, lam=None, diag_operators=None, off_diag_operators=None,
              return_raw=True, avg_log_weight=None, warmup_steps=None, verbosity=7,
              number_of_outputs=100, off_diag_stride=1, off_diag_batch_size=None,
-             precision=None, max_hops_per_step=None, _step_offset=0):
+             precision=None, max_hops_per_step=None, _step_offset=0, _shards=None):
     """GFMC on one B200 with PyGFMC's run_gfmc signature and return tuple.
 
     ``precision``: ``"fp64"`` (every step quantity in float64, the build that
@@ -904,7 +904,25 @@ def run_gfmc(walkers, n_steps, hamiltonian, step_size, guide, p_array, *, method
     step_f = float(step_size)
 
     torch = _torch()
-    eng = GFMCEngine(hamiltonian, guide, N_walker, precision=precision)
+    n_dev = 1
+    if _shards is not None:
+        # a population sharded over GPUs (no measurement operators here)
+        from .distributed import ShardedPopulation
+        n_dev, shard_devices = _shards
+        if shard_devices is None:
+            import torch.distributed as dist
+            grouped = dist.is_available() and dist.is_initialized() and dist.get_world_size() == n_dev
+            if not grouped:
+                if torch.cuda.device_count() < n_dev:
+                    raise ValueError(f"n_devices={n_dev} but {torch.cuda.device_count()} GPU(s) are "
+                                     "visible and no torch.distributed group of that size is set up")
+                shard_devices = [f"cuda:{d}" for d in range(n_dev)]
+        if N_walker % n_dev:
+            raise ValueError(f"N_walkers={N_walker} must be divisible by n_devices={n_dev}")
+        eng = ShardedPopulation(hamiltonian, guide, N_walker, precision=precision,
+                                devices=shard_devices)
+    else:
+        eng = GFMCEngine(hamiltonian, guide, N_walker, precision=precision)
     if max_hops_per_step is not None:
         eng.set_max_iters(_validated_int("max_hops_per_step", max_hops_per_step, 1))
     eng.load(np.asarray(config) if not torch.is_tensor(config) else config)
@@ -1119,7 +1137,7 @@ def run_gfmc(walkers, n_steps, hamiltonian, step_size, guide, p_array, *, method
         "it_per_sec": n_steps / runtime,
         "runtime": runtime,
         "total_wall_time": time.time() - wall_start,
-        "number_of_devices": 1,
+        "number_of_devices": n_dev,
         "guide_state_carried": int(carried),
         "moves_per_walker_step": hops_np / float(N_walker),
         "parameters/n_steps": int(n_steps),
@@ -1174,17 +1192,45 @@ def run_gfmc(walkers, n_steps, hamiltonian, step_size, guide, p_array, *, method
     return out_w, energy, obs, stats
 
 
+def _default_n_devices():
+    try:
+        import torch.distributed as dist
+        if dist.is_available() and dist.is_initialized():
+            return dist.get_world_size()
+    except Exception:
+        pass
+    return 1
+
+
 def run(walkers, n_steps, hamiltonian, step_size, guide, p_array, *, method="cont_time",
         rng_key=None, lam=None, **kwargs):
-    """Drop-in for ``pygfmc.run`` (engine/multi_gpu.py:822-868) on one B200.
+    """Drop-in for ``pygfmc.run`` (engine/multi_gpu.py:822-868): the run on
+    one GPU, or with ``n_devices > 1`` a population sharded over GPUs.
 
-    ``n_devices`` is accepted; this engine runs one GPU per process, so a
-    value above 1 raises (multi-GPU runs use one process per GPU)."""
+    ``n_devices`` (default: the world size of an initialised torch.distributed
+    group, else 1; PyGFMC's default is every visible device): with a process
+    group of that size, one shard per process (torchrun, one process per
+    GPU); otherwise the shards live in this process on ``cuda:0 ..
+    cuda:n_devices-1`` (``shard_devices=[...]`` names other devices, and may
+    repeat one to emulate the ranks on a single GPU).  The walker count must
+    be divisible by ``n_devices``.  Each process passes the whole population
+    and gets the whole final population back.  Unlike PyGFMC's sharded run,
+    the trajectory does not depend on the device count: every walker keeps
+    its global random stream and the resampling is global, so the sharded run
+    follows the one-GPU run (identical configurations, weights to rounding).
+    As in PyGFMC, runs with ``diag_operators`` stay on one device; so do runs
+    with ``off_diag_operators`` here (PyGFMC shards those)."""
     n_devices = kwargs.pop("n_devices", None)
-    if n_devices is not None:
-        n_devices = _validated_int("n_devices", n_devices, 1)
-        if n_devices > 1:
-            raise ValueError("pygfmc_b200.run drives one GPU per process; launch one process per "
-                             "GPU (torchrun) for more")
+    shard_devices = kwargs.pop("shard_devices", None)
+    n_devices = _default_n_devices() if n_devices is None else _validated_int("n_devices", n_devices, 1)
+    if shard_devices is not None and len(shard_devices) != n_devices:
+        raise ValueError(f"shard_devices names {len(shard_devices)} devices for n_devices={n_devices}")
+    if n_devices > 1 and (kwargs.get("diag_operators") or kwargs.get("off_diag_operators")):
+        _emit(f"[gfmc] - [run] - n_devices={n_devices} with measurement operators: running on one "
+              "device", kwargs.get("verbosity", 7), 1)
+        n_devices = 1
+    if n_devices > 1:
+        return run_gfmc(walkers, n_steps, hamiltonian, step_size, guide, p_array, method=method,
+                        rng_key=rng_key, lam=lam, _shards=(n_devices, shard_devices), **kwargs)
     return run_gfmc(walkers, n_steps, hamiltonian, step_size, guide, p_array, method=method,
                     rng_key=rng_key, lam=lam, **kwargs)
