@@ -15,12 +15,68 @@ __all__ = ["Walker", "prepare_walkers_random", "prepare_walkers_sz",
            "prepare_walkers_from_configs", "prepare_walkers_occupations"]
 
 
+def _compact_config(config):
+    """The smallest lossless storage of a configuration array: int8 when every
+    value is an integer in int8's range (+-1 spins, small occupations), the
+    array itself otherwise (walker.py _compact_config:31-47)."""
+    arr = np.asarray(config)
+    r = np.rint(arr)
+    if arr.size and np.array_equal(arr, r) and r.min() >= -128 and r.max() <= 127:
+        return r.astype(np.int8)
+    return arr
+
+
 class Walker(NamedTuple):
     """Population (or one walker): ``config`` (N_walkers, N_sites), ``log_weight``
     and ``e_loc`` (N_walkers,) -- walkers/walker.py Walker:50-64."""
     config: np.ndarray
     log_weight: np.ndarray
     e_loc: np.ndarray
+
+    def save(self, path, rng_key=None, group="walkers", **attrs):
+        """Checkpoint the walkers, the chain's key and scalar metadata
+        (walker.py Walker.save:66-103): datasets ``config`` (in the smallest
+        lossless dtype), ``log_weight``, ``e_loc`` and ``rng_key`` under
+        ``group``, the keyword arguments (typically ``avg_log_weight=``) as
+        attributes.  h5py is not available to this package, so the container
+        is a NumPy ``.npz`` archive holding the same names as
+        ``<group>/<dataset>`` and ``<group>/attrs/<name>``; the file is
+        written at ``path`` exactly.  Pass ``stats['parameters/rng_key_next']``
+        as ``rng_key``: with the walkers and ``avg_log_weight`` it is the whole
+        resume state."""
+        d = {f"{group}/config": _compact_config(self.config),
+             f"{group}/config_dtype": np.asarray(str(np.asarray(self.config).dtype)),
+             f"{group}/log_weight": np.asarray(self.log_weight),
+             f"{group}/e_loc": np.asarray(self.e_loc)}
+        if rng_key is not None:
+            d[f"{group}/rng_key"] = np.asarray(_rnd.as_key(rng_key), dtype=np.uint32)
+        for k, v in attrs.items():
+            if np.ndim(v) != 0:
+                raise ValueError(f"attribute {k!r} must be a scalar")
+            d[f"{group}/attrs/{k}"] = np.asarray(v)
+        with open(path, "wb") as f:
+            np.savez(f, **d)
+
+    @classmethod
+    def load(cls, path, group="walkers", dtype=None, config_dtype=None):
+        """Read a checkpoint written by :meth:`save` (walker.py
+        Walker.load:105-140): returns ``(walker, rng_key, avg_log_weight)``,
+        the last two None when not saved.  ``dtype`` (default float64, this
+        package's x64 mode) is the weights' and local energies' dtype,
+        ``config_dtype`` (default ``dtype``) the configurations'."""
+        dtype = np.dtype(np.float64 if dtype is None else dtype)
+        config_dtype = dtype if config_dtype is None else np.dtype(config_dtype)
+        with np.load(path, allow_pickle=False) as z:
+            if f"{group}/config" not in z.files:
+                raise KeyError(f"{path} holds no walker group {group!r}")
+            w = cls(config=np.asarray(z[f"{group}/config"], dtype=config_dtype),
+                    log_weight=np.asarray(z[f"{group}/log_weight"], dtype=dtype),
+                    e_loc=np.asarray(z[f"{group}/e_loc"], dtype=dtype))
+            key = np.asarray(z[f"{group}/rng_key"], dtype=np.uint32) \
+                if f"{group}/rng_key" in z.files else None
+            alw_k = f"{group}/attrs/avg_log_weight"
+            alw = dtype.type(z[alw_k]) if alw_k in z.files else None
+        return w, key, alw
 
 
 def _zeros(n, x64):
