@@ -16,8 +16,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-__all__ = ["SpinHalf", "BoseHubbard", "SzSzStructureFactor", "Lattice", "chain", "square",
-           "kagome", "edges_array"]
+__all__ = ["SpinHalf", "BoseHubbard", "StructureFactor", "SzSzStructureFactor", "Lattice", "chain",
+           "square", "kagome", "edges_array"]
 
 
 def edges_array(edges):
@@ -393,6 +393,73 @@ class BoseHubbard:
         x[a[idx]] += da[idx]
         x[b[idx]] += db[idx]
         return x
+
+
+# channel -> coefficients (a, b) of PM = S+S- + S-S+ and PP = S+S+ + S-S- per
+# pair; the diagonal channel has none
+_SF_CHANNEL_COEFFS = {"spsm": (1.0, 0.0), "spsp": (0.0, 1.0), "spsm+spsp": (1.0, 1.0), "szsz": None}
+
+
+def StructureFactor(positions, k, channel="SpSm", dtype=np.float32):
+    """The k-resolved pair correlator sum_{i<j} [1 + cos(k.(r_i - r_j))]
+    (A_i B_j + h.c.) as one SpinHalf measurement operator
+    (hamiltonian/SpinHalf.py StructureFactor:464-628): one transition slot per
+    pair with nonzero weight (weights below 1e-12 dropped), couplings
+    J_x = 2 (a + b) W, J_y = 2 (a - b) W for the channel's (a, b) on
+    (PM, PP), built without the propagator sign check (a measurement operator
+    needs rates >= 0).  Channels "SpSm", "SpSp", "SpSm+SpSp" are off-diagonal
+    (off_diag_operators); "SzSz" is the diagonal J_z = 2 W operator
+    (diag_operators) and warns that SzSzStructureFactor measures it for many
+    k at once.  The +1 shift keeps every weight non-negative; subtract the
+    k = 0 operator to remove it.  No periodic image is chosen: k must lie in
+    the reciprocal lattice of the simulation cell."""
+    import warnings
+    ch = str(channel).lower().replace(" ", "")
+    if ch not in _SF_CHANNEL_COEFFS:
+        hint = {"yy": " -- YY needs a negative PP coefficient: measure SpSm minus SpSp.",
+                "sysy": " -- YY needs a negative PP coefficient: measure SpSm minus SpSp.",
+                "zz": " -- the diagonal channel is spelled 'SzSz'.",
+                "sz": " -- the diagonal channel is spelled 'SzSz'.",
+                "ss": " -- S.S mixes the diagonal and off-diagonal paths: measure SpSm and SzSz "
+                      "separately and add.",
+                "s.s": " -- S.S mixes the diagonal and off-diagonal paths: measure SpSm and SzSz "
+                       "separately and add.",
+                "heisenberg": " -- S.S mixes the diagonal and off-diagonal paths: measure SpSm and "
+                              "SzSz separately and add."}.get(ch, "")
+        raise ValueError(f"channel={channel!r} is not reachable. The complete set is ['SpSm', "
+                         "'SpSp', 'SpSm+SpSp'], the non-negative cone over PM = S+S-+S-S+ and "
+                         f"PP = S+S++S-S-, plus the diagonal 'SzSz'{hint}")
+    r = np.asarray(positions, dtype=np.float64)
+    if r.ndim != 2:
+        raise ValueError(f"positions must be (N, d), got {r.shape}")
+    N = r.shape[0]
+    kv = np.asarray(k, dtype=np.float64)
+    if kv.ndim > 1 and kv.shape[0] != 1:
+        raise ValueError(f"k must be ONE wavevector (d,), got {kv.shape}; build one operator per "
+                         "wavevector.")
+    kv = kv.reshape(-1)
+    if kv.size != r.shape[1]:
+        raise ValueError(f"k has {kv.size} components but positions are {r.shape[1]}-dimensional; "
+                         "they must match.")
+    if N < 2:
+        raise ValueError(f"positions must hold at least two sites, got N={N}")
+    iu = np.triu_indices(N, k=1)
+    pairs = np.stack(iu, axis=1)
+    W = 1.0 + np.cos((r[iu[0]] - r[iu[1]]) @ kv)
+    keep = W > 1e-12
+    pairs, W = pairs[keep].astype(np.int32), W[keep]
+    if len(pairs) == 0:
+        raise ValueError("no pairs with nonzero weight -- every weight vanished, which means k maps "
+                         "every displacement to the zone boundary. Check k.")
+    if ch == "szsz":
+        warnings.warn("StructureFactor(channel='SzSz') is a DIAGONAL operator (M_total = 1): pass it "
+                      "in diag_operators. SzSzStructureFactor(positions, k_vectors) measures the same "
+                      "correlator for many k at once in O(N n_k), without the 1+cos shift and the "
+                      "k = 0 subtraction.", UserWarning, stacklevel=2)
+        return SpinHalf.create(pairs, J_z=2.0 * W, N=N, dtype=dtype, sign_check=False)
+    a, b = _SF_CHANNEL_COEFFS[ch]
+    return SpinHalf.create(pairs, J_x=2.0 * (a + b) * W, J_y=2.0 * (a - b) * W, J_z=0.0, N=N,
+                           dtype=dtype, sign_check=False)
 
 
 class SzSzStructureFactor:

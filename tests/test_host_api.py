@@ -296,3 +296,41 @@ def test_spinhalf_sign_checks_name_the_remedy():
     assert float(np.ravel(ok.J_pm)[0]) == pytest.approx(-0.35)
     meas = P.SpinHalf.create(edges, J_x=-0.3, J_y=-1.1, J_z=0.5, sign_check=False)
     assert float(np.ravel(meas.J_pmpm)[0]) == pytest.approx(0.2)
+
+
+def test_structure_factor_factory():
+    """hamiltonian/SpinHalf.py StructureFactor:464-628: one slot per pair of
+    nonzero weight 1 + cos(k.dr), J_x = 2 (a + b) W, J_y = 2 (a - b) W per
+    channel, the diagonal channel warns, unreachable channels are named."""
+    import warnings
+    L = 8
+    pos = np.arange(L, dtype=float)[:, None]
+    k = [np.pi / 2]
+    ops = {ch: P.hamiltonian.StructureFactor(pos, k, ch, dtype=np.float64)
+           for ch in ("SpSm", "SpSp", "spsm + spsp")}
+    iu = np.triu_indices(L, 1)
+    W = 1.0 + np.cos((pos[iu[0]] - pos[iu[1]]) @ np.asarray(k))
+    keep = W > 1e-12
+    assert len(ops["SpSm"].edge_i) == keep.sum() < len(W)        # cos = -1 pairs dropped
+    np.testing.assert_allclose(ops["SpSm"].J_pm, W[keep], rtol=1e-15)     # (J_x + J_y) / 4 = a W
+    np.testing.assert_allclose(ops["SpSm"].J_pmpm, 0.0, atol=0)
+    np.testing.assert_allclose(ops["SpSp"].J_pm, 0.0, atol=1e-15)
+    np.testing.assert_allclose(ops["SpSp"].J_pmpm, W[keep], rtol=1e-15)
+    np.testing.assert_allclose(ops["spsm + spsp"].J_pm, W[keep], rtol=1e-15)
+    np.testing.assert_allclose(ops["spsm + spsp"].J_pmpm, W[keep], rtol=1e-15)
+    assert ops["SpSm"].M_total == 1 + keep.sum()
+    # rates of a measurement operator are non-negative
+    x = P.prepare_walkers_random(1, L, P.PRNGKey(1)).config[0]
+    assert np.all(ops["spsm + spsp"].get_rates(x)[0][1:] >= 0)
+    with warnings.catch_warnings(record=True) as rec:
+        warnings.simplefilter("always")
+        zz = P.hamiltonian.StructureFactor(pos, k, "SzSz", dtype=np.float64)
+    assert any("DIAGONAL" in str(r.message) for r in rec) and zz.M_total == 1
+    np.testing.assert_allclose(zz.J_z, 2.0 * W[keep], rtol=1e-15)
+    for bad, msg in (("YY", "SpSm minus SpSp"), ("zz", "spelled 'SzSz'"), ("S.S", "separately")):
+        with pytest.raises(ValueError, match=msg):
+            P.hamiltonian.StructureFactor(pos, k, bad)
+    with pytest.raises(ValueError, match="ONE wavevector"):
+        P.hamiltonian.StructureFactor(pos, [[0.1], [0.2]])
+    with pytest.raises(ValueError, match="zone boundary"):
+        P.hamiltonian.StructureFactor(np.array([[0.0], [1.0]]), [np.pi])
