@@ -115,6 +115,7 @@ struct gfmc_handle {
   int rbm_on = 0;
   RbmTables rbm{};
   void *d_rbm = nullptr;
+  void *d_rbm_rt = nullptr, *d_rbm_ch = nullptr;   // the float32 RBM kernel's tables
   int rbm_grid = 0;
   int state_len = 0;     // carried state values per walker (N, or Hp for the RBM)
   // MLP guide (Bose-Hubbard, float32 build): bf16 layer weights, biases
@@ -168,7 +169,7 @@ uint16_t bf16_bits(float x) {
 // RBM tables: W rounded to bf16 in the site-major (N, Hp) and hidden-major
 // (Hp, N) layouts, b and a in float; the hidden axis padded with zeros to a
 // multiple of 256 (32 lanes x 8-element vector loads).
-int build_rbm(gfmc_handle *h, const gfmc_guide_desc *gd, int N) {
+int build_rbm(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_desc *gd, int N) {
   const int H = gd->n_hidden;
   if (H < 1 || H > 1024) return fail(GFMC_ERR_INVALID, "n_hidden must be in [1, 1024], got %d", H);
   if (!gd->rbm_W || !gd->rbm_b || !gd->rbm_a)
@@ -206,6 +207,66 @@ int build_rbm(gfmc_handle *h, const gfmc_guide_desc *gd, int N) {
   h->rbm.H = H;
   h->rbm.Hp = Hp;
   h->rbm.Np = Np;
+  // the float32 kernel's derived tables (tanh(2 W) rows and the lanes'
+  // log2 prod cosh(2 W)) and its slot chunks (rbm_f32.cu)
+  const int n_hx = md->n_hx, n_edges = md->n_jpm ? md->n_edges : 0;
+  const int M = 1 + n_hx + n_edges;
+  const int U = rbm_chunk_sites(Hp, N, M);
+  if (U < 2) return fail(GFMC_ERR_UNSUPPORTED, "RBM guide: %d moves exceed the shared memory of one SM", M - 1);
+  h->rbm.RS = Hp + 32;
+  GFMC_CUDA(cudaMalloc(&h->d_rbm_rt, sizeof(float) * (size_t)N * h->rbm.RS));
+  h->rbm.RT = (float *)h->d_rbm_rt;
+  std::vector<int> cstart, csites, cn;
+  std::vector<uint16_t> cpos;
+  rbm_build_chunks(N, n_hx, n_edges, md->edge_i, md->edge_j, U, cstart, csites, cn, cpos);
+  // slot records: sites, staged rows, couplings, scaled a terms
+  std::vector<int32_t> rec((size_t)8 * cpos.size(), 0);
+  auto fbits = [](double v) {
+    const float f = (float)v;
+    int32_t b;
+    memcpy(&b, &f, 4);
+    return b;
+  };
+  const double l2a = 2.0 * 1.4426950408889634;
+  for (size_t o = 0; o < cpos.size(); ++o) {
+    int32_t *R = rec.data() + 8 * o;
+    const int pi = cpos[o] & 255, pj = cpos[o] >> 8;
+    if ((int)o < n_hx) {
+      const double hx = md->hx_half ? md->hx_half[o] : 0.0;
+      R[0] = (int32_t)o | (pi << 16);
+      R[1] = 0xFFFF | (pi << 16);
+      R[2] = R[3] = fbits(hx);
+      R[4] = fbits(l2a * gd->rbm_a[o]);
+    } else {
+      const int e = (int)o - n_hx, i = md->edge_i[e], j = md->edge_j[e];
+      R[0] = i | (pi << 16);
+      R[1] = j | (pj << 16);
+      R[2] = fbits(md->jpm[e]);
+      R[3] = fbits(md->jpmpm[e]);
+      R[4] = fbits(l2a * gd->rbm_a[i]);
+      R[5] = fbits(l2a * gd->rbm_a[j]);
+    }
+  }
+  const size_t s1 = cstart.size() * 4, s2 = csites.size() * 4, s3 = cn.size() * 4,
+               s4 = rec.size() * 4;
+  const size_t p2 = al(s1), p3 = p2 + al(s2), p4 = p3 + al(s3), ctot = p4 + al(s4) + 256;
+  std::vector<unsigned char> ch(ctot, 0);
+  memcpy(ch.data(), cstart.data(), s1);
+  if (s2) memcpy(ch.data() + p2, csites.data(), s2);
+  if (s3) memcpy(ch.data() + p3, cn.data(), s3);
+  if (s4) memcpy(ch.data() + p4, rec.data(), s4);
+  GFMC_CUDA(cudaMalloc(&h->d_rbm_ch, ctot));
+  GFMC_CUDA(cudaMemcpy(h->d_rbm_ch, ch.data(), ctot, cudaMemcpyHostToDevice));
+  unsigned char *cb = (unsigned char *)h->d_rbm_ch;
+  h->rbm.ch_start = (const int *)cb;
+  h->rbm.ch_sites = (const int *)(cb + p2);
+  h->rbm.ch_n = (const int *)(cb + p3);
+  h->rbm.ch_rec = (int4 *)(cb + p4);
+  h->rbm.n_rec = (int)cpos.size();
+  h->rbm.n_chunks = (int)cn.size();
+  h->rbm.ch_U = U;
+  GFMC_CUDA(launch_rbm_derive(h->rbm, N, 0));
+  GFMC_CUDA(cudaDeviceSynchronize());
   h->rbm_on = 1;
   h->carry = 1;
   h->state_len = Hp;
@@ -290,7 +351,7 @@ cudaError_t launch_step(gfmc_handle *h, const DevModel<T> &m, const DevGuide<T> 
 
 // Per-block partial maxima of log_w a step launch over n walkers writes.
 int step_partials(const gfmc_handle *h, int n) {
-  if (h->rbm_on) return rbm_partials(h->rbm_grid, n);
+  if (h->rbm_on) return rbm_partials(h->rbm_grid, n, h->precision == GFMC_PRECISION_MIXED);
   if (h->mlp_on) return mlp_partials(h->mlp_grid, n);
   return evolve_partials(h->plan, n);
 }
@@ -699,7 +760,9 @@ int ensure_scratch(gfmc_handle *h, int n, int n_steps) {
   }
   if (!h->pmax) {
     size_t np = (size_t)(h->plan.grid > 0 ? h->plan.grid : 1) * (h->plan.wpb > 0 ? h->plan.wpb : 1);
-    if (h->rbm_on) np = std::max(np, (size_t)rbm_partials(h->rbm_grid, h->rbm_grid * 4));
+    if (h->rbm_on)
+      np = std::max(np, (size_t)rbm_partials(h->rbm_grid, h->rbm_grid * RBF_WARPS,
+                                             h->precision == GFMC_PRECISION_MIXED));
     if (h->mlp_on) np = std::max(np, (size_t)mlp_partials(h->mlp_grid, h->mlp_grid));
     GFMC_CUDA(cudaMalloc(&h->pmax, sizeof(double) * np));
   }
@@ -1202,7 +1265,7 @@ int gfmc_create(const gfmc_model_desc *model, const gfmc_guide_desc *guide, int 
   h->M = precision == GFMC_PRECISION_FP64 ? h->m64.M : h->m32.M;
   h->state_len = h->N;
   if (guide && guide->kind == GFMC_GUIDE_RBM_SPIN_HALF) {
-    rc = build_rbm(h, guide, h->N);
+    rc = build_rbm(h, model, guide, h->N);
     if (rc == GFMC_OK)
       h->rbm_grid = precision == GFMC_PRECISION_FP64 ? rbm_grid<double>(h->m64, h->rbm)
                                                      : rbm_grid<float>(h->m32, h->rbm);
@@ -1241,6 +1304,8 @@ int gfmc_destroy(gfmc_handle *h) {
   cudaFree(h->diag.ring_vals); cudaFree(h->diag_partial);
   cudaFree(h->fw_partial); cudaFree(h->fw_logG); cudaFree(h->fw_E); cudaFree(h->ctr1);
   cudaFree(h->d_rbm);
+  cudaFree(h->d_rbm_rt);
+  cudaFree(h->d_rbm_ch);
   cudaFree(h->d_mlp);
   cudaFree(h->mtr_cfg); cudaFree(h->mtr_rates); cudaFree(h->mtr_rsum); cudaFree(h->mtr_gw);
   cudaFree(h->mtr_e); cudaFree(h->mtr_coef); cudaFree(h->mtr_h1); cudaFree(h->mtr_h1T);
@@ -1592,6 +1657,7 @@ int gfmc_rbm_train_step(gfmc_handle *h, int n, const void *cfg, const int32_t *p
                               h->tr_ga, h->ad_m, h->ad_v, (float)lr, 0.9f, 0.999f, 1e-8f,
                               h->adam_step, (__nv_bfloat16 *)r.WT, (__nv_bfloat16 *)r.W,
                               (float *)r.b, (float *)r.a, s);
+  if (e == cudaSuccess) e = launch_rbm_derive(r, h->N, s);   // the float32 kernel's tables
   if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "Adam step: %s", cudaGetErrorString(e));
   // the guide changed: carried theta is stale
   h->field_valid = 0;

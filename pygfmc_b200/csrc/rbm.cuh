@@ -7,6 +7,8 @@
 #pragma once
 #include <cuda_bf16.h>
 
+#include <vector>
+
 #include "engine.cuh"
 
 namespace gfmc {
@@ -18,6 +20,21 @@ struct RbmTables {
   const float *b;            // (Hp,)
   const float *a;            // (N,)
   int H, Hp, Np;
+  // The float32 step kernel's tables (rbm_f32.cu), derived from WT:
+  // RT row i (RS = Hp + 32 floats) = tanh(2 W[h, i]) for every h, then per
+  // lane l the log2 of prod_{h in lane l} cosh(2 W[h, i]).
+  float *RT;
+  int RS;
+  // Slots in chunks whose flipped sites' RT rows are staged together:
+  // chunk c covers slots [ch_start[c], ch_start[c + 1]) and stages the rows
+  // ch_sites[c U .. c U + ch_n[c]).  Slot o's record is ch_rec[2 o],
+  // ch_rec[2 o + 1]: (i | row_i << 16, j | row_j << 16 (j = 0xFFFF and
+  // row_j = row_i for a site flip), the couplings for anti-parallel and
+  // parallel spins (float bits; a site flip's h_x / 2 twice)) and
+  // (2 log2(e) a_i, 2 log2(e) a_j (0 for a site flip), 0, 0).
+  const int *ch_start, *ch_sites, *ch_n;
+  int4 *ch_rec;
+  int n_chunks, ch_U, n_rec;
 };
 
 // Hidden units per lane of the step kernel's warp (Hp / 32).
@@ -29,10 +46,28 @@ inline int rbm_hpl(int Hp) { return Hp / 32; }
 template <typename T>
 cudaError_t launch_rbm_evolve(const DevModel<T> &m, const RbmTables &r, const EvolveArgs &a,
                               int grid, cudaStream_t s);
-// Grid (blocks of 128 threads) that keeps every SM busy for this model.
+// Grid (blocks) that keeps every SM busy for this model.
 template <typename T> int rbm_grid(const DevModel<T> &m, const RbmTables &r);
-// Per-warp partial maxima of log_w a launch over n_walkers writes.
-int rbm_partials(int grid, int n_walkers);
+// Per-warp partial maxima of log_w a launch over n walkers writes (f32: the
+// float32 kernel's blocks of 8 warps, else the float64 kernel's blocks of 4).
+int rbm_partials(int grid, int n_walkers, bool f32);
+
+// The float32 step kernel (rbm_f32.cu): the walkers of a block evaluate their
+// rates in lockstep over staged chunks of the derived tables.
+cudaError_t launch_rbm_evolve_f32(const DevModel<float> &m, const RbmTables &r,
+                                  const EvolveArgs &a, int grid, cudaStream_t s);
+int rbm_grid_f32(const DevModel<float> &m, const RbmTables &r);
+constexpr int RBF_WARPS = 8;   // warps (walkers) per block of the float32 kernel
+// Sites staged per chunk (at most 16) for the model's slot count, so that
+// two blocks fit on an SM; 0 when not even two sites fit.
+int rbm_chunk_sites(int Hp, int N, int M);
+// Host: greedy chunks of the off-diagonal slots (site flips first, then the
+// edges edge_i / edge_j), at most U sites each.
+void rbm_build_chunks(int N, int n_hx, int n_edges, const int *edge_i, const int *edge_j, int U,
+                      std::vector<int> &start, std::vector<int> &sites, std::vector<int> &nsites,
+                      std::vector<uint16_t> &pos);
+// RT from WT (after the guide's weights are written).
+cudaError_t launch_rbm_derive(const RbmTables &r, int N, cudaStream_t s);
 
 // theta (float32, (n, Hp)) of the packed spin configurations cfg[parents[w]]
 // (parents nullable) on the tensor cores (rbm_gemm.cu); status bit 8 when a
