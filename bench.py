@@ -601,7 +601,8 @@ def secondary_measurements(P, steps_scale=1.0):
     the MLP step on the 64-site Bose ring (320-256-256-1, 32768 walkers) with
     its training step, the Gutzwiller + density-Jastrow step on that ring,
     the kagome nearest-neighbour step (432 sites, 131072 walkers) and the
-    100-site chain (1024 walkers)."""
+    100-site chain (1024 walkers); then the short sigma study
+    (sigma_short)."""
     import torch
     dev = torch.device("cuda", torch.cuda.current_device())
     sampler = ClockSampler(gpu_uuid(torch, dev)).start()
@@ -632,7 +633,46 @@ def secondary_measurements(P, steps_scale=1.0):
         "heisenberg_chain100_nn_jastrow_cont_time")
     torch.cuda.synchronize()
     out["clocks"] = summarize_clocks(sampler.stop())
+    out["sigma_short"] = sigma_short(P, steps_scale)
     return out
+
+
+def sigma_short(P, steps_scale=1.0):
+    """A short version of the sigma study (--study sigma) on the 16x16
+    Heisenberg lattice: an RBM (H = 512) trained by variance minimisation for
+    150 iterations on 32768 walkers, then fixed-length productions of the
+    trained RBM (float32 build, 400 steps) and of the long-range Jastrow
+    guide (float64 build, 2000 steps), 32768 walkers each, tau = 0.05,
+    blocked jackknife (10 blocks) at p = 32; GPU seconds to sigma(E/N) = 1e-5
+    = production time x (sigma / 1e-5)^2.  Short runs: the ratio is an
+    estimate (the full study trains for 600 iterations and runs longer)."""
+    import torch
+    lat, H, GJ, _, _ = build_system(P, "fp64")
+    n = N_WALKERS
+    trained, hist = P.learn.train_rbm_guide(
+        P.prepare_walkers_sz(n, 256, P.PRNGKey(13), sz=0), H, P.RBMSpinHalf(256, 512, seed=0, sigma=0.01),
+        n_iterations=max(10, int(150 * steps_scale)), steps_per_iteration=3, step_size=TAU, lr=3e-4,
+        rng_key=P.PRNGKey(14), warmup_steps=100, verbosity=0)
+    res = {}
+    for key, G, steps, prec in (("rbm_h512_mixed", trained, max(40, int(400 * steps_scale)), "mixed"),
+                                ("jastrow_fp64", GJ, max(200, int(2000 * steps_scale)), "fp64")):
+        w = P.prepare_walkers_sz(n, 256, P.PRNGKey(11), sz=0)
+        torch.cuda.synchronize()
+        wf, _, _, st, raw = P.run(w, steps, H, TAU, G, [8, 32], rng_key=P.PRNGKey(12),
+                                  warmup_steps=200, verbosity=0, precision=prec)
+        Ej, err = P.estimators.jackknife_energy([32], raw["log_weights"], raw["energy"], 10)
+        sig = err[32] / 256
+        res[key] = {"E_per_site": Ej[32] / 256, "sigma_per_site": sig, "steps": steps,
+                    "production_gpu_s": st["runtime"],
+                    "gpu_s_to_1e-5": st["runtime"] * (sig / 1e-5) ** 2,
+                    "local_energy_var_per_site": float(np.var(wf.e_loc) / 256)}
+    r, j = res["rbm_h512_mixed"], res["jastrow_fp64"]
+    return {"workload": "heisenberg_16x16_rbm_h512_vs_longrange_jastrow", "n_walkers": n, "tau": TAU,
+            "p": 32, "jackknife_blocks": 10, "train_iterations": len(hist["variance"]),
+            "train_gpu_s": hist["seconds"], "methods": res,
+            "learned_over_jastrow_fp64_time_ratio": r["gpu_s_to_1e-5"] / j["gpu_s_to_1e-5"],
+            "energy_difference_in_sigma": abs(r["E_per_site"] - j["E_per_site"])
+            / float(np.hypot(r["sigma_per_site"], j["sigma_per_site"]))}
 
 
 def main():

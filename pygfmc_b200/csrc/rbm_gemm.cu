@@ -12,8 +12,12 @@
 // above 512 run in passes of 512 columns.  Every wait is bounded: a wait that
 // runs out sets GFMC status bit 8 and the CTA still frees its TMEM.
 //
-// Roofline: tensor bound at 2 * 128 * Hp * Np flops per CTA; bytes per
-// walker: Np / 8 of spins in, 4 Hp of theta out, W re-read from L2 per CTA.
+// Roofline: 2 Np Hp flops and 4 Hp bytes of theta written per walker: the
+// float32 output bounds it (HBM), the tensor work is half that time.  The
+// persistent kernel below (one CTA per SM, W resident per pass, A in a
+// two-stage ring, two TMEM accumulators) is the one launched whenever a
+// pass's W tile fits in shared memory; the one-CTA-per-tile kernel above
+// takes the rest.
 #include <cuda_bf16.h>
 
 #include "rbm.cuh"
@@ -143,10 +147,213 @@ rbm_theta_kernel(const uint64_t *cfg, const int *parents, int NW, int n, int Np,
 
 size_t theta_smem_bytes() { return 1024 + GT * 128 + MAXN * 128 + 16; }
 
+// ---------------------------------------------------------------------------
+// Persistent version: one CTA of 8 warps per SM.  The hidden axis runs in
+// passes of PW columns (256, or 128 / 64 when a pass's W tile would not fit);
+// the pass's W tile (PW rows x Np sites, bf16, K-chunks of 64 sites in the
+// 128-byte swizzled K-major layout) stays in shared memory while the CTA
+// walks its walker tiles (128 walkers each):
+//  * warps 0-3 (one walker row per thread) expand the spin words of each
+//    64-site chunk into a two-stage ring of A tiles (bf16 +-1);
+//  * thread 0 issues the chunk's four MMAs (K = 16 each, N = PW) into one of
+//    two TMEM accumulators and commits them to the ring stage's "free"
+//    mbarrier, and after a tile's last chunk to the accumulator's "full" one;
+//  * warps 4-7 (warp 4 + q reads TMEM lanes 32 q .. 32 q + 31) add b and
+//    write theta while the next tile accumulates in the other buffer.
+// Every wait is bounded (status bit 8); a wait that runs out stops every
+// role at its next wait, and the CTA frees its TMEM.
+constexpr int PT = 256;   // threads
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Bounded wait of one thread on completion `k` (parity k & 1); false (and
+// the CTA's abort flag set) when the limit ran out or another role aborted.
+__device__ __forceinline__ bool bwait(uint64_t *bar, uint32_t k, volatile int *abort_flag) {
+  for (uint32_t it = 0; it < WAIT_LIMIT; ++it) {
+    if (mbar_try_wait(bar, k & 1u)) return true;
+    if ((it & 1023u) == 0 && *abort_flag) return false;
+  }
+  *abort_flag = 1;
+  return false;
+}
+
+__global__ void __launch_bounds__(PT, 1)
+rbm_theta_persist(const uint64_t *cfg, const int *parents, int NW, int n, int Np,
+                  const __nv_bfloat16 *W, const float *b, int Hp, int PW, float *theta,
+                  int *status) {
+  extern __shared__ unsigned char dsm[];
+  unsigned char *base = (unsigned char *)(((uintptr_t)dsm + 1023) & ~(uintptr_t)1023);
+  const int nk = Np / KC;
+  unsigned char *Bt = base;                                   // nk x PW x 128 bytes
+  unsigned char *At = Bt + (size_t)nk * PW * 128;             // 2 stages x 128 x 128 bytes
+  uint64_t *bar = reinterpret_cast<uint64_t *>(At + 2 * GT * 128);
+  uint64_t *a_full = bar, *a_free = bar + 2, *acc_full = bar + 4, *acc_free = bar + 6;
+  uint32_t *slot = reinterpret_cast<uint32_t *>(bar + 8);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(slot + 1);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const uint32_t ncols = 2u * (uint32_t)PW;                   // two accumulators
+
+  if (warp == 0) tmem_alloc(slot, ncols);
+  if (tid == 0) {
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(a_full + i, GT);
+      mbar_init(a_free + i, 1);
+      mbar_init(acc_full + i, 1);
+      mbar_init(acc_free + i, GT);
+    }
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = *slot;
+  const uint32_t idesc = idesc_m128((uint32_t)PW);
+  const int n_tiles = (n + GT - 1) / GT;
+  uint32_t g = 0, T = 0;   // chunks and tiles this CTA has produced (over every pass)
+
+  for (int hb = 0; hb < Hp; hb += PW) {
+    // the pass's W tile: rows hb .. hb + PW - 1, every chunk
+    for (int idx = tid; idx < nk * PW; idx += PT) {
+      const int kc = idx / PW, r = idx - kc * PW;
+      const uint4 *srcw = reinterpret_cast<const uint4 *>(W + (size_t)(hb + r) * Np + (size_t)kc * KC);
+      unsigned char *tile = Bt + (size_t)kc * PW * 128;
+#pragma unroll
+      for (int c = 0; c < 8; ++c) *reinterpret_cast<uint4 *>(sw_chunk(tile, r, c)) = __ldg(srcw + c);
+    }
+    fence_async_smem();
+    __syncthreads();
+    const uint32_t g0 = g, T0 = T;
+    if (warp < 4) {
+      // ---- producers (and thread 0: the MMA issuer)
+      uint32_t gg = g0, TT = T0;
+      for (int t = blockIdx.x; t < n_tiles && !*abort_flag; t += gridDim.x, ++TT) {
+        const int w = t * GT + tid;
+        const int src = w < n ? (parents ? parents[w] : w) : 0;
+        const uint32_t buf = TT & 1u, use = TT >> 1;
+        for (int kc = 0; kc < nk; ++kc, ++gg) {
+          const uint32_t s = gg & 1u, u = gg >> 1;
+          if (u >= 1 && !bwait(a_free + s, u - 1, abort_flag)) break;
+          unsigned char *A = At + (size_t)s * GT * 128;
+          const uint64_t word = w < n && kc < NW ? cfg[(size_t)src * NW + kc] : 0ull;
+#pragma unroll
+          for (int c = 0; c < 8; ++c) {
+            uint32_t q[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const int k0 = 8 * c + 2 * e;
+              const uint32_t lo = ((word >> k0) & 1ull) ? 0x3F80u : 0xBF80u;
+              const uint32_t hi = ((word >> (k0 + 1)) & 1ull) ? 0x3F80u : 0xBF80u;
+              q[e] = w < n ? (lo | (hi << 16)) : 0u;
+            }
+            *reinterpret_cast<uint4 *>(sw_chunk(A, tid, c)) = make_uint4(q[0], q[1], q[2], q[3]);
+          }
+          fence_async_smem();
+          mbar_arrive(a_full + s);
+          if (tid == 0) {
+            if (!bwait(a_full + s, u, abort_flag)) break;
+            if (kc == 0 && use >= 1 && !bwait(acc_free + buf, use - 1, abort_flag)) break;
+            fence_after();
+            const uint32_t a0 = smem_u32(A);
+            const uint32_t b0 = smem_u32(Bt + (size_t)kc * PW * 128);
+            const uint32_t d = tmem + buf * (uint32_t)PW;
+#pragma unroll
+            for (int kk = 0; kk < KC / 16; ++kk)
+              mma_bf16(d, sw128_desc(a0 + 32u * kk), sw128_desc(b0 + 32u * kk), idesc,
+                       (kc > 0 || kk > 0) ? 1u : 0u);
+            mma_commit(a_free + s);
+            if (kc == nk - 1) mma_commit(acc_full + buf);
+          }
+        }
+      }
+    } else {
+      // ---- epilogue: theta = accumulator + b
+      const int q = warp - 4;
+      uint32_t TT = T0;
+      for (int t = blockIdx.x; t < n_tiles && !*abort_flag; t += gridDim.x, ++TT) {
+        const uint32_t buf = TT & 1u, use = TT >> 1;
+        if (!bwait(acc_full + buf, use, abort_flag)) break;
+        fence_after();
+        const int w = t * GT + 32 * q + (tid & 31);
+        for (int c0 = 0; c0 < PW; c0 += 32) {
+          uint32_t v[32];
+          tmem_ld32_async(tmem + ((uint32_t)(32 * q) << 16) + buf * (uint32_t)PW + (uint32_t)c0, v);
+          tmem_ld_wait(v);
+          if (w < n) {
+            float *out = theta + (size_t)w * Hp + hb + c0;
+            const float *bb = b + hb + c0;
+#pragma unroll
+            for (int i = 0; i < 32; i += 4)
+              *reinterpret_cast<float4 *>(out + i) =
+                  make_float4(__uint_as_float(v[i]) + bb[i], __uint_as_float(v[i + 1]) + bb[i + 1],
+                              __uint_as_float(v[i + 2]) + bb[i + 2],
+                              __uint_as_float(v[i + 3]) + bb[i + 3]);
+          }
+        }
+        fence_before();
+        mbar_arrive(acc_free + buf);
+      }
+    }
+    // tiles of this pass: the same count in every role
+    uint32_t my = 0;
+    for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) ++my;
+    g = g0 + my * (uint32_t)nk;
+    T = T0 + my;
+    fence_before();
+    __syncthreads();   // every role done with the pass before its W tile is replaced
+    fence_after();
+    if (*abort_flag) break;
+  }
+  if (*abort_flag) {
+    if (tid == 0) {
+      atomicOr(status, 8);
+      // the MMAs committed last: one more bounded wait before the TMEM is freed
+      if (T > 0)
+        for (uint32_t it = 0; it < WAIT_LIMIT; ++it)
+          if (mbar_try_wait(acc_full + ((T - 1) & 1u), ((T - 1) >> 1) & 1u)) break;
+    }
+  }
+  fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, ncols);
+}
+
+// Pass width of the persistent kernel for Np padded sites: the widest of
+// 256, 128, 64 columns whose W tile fits beside the A ring; 0 when none does.
+int theta_pass_width(int Np, int Hp) {
+  for (int pw = 256; pw >= 64; pw /= 2) {
+    if (Hp % pw) continue;
+    const size_t bytes = 1024 + (size_t)(Np / KC) * pw * 128 + 2 * GT * 128 + 128;
+    if (bytes <= (size_t)227 * 1024) return pw;
+  }
+  return 0;
+}
+
+size_t theta_persist_smem(int Np, int PW) {
+  return 1024 + (size_t)(Np / KC) * PW * 128 + 2 * GT * 128 + 128;
+}
+
 }  // namespace
 
 cudaError_t launch_rbm_theta(const RbmTables &r, int n, const void *cfg, const int *parents,
                              int NW, float *theta, int *status, cudaStream_t s) {
+  const int PW = theta_pass_width(r.Np, r.Hp);
+  if (PW > 0 && n > 0) {
+    const size_t smem = theta_persist_smem(r.Np, PW);
+    cudaError_t e = cudaFuncSetAttribute(rbm_theta_persist,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int tiles = (n + GT - 1) / GT;
+    const int grid = tiles < sms ? tiles : sms;
+    rbm_theta_persist<<<grid, PT, smem, s>>>(reinterpret_cast<const uint64_t *>(cfg), parents, NW,
+                                             n, r.Np, r.W, r.b, r.Hp, PW, theta, status);
+    return cudaGetLastError();
+  }
   const size_t smem = theta_smem_bytes();
   cudaError_t e = cudaFuncSetAttribute(rbm_theta_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
