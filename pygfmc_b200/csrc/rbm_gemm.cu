@@ -188,7 +188,9 @@ rbm_theta_persist(const uint64_t *cfg, const int *parents, int NW, int n, int Np
   const int nk = Np / KC;
   unsigned char *Bt = base;                                   // nk x PW x 128 bytes
   unsigned char *At = Bt + (size_t)nk * PW * 128;             // 2 stages x 128 x 128 bytes
-  uint64_t *bar = reinterpret_cast<uint64_t *>(At + 2 * GT * 128);
+  // epilogue staging: per epilogue warp a 32 x 32 float tile (rows padded to 33)
+  float *Et = reinterpret_cast<float *>(At + 2 * GT * 128);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(Et + 4 * 32 * 33);
   uint64_t *a_full = bar, *a_free = bar + 2, *acc_full = bar + 4, *acc_free = bar + 6;
   uint32_t *slot = reinterpret_cast<uint32_t *>(bar + 8);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(slot + 1);
@@ -233,11 +235,24 @@ rbm_theta_persist(const uint64_t *cfg, const int *parents, int NW, int n, int Np
         const int w = t * GT + tid;
         const int src = w < n ? (parents ? parents[w] : w) : 0;
         const uint32_t buf = TT & 1u, use = TT >> 1;
+        // the walker's spin words of up to 8 chunks at once (one load latency
+        // per tile instead of one per chunk)
+        uint64_t words[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+          words[k] = (w < n && k < NW && k < nk) ? cfg[(size_t)src * NW + k] : 0ull;
         for (int kc = 0; kc < nk; ++kc, ++gg) {
           const uint32_t s = gg & 1u, u = gg >> 1;
           if (u >= 1 && !bwait(a_free + s, u - 1, abort_flag)) break;
           unsigned char *A = At + (size_t)s * GT * 128;
-          const uint64_t word = w < n && kc < NW ? cfg[(size_t)src * NW + kc] : 0ull;
+          uint64_t word = 0ull;
+          if (kc < 8) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+              if (k == kc) word = words[k];
+          } else if (w < n && kc < NW) {
+            word = cfg[(size_t)src * NW + kc];
+          }
 #pragma unroll
           for (int c = 0; c < 8; ++c) {
             uint32_t q[4];
@@ -271,26 +286,35 @@ rbm_theta_persist(const uint64_t *cfg, const int *parents, int NW, int n, int Np
     } else {
       // ---- epilogue: theta = accumulator + b
       const int q = warp - 4;
+      // the pass's biases of this lane's column in each 32-column block
+      float bias[8];
+#pragma unroll
+      for (int cb = 0; cb < 8; ++cb)
+        bias[cb] = 32 * cb < PW ? b[hb + 32 * cb + (tid & 31)] : 0.0f;
       uint32_t TT = T0;
       for (int t = blockIdx.x; t < n_tiles && !*abort_flag; t += gridDim.x, ++TT) {
         const uint32_t buf = TT & 1u, use = TT >> 1;
         if (!bwait(acc_full + buf, use, abort_flag)) break;
         fence_after();
-        const int w = t * GT + 32 * q + (tid & 31);
-        for (int c0 = 0; c0 < PW; c0 += 32) {
+        // a 32 x 32 block (this warp's walkers x 32 columns) at a time: into
+        // the warp's staging tile by rows (one walker per lane), out by rows
+        // of the output (one column per lane: 128 contiguous bytes per store)
+        const int lane = tid & 31, w0 = t * GT + 32 * q;
+        float *E = Et + q * 32 * 33;
+#pragma unroll
+        for (int cb = 0; cb < 8; ++cb) {
+          const int c0 = 32 * cb;
+          if (c0 >= PW) break;
           uint32_t v[32];
           tmem_ld32_async(tmem + ((uint32_t)(32 * q) << 16) + buf * (uint32_t)PW + (uint32_t)c0, v);
           tmem_ld_wait(v);
-          if (w < n) {
-            float *out = theta + (size_t)w * Hp + hb + c0;
-            const float *bb = b + hb + c0;
 #pragma unroll
-            for (int i = 0; i < 32; i += 4)
-              *reinterpret_cast<float4 *>(out + i) =
-                  make_float4(__uint_as_float(v[i]) + bb[i], __uint_as_float(v[i + 1]) + bb[i + 1],
-                              __uint_as_float(v[i + 2]) + bb[i + 2],
-                              __uint_as_float(v[i + 3]) + bb[i + 3]);
-          }
+          for (int i = 0; i < 32; ++i) E[lane * 33 + i] = __uint_as_float(v[i]);
+          __syncwarp();
+          const float bb = bias[cb];
+          for (int rr = 0; rr < 32; ++rr)
+            if (w0 + rr < n) theta[(size_t)(w0 + rr) * Hp + hb + c0 + lane] = E[rr * 33 + lane] + bb;
+          __syncwarp();
         }
         fence_before();
         mbar_arrive(acc_free + buf);
@@ -325,14 +349,14 @@ rbm_theta_persist(const uint64_t *cfg, const int *parents, int NW, int n, int Np
 int theta_pass_width(int Np, int Hp) {
   for (int pw = 256; pw >= 64; pw /= 2) {
     if (Hp % pw) continue;
-    const size_t bytes = 1024 + (size_t)(Np / KC) * pw * 128 + 2 * GT * 128 + 128;
+    const size_t bytes = 1024 + (size_t)(Np / KC) * pw * 128 + 2 * GT * 128 + 4 * 32 * 33 * 4 + 128;
     if (bytes <= (size_t)227 * 1024) return pw;
   }
   return 0;
 }
 
 size_t theta_persist_smem(int Np, int PW) {
-  return 1024 + (size_t)(Np / KC) * PW * 128 + 2 * GT * 128 + 128;
+  return 1024 + (size_t)(Np / KC) * PW * 128 + 2 * GT * 128 + 4 * 32 * 33 * 4 + 128;
 }
 
 }  // namespace
@@ -342,12 +366,20 @@ cudaError_t launch_rbm_theta(const RbmTables &r, int n, const void *cfg, const i
   const int PW = theta_pass_width(r.Np, r.Hp);
   if (PW > 0 && n > 0) {
     const size_t smem = theta_persist_smem(r.Np, PW);
-    cudaError_t e = cudaFuncSetAttribute(rbm_theta_persist,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // the kernel's shared-memory limit (its largest size) and the SM count,
+    // once per device
+    static int sms_of[64] = {0};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    int dev = 0, sms = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int sms = (dev >= 0 && dev < 64) ? sms_of[dev] : 0;
+    if (sms == 0) {
+      e = cudaFuncSetAttribute(rbm_theta_persist, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               227 * 1024);
+      if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      if (e != cudaSuccess) return e;
+      if (dev >= 0 && dev < 64) sms_of[dev] = sms;
+    }
     const int tiles = (n + GT - 1) / GT;
     const int grid = tiles < sms ? tiles : sms;
     rbm_theta_persist<<<grid, PT, smem, s>>>(reinterpret_cast<const uint64_t *>(cfg), parents, NW,
