@@ -41,6 +41,7 @@ extern "C" {
 #define GFMC_GUIDE_JASTROW_BOSE_HUBBARD 2
 #define GFMC_GUIDE_RBM_SPIN_HALF 3        /* no counterpart in PyGFMC */
 #define GFMC_GUIDE_MLP_BOSE_HUBBARD 4     /* no counterpart in PyGFMC */
+#define GFMC_GUIDE_EXACT_SPIN_HALF 5      /* ExactGroundState on a SpinHalf model */
 
 #define GFMC_METHOD_CONT_TIME 0
 #define GFMC_METHOD_SINGLE_STEP 1
@@ -109,6 +110,14 @@ typedef struct {
   int mlp_H1, mlp_H2;
   const float *mlp_W1, *mlp_b1, *mlp_W2, *mlp_b2, *mlp_w3;
   double mlp_b3;
+  /* ExactGroundState (GFMC_GUIDE_EXACT_SPIN_HALF; wavefunction/
+   * exact_ground_state.py:43-190): psi_T(x) = exp(exact_log_amp[idx(x)]) with
+   * idx(x) = sum_i b_i 2^(N-1-i), b_i = 1 for x_i = -1 (site 0 most
+   * significant; the positional index over SpinHalf.local_hilbert_space
+   * (1, -1)); exact_log_amp has 2^exact_n_sites entries, exact_n_sites = the
+   * model's N <= 26.  Nodes carry a large negative log amplitude, not -inf. */
+  int exact_n_sites;
+  const double *exact_log_amp;
 } gfmc_guide_desc;
 
 typedef struct gfmc_handle gfmc_handle;

@@ -106,6 +106,10 @@ typedef struct {
   int mlp_H1, mlp_H2, mlp_np1;
   const double *mlp_W1, *mlp_b1, *mlp_W2, *mlp_b2, *mlp_w3;
   double mlp_b3;
+  /* ExactGroundState (wavefunction/exact_ground_state.py:43-190) on spin-1/2:
+   * log |psi_0| over the 2^N basis states, indexed over the digits of
+   * SpinHalf.local_hilbert_space (1, -1) with site 0 most significant. */
+  int exact_N; const double *log_amp;
 } om_guide;
 
 /* Extra scratch doubles om_rates needs for a guide (theta and theta'). */
@@ -289,6 +293,13 @@ static void jbh_log_diff(const om_guide *g, const om_model *m, const double *n,
   }
 }
 
+/* ExactGroundState.basis_index:141-147: digit 1 for a down spin (x = -1). */
+static long exact_index(const double *x, int N) {
+  long idx = 0;
+  for (int i = 0; i < N; ++i) idx = 2 * idx + (x[i] < 0.0 ? 1 : 0);
+  return idx;
+}
+
 /* evolution.transition_rates:205-261 (guide ratio folded in, masked zeros) */
 static void om_rates(const om_model *m, const om_guide *g, const double *x,
                      double *r, double *scratch) {
@@ -304,6 +315,19 @@ static void om_rates(const om_model *m, const om_guide *g, const double *x,
       for (int e = 0; e < m->n_jpm; ++e) {
         double *re = &r[1 + m->n_hx + e];
         if (*re != 0.0) *re *= exp(jsh_edge_ld(g, m, x, e));
+      }
+    } else if (g && g->kind == 5) {
+      /* log_diff_from_configs:150-190: the successor of a flip differs from x
+       * in the flipped sites' digits */
+      const int N = m->N;
+      const long ix = exact_index(x, N);
+      const double l0 = g->log_amp[ix];
+      for (int k = 0; k < m->n_hx; ++k)
+        if (r[1 + k] != 0.0) r[1 + k] *= exp(g->log_amp[ix ^ (1L << (N - 1 - k))] - l0);
+      for (int e = 0; e < m->n_jpm; ++e) {
+        double *re = &r[1 + m->n_hx + e];
+        const long fl = (1L << (N - 1 - m->ei[e])) ^ (1L << (N - 1 - m->ej[e]));
+        if (*re != 0.0) *re *= exp(g->log_amp[ix ^ fl] - l0);
       }
     } else if (g && g->kind == 3) {
       double *theta = scratch + M;   /* om_guide_scratch doubles past the M-slot area */

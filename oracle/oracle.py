@@ -65,7 +65,7 @@ class _Guide(ctypes.Structure):
                 ("n_hidden", ctypes.c_int), ("rbm_W", _dp), ("rbm_b", _dp), ("rbm_a", _dp),
                 ("mlp_H1", ctypes.c_int), ("mlp_H2", ctypes.c_int), ("mlp_np1", ctypes.c_int),
                 ("mlp_W1", _dp), ("mlp_b1", _dp), ("mlp_W2", _dp), ("mlp_b2", _dp), ("mlp_w3", _dp),
-                ("mlp_b3", ctypes.c_double)]
+                ("mlp_b3", ctypes.c_double), ("exact_N", ctypes.c_int), ("log_amp", _dp)]
 
 
 def build():
@@ -407,6 +407,30 @@ def mlp_bose_hubbard(W1, b1, W2, b2, w3, b3, n_max):
     s.mlp_W1 = _p(g._arr(W1.ravel())); s.mlp_b1 = _p(g._arr(b1))
     s.mlp_W2 = _p(g._arr(W2.ravel())); s.mlp_b2 = _p(g._arr(b2)); s.mlp_w3 = _p(g._arr(w3))
     s.mlp_b3 = float(b3)
+    g.s = s
+    return g
+
+
+def exact_spin_half(log_amp, local_hilbert_space=(1.0, -1.0)):
+    """ExactGroundState on spin-1/2 (wavefunction/exact_ground_state.py:
+    43-190): log |psi_0| over the 2^N positional basis states of
+    local_hilbert_space (site 0 most significant), float64.  The C side
+    indexes over (1, -1), so a table over (-1, 1) is stored reversed (the
+    complementary index)."""
+    la = np.asarray(log_amp, np.float64).ravel()
+    N = int(la.size).bit_length() - 1
+    if la.size != 2 ** N:
+        raise ValueError(f"log_amp has {la.size} entries, not a power of two")
+    vals = tuple(float(v) for v in local_hilbert_space)
+    if vals == (-1.0, 1.0):
+        la = la[::-1]
+    elif vals != (1.0, -1.0):
+        raise ValueError(f"spin-1/2 local space expected, got {vals}")
+    g = OracleModel()
+    s = _Guide()
+    s.kind = 5
+    s.exact_N = N
+    s.log_amp = _p(g._arr(la))
     g.s = s
     return g
 

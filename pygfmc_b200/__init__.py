@@ -9,16 +9,18 @@ from . import diagnostics, hamiltonian, learn, random, walkers, wavefunction
 from .diagnostics import statistics
 from .engine import GFMCEngine, run, run_gfmc
 from .estimators import evaluate_observables
-from .hamiltonian import BoseHubbard, SpinHalf, chain, kagome, square
+from .hamiltonian import BoseHubbard, SpinHalf, chain, exact_diagonalization, kagome, square
 from .random import PRNGKey
 from .walkers import (Walker, prepare_walkers_from_configs, prepare_walkers_occupations,
                       prepare_walkers_random, prepare_walkers_sz)
-from .wavefunction import JastrowBoseHubbard, JastrowSpinHalf, MLPBoseHubbard, RBMSpinHalf
+from .wavefunction import (ExactGroundState, JastrowBoseHubbard, JastrowSpinHalf, MLPBoseHubbard,
+                           RBMSpinHalf)
 
 __version__ = "0.1.0"
 
 __all__ = ["run", "run_gfmc", "statistics", "GFMCEngine", "evaluate_observables", "SpinHalf", "BoseHubbard",
            "chain", "square", "kagome", "PRNGKey", "Walker", "prepare_walkers_random",
            "prepare_walkers_sz", "prepare_walkers_from_configs", "prepare_walkers_occupations",
-           "JastrowSpinHalf", "JastrowBoseHubbard", "RBMSpinHalf", "MLPBoseHubbard", "hamiltonian", "random", "walkers",
+           "JastrowSpinHalf", "JastrowBoseHubbard", "RBMSpinHalf", "MLPBoseHubbard", "ExactGroundState",
+           "exact_diagonalization", "hamiltonian", "random", "walkers",
            "wavefunction", "__version__"]

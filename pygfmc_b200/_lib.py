@@ -24,6 +24,7 @@ GUIDE_JASTROW_SPIN_HALF = 1
 GUIDE_JASTROW_BOSE_HUBBARD = 2
 GUIDE_RBM_SPIN_HALF = 3
 GUIDE_MLP_BOSE_HUBBARD = 4
+GUIDE_EXACT_SPIN_HALF = 5
 METHODS = {"cont_time": 0, "single_step": 1, "multi_step": 2}
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
@@ -59,7 +60,8 @@ class GuideDesc(ctypes.Structure):
                 ("n_hidden", ctypes.c_int), ("rbm_W", _fp), ("rbm_b", _fp), ("rbm_a", _fp),
                 ("mlp_H1", ctypes.c_int), ("mlp_H2", ctypes.c_int), ("mlp_W1", _fp),
                 ("mlp_b1", _fp), ("mlp_W2", _fp), ("mlp_b2", _fp), ("mlp_w3", _fp),
-                ("mlp_b3", ctypes.c_double)]
+                ("mlp_b3", ctypes.c_double),
+                ("exact_n_sites", ctypes.c_int), ("exact_log_amp", _dp)]
 
 
 class DiagDesc(ctypes.Structure):

@@ -458,14 +458,25 @@ int build_tables(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_des
     return fail(GFMC_ERR_INVALID, "JastrowSpinHalf needs the SpinHalf transition layout");
   if (gk == GFMC_GUIDE_JASTROW_BOSE_HUBBARD && md->kind != GFMC_MODEL_BOSE_HUBBARD)
     return fail(GFMC_ERR_INVALID, "JastrowBoseHubbard needs a BoseHubbard operator");
+  if (gk == GFMC_GUIDE_EXACT_SPIN_HALF) {
+    if (md->kind != GFMC_MODEL_SPIN_HALF)
+      return fail(GFMC_ERR_INVALID, "the exact-amplitude guide needs a SpinHalf model");
+    if (gd->exact_n_sites != N || N < 1 || N > 26 || !gd->exact_log_amp)
+      return fail(GFMC_ERR_INVALID, "exact-amplitude guide over %d sites (2^N amplitudes) for a "
+                  "model of %d sites (N <= 26)", gd->exact_n_sites, N);
+  }
   if (gk != GFMC_GUIDE_NONE && gk != GFMC_GUIDE_JASTROW_SPIN_HALF &&
-      gk != GFMC_GUIDE_JASTROW_BOSE_HUBBARD)
+      gk != GFMC_GUIDE_JASTROW_BOSE_HUBBARD && gk != GFMC_GUIDE_EXACT_SPIN_HALF)
     return fail(GFMC_ERR_UNSUPPORTED, "unknown guide kind %d", gk);
   g.kind = gk;
+  const bool jastrow = gk == GFMC_GUIDE_JASTROW_SPIN_HALF || gk == GFMC_GUIDE_JASTROW_BOSE_HUBBARD;
+  // exact amplitudes: one table of log |psi_0| in the build's precision, no
+  // carried state (the ratio needs nothing but the configuration)
+  if (gk == GFMC_GUIDE_EXACT_SPIN_HALF) put("lamp", gd->exact_log_amp, (size_t)1 << N);
   size_t o_jdig = 0, o_slq = 0, o_sit = 0;
   size_t o_nbr = 0, o_nbrw = 0, o_cnt = 0, o_tpw = 0, o_jd = 0, o_ep = 0, o_em = 0, o_tep = 0,
            o_xy = 0;
-  if (gk != GFMC_GUIDE_NONE) {
+  if (jastrow) {
     // per-site partner lists, duplicates merged (each partner once per site)
     std::vector<std::map<int, double>> lists(N);
     for (int p = 0; p < gd->n_pairs; ++p) {
@@ -679,7 +690,8 @@ int build_tables(gfmc_handle *h, const gfmc_model_desc *md, const gfmc_guide_des
   m.hx_half = ptr("hx_half");
   m.t = ptr("t"); m.eta = ptr("eta"); m.U = ptr("U"); m.mu = ptr("mu"); m.hpm = ptr("hpm");
   m.sqrt_tab = ptr("sqrt");
-  if (gk != GFMC_GUIDE_NONE) {
+  g.lamp = ptr("lamp");
+  if (jastrow) {
     g.nbr = (const uint32_t *)(base + o_nbr);
     g.nbr_w = (const T *)(base + o_nbrw);
     g.nbr_cnt = (const int *)(base + o_cnt);

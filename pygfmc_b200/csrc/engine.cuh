@@ -10,7 +10,10 @@ namespace gfmc {
 
 enum Family { SPIN_HALF = 0, BOSE_HUBBARD = 1 };
 enum Method { CONT_TIME = 0, SINGLE_STEP = 1, MULTI_STEP = 2, EVALUATE = 3, APPLY = 4, MIN_RATE = 5 };
-enum GuideKind { GUIDE_NONE = 0, GUIDE_JASTROW_SPIN = 1, GUIDE_JASTROW_BOSE = 2, GUIDE_RBM_SPIN = 3 };
+enum GuideKind {
+  GUIDE_NONE = 0, GUIDE_JASTROW_SPIN = 1, GUIDE_JASTROW_BOSE = 2, GUIDE_RBM_SPIN = 3,
+  GUIDE_EXACT_SPIN = 5
+};
 
 // Status bits the kernels raise (atomicOr into a device word).
 enum StatusBits {
@@ -93,6 +96,10 @@ template <typename T> struct DevGuide {
   int ti, Lx, Ly, tE_off;
   const T *tE;
   const int *tq;
+  // exact amplitudes (GUIDE_EXACT_SPIN): log |psi_0| over the 2^N basis
+  // states, indexed by the configuration's bits with site 0 most
+  // significant; the walker's factors are then the plain spins x_k
+  const T *lamp;
   int dense;              // couplings as a dense symmetric (N, N) matrix Jd
   const T *Jd;            // (N, N) row-major, zero diagonal (dense == 1)
   // Jd as jdig_d balanced base-128 int8 digits for the population product

@@ -147,6 +147,23 @@ template <typename T> __device__ __forceinline__ T spin_x(const uint64_t *bits, 
   return ((bits[k >> 6] >> (k & 63)) & 1ull) ? T(1) : T(-1);
 }
 
+// Basis index of a spin-1/2 walker under the exact-amplitude guide
+// (ExactGroundState.basis_index, wavefunction/exact_ground_state.py:141-147,
+// digits over SpinHalf.local_hilbert_space (1, -1)): bit N-1-k is set for a
+// down spin at site k.  S holds the plain spins; N <= 26, one site per lane.
+template <typename T>
+__device__ __forceinline__ int exact_index(int N, const T *S, int lane) {
+  const unsigned down = __ballot_sync(FULL, lane < N && S[lane < N ? lane : 0] < T(0));
+  return (int)(__brev(down) >> (32 - N));
+}
+
+// psi(y) / psi(x) under the exact-amplitude guide, y = x with the index bits
+// `flip` toggled: exp(log_amp[y] - log_amp[x]) (log_diff_from_configs:150-190).
+template <typename T>
+__device__ __forceinline__ T exact_ratio(const DevGuide<T> &g, int gx, int flip) {
+  return math_exp(g.lamp[gx ^ flip] - g.lamp[gx]);
+}
+
 template <typename T, int FAM>
 __device__ __forceinline__ T site_val(const uint64_t *bits, const uint8_t *occ, int k) {
   if (FAM == SPIN_HALF) return spin_x<T>(bits, k);
@@ -213,7 +230,7 @@ __device__ __forceinline__ void field_init(const DevModel<T> &m, const DevGuide<
 template <typename T>
 __device__ __forceinline__ void signed_init(const DevModel<T> &m, const DevGuide<T> &g,
                                             const uint64_t *bits, T *S, int lane) {
-  if (g.kind == GUIDE_NONE) {
+  if (g.kind != GUIDE_JASTROW_SPIN) {   // no guide, or exact amplitudes: the spins
     for (int k = lane; k < m.N; k += 32) S[k] = spin_x<T>(bits, k);
     __syncwarp();
     return;
@@ -233,7 +250,7 @@ template <typename T>
 __device__ __forceinline__ void flip_one(const DevModel<T> &m, const DevGuide<T> &g, T *S, int a,
                                          int lane) {
   const T sa = S[a];
-  if (g.kind != GUIDE_NONE) {
+  if (g.kind == GUIDE_JASTROW_SPIN) {
     const bool ua = sa > T(0);
     if (g.ti) {
       const int ca = g.tE_off - g.tq[a];
@@ -271,7 +288,7 @@ __device__ __forceinline__ void flip_one(const DevModel<T> &m, const DevGuide<T>
 template <typename T>
 __device__ __forceinline__ void flip_pair(const DevModel<T> &m, const DevGuide<T> &g, T *S, int a,
                                           int b, int lane) {
-  if (g.kind == GUIDE_NONE || !g.dense) {
+  if (g.kind != GUIDE_JASTROW_SPIN || !g.dense) {
     flip_one(m, g, S, a, lane);
     flip_one(m, g, S, b, lane);
     return;
@@ -371,17 +388,31 @@ __device__ __forceinline__ void apply_move(const DevModel<T> &m, const DevGuide<
   }
 }
 
+// The walker's basis index when the exact-amplitude guide is on (general
+// spin layout; a warp-uniform branch), else 0.
+template <typename T, int FAM, int FAST>
+__device__ __forceinline__ int exact_gx(const DevModel<T> &m, const DevGuide<T> &g, const T *SF,
+                                        int lane) {
+  if (FAST || FAM != SPIN_HALF || g.kind != GUIDE_EXACT_SPIN) return 0;
+  return exact_index(m.N, SF, lane);
+}
+
 // Off-diagonal element of move o (<= 0 for a sign-free model) with the
 // guide ratio folded in (evolution.transition_rates:255-260).  Spin-1/2: a
 // site flip costs -h_x/2 A_k = hx_half |s_k|; an edge flip the coupling of
 // its spin alignment times A_i A_j c_e = |s_i s_j| c_e (c_e = exp(4 Jsum_e
 // x_i x_j), the pair's own term).  *anti: the edge's spins are anti-parallel.
+// Under the exact-amplitude guide (general layout only) the ratio is
+// exact_ratio at the walker's basis index gx; zero elements stay zero
+// without looking the ratio up (transition_rates:252-260).
 template <typename T, int FAM, int FAST>
 __device__ __forceinline__ T offdiag(const DevModel<T> &m, const DevGuide<T> &g,
-                                     const uint8_t *occ, const T *SF, int o, int *anti_out) {
+                                     const uint8_t *occ, const T *SF, int o, int *anti_out,
+                                     int gx) {
   if (FAM == SPIN_HALF) {
     if (!FAST && o < m.n_hx) {
       const T v = m.hx_half[o];
+      if (v != T(0) && g.kind == GUIDE_EXACT_SPIN) return v * exact_ratio(g, gx, 1 << (m.N - 1 - o));
       return v != T(0) ? v * fabs(SF[o]) : v;
     }
     const int e = FAST ? o : o - m.n_hx;
@@ -395,6 +426,11 @@ __device__ __forceinline__ T offdiag(const DevModel<T> &m, const DevGuide<T> &g,
     if (FAST == 1) return (-m.k_anti) * math_min(p, T(0));
     if (FAST == 2) return (anti ? -m.k_anti : m.k_par) * p;
     const T b = m.uniform_pm ? (anti ? m.jpm0 : m.jpmpm0) : (anti ? m.jpm[e] : m.jpmpm[e]);
+    if (g.kind == GUIDE_EXACT_SPIN) {
+      if (b == T(0)) return b;
+      const int i = (int)(pe & 0xFFFF), j = (int)(pe >> 16);
+      return b * exact_ratio(g, gx, (1 << (m.N - 1 - i)) ^ (1 << (m.N - 1 - j)));
+    }
     if (g.kind != GUIDE_NONE && b != T(0)) {
       const T c = g.uniform_c ? (anti ? g.c_anti0 : g.c_par0) : (anti ? g.c_anti[e] : g.c_par[e]);
       return b * fabs(p) * c;
@@ -434,6 +470,7 @@ __device__ __forceinline__ Eval<T> evaluate(const DevModel<T> &m, const DevGuide
   ev.C = C;
   const bool spin = FAM == SPIN_HALF;
   const bool fused_diag = spin && m.has_jz && m.n_jpm == m.E && m.E > 0;
+  const int gx = exact_gx<T, FAM, FAST>(m, g, SF, lane);
   int na = 0;
   T jzs = T(0);
   T acc = T(0);
@@ -445,7 +482,7 @@ __device__ __forceinline__ Eval<T> evaluate(const DevModel<T> &m, const DevGuide
     const int o = lamform ? s0 + j - 1 : s0 + j;
     if (!lamform || o >= 0) {
       int anti = -1;
-      const T v = offdiag<T, FAM, FAST>(m, g, occ, SF, o, &anti);
+      const T v = offdiag<T, FAM, FAST>(m, g, occ, SF, o, &anti, gx);
       if (fused_diag && anti >= 0) {
         if (FAST || m.uniform_jz) na += anti;
         else jzs += anti ? -m.jz[o - m.n_hx] / T(4) : m.jz[o - m.n_hx] / T(4);
@@ -498,11 +535,11 @@ __device__ __forceinline__ Eval<T> evaluate(const DevModel<T> &m, const DevGuide
 // Scanned value and weight of slot s (valid slots only).
 template <typename T, int FAM, int FAST>
 __device__ __forceinline__ T slot_q(const DevModel<T> &m, const DevGuide<T> &g, const uint8_t *occ,
-                                    const T *SF, int s, int mode, T diag) {
+                                    const T *SF, int s, int mode, T diag, int gx) {
   const bool lamform = mode != MODE_OFF;
   if (lamform && s == 0) return diag;
   int anti;
-  const T v = offdiag<T, FAM, FAST>(m, g, occ, SF, lamform ? s - 1 : s, &anti);
+  const T v = offdiag<T, FAM, FAST>(m, g, occ, SF, lamform ? s - 1 : s, &anti, gx);
   return lamform ? v : -v;
 }
 
@@ -526,13 +563,14 @@ __device__ __forceinline__ int sample_slot(const DevModel<T> &m, const DevGuide<
   const int C = ev.C;
   const int last_lane = (n_slots - 1) / C;
   const bool lamc = mode == MODE_LAM;   // cdf = lam - cumsum
+  const int gx = exact_gx<T, FAM, FAST>(m, g, SF, lane);
   const T cend = lamc ? lam - ev.end : ev.end;
   const unsigned bal = __ballot_sync(FULL, lane <= last_lane && cend > u);
   const int L = bal ? __ffs(bal) - 1 : last_lane;
   const T exclL = __shfl_sync(FULL, ev.excl, L);
   int s = L * C + lane;
   bool valid = lane < C && s < n_slots;
-  T qv = valid ? slot_q<T, FAM, FAST>(m, g, occ, SF, s, mode, ev.diag) : T(0);
+  T qv = valid ? slot_q<T, FAM, FAST>(m, g, occ, SF, s, mode, ev.diag, gx) : T(0);
   const T pre = warp_inclusive_scan(qv, lane);
   const T c = lamc ? lam - (exclL + pre) : exclL + pre;
   const unsigned hit = __ballot_sync(FULL, valid && c > u);
@@ -544,7 +582,7 @@ __device__ __forceinline__ int sample_slot(const DevModel<T> &m, const DevGuide<
   for (int L2 = L - 1; L2 >= 0; --L2) {
     s = L2 * C + lane;
     valid = lane < C && s < n_slots;
-    qv = valid ? slot_q<T, FAM, FAST>(m, g, occ, SF, s, mode, ev.diag) : T(0);
+    qv = valid ? slot_q<T, FAM, FAST>(m, g, occ, SF, s, mode, ev.diag, gx) : T(0);
     w = slot_w(mode, s, qv, lam);
     bk = __ballot_sync(FULL, valid && w > T(0));
     if (bk) return L2 * C + 31 - __clz(bk);
@@ -788,9 +826,10 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta
       const Eval<T> ev = evaluate<T, FAM, FAST>(m, g, occ, SF, m.M, MODE_POS, lane);
       T mn = ev.diag;
       bool bad = !isfinite(ev.diag);
+      const int gx = exact_gx<T, FAM, FAST>(m, g, SF, lane);
       for (int o = lane; o < m.n_off; o += 32) {
         int anti;
-        const T v = offdiag<T, FAM, FAST>(m, g, occ, SF, o, &anti);
+        const T v = offdiag<T, FAM, FAST>(m, g, occ, SF, o, &anti, gx);
         mn = v < mn ? v : mn;
         bad = bad || !isfinite(v);
       }
@@ -842,10 +881,11 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta
 
 template <typename T>
 void staging_plan(const DevModel<T> &m, const DevGuide<T> &g, int *stage_nbr, size_t *cta) {
+  const bool jastrow = g.kind == GUIDE_JASTROW_SPIN || g.kind == GUIDE_JASTROW_BOSE;
   size_t nbr_bytes =
-      g.kind ? (size_t)m.N * g.deg * (sizeof(uint32_t) + 3 * sizeof(T)) + m.N * 4 : 0;
+      jastrow ? (size_t)m.N * g.deg * (sizeof(uint32_t) + 3 * sizeof(T)) + m.N * 4 : 0;
   // (translation-invariant dense tables are staged by stage_tables itself)
-  *stage_nbr = (g.kind != GUIDE_NONE) && !g.dense && nbr_bytes <= 48 * 1024;
+  *stage_nbr = jastrow && !g.dense && nbr_bytes <= 48 * 1024;
   DevModel<T> mm = m;
   DevGuide<T> gg = g;
   *cta = stage_tables(mm, gg, *stage_nbr, nullptr, false);

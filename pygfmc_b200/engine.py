@@ -149,6 +149,29 @@ def _is_bose_jastrow(guide):
     return all(hasattr(guide, a) for a in BOSE_JASTROW_ATTRS) and not _is_spin_jastrow(guide)
 
 
+EXACT_GUIDE_ATTRS = ("N", "log_amp", "local_hilbert_space", "basis_index")
+
+
+def _is_exact_guide(guide):
+    return all(hasattr(guide, a) for a in EXACT_GUIDE_ATTRS)
+
+
+def exact_amplitude_table(guide):
+    """log |psi_0| of an ExactGroundState-shaped guide in the device's basis
+    order (bit N-1-i set for a down spin at site i: the digits of
+    SpinHalf.local_hilbert_space (1, -1)), widened exactly to float64; a guide
+    indexed over (-1, 1) has the complementary index, i.e. the reversed
+    table."""
+    values = tuple(float(v) for v in np.asarray(guide.local_hilbert_space, np.float64).ravel())
+    if values not in ((1.0, -1.0), (-1.0, 1.0)):
+        raise TypeError(f"the exact-amplitude guide runs on spin-1/2 configurations; its "
+                        f"local_hilbert_space is {list(values)}")
+    la = np.asarray(guide.log_amp, np.float64).ravel()
+    if la.shape[0] != 2 ** int(guide.N):
+        raise ValueError(f"log_amp has {la.shape[0]} entries for 2**{int(guide.N)} states")
+    return np.ascontiguousarray(la if values == (1.0, -1.0) else la[::-1])
+
+
 def require_guide_protocol(guide):
     if guide is None:
         return
@@ -156,11 +179,11 @@ def require_guide_protocol(guide):
         raise TypeError(f"Guide {type(guide).__name__!r} must implement at least one of "
                         "log_diff_from_operator, log_diff_from_configs, or log_psi "
                         "(the guide protocol, pygfmc.Guide).")
-    if not (_is_spin_jastrow(guide) or _is_bose_jastrow(guide)
+    if not (_is_spin_jastrow(guide) or _is_bose_jastrow(guide) or _is_exact_guide(guide)
             or isinstance(guide, (RBMSpinHalf, MLPBoseHubbard)) or hasattr(guide, "_gfmc_guide_desc")):
         raise TypeError(f"Guide {type(guide).__name__!r} has no device implementation in the B200 "
-                        "engine (supported: JastrowSpinHalf, JastrowBoseHubbard -- PyGFMC's or "
-                        "this package's -- RBMSpinHalf, MLPBoseHubbard).")
+                        "engine (supported: JastrowSpinHalf, JastrowBoseHubbard, ExactGroundState "
+                        "on SpinHalf -- PyGFMC's or this package's -- RBMSpinHalf, MLPBoseHubbard).")
 
 
 def spin_jastrow_tables(guide):
@@ -257,6 +280,18 @@ def guide_desc(guide, op, keep):
         return g
     if hasattr(guide, "_gfmc_guide_desc"):
         return guide._gfmc_guide_desc(op, keep)
+    if _is_exact_guide(guide):
+        if not _is_spin_half(op):
+            raise TypeError(f"the exact-amplitude guide runs on SpinHalf models only; got "
+                            f"{type(op).__name__}")
+        N = int(guide.N)
+        if N != int(op.N) or N > 26:
+            raise ValueError(f"ExactGroundState over {N} sites for an operator of {int(op.N)} sites "
+                             "(the device table holds at most 2**26 amplitudes)")
+        g.kind = _lib.GUIDE_EXACT_SPIN_HALF
+        g.exact_n_sites = N
+        g.exact_log_amp = keep.f64(exact_amplitude_table(guide))
+        return g
     if _is_spin_jastrow(guide):
         if not _is_spin_half(op):
             raise TypeError(f"JastrowSpinHalf needs an operator with the SpinHalf transition layout "

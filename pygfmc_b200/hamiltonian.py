@@ -17,7 +17,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 __all__ = ["SpinHalf", "BoseHubbard", "StructureFactor", "SzSzStructureFactor", "Lattice", "chain",
-           "square", "kagome", "edges_array"]
+           "square", "kagome", "edges_array", "exact_diagonalization"]
 
 
 def edges_array(edges):
@@ -576,3 +576,115 @@ def kagome(Lx: int, Ly: int, periodic: bool = True) -> Lattice:
                    extras=dict(positions=pos, primitive_vectors=np.array([a1, a2]),
                                supercell_dims=np.array([Lx, Ly]), sublattice_offsets=basis,
                                torus=np.array([Lx * a1, Ly * a2])))
+
+
+# ---------------------------------------------------------------------------
+# exact diagonalisation over the Hamiltonian protocol (host, float64)
+# ---------------------------------------------------------------------------
+_ED_MAX_DIM = 2 ** 24
+_ED_DENSE_DIM = 2048
+
+
+def _basis(values, N):
+    """Every configuration of N sites, row r holding the digits of r in base
+    d = len(values) with site 0 most significant, mapped to the values."""
+    d = len(values)
+    powers = d ** np.arange(N - 1, -1, -1, dtype=np.int64)
+    digits = (np.arange(d ** N, dtype=np.int64)[:, None] // powers) % d
+    return np.asarray(values, np.float64)[digits], powers
+
+
+def _basis_index(configs, values, powers):
+    """Positional index of each row of configs (nearest local value per site)."""
+    c = np.atleast_2d(np.asarray(configs, np.float64))
+    digit = np.argmin(np.abs(c[..., None] - np.asarray(values, np.float64)), axis=-1)
+    return digit.astype(np.int64) @ powers
+
+
+def _protocol_matrix(op, configs, values, powers):
+    """Sparse matrix of op over the basis from get_rates alone: H[y, x] is the
+    rate of the transition x -> y (the diagonal element at slot 0)."""
+    from scipy import sparse
+    dim = len(configs)
+    rows, cols, vals = [], [], []
+    for i, x in enumerate(configs):
+        rates, succ = op.get_rates(x, return_configs=True)
+        rates = np.asarray(rates, np.float64)
+        nz = np.nonzero(rates)[0]
+        if nz.size == 0:
+            continue
+        sub = np.asarray(succ, np.float64)[nz]
+        ok = np.all(np.min(np.abs(sub[..., None] - np.asarray(values)), axis=-1) < 1e-6, axis=1)
+        if not np.all(ok):
+            raise ValueError(f"a transition of nonzero amplitude leaves the basis at configuration "
+                             f"{x.tolist()}")
+        rows.append(_basis_index(sub, values, powers))
+        cols.append(np.full(nz.size, i, np.int64))
+        vals.append(rates[nz])
+    if not rows:
+        return sparse.csr_matrix((dim, dim))
+    H = sparse.coo_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                          shape=(dim, dim)).tocsr()
+    if not np.all(np.isfinite(H.data)):
+        raise ValueError("the operator matrix has non-finite elements")
+    asym = abs(H - H.T).max() if H.nnz else 0.0
+    if asym > 1e-10 * max(1.0, abs(H).max()):
+        raise ValueError(f"the operator matrix is not Hermitian (max |H - H^T| = {asym:.3e})")
+    return H
+
+
+def exact_diagonalization(hamiltonian, local_hilbert_space=None, N=None, diag_operators=None,
+                          off_diag_operators=None, number_of_states=1, return_states=False):
+    """Lowest eigenpairs of ``hamiltonian`` and observables on each
+    (hamiltonian/exact.py:212-375): the matrix comes from the protocol's
+    ``get_rates(x, return_configs=True)`` over the positional basis (site 0
+    most significant digit of ``local_hilbert_space``), dense below 2048
+    states, otherwise Lanczos on the sparse matrix.  Returns ``(energies,
+    diag_obs, off_diag_obs)`` and the states (dim, number_of_states) when
+    ``return_states``; ``diag_obs[name][k] = sum_x |psi_k(x)|^2 O(x)`` through
+    ``diagonal_weight``, ``off_diag_obs[name][k] = psi_k^T O psi_k``."""
+    if local_hilbert_space is None:
+        local_hilbert_space = getattr(hamiltonian, "local_hilbert_space", None)
+        if local_hilbert_space is None:
+            raise ValueError(f"{type(hamiltonian).__name__} exposes no local_hilbert_space; pass it")
+    values = np.asarray(local_hilbert_space, dtype=np.float64).ravel()
+    d = values.size
+    if d < 2 or not np.all(np.isfinite(values)) or np.unique(values).size != d:
+        raise ValueError(f"local_hilbert_space must hold at least two distinct finite values, got "
+                         f"{values.tolist()}")
+    own = getattr(hamiltonian, "local_hilbert_space", None)
+    if own is not None and not np.array_equal(np.sort(np.asarray(own, np.float64).ravel()),
+                                              np.sort(values)):
+        raise ValueError(f"local_hilbert_space {values.tolist()} is not the set of values "
+                         f"{list(own)} the Hamiltonian acts on")
+    if N is None:
+        N = getattr(hamiltonian, "N", None)
+        if N is None:
+            raise ValueError(f"{type(hamiltonian).__name__} exposes no N; pass it")
+    N = int(N)
+    dim = d ** N
+    if dim > _ED_MAX_DIM:
+        raise ValueError(f"a basis of {d}**{N} = {dim} states is above the {_ED_MAX_DIM} limit")
+    k = int(number_of_states)
+    if k != number_of_states or not 1 <= k <= dim:
+        raise ValueError(f"number_of_states must be an integer in [1, {dim}], got {number_of_states!r}")
+    configs, powers = _basis(values, N)
+    H = _protocol_matrix(hamiltonian, configs, values, powers)
+    if dim <= _ED_DENSE_DIM or k >= dim - 1:
+        w, v = np.linalg.eigh(H.toarray())
+        energies, states = w[:k], v[:, :k]
+    else:
+        from scipy.sparse.linalg import eigsh
+        w, v = eigsh(H, k=k, which="SA", tol=1e-12)
+        order = np.argsort(w)
+        energies, states = w[order], v[:, order]
+    diag_obs = {}
+    for name, op in (diag_operators or {}).items():
+        dw = np.array([float(np.asarray(op.diagonal_weight(x))) for x in configs])
+        diag_obs[name] = (np.abs(states) ** 2 * dw[:, None]).sum(axis=0)
+    off_obs = {}
+    for name, op in (off_diag_operators or {}).items():
+        O = _protocol_matrix(op, configs, values, powers)
+        off_obs[name] = np.einsum("ik,ik->k", states, O @ states)
+    out = (np.asarray(energies, np.float64), diag_obs, off_obs)
+    return out + (states,) if return_states else out

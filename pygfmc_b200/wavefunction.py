@@ -14,7 +14,8 @@ import numpy as np
 
 from .hamiltonian import BoseHubbard, edges_array
 
-__all__ = ["JastrowSpinHalf", "JastrowBoseHubbard", "RBMSpinHalf", "MLPBoseHubbard", "round_bf16"]
+__all__ = ["JastrowSpinHalf", "JastrowBoseHubbard", "RBMSpinHalf", "MLPBoseHubbard", "ExactGroundState",
+           "round_bf16"]
 
 LAYOUT_ATTRS = ("n_hx_static", "n_jpm_static", "edge_i", "edge_j")
 
@@ -343,3 +344,131 @@ class MLPBoseHubbard:
 
     def log_diff_from_configs(self, config, new_configs):
         return self.log_psi(new_configs) - self.log_psi(config)
+
+
+# floor on |psi_0| before the log: a node of the exact ground state gets a
+# large negative log amplitude rather than -inf (exact_ground_state.py:36)
+AMP_FLOOR = 1e-30
+
+
+class ExactGroundState:
+    """psi_T(x) = |psi_0[idx(x)]| with psi_0 the exact ground state
+    (wavefunction/exact_ground_state.py:43-190): the zero-variance limit, in
+    which every walker's local energy is E0.  ``idx`` is the positional basis
+    index over ``local_hilbert_space`` (default the Hamiltonian's own), site 0
+    the most significant digit.  ``log_amp`` (d^N values) is given, or taken
+    from :func:`pygfmc_b200.hamiltonian.exact_diagonalization` (then ``E0`` is
+    stored, else NaN), and kept rounded to ``dtype``.
+
+    On the device (SpinHalf models, N <= 26) the ratio of a move is
+    exp(log_amp[y] - log_amp[x]) in the run's precision, looked up at the
+    walker's basis index; ``log_diff_from_configs`` is the host version."""
+
+    def __init__(self, hamiltonian, *, log_amp=None, dtype=np.float32, local_hilbert_space=None,
+                 N=None):
+        name = type(hamiltonian).__name__
+        values = local_hilbert_space
+        if values is None:
+            values = getattr(hamiltonian, "local_hilbert_space", None)
+        if values is None:
+            raise ValueError(f"{name} exposes no local_hilbert_space: pass local_hilbert_space=(...), "
+                             "e.g. (1, -1) for spin-1/2")
+        values = tuple(float(v) for v in np.asarray(values, dtype=float).ravel())
+        if len(values) < 2:
+            raise ValueError(f"local_hilbert_space needs at least two values, got {list(values)}")
+        if N is None:
+            N = getattr(hamiltonian, "N", None)
+        if N is None:
+            raise ValueError(f"{name} exposes no N: pass N=...")
+        d, N = len(values), int(N)
+        self.local_hilbert_space = values
+        self.N = N
+        self._powers = tuple(int(d ** k) for k in range(N - 1, -1, -1))
+        if log_amp is None:
+            from .hamiltonian import exact_diagonalization
+            energies, _, _, states = exact_diagonalization(hamiltonian, values, N, number_of_states=1,
+                                                           return_states=True)
+            psi0 = np.asarray(states[:, 0])
+            if psi0.min() < -1e-6 and psi0.max() > 1e-6:
+                import warnings
+                warnings.warn(f"ExactGroundState: psi_0 changes sign (min {psi0.min():.3e}, max "
+                              f"{psi0.max():.3e}); the guide assumes a sign-problem-free Hamiltonian "
+                              "and uses |psi_0|", UserWarning)
+            self.E0 = float(energies[0])
+            log_amp = np.log(np.maximum(np.abs(psi0), AMP_FLOOR))
+        else:
+            self.E0 = float("nan")
+        log_amp = np.asarray(log_amp, dtype=dtype).ravel()
+        if log_amp.shape[0] != d ** N:
+            raise ValueError(f"log_amp has {log_amp.shape[0]} entries for a basis of {d}**{N} = "
+                             f"{d ** N} states")
+        self.log_amp = log_amp
+        self.hamiltonian = hamiltonian
+        self.dtype = np.dtype(dtype)
+        self.M_total = int(hamiltonian.M_total)
+
+    def basis_index(self, config):
+        """Index of config (..., N) in log_amp (exact_ground_state.py:141-147)."""
+        c = np.asarray(config, dtype=np.float64)
+        digit = np.argmin(np.abs(c[..., None] - np.asarray(self.local_hilbert_space)), axis=-1)
+        return digit.astype(np.int64) @ np.asarray(self._powers, dtype=np.int64)
+
+    def log_psi(self, config):
+        return self.log_amp[self.basis_index(config)]
+
+    def log_diff_from_configs(self, config, new_configs=None, cache=None):
+        """log psi(y) - log psi(x) in ``dtype`` for the given successors, or
+        for every transition of the bound Hamiltonian with element 0 pinned to
+        0 (exact_ground_state.py:150-190); indices outside the basis (zero-rate
+        transitions of a bounded local space) are clipped."""
+        dim = self.log_amp.shape[0]
+        old = self.log_amp[self.basis_index(config)]
+        if new_configs is None:
+            new_configs = np.stack([self.hamiltonian.generate_state(np.asarray(config), k)
+                                    for k in range(self.M_total)])
+            out = self.log_amp[np.clip(self.basis_index(new_configs), 0, dim - 1)] - old
+            out[0] = 0
+            return out.astype(self.dtype)
+        new = np.clip(self.basis_index(new_configs), 0, dim - 1)
+        return (self.log_amp[new] - old).astype(self.dtype)
+
+    def save(self, path, group="exact_ground_state", **attrs):
+        """``log_amp``, ``local_hilbert_space`` and the attributes N, family,
+        E0 (plus keyword scalars) under ``group`` (exact_ground_state.py:
+        193-210), in a NumPy ``.npz`` archive as ``Walker.save`` writes one."""
+        d = {f"{group}/log_amp": np.asarray(self.log_amp),
+             f"{group}/local_hilbert_space": np.asarray(self.local_hilbert_space, dtype=float),
+             f"{group}/attrs/N": np.asarray(self.N),
+             f"{group}/attrs/family": np.asarray(type(self.hamiltonian).__name__),
+             f"{group}/attrs/E0": np.asarray(self.E0)}
+        for k, v in attrs.items():
+            if np.ndim(v) != 0:
+                raise ValueError(f"attribute {k!r} must be a scalar")
+            d[f"{group}/attrs/{k}"] = np.asarray(v)
+        with open(path, "wb") as f:
+            np.savez(f, **d)
+
+    @classmethod
+    def load(cls, path, hamiltonian, group="exact_ground_state", dtype=np.float32):
+        """A guide written by :meth:`save`, bound to ``hamiltonian``
+        (exact_ground_state.py:212-256); ValueError when the saved family or
+        N differs from the Hamiltonian's."""
+        with np.load(path, allow_pickle=False) as z:
+            need = [f"{group}/{k}" for k in ("log_amp", "attrs/N", "attrs/family", "attrs/E0")]
+            missing = [k for k in need if k not in z.files]
+            if missing:
+                raise ValueError(f"{path}:{group} is not an ExactGroundState file (missing {missing})")
+            log_amp = np.asarray(z[f"{group}/log_amp"])
+            family = str(z[f"{group}/attrs/family"])
+            N = int(z[f"{group}/attrs/N"])
+            E0 = float(z[f"{group}/attrs/E0"])
+            lhs_k = f"{group}/local_hilbert_space"
+            lhs = tuple(float(v) for v in z[lhs_k]) if lhs_k in z.files else None
+        if family != type(hamiltonian).__name__:
+            raise ValueError(f"saved guide family={family!r} but loading into "
+                             f"{type(hamiltonian).__name__!r}")
+        if getattr(hamiltonian, "N", None) is not None and N != int(hamiltonian.N):
+            raise ValueError(f"saved guide N={N} but the Hamiltonian has N={int(hamiltonian.N)}")
+        guide = cls(hamiltonian, log_amp=log_amp, dtype=dtype, local_hilbert_space=lhs, N=N)
+        guide.E0 = E0
+        return guide
