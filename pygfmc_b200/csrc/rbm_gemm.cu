@@ -148,21 +148,26 @@ rbm_theta_kernel(const uint64_t *cfg, const int *parents, int NW, int n, int Np,
 size_t theta_smem_bytes() { return 1024 + GT * 128 + MAXN * 128 + 16; }
 
 // ---------------------------------------------------------------------------
-// Persistent version: one CTA of 8 warps per SM.  The hidden axis runs in
+// Persistent version: one CTA of 9 warps per SM.  The hidden axis runs in
 // passes of PW columns (256, or 128 / 64 when a pass's W tile would not fit);
 // the pass's W tile (PW rows x Np sites, bf16, K-chunks of 64 sites in the
 // 128-byte swizzled K-major layout) stays in shared memory while the CTA
 // walks its walker tiles (128 walkers each):
 //  * warps 0-3 (one walker row per thread) expand the spin words of each
 //    64-site chunk into a two-stage ring of A tiles (bf16 +-1);
-//  * thread 0 issues the chunk's four MMAs (K = 16 each, N = PW) into one of
-//    two TMEM accumulators and commits them to the ring stage's "free"
-//    mbarrier, and after a tile's last chunk to the accumulator's "full" one;
+//  * warp 8 waits for each chunk (lane 0 waits, the other lanes hold at a
+//    shuffle, so the warp never spins divergently) and its lane 0 issues the
+//    chunk's four MMAs (K = 16 each, N = PW) into one of two TMEM
+//    accumulators, commits them to the ring stage's "free" mbarrier, and
+//    after a tile's last chunk to the accumulator's "full" one;
 //  * warps 4-7 (warp 4 + q reads TMEM lanes 32 q .. 32 q + 31) add b and
 //    write theta while the next tile accumulates in the other buffer.
-// Every wait is bounded (status bit 8); a wait that runs out stops every
-// role at its next wait, and the CTA frees its TMEM.
-constexpr int PT = 256;   // threads
+// The tiles of a pass go round the CTAs from an offset that advances by
+// n_tiles mod grid per pass, so the CTAs that took one tile more in one pass
+// take one less in the next.  Every wait is bounded (status bit 8); a wait
+// that runs out stops every role at its next wait, and the CTA frees its
+// TMEM.
+constexpr int PT = 288;   // threads: 4 producer, 4 epilogue and 1 MMA warp
 
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
@@ -214,9 +219,12 @@ rbm_theta_persist(const uint64_t *cfg, const int *parents, int NW, int n, int Np
   const uint32_t tmem = *slot;
   const uint32_t idesc = idesc_m128((uint32_t)PW);
   const int n_tiles = (n + GT - 1) / GT;
+  const int G = (int)gridDim.x, rot = n_tiles % G;
   uint32_t g = 0, T = 0;   // chunks and tiles this CTA has produced (over every pass)
 
-  for (int hb = 0; hb < Hp; hb += PW) {
+  for (int hb = 0, pass = 0; hb < Hp; hb += PW, ++pass) {
+    // this CTA's first tile in the pass
+    const int first = (int)(((long long)blockIdx.x - (long long)pass * rot) % G + G) % G;
     // the pass's W tile: rows hb .. hb + PW - 1, every chunk
     for (int idx = tid; idx < nk * PW; idx += PT) {
       const int kc = idx / PW, r = idx - kc * PW;
@@ -229,12 +237,11 @@ rbm_theta_persist(const uint64_t *cfg, const int *parents, int NW, int n, int Np
     __syncthreads();
     const uint32_t g0 = g, T0 = T;
     if (warp < 4) {
-      // ---- producers (and thread 0: the MMA issuer)
-      uint32_t gg = g0, TT = T0;
-      for (int t = blockIdx.x; t < n_tiles && !*abort_flag; t += gridDim.x, ++TT) {
+      // ---- producers
+      uint32_t gg = g0;
+      for (int t = first; t < n_tiles && !*abort_flag; t += G) {
         const int w = t * GT + tid;
         const int src = w < n ? (parents ? parents[w] : w) : 0;
-        const uint32_t buf = TT & 1u, use = TT >> 1;
         // the walker's spin words of up to 8 chunks at once (one load latency
         // per tile instead of one per chunk)
         uint64_t words[8];
@@ -267,11 +274,25 @@ rbm_theta_persist(const uint64_t *cfg, const int *parents, int NW, int n, int Np
           }
           fence_async_smem();
           mbar_arrive(a_full + s);
-          if (tid == 0) {
-            if (!bwait(a_full + s, u, abort_flag)) break;
-            if (kc == 0 && use >= 1 && !bwait(acc_free + buf, use - 1, abort_flag)) break;
-            fence_after();
-            const uint32_t a0 = smem_u32(A);
+        }
+      }
+    } else if (warp == 8) {
+      // ---- the MMA issuer
+      const int lane = tid & 31;
+      uint32_t gg = g0, TT = T0;
+      bool ok = true;
+      for (int t = first; t < n_tiles && ok; t += G, ++TT) {
+        const uint32_t buf = TT & 1u, use = TT >> 1;
+        for (int kc = 0; kc < nk; ++kc, ++gg) {
+          const uint32_t s = gg & 1u, u = gg >> 1;
+          if (lane == 0)
+            ok = bwait(a_full + s, u, abort_flag) &&
+                 (kc != 0 || use < 1 || bwait(acc_free + buf, use - 1, abort_flag));
+          ok = __shfl_sync(0xffffffffu, ok, 0);
+          if (!ok) break;
+          fence_after();
+          if (lane == 0) {
+            const uint32_t a0 = smem_u32(At + (size_t)s * GT * 128);
             const uint32_t b0 = smem_u32(Bt + (size_t)kc * PW * 128);
             const uint32_t d = tmem + buf * (uint32_t)PW;
 #pragma unroll
@@ -281,6 +302,7 @@ rbm_theta_persist(const uint64_t *cfg, const int *parents, int NW, int n, int Np
             mma_commit(a_free + s);
             if (kc == nk - 1) mma_commit(acc_full + buf);
           }
+          __syncwarp();
         }
       }
     } else {
@@ -292,7 +314,7 @@ rbm_theta_persist(const uint64_t *cfg, const int *parents, int NW, int n, int Np
       for (int cb = 0; cb < 8; ++cb)
         bias[cb] = 32 * cb < PW ? b[hb + 32 * cb + (tid & 31)] : 0.0f;
       uint32_t TT = T0;
-      for (int t = blockIdx.x; t < n_tiles && !*abort_flag; t += gridDim.x, ++TT) {
+      for (int t = first; t < n_tiles && !*abort_flag; t += G, ++TT) {
         const uint32_t buf = TT & 1u, use = TT >> 1;
         if (!bwait(acc_full + buf, use, abort_flag)) break;
         fence_after();
@@ -312,6 +334,7 @@ rbm_theta_persist(const uint64_t *cfg, const int *parents, int NW, int n, int Np
           for (int i = 0; i < 32; ++i) E[lane * 33 + i] = __uint_as_float(v[i]);
           __syncwarp();
           const float bb = bias[cb];
+#pragma unroll 8
           for (int rr = 0; rr < 32; ++rr)
             if (w0 + rr < n) theta[(size_t)(w0 + rr) * Hp + hb + c0 + lane] = E[rr * 33 + lane] + bb;
           __syncwarp();
@@ -322,7 +345,7 @@ rbm_theta_persist(const uint64_t *cfg, const int *parents, int NW, int n, int Np
     }
     // tiles of this pass: the same count in every role
     uint32_t my = 0;
-    for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) ++my;
+    for (int t = first; t < n_tiles; t += G) ++my;
     g = g0 + my * (uint32_t)nk;
     T = T0 + my;
     fence_before();
