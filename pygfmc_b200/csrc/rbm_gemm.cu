@@ -18,6 +18,8 @@
 // two-stage ring, two TMEM accumulators) is the one launched whenever a
 // pass's W tile fits in shared memory; the one-CTA-per-tile kernel above
 // takes the rest.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 
 #include "rbm.cuh"
@@ -161,7 +163,11 @@ size_t theta_smem_bytes() { return 1024 + GT * 128 + MAXN * 128 + 16; }
 //    accumulators, commits them to the ring stage's "free" mbarrier, and
 //    after a tile's last chunk to the accumulator's "full" one;
 //  * warps 4-7 (warp 4 + q reads TMEM lanes 32 q .. 32 q + 31) add b and
-//    write theta while the next tile accumulates in the other buffer.
+//    write theta while the next tile accumulates in the other buffer: each
+//    32 x 32 block goes into one of the warp's two staging boxes in shared
+//    memory (128-byte swizzled rows, the layout of the output's tensor map)
+//    and leaves by one TMA tensor store (this GPU's own memory, no
+//    multicast), so the stores stream while the warp reads the next block.
 // The tiles of a pass go round the CTAs from an offset that advances by
 // n_tiles mod grid per pass, so the CTAs that took one tile more in one pass
 // take one less in the next.  Every wait is bounded (status bit 8); a wait
@@ -172,6 +178,39 @@ constexpr int PT = 288;   // threads: 4 producer, 4 epilogue and 1 MMA warp
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
+
+// TMA tensor store of one box at (x, y) from shared memory, and the bulk
+// groups of the issuing thread: commit, wait until at most one group is
+// still reading shared memory, wait until every group has read it / has
+// completed.
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap *map, uint32_t saddr, int x, int y) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];"
+               ::"l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(saddr) : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read1() {
+  asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_read0() {
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+// TMA tensor load of one box at (x, y) into shared memory, completing on
+// mbarrier bar (whose expected bytes the issuer has armed).
+__device__ __forceinline__ void tma_load_2d(const CUtensorMap *map, uint32_t saddr, int x, int y,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+      ::"r"(saddr), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+constexpr int STAGE_BYTES = 32 * 128;   // one 32 x 32 float box
 
 // Bounded wait of one thread on completion `k` (parity k & 1); false (and
 // the CTA's abort flag set) when the limit ran out or another role aborted.
@@ -186,18 +225,22 @@ __device__ __forceinline__ bool bwait(uint64_t *bar, uint32_t k, volatile int *a
 
 __global__ void __launch_bounds__(PT, 1)
 rbm_theta_persist(const uint64_t *cfg, const int *parents, int NW, int n, int Np,
-                  const __nv_bfloat16 *W, const float *b, int Hp, int PW, float *theta,
-                  int *status) {
+                  const __nv_bfloat16 *W, const float *b, int Hp, int PW,
+                  const __grid_constant__ CUtensorMap tmap,
+                  const __grid_constant__ CUtensorMap wmap, int *status) {
   extern __shared__ unsigned char dsm[];
   unsigned char *base = (unsigned char *)(((uintptr_t)dsm + 1023) & ~(uintptr_t)1023);
   const int nk = Np / KC;
   unsigned char *Bt = base;                                   // nk x PW x 128 bytes
   unsigned char *At = Bt + (size_t)nk * PW * 128;             // 2 stages x 128 x 128 bytes
-  // epilogue staging: per epilogue warp a 32 x 32 float tile (rows padded to 33)
-  float *Et = reinterpret_cast<float *>(At + 2 * GT * 128);
-  uint64_t *bar = reinterpret_cast<uint64_t *>(Et + 4 * 32 * 33);
+  // epilogue staging: per epilogue warp two boxes (1024-byte aligned, as the
+  // 128-byte swizzle wants), then the pass's biases
+  unsigned char *St = At + 2 * GT * 128;
+  float *bsm = reinterpret_cast<float *>(St + 4 * 2 * STAGE_BYTES);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(bsm + 256);
   uint64_t *a_full = bar, *a_free = bar + 2, *acc_full = bar + 4, *acc_free = bar + 6;
-  uint32_t *slot = reinterpret_cast<uint32_t *>(bar + 8);
+  uint64_t *w_full = bar + 8;   // the pass's W tile has landed (one phase per pass)
+  uint32_t *slot = reinterpret_cast<uint32_t *>(bar + 9);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(slot + 1);
   const int tid = threadIdx.x, warp = tid >> 5;
   const uint32_t ncols = 2u * (uint32_t)PW;                   // two accumulators
@@ -210,6 +253,7 @@ rbm_theta_persist(const uint64_t *cfg, const int *parents, int NW, int n, int Np
       mbar_init(acc_full + i, 1);
       mbar_init(acc_free + i, GT);
     }
+    mbar_init(w_full, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -221,18 +265,21 @@ rbm_theta_persist(const uint64_t *cfg, const int *parents, int NW, int n, int Np
   const int n_tiles = (n + GT - 1) / GT;
   const int G = (int)gridDim.x, rot = n_tiles % G;
   uint32_t g = 0, T = 0;   // chunks and tiles this CTA has produced (over every pass)
+  int w_issued = 0;        // W tiles requested (passes begun)
 
   for (int hb = 0, pass = 0; hb < Hp; hb += PW, ++pass) {
     // this CTA's first tile in the pass
     const int first = (int)(((long long)blockIdx.x - (long long)pass * rot) % G + G) % G;
-    // the pass's W tile: rows hb .. hb + PW - 1, every chunk
-    for (int idx = tid; idx < nk * PW; idx += PT) {
-      const int kc = idx / PW, r = idx - kc * PW;
-      const uint4 *srcw = reinterpret_cast<const uint4 *>(W + (size_t)(hb + r) * Np + (size_t)kc * KC);
-      unsigned char *tile = Bt + (size_t)kc * PW * 128;
-#pragma unroll
-      for (int c = 0; c < 8; ++c) *reinterpret_cast<uint4 *>(sw_chunk(tile, r, c)) = __ldg(srcw + c);
+    // the pass's W tile (rows hb .. hb + PW - 1, every 64-site chunk) by TMA
+    // in the 128-byte swizzled layout the MMA descriptors expect; the MMA
+    // issuer waits for it
+    ++w_issued;
+    if (tid == 0) {
+      mbar_expect_tx(w_full, (uint32_t)(nk * PW * 128));
+      for (int kc = 0; kc < nk; ++kc)
+        tma_load_2d(&wmap, smem_u32(Bt + (size_t)kc * PW * 128), kc * KC, hb, w_full);
     }
+    for (int i = tid; i < PW; i += PT) bsm[i] = b[hb + i];
     fence_async_smem();
     __syncthreads();
     const uint32_t g0 = g, T0 = T;
@@ -281,6 +328,8 @@ rbm_theta_persist(const uint64_t *cfg, const int *parents, int NW, int n, int Np
       const int lane = tid & 31;
       uint32_t gg = g0, TT = T0;
       bool ok = true;
+      if (lane == 0) ok = bwait(w_full, (uint32_t)pass, abort_flag);
+      ok = __shfl_sync(0xffffffffu, ok, 0);
       for (int t = first; t < n_tiles && ok; t += G, ++TT) {
         const uint32_t buf = TT & 1u, use = TT >> 1;
         for (int kc = 0; kc < nk; ++kc, ++gg) {
@@ -307,41 +356,48 @@ rbm_theta_persist(const uint64_t *cfg, const int *parents, int NW, int n, int Np
       }
     } else {
       // ---- epilogue: theta = accumulator + b
-      const int q = warp - 4;
-      // the pass's biases of this lane's column in each 32-column block
-      float bias[8];
-#pragma unroll
-      for (int cb = 0; cb < 8; ++cb)
-        bias[cb] = 32 * cb < PW ? b[hb + 32 * cb + (tid & 31)] : 0.0f;
+      const int q = warp - 4, lane = tid & 31;
+      unsigned char *S0 = St + (size_t)q * 2 * STAGE_BYTES;
+      uint32_t nst = 0;   // boxes this warp has stored in the pass
       uint32_t TT = T0;
       for (int t = first; t < n_tiles && !*abort_flag; t += G, ++TT) {
         const uint32_t buf = TT & 1u, use = TT >> 1;
         if (!bwait(acc_full + buf, use, abort_flag)) break;
         fence_after();
-        // a 32 x 32 block (this warp's walkers x 32 columns) at a time: into
-        // the warp's staging tile by rows (one walker per lane), out by rows
-        // of the output (one column per lane: 128 contiguous bytes per store)
-        const int lane = tid & 31, w0 = t * GT + 32 * q;
-        float *E = Et + q * 32 * 33;
-#pragma unroll
-        for (int cb = 0; cb < 8; ++cb) {
+        // this warp's 32 walkers (one per lane) x 32 columns at a time
+        const int w0 = t * GT + 32 * q;
+        for (int cb = 0; cb < PW / 32; ++cb) {
           const int c0 = 32 * cb;
-          if (c0 >= PW) break;
           uint32_t v[32];
           tmem_ld32_async(tmem + ((uint32_t)(32 * q) << 16) + buf * (uint32_t)PW + (uint32_t)c0, v);
           tmem_ld_wait(v);
+          if (w0 >= n) continue;   // (the last tile's rows past the population)
+          unsigned char *S = S0 + (size_t)(nst & 1u) * STAGE_BYTES;
+          // the box stored two blocks ago has left this buffer
+          if (nst >= 2 && lane == 0) bulk_wait_read1();
+          __syncwarp();
 #pragma unroll
-          for (int i = 0; i < 32; ++i) E[lane * 33 + i] = __uint_as_float(v[i]);
+          for (int j = 0; j < 8; ++j) {
+            const float4 bj = *reinterpret_cast<const float4 *>(bsm + c0 + 4 * j);
+            *reinterpret_cast<float4 *>(sw_chunk(S, lane, j)) =
+                make_float4(__uint_as_float(v[4 * j]) + bj.x, __uint_as_float(v[4 * j + 1]) + bj.y,
+                            __uint_as_float(v[4 * j + 2]) + bj.z, __uint_as_float(v[4 * j + 3]) + bj.w);
+          }
+          fence_async_smem();
           __syncwarp();
-          const float bb = bias[cb];
-#pragma unroll 8
-          for (int rr = 0; rr < 32; ++rr)
-            if (w0 + rr < n) theta[(size_t)(w0 + rr) * Hp + hb + c0 + lane] = E[rr * 33 + lane] + bb;
-          __syncwarp();
+          if (lane == 0) {
+            tma_store_2d(&tmap, smem_u32(S), hb + c0, w0);
+            bulk_commit();
+          }
+          ++nst;
         }
         fence_before();
         mbar_arrive(acc_free + buf);
       }
+      // the staging boxes are read out before the pass ends (the next pass
+      // reuses them)
+      if (lane == 0) bulk_wait_read0();
+      __syncwarp();
     }
     // tiles of this pass: the same count in every role
     uint32_t my = 0;
@@ -360,8 +416,14 @@ rbm_theta_persist(const uint64_t *cfg, const int *parents, int NW, int n, int Np
       if (T > 0)
         for (uint32_t it = 0; it < WAIT_LIMIT; ++it)
           if (mbar_try_wait(acc_full + ((T - 1) & 1u), ((T - 1) >> 1) & 1u)) break;
+      // and the last W tile's copies have landed before the shared memory goes
+      if (w_issued > 0)
+        for (uint32_t it = 0; it < WAIT_LIMIT; ++it)
+          if (mbar_try_wait(w_full, (uint32_t)(w_issued - 1) & 1u)) break;
     }
   }
+  // the output boxes in flight have landed before the CTA leaves
+  if (warp >= 4 && warp < 8 && (tid & 31) == 0) bulk_wait_all();
   fence_before();
   __syncthreads();
   if (warp == 0) tmem_dealloc(tmem, ncols);
@@ -372,14 +434,56 @@ rbm_theta_persist(const uint64_t *cfg, const int *parents, int NW, int n, int Np
 int theta_pass_width(int Np, int Hp) {
   for (int pw = 256; pw >= 64; pw /= 2) {
     if (Hp % pw) continue;
-    const size_t bytes = 1024 + (size_t)(Np / KC) * pw * 128 + 2 * GT * 128 + 4 * 32 * 33 * 4 + 128;
+    const size_t bytes = 1024 + (size_t)(Np / KC) * pw * 128 + 2 * GT * 128 + 8 * STAGE_BYTES + 1024 + 128;
     if (bytes <= (size_t)227 * 1024) return pw;
   }
   return 0;
 }
 
 size_t theta_persist_smem(int Np, int PW) {
-  return 1024 + (size_t)(Np / KC) * PW * 128 + 2 * GT * 128 + 4 * 32 * 33 * 4 + 128;
+  return 1024 + (size_t)(Np / KC) * PW * 128 + 2 * GT * 128 + 8 * STAGE_BYTES + 1024 + 128;
+}
+
+// cuTensorMapEncodeTiled from the driver, looked up once (no link against
+// the driver library); nullptr when unavailable.
+PFN_cuTensorMapEncodeTiled encode_tiled() {
+  static PFN_cuTensorMapEncodeTiled fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled>(p);
+  }
+  return fn;
+}
+
+// Tensor map of W (Hp rows of Np bf16) in boxes of 64 sites x PW rows with
+// the 128-byte swizzle; false when the driver refuses it.
+bool w_tensor_map(const __nv_bfloat16 *W, int Hp, int Np, int PW, CUtensorMap *tm) {
+  PFN_cuTensorMapEncodeTiled enc = encode_tiled();
+  if (!enc) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)Np, (cuuint64_t)Hp};
+  const cuuint64_t stride[1] = {(cuuint64_t)Np * sizeof(__nv_bfloat16)};
+  const cuuint32_t box[2] = {(cuuint32_t)KC, (cuuint32_t)PW}, es[2] = {1, 1};
+  return enc(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16 *>(W), dims, stride, box,
+             es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Tensor map of theta (n rows of Hp floats) in 32 x 32 boxes with the
+// 128-byte swizzle; false when the driver refuses it.
+bool theta_tensor_map(float *theta, int n, int Hp, CUtensorMap *tm) {
+  PFN_cuTensorMapEncodeTiled enc = encode_tiled();
+  if (!enc) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)Hp, (cuuint64_t)n};
+  const cuuint64_t stride[1] = {(cuuint64_t)Hp * sizeof(float)};
+  const cuuint32_t box[2] = {32, 32}, es[2] = {1, 1};
+  return enc(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, theta, dims, stride, box, es,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+             CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 }  // namespace
@@ -387,7 +491,9 @@ size_t theta_persist_smem(int Np, int PW) {
 cudaError_t launch_rbm_theta(const RbmTables &r, int n, const void *cfg, const int *parents,
                              int NW, float *theta, int *status, cudaStream_t s) {
   const int PW = theta_pass_width(r.Np, r.Hp);
-  if (PW > 0 && n > 0) {
+  CUtensorMap tm, wm;
+  if (PW > 0 && n > 0 && theta_tensor_map(theta, n, r.Hp, &tm) &&
+      w_tensor_map(r.W, r.Hp, r.Np, PW, &wm)) {
     const size_t smem = theta_persist_smem(r.Np, PW);
     // the kernel's shared-memory limit (its largest size) and the SM count,
     // once per device
@@ -406,7 +512,7 @@ cudaError_t launch_rbm_theta(const RbmTables &r, int n, const void *cfg, const i
     const int tiles = (n + GT - 1) / GT;
     const int grid = tiles < sms ? tiles : sms;
     rbm_theta_persist<<<grid, PT, smem, s>>>(reinterpret_cast<const uint64_t *>(cfg), parents, NW,
-                                             n, r.Np, r.W, r.b, r.Hp, PW, theta, status);
+                                             n, r.Np, r.W, r.b, r.Hp, PW, tm, wm, status);
     return cudaGetLastError();
   }
   const size_t smem = theta_smem_bytes();
