@@ -223,6 +223,13 @@ __device__ __forceinline__ bool bwait(uint64_t *bar, uint32_t k, volatile int *a
   return false;
 }
 
+// First tile of this CTA in pass p: the tiles go round the CTAs from an
+// offset that advances by n_tiles mod G per pass.
+__device__ __forceinline__ int first_tile(int p, int n_tiles, int G) {
+  const long long rot = n_tiles % G;
+  return (int)((((long long)blockIdx.x - (long long)p * rot) % G + G) % G);
+}
+
 __global__ void __launch_bounds__(PT, 1)
 rbm_theta_persist(const uint64_t *cfg, const int *parents, int NW, int n, int Np,
                   const __nv_bfloat16 *W, const float *b, int Hp, int PW,
@@ -236,11 +243,13 @@ rbm_theta_persist(const uint64_t *cfg, const int *parents, int NW, int n, int Np
   // epilogue staging: per epilogue warp two boxes (1024-byte aligned, as the
   // 128-byte swizzle wants), then the pass's biases
   unsigned char *St = At + 2 * GT * 128;
-  float *bsm = reinterpret_cast<float *>(St + 4 * 2 * STAGE_BYTES);
-  uint64_t *bar = reinterpret_cast<uint64_t *>(bsm + 256);
+  float *bsm = reinterpret_cast<float *>(St + 4 * 2 * STAGE_BYTES);   // every bias
+  uint64_t *bar = reinterpret_cast<uint64_t *>(bsm + 1024);
   uint64_t *a_full = bar, *a_free = bar + 2, *acc_full = bar + 4, *acc_free = bar + 6;
   uint64_t *w_full = bar + 8;   // the pass's W tile has landed (one phase per pass)
-  uint32_t *slot = reinterpret_cast<uint32_t *>(bar + 9);
+  uint64_t *w_free = bar + 9;   // the pass's MMAs are done with it (one phase per pass)
+  uint64_t *fin = bar + 10;     // every MMA of the CTA is done (one phase)
+  uint32_t *slot = reinterpret_cast<uint32_t *>(bar + 11);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(slot + 1);
   const int tid = threadIdx.x, warp = tid >> 5;
   const uint32_t ncols = 2u * (uint32_t)PW;                   // two accumulators
@@ -254,6 +263,8 @@ rbm_theta_persist(const uint64_t *cfg, const int *parents, int NW, int n, int Np
       mbar_init(acc_free + i, GT);
     }
     mbar_init(w_full, 1);
+    mbar_init(w_free, 1);
+    mbar_init(fin, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -263,30 +274,17 @@ rbm_theta_persist(const uint64_t *cfg, const int *parents, int NW, int n, int Np
   const uint32_t tmem = *slot;
   const uint32_t idesc = idesc_m128((uint32_t)PW);
   const int n_tiles = (n + GT - 1) / GT;
-  const int G = (int)gridDim.x, rot = n_tiles % G;
-  uint32_t g = 0, T = 0;   // chunks and tiles this CTA has produced (over every pass)
-  int w_issued = 0;        // W tiles requested (passes begun)
+  const int G = (int)gridDim.x;
+  const int n_pass = Hp / PW;
+  // every bias once (Hp <= 1024)
+  for (int i = tid; i < Hp; i += PT) bsm[i] = b[i];
+  __syncthreads();
 
-  for (int hb = 0, pass = 0; hb < Hp; hb += PW, ++pass) {
-    // this CTA's first tile in the pass
-    const int first = (int)(((long long)blockIdx.x - (long long)pass * rot) % G + G) % G;
-    // the pass's W tile (rows hb .. hb + PW - 1, every 64-site chunk) by TMA
-    // in the 128-byte swizzled layout the MMA descriptors expect; the MMA
-    // issuer waits for it
-    ++w_issued;
-    if (tid == 0) {
-      mbar_expect_tx(w_full, (uint32_t)(nk * PW * 128));
-      for (int kc = 0; kc < nk; ++kc)
-        tma_load_2d(&wmap, smem_u32(Bt + (size_t)kc * PW * 128), kc * KC, hb, w_full);
-    }
-    for (int i = tid; i < PW; i += PT) bsm[i] = b[hb + i];
-    fence_async_smem();
-    __syncthreads();
-    const uint32_t g0 = g, T0 = T;
-    if (warp < 4) {
-      // ---- producers
-      uint32_t gg = g0;
-      for (int t = first; t < n_tiles && !*abort_flag; t += G) {
+  if (warp < 4) {
+    // ---- producers
+    uint32_t gg = 0;
+    for (int pass = 0; pass < n_pass && !*abort_flag; ++pass) {
+      for (int t = first_tile(pass, n_tiles, G); t < n_tiles && !*abort_flag; t += G) {
         const int w = t * GT + tid;
         const int src = w < n ? (parents ? parents[w] : w) : 0;
         // the walker's spin words of up to 8 chunks at once (one load latency
@@ -323,14 +321,32 @@ rbm_theta_persist(const uint64_t *cfg, const int *parents, int NW, int n, int Np
           mbar_arrive(a_full + s);
         }
       }
-    } else if (warp == 8) {
-      // ---- the MMA issuer
-      const int lane = tid & 31;
-      uint32_t gg = g0, TT = T0;
-      bool ok = true;
-      if (lane == 0) ok = bwait(w_full, (uint32_t)pass, abort_flag);
+    }
+  } else if (warp == 8) {
+    // ---- the MMA issuer, which also brings in each pass's W tile (by TMA,
+    //      in the 128-byte swizzled layout the MMA descriptors expect) as soon
+    //      as the previous pass's MMAs have finished reading the last one
+    const int lane = tid & 31;
+    uint32_t gg = 0, TT = 0;
+    int w_issued = 0;
+    bool ok = true;
+    for (int pass = 0; pass < n_pass && ok; ++pass) {
+      const int hb = pass * PW;
+      if (lane == 0) {
+        if (pass > 0) {
+          mma_commit(w_free);
+          ok = bwait(w_free, (uint32_t)(pass - 1), abort_flag);
+        }
+        if (ok) {
+          mbar_expect_tx(w_full, (uint32_t)(nk * PW * 128));
+          for (int kc = 0; kc < nk; ++kc)
+            tma_load_2d(&wmap, smem_u32(Bt + (size_t)kc * PW * 128), kc * KC, hb, w_full);
+          ++w_issued;
+          ok = bwait(w_full, (uint32_t)pass, abort_flag);
+        }
+      }
       ok = __shfl_sync(0xffffffffu, ok, 0);
-      for (int t = first; t < n_tiles && ok; t += G, ++TT) {
+      for (int t = first_tile(pass, n_tiles, G); t < n_tiles && ok; t += G, ++TT) {
         const uint32_t buf = TT & 1u, use = TT >> 1;
         for (int kc = 0; kc < nk; ++kc, ++gg) {
           const uint32_t s = gg & 1u, u = gg >> 1;
@@ -354,13 +370,27 @@ rbm_theta_persist(const uint64_t *cfg, const int *parents, int NW, int n, int Np
           __syncwarp();
         }
       }
-    } else {
-      // ---- epilogue: theta = accumulator + b
-      const int q = warp - 4, lane = tid & 31;
-      unsigned char *S0 = St + (size_t)q * 2 * STAGE_BYTES;
-      uint32_t nst = 0;   // boxes this warp has stored in the pass
-      uint32_t TT = T0;
-      for (int t = first; t < n_tiles && !*abort_flag; t += G, ++TT) {
+    }
+    if (lane == 0) {
+      // every MMA this warp issued and, after a wait that ran out, the last
+      // W copies finish (bounded) before the CTA frees its memory
+      mma_commit(fin);
+      for (uint32_t it = 0; it < WAIT_LIMIT; ++it)
+        if (mbar_try_wait(fin, 0u)) break;
+      if (!ok && w_issued > 0)
+        for (uint32_t it = 0; it < WAIT_LIMIT; ++it)
+          if (mbar_try_wait(w_full, (uint32_t)(w_issued - 1) & 1u)) break;
+    }
+    __syncwarp();
+  } else {
+    // ---- epilogue: theta = accumulator + b
+    const int q = warp - 4, lane = tid & 31;
+    unsigned char *S0 = St + (size_t)q * 2 * STAGE_BYTES;
+    uint32_t nst = 0;   // boxes this warp has stored
+    uint32_t TT = 0;
+    for (int pass = 0; pass < n_pass && !*abort_flag; ++pass) {
+      const int hb = pass * PW;
+      for (int t = first_tile(pass, n_tiles, G); t < n_tiles && !*abort_flag; t += G, ++TT) {
         const uint32_t buf = TT & 1u, use = TT >> 1;
         if (!bwait(acc_full + buf, use, abort_flag)) break;
         fence_after();
@@ -378,7 +408,7 @@ rbm_theta_persist(const uint64_t *cfg, const int *parents, int NW, int n, int Np
           __syncwarp();
 #pragma unroll
           for (int j = 0; j < 8; ++j) {
-            const float4 bj = *reinterpret_cast<const float4 *>(bsm + c0 + 4 * j);
+            const float4 bj = *reinterpret_cast<const float4 *>(bsm + hb + c0 + 4 * j);
             *reinterpret_cast<float4 *>(sw_chunk(S, lane, j)) =
                 make_float4(__uint_as_float(v[4 * j]) + bj.x, __uint_as_float(v[4 * j + 1]) + bj.y,
                             __uint_as_float(v[4 * j + 2]) + bj.z, __uint_as_float(v[4 * j + 3]) + bj.w);
@@ -394,38 +424,14 @@ rbm_theta_persist(const uint64_t *cfg, const int *parents, int NW, int n, int Np
         fence_before();
         mbar_arrive(acc_free + buf);
       }
-      // the staging boxes are read out before the pass ends (the next pass
-      // reuses them)
-      if (lane == 0) bulk_wait_read0();
-      __syncwarp();
     }
-    // tiles of this pass: the same count in every role
-    uint32_t my = 0;
-    for (int t = first; t < n_tiles; t += G) ++my;
-    g = g0 + my * (uint32_t)nk;
-    T = T0 + my;
-    fence_before();
-    __syncthreads();   // every role done with the pass before its W tile is replaced
-    fence_after();
-    if (*abort_flag) break;
+    // the output boxes in flight have landed before the CTA leaves
+    if (lane == 0) bulk_wait_all();
+    __syncwarp();
   }
-  if (*abort_flag) {
-    if (tid == 0) {
-      atomicOr(status, 8);
-      // the MMAs committed last: one more bounded wait before the TMEM is freed
-      if (T > 0)
-        for (uint32_t it = 0; it < WAIT_LIMIT; ++it)
-          if (mbar_try_wait(acc_full + ((T - 1) & 1u), ((T - 1) >> 1) & 1u)) break;
-      // and the last W tile's copies have landed before the shared memory goes
-      if (w_issued > 0)
-        for (uint32_t it = 0; it < WAIT_LIMIT; ++it)
-          if (mbar_try_wait(w_full, (uint32_t)(w_issued - 1) & 1u)) break;
-    }
-  }
-  // the output boxes in flight have landed before the CTA leaves
-  if (warp >= 4 && warp < 8 && (tid & 31) == 0) bulk_wait_all();
   fence_before();
   __syncthreads();
+  if (*abort_flag && tid == 0) atomicOr(status, 8);
   if (warp == 0) tmem_dealloc(tmem, ncols);
 }
 
@@ -434,14 +440,14 @@ rbm_theta_persist(const uint64_t *cfg, const int *parents, int NW, int n, int Np
 int theta_pass_width(int Np, int Hp) {
   for (int pw = 256; pw >= 64; pw /= 2) {
     if (Hp % pw) continue;
-    const size_t bytes = 1024 + (size_t)(Np / KC) * pw * 128 + 2 * GT * 128 + 8 * STAGE_BYTES + 1024 + 128;
+    const size_t bytes = 1024 + (size_t)(Np / KC) * pw * 128 + 2 * GT * 128 + 8 * STAGE_BYTES + 4096 + 128;
     if (bytes <= (size_t)227 * 1024) return pw;
   }
   return 0;
 }
 
 size_t theta_persist_smem(int Np, int PW) {
-  return 1024 + (size_t)(Np / KC) * PW * 128 + 2 * GT * 128 + 8 * STAGE_BYTES + 1024 + 128;
+  return 1024 + (size_t)(Np / KC) * PW * 128 + 2 * GT * 128 + 8 * STAGE_BYTES + 4096 + 128;
 }
 
 // cuTensorMapEncodeTiled from the driver, looked up once (no link against
@@ -492,7 +498,7 @@ cudaError_t launch_rbm_theta(const RbmTables &r, int n, const void *cfg, const i
                              int NW, float *theta, int *status, cudaStream_t s) {
   const int PW = theta_pass_width(r.Np, r.Hp);
   CUtensorMap tm, wm;
-  if (PW > 0 && n > 0 && theta_tensor_map(theta, n, r.Hp, &tm) &&
+  if (PW > 0 && n > 0 && r.Hp <= 1024 && theta_tensor_map(theta, n, r.Hp, &tm) &&
       w_tensor_map(r.W, r.Hp, r.Np, PW, &wm)) {
     const size_t smem = theta_persist_smem(r.Np, PW);
     // the kernel's shared-memory limit (its largest size) and the SM count,
