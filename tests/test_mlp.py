@@ -180,9 +180,14 @@ def _mlp_systems(O):
 @pytest.mark.gpu
 def test_mlp_local_energy_matches_oracle(oracle):
     """e_L through gfmc_local_energy (tcgen05 second layer over the 128-move
-    tiles): within 2e-3 of the rate scale sum |r| per walker (float32, and
-    bf16 first-layer activations whose rounding may differ by one unit from
-    the float64 oracle's), 1e-4 on average."""
+    tiles) against the float64 oracle, relative to the rate scale sum |r| per
+    walker.  The first layer's tanh is the hardware approximation (relative
+    error up to 2^-11) and its output is rounded to bf16 (step 2^-8), so about
+    one activation in eight near a rounding boundary lands one bf16 unit away
+    from the oracle's: most walkers carry a few such units.  Measured on these
+    systems: median 5e-7 .. 7e-6, at most 10 % of walkers above 1e-4, maximum
+    1.5e-3.  Asserted: median 3e-5, at most 30 % above 1e-4, 1e-4 on average,
+    every walker within 2e-3."""
     O = oracle
     P._lib.load()
     for name, H, G, m, g, cfg in _mlp_systems(O):
@@ -195,6 +200,8 @@ def test_mlp_local_energy_matches_oracle(oracle):
         err = np.abs(el - ref) / scale
         assert np.all(err <= 2e-3), (name, err.max())
         assert err.mean() <= 1e-4, (name, err.mean())
+        assert np.median(err) <= 3e-5, (name, np.median(err))
+        assert (err > 1e-4).mean() <= 0.3, (name, (err > 1e-4).mean())
         assert eng.status() == 0, name
 
 
