@@ -254,6 +254,7 @@ __device__ __forceinline__ void flip_one(const DevModel<T> &m, const DevGuide<T>
     const bool ua = sa > T(0);
     if (g.ti) {
       const int ca = g.tE_off - g.tq[a];
+#pragma unroll 8
       for (int k = lane; k < m.N; k += 32) {
         const T sk = S[k];
         S[k] = sk * g.tE[g.tq[k] + ca + ((sk > T(0)) != ua)];
@@ -298,6 +299,7 @@ __device__ __forceinline__ void flip_pair(const DevModel<T> &m, const DevGuide<T
   if (g.ti) {
     const int qa = g.tq[a], qb = g.tq[b];
     const int ca = g.tE_off - qa, cb = g.tE_off - qb;
+#pragma unroll 8
     for (int k = lane; k < m.N; k += 32) {
       const T sk = S[k];
       const bool uk = sk > T(0);
