@@ -170,14 +170,17 @@ def test_rbm_mixed_run_matches_exact_energy():
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("N,H,n", [(16, 40, 300), (256, 512, 1024), (100, 700, 257),
-                                   (256, 512, 65613), (100, 700, 37893)])
+                                   (256, 512, 65613), (100, 700, 37893), (432, 432, 20011),
+                                   (600, 256, 3001)])
 def test_rbm_theta_gemm_on_tensor_cores(N, H, n):
     """theta = b + W s from the tcgen05 kernel (bf16 inputs, f32 accumulation)
     equals the float64 product of the same bf16 weights to float32 rounding;
     padded hidden units are exactly zero; the parent map is honoured.  The
     two large populations give every CTA several tiles in two and three
     passes, with the per-pass rotation of the tile assignment (513 and 297
-    tiles over the SMs)."""
+    tiles over the SMs); the 432-site case takes passes of 128 hidden
+    columns over 7 site chunks, the 600-site case 10 site chunks (spin words
+    loaded per chunk past the eighth)."""
     import torch
     P._lib.load()
     e = P.chain(N).edges
