@@ -18,6 +18,8 @@
 // two-stage ring, two TMEM accumulators) is the one launched whenever a
 // pass's W tile fits in shared memory; the one-CTA-per-tile kernel above
 // takes the rest.
+#include <atomic>
+
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
@@ -453,16 +455,15 @@ size_t theta_persist_smem(int Np, int PW) {
 // cuTensorMapEncodeTiled from the driver, looked up once (no link against
 // the driver library); nullptr when unavailable.
 PFN_cuTensorMapEncodeTiled encode_tiled() {
-  static PFN_cuTensorMapEncodeTiled fn = nullptr;
-  static bool tried = false;
-  if (!tried) {
-    tried = true;
+  // (a function-local static: initialised once, also under concurrent callers)
+  static const PFN_cuTensorMapEncodeTiled fn = []() -> PFN_cuTensorMapEncodeTiled {
     void *p = nullptr;
     cudaDriverEntryPointQueryResult q;
     if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
         q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled>(p);
-  }
+      return reinterpret_cast<PFN_cuTensorMapEncodeTiled>(p);
+    return nullptr;
+  }();
   return fn;
 }
 
@@ -503,17 +504,19 @@ cudaError_t launch_rbm_theta(const RbmTables &r, int n, const void *cfg, const i
     const size_t smem = theta_persist_smem(r.Np, PW);
     // the kernel's shared-memory limit (its largest size) and the SM count,
     // once per device
-    static int sms_of[64] = {0};
+    // (several host threads may launch at once: the per-device entries are
+    // atomics, and a race only repeats the idempotent attribute calls)
+    static std::atomic<int> sms_of[64];
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    int sms = (dev >= 0 && dev < 64) ? sms_of[dev] : 0;
+    int sms = (dev >= 0 && dev < 64) ? sms_of[dev].load(std::memory_order_acquire) : 0;
     if (sms == 0) {
       e = cudaFuncSetAttribute(rbm_theta_persist, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                227 * 1024);
       if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
       if (e != cudaSuccess) return e;
-      if (dev >= 0 && dev < 64) sms_of[dev] = sms;
+      if (dev >= 0 && dev < 64) sms_of[dev].store(sms, std::memory_order_release);
     }
     const int tiles = (n + GT - 1) / GT;
     const int grid = tiles < sms ? tiles : sms;
