@@ -790,8 +790,9 @@ def main():
     e0 = eng.local_energy()
     alw = float((-e0).mean().item())
     stream = torch.cuda.current_stream()
-    logG = torch.empty(1, dtype=torch.float64, device=dev)
-    Es = torch.empty(1, dtype=torch.float64, device=dev)
+    # log G and E_n of a step side by side: the e2e leg reads both in one copy
+    lgE = torch.empty(2, dtype=torch.float64, device=dev)
+    logG, Es = lgE[0:1], lgE[1:2]
     key = P.PRNGKey(1000 + rank)
     # warm-up: equilibrate (also refines alw)
     wk = max(args.warmup, 3)
@@ -857,8 +858,7 @@ def main():
                                        eng._ptr(eng.cfg_tmp), null, null, null, eng._stream()),
                      "gfmc_gather")
         packed_h.copy_(eng.cfg_tmp, non_blocking=True)
-        out_h[0:1].copy_(logG, non_blocking=True)
-        out_h[1:2].copy_(Es, non_blocking=True)
+        out_h.copy_(lgE, non_blocking=True)
         stream.synchronize()
     t_e2e = time.perf_counter() - t0
     if world > 1:

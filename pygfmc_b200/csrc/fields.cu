@@ -15,10 +15,11 @@
 // * x (+-1, or an occupation 0..n_max) is an int8, so every digit's product
 //   I_d[w, k] = sum_p x_p j_d[k, p] is exact in int32 (tcgen05.mma
 //   kind::i8, s8 x s8 -> s32);
-// * the epilogue combines the digits from the least significant one,
-//   acc = I_d + acc / 128 in float64 (each step exact until the bits run
-//   past 53; about 1.5 ulp in all), F = acc S / 128 -- closer to the exact
-//   sum than a sequential float64 accumulation of the N terms.
+// * the epilogue combines the digits exactly in int64, four at a time, and
+//   the two groups of the float64 build with one rounding (combine_digits),
+//   F = acc S / 128 -- closer to the exact sum than a sequential float64
+//   accumulation of the N terms (and two int-to-float64 conversions per
+//   output instead of eight).
 //
 // A CTA (8 warps) takes 128 walkers (TMEM lanes) and 256 / D output sites;
 // the B operand holds all D digits of those sites (row d (256 / D) + j), so
@@ -29,6 +30,7 @@
 // into the B tile (256 x 128); thread 0 issues four MMAs of K = 32 per chunk
 // and commits to the stage's mbarrier.  Every wait is bounded: one that runs
 // out sets status bit ST_TIMEOUT, and the CTA still frees its TMEM.
+#include <atomic>
 #include <cstdint>
 
 #include "engine.cuh"
@@ -103,6 +105,24 @@ __device__ __forceinline__ uint4 x_chunk(const unsigned char *crow, uint64_t wd,
         if (p0 + 4 * e + b >= N) q[e] &= ~(0xFFu << (8 * b));
   }
   return make_uint4(q[0], q[1], q[2], q[3]);
+}
+
+// sum_d I_d 128^-d of output e from its D digit products: four digits at a
+// time exactly in int64 (|I_d| < 2^23, so each group stays far below 2^53),
+// then one rounding when the two groups of the float64 build meet (the
+// float32 build's four digits give the sum exactly).
+template <int D>
+__device__ __forceinline__ double combine_digits(const int32_t (&I)[D][4], int e) {
+  long long hi = I[0][e];
+#pragma unroll
+  for (int d = 1; d < 4; ++d) hi = hi * 128 + I[d][e];
+  if (D == 8) {
+    long long lo = I[4 % D][e];
+#pragma unroll
+    for (int d = 5; d < 8; ++d) lo = lo * 128 + I[d % D][e];
+    return fma((double)lo, 0x1p-28, (double)hi) * 0x1p-21;
+  }
+  return (double)hi * 0x1p-21;
 }
 
 template <typename T, int FAM, int D>
@@ -223,9 +243,7 @@ __global__ void __launch_bounds__(FT, 1) fields_i8_kernel(DevModel<T> m, DevGuid
       T v[4];
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
-        double acc = (double)I[D - 1][e];
-#pragma unroll
-        for (int d = D - 2; d >= 0; --d) acc = (double)I[d][e] + acc * (1.0 / 128.0);
+        const double acc = combine_digits<D>(I, e);
         const int k = k0 + j0 + e;
         v[e] = (T)(acc * scale);
         if (FAM == SPIN_HALF) {
@@ -257,11 +275,243 @@ __global__ void __launch_bounds__(FT, 1) fields_i8_kernel(DevModel<T> m, DevGuid
   if (warp == 0) tmem_dealloc(tmem, BN);
 }
 
+
+// ---------------------------------------------------------------------------
+// Persistent version (when the digit rows of a site tile fit in shared memory
+// beside the A ring): a CTA keeps one site tile's digit rows resident and
+// walks its walker tiles with 21 warps in three roles:
+//   warps 0-3  expand the walkers' configurations (one row per thread) into a
+//              two-stage ring of int8 A chunks;
+//   warp 20    issues the four K = 32 MMAs of each chunk (lane 0) into one of
+//              two TMEM accumulators (256 columns each);
+//   warps 4-19 form F and the factors of the other accumulator (the same
+//              digit recombination and exp as the kernel above, so the
+//              outputs are identical), four warps per TMEM lane quarter, a
+//              quarter of the tile's sites each: the float64 recombination
+//              and exp of every output are the kernel's work, and they need
+//              the warps to hide their latency.
+// Every wait is bounded; a wait that runs out stops every role at its next
+// wait, sets ST_TIMEOUT, and the CTA frees its TMEM after its MMAs end.
+constexpr int PEW = 16;              // epilogue warps
+constexpr int PFT = (5 + PEW) * 32;
+
+__device__ __forceinline__ bool pwait(uint64_t *bar, uint32_t k, volatile int *abort_flag) {
+  for (uint32_t it = 0; it < WAIT_LIMIT; ++it) {
+    if (mbar_try_wait(bar, k & 1u)) return true;
+    if ((it & 1023u) == 0 && *abort_flag) return false;
+  }
+  *abort_flag = 1;
+  return false;
+}
+__device__ __forceinline__ void pbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__host__ __device__ inline size_t persist_smem(int Kp) {
+  return 1024 + (size_t)(Kp / KCH) * BN * KCH + 2 * (size_t)MT * KCH + 128;
+}
+
+template <typename T, int FAM, int D>
+__global__ void __launch_bounds__(PFT, 1)
+fields_i8_persist(DevModel<T> m, DevGuide<T> g, int n, const void *cfg_v, T *out, int *status,
+                  int n_st, int cps) {
+  constexpr int NT = BN / D;   // output sites per site tile
+  extern __shared__ unsigned char dsm[];
+  unsigned char *base = (unsigned char *)(((uintptr_t)dsm + 1023) & ~(uintptr_t)1023);
+  const int N = m.N, Kp = g.jdig_kp, nk = Kp / KCH;
+  unsigned char *Bs = base;                               // nk x BN rows x 128 bytes, resident
+  unsigned char *As = Bs + (size_t)nk * BN * KCH;         // 2 stages x MT rows x 128 bytes
+  uint64_t *bar = reinterpret_cast<uint64_t *>(As + 2 * MT * KCH);
+  uint64_t *a_full = bar, *a_free = bar + 2, *acc_full = bar + 4, *acc_free = bar + 6;
+  uint64_t *fin = bar + 8;
+  uint32_t *slot = reinterpret_cast<uint32_t *>(bar + 9);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(slot + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int cfgb = FAM == SPIN_HALF ? ((N + 63) / 64) * 8 : ((N + 15) / 16) * 16;
+  const unsigned char *cfg = reinterpret_cast<const unsigned char *>(cfg_v);
+  const int y = (int)blockIdx.x % n_st, c0 = (int)blockIdx.x / n_st;   // site tile, first walker tile
+  const int k0 = y * NT;
+  const int n_wt = (n + MT - 1) / MT;
+
+  if (warp == 0) tmem_alloc(slot, 2 * BN);
+  if (tid == 0) {
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(a_full + i, MT);
+      mbar_init(a_free + i, 1);
+      mbar_init(acc_full + i, 1);
+      mbar_init(acc_free + i, PEW * 32);
+    }
+    mbar_init(fin, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  // the site tile's digit rows of every chunk (the digit buffer is padded to
+  // whole chunks and tiles)
+  const int8_t *Bg = g.jdig + (size_t)y * BN * Kp;
+  for (int i = tid; i < nk * BN * 8; i += PFT) {
+    const int kc = i / (BN * 8), rem = i - kc * (BN * 8), r = rem >> 3, c = rem & 7;
+    cp16(sw_chunk(Bs + (size_t)kc * BN * KCH, r, c), Bg + (size_t)r * Kp + (size_t)kc * KCH + 16 * c);
+  }
+  cp_commit();
+  cp_wait<0>();
+  fence_async_smem();
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = *slot;
+
+  if (warp < 4) {
+    // ---- producers: walker row tid of each tile, 128 sites per chunk
+    uint32_t gg = 0;
+    for (int t = c0; t < n_wt && !*abort_flag; t += cps) {
+      const int w = t * MT + tid;
+      const unsigned char *crow = w < n ? cfg + (size_t)w * cfgb : nullptr;
+      for (int kc = 0; kc < nk; ++kc, ++gg) {
+        const uint32_t st = gg & 1u, u = gg >> 1;
+        if (u >= 1 && !pwait(a_free + st, u - 1, abort_flag)) break;
+        unsigned char *A = As + (size_t)st * MT * KCH;
+        const int p0 = kc * KCH;
+        uint64_t wd0 = 0, wd1 = 0;
+        if (FAM == SPIN_HALF && crow != nullptr) {
+          if (p0 < N) wd0 = reinterpret_cast<const uint64_t *>(crow)[p0 >> 6];
+          if (p0 + 64 < N) wd1 = reinterpret_cast<const uint64_t *>(crow)[(p0 >> 6) + 1];
+        }
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+          *reinterpret_cast<uint4 *>(sw_chunk(A, tid, c)) =
+              x_chunk<FAM>(crow, c < 4 ? wd0 : wd1, N, p0 + 16 * c);
+        fence_async_smem();
+        pbar_arrive(a_full + st);
+      }
+    }
+  } else if (warp == 4 + PEW) {
+    // ---- the MMA issuer (lane 0 waits and issues, the warp stays converged)
+    uint32_t gg = 0, TT = 0;
+    bool ok = true;
+    for (int t = c0; t < n_wt && ok; t += cps, ++TT) {
+      const uint32_t buf = TT & 1u, use = TT >> 1;
+      for (int kc = 0; kc < nk; ++kc, ++gg) {
+        const uint32_t st = gg & 1u, u = gg >> 1;
+        if (lane == 0)
+          ok = pwait(a_full + st, u, abort_flag) &&
+               (kc != 0 || use < 1 || pwait(acc_free + buf, use - 1, abort_flag));
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (!ok) break;
+        fence_after();
+        if (lane == 0) {
+          const uint32_t a0 = smem_u32(As + (size_t)st * MT * KCH);
+          const uint32_t b0 = smem_u32(Bs + (size_t)kc * BN * KCH);
+#pragma unroll
+          for (int kk = 0; kk < KCH / 32; ++kk)
+            mma_i8(tmem + buf * BN, sw128_desc(a0 + 32u * kk), sw128_desc(b0 + 32u * kk),
+                   (kc > 0 || kk > 0) ? 1u : 0u);
+          mma_commit(a_free + st);
+          if (kc == nk - 1) mma_commit(acc_full + buf);
+        }
+        __syncwarp();
+      }
+    }
+    if (lane == 0) {
+      // every MMA of the CTA has ended (bounded) before the TMEM is freed
+      mma_commit(fin);
+      for (uint32_t it = 0; it < WAIT_LIMIT; ++it)
+        if (mbar_try_wait(fin, 0u)) break;
+    }
+    __syncwarp();
+  } else {
+    // ---- epilogue: F and the factors of one accumulator
+    const int ew = warp - 4, q = ew & 3, part = ew >> 2;
+    const double scale = g.jdig_scale;   // S / 128
+    uint32_t TT = 0;
+    for (int t = c0; t < n_wt && !*abort_flag; t += cps, ++TT) {
+      const uint32_t buf = TT & 1u, use = TT >> 1;
+      if (!pwait(acc_full + buf, use, abort_flag)) break;
+      fence_after();
+      const int w = t * MT + 32 * q + lane;
+      const uint32_t trow = tmem + ((uint32_t)(32 * q) << 16) + buf * BN;
+      // the tile's NT sites lie in one 64-bit spin word
+      uint64_t wb = 0;
+      if (FAM == SPIN_HALF && w < n && k0 < N)
+        wb = reinterpret_cast<const uint64_t *>(cfg + (size_t)w * cfgb)[k0 >> 6];
+      const bool vec = (N % 4) == 0;
+      for (int j0 = part * (NT / 4); j0 < (part + 1) * (NT / 4); j0 += 4) {
+        int32_t I[D][4];
+#pragma unroll
+        for (int d = 0; d < D; ++d) tmem_ld4_async(trow + (uint32_t)(d * NT + j0), I[d]);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        T v[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const double acc = combine_digits<D>(I, e);
+          const int k = k0 + j0 + e;
+          v[e] = (T)(acc * scale);
+          if (FAM == SPIN_HALF) {
+            const T x = ((wb >> (k & 63)) & 1ull) ? T(1) : T(-1);
+            const T hk = (g.has_h && k < N) ? g.h[k] : T(0);
+            v[e] = x * math_exp(T(-2) * x * (v[e] + hk));
+          }
+        }
+        const int kb = k0 + j0;
+        if (w < n) {
+          T *o = out + (size_t)w * N + kb;
+          if (vec && kb + 3 < N) {
+            if (sizeof(T) == 8) {
+              reinterpret_cast<double2 *>(o)[0] = make_double2((double)v[0], (double)v[1]);
+              reinterpret_cast<double2 *>(o)[1] = make_double2((double)v[2], (double)v[3]);
+            } else {
+              *reinterpret_cast<float4 *>(o) = make_float4((float)v[0], (float)v[1], (float)v[2], (float)v[3]);
+            }
+          } else {
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+              if (kb + e < N) o[e] = v[e];
+          }
+        }
+      }
+      fence_before();
+      pbar_arrive(acc_free + buf);
+    }
+  }
+  fence_before();
+  __syncthreads();
+  if (*abort_flag && tid == 0) atomicOr(status, ST_TIMEOUT);
+  if (warp == 0) tmem_dealloc(tmem, 2 * BN);
+}
+
 constexpr size_t I8_SMEM = 1024 + 2 * (size_t)STAGE + 32;
 
 template <typename T, int D>
 cudaError_t launch_d(const DevModel<T> &m, const DevGuide<T> &g, int n, const void *cfg, T *out,
                      int *status, cudaStream_t s) {
+  const size_t psmem = persist_smem(g.jdig_kp);
+  if (psmem <= (size_t)227 * 1024) {
+    // persistent: CTAs per site tile from the SM count (cached per device;
+    // a race between host threads only repeats the idempotent calls)
+    auto pk = m.family == SPIN_HALF ? fields_i8_persist<T, SPIN_HALF, D>
+                                    : fields_i8_persist<T, BOSE_HUBBARD, D>;
+    static std::atomic<int> sms_of[64];
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    int sms = (dev >= 0 && dev < 64) ? sms_of[dev].load(std::memory_order_acquire) : 0;
+    if (sms == 0) {
+      e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      if (e != cudaSuccess) return e;
+      if (dev >= 0 && dev < 64) sms_of[dev].store(sms, std::memory_order_release);
+    }
+    // at least 120 KB: one CTA per SM, so that no two CTAs contend for the
+    // 512 TMEM columns each allocates
+    const size_t lsmem = psmem > (size_t)120 * 1024 ? psmem : (size_t)120 * 1024;
+    e = cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem);
+    if (e != cudaSuccess) return e;
+    const int NT = BN / D;
+    const int n_st = (m.N + NT - 1) / NT, n_wt = (n + MT - 1) / MT;
+    int cps = sms / n_st;
+    if (cps < 1) cps = 1;
+    if (cps > n_wt) cps = n_wt;
+    pk<<<n_st * cps, PFT, lsmem, s>>>(m, g, n, cfg, out, status, n_st, cps);
+    return cudaGetLastError();
+  }
   auto kern = m.family == SPIN_HALF ? fields_i8_kernel<T, SPIN_HALF, D>
                                     : fields_i8_kernel<T, BOSE_HUBBARD, D>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)I8_SMEM);

@@ -6,7 +6,9 @@ jastrow_bose_hubbard.py:172-286): the 16 x 16 all-pairs Jastrow of the
 benchmark workload, a 6 x 6 torus (N off the kernel's 16-site chunks and
 128-site tiles), a 300-site random dense guide with a field (three site
 tiles), and a 1040-site dense Bose guide (configurations too large to stage
-per block).  Walker counts are not multiples of the 64-walker tile.  Float64
+per block; its digit rows too wide for the persistent kernel, so the
+one-tile-per-CTA kernel runs).  The 20011-walker population gives the
+persistent kernel's CTAs several walker tiles each.  Walker counts are not multiples of the 64-walker tile.  Float64
 build within 1e-12 of the rate scale; float32 build within 3e-4 (float32
 fields summed over up to 1040 partners in the exponent)."""
 import numpy as np
@@ -28,14 +30,14 @@ def _torus_longrange(L, amp):
 
 def _spin_cases(O):
     out = []
-    for L, amp, n in ((16, 0.3, 1000), (6, 0.25, 77)):
+    for L, amp, n in ((16, 0.3, 1000), (6, 0.25, 77), (16, 0.3, 20011)):
         lat, pairs, beta = _torus_longrange(L, amp)
         H = P.SpinHalf.create(lat.edges, J_x=-1.0, J_y=-1.0, J_z=1.0, dtype=np.float64)
         m = O.spin_half(lat.edges, J_x=-1.0, J_y=-1.0, J_z=1.0)
         G = P.JastrowSpinHalf(lat.N, pairs, beta=beta)
         g = oracle_guide(O, G, m)
         cfg = P.prepare_walkers_sz(n, lat.N, P.PRNGKey(L), sz=0).config
-        out.append((f"square{L}_longrange", H, G, m, g, cfg))
+        out.append((f"square{L}_longrange_{n}", H, G, m, g, cfg))
     N = 300
     rng = np.random.default_rng(3)
     e = P.chain(N).edges
