@@ -1,10 +1,17 @@
 """The plain Jastrow-guided method as the judge of the learned guides: a
 guide trained on the run's own walkers (RBM on the periodic 4 x 4 Heisenberg
 lattice, MLP on a 6-site Bose-Hubbard ring) must give the Jastrow-guided
-run's energy within two combined error bars (blocked jackknife at the
-largest window) and a lower local-energy variance than the Jastrow guide --
-what the learned guide gains over the method without it.  Both are also
-checked against exact diagonalisation."""
+run's energy within its error bars (blocked jackknife at the largest window)
+and a lower local-energy variance than the Jastrow guide -- what the learned
+guide gains over the method without it.  Both are also checked against exact
+diagonalisation.
+
+The agreement is asserted at three combined standard errors.  Two unbiased
+estimates from one realisation differ by more than two combined errors
+about 5 % of the time (more with jackknife-estimated errors), and the
+training's float atomics make every realisation a new draw, so a 2-sigma
+assertion would fail that often with nothing wrong; 3 sigma fails about
+0.3 % of the time.  The long sigma study reports the 2-sigma criterion."""
 import itertools
 
 import numpy as np
@@ -26,7 +33,7 @@ def _production(w, H, G, tau, precision, steps=2000, p=32):
 
 def _assert_judged(learned, jastrow, E0, n_sites):
     (El, sl, vl), (Ej, sj, vj) = learned, jastrow
-    assert abs(El - Ej) <= 2.0 * np.hypot(sl, sj), (learned, jastrow)
+    assert abs(El - Ej) <= 3.0 * np.hypot(sl, sj), (learned, jastrow)
     assert vl < vj, (learned, jastrow)
     for E, s in ((El, sl), (Ej, sj)):
         assert abs(E - E0) <= max(4.0 * s, 2e-3 * abs(E0)), (E, s, E0)
