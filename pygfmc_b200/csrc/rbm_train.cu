@@ -11,6 +11,9 @@
 //     base rows (w):    U = -g_w R_w tanh(theta_w),  V = s_w,  R_w = sum_s r_ws
 //   dL/db = sum_r U_r,   dL/da_i = sum_(w,s) g_w r_ws (-2 s_wi) [i flipped by s].
 //
+// Up to 256 padded sites the contraction runs in float32 without row tiles
+// (rbm_grad_acc_kernel, below); wider lattices use the tensor-core
+// contraction:
 // rbm_grad_kernel: one CTA per (128-unit hidden tile, block of walkers).
 // Each 64-row chunk: 64 threads decode the rows (sites, coefficient, spins)
 // into shared memory; every thread then produces its hidden unit's 64 values
@@ -414,6 +417,114 @@ __global__ void __launch_bounds__(3 * TT, 1) rbm_grad_kernel(GradArgs g, const f
                  : "memory");
 }
 
+// ---- the gradient in float32 without row tiles (Np <= 256) -----------------------
+// Every slot row's V is its walker's spins with the move's sites flipped
+// (V_r = s_w + Delta_r, Delta_r = the record's y, z at sites i, j), and the
+// base row is -(sum of the slot coefficients) tanh(theta) against s_w, so
+//   dL/dW = sum_w ub_w s_w^T + sum_(w,s) T_ws Delta_ws^T,
+//   ub_w = sum_s c_ws (tanh theta'_ws - tanh theta_w),  T_ws = c_ws tanh theta'_ws:
+// the cancellation between a walker's base row and its slot rows happens in
+// float32 inside ub_w, before any rounding (the tensor-core contraction
+// below rounds U to bf16 first, which leaves dW about 1e-2 off at 256
+// sites).  A CTA takes 128 hidden units and a block of walkers; each of its
+// four groups of 128 threads (one unit per thread) holds theta, tanh theta
+// and ub of 16 walkers in registers and runs over the slots (each group from
+// its own starting slot), summing T Delta for the slot's two sites over its
+// walkers in registers and adding that into the CTA's float32 dW tile in
+// shared memory; after the slots, the rank-1 terms ub_w s_w^T go into the
+// tile (each thread its own sites, no atomics).  The tile goes into grad_W
+// at the end.
+constexpr int AG = 4;          // walker groups per CTA
+constexpr int AW = 16;         // walkers per thread per chunk
+constexpr int ACW = AG * AW;   // walkers per chunk
+
+__host__ __device__ inline size_t acc_smem(int Np, int NW) {
+  return 1024 + (size_t)Np * TT * 4 + (size_t)ACW * TT * 4 + (size_t)ACW * NW * 8;
+}
+
+__global__ void __launch_bounds__(AG * TT, 1) rbm_grad_acc_kernel(GradArgs g, const float4 *recs) {
+  extern __shared__ unsigned char dsm[];
+  unsigned char *base = (unsigned char *)(((uintptr_t)dsm + 1023) & ~(uintptr_t)1023);
+  const int Np = g.Np, N = g.N, NW = g.NW;
+  float *dWs = reinterpret_cast<float *>(base);                         // (Np, 128)
+  float *ubs = dWs + (size_t)Np * TT;                                   // (ACW, 128)
+  uint64_t *xs = reinterpret_cast<uint64_t *>(ubs + (size_t)ACW * TT);  // (ACW, NW)
+  const int tid = threadIdx.x, h = tid & (TT - 1), grp = tid / TT;
+  const int h0 = blockIdx.x * TT;
+  const int w0 = blockIdx.y * g.walkers_per_cta;
+  int w1 = w0 + g.walkers_per_cta;
+  if (w1 > g.n) w1 = g.n;
+  const int rows_per_w = g.n_off + 1, n_off = g.n_off;
+  for (int k = tid; k < Np * TT; k += AG * TT) dWs[k] = 0.0f;
+  __syncthreads();
+  float acc_b = 0.0f;
+  for (int c0 = w0; c0 < w1; c0 += ACW) {
+    // this thread's walkers: c0 + grp * AW + q
+    float th[AW], tt[AW], ub[AW];
+#pragma unroll
+    for (int q = 0; q < AW; ++q) {
+      const int w = c0 + grp * AW + q;
+      th[q] = w < w1 ? g.theta[(size_t)w * g.Hp + h0 + h] : 0.0f;
+      tt[q] = tanh_approx(th[q]);
+      ub[q] = 0.0f;
+    }
+    for (int k = tid; k < ACW * NW; k += AG * TT) {
+      const int wl = k / NW, wi = k - wl * NW;
+      xs[k] = c0 + wl < w1 ? g.cfg[(size_t)(c0 + wl) * NW + wi] : 0ull;
+    }
+    // slots, each group from its own starting point (the groups rarely add
+    // into the same sites at once)
+    for (int so = 0; so < n_off; ++so) {
+      int sl = so + grp * (n_off / AG);
+      if (sl >= n_off) sl -= n_off;
+      int i, j;
+      if (sl < g.n_hx) { i = sl; j = Np; }
+      else { const uint32_t pe = g.edge[sl - g.n_hx]; i = (int)(pe & 0xFFFF); j = (int)(pe >> 16); }
+      const float Wi = __bfloat162float(g.WT[(size_t)i * g.Hp + h0 + h]);
+      const float Wj = j < Np ? __bfloat162float(g.WT[(size_t)j * g.Hp + h0 + h]) : 0.0f;
+      float yi = 0.0f, yj = 0.0f;
+#pragma unroll
+      for (int q = 0; q < AW; ++q) {
+        const int w = c0 + grp * AW + q;
+        if (w < w1) {
+          const float4 rec = __ldg(recs + (size_t)w * rows_per_w + sl);
+          if (rec.x != 0.0f) {
+            const float t = tanh_approx(fmaf(rec.z, Wj, fmaf(rec.y, Wi, th[q])));
+            ub[q] = fmaf(rec.x, t - tt[q], ub[q]);
+            const float T = rec.x * t;
+            yi = fmaf(T, rec.y, yi);
+            yj = fmaf(T, rec.z, yj);
+          }
+        }
+      }
+      if (yi != 0.0f) atomicAdd(&dWs[(size_t)i * TT + h], yi);
+      if (j < Np && yj != 0.0f) atomicAdd(&dWs[(size_t)j * TT + h], yj);
+    }
+#pragma unroll
+    for (int q = 0; q < AW; ++q) {
+      ubs[(size_t)(grp * AW + q) * TT + h] = ub[q];
+      acc_b += ub[q];
+    }
+    __syncthreads();
+    // the rank-1 terms sum_w ub_w s_w over this chunk: thread (h, grp) owns
+    // the sites k = grp, grp + AG, ...
+    for (int k = grp; k < N; k += AG) {
+      float a = 0.0f;
+      for (int wl = 0; wl < ACW; ++wl) {
+        const float u = ubs[(size_t)wl * TT + h];
+        a += ((xs[(size_t)wl * NW + (k >> 6)] >> (k & 63)) & 1ull) ? u : -u;
+      }
+      dWs[(size_t)k * TT + h] += a;
+    }
+    __syncthreads();
+  }
+  for (int k = grp; k < Np; k += AG) {
+    const float v = dWs[(size_t)k * TT + h];
+    if (v != 0.0f) atomicAdd(&g.grad_W[(size_t)(h0 + h) * Np + k], v);
+  }
+  if (acc_b != 0.0f) atomicAdd(&g.grad_b[h0 + h], acc_b);
+}
+
 // Per-walker coefficients g_w = 2 omega_w (e_w - E) / sum omega and the
 // weighted mean and variance of e (one block; float64 sums in a fixed order).
 __global__ void train_coeff_kernel(int n, const double *e, const double *omega, float *gw,
@@ -528,9 +639,23 @@ cudaError_t launch_rbm_grad(const GradArgs &a, void *recs, int sms, cudaStream_t
   rbm_records_kernel<<<(a.n + 15) / 16, 256, sizeof(float) * a.Np, s>>>(a, (float4 *)recs);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
+  const int tiles = a.Hp / TT;
+  const size_t asmem = acc_smem(a.Np, a.NW);
+  if (a.Np <= 256 && asmem <= 227 * 1024) {
+    e = cudaFuncSetAttribute(rbm_grad_acc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)asmem);
+    if (e != cudaSuccess) return e;
+    int blocks = (sms + tiles - 1) / tiles;
+    if (blocks > a.n) blocks = a.n;
+    if (blocks < 1) blocks = 1;
+    GradArgs g = a;
+    g.walkers_per_cta = (a.n + blocks - 1) / blocks;
+    blocks = (a.n + g.walkers_per_cta - 1) / g.walkers_per_cta;
+    rbm_grad_acc_kernel<<<dim3(tiles, blocks), AG * TT, asmem, s>>>(g, (const float4 *)recs);
+    return cudaGetLastError();
+  }
   e = cudaFuncSetAttribute(rbm_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  const int tiles = a.Hp / TT;
   int blocks = (2 * sms + tiles - 1) / tiles;
   if (blocks > a.n) blocks = a.n;
   if (blocks < 1) blocks = 1;

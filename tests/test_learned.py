@@ -45,9 +45,11 @@ def test_oracle_gradient_matches_finite_differences():
 @pytest.mark.gpu
 @pytest.mark.parametrize("N,H,n", [(16, 32, 256), (64, 200, 384), (300, 96, 128), (432, 64, 96)])
 def test_device_gradient_matches_oracle(N, H, n):
-    """Up to 256 sites the gradient tile is double buffered in both operands;
-    above, one site buffer and two MMAs per K step (sites 0..255 and the
-    rest) -- the 300-site chain and the 432-site kagome lattice."""
+    """Up to 256 padded sites the contraction runs in float32 (the walker's
+    base row cancels against its slot rows before any rounding): dW within
+    1e-4 of float64 (measured 4e-6 .. 1.2e-5).  Above, the tensor-core
+    contraction with bf16 U (one site buffer and two MMAs per K step:
+    the 300-site chain and the 432-site kagome lattice): within 2e-2."""
     from oracle import learned
     P._lib.load()
     Hm, G = _system(N, H)
@@ -57,7 +59,8 @@ def test_device_gradient_matches_oracle(N, H, n):
     gW, gb, ga, (E, L) = eng.rbm_gradient()
     rE, rL, rW, rb, ra = learned.variance_loss_and_grads(Hm, G.W, G.b, G.a, x)
     assert abs(E - rE) < 1e-4 * abs(rE) and abs(L - rL) < 2e-3 * rL + 1e-6
-    for got, ref, tol in ((gW, rW, 2e-2), (gb, rb, 2e-2), (ga, ra, 1e-2)):
+    wtol = 1e-4 if N <= 256 else 2e-2
+    for got, ref, tol in ((gW, rW, wtol), (gb, rb, 2e-2), (ga, ra, 1e-2)):
         g = got.cpu().numpy().astype(np.float64)
         err = np.linalg.norm(g - ref) / np.linalg.norm(ref)
         assert err < tol, (err, tol)
