@@ -601,10 +601,103 @@ def _basis_index(configs, values, powers):
     return digit.astype(np.int64) @ powers
 
 
+def _value_digits(configs, values):
+    """Digit (position in values) of every site value of configs."""
+    return np.argmin(np.abs(np.asarray(configs, np.float64)[..., None] - np.asarray(values, np.float64)),
+                     axis=-1).astype(np.int64)
+
+
+def _batch_matrix(op, configs, values, powers):
+    """The matrix of this package's SpinHalf / BoseHubbard over the whole
+    basis at once (their get_rates formulas on every configuration, the
+    successor's index from the changed sites' digits); None for other
+    operators.  Equal element for element to the per-configuration build."""
+    from scipy import sparse
+    if not isinstance(op, (SpinHalf, BoseHubbard)):
+        return None
+    X = np.asarray(configs, np.float64)
+    dim = len(X)
+    dig = _value_digits(X, values)
+    idx = np.arange(dim, dtype=np.int64)
+    vals = np.asarray(values, np.float64)
+    rows, cols, data = [idx], [idx], [np.broadcast_to(np.asarray(op.diagonal_weight(X), np.float64), (dim,))]
+
+    def digit_of(v):
+        """Digit of site values v (must be in the basis where the rate is nonzero)."""
+        d = np.argmin(np.abs(v[..., None] - vals), axis=-1).astype(np.int64)
+        ok = np.abs(vals[d] - v) < 1e-6
+        return d, ok
+
+    def add(rate, changes):
+        """rate (dim,) of a move changing sites by the given (site, new value) arrays."""
+        nz = rate != 0.0
+        if not np.any(nz):
+            return
+        new = idx.copy()
+        for site, v in changes:
+            d, ok = digit_of(v)
+            if not np.all(ok[nz]):
+                raise ValueError("a transition of nonzero amplitude leaves the basis")
+            new = new + (d - dig[idx, site]) * powers[site]
+        rows.append(new[nz]); cols.append(idx[nz]); data.append(rate[nz])
+
+    if isinstance(op, SpinHalf):
+        N = op.N
+        if op.n_hx_static:
+            hx = np.broadcast_to(np.asarray(op.h_x_half, np.float64), (N,))
+            for k in range(N):
+                add(np.full(dim, hx[k]), [(k, -X[:, k])])
+        if op.n_jpm_static:
+            jpm = np.broadcast_to(np.asarray(op.J_pm, np.float64), (len(op.edge_i),))
+            jpp = np.broadcast_to(np.asarray(op.J_pmpm, np.float64), (len(op.edge_i),))
+            for e, (i, j) in enumerate(zip(np.asarray(op.edge_i, int), np.asarray(op.edge_j, int))):
+                anti = X[:, i] != X[:, j]
+                add(np.where(anti, jpm[e], jpp[e]), [(i, -X[:, i]), (j, -X[:, j])])
+    else:
+        a, b, da, db = op.moves()
+        n = X
+        nmax = float(op.n_max)
+        ei, ej = np.asarray(op.edge_i, int), np.asarray(op.edge_j, int)
+        blocks = []
+        if op.n_hop_off:
+            t = op._per_edge(op.t)
+            blocks.append(lambda: [-t[e] * np.sqrt(n[:, ei[e]] * (n[:, ej[e]] + 1.0)) * (n[:, ej[e]] < nmax)
+                                   for e in range(len(ei))])
+            blocks.append(lambda: [-t[e] * np.sqrt((n[:, ei[e]] + 1.0) * n[:, ej[e]]) * (n[:, ei[e]] < nmax)
+                                   for e in range(len(ei))])
+        if op.n_eta_off:
+            eta = op._per_edge(op.eta)
+            blocks.append(lambda: [-eta[e] * np.sqrt((n[:, ei[e]] + 1.0) * (n[:, ej[e]] + 1.0))
+                                   * ((n[:, ei[e]] < nmax) & (n[:, ej[e]] < nmax)) for e in range(len(ei))])
+            blocks.append(lambda: [-eta[e] * np.sqrt(n[:, ei[e]] * n[:, ej[e]]) for e in range(len(ei))])
+        if op.n_hpm_off:
+            hp = op._per_site(op.h_pm)
+            hp = np.broadcast_to(np.asarray(hp, np.float64), (op.N,))
+            blocks.append(lambda: [hp[k] * np.sqrt(n[:, k] + 1.0) * (n[:, k] < nmax) for k in range(op.N)])
+            blocks.append(lambda: [hp[k] * np.sqrt(n[:, k]) for k in range(op.N)])
+        slot = 1
+        for blk in blocks:
+            for rate in blk():
+                changes = [(int(a[slot]), n[:, a[slot]] + da[slot])]
+                if db[slot] != 0:
+                    changes.append((int(b[slot]), n[:, b[slot]] + db[slot]))
+                add(np.asarray(rate, np.float64), changes)
+                slot += 1
+        assert slot == op.M_total, (slot, op.M_total)
+    H = sparse.coo_matrix((np.concatenate(data), (np.concatenate(rows), np.concatenate(cols))),
+                          shape=(dim, dim)).tocsr()
+    H.sum_duplicates()
+    return H
+
+
 def _protocol_matrix(op, configs, values, powers):
     """Sparse matrix of op over the basis from get_rates alone: H[y, x] is the
-    rate of the transition x -> y (the diagonal element at slot 0)."""
+    rate of the transition x -> y (the diagonal element at slot 0); this
+    package's own operators take the vectorised build."""
     from scipy import sparse
+    Hb = _batch_matrix(op, configs, values, powers)
+    if Hb is not None:
+        return _checked(Hb)
     dim = len(configs)
     rows, cols, vals = [], [], []
     for i, x in enumerate(configs):
@@ -625,6 +718,11 @@ def _protocol_matrix(op, configs, values, powers):
         return sparse.csr_matrix((dim, dim))
     H = sparse.coo_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
                           shape=(dim, dim)).tocsr()
+    return _checked(H)
+
+
+def _checked(H):
+    """H after the finiteness and symmetry checks of the protocol build."""
     if not np.all(np.isfinite(H.data)):
         raise ValueError("the operator matrix has non-finite elements")
     asym = abs(H - H.T).max() if H.nnz else 0.0

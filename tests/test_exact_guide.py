@@ -243,3 +243,48 @@ def test_lowering_to_the_c_abi():
         guide_desc(RefShapedExactGuide(np.zeros(4), 27), _ring(N=27), keep)
     with pytest.raises(ValueError, match="sites"):
         guide_desc(g, _ring(N=8), keep)
+
+
+class _ProtocolOnly:
+    """Forwards just the Hamiltonian protocol (the generic matrix build)."""
+
+    def __init__(self, op):
+        self.op = op
+        self.N, self.M_total, self.local_hilbert_space = op.N, op.M_total, op.local_hilbert_space
+
+    def get_rates(self, config, return_configs=False):
+        return self.op.get_rates(config, return_configs=return_configs)
+
+    def generate_state(self, config, idx):
+        return self.op.generate_state(config, idx)
+
+    def diagonal_weight(self, config):
+        return self.op.diagonal_weight(config)
+
+
+@pytest.mark.parametrize("case", ["spin_fields", "spin_reversed", "bose", "bose_permuted"])
+def test_vectorised_matrix_equals_the_protocol_build(case):
+    """This package's operators take a vectorised matrix build; it equals the
+    per-configuration build from get_rates: off-diagonal elements exactly, the
+    diagonal to rounding (numpy sums diagonal_weight over a batch in another
+    order than over one configuration)."""
+    rng = np.random.default_rng(11)
+    if case.startswith("spin"):
+        e = P.chain(8).edges
+        jx = -rng.uniform(0.5, 1.5, 8)
+        op = P.SpinHalf.create(e, J_x=jx, J_y=jx + rng.uniform(0, 0.2, 8), J_z=rng.uniform(0.5, 1.5, 8),
+                               h_z=0.3, h_x=0.2, dtype=np.float64)
+        values = (1.0, -1.0) if case == "spin_fields" else (-1.0, 1.0)
+    else:
+        op = P.BoseHubbard.create(P.chain(4).edges, t=1.0, U=2.0, mu=0.5, h_pm=0.1, eta=0.2, n_max=2,
+                                  dtype=np.float64)
+        values = (0.0, 1.0, 2.0) if case == "bose" else (2.0, 0.0, 1.0)
+    cfg, powers = P.hamiltonian._basis(values, op.N)
+    fast = P.hamiltonian._batch_matrix(op, cfg, values, powers).toarray()
+    slow = P.hamiltonian._protocol_matrix(_ProtocolOnly(op), cfg, values, powers).toarray()
+    off = ~np.eye(len(fast), dtype=bool)
+    np.testing.assert_array_equal(fast[off], slow[off])
+    np.testing.assert_allclose(np.diag(fast), np.diag(slow), rtol=1e-14, atol=1e-15)
+    E_fast, _, _ = P.exact_diagonalization(op, values)
+    E_slow, _, _ = P.exact_diagonalization(_ProtocolOnly(op), values)
+    np.testing.assert_allclose(E_fast, E_slow, atol=1e-12)
