@@ -288,3 +288,22 @@ def test_vectorised_matrix_equals_the_protocol_build(case):
     E_fast, _, _ = P.exact_diagonalization(op, values)
     E_slow, _, _ = P.exact_diagonalization(_ProtocolOnly(op), values)
     np.testing.assert_allclose(E_fast, E_slow, atol=1e-12)
+
+
+def test_bose_hubbard_exact_guide_on_the_host():
+    """The host guide on a Bose-Hubbard chain (exact_ground_state tests:
+    85-103, their bose_hubbard case): the guided rates sum to E0 on every
+    configuration of the support, over both the default digit order and a
+    permuted local space; the device lowering refuses it (spin-1/2 only)."""
+    B = P.BoseHubbard.create(P.chain(3).edges, t=1.0, U=2.0, mu=0.5, h_pm=0.1, eta=0.2, n_max=2,
+                             dtype=np.float64)
+    for values in ((0.0, 1.0, 2.0), (2.0, 0.0, 1.0)):
+        g = P.ExactGroundState(B, local_hilbert_space=values, dtype=np.float64)
+        cfg = _all(3, values)
+        psi = np.exp(g.log_amp[g.basis_index(cfg)])
+        support = psi > 1e-10
+        assert support.any()
+        e = np.array([_host_local_energy(B, g, x) for x in cfg[support]])
+        np.testing.assert_allclose(e, g.E0, rtol=0, atol=1e-10)
+    with pytest.raises(TypeError, match="SpinHalf"):
+        guide_desc(g, B, _Keep())
