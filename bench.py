@@ -48,6 +48,13 @@ TAU = 0.05
 # DRAM sees less than the algorithmic bytes.
 EVOLVE_TRAFFIC_BYTES = {("fp64", 32768): 112.1e6}
 
+# DRAM traffic of one rbm_theta_persist launch (16x16, H = 512, 65536
+# walkers), from the `--set full` capture of
+# `bench.py --guide rbm --steps 3 --warmup 3` (-k regex:rbm_theta_persist
+# -s 2 -c 1): 3.0 MB read + 74.6 MB written (the rest of the 134 MB output
+# is still in L2 when the kernel ends).
+THETA_TRAFFIC_BYTES = {(256, 512, 65536): 77.6e6}
+
 
 def build_system(P, precision):
     lat = P.square(L)
@@ -368,7 +375,8 @@ def rbm_bench(P, args):
             "jastrow_fp64": plain["fp64"], "jastrow_mixed": plain["mixed"],
             "roofline": {"bound": "tensor", "kernel": "rbm_theta_persist", "achieved": g["tflops"],
                          "peak": g["peak_tflops"], "unit": "TFLOP/s", "frac": g["frac"],
-                         "traffic": None, "peak_source": g["peak_source"],
+                         "traffic": THETA_TRAFFIC_BYTES.get((lat.N, hid, n)),
+                         "peak_source": g["peak_source"],
                          "hbm_floor_ms": g["hbm_floor_ms"], "hbm_frac": g["hbm_frac"],
                          "note": "the GEMM's floor is its float32 output through HBM (hbm_floor_ms); "
                                  "the branching step itself is bound by the per-slot product "
