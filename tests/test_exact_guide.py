@@ -307,3 +307,14 @@ def test_bose_hubbard_exact_guide_on_the_host():
         np.testing.assert_allclose(e, g.E0, rtol=0, atol=1e-10)
     with pytest.raises(TypeError, match="SpinHalf"):
         guide_desc(g, B, _Keep())
+
+
+def test_lowering_refuses_a_non_spin_local_space():
+    """A guide indexed over occupations (0, 1) is not a spin-1/2 table: the
+    lowering refuses it rather than reading it with the wrong digit order."""
+    ref = RefShapedExactGuide(np.zeros(64), 6)
+    ref.local_hilbert_space = (0.0, 1.0)
+    with pytest.raises(TypeError, match="spin-1/2"):
+        exact_amplitude_table(ref)
+    with pytest.raises(TypeError, match="spin-1/2"):
+        guide_desc(ref, _ring(), _Keep())
