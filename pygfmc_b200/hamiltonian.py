@@ -583,6 +583,7 @@ def kagome(Lx: int, Ly: int, periodic: bool = True) -> Lattice:
 # ---------------------------------------------------------------------------
 _ED_MAX_DIM = 2 ** 24
 _ED_DENSE_DIM = 2048
+_ED_MAX_BYTES = 16 * 2 ** 30
 
 
 def _basis(values, N):
@@ -766,9 +767,18 @@ def exact_diagonalization(hamiltonian, local_hilbert_space=None, N=None, diag_op
     k = int(number_of_states)
     if k != number_of_states or not 1 <= k <= dim:
         raise ValueError(f"number_of_states must be an integer in [1, {dim}], got {number_of_states!r}")
+    # the basis (float64 values), the matrix triplets (at most M_total per
+    # state: two int64 indices and a float64 value) and, for a full solve,
+    # the dense matrix with its eigenvectors
+    m_total = int(getattr(hamiltonian, "M_total", 1))
+    dense = dim <= _ED_DENSE_DIM or k >= dim - 1
+    need = max(dim * N * 8 + dim * m_total * 24, 2 * dim * dim * 8 if dense else 0)
+    if need > _ED_MAX_BYTES:
+        raise ValueError(f"exact diagonalisation of {dim} states would allocate about "
+                         f"{need / 2 ** 30:.1f} GiB, above the {_ED_MAX_BYTES / 2 ** 30:.0f} GiB limit")
     configs, powers = _basis(values, N)
     H = _protocol_matrix(hamiltonian, configs, values, powers)
-    if dim <= _ED_DENSE_DIM or k >= dim - 1:
+    if dense:
         w, v = np.linalg.eigh(H.toarray())
         energies, states = w[:k], v[:, :k]
     else:

@@ -90,6 +90,15 @@ def test_exact_diagonalization_rejects_bad_arguments():
         P.exact_diagonalization(H, number_of_states=65)
     with pytest.raises(ValueError, match="limit"):
         P.exact_diagonalization(_ring(N=25))
+    # the allocation estimate (basis, matrix triplets, dense solve) is checked
+    # before anything is built
+    old = P.hamiltonian._ED_MAX_BYTES
+    try:
+        P.hamiltonian._ED_MAX_BYTES = 2 ** 20
+        with pytest.raises(ValueError, match="GiB"):
+            P.exact_diagonalization(_ring(N=12))
+    finally:
+        P.hamiltonian._ED_MAX_BYTES = old
 
 
 @pytest.mark.parametrize("values", [(1.0, -1.0), (-1.0, 1.0)])
