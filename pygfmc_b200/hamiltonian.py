@@ -495,6 +495,28 @@ class SzSzStructureFactor:
         return 0.25 * (c ** 2 + s_ ** 2) - float(self.offset)
 
 
+def is_valid_k(k_vectors, lattice_vectors, atol=1e-5):
+    """Whether each wavevector is in the reciprocal lattice of the simulation
+    cell (hamiltonian/observables.py:14-65): k . L_j / (2 pi) within ``atol``
+    of an integer for every periodic vector L_j (the rows of the (d, d)
+    ``lattice_vectors``, the vectors the boundary identifies).  Only such k
+    make the structure factors independent of which periodic image the
+    positions encode.  Returns a bool for one (d,) wavevector, a boolean
+    (n_k,) array for an (n_k, d) stack; the default ``atol`` admits
+    wavevectors built in float32."""
+    lat = np.asarray(lattice_vectors, dtype=np.float64)
+    if lat.ndim != 2 or lat.shape[0] != lat.shape[1]:
+        raise ValueError(f"lattice_vectors must be (d, d), one periodic vector per row; got {lat.shape}.")
+    k = np.asarray(k_vectors, dtype=np.float64)
+    one = k.ndim == 1
+    k2 = np.atleast_2d(k)
+    if k2.ndim != 2 or k2.shape[1] != lat.shape[0]:
+        raise ValueError(f"k_vectors must be (d,) or (n_k, d) with d = {lat.shape[0]}; got {k.shape}.")
+    turns = (k2 @ lat.T) / (2.0 * np.pi)               # (n_k, d) windings per periodic vector
+    ok = np.all(np.abs(turns - np.rint(turns)) <= atol, axis=1)
+    return bool(ok[0]) if one else ok
+
+
 # ---- lattices ----------------------------------------------------------------
 @dataclass(frozen=True)
 class Lattice:
@@ -722,6 +744,29 @@ def _protocol_matrix(op, configs, values, powers):
     return _checked(H)
 
 
+def _diagonal_values(op, configs):
+    """``op.diagonal_weight`` over the basis (hamiltonian/exact.py:182-192):
+    shape (dim,), or (dim, n_vals) for a vector-valued operator such as a
+    structure factor over several wavevectors.  This package's operators
+    evaluate the whole basis at once; any other goes configuration by
+    configuration, so a diagonal_weight written for one configuration is
+    never handed a batch."""
+    dim = len(configs)
+    if isinstance(op, (SpinHalf, BoseHubbard, SzSzStructureFactor)):
+        vals = np.asarray(op.diagonal_weight(configs), np.float64)
+        if vals.ndim == 0:                       # an operator with no diagonal term
+            vals = np.full(dim, float(vals))
+    else:
+        vals = np.array([np.asarray(op.diagonal_weight(x), np.float64) for x in configs])
+    if vals.ndim not in (1, 2) or vals.shape[0] != dim:
+        raise ValueError(f"{type(op).__name__}.diagonal_weight gives values of shape "
+                         f"{vals.shape[1:] if vals.ndim else ()} per configuration; a scalar or "
+                         "a vector is expected")
+    if not np.all(np.isfinite(vals)):
+        raise ValueError(f"{type(op).__name__}.diagonal_weight is not finite on the whole basis")
+    return vals
+
+
 def _checked(H):
     """H after the finiteness and symmetry checks of the protocol build."""
     if not np.all(np.isfinite(H.data)):
@@ -761,6 +806,15 @@ def exact_diagonalization(hamiltonian, local_hilbert_space=None, N=None, diag_op
         if N is None:
             raise ValueError(f"{type(hamiltonian).__name__} exposes no N; pass it")
     N = int(N)
+    # a basis of the wrong size gives a plausible spectrum of another problem:
+    # cross-check the site count and local dimension the operator reports
+    own_N = getattr(hamiltonian, "N", None)
+    if own_N is not None and int(own_N) != N:
+        raise ValueError(f"N={N} but {type(hamiltonian).__name__} acts on {int(own_N)} sites")
+    own_d = getattr(hamiltonian, "d", None)
+    if own_d is not None and int(own_d) != d:
+        raise ValueError(f"local_hilbert_space has {d} values but {type(hamiltonian).__name__} "
+                         f"reports a local dimension of {int(own_d)}")
     dim = d ** N
     if dim > _ED_MAX_DIM:
         raise ValueError(f"a basis of {d}**{N} = {dim} states is above the {_ED_MAX_DIM} limit")
@@ -783,13 +837,16 @@ def exact_diagonalization(hamiltonian, local_hilbert_space=None, N=None, diag_op
         energies, states = w[:k], v[:, :k]
     else:
         from scipy.sparse.linalg import eigsh
-        w, v = eigsh(H, k=k, which="SA", tol=1e-12)
+        # a fixed start vector: ARPACK's own seed advances between calls, and
+        # two solves of one matrix would then differ in their last bits
+        v0 = np.random.default_rng(0).standard_normal(dim)
+        w, v = eigsh(H, k=k, which="SA", tol=1e-12, v0=v0)
         order = np.argsort(w)
         energies, states = w[order], v[:, order]
     diag_obs = {}
     for name, op in (diag_operators or {}).items():
-        dw = np.array([float(np.asarray(op.diagonal_weight(x))) for x in configs])
-        diag_obs[name] = (np.abs(states) ** 2 * dw[:, None]).sum(axis=0)
+        # (k,) for a scalar operator, (k, n_vals) for a vector-valued one
+        diag_obs[name] = (states ** 2).T @ _diagonal_values(op, configs)
     off_obs = {}
     for name, op in (off_diag_operators or {}).items():
         O = _protocol_matrix(op, configs, values, powers)

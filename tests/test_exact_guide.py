@@ -90,6 +90,8 @@ def test_exact_diagonalization_rejects_bad_arguments():
         P.exact_diagonalization(H, number_of_states=65)
     with pytest.raises(ValueError, match="limit"):
         P.exact_diagonalization(_ring(N=25))
+    with pytest.raises(ValueError, match="acts on 6 sites"):
+        P.exact_diagonalization(H, N=7)
     # the allocation estimate (basis, matrix triplets, dense solve) is checked
     # before anything is built
     old = P.hamiltonian._ED_MAX_BYTES
@@ -99,6 +101,52 @@ def test_exact_diagonalization_rejects_bad_arguments():
             P.exact_diagonalization(_ring(N=12))
     finally:
         P.hamiltonian._ED_MAX_BYTES = old
+
+
+class _OneConfigDiagonal:
+    """A diagonal operator that accepts one configuration at a time (a batch
+    would fail its shape check), vector-valued like a structure factor."""
+
+    def __init__(self, sf):
+        self.sf = sf
+
+    def diagonal_weight(self, x):
+        x = np.asarray(x)
+        assert x.ndim == 1
+        return self.sf.diagonal_weight(x)
+
+
+def test_vector_valued_diagonal_observables():
+    """A structure factor over several wavevectors gives (k, n_k) expectations
+    (hamiltonian/exact.py:366-369): sum_x |psi_k(x)|^2 S(q; x) for each q, the
+    same through the whole-basis and the per-configuration evaluation."""
+    N = 8
+    H = _ring(h_x=0.3, N=N)
+    q = 2 * np.pi * np.arange(N)[:, None] / N
+    sf = P.hamiltonian.SzSzStructureFactor(np.arange(N, dtype=np.float64)[:, None], q, dtype=np.float64)
+    E, dobs, _, psi = P.exact_diagonalization(
+        H, diag_operators={"sf": sf, "sf1": _OneConfigDiagonal(sf), "H": H},
+        number_of_states=2, return_states=True)
+    assert dobs["sf"].shape == (2, N) and dobs["H"].shape == (2,)
+    cfg, _ = P.hamiltonian._basis((1.0, -1.0), N)
+    direct = np.array([[np.sum(psi[:, k] ** 2 * np.array([sf.diagonal_weight(x)[j] for x in cfg]))
+                        for j in range(N)] for k in range(2)])
+    np.testing.assert_allclose(dobs["sf"], direct, rtol=0, atol=1e-12)
+    np.testing.assert_allclose(dobs["sf1"], dobs["sf"], rtol=0, atol=1e-12)
+    # S(q) is a pair sum over i < j, and sum_q cos(q (r_i - r_j)) = 0 for
+    # i != j over the N wavevectors of the ring: the q-sum vanishes
+    np.testing.assert_allclose(dobs["sf"].sum(axis=1), 0.0, atol=1e-10)
+
+
+def test_lanczos_solves_are_reproducible():
+    """Two solves of one 4096-state matrix in one process agree bit for bit
+    (a fixed Lanczos start vector), so two ExactGroundState guides built from
+    one Hamiltonian are the same guide."""
+    H = _ring(N=12)
+    E1, _, _, v1 = P.exact_diagonalization(H, number_of_states=2, return_states=True)
+    E2, _, _, v2 = P.exact_diagonalization(H, number_of_states=2, return_states=True)
+    np.testing.assert_array_equal(E1, E2)
+    np.testing.assert_array_equal(v1, v2)
 
 
 @pytest.mark.parametrize("values", [(1.0, -1.0), (-1.0, 1.0)])

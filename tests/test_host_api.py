@@ -334,3 +334,37 @@ def test_structure_factor_factory():
         P.hamiltonian.StructureFactor(pos, [[0.1], [0.2]])
     with pytest.raises(ValueError, match="zone boundary"):
         P.hamiltonian.StructureFactor(np.array([[0.0], [1.0]]), [np.pi])
+
+
+def test_is_valid_k():
+    """hamiltonian/observables.py is_valid_k:14-65 (the pins of PyGFMC's
+    tests/core/test_structure_factor_operator.py:190-202): k . L_j / 2 pi an
+    integer for every periodic vector; a bool for one wavevector, an array for
+    a stack; and only a valid k leaves SzSzStructureFactor unchanged when the
+    positions move to other periodic images."""
+    is_valid_k = P.hamiltonian.is_valid_k
+    L = np.array([[4.0, 0.0], [2.0, 2.0 * np.sqrt(3.0)]])       # a triangular torus
+    ks = 2 * np.pi * np.array([[0, 0], [1, 0], [0, 1], [3, -2]]) @ np.linalg.inv(L).T
+    got = is_valid_k(ks, L)
+    assert isinstance(got, np.ndarray) and got.dtype == bool and got.all()
+    assert is_valid_k(ks[1], L) is True
+    assert is_valid_k(0.5 * ks[1], L) is False
+    assert is_valid_k(ks[3] + 1e-7, L) is True                    # float32-built k pass
+    np.testing.assert_array_equal(is_valid_k(np.vstack([ks[2], 0.5 * ks[2]]), L), [True, False])
+    np.testing.assert_array_equal(is_valid_k(2 * np.pi * np.arange(3)[:, None] / 8, [[8.0]]),
+                                  [True, True, True])
+    assert is_valid_k([1.0], [[8.0]]) is False
+    with pytest.raises(ValueError, match=r"\(d, d\)"):
+        is_valid_k(ks, L[:1])
+    with pytest.raises(ValueError, match="k_vectors must be"):
+        is_valid_k(np.zeros(3), L)
+    # image independence of the structure factor exactly for valid k
+    rng = np.random.default_rng(5)
+    N = 6
+    pos = rng.normal(size=(N, 2))
+    shifted = pos + rng.integers(-2, 3, size=(N, 2)) @ L
+    x = rng.choice([1.0, -1.0], size=(16, N))
+    for k, same in ((ks[3], True), (1.3 * ks[3], False)):
+        a = P.hamiltonian.SzSzStructureFactor(pos, k[None], dtype=np.float64).diagonal_weight(x)
+        b = P.hamiltonian.SzSzStructureFactor(shifted, k[None], dtype=np.float64).diagonal_weight(x)
+        assert (np.max(np.abs(a - b)) < 1e-9) == same
