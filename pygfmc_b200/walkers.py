@@ -5,6 +5,7 @@ draws for the same key (``jax.random.randint`` / ``jax.random.permutation``
 restated over the Threefry stream in :mod:`pygfmc_b200.random`), in PyGFMC's
 float64 mode (``jax_enable_x64``) unless ``x64=False``.
 """
+import ctypes
 from typing import NamedTuple, Sequence
 
 import numpy as np
@@ -12,7 +13,12 @@ import numpy as np
 from . import random as _rnd
 
 __all__ = ["Walker", "prepare_walkers_random", "prepare_walkers_sz",
-           "prepare_walkers_from_configs", "prepare_walkers_occupations"]
+           "prepare_walkers_from_configs", "prepare_walkers_occupations", "reconfiguration",
+           "RECONFIGURATION_MAX_WALKERS"]
+
+# population limit of reconfiguration(): its device scratch is a fixed array
+# (GFMC_NOALLOC_MAX_WALKERS in the C header)
+RECONFIGURATION_MAX_WALKERS = 131072
 
 
 def _compact_config(config):
@@ -193,3 +199,58 @@ def prepare_walkers_occupations(N_walkers, N_sites, n_total, n_max, rng_key, x64
             out[w, i] = v
             s -= v
     return Walker(config=out, log_weight=_zeros(N_walkers, x64), e_loc=_zeros(N_walkers, x64))
+
+
+def reconfiguration(walkers, rng_key):
+    """Systematic resampling of a walker population on the GPU
+    (walkers/reconfiguration.py:27-62): ``(new_walkers, log_G_n - log N,
+    E_n, indices)`` with log G_n = logsumexp(log_weight), weights
+    w = exp(log_weight - log G_n), E_n = sum w e_loc, the offset
+    psi = uniform(rng_key) and indices[i] the first walker whose cumulative
+    weight exceeds (i + psi) / N (capped at the last walker of positive
+    weight, systematic_parents:9-24).  The new walkers are the parents'
+    configurations and local energies with log weights reset to zero, in
+    the dtype of the input's.
+
+    The weights, the float64 cumulative sum, the search and E_n run on the
+    device (``gfmc_reconfigure_noalloc``, the kernels of the engine's own
+    resampling); the configurations stay where the caller keeps them (host
+    arrays) and are gathered there through the returned parents.  At most
+    ``RECONFIGURATION_MAX_WALKERS`` walkers per call (ValueError above).  A
+    population whose weights sum to zero or overflow gives a non-finite
+    log G and E_n, as the reference's does; its indices are then in range
+    but carry no meaning.  Needs a CUDA device (no CPU fallback)."""
+    from . import _lib
+    from .engine import _torch
+    config = np.asarray(walkers.config)
+    log_w = np.asarray(walkers.log_weight)
+    e_loc = np.asarray(walkers.e_loc)
+    if log_w.ndim != 1 or e_loc.shape != log_w.shape or config.ndim < 1 or config.shape[0] != log_w.shape[0]:
+        raise ValueError(f"walkers must hold log_weight and e_loc of shape (N_walkers,) and config of "
+                         f"N_walkers rows; got {log_w.shape}, {e_loc.shape} and {config.shape}.")
+    n = log_w.shape[0]
+    if n < 1:
+        raise ValueError("reconfiguration needs at least one walker.")
+    if n > RECONFIGURATION_MAX_WALKERS:
+        raise ValueError(f"reconfiguration takes at most {RECONFIGURATION_MAX_WALKERS} walkers per call; "
+                         f"got {n}.  A larger population runs through run() / GFMCEngine, whose "
+                         "resampling has no such limit.")
+    key = np.ascontiguousarray(_rnd.as_key(rng_key), dtype=np.uint32)
+    torch = _torch()
+    lib = _lib.load()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    stream = torch.cuda.current_stream(dev)
+    d_lw = torch.as_tensor(np.ascontiguousarray(log_w, dtype=np.float64)).to(dev, non_blocking=False)
+    d_el = torch.as_tensor(np.ascontiguousarray(e_loc, dtype=np.float64)).to(dev, non_blocking=False)
+    parents = torch.empty(n, dtype=torch.int32, device=dev)
+    scalars = torch.empty(2, dtype=torch.float64, device=dev)      # log G_n - log N, E_n
+    vp = lambda t: ctypes.c_void_p(t.data_ptr())                      # noqa: E731
+    rc = lib.gfmc_reconfigure_noalloc(n, vp(d_lw), vp(d_el),
+                                      key.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+                                      vp(parents), vp(scalars[0:1]), vp(scalars[1:2]),
+                                      ctypes.c_void_p(stream.cuda_stream))
+    _lib.check(rc, "reconfiguration")
+    idx = parents.cpu().numpy()          # waits for the stream
+    log_avg, E_n = scalars.cpu().numpy().tolist()
+    new = Walker(config=config[idx], log_weight=np.zeros(n, dtype=log_w.dtype), e_loc=e_loc[idx])
+    return new, log_avg, E_n, idx
