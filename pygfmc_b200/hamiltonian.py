@@ -12,12 +12,13 @@ itself never calls them.
 """
 from __future__ import annotations
 
+import itertools
 from dataclasses import dataclass, field
 
 import numpy as np
 
-__all__ = ["SpinHalf", "BoseHubbard", "StructureFactor", "SzSzStructureFactor", "Lattice", "chain",
-           "square", "kagome", "edges_array", "exact_diagonalization"]
+__all__ = ["SpinHalf", "BoseHubbard", "StructureFactor", "SzSzStructureFactor", "is_valid_k", "Lattice",
+           "chain", "square", "kagome", "pyrochlore", "edges_array", "exact_diagonalization"]
 
 
 def edges_array(edges):
@@ -562,6 +563,64 @@ def square(Lx: int, Ly: int = None, periodic: bool = True) -> Lattice:
     pos = np.array([(x, y) for y in range(Ly) for x in range(Lx)], dtype=float)
     return Lattice(name="square", N=Lx * Ly, edges=sorted(edges), J_x=-1.0, J_y=-1.0, J_z=1.0,
                    extras=dict(positions=pos, torus=np.array([Lx, Ly]), periodic=periodic))
+
+
+def pyrochlore(nx: int, ny: int, nz: int, periodic: bool = True) -> Lattice:
+    """Pyrochlore lattice of nx x ny x nz four-site cells
+    (hamiltonian/lattice.py pyrochlore:49-183): the FCC lattice with primitive
+    vectors a1 = (1/2, 1/2, 0), a2 = (1/2, 0, 1/2), a3 = (0, 1/2, 1/2)
+    (conventional cubic cell of side 1) and a tetrahedral basis at 0, a1/2,
+    a2/2, a3/2; site 4 (z + nz y + nz ny x) + b for cell (x, y, z) and
+    sublattice b, so N = 4 nx ny nz and, periodic, 3N bonds (coordination 6).
+
+    The bonds are found geometrically: every sublattice pair and cell offset
+    in {-1, 0, 1}^3 whose displacement has the nearest-neighbour length
+    1/(2 sqrt 2) -- the three bonds of a site inside its own ("up")
+    tetrahedron and three into neighbouring cells' ("down") tetrahedra.
+    They are listed as sorted (i < j) pairs, the order PyGFMC's edge list
+    has.  Periodic boundaries need nx, ny, nz >= 2 (a single cell would wrap
+    a bond onto itself); open ones keep the bonds inside the block.
+    ``extras``: positions (N, 3), primitive_vectors, sublattice_offsets,
+    supercell_dims and the torus vectors (rows nx a1, ny a2, nz a3).  The
+    hexagonal loops PyGFMC also lists there serve only its plaquette model,
+    which this package does not provide."""
+    dims = (int(nx), int(ny), int(nz))
+    if min(dims) < 1:
+        raise ValueError(f"pyrochlore needs at least one cell per direction, got {dims}")
+    if periodic and min(dims) < 2:
+        raise ValueError(f"pyrochlore requires nx, ny, nz >= 2 for periodic boundary conditions "
+                         f"(got {nx}, {ny}, {nz}); a dimension of one cell wraps a bond onto itself.")
+    prim = np.array([[0.5, 0.5, 0.0], [0.5, 0.0, 0.5], [0.0, 0.5, 0.5]])
+    basis = np.vstack([np.zeros(3), prim / 2.0])
+    nn = 1.0 / (2.0 * np.sqrt(2.0))
+    # the bond templates: (b, c, cell offset) at nearest-neighbour distance
+    tmpl = []
+    for off in itertools.product((-1, 0, 1), repeat=3):
+        shift = np.asarray(off, np.float64) @ prim
+        for b in range(4):
+            for c in range(4):
+                if np.isclose(np.linalg.norm(shift + basis[c] - basis[b]), nn, atol=1e-12):
+                    tmpl.append((b, c, off))
+    assert len(tmpl) == 24, len(tmpl)          # 6 neighbours of each of the 4 sublattices
+
+    def cell(x, y, z):
+        return z + dims[2] * (y + dims[1] * x)
+
+    edges = set()
+    for x, y, z in itertools.product(*(range(d) for d in dims)):
+        for b, c, (ox, oy, oz) in tmpl:
+            t = (x + ox, y + oy, z + oz)
+            if not periodic and not all(0 <= t[k] < dims[k] for k in range(3)):
+                continue
+            i = 4 * cell(x, y, z) + b
+            j = 4 * cell(*(t[k] % dims[k] for k in range(3))) + c
+            edges.add((min(i, j), max(i, j)))
+    pos = np.array([x * prim[0] + y * prim[1] + z * prim[2] + basis[b]
+                    for x, y, z in itertools.product(*(range(d) for d in dims)) for b in range(4)])
+    return Lattice(name="pyrochlore", N=4 * dims[0] * dims[1] * dims[2], edges=sorted(edges),
+                   extras=dict(positions=pos, primitive_vectors=prim, sublattice_offsets=basis,
+                               supercell_dims=np.array(dims, dtype=np.int32),
+                               torus=np.asarray(dims, np.float64)[:, None] * prim))
 
 
 def kagome(Lx: int, Ly: int, periodic: bool = True) -> Lattice:

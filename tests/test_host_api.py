@@ -1,5 +1,7 @@
 """Host-side API: constructors and validation mirror PyGFMC, the walker
 initialisers draw PyGFMC's walkers, and the lattices are the reference's."""
+import itertools
+
 import numpy as np
 import pytest
 
@@ -100,6 +102,79 @@ def test_lattices():
     assert kg.N == 432 and len(kg.edges) == 864
     deg = np.bincount(np.asarray(kg.edges).ravel(), minlength=432)
     assert np.all(deg == 4)
+
+
+def _pairs_at(pos, d, torus=None):
+    """Every (i < j) pair at distance d, with the minimum image over the torus
+    translations when given (brute force over all pairs)."""
+    disp = pos[None, :, :] - pos[:, None, :]
+    if torus is not None:
+        shifts = np.array(list(itertools.product((-1, 0, 1), repeat=3))) @ torus
+        dist = np.min(np.linalg.norm(disp[:, :, None, :] + shifts[None, None], axis=-1), axis=-1)
+    else:
+        dist = np.linalg.norm(disp, axis=-1)
+    i, j = np.nonzero(np.triu(np.isclose(dist, d, atol=1e-9), 1))
+    return sorted(zip(i.tolist(), j.tolist()))
+
+
+@pytest.mark.parametrize("dims,periodic", [((2, 2, 2), True), ((3, 3, 3), True), ((3, 2, 4), True),
+                                           ((2, 3, 2), False), ((1, 1, 1), False)])
+def test_pyrochlore(dims, periodic):
+    """hamiltonian/lattice.py pyrochlore:49-183: N = 4 nx ny nz, 3N bonds and
+    coordination 6 when periodic, cell index z + nz y + nz ny x, bonds as
+    sorted (i < j) pairs; the bond set equals a brute-force search for pairs
+    at the nearest-neighbour distance 1/(2 sqrt 2) (minimum image on the
+    torus; every cell size here has a unique minimum image except 2, where
+    the search over images still finds exactly the lattice's bonds)."""
+    lat = P.hamiltonian.pyrochlore(*dims, periodic=periodic)
+    nx, ny, nz = dims
+    assert lat.N == 4 * nx * ny * nz and lat.edges == sorted(lat.edges)
+    assert all(i < j for i, j in lat.edges)
+    pos = lat.extras["positions"]
+    prim = lat.extras["primitive_vectors"]
+    if nz > 1:
+        np.testing.assert_allclose(pos[4 * 1], prim[2])                # cell (0, 0, 1): z fastest
+    if ny > 1:
+        np.testing.assert_allclose(pos[4 * nz], prim[1])               # cell (0, 1, 0)
+    nn = 1.0 / (2.0 * np.sqrt(2.0))
+    want = _pairs_at(pos, nn, lat.extras["torus"] if periodic else None)
+    assert lat.edges == want
+    for c in range(lat.N // 4):                                        # each cell's up tetrahedron
+        for a, b in itertools.combinations(range(4 * c, 4 * c + 4), 2):
+            assert (a, b) in set(lat.edges)
+    if periodic:
+        assert len(lat.edges) == 3 * lat.N
+        assert np.all(np.bincount(np.asarray(lat.edges).ravel(), minlength=lat.N) == 6)
+    else:
+        assert len(lat.edges) == len(_pairs_at(pos, nn))
+
+
+@pytest.mark.parametrize("name,fn,args,periodic", [
+    ("pyrochlore_2x2x2", "pyrochlore", (2, 2, 2), True), ("pyrochlore_3x2x4", "pyrochlore", (3, 2, 4), True),
+    ("pyrochlore_4x4x4", "pyrochlore", (4, 4, 4), True),
+    ("pyrochlore_2x3x2_open", "pyrochlore", (2, 3, 2), False),
+    ("pyrochlore_1x1x1_open", "pyrochlore", (1, 1, 1), False),
+    ("kagome_12x12", "kagome", (12, 12), True), ("kagome_3x2_open", "kagome", (3, 2), False),
+    ("chain_100", "chain", (100,), True), ("chain_7_open", "chain", (7,), False)])
+def test_lattices_match_the_reference_fixture(name, fn, args, periodic):
+    """Edge lists (in order) and positions equal those of PyGFMC's own
+    hamiltonian/lattice.py on the same arguments (tests/golden/lattices.npz,
+    written by tests/golden/make_lattice_golden.py from that file)."""
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "lattices.npz"))
+    lat = getattr(P.hamiltonian, fn)(*args, periodic=periodic)
+    assert lat.N == int(z[f"{name}/N"])
+    assert lat.edges == [tuple(e) for e in z[f"{name}/edges"].tolist()]
+    if f"{name}/positions" in z.files:
+        np.testing.assert_allclose(lat.extras["positions"], z[f"{name}/positions"], rtol=0, atol=1e-14)
+
+
+def test_pyrochlore_rejects_single_cell_tori():
+    for dims in ((1, 2, 2), (2, 1, 2), (2, 2, 1)):
+        with pytest.raises(ValueError, match=">= 2"):
+            P.hamiltonian.pyrochlore(*dims)
+    with pytest.raises(ValueError, match="at least one cell"):
+        P.hamiltonian.pyrochlore(0, 2, 2, periodic=False)
 
 
 def test_run_validation_errors_before_any_work():
