@@ -5,11 +5,12 @@ step_size, guide, p_array, *, method, rng_key, lam, warmup_steps, ...)`` with
 PyGFMC's SpinHalf / BoseHubbard Hamiltonians and Jastrow guides, executed by
 hand-written CUDA kernels behind a C ABI (``include/gfmc_b200.h``).
 """
-from . import diagnostics, hamiltonian, learn, random, walkers, wavefunction
+from . import diagnostics, hamiltonian, learn, protocols, random, walkers, wavefunction
 from .diagnostics import statistics
 from .engine import GFMCEngine, run, run_gfmc
 from .estimators import evaluate_observables
 from .hamiltonian import BoseHubbard, SpinHalf, chain, exact_diagonalization, kagome, square
+from .protocols import DiagonalOperator, Guide, Operator
 from .random import PRNGKey
 from .walkers import (Walker, prepare_walkers_from_configs, prepare_walkers_occupations,
                       prepare_walkers_random, prepare_walkers_sz)
@@ -22,5 +23,6 @@ __all__ = ["run", "run_gfmc", "statistics", "GFMCEngine", "evaluate_observables"
            "chain", "square", "kagome", "PRNGKey", "Walker", "prepare_walkers_random",
            "prepare_walkers_sz", "prepare_walkers_from_configs", "prepare_walkers_occupations",
            "JastrowSpinHalf", "JastrowBoseHubbard", "RBMSpinHalf", "MLPBoseHubbard", "ExactGroundState",
-           "exact_diagonalization", "hamiltonian", "random", "walkers",
+           "exact_diagonalization", "Operator", "DiagonalOperator", "Guide", "hamiltonian", "protocols",
+           "random", "walkers",
            "wavefunction", "__version__"]

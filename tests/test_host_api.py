@@ -169,6 +169,24 @@ def test_lattices_match_the_reference_fixture(name, fn, args, periodic):
         np.testing.assert_allclose(lat.extras["positions"], z[f"{name}/positions"], rtol=0, atol=1e-14)
 
 
+def test_protocol_classes():
+    """PyGFMC's top-level Operator / DiagonalOperator / Guide (protocols.py:25-143)
+    exist with the same member names, and this package's objects have the
+    members the protocols require."""
+    import typing
+    for cls, members in ((P.Operator, ("M_total", "get_rates", "generate_state", "move")),
+                         (P.DiagonalOperator, ("diagonal_weight",)),
+                         (P.Guide, ("log_diff_from_operator", "log_diff_from_configs", "log_psi",
+                                    "build_cache", "incremental", "init_state", "update_state"))):
+        assert typing.Protocol in cls.__mro__
+        for m in members:
+            assert hasattr(cls, m) or m in cls.__annotations__, (cls.__name__, m)
+    H = P.SpinHalf.create(P.chain(6).edges, J_x=-1.0, J_y=-1.0, J_z=1.0, dtype=np.float64)
+    assert all(hasattr(H, m) for m in ("M_total", "get_rates", "generate_state", "diagonal_weight"))
+    for g in (P.JastrowSpinHalf(6, P.chain(6).edges, beta=0.3), P.ExactGroundState(H)):
+        assert any(hasattr(g, m) for m in ("log_diff_from_operator", "log_diff_from_configs", "log_psi"))
+
+
 def test_pyrochlore_rejects_single_cell_tori():
     for dims in ((1, 2, 2), (2, 1, 2), (2, 2, 1)):
         with pytest.raises(ValueError, match=">= 2"):
