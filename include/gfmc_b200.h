@@ -354,6 +354,16 @@ int gfmc_evolve(gfmc_handle *h, int method, double step, double lam, double alw,
                 const uint32_t key[2], long long walker_offset, int n_walkers, const void *cfg,
                 const int32_t *parents, int parents_valid, void *cfg_out, double *log_w,
                 double *e_loc, uint64_t *hops, void *stream);
+/* One evolution of a population with its own log weights, no resampling:
+ * replaces PyGFMC's evolve_walkers (engine/evolution.py:761-843).  Walker i
+ * (packed row i of cfg) draws from fold_in(key, i) = split(key, n)[i],
+ * propagates into row i of cfg_out (cfg_out != cfg), and its log weight
+ * accumulates onto log_w[i] in place (the step's terms added to the incoming
+ * value in PyGFMC's order); e_loc[i] is the local energy of its final
+ * configuration.  The guide state is built from cfg. */
+int gfmc_evolve_walkers(gfmc_handle *h, int method, double step, double lam, double alw,
+                        const uint32_t key[2], int n_walkers, const void *cfg, void *cfg_out,
+                        double *log_w, double *e_loc, uint64_t *hops, void *stream);
 /* Systematic resampling of a population sharded over ranks in contiguous
  * blocks (walkers/reconfiguration.py:9-62 applied to the concatenated
  * population):

@@ -123,6 +123,9 @@ SIGNATURES = {
     "gfmc_evolve": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                    ctypes.c_double, _u32p, ctypes.c_longlong, ctypes.c_int, _vp,
                                    _vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp]),
+    "gfmc_evolve_walkers": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                           ctypes.c_double, _u32p, ctypes.c_int, _vp, _vp, _vp, _vp,
+                                           _vp, _vp]),
     "gfmc_dist_local_max": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _dp, _vp]),
     "gfmc_dist_local_sums": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.c_double, _dp,
                                             _vp]),

@@ -1775,13 +1775,18 @@ int gfmc_rbm_hidden_padded(const gfmc_handle *h) {
   return (h && h->rbm_on) ? h->rbm.Hp : GFMC_ERR_INVALID;
 }
 
-int gfmc_evolve(gfmc_handle *h, int method, double step, double lam, double alw,
-                const uint32_t key[2], long long walker_offset, int n, const void *cfg,
-                const int32_t *parents, int parents_valid, void *cfg_out, double *log_w,
-                double *e_loc, uint64_t *hops, void *stream) {
+// The evolve half of a step alone (gfmc_evolve, gfmc_evolve_walkers): lw_in,
+// when given, seeds each walker's log weight (read at its parent); log_w may
+// be the same array when there is no parent map, since the warp that owns a
+// walker reads its entry before it writes it and no other warp touches it.
+static int evolve_only(gfmc_handle *h, const char *name, int method, double step, double lam,
+                       double alw, const uint32_t key[2], long long walker_offset, int n,
+                       const void *cfg, const int32_t *parents, int parents_valid, void *cfg_out,
+                       const double *lw_in, double *log_w, double *e_loc, uint64_t *hops,
+                       void *stream) {
   if (!h || !key || n <= 0 || !cfg || !cfg_out || cfg == cfg_out || !log_w || !e_loc ||
-      (parents_valid && !parents) || walker_offset < 0)
-    return fail(GFMC_ERR_INVALID, "gfmc_evolve: bad argument");
+      (parents_valid && !parents) || walker_offset < 0 || (lw_in == log_w && parents_valid))
+    return fail(GFMC_ERR_INVALID, "%s: bad argument", name);
   int rc = check_method(method, step);
   if (rc) return rc;
   if (h->mlp_on && method != CONT_TIME)
@@ -1803,6 +1808,7 @@ int gfmc_evolve(gfmc_handle *h, int method, double step, double lam, double alw,
   a.cfg_in = cfg;
   a.cfg_out = cfg_out;
   a.log_w = log_w;
+  a.lw_in = lw_in;
   a.e_loc = e_loc;
   a.hops = (unsigned long long *)hops;
   a.work_ctr = h->ctr;
@@ -1825,6 +1831,21 @@ int gfmc_evolve(gfmc_handle *h, int method, double step, double lam, double alw,
                                             : launch_step<float>(h, h->m32, h->g32, a, s);
   if (e != cudaSuccess) return fail(GFMC_ERR_CUDA, "evolve launch: %s", cudaGetErrorString(e));
   return GFMC_OK;
+}
+
+int gfmc_evolve(gfmc_handle *h, int method, double step, double lam, double alw,
+                const uint32_t key[2], long long walker_offset, int n, const void *cfg,
+                const int32_t *parents, int parents_valid, void *cfg_out, double *log_w,
+                double *e_loc, uint64_t *hops, void *stream) {
+  return evolve_only(h, "gfmc_evolve", method, step, lam, alw, key, walker_offset, n, cfg, parents,
+                     parents_valid, cfg_out, nullptr, log_w, e_loc, hops, stream);
+}
+
+int gfmc_evolve_walkers(gfmc_handle *h, int method, double step, double lam, double alw,
+                        const uint32_t key[2], int n, const void *cfg, void *cfg_out,
+                        double *log_w, double *e_loc, uint64_t *hops, void *stream) {
+  return evolve_only(h, "gfmc_evolve_walkers", method, step, lam, alw, key, 0, n, cfg, nullptr, 0,
+                     cfg_out, log_w, log_w, e_loc, hops, stream);
 }
 
 static int dist_prepare(gfmc_handle *h, int n) {

@@ -147,6 +147,10 @@ struct EvolveArgs {
   // whose first evaluation is then that record; nullable
   const void *eval_in;
   void *eval_out;
+  // incoming log weights, read at parents[w] (nullable: every walker starts
+  // from 0, its state after resampling); the step's log weight accumulates
+  // onto it as PyGFMC's evolve_walkers does (engine/evolution.py:356-400)
+  const double *lw_in;
 };
 constexpr int EVAL_REC = 68;
 

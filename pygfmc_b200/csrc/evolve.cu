@@ -665,7 +665,7 @@ evolve_kernel(DevModel<T> m, DevGuide<T> g, EvolveArgs a, int stage_nbr, int cta
     if (FAM != SPIN_HALF && guided) bose_factors(g, SF, m.N, lane);
 
     const Key kw = fold(a.key, (uint32_t)(a.walker_offset + walker));
-    double lw = 0.0;
+    double lw = a.lw_in ? a.lw_in[src] : 0.0;
     T eloc = T(0);
     int hops = 0;
     T draws = T(0);   // draws of 16 holds (cont/multi) or uniforms of 32 sub-steps (single)

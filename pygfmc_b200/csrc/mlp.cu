@@ -387,7 +387,7 @@ __global__ void __launch_bounds__(MT, 1) mlp_evolve_kernel(DevModel<float> m, Ml
     }
 
     const Key kw = fold(a.key, (uint32_t)(a.walker_offset + walker));
-    double lw = 0.0;
+    double lw = a.lw_in ? a.lw_in[src] : 0.0;
     float eloc = 0.0f;
     int hops = 0;
     if (a.method == CONT_TIME) {

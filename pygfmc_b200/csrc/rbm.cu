@@ -161,7 +161,7 @@ rbm_evolve_kernel(DevModel<T> m, RbmTables r, EvolveArgs a) {
     }
 
     const Key kw = fold(a.key, (uint32_t)(a.walker_offset + walker));
-    double lw = 0.0;
+    double lw = a.lw_in ? a.lw_in[src] : 0.0;
     T eloc = T(0);
     int hops = 0;
     T draws = T(0);

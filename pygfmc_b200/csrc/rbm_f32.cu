@@ -306,7 +306,7 @@ rbm_evolve_f32_kernel(DevModel<float> m, RbmTables r, EvolveArgs a) {
       }
     }
     w.kw = fold(a.key, (uint32_t)(a.walker_offset + wk));
-    w.lw = 0.0;
+    w.lw = a.lw_in ? a.lw_in[w.src] : 0.0;
     w.eloc = 0.0f;
     w.t = 0.0f;
     w.draws = 0.0f;

@@ -28,7 +28,8 @@ from .wavefunction import JastrowBoseHubbard, JastrowSpinHalf, MLPBoseHubbard, R
 from .estimators import (autocorrelation_stats, diagonal_estimates, off_diagonal_estimates,
                          validated_p_array, windowed_energy_host)
 
-__all__ = ["run", "run_gfmc", "GFMCEngine", "DEFAULT_WARMUP_STEPS"]
+__all__ = ["run", "run_gfmc", "GFMCEngine", "DEFAULT_WARMUP_STEPS", "evolve_walkers",
+           "estimate_average_log_branch_weight"]
 
 DEFAULT_WARMUP_STEPS = 1000
 _AUX_ROOT = 9_000
@@ -860,6 +861,85 @@ def _weight_dtype(lw):
         return np.dtype(np.float64)
     name = str(dt).replace("torch.", "")
     return np.dtype(np.float32) if name in ("float32", "bfloat16", "float16") else np.dtype(np.float64)
+
+
+def _population_engine(walkers, hamiltonian, guide, precision):
+    """A GFMCEngine holding the host population ``walkers`` (validated)."""
+    config = np.asarray(walkers.config)
+    n = config.shape[0] if config.ndim == 2 else -1
+    if n < 1 or np.shape(walkers.log_weight) != (n,) or np.shape(walkers.e_loc) != (n,):
+        raise ValueError(f"walkers must hold config (N_walkers, N_sites) with N_walkers >= 1 and "
+                         f"log_weight, e_loc of shape (N_walkers,); got {config.shape}, "
+                         f"{np.shape(walkers.log_weight)} and {np.shape(walkers.e_loc)}.")
+    require_operator_protocol(hamiltonian)
+    if guide is not None:
+        require_guide_protocol(guide)
+    if precision is None:
+        precision = "fp64" if _weight_dtype(walkers.log_weight) == np.float64 \
+            and not isinstance(guide, MLPBoseHubbard) else "mixed"
+    eng = GFMCEngine(hamiltonian, guide, n, precision=precision)
+    eng.load(config)
+    return eng
+
+
+def evolve_walkers(walkers, hamiltonian, step_size, guide, method, rng_key, avg_log_weight,
+                   lam=None, cache=None, rates=None, state=None, return_rates=False, precision=None):
+    """One evolution of the whole population without resampling, on the GPU
+    (engine/evolution.py evolve_walkers:761-843): walker i draws from
+    split(rng_key, N_walkers)[i]; its log weight accumulates onto
+    ``walkers.log_weight`` (the step's terms added to the incoming value in
+    PyGFMC's order, then avg_log_weight x beta or x n_bra subtracted); its
+    ``e_loc`` is the local energy of its final configuration.  ``step_size``
+    is beta for cont_time and the number of sub-steps for the discrete
+    methods, which need ``lam``.
+
+    ``cache``, ``rates`` and ``state`` are accepted for PyGFMC's signature
+    and not needed: the device builds the tables and the guide state from the
+    configurations, which gives the same walk (in PyGFMC they only spare a
+    recomputation).  ``return_rates=True`` is refused: the device keeps each
+    walker's evaluation itself, and chained steps belong to ``run`` /
+    ``GFMCEngine``.  Float64 weights select the fp64 build, float32 the mixed
+    build (log weights accumulate in float64 there and are returned in the
+    input's dtype), or pass ``precision``.  Returns a Walker of host arrays
+    in the input's dtypes."""
+    require_step_size(method, step_size)
+    lam = require_lam(method, lam)
+    if return_rates:
+        raise ValueError("return_rates=True is not available: the device engine carries each walker's "
+                         "rate evaluation from step to step itself; use run() or GFMCEngine for "
+                         "chained steps.")
+    eng = _population_engine(walkers, hamiltonian, guide, precision)
+    torch = eng.torch
+    lw = torch.as_tensor(np.ascontiguousarray(walkers.log_weight, dtype=np.float64)).to(eng.device)
+    cfg_out = torch.empty_like(eng.cfg)
+    key = np.ascontiguousarray(_rnd.as_key(rng_key), dtype=np.uint32)
+    _lib.check(eng.L.gfmc_evolve_walkers(
+        eng.h, _lib.METHODS[method], float(step_size), float(lam if lam is not None else 0.0),
+        float(avg_log_weight), key.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), eng.n,
+        eng._ptr(eng.cfg), eng._ptr(cfg_out), eng._ptr(lw), eng._ptr(eng.e_loc), ctypes.c_void_p(0),
+        eng._stream()), "evolve_walkers")
+    _device_status_check(eng)
+    out = torch.empty((eng.n, eng.N), dtype=torch.float64, device=eng.device)
+    _lib.check(eng.L.gfmc_unpack(eng.h, eng.n, eng._ptr(cfg_out), eng._ptr(out), eng._stream()),
+               "gfmc_unpack")
+    cfg_dt = np.asarray(walkers.config).dtype
+    return Walker(config=out.cpu().numpy().astype(cfg_dt, copy=False),
+                  log_weight=lw.cpu().numpy().astype(np.asarray(walkers.log_weight).dtype, copy=False),
+                  e_loc=eng.e_loc.cpu().numpy().astype(np.asarray(walkers.e_loc).dtype, copy=False))
+
+
+def estimate_average_log_branch_weight(walkers, hamiltonian, guide, method="cont_time", lam=None,
+                                       cache=None, precision=None):
+    """The starting avg_log_weight of a run (engine/estimators.py:722-751):
+    mean(-e_L) for cont_time (per unit imaginary time), mean(log(lam - e_L))
+    for the discrete methods (per sub-step), e_L = the sum of the
+    guide-transformed rates of each walker's configuration, evaluated on the
+    GPU.  ``cache`` is accepted for PyGFMC's signature and not needed."""
+    lam = require_lam(method, lam)
+    eng = _population_engine(walkers, hamiltonian, guide, precision)
+    e = eng.local_energy().cpu().numpy()
+    _device_status_check(eng)
+    return float(np.mean(-e)) if method == "cont_time" else float(np.mean(np.log(lam - e)))
 
 
 def run_gfmc(walkers, n_steps, hamiltonian, step_size, guide, p_array, *, method="cont_time",
