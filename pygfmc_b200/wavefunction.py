@@ -150,6 +150,14 @@ class JastrowBoseHubbard:
     and the parameters ``_beta``, ``_h``, ``_d`` in the form they were given
     (None, a 0-d tied value or one per pair / site), rounded to ``dtype``.
     The engine lowers a guide from exactly these attributes.
+
+    ``incremental`` is kept as an attribute and does not change what runs:
+    the device always carries each walker's weighted neighbour sums, updates
+    them additively per move and rebuilds them every 100 steps (50 in the
+    float32 build) -- the policy of PyGFMC's incremental mode
+    (engine/evolution.py:167,181-189) -- so its
+    ratios agree with both of PyGFMC's modes to rounding, not bit for bit
+    with either.
     """
 
     def __init__(self, N, pairs, beta, h=None, d=None, dtype=np.float32, incremental=False):
