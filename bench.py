@@ -662,9 +662,10 @@ def sigma_short(P, steps_scale=1.0):
     """A short version of the sigma study (--study sigma) on the 16x16
     Heisenberg lattice: an RBM (H = 512) trained by variance minimisation for
     150 iterations on 32768 walkers, then fixed-length productions of the
-    trained RBM (float32 build, 400 steps) and of the long-range Jastrow
-    guide (float64 build, 2000 steps), 32768 walkers each, tau = 0.05,
-    blocked jackknife (10 blocks) at p = 32; GPU seconds to sigma(E/N) = 1e-5
+    trained RBM (float32 build, 1000 steps) and of the long-range Jastrow
+    guide (float64 build, 5000 steps), 32768 walkers each, tau = 0.05,
+    blocked jackknife (10 blocks, each at least three times the p = 32
+    window) at p = 32; GPU seconds to sigma(E/N) = 1e-5
     = production time x (sigma / 1e-5)^2.  Short runs: the ratio is an
     estimate (the full study trains for 600 iterations and runs longer)."""
     import torch
@@ -675,8 +676,8 @@ def sigma_short(P, steps_scale=1.0):
         n_iterations=max(10, int(150 * steps_scale)), steps_per_iteration=3, step_size=TAU, lr=3e-4,
         rng_key=P.PRNGKey(14), warmup_steps=100, verbosity=0)
     res = {}
-    for key, G, steps, prec in (("rbm_h512_mixed", trained, max(40, int(400 * steps_scale)), "mixed"),
-                                ("jastrow_fp64", GJ, max(200, int(2000 * steps_scale)), "fp64")):
+    for key, G, steps, prec in (("rbm_h512_mixed", trained, max(40, int(1000 * steps_scale)), "mixed"),
+                                ("jastrow_fp64", GJ, max(200, int(5000 * steps_scale)), "fp64")):
         w = P.prepare_walkers_sz(n, 256, P.PRNGKey(11), sz=0)
         torch.cuda.synchronize()
         wf, _, _, st, raw = P.run(w, steps, H, TAU, G, [8, 32], rng_key=P.PRNGKey(12),
