@@ -874,6 +874,8 @@ def _population_engine(walkers, hamiltonian, guide, precision):
     require_operator_protocol(hamiltonian)
     if guide is not None:
         require_guide_protocol(guide)
+    if precision not in (None, "fp64", "mixed"):
+        raise ValueError(f"precision must be 'fp64', 'mixed' or None, got {precision!r}")
     if precision is None:
         precision = "fp64" if _weight_dtype(walkers.log_weight) == np.float64 \
             and not isinstance(guide, MLPBoseHubbard) else "mixed"

@@ -46,6 +46,10 @@ def test_arguments_are_checked_before_any_device_work():
         evolve_walkers(w._replace(e_loc=w.e_loc[:3]), H, 0.1, None, "cont_time", key, 0.0)
     with pytest.raises(ValueError, match="lam"):
         estimate_average_log_branch_weight(w, H, None, method="multi_step")
+    with pytest.raises(ValueError, match="precision"):
+        evolve_walkers(w, H, 0.1, None, "cont_time", key, 0.0, precision="fp16")
+    with pytest.raises(TypeError):
+        evolve_walkers(w, object(), 0.1, None, "cont_time", key, 0.0)       # not an operator
     assert {"evolve_walkers", "estimate_average_log_branch_weight"} <= set(P.engine.__all__)
 
 
