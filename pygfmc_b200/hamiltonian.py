@@ -846,37 +846,30 @@ def exact_diagonalization(hamiltonian, local_hilbert_space=None, N=None, diag_op
     diag_obs, off_diag_obs)`` and the states (dim, number_of_states) when
     ``return_states``; ``diag_obs[name][k] = sum_x |psi_k(x)|^2 O(x)`` through
     ``diagonal_weight``, ``off_diag_obs[name][k] = psi_k^T O psi_k``."""
+    # the checks in PyGFMC's order and with its key phrases
+    # (hamiltonian/exact.py:266-345)
+    name = type(hamiltonian).__name__
     if local_hilbert_space is None:
         local_hilbert_space = getattr(hamiltonian, "local_hilbert_space", None)
         if local_hilbert_space is None:
-            raise ValueError(f"{type(hamiltonian).__name__} exposes no local_hilbert_space; pass it")
+            raise ValueError(f"local_hilbert_space was not given and {name} exposes no "
+                             "local_hilbert_space attribute.")
     values = np.asarray(local_hilbert_space, dtype=np.float64).ravel()
     d = values.size
-    if d < 2 or not np.all(np.isfinite(values)) or np.unique(values).size != d:
-        raise ValueError(f"local_hilbert_space must hold at least two distinct finite values, got "
-                         f"{values.tolist()}")
-    own = getattr(hamiltonian, "local_hilbert_space", None)
-    if own is not None and not np.array_equal(np.sort(np.asarray(own, np.float64).ravel()),
-                                              np.sort(values)):
-        raise ValueError(f"local_hilbert_space {values.tolist()} is not the set of values "
-                         f"{list(own)} the Hamiltonian acts on")
+    if d < 2:
+        raise ValueError(f"local_hilbert_space needs at least two values, got {values.tolist()}.")
+    if not np.all(np.isfinite(values)) or np.unique(values).size != d:
+        raise ValueError(f"local_hilbert_space must hold distinct finite values, got {values.tolist()}.")
     if N is None:
         N = getattr(hamiltonian, "N", None)
         if N is None:
-            raise ValueError(f"{type(hamiltonian).__name__} exposes no N; pass it")
+            raise ValueError(f"N was not given and {name} exposes no N attribute, so the size of "
+                             "the basis is unknown.")
     N = int(N)
-    # a basis of the wrong size gives a plausible spectrum of another problem:
-    # cross-check the site count and local dimension the operator reports
-    own_N = getattr(hamiltonian, "N", None)
-    if own_N is not None and int(own_N) != N:
-        raise ValueError(f"N={N} but {type(hamiltonian).__name__} acts on {int(own_N)} sites")
-    own_d = getattr(hamiltonian, "d", None)
-    if own_d is not None and int(own_d) != d:
-        raise ValueError(f"local_hilbert_space has {d} values but {type(hamiltonian).__name__} "
-                         f"reports a local dimension of {int(own_d)}")
     dim = d ** N
     if dim > _ED_MAX_DIM:
-        raise ValueError(f"a basis of {d}**{N} = {dim} states is above the {_ED_MAX_DIM} limit")
+        raise ValueError(f"basis of {d}**{N} = {dim} states exceeds the {_ED_MAX_DIM} limit; exact "
+                         "diagonalisation is not the right tool at this size.")
     k = int(number_of_states)
     if k != number_of_states or not 1 <= k <= dim:
         raise ValueError(f"number_of_states must be an integer in [1, {dim}], got {number_of_states!r}")
@@ -889,6 +882,21 @@ def exact_diagonalization(hamiltonian, local_hilbert_space=None, N=None, diag_op
     if need > _ED_MAX_BYTES:
         raise ValueError(f"exact diagonalisation of {dim} states would allocate about "
                          f"{need / 2 ** 30:.1f} GiB, above the {_ED_MAX_BYTES / 2 ** 30:.0f} GiB limit")
+    # a basis of the wrong size or values gives a plausible spectrum of another
+    # problem: cross-check what the operator reports
+    own_N = getattr(hamiltonian, "N", None)
+    if own_N is not None and int(own_N) != N:
+        raise ValueError(f"N={N} but the Hamiltonian reports N={int(own_N)}; the basis would not be "
+                         "the one it acts on.")
+    own_d = getattr(hamiltonian, "d", None)
+    if own_d is not None and int(own_d) != d:
+        raise ValueError(f"local_hilbert_space has {d} values {values.tolist()} but the Hamiltonian "
+                         f"reports a local dimension of {int(own_d)}.")
+    own = getattr(hamiltonian, "local_hilbert_space", None)
+    if own is not None and not np.array_equal(np.sort(np.asarray(own, np.float64).ravel()),
+                                              np.sort(values)):
+        raise ValueError(f"local_hilbert_space {values.tolist()} is not the set of values "
+                         f"{list(own)} the Hamiltonian acts on")
     configs, powers = _basis(values, N)
     H = _protocol_matrix(hamiltonian, configs, values, powers)
     if dense:

@@ -90,8 +90,33 @@ def test_exact_diagonalization_rejects_bad_arguments():
         P.exact_diagonalization(H, number_of_states=65)
     with pytest.raises(ValueError, match="limit"):
         P.exact_diagonalization(_ring(N=25))
-    with pytest.raises(ValueError, match="acts on 6 sites"):
+    with pytest.raises(ValueError, match="Hamiltonian reports N=6"):
         P.exact_diagonalization(H, N=7)
+
+
+class _ThreeStateStandIn:
+    """A three-state operator's reported sizes (spin 1 on three sites)."""
+    N, d, M_total = 3, 3, 1
+
+
+def test_exact_diagonalization_messages_of_the_reference():
+    """The validation pins of PyGFMC's tests/core/test_exact_diagonalization.py
+    :95-113, in its order: too few values, a basis above the limit (checked
+    before the site count), state counts outside [1, dim], an N or a local
+    dimension contradicting the operator."""
+    h = P.SpinHalf.create(P.chain(4).edges, -1.0, -1.0, 1.0, dtype=np.float64)
+    with pytest.raises(ValueError, match="at least two values"):
+        P.exact_diagonalization(h, (1,), 4)
+    with pytest.raises(ValueError, match="exceeds the"):
+        P.exact_diagonalization(h, (-1, 1), 40)
+    with pytest.raises(ValueError, match="number_of_states"):
+        P.exact_diagonalization(h, (-1, 1), 4, number_of_states=0)
+    with pytest.raises(ValueError, match="number_of_states"):
+        P.exact_diagonalization(h, (-1, 1), 4, number_of_states=17)     # dim = 16
+    with pytest.raises(ValueError, match="Hamiltonian reports N"):
+        P.exact_diagonalization(h, (-1, 1), 5)
+    with pytest.raises(ValueError, match="local dimension"):
+        P.exact_diagonalization(_ThreeStateStandIn(), (-1, 1), 3)
     # the allocation estimate (basis, matrix triplets, dense solve) is checked
     # before anything is built
     old = P.hamiltonian._ED_MAX_BYTES
