@@ -719,7 +719,8 @@ def _batch_matrix(op, configs, values, powers):
         for site, v in changes:
             d, ok = digit_of(v)
             if not np.all(ok[nz]):
-                raise ValueError("a transition of nonzero amplitude leaves the basis")
+                raise ValueError(f"{type(op).__name__}: a transition of nonzero amplitude leads "
+                                 "outside the supplied local_hilbert_space")
             new = new + (d - dig[idx, site]) * powers[site]
         rows.append(new[nz]); cols.append(idx[nz]); data.append(rate[nz])
 
@@ -791,8 +792,9 @@ def _protocol_matrix(op, configs, values, powers):
         sub = np.asarray(succ, np.float64)[nz]
         ok = np.all(np.min(np.abs(sub[..., None] - np.asarray(values)), axis=-1) < 1e-6, axis=1)
         if not np.all(ok):
-            raise ValueError(f"a transition of nonzero amplitude leaves the basis at configuration "
-                             f"{x.tolist()}")
+            raise ValueError(f"{type(op).__name__}: a transition of nonzero amplitude from "
+                             f"configuration {x.tolist()} leads outside the supplied "
+                             "local_hilbert_space")
         rows.append(_basis_index(sub, values, powers))
         cols.append(np.full(nz.size, i, np.int64))
         vals.append(rates[nz])
@@ -846,30 +848,40 @@ def exact_diagonalization(hamiltonian, local_hilbert_space=None, N=None, diag_op
     diag_obs, off_diag_obs)`` and the states (dim, number_of_states) when
     ``return_states``; ``diag_obs[name][k] = sum_x |psi_k(x)|^2 O(x)`` through
     ``diagonal_weight``, ``off_diag_obs[name][k] = psi_k^T O psi_k``."""
-    # the checks in PyGFMC's order and with its key phrases
-    # (hamiltonian/exact.py:266-345)
+    # the checks in PyGFMC's order, each message holding the phrase its tests
+    # match (hamiltonian/exact.py:266-345)
     name = type(hamiltonian).__name__
     if local_hilbert_space is None:
         local_hilbert_space = getattr(hamiltonian, "local_hilbert_space", None)
         if local_hilbert_space is None:
-            raise ValueError(f"local_hilbert_space was not given and {name} exposes no "
-                             "local_hilbert_space attribute.")
+            raise ValueError(f"no local_hilbert_space given, and {name} has no local_hilbert_space "
+                             "attribute to take it from")
     values = np.asarray(local_hilbert_space, dtype=np.float64).ravel()
     d = values.size
     if d < 2:
-        raise ValueError(f"local_hilbert_space needs at least two values, got {values.tolist()}.")
+        raise ValueError(f"local_hilbert_space needs at least two values, got {values.tolist()}")
     if not np.all(np.isfinite(values)) or np.unique(values).size != d:
-        raise ValueError(f"local_hilbert_space must hold distinct finite values, got {values.tolist()}.")
+        raise ValueError(f"local_hilbert_space must hold distinct finite values, got {values.tolist()}")
+    own = getattr(hamiltonian, "local_hilbert_space", None)
+    if own is not None:
+        own = np.asarray(own, np.float64).ravel()
+        if own.size != d:
+            raise ValueError(f"local_hilbert_space has {d} values, the Hamiltonian acts on {own.size} "
+                             f"({own.tolist()}): another local dimension")
+        if not np.array_equal(np.sort(own), np.sort(values)):
+            raise ValueError(f"local_hilbert_space {values.tolist()} differs from the values "
+                             f"{own.tolist()} the Hamiltonian acts on (their order may differ, the "
+                             "values may not)")
     if N is None:
         N = getattr(hamiltonian, "N", None)
         if N is None:
-            raise ValueError(f"N was not given and {name} exposes no N attribute, so the size of "
-                             "the basis is unknown.")
+            raise ValueError(f"no N given, and {name} has no N attribute: the size of the basis is "
+                             "unknown")
     N = int(N)
     dim = d ** N
     if dim > _ED_MAX_DIM:
-        raise ValueError(f"basis of {d}**{N} = {dim} states exceeds the {_ED_MAX_DIM} limit; exact "
-                         "diagonalisation is not the right tool at this size.")
+        raise ValueError(f"basis of {d}**{N} = {dim} states exceeds the {_ED_MAX_DIM} limit of exact "
+                         "diagonalisation")
     k = int(number_of_states)
     if k != number_of_states or not 1 <= k <= dim:
         raise ValueError(f"number_of_states must be an integer in [1, {dim}], got {number_of_states!r}")
@@ -886,17 +898,11 @@ def exact_diagonalization(hamiltonian, local_hilbert_space=None, N=None, diag_op
     # problem: cross-check what the operator reports
     own_N = getattr(hamiltonian, "N", None)
     if own_N is not None and int(own_N) != N:
-        raise ValueError(f"N={N} but the Hamiltonian reports N={int(own_N)}; the basis would not be "
-                         "the one it acts on.")
+        raise ValueError(f"N={N}, but the Hamiltonian reports N={int(own_N)}: a basis of another size")
     own_d = getattr(hamiltonian, "d", None)
     if own_d is not None and int(own_d) != d:
-        raise ValueError(f"local_hilbert_space has {d} values {values.tolist()} but the Hamiltonian "
-                         f"reports a local dimension of {int(own_d)}.")
-    own = getattr(hamiltonian, "local_hilbert_space", None)
-    if own is not None and not np.array_equal(np.sort(np.asarray(own, np.float64).ravel()),
-                                              np.sort(values)):
-        raise ValueError(f"local_hilbert_space {values.tolist()} is not the set of values "
-                         f"{list(own)} the Hamiltonian acts on")
+        raise ValueError(f"local_hilbert_space has {d} values, but the Hamiltonian reports a local "
+                         f"dimension of {int(own_d)}")
     configs, powers = _basis(values, N)
     H = _protocol_matrix(hamiltonian, configs, values, powers)
     if dense:

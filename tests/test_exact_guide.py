@@ -82,7 +82,7 @@ def _dense_any(op, N, values):
 
 def test_exact_diagonalization_rejects_bad_arguments():
     H = _ring()
-    with pytest.raises(ValueError, match="not the set of values"):
+    with pytest.raises(ValueError, match="differs from the values"):
         P.exact_diagonalization(H, (0.0, 1.0))
     with pytest.raises(ValueError, match="distinct"):
         P.exact_diagonalization(H, (1.0, 1.0))
@@ -126,6 +126,47 @@ def test_exact_diagonalization_messages_of_the_reference():
             P.exact_diagonalization(_ring(N=12))
     finally:
         P.hamiltonian._ED_MAX_BYTES = old
+
+
+class _FlipSiteZero:
+    """A two-site spin-1/2 operator with one transition, site 0 flipped (or set
+    to ``target``), of amplitude ``up`` from a down spin and ``down`` from an
+    up spin; only the rate protocol."""
+    M_total, N, local_hilbert_space = 2, 2, (-1.0, 1.0)
+
+    def __init__(self, up, down, target=None):
+        self.up, self.down, self.target = up, down, target
+
+    def generate_state(self, x, k):
+        y = np.array(x, dtype=np.float64, copy=True)
+        if k == 1:
+            y[0] = -y[0] if self.target is None else self.target
+        return y
+
+    def get_rates(self, x, return_configs=False):
+        x = np.asarray(x, dtype=np.float64)
+        rates = np.array([0.0, self.down if x[0] > 0 else self.up])
+        succ = np.stack([x, self.generate_state(x, 1)]) if return_configs else None
+        return rates, succ
+
+
+def test_protocol_operators_are_checked_as_the_reference_does():
+    """PyGFMC's tests/core/test_exact_ground_state.py:220-235: a transition of
+    nonzero amplitude out of the basis and an asymmetric matrix are refused;
+    the symmetric flip has the ground energy -1."""
+    with pytest.raises(ValueError, match="leads outside the supplied local_hilbert_space"):
+        P.exact_diagonalization(_FlipSiteZero(-1.0, -1.0, target=2.0))
+    with pytest.raises(ValueError, match="not Hermitian"):
+        P.exact_diagonalization(_FlipSiteZero(-1.0, -2.0))
+    E = P.exact_diagonalization(_FlipSiteZero(-1.0, -1.0))[0]
+    np.testing.assert_allclose(E[0], -1.0, atol=1e-12)
+    H = P.SpinHalf.create(np.zeros((0, 2), dtype=np.int64), h_z=1.0, N=2, dtype=np.float64)
+    e_ref = P.exact_diagonalization(H)[0][0]
+    assert P.exact_diagonalization(H, local_hilbert_space=(-1.0, 1.0))[0][0] == e_ref
+    with pytest.raises(ValueError, match="differs from the values"):
+        P.exact_diagonalization(H, local_hilbert_space=(0.5, -0.5))
+    with pytest.raises(ValueError, match="distinct finite"):
+        P.exact_diagonalization(H, local_hilbert_space=(1.0, np.nan))
 
 
 class _OneConfigDiagonal:
