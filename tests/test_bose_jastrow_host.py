@@ -1,0 +1,66 @@
+"""JastrowBoseHubbard's ratios on the host and in the oracle, over every block
+of the Bose-Hubbard transition layout (hopping, pair creation and
+annihilation, single-site terms) and every parameter form (tied, per pair /
+per site, absent), with guide pairs that differ from the bonds and repeat one
+pair -- the cases of PyGFMC's tests/core/test_jastrow_bose_hubbard.py:19-66:
+``log_diff_from_operator`` equals log_psi differences over the successors
+``get_rates`` returns, and the oracle's guided rates (what the device is
+checked against) are the bare rates times exp of those ratios.  Host only."""
+import itertools
+
+import numpy as np
+import pytest
+
+import pygfmc_b200 as P
+from oracle_guides import oracle_guide
+
+L = 9
+EDGES = np.asarray(P.chain(L).edges)
+PAIRS = np.concatenate([EDGES, [[0, 4], [2, 7], [1, 2]]])      # (1, 2) twice
+_rng = np.random.default_rng(3)
+MODELS = {
+    "hopping": dict(t=1.0, U=2.0, n_max=2),
+    "hopping+pairs": dict(t=1.0, eta=0.25, U=4.0, mu=1.0, n_max=3),
+    "pairs+h_pm": dict(eta=0.3, h_pm=0.2, U=1.0, n_max=3, N=L),
+    "all": dict(t=1.0, eta=0.2, h_pm=0.1, U=3.0, mu=0.5, n_max=2, N=L),
+}
+FORMS = {
+    "tied beta, h, d": dict(beta=0.21, h=0.13, d=0.37),
+    "tied beta only": dict(beta=0.21),
+    "per pair / per site": dict(beta=_rng.uniform(-0.2, 0.4, len(PAIRS)),
+                                h=_rng.uniform(-0.3, 0.3, L), d=_rng.uniform(0.1, 0.6, L)),
+    "tied beta, per site d, no h": dict(beta=0.15, d=_rng.uniform(0.1, 0.6, L)),
+}
+
+
+def _guide(form):
+    return P.JastrowBoseHubbard(L, PAIRS, dtype=np.float64, **FORMS[form])
+
+
+@pytest.mark.parametrize("name,form", list(itertools.product(MODELS, FORMS)))
+def test_ratio_equals_log_psi_differences(name, form):
+    H = P.BoseHubbard.create(EDGES, dtype=np.float64, **MODELS[name])
+    G = _guide(form)
+    x = np.random.default_rng(0).integers(0, int(H.n_max) + 1, (40, L)).astype(np.float64)
+    for c in x:
+        fast = np.asarray(G.log_diff_from_operator(c, H), np.float64)
+        rates, succ = H.get_rates(c, return_configs=True)
+        assert fast.shape == (H.M_total,)
+        ref = np.array([G.log_psi(s) for s in succ]) - G.log_psi(c)
+        live = np.asarray(rates) != 0          # the moves that exist from c
+        np.testing.assert_allclose(fast[live], ref[live], rtol=0, atol=1e-12)
+
+
+@pytest.mark.parametrize("name,form", list(itertools.product(MODELS, FORMS)))
+def test_oracle_guided_rates(oracle, name, form):
+    H = P.BoseHubbard.create(EDGES, dtype=np.float64, **MODELS[name])
+    G = _guide(form)
+    kw = {k: v for k, v in MODELS[name].items() if k != "N"}
+    m = oracle.bose_hubbard(EDGES, **kw)
+    g = oracle_guide(oracle, G, m)
+    x = np.random.default_rng(1).integers(0, int(H.n_max) + 1, (16, L)).astype(np.float64)
+    guided, bare = oracle.rates(m, g, x), oracle.rates(m, oracle.no_guide(), x)
+    for w in range(len(x)):
+        ld = np.asarray(G.log_diff_from_operator(x[w], H), np.float64)
+        expect = bare[w] * np.exp(np.where(bare[w] == 0, 0.0, ld))
+        np.testing.assert_allclose(guided[w], expect, rtol=1e-12, atol=1e-14, err_msg=f"{name} {form}")
