@@ -353,6 +353,20 @@ class BoseHubbard:
                 a += list(range(N)); b += list(range(N)); da += [s] * N; db += [0] * N
         return np.array(a), np.array(b), np.array(da), np.array(db)
 
+    def move(self, config, idx):
+        """The sites transition ``idx`` changes and their increments
+        (hamiltonian/bose_hubbard.py move:427-435): ``(sites, deltas)`` of
+        shape (2,) each, ``generate_state`` being ``config`` with ``deltas``
+        added at ``sites``; the diagonal has zero increments and a single-site
+        term repeats its site with increment 0."""
+        a, b, da, db = self.moves()
+        k = int(idx)
+        if not 0 <= k < len(a):
+            raise ValueError(f"transition index {k} outside [0, {len(a)})")
+        dt = np.asarray(config).dtype
+        dt = dt if dt.kind == "f" else np.dtype(np.float64)
+        return np.array([a[k], b[k]]), np.array([da[k], db[k]], dtype=dt)
+
     def diagonal_weight(self, config):
         n = np.asarray(config, dtype=np.float64)
         out = 0.0

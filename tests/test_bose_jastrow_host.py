@@ -5,7 +5,9 @@ per site, absent), with guide pairs that differ from the bonds and repeat one
 pair -- the cases of PyGFMC's tests/core/test_jastrow_bose_hubbard.py:19-66:
 ``log_diff_from_operator`` equals log_psi differences over the successors
 ``get_rates`` returns, and the oracle's guided rates (what the device is
-checked against) are the bare rates times exp of those ratios.  Host only."""
+checked against) are the bare rates times exp of those ratios.  Also the
+operators' ``move`` and ``diagonal_weight`` against ``generate_state`` and
+``get_rates`` (tests/core/test_get_rates_all_classes.py).  Host only."""
 import itertools
 
 import numpy as np
@@ -64,3 +66,46 @@ def test_oracle_guided_rates(oracle, name, form):
         ld = np.asarray(G.log_diff_from_operator(x[w], H), np.float64)
         expect = bare[w] * np.exp(np.where(bare[w] == 0, 0.0, ld))
         np.testing.assert_allclose(guided[w], expect, rtol=1e-12, atol=1e-14, err_msg=f"{name} {form}")
+
+
+def test_move_reproduces_generate_state():
+    """hamiltonian/bose_hubbard.py move:427-435 (PyGFMC's
+    tests/core/test_get_rates_all_classes.py:154-177): adding ``deltas`` at
+    ``sites`` gives ``generate_state`` for every transition."""
+    ring = np.asarray([[i, (i + 1) % 6] for i in range(6)])
+    H = P.BoseHubbard.create(ring, t=1.0, eta=0.3, U=2.0, mu=0.5, h_pm=0.2, N=6, n_max=2,
+                             dtype=np.float64)
+    rng = np.random.default_rng(0)
+    for _ in range(3):
+        x = rng.choice(np.asarray(H.local_hilbert_space), size=H.N)
+        for idx in range(H.M_total):
+            sites, deltas = H.move(x, idx)
+            assert sites.shape == (2,) and deltas.shape == (2,)
+            y = np.array(x, copy=True)
+            y[sites[0]] += deltas[0]
+            y[sites[1]] += deltas[1]
+            np.testing.assert_array_equal(y, H.generate_state(x, idx))
+    with pytest.raises(ValueError):
+        H.move(x, H.M_total)
+
+
+def test_diagonal_weight_is_the_first_rate():
+    """tests/core/test_get_rates_all_classes.py:110-125 on the all-parameters
+    models: ``diagonal_weight`` equals slot 0 of ``get_rates`` on random
+    configurations, and the diagonal is not constant."""
+    rng = np.random.default_rng(0)
+    pairs = [(i, j) for i in range(6) for j in range(i + 1, 6)]
+    n = len(pairs)
+    jx = -rng.uniform(0.6, 1.2, n)
+    S = P.SpinHalf.create(pairs, J_x=jx, J_y=jx + rng.uniform(0.05, 0.4, n), J_z=rng.uniform(-1, 1, n),
+                          h_z=-rng.uniform(-1, 1, 6), h_x=rng.uniform(0.1, 0.6, 6), dtype=np.float64)
+    rng = np.random.default_rng(2)
+    B = P.BoseHubbard.create(pairs, t=rng.uniform(0.2, 1.0, n), eta=rng.uniform(0.2, 1.0, n), U=1.3,
+                             mu=-0.4, n_max=2, dtype=np.float64)
+    for H in (S, B):
+        vals = np.asarray(H.local_hilbert_space)
+        x = np.random.default_rng(1234).choice(vals, size=(512, H.N))
+        fast = np.asarray(H.diagonal_weight(x), np.float64)
+        slow = np.array([H.get_rates(c)[0][0] for c in x])
+        assert np.ptp(slow) > 0
+        np.testing.assert_allclose(fast, slow, rtol=0, atol=1e-12)
