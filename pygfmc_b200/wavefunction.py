@@ -157,7 +157,9 @@ class JastrowBoseHubbard:
     float32 build) -- the policy of PyGFMC's incremental mode
     (engine/evolution.py:167,181-189) -- so its
     ratios agree with both of PyGFMC's modes to rounding, not bit for bit
-    with either.
+    with either.  The host methods of that mode (``init_state``,
+    ``update_state``, the ``state=`` argument) exist for code that drives
+    them itself.
     """
 
     def __init__(self, N, pairs, beta, h=None, d=None, dtype=np.float32, incremental=False):
@@ -206,18 +208,58 @@ class JastrowBoseHubbard:
         return out + (h * n).sum(-1)
 
     def log_diff_from_operator(self, config, op, cache=None, state=None):
-        if not isinstance(op, BoseHubbard):
-            raise TypeError(f"{type(self).__name__} evaluates ratios for a BoseHubbard operator; "
-                            f"got {type(op).__name__}")
+        """log psi(x') - log psi(x) for every transition of ``op`` (entry 0:
+        0), from the successor configurations (jastrow_bose_hubbard.py
+        log_diff_from_operator:253-286, whose non-BoseHubbard branch does the
+        same).  ``state`` (the incremental neighbour sums) is accepted and
+        not needed: the ratios come from log_psi directly."""
         n = np.asarray(config, dtype=np.float64)
         base = self.log_psi(n)
-        out = np.zeros(op.M_total)
-        for k in range(1, op.M_total):
-            out[k] = self.log_psi(op.generate_state(n, k)) - base
-        return out
+        if isinstance(op, BoseHubbard):
+            out = np.zeros(op.M_total)
+            for k in range(1, op.M_total):
+                out[k] = self.log_psi(op.generate_state(n, k)) - base
+            return out
+        _, succ = op.get_rates(n, return_configs=True)
+        return self.log_psi(np.asarray(succ, np.float64)) - base
 
     def build_cache(self, op):
         return None
+
+    def _pair_weight(self):
+        """Weight of each pair in the neighbour sums: -beta, or 1 for a tied
+        beta (whose value then scales the sums)."""
+        if np.ndim(self._beta) == 0:
+            return np.ones(len(self.pair_i))
+        return -np.asarray(self._beta, np.float64)
+
+    def init_state(self, config, cache=None):
+        """The incremental mode's per-walker state (jastrow_bose_hubbard.py
+        init_state:230-235): the weighted neighbour sums
+        S_a = sum over the pairs (a, b) of w_ab x_b, shape (N,)."""
+        n = np.asarray(config, dtype=np.float64)
+        w = self._pair_weight()
+        s = np.zeros(self.N)
+        np.add.at(s, self.pair_i, w * n[self.pair_j])
+        np.add.at(s, self.pair_j, w * n[self.pair_i])
+        return s
+
+    def update_state(self, state, config, sites, deltas, cache=None):
+        """``state`` after the move that adds ``deltas`` to ``sites`` (the
+        form ``BoseHubbard.move`` returns; update_state:237-251): every
+        partner q of a moved site s gains w_sq delta_s."""
+        s = np.array(state, dtype=np.float64, copy=True)
+        if len(self.pair_i) == 0:
+            return s
+        w = self._pair_weight()
+        for k in range(2):
+            site, dk = int(sites[k]), float(deltas[k])
+            if dk == 0.0:
+                continue
+            on_i, on_j = self.pair_i == site, self.pair_j == site
+            np.add.at(s, self.pair_j[on_i], w[on_i] * dk)
+            np.add.at(s, self.pair_i[on_j], w[on_j] * dk)
+        return s
 
 
 def round_bf16(x):

@@ -109,3 +109,65 @@ def test_diagonal_weight_is_the_first_rate():
         slow = np.array([H.get_rates(c)[0][0] for c in x])
         assert np.ptp(slow) > 0
         np.testing.assert_allclose(fast, slow, rtol=0, atol=1e-12)
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_incremental_state_follows_the_moves(form):
+    """tests/core/test_jastrow_bose_hubbard.py:69-90: the neighbour sums
+    updated through 200 random moves (``BoseHubbard.move``) equal a rebuild to
+    rounding, and the ratios with that state equal the plain ones."""
+    H = P.BoseHubbard.create(EDGES, dtype=np.float64, **MODELS["all"])
+    G = P.JastrowBoseHubbard(L, PAIRS, dtype=np.float64, incremental=True, **FORMS[form])
+    rng = np.random.default_rng(5)
+    x = rng.integers(0, int(H.n_max) + 1, L).astype(np.float64)
+    state = G.init_state(x)
+    for _ in range(200):
+        idx = int(rng.integers(0, H.M_total))
+        sites, deltas = H.move(x, idx)
+        state = G.update_state(state, x, sites, deltas)
+        x = H.generate_state(x, idx)
+    np.testing.assert_allclose(state, G.init_state(x), rtol=0, atol=1e-12)
+    np.testing.assert_array_equal(G.log_diff_from_operator(x, H, state=state),
+                                  G.log_diff_from_operator(x, H))
+
+
+def test_incremental_update_without_pairs_is_a_no_op():
+    H = P.BoseHubbard.create(EDGES, dtype=np.float64, **MODELS["all"])
+    G = P.JastrowBoseHubbard(L, np.zeros((0, 2), dtype=np.int64), beta=0.3, d=0.2, incremental=True)
+    x = np.random.default_rng(1).integers(0, int(H.n_max) + 1, L).astype(np.float64)
+    state = G.init_state(x)
+    assert state.shape == (L,) and not np.any(state)
+    sites, deltas = H.move(x, 1)
+    np.testing.assert_array_equal(G.update_state(state, x, sites, deltas), state)
+
+
+def test_a_wrong_coupling_is_detected():
+    """Non-vacuity of the ratio checks: the opposite beta disagrees."""
+    H = P.BoseHubbard.create(EDGES, dtype=np.float64, **MODELS["all"])
+    good = P.JastrowBoseHubbard(L, PAIRS, beta=0.21, h=0.13, d=0.37, dtype=np.float64)
+    bad = P.JastrowBoseHubbard(L, PAIRS, beta=-0.21, h=0.13, d=0.37, dtype=np.float64)
+    x = np.array([2, 0, 1, 1, 2, 0, 1, 2, 1], dtype=np.float64)
+    rates, succ = H.get_rates(x, return_configs=True)
+    ref = np.array([good.log_psi(s) for s in succ]) - good.log_psi(x)
+    assert np.max(np.abs(bad.log_diff_from_operator(x, H) - ref)) > 0.1
+
+
+def test_parameters_keep_their_form_and_bad_shapes_raise():
+    """tests/core/test_jastrow_bose_hubbard.py:115-135: tied parameters stay
+    0-d, per-pair / per-site ones stay arrays, an absent h reads as zeros;
+    wrong lengths and a missing beta raise."""
+    g = P.JastrowBoseHubbard(L, PAIRS, beta=0.5)
+    assert np.ndim(g._beta) == 0 and g._h is None and g._d is None
+    g = P.JastrowBoseHubbard(L, PAIRS, beta=0.1, h=0.2, d=0.5)
+    assert (np.ndim(g._beta), np.ndim(g._h), np.ndim(g._d)) == (0, 0, 0)
+    g = P.JastrowBoseHubbard(L, PAIRS, **FORMS["per pair / per site"])
+    assert (g._beta.shape, g._h.shape, g._d.shape) == ((len(PAIRS),), (L,), (L,))
+    g = P.JastrowBoseHubbard(L, PAIRS, beta=0.1, d=0.5)
+    assert g._h is None and np.all(g.h == 0.0)
+    assert np.allclose(g.beta, 0.1) and g.beta.shape == (len(PAIRS),)
+    with pytest.raises(ValueError):
+        P.JastrowBoseHubbard(L, PAIRS, beta=0.1, d=np.ones(L + 1))
+    with pytest.raises(ValueError):
+        P.JastrowBoseHubbard(L, PAIRS, beta=np.ones(L))
+    with pytest.raises(ValueError):
+        P.JastrowBoseHubbard(L, PAIRS, beta=None)
