@@ -144,3 +144,34 @@ def test_arguments(golden):
     with pytest.warns(UserWarning, match="few"):
         evaluate_observables(raw, n_blocks=10)
     assert P.evaluate_observables is evaluate_observables
+
+
+@pytest.mark.parametrize("trim", [0, 4])
+def test_off_diagonal_windows_on_an_irregular_grid(trim):
+    """tests/core/test_estimator_window_reuse.py:8-33: rows measured at
+    irregular main-chain steps, three operators, three windows; each estimate
+    equals the explicit sum over usable rows of bra x exp(norm) x value over
+    the sum of bra x ket (bra: the m weights before the row's step, ket: the
+    m after), rows with k < p + max(0, trim - m) or k >= n - m left out."""
+    rng = np.random.default_rng(19)
+    n, windows = 40, [2, 4, 8]
+    steps = np.array([0, 2, 3, 6, 9, 10, 15, 18, 24, 31, 35, 39])
+    names = ["first", "second", "third"]
+    lw = rng.normal(0, 0.1, n)
+    values = rng.normal(size=(len(steps), len(names), len(windows)))
+    norms = rng.normal(0, 0.1, values.shape)
+    got = off_diagonal_estimates(windows, [p // 2 for p in windows], lw,
+                                 {nm: values[:, i] for i, nm in enumerate(names)},
+                                 {nm: norms[:, i] for i, nm in enumerate(names)}, steps, trim)
+    for j, p in enumerate(windows):
+        m = p // 2
+        for i, nm in enumerate(names):
+            num = den = 0.0
+            for row, k in enumerate(steps):
+                if k < p + max(0, trim - m) or k >= n - m:
+                    continue
+                bra = np.exp(lw[k - m + 1:k + 1].sum())
+                ket = np.exp(lw[k + 1:k + m + 1].sum())
+                num += bra * np.exp(norms[row, i, j]) * values[row, i, j]
+                den += bra * ket
+            assert got[nm][p] == pytest.approx(num / den, abs=1e-14)
