@@ -49,8 +49,11 @@ def _uniforms(key, n):
 
 
 def statistics(walkers, hamiltonian, step_size, guide, method, rng_key, avg_log_weight=None,
-               lam=None, M=10, quiet=False, m_array=None, precision=None, _engine=None):
-    """Diagnostic branching steps from ``walkers`` (see the module docstring).
+               lam=None, M=10, quiet=False, m_array=None, cache=None, precision=None,
+               _engine=None):
+    """Diagnostic branching steps from ``walkers`` (see the module docstring;
+    the signature of engine/estimators.py statistics:1139-1143, ``cache``
+    accepted and not needed, since the device builds its own tables).
     Returns ``(walkers_after, stats)`` with the reference's keys:
     n_unique_pre/post, unique_fraction, diag_min/max, changed_rate,
     overlap_rate, H_diag_max/min_observed, escape_rate_* / hops_per_step_* /
