@@ -116,14 +116,14 @@ class JastrowSpinHalf:
         """(n_pairs, 2) pairs (min, max) in constructor order."""
         return np.stack([self._pair_site, self.site_other[self._pair_site, self._pair_slot]], axis=1)
 
-    def log_psi(self, config):
+    def log_psi(self, config, cache=None):
         x = np.asarray(config, dtype=np.float64)
         pr = self.pairs
         J = -self.beta.astype(np.float64)
         pair = (J * x[..., pr[:, 0]] * x[..., pr[:, 1]]).sum(-1)
         return pair + (self.h.astype(np.float64) * x).sum(-1)
 
-    def log_diff_from_configs(self, config, new_configs):
+    def log_diff_from_configs(self, config, new_configs, cache=None):
         return self.log_psi(new_configs) - self.log_psi(config)
 
     def log_diff_from_operator(self, config, op, cache=None):
@@ -200,7 +200,7 @@ class JastrowBoseHubbard:
     def d(self):
         return np.zeros(self.N, self.dtype) if self._d is None else np.broadcast_to(self._d, (self.N,))
 
-    def log_psi(self, config):
+    def log_psi(self, config, cache=None):
         n = np.asarray(config, dtype=np.float64)
         d, beta, h = (np.asarray(v, np.float64) for v in (self.d, self.beta, self.h))
         out = -(d * n * n).sum(-1)
@@ -317,13 +317,13 @@ class RBMSpinHalf:
         s = np.asarray(config, dtype=np.float64)
         return s @ self.W.astype(np.float64).T + self.b.astype(np.float64)
 
-    def log_psi(self, config):
+    def log_psi(self, config, cache=None):
         s = np.asarray(config, dtype=np.float64)
         t = self.theta(s)
         lc = np.abs(t) + np.log1p(np.exp(-2.0 * np.abs(t))) - np.log(2.0)
         return lc.sum(-1) + s @ self.a.astype(np.float64)
 
-    def log_diff_from_configs(self, config, new_configs):
+    def log_diff_from_configs(self, config, new_configs, cache=None):
         return self.log_psi(new_configs) - self.log_psi(config)
 
     def log_diff_from_operator(self, config, op, cache=None):
@@ -382,7 +382,7 @@ class MLPBoseHubbard:
         self.b2 = np.broadcast_to(np.asarray(0.0 if b2 is None else b2, np.float32), (H2,)).copy()
         self.b3 = float(np.float32(b3))
 
-    def log_psi(self, config):
+    def log_psi(self, config, cache=None):
         n = np.asarray(config, dtype=np.float64)
         idx = np.arange(self.N) * (self.n_max + 1) + n.astype(np.int64)
         z1 = self.W1.astype(np.float64)[:, idx].sum(-1).T if n.ndim > 1 else \
@@ -392,7 +392,7 @@ class MLPBoseHubbard:
         h2 = np.tanh(h1 @ self.W2.astype(np.float64).T + self.b2.astype(np.float64))
         return h2 @ self.w3.astype(np.float64) + self.b3
 
-    def log_diff_from_configs(self, config, new_configs):
+    def log_diff_from_configs(self, config, new_configs, cache=None):
         return self.log_psi(new_configs) - self.log_psi(config)
 
 
@@ -463,7 +463,7 @@ class ExactGroundState:
         digit = np.argmin(np.abs(c[..., None] - np.asarray(self.local_hilbert_space)), axis=-1)
         return digit.astype(np.int64) @ np.asarray(self._powers, dtype=np.int64)
 
-    def log_psi(self, config):
+    def log_psi(self, config, cache=None):
         return self.log_amp[self.basis_index(config)]
 
     def log_diff_from_configs(self, config, new_configs=None, cache=None):

@@ -461,3 +461,29 @@ def test_is_valid_k():
         a = P.hamiltonian.SzSzStructureFactor(pos, k[None], dtype=np.float64).diagonal_weight(x)
         b = P.hamiltonian.SzSzStructureFactor(shifted, k[None], dtype=np.float64).diagonal_weight(x)
         assert (np.max(np.abs(a - b)) < 1e-9) == same
+
+
+def test_three_ratio_routines_agree():
+    """tests/core/test_guides.py:144-165: log_diff_from_operator,
+    log_diff_from_configs and log_psi give the same log-ratios, each called
+    as PyGFMC's engine calls them (the optional cache argument passed)."""
+    e = P.chain(8).edges
+    H = P.SpinHalf.create(e, J_x=-1.0, J_y=-1.0, J_z=1.0, h_x=0.4, dtype=np.float64)
+    guides = [P.JastrowSpinHalf(8, e, beta=0.3, h=0.05, dtype=np.float64),
+              P.RBMSpinHalf(8, 12, seed=1, sigma=0.3), P.ExactGroundState(H, dtype=np.float64)]
+    rng = np.random.default_rng(3)
+    for g in guides:
+        cache = g.build_cache(H) if hasattr(g, "build_cache") else None
+        for _ in range(3):
+            x = rng.choice([-1.0, 1.0], size=8)
+            _, succ = H.get_rates(x, return_configs=True)
+            from_cfg = np.asarray(g.log_diff_from_configs(x, succ, None), np.float64)
+            if hasattr(g, "log_diff_from_operator"):
+                from_op = np.asarray(g.log_diff_from_operator(x, H, cache), np.float64)
+                np.testing.assert_allclose(from_op[1:], from_cfg[1:], rtol=0, atol=1e-10,
+                                           err_msg=type(g).__name__)
+            if hasattr(g, "log_psi"):
+                base = g.log_psi(x, None)
+                want = np.array([g.log_psi(c, None) - base for c in succ])
+                np.testing.assert_allclose(from_cfg[1:], want[1:], rtol=0, atol=1e-10,
+                                           err_msg=type(g).__name__)
