@@ -263,7 +263,10 @@ def evaluate_observables(raw, p_array=None, n_blocks=None):
         if raw.get("off_diag_steps") is None or off_norm is None:
             raise ValueError("off_diag_steps and off_diag_norm are required whenever off_diag is "
                              "supplied.")
-        off_steps = np.asarray(raw["off_diag_steps"], dtype=np.int64)
+        steps_in = np.asarray(raw["off_diag_steps"])
+        if steps_in.dtype.kind == "f" and not np.array_equal(steps_in, np.rint(steps_in)):
+            raise ValueError("off_diag_steps must be integer-valued main-chain steps.")
+        off_steps = steps_in.astype(np.int64)
         rows = {len(v) for v in off.values()} | {len(v) for v in off_norm.values()}
         if rows != {len(off_steps)} or np.any(np.diff(off_steps) <= 0) or \
                 (len(off_steps) and (off_steps[0] < 0 or off_steps[-1] >= n)):

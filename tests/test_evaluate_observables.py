@@ -139,6 +139,10 @@ def test_arguments(golden):
         evaluate_observables({**raw, "p_array": [2, 4, 8]})
     with pytest.raises(ValueError, match="off_diag_steps"):
         evaluate_observables({**raw, "off_diag_steps": None})
+    with pytest.raises(ValueError, match="integer-valued"):
+        evaluate_observables({**raw, "off_diag_steps": np.arange(300) + 0.5})
+    with pytest.raises(ValueError, match="increasing"):
+        evaluate_observables({**raw, "off_diag_steps": np.arange(300)[::-1].copy()})
     with pytest.raises(ValueError, match="at least 2 usable blocks"):
         evaluate_observables(raw, n_blocks=1)
     with pytest.warns(UserWarning, match="few"):
