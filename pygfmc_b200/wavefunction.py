@@ -141,6 +141,68 @@ class JastrowSpinHalf:
         require_spin_half_layout(op, type(self).__name__)
         return None
 
+    def save(self, path, group="jastrow_spin_half", **attrs):
+        """Write the guide (jastrow_spin_half.py save:192-224): the pairs in
+        constructor order, beta (0-d when tied, else per pair) and h (absent,
+        0-d or per site) in the form they were given, N, and the keyword
+        arguments as scalar attributes.  h5py is not available to this
+        package, so the container is a NumPy ``.npz`` archive with the names
+        ``<group>/<name>`` and ``<group>/attrs/<name>``, written at ``path``."""
+        d = {f"{group}/pairs": self.pairs.astype(np.int32), f"{group}/beta": -np.asarray(self._J),
+             f"{group}/attrs/N": np.asarray(self.N)}
+        if self._h is not None:
+            d[f"{group}/h"] = np.asarray(self._h)
+        _put_attrs(d, group, attrs)
+        with open(path, "wb") as f:
+            np.savez(f, **d)
+
+    @classmethod
+    def load(cls, path, hamiltonian=None, group="jastrow_spin_half", dtype=np.float32):
+        """A guide written by :meth:`save` (jastrow_spin_half.py load:226-266).
+        With ``hamiltonian`` the site count is the largest of the saved N,
+        the Hamiltonian's N and its highest edge index + 1, and a per-site h
+        is padded with zeros to it."""
+        with np.load(path, allow_pickle=False) as z:
+            if f"{group}/pairs" not in z.files:
+                raise KeyError(f"{path} holds no JastrowSpinHalf group {group!r}")
+            pairs = np.asarray(z[f"{group}/pairs"], dtype=np.int64)
+            beta = np.asarray(z[f"{group}/beta"])
+            h = np.asarray(z[f"{group}/h"]) if f"{group}/h" in z.files else None
+            N = int(z[f"{group}/attrs/N"])
+        if hamiltonian is not None:
+            edges = np.asarray(getattr(hamiltonian, "edges", np.zeros((0, 2))))
+            N = max(N, int(edges.max(initial=-1)) + 1, int(hamiltonian.N))
+            if h is not None and h.ndim == 1 and h.shape[0] < N:
+                h = np.concatenate([h, np.zeros(N - h.shape[0], dtype=h.dtype)])
+        return cls(N, pairs, float(beta) if beta.ndim == 0 else beta,
+                   h=None if h is None else (float(h) if h.ndim == 0 else h), dtype=dtype)
+
+    @classmethod
+    def from_jax(cls, dtype, N, site_other, site_J, site_valid_mask, h, pair_site, pair_slot,
+                 site_pair):
+        """A guide from its stored arrays, bypassing the constructor
+        (jastrow_spin_half.py from_jax:267-286): ``site_J`` is the coupling
+        J = -beta as stored (0-d when tied, else per pair), ``h`` None / 0-d /
+        per site, ``pair_site`` / ``pair_slot`` locate each pair in the
+        per-site tables."""
+        obj = object.__new__(cls)
+        obj.dtype, obj.N = np.dtype(dtype), int(N)
+        obj.site_other = np.asarray(site_other)
+        obj._J = np.asarray(site_J)
+        obj.site_valid_mask = np.asarray(site_valid_mask, dtype=bool)
+        obj._h = None if h is None else np.asarray(h)
+        obj._pair_site, obj._pair_slot = np.asarray(pair_site), np.asarray(pair_slot)
+        obj._site_pair = np.asarray(site_pair)
+        return obj
+
+
+def _put_attrs(d, group, attrs):
+    """Scalar attributes into a save dict under ``<group>/attrs/``."""
+    for k, v in attrs.items():
+        if np.ndim(v) != 0:
+            raise ValueError(f"attribute {k!r} must be a scalar")
+        d[f"{group}/attrs/{k}"] = np.asarray(v)
+
 
 class JastrowBoseHubbard:
     """log psi_T(x) = -sum_pairs beta_ij x_i x_j + sum_i h_i x_i - sum_i d_i x_i^2.
@@ -260,6 +322,40 @@ class JastrowBoseHubbard:
             np.add.at(s, self.pair_j[on_i], w[on_i] * dk)
             np.add.at(s, self.pair_i[on_j], w[on_j] * dk)
         return s
+
+    def save(self, path, group="jastrow_bose_hubbard", **attrs):
+        """Write the guide (jastrow_bose_hubbard.py save:290-304): the pairs,
+        beta, h and d in the form they were given (absent, 0-d or per pair /
+        site), N, the incremental flag and the keyword arguments as scalar
+        attributes, in a NumPy ``.npz`` archive written at ``path`` (names
+        ``<group>/<name>``, ``<group>/attrs/<name>``)."""
+        d = {f"{group}/pairs": np.stack([self.pair_i, self.pair_j], axis=1).astype(np.int32),
+             f"{group}/attrs/N": np.asarray(self.N),
+             f"{group}/attrs/incremental": np.asarray(int(self.incremental))}
+        for name in ("beta", "h", "d"):
+            v = getattr(self, "_" + name)
+            if v is not None:
+                d[f"{group}/{name}"] = np.asarray(v)
+        _put_attrs(d, group, attrs)
+        with open(path, "wb") as f:
+            np.savez(f, **d)
+
+    @classmethod
+    def load(cls, path, group="jastrow_bose_hubbard", dtype=np.float32):
+        """A guide written by :meth:`save` (jastrow_bose_hubbard.py
+        load:306-316), every parameter back in its saved form."""
+        with np.load(path, allow_pickle=False) as z:
+            if f"{group}/pairs" not in z.files:
+                raise KeyError(f"{path} holds no JastrowBoseHubbard group {group!r}")
+            pairs = np.asarray(z[f"{group}/pairs"], dtype=np.int64)
+            p = {}
+            for name in ("beta", "h", "d"):
+                v = np.asarray(z[f"{group}/{name}"]) if f"{group}/{name}" in z.files else None
+                p[name] = None if v is None else (float(v) if v.ndim == 0 else v)
+            N = int(z[f"{group}/attrs/N"])
+            inc = bool(int(z[f"{group}/attrs/incremental"])) if f"{group}/attrs/incremental" in z.files \
+                else False
+        return cls(N, pairs, p["beta"], h=p["h"], d=p["d"], dtype=dtype, incremental=inc)
 
 
 def round_bf16(x):
