@@ -667,10 +667,31 @@ def kagome(Lx: int, Ly: int, periodic: bool = True) -> Lattice:
                 edges.add((min(i, j), max(i, j)))
     pos = np.array([x * a1 + y * a2 + basis[b] for y in range(Ly) for x in range(Lx)
                     for b in range(3)])
+    # one hexagon per cell, centred at the cell origin + (a1 + a2) / 2: its
+    # corners are the sites at distance 1 from the centre (in this cell and
+    # the cells +a1, +a2), listed counter-clockwise from angle 0; an open
+    # lattice keeps the hexagons whose corners all lie inside it
+    hexagons, centres = [], []
+    for y in range(Ly):
+        for x in range(Lx):
+            c = x * a1 + y * a2 + (a1 + a2) / 2
+            corners = []
+            for dx, dy, b in itertools.product((0, 1), (0, 1), range(3)):
+                r = (x + dx) * a1 + (y + dy) * a2 + basis[b]
+                if np.isclose(np.linalg.norm(r - c), 1.0, atol=1e-9):
+                    ang = np.arctan2(r[1] - c[1], r[0] - c[0]) % (2 * np.pi)
+                    corners.append((round(ang, 9) % round(2 * np.pi, 9), x + dx, y + dy, b))
+            if not periodic and any(cx >= Lx or cy >= Ly for _, cx, cy, _ in corners):
+                continue
+            corners.sort()
+            hexagons.append([3 * ((cx % Lx) + Lx * (cy % Ly)) + b for _, cx, cy, b in corners])
+            centres.append(c)
     return Lattice(name="kagome", N=3 * Lx * Ly, edges=sorted(edges),
                    extras=dict(positions=pos, primitive_vectors=np.array([a1, a2]),
                                supercell_dims=np.array([Lx, Ly]), sublattice_offsets=basis,
-                               torus=np.array([Lx * a1, Ly * a2])))
+                               torus=np.array([Lx * a1, Ly * a2]),
+                               hexagons=np.array(hexagons, dtype=np.int32).reshape(-1, 6),
+                               hexagon_centers=np.array(centres, dtype=np.float64).reshape(-1, 2)))
 
 
 # ---------------------------------------------------------------------------

@@ -4,7 +4,8 @@ Source: PyGFMC's ``codes/pygfmc/hamiltonian/lattice.py``, which needs only
 numpy and is loaded on its own from the given path (without importing the
 pygfmc package, which needs jax).  For each case the fixture holds the edge
 list (sorted (i < j) pairs, the order that fixes the transition slots of a
-Hamiltonian built on it) and the site positions.  Run from the repository
+Hamiltonian built on it), the site positions and, for kagome, the hexagonal
+loops with their centres.  Run from the repository
 root with the path of PyGFMC's file:
 
     python tests/golden/make_lattice_golden.py <PyGFMC>/codes/pygfmc/hamiltonian/lattice.py
@@ -44,6 +45,10 @@ def main(src):
         pos = lat.extras.get("positions") if lat.extras else None
         if pos is not None:
             out[f"{name}/positions"] = np.asarray(pos, dtype=np.float64)
+        if fn == "kagome":                  # the hexagonal loops, one per cell
+            out[f"{name}/hexagons"] = np.asarray(lat.extras["hexagons"], dtype=np.int32).reshape(-1, 6)
+            out[f"{name}/hexagon_centers"] = np.asarray(lat.extras["hexagon_centers"],
+                                                        dtype=np.float64).reshape(-1, 2)
     np.savez_compressed(OUT, **out)
     print(f"wrote {OUT}: {len(CASES)} lattices")
 

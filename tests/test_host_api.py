@@ -167,6 +167,10 @@ def test_lattices_match_the_reference_fixture(name, fn, args, periodic):
     assert lat.edges == [tuple(e) for e in z[f"{name}/edges"].tolist()]
     if f"{name}/positions" in z.files:
         np.testing.assert_allclose(lat.extras["positions"], z[f"{name}/positions"], rtol=0, atol=1e-14)
+    if f"{name}/hexagons" in z.files:                  # kagome: one loop per cell, CCW from angle 0
+        np.testing.assert_array_equal(lat.extras["hexagons"], z[f"{name}/hexagons"])
+        np.testing.assert_allclose(lat.extras["hexagon_centers"], z[f"{name}/hexagon_centers"],
+                                   rtol=0, atol=1e-14)
 
 
 def test_protocol_classes():
